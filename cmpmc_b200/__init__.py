@@ -1,0 +1,17 @@
+"""cmpmc_b200 -- CMPMC's phonon / charge transport path on NVIDIA B200 (sm_100a).
+
+The public API mirrors the reference's C++ API (run_events, SimulationEngine,
+CrystalLattice, DetectorModel, ...); the work runs in hand-written CUDA kernels behind
+the C ABI in include/cmpmc_gpu.h.
+"""
+from .api import (AluminumFilm, CmpmcError, CrystalConfig, CrystalLattice, CylinderSolid, DetectorModel,
+                  EventInput, ExcitationType, KaplanFilm, PackedEvents, PhononMode, Rng, RunOptions, RunResult,
+                  SimStats, SimulationEngine, SuperconductorFilmConfig, SurfaceId, SurfaceProperty,
+                  UniformElectricField, UnvalidatedModuleError, Workload, materials, run_events, units, workloads)
+
+__all__ = [
+    "AluminumFilm", "CmpmcError", "CrystalConfig", "CrystalLattice", "CylinderSolid", "DetectorModel", "EventInput",
+    "ExcitationType", "KaplanFilm", "PackedEvents", "PhononMode", "Rng", "RunOptions", "RunResult", "SimStats",
+    "SimulationEngine", "SuperconductorFilmConfig", "SurfaceId", "SurfaceProperty", "UniformElectricField",
+    "UnvalidatedModuleError", "Workload", "materials", "run_events", "units", "workloads",
+]

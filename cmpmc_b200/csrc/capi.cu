@@ -1,0 +1,425 @@
+// capi.cu -- device context and the run_events entry point of the C ABI.
+//
+// cmpmc_gpu_run_events is the device half of run_events (transport/parallel.hpp:76-148):
+// the caller has already run the generator on the host (one Rng::for_stream(seed, ev)
+// per event) and passes each event's post-generator Rng state with its initial stacks.
+// The call uploads them (unless they are already on the device), runs the transport
+// kernel, then the merge kernels (hit_offsets scan, hit scatter into event order, stats
+// reduction), and returns RunResult's content. Buffers grow on demand and are reused
+// across calls; a capacity overflow reruns the (deterministic) transport with more room.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "device.cuh"
+#include "internal.hpp"
+
+using namespace cmpmc_gpu;
+
+namespace {
+
+thread_local std::string g_create_error;
+thread_local int g_create_status = CMPMC_OK;
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = std::max<size_t>(bytes + bytes / 8, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct HostBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = std::max<size_t>(bytes + bytes / 8, 256);
+        cudaError_t e = cudaMallocHost(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct Counters {
+    unsigned long long hit_count;
+    unsigned long long next_work;
+    unsigned err;
+    unsigned pad;
+};
+
+}  // namespace
+
+struct cmpmc_gpu_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    cmpmc_crystal_config cfg{};
+    cmpmc_detector det{};
+    Lattice L{};
+    Detector D{};
+    DevBuf tables;  // oct LUT + CDF tables
+    int tpb = 128;
+    int bps = 0;  // 0: occupancy-derived
+    uint32_t stack_cap = 1024;
+    uint32_t cstack_cap = 64;
+    uint64_t hit_cap = 0;
+    DevBuf in_rng, in_inj, in_phoff, in_ph, in_choff, in_ch;
+    DevBuf stack, cstack, hit_stage, hit_key, counters, ev_stats, ev_nhits, offsets, hits_out, total;
+    HostBuf h_hits, h_offsets, h_evstats, h_total, h_counters;
+    cudaEvent_t e_start = nullptr, e_k0 = nullptr, e_k1 = nullptr, e_end = nullptr;
+    std::string last_error;
+    int last_status = CMPMC_OK;
+};
+
+namespace {
+
+int fail(cmpmc_gpu_ctx* ctx, int status, const std::string& msg) {
+    if (ctx) {
+        ctx->last_error = msg;
+        ctx->last_status = status;
+    } else {
+        g_create_error = msg;
+        g_create_status = status;
+    }
+    return status;
+}
+
+int cuda_fail(cmpmc_gpu_ctx* ctx, cudaError_t e, const char* what) {
+    return fail(ctx, CMPMC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                     \
+    do {                                                   \
+        cudaError_t _e = (call);                           \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); \
+    } while (0)
+
+}  // namespace
+
+extern "C" {
+
+int cmpmc_gpu_device_count(int* count) {
+    int n = 0;
+    const cudaError_t e = cudaGetDeviceCount(&n);
+    if (count) *count = (e == cudaSuccess) ? n : 0;
+    return (e == cudaSuccess && n > 0) ? CMPMC_OK : CMPMC_ERR_NO_DEVICE;
+}
+
+int cmpmc_gpu_create(const cmpmc_lattice* lat, const cmpmc_detector* det, int device, cmpmc_gpu_ctx** out) {
+    cmpmc_gpu_ctx* ctx = nullptr;
+    if (!out) return fail(nullptr, CMPMC_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!lat || !det) return fail(nullptr, CMPMC_ERR_INVALID, "lattice and detector are required");
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0)
+        return fail(nullptr, CMPMC_ERR_NO_DEVICE, "no CUDA device is visible");
+    if (device < 0 || device >= n_dev) return fail(nullptr, CMPMC_ERR_INVALID, "device index out of range");
+    std::string err;
+    const int st = validate_config(lat->cfg, *det, false, err);
+    if (st != CMPMC_OK) return fail(nullptr, st, err);
+
+    ctx = new cmpmc_gpu_ctx();
+    ctx->device = device;
+    ctx->cfg = lat->cfg;
+    ctx->det = *det;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->e_start);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->e_k0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->e_k1);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->e_end);
+    const size_t oct_bytes = lat->oct.size() * sizeof(OctEntry);
+    const size_t cdf_bytes = 2 * kNCdf * sizeof(double);
+    if (e == cudaSuccess) e = ctx->tables.ensure(oct_bytes + cdf_bytes);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(ctx->tables.p, lat->oct.data(), oct_bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(static_cast<char*>(ctx->tables.p) + oct_bytes, lat->cdf_lt.data(), kNCdf * sizeof(double),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(static_cast<char*>(ctx->tables.p) + oct_bytes + kNCdf * sizeof(double), lat->cdf_tt.data(),
+                       kNCdf * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        const std::string msg = std::string("context setup: ") + cudaGetErrorString(e);
+        cmpmc_gpu_destroy(ctx);
+        return fail(nullptr, CMPMC_ERR_CUDA, msg);
+    }
+    ctx->L = lat->view;
+    ctx->L.oct = static_cast<const OctEntry*>(ctx->tables.p);
+    ctx->L.cdf_lt = reinterpret_cast<const double*>(static_cast<char*>(ctx->tables.p) + oct_bytes);
+    ctx->L.cdf_tt = ctx->L.cdf_lt + kNCdf;
+    ctx->D = detector_view(*det);
+    // Keep the 3 MiB group-velocity table resident in L2 (it is gathered on every step).
+    cudaStreamAttrValue attr;
+    std::memset(&attr, 0, sizeof(attr));
+    attr.accessPolicyWindow.base_ptr = ctx->tables.p;
+    attr.accessPolicyWindow.num_bytes = oct_bytes + cdf_bytes;
+    attr.accessPolicyWindow.hitRatio = 1.0f;
+    attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    if (cudaStreamSetAttribute(ctx->stream, cudaStreamAttributeAccessPolicyWindow, &attr) != cudaSuccess)
+        (void)cudaGetLastError();  // optional: not every configuration grants a persisting L2 window
+    *out = ctx;
+    return CMPMC_OK;
+}
+
+void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (DevBuf* b : {&ctx->tables, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
+                      &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
+                      &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total})
+        b->release();
+    for (HostBuf* b : {&ctx->h_hits, &ctx->h_offsets, &ctx->h_evstats, &ctx->h_total, &ctx->h_counters})
+        b->release();
+    for (cudaEvent_t ev : {ctx->e_start, ctx->e_k0, ctx->e_k1, ctx->e_end})
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int cmpmc_gpu_last_error(const cmpmc_gpu_ctx* ctx, char* buf, size_t size) {
+    const std::string& m = ctx ? ctx->last_error : g_create_error;
+    const int st = ctx ? ctx->last_status : g_create_status;
+    if (buf && size) {
+        const size_t n = std::min(size - 1, m.size());
+        std::memcpy(buf, m.data(), n);
+        buf[n] = '\0';
+    }
+    return st;
+}
+
+int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_per_sm, uint64_t stack_capacity,
+                        uint64_t hit_capacity) {
+    if (!ctx) return CMPMC_ERR_INVALID;
+    if (threads_per_block < 0 || threads_per_block > 128 || (threads_per_block % 32) != 0 || blocks_per_sm < 0)
+        return fail(ctx, CMPMC_ERR_INVALID, "threads_per_block must be a multiple of 32 in [32, 128]");
+    if (threads_per_block) ctx->tpb = threads_per_block;
+    if (blocks_per_sm) ctx->bps = blocks_per_sm;
+    if (stack_capacity) ctx->stack_cap = static_cast<uint32_t>(std::min<uint64_t>(stack_capacity, 1u << 24));
+    if (hit_capacity) ctx->hit_cap = hit_capacity;
+    return CMPMC_OK;
+}
+
+int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_out* out) {
+    if (!ctx || !d || !out) return CMPMC_ERR_INVALID;
+    std::memset(out, 0, sizeof(*out));
+    ctx->last_status = CMPMC_OK;
+    ctx->last_error.clear();
+    const uint64_t n = d->n_events;
+    if (d->form != CMPMC_FORM_PLAIN_FP64 && d->form != CMPMC_FORM_BATCHED_FP32)
+        return fail(ctx, CMPMC_ERR_INVALID, "unknown transport form");
+    if (n > (1ull << 31)) return fail(ctx, CMPMC_ERR_INVALID, "too many events in one call");
+    if (n > 0 && (!d->rng_state || !d->injected_eV || !d->phonon_offsets))
+        return fail(ctx, CMPMC_ERR_INVALID, "rng_state, injected_eV and phonon_offsets are required");
+    const bool has_charges = d->charge_offsets != nullptr;
+    std::string err;
+    const int vst = validate_config(ctx->cfg, ctx->det, has_charges, err);
+    if (vst != CMPMC_OK) return fail(ctx, vst, err);
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = ctx->stream;
+    int launches = 0;
+
+    CK(cudaEventRecord(ctx->e_start, s), "event");
+    // ---- inputs ------------------------------------------------------------------
+    RunArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.n_events = n;
+    a.first_event = d->first_event;
+    a.keep_hits = d->keep_hits;
+    a.seed = d->seed;
+    uint64_t n_ph = 0, n_ch = 0;
+    if (d->inputs_on_device) {
+        a.rng_state = d->rng_state;
+        a.injected = d->injected_eV;
+        a.ph_off = d->phonon_offsets;
+        a.ph = d->phonons;
+        a.ch_off = d->charge_offsets;
+        a.ch = d->charges;
+    } else if (n > 0) {
+        n_ph = d->phonon_offsets[n];
+        n_ch = has_charges ? d->charge_offsets[n] : 0;
+        if ((n_ph && !d->phonons) || (n_ch && !d->charges))
+            return fail(ctx, CMPMC_ERR_INVALID, "track arrays are required for non-empty stacks");
+        CK(ctx->in_rng.ensure(n * 32), "alloc rng");
+        CK(ctx->in_inj.ensure(n * 8), "alloc injected");
+        CK(ctx->in_phoff.ensure((n + 1) * 8), "alloc offsets");
+        CK(ctx->in_ph.ensure(std::max<uint64_t>(n_ph, 1) * sizeof(cmpmc_phonon_track)), "alloc phonons");
+        CK(cudaMemcpyAsync(ctx->in_rng.p, d->rng_state, n * 32, cudaMemcpyHostToDevice, s), "copy rng");
+        CK(cudaMemcpyAsync(ctx->in_inj.p, d->injected_eV, n * 8, cudaMemcpyHostToDevice, s), "copy injected");
+        CK(cudaMemcpyAsync(ctx->in_phoff.p, d->phonon_offsets, (n + 1) * 8, cudaMemcpyHostToDevice, s), "copy offsets");
+        if (n_ph)
+            CK(cudaMemcpyAsync(ctx->in_ph.p, d->phonons, n_ph * sizeof(cmpmc_phonon_track), cudaMemcpyHostToDevice, s),
+               "copy phonons");
+        a.rng_state = ctx->in_rng.as<uint64_t>();
+        a.injected = ctx->in_inj.as<double>();
+        a.ph_off = ctx->in_phoff.as<uint64_t>();
+        a.ph = ctx->in_ph.as<cmpmc_phonon_track>();
+        if (has_charges) {
+            CK(ctx->in_choff.ensure((n + 1) * 8), "alloc charge offsets");
+            CK(ctx->in_ch.ensure(std::max<uint64_t>(n_ch, 1) * sizeof(cmpmc_charge_track)), "alloc charges");
+            CK(cudaMemcpyAsync(ctx->in_choff.p, d->charge_offsets, (n + 1) * 8, cudaMemcpyHostToDevice, s),
+               "copy charge offsets");
+            if (n_ch)
+                CK(cudaMemcpyAsync(ctx->in_ch.p, d->charges, n_ch * sizeof(cmpmc_charge_track),
+                                   cudaMemcpyHostToDevice, s),
+                   "copy charges");
+            a.ch_off = ctx->in_choff.as<uint64_t>();
+            a.ch = ctx->in_ch.as<cmpmc_charge_track>();
+        }
+    }
+
+    // ---- launch geometry and work buffers ------------------------------------------
+    const bool batched = d->form == CMPMC_FORM_BATCHED_FP32;
+    int bps = ctx->bps;
+    if (!bps) {
+        CK(batched ? batched_fp32_occupancy(ctx->tpb, &bps) : plain_fp64_occupancy(ctx->tpb, &bps), "occupancy");
+        bps = std::max(bps, 1);
+    }
+    uint64_t grid = static_cast<uint64_t>(ctx->num_sms) * bps;
+    const uint64_t per_thread_units = std::max<uint64_t>(n, 1);
+    grid = std::min<uint64_t>(grid, (per_thread_units + ctx->tpb - 1) / ctx->tpb);
+    grid = std::max<uint64_t>(grid, 1);
+    const uint64_t slots = grid * ctx->tpb;
+
+    CK(ctx->ev_stats.ensure(std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats)), "alloc event stats");
+    CK(ctx->ev_nhits.ensure(std::max<uint64_t>(n, 1) * 8), "alloc event hit counts");
+    CK(ctx->offsets.ensure((n + 1) * 8), "alloc hit offsets");
+    CK(ctx->counters.ensure(sizeof(Counters)), "alloc counters");
+    CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
+    CK(ctx->h_counters.ensure(sizeof(Counters)), "alloc host counters");
+    CK(ctx->cstack.ensure(slots * ctx->cstack_cap * sizeof(GCharge)), "alloc charge stacks");
+    a.cstack = ctx->cstack.as<GCharge>();
+    a.cstack_cap = ctx->cstack_cap;
+    a.ev_stats = ctx->ev_stats.as<cmpmc_sim_stats>();
+    a.ev_nhits = ctx->ev_nhits.as<uint64_t>();
+    Counters* dc = ctx->counters.as<Counters>();
+    a.hit_count = &dc->hit_count;
+    a.next_work = &dc->next_work;
+    a.err = &dc->err;
+
+    uint64_t hit_cap = ctx->hit_cap;
+    if (!hit_cap) {
+        const uint64_t units = d->inputs_on_device ? n : std::max<uint64_t>(n, n_ph + n_ch);
+        hit_cap = std::max<uint64_t>(4096, units * 32);
+    }
+    Counters hc{};
+    float kms = 0.0f;
+    for (int attempt = 0;; ++attempt) {
+        if (!d->keep_hits) hit_cap = 1;
+        CK(ctx->stack.ensure(slots * ctx->stack_cap * sizeof(GTrack)), "alloc phonon stacks");
+        CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
+        CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
+        a.stack = ctx->stack.as<GTrack>();
+        a.stack_cap = ctx->stack_cap;
+        a.hit_stage = ctx->hit_stage.as<cmpmc_sensor_hit>();
+        a.hit_key = ctx->hit_key.as<uint64_t>();
+        a.hit_cap = hit_cap;
+        CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s), "memset counters");
+        CK(cudaEventRecord(ctx->e_k0, s), "event");
+        if (n > 0) {
+            CK(batched ? launch_batched_fp32(ctx->L, ctx->D, a, static_cast<int>(grid), ctx->tpb, s)
+                       : launch_plain_fp64(ctx->L, ctx->D, a, static_cast<int>(grid), ctx->tpb, s),
+               "transport launch");
+            ++launches;
+        }
+        CK(cudaEventRecord(ctx->e_k1, s), "event");
+        CK(cudaMemcpyAsync(ctx->h_counters.p, ctx->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s),
+           "copy counters");
+        CK(cudaStreamSynchronize(s), "transport kernel");
+        hc = *ctx->h_counters.as<Counters>();
+        CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
+        const bool stack_over = (hc.err & (kErrPhononStack | kErrChargeStack)) != 0;
+        const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
+        if (!stack_over && !hits_over) break;
+        if (attempt >= 6) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack or hit buffer overflow persists");
+        if (hc.err & kErrPhononStack) ctx->stack_cap = std::min<uint32_t>(ctx->stack_cap * 4, 1u << 24);
+        if (hc.err & kErrChargeStack) {
+            ctx->cstack_cap *= 4;
+            CK(ctx->cstack.ensure(slots * ctx->cstack_cap * sizeof(GCharge)), "alloc charge stacks");
+            a.cstack = ctx->cstack.as<GCharge>();
+            a.cstack_cap = ctx->cstack_cap;
+        }
+        if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
+    }
+    if (d->keep_hits) ctx->hit_cap = std::max<uint64_t>(ctx->hit_cap, hit_cap);
+    if (hc.err) return fail(ctx, CMPMC_ERR_DEVICE, "transport kernel reported error word " + std::to_string(hc.err));
+
+    // ---- merge ------------------------------------------------------------------------
+    const uint64_t n_hits = d->keep_hits ? hc.hit_count : 0;
+    CK(ctx->hits_out.ensure(std::max<uint64_t>(n_hits, 1) * sizeof(cmpmc_sensor_hit)), "alloc hits");
+    if (n > 0) {
+        CK(launch_finish(a, ctx->offsets.as<uint64_t>(), ctx->hits_out.as<cmpmc_sensor_hit>(), n_hits,
+                         ctx->total.as<cmpmc_sim_stats>(), s, &launches),
+           "merge kernels");
+    } else {
+        CK(cudaMemsetAsync(ctx->offsets.p, 0, 8, s), "memset offsets");
+        CK(cudaMemsetAsync(ctx->total.p, 0, sizeof(cmpmc_sim_stats), s), "memset totals");
+    }
+    CK(ctx->h_total.ensure(sizeof(cmpmc_sim_stats)), "alloc host totals");
+    CK(cudaMemcpyAsync(ctx->h_total.p, ctx->total.p, sizeof(cmpmc_sim_stats), cudaMemcpyDeviceToHost, s),
+       "copy totals");
+    if (d->outputs_on_device) {
+        out->hits = ctx->hits_out.as<cmpmc_sensor_hit>();
+        out->hit_offsets = ctx->offsets.as<uint64_t>();
+        out->event_stats = d->want_event_stats ? ctx->ev_stats.as<cmpmc_sim_stats>() : nullptr;
+    } else {
+        CK(ctx->h_hits.ensure(std::max<uint64_t>(n_hits, 1) * sizeof(cmpmc_sensor_hit)), "alloc host hits");
+        CK(ctx->h_offsets.ensure((n + 1) * 8), "alloc host offsets");
+        if (n_hits)
+            CK(cudaMemcpyAsync(ctx->h_hits.p, ctx->hits_out.p, n_hits * sizeof(cmpmc_sensor_hit),
+                               cudaMemcpyDeviceToHost, s),
+               "copy hits");
+        CK(cudaMemcpyAsync(ctx->h_offsets.p, ctx->offsets.p, (n + 1) * 8, cudaMemcpyDeviceToHost, s), "copy offsets");
+        if (d->want_event_stats && n > 0) {
+            CK(ctx->h_evstats.ensure(n * sizeof(cmpmc_sim_stats)), "alloc host event stats");
+            CK(cudaMemcpyAsync(ctx->h_evstats.p, ctx->ev_stats.p, n * sizeof(cmpmc_sim_stats),
+                               cudaMemcpyDeviceToHost, s),
+               "copy event stats");
+        }
+        out->hits = ctx->h_hits.as<cmpmc_sensor_hit>();
+        out->hit_offsets = ctx->h_offsets.as<uint64_t>();
+        out->event_stats = d->want_event_stats ? ctx->h_evstats.as<cmpmc_sim_stats>() : nullptr;
+    }
+    CK(cudaEventRecord(ctx->e_end, s), "event");
+    CK(cudaStreamSynchronize(s), "merge kernels");
+    float tms = 0.0f;
+    CK(cudaEventElapsedTime(&tms, ctx->e_start, ctx->e_end), "event time");
+    out->stats = *ctx->h_total.as<cmpmc_sim_stats>();
+    out->n_hits = n_hits;
+    out->kernel_ms = kms;
+    out->total_ms = tms;
+    out->device_error = hc.err;
+    out->kernel_launches = static_cast<uint32_t>(launches);
+    return CMPMC_OK;
+}
+
+}  // extern "C"

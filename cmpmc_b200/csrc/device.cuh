@@ -1,0 +1,143 @@
+// device.cuh -- device-side data structures shared by the kernels and the context.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/cmpmc_gpu.h"
+#include "transport.cuh"
+
+namespace cmpmc_gpu {
+
+// error word bits written by the kernels (never a trap)
+enum : unsigned {
+    kErrPhononStack = 1u,
+    kErrChargeStack = 2u,
+    kErrQueue = 4u,
+};
+
+// A pushed phonon in a per-thread global-memory LIFO (112 B, 16-byte aligned)
+struct alignas(16) GTrack {
+    double px, py, pz, kx, ky, kz, vx, vy, vz, E, vmag, t, w;
+    uint32_t bounces;
+    int mode;
+};
+
+struct alignas(16) GCharge {
+    double px, py, pz, qx, qy, qz, ekin, t, w;
+    int valley, type;
+};
+
+// Per-event output record: SimStats of the event plus its hit count
+struct EventOut {
+    cmpmc_sim_stats st;
+};
+
+// Everything the transport kernels read or write for one run
+struct RunArgs {
+    uint64_t n_events;
+    uint64_t first_event;
+    const uint64_t* rng_state;        // [n][4]
+    const double* injected;           // [n]
+    const uint64_t* ph_off;           // [n+1]
+    const cmpmc_phonon_track* ph;     // initial phonons
+    const uint64_t* ch_off;           // [n+1] or nullptr
+    const cmpmc_charge_track* ch;     // initial charges
+    int keep_hits;
+    uint64_t seed;                    // substream seed of the batched form
+    // per-slot stacks
+    GTrack* stack;
+    uint32_t stack_cap;
+    GCharge* cstack;
+    uint32_t cstack_cap;
+    // hit staging: record + (event << 32 | index within event)
+    cmpmc_sensor_hit* hit_stage;
+    uint64_t* hit_key;
+    uint64_t hit_cap;
+    unsigned long long* hit_count;
+    unsigned long long* next_work;
+    // outputs
+    cmpmc_sim_stats* ev_stats;        // [n]
+    uint64_t* ev_nhits;               // [n]
+    unsigned* err;
+};
+
+CMPMC_HD GTrack pack_track(const Track& t) {
+    GTrack g;
+    g.px = t.pos.x; g.py = t.pos.y; g.pz = t.pos.z;
+    g.kx = t.k.x; g.ky = t.k.y; g.kz = t.k.z;
+    g.vx = t.vg.x; g.vy = t.vg.y; g.vz = t.vg.z;
+    g.E = t.E; g.vmag = t.vmag; g.t = t.t; g.w = t.w;
+    g.bounces = t.bounces;
+    g.mode = t.mode;
+    return g;
+}
+CMPMC_HD Track unpack_track(const GTrack& g) {
+    Track t;
+    t.pos = v3(g.px, g.py, g.pz);
+    t.k = v3(g.kx, g.ky, g.kz);
+    t.vg = v3(g.vx, g.vy, g.vz);
+    t.E = g.E; t.vmag = g.vmag; t.t = g.t; t.w = g.w;
+    t.bounces = g.bounces;
+    t.mode = g.mode;
+    return t;
+}
+CMPMC_HD Track track_from_input(const cmpmc_phonon_track& r) {
+    Track t;
+    t.pos = v3(r.pos[0], r.pos[1], r.pos[2]);
+    t.k = v3(r.k_dir[0], r.k_dir[1], r.k_dir[2]);
+    t.vg = v3(r.vg_dir[0], r.vg_dir[1], r.vg_dir[2]);
+    t.E = r.energy; t.vmag = r.vg_mag; t.t = r.time; t.w = r.weight;
+    t.bounces = r.bounces;
+    t.mode = r.mode;
+    return t;
+}
+CMPMC_HD Charge charge_from_input(const cmpmc_charge_track& r) {
+    Charge c;
+    c.pos = v3(r.pos[0], r.pos[1], r.pos[2]);
+    c.p = v3(r.p_eV[0], r.p_eV[1], r.p_eV[2]);
+    c.ekin = r.ekin; c.t = r.time; c.w = r.weight;
+    c.valley = r.valley;
+    c.type = r.type;
+    return c;
+}
+
+CMPMC_HD void stats_from_event(const EvStats& e, double injected, cmpmc_sim_stats& s) {
+    s.total_steps = e.total_steps;
+    s.isotope_scatters = e.isotope_scatters;
+    s.polycrystal_scatters = e.polycrystal_scatters;
+    s.decays_L_to_TT = e.decays_TT;
+    s.decays_L_to_LT = e.decays_LT;
+    s.surface_refls = e.surface_refls;
+    s.surface_downconversions = e.surface_downconversions;
+    s.sensor_hits = e.sensor_hits;
+    s.killed_tracks = e.killed_tracks;
+    s.charge_steps = e.charge_steps;
+    s.luke_phonons_emitted = e.luke_emitted;
+    s.intervalley_scatters = e.intervalley_scatters;
+    s.charges_trapped = e.charges_trapped;
+    s.trap_ionizations = e.trap_ionizations;
+    s.charge_surface_refls = e.charge_surface_refls;
+    s.charges_collected = e.charges_collected;
+    s.total_luke_phonon_eV = e.luke_eV;
+    s.charge_recomb_edep_eV = e.recomb_eV;
+    s.sc_pair_breakings = 0;
+    s.qp_diffusion_steps = 0;
+    s.qp_phonons_radiated = 0;
+    s.qp_recombinations = 0;
+    s.qp_local_traps = 0;
+    s.total_injected_eV = injected;
+    s.total_deposited_eV = e.deposited_eV;
+    s.escaped_or_killed_eV = e.escaped_eV;
+}
+
+// kernels (launch wrappers return the cudaError_t of the launch)
+cudaError_t launch_plain_fp64(const Lattice& L, const Detector& D, const RunArgs& a, int grid, int block,
+                              cudaStream_t s);
+cudaError_t plain_fp64_occupancy(int block, int* blocks_per_sm);
+cudaError_t launch_batched_fp32(const Lattice& L, const Detector& D, const RunArgs& a, int grid, int block,
+                                cudaStream_t s);
+cudaError_t batched_fp32_occupancy(int block, int* blocks_per_sm);
+cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
+                          cmpmc_sim_stats* total, cudaStream_t s, int* launches);
+
+}  // namespace cmpmc_gpu

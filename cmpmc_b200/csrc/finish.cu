@@ -1,0 +1,121 @@
+// finish.cu -- the merge step of run_events on the device (parallel.hpp:133-145):
+// per-event hit counts -> hit_offsets (exclusive scan), staged hits -> event order,
+// per-event SimStats -> run totals. All three are deterministic (fixed summation order).
+#include "device.cuh"
+
+namespace cmpmc_gpu {
+
+namespace {
+
+constexpr int kScanThreads = 1024;
+constexpr int kReduceThreads = 128;
+constexpr int kStatsWords = sizeof(cmpmc_sim_stats) / 8;
+
+// SimStats word kinds: doubles at 16, 17, 23, 24, 25 (engine.hpp:49-50, 60-62)
+__host__ __device__ constexpr bool stats_word_is_double(int i) {
+    return i == 16 || i == 17 || i == 23 || i == 24 || i == 25;
+}
+
+// Single-block chunked exclusive scan: thread t owns a contiguous slice of events.
+__global__ void __launch_bounds__(kScanThreads) k_scan(const uint64_t* __restrict__ counts, uint64_t n,
+                                                       uint64_t* __restrict__ offsets) {
+    __shared__ uint64_t part[kScanThreads];
+    const int t = threadIdx.x;
+    const uint64_t chunk = (n + kScanThreads - 1) / kScanThreads;
+    const uint64_t lo = min(n, t * chunk), hi = min(n, lo + chunk);
+    uint64_t s = 0;
+    for (uint64_t i = lo; i < hi; ++i) s += counts[i];
+    part[t] = s;
+    __syncthreads();
+    // Hillis-Steele inclusive scan over the 1024 partial sums
+    for (int d = 1; d < kScanThreads; d <<= 1) {
+        const uint64_t v = (t >= d) ? part[t - d] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint64_t run = part[t] - s;
+    if (t == 0) offsets[0] = 0;
+    for (uint64_t i = lo; i < hi; ++i) {
+        run += counts[i];
+        offsets[i + 1] = run;
+    }
+}
+
+__global__ void k_scatter(const cmpmc_sensor_hit* __restrict__ stage, const uint64_t* __restrict__ key,
+                          const unsigned long long* __restrict__ count, uint64_t stage_cap,
+                          const uint64_t* __restrict__ offsets, cmpmc_sensor_hit* __restrict__ out,
+                          uint64_t out_cap) {
+    const uint64_t n = min(static_cast<uint64_t>(*count), stage_cap);
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t k = key[i];
+        const uint64_t dst = offsets[k >> 32] + (k & 0xffffffffull);
+        if (dst < out_cap) out[dst] = stage[i];
+    }
+}
+
+__global__ void __launch_bounds__(kReduceThreads) k_reduce_stats(const cmpmc_sim_stats* __restrict__ ev,
+                                                                 uint64_t n, cmpmc_sim_stats* total) {
+    __shared__ uint64_t acc[kReduceThreads][kStatsWords];
+    const int t = threadIdx.x;
+    const uint64_t chunk = (n + kReduceThreads - 1) / kReduceThreads;
+    const uint64_t lo = min(n, t * chunk), hi = min(n, lo + chunk);
+    uint64_t u[kStatsWords];
+    double d[kStatsWords];
+#pragma unroll
+    for (int w = 0; w < kStatsWords; ++w) {
+        u[w] = 0;
+        d[w] = 0.0;
+    }
+    for (uint64_t i = lo; i < hi; ++i) {
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(ev + i);
+#pragma unroll
+        for (int w = 0; w < kStatsWords; ++w) {
+            const uint64_t x = src[w];
+            if (stats_word_is_double(w)) d[w] += __longlong_as_double(static_cast<long long>(x));
+            else u[w] += x;
+        }
+    }
+#pragma unroll
+    for (int w = 0; w < kStatsWords; ++w)
+        acc[t][w] = stats_word_is_double(w) ? static_cast<uint64_t>(__double_as_longlong(d[w])) : u[w];
+    __syncthreads();
+    for (int stride = kReduceThreads / 2; stride > 0; stride >>= 1) {
+        if (t < stride) {
+            for (int w = 0; w < kStatsWords; ++w) {
+                if (stats_word_is_double(w)) {
+                    const double a = __longlong_as_double(static_cast<long long>(acc[t][w]));
+                    const double b = __longlong_as_double(static_cast<long long>(acc[t + stride][w]));
+                    acc[t][w] = static_cast<uint64_t>(__double_as_longlong(a + b));
+                } else {
+                    acc[t][w] += acc[t + stride][w];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (t < kStatsWords) reinterpret_cast<uint64_t*>(total)[t] = acc[0][t];
+}
+
+}  // namespace
+
+cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
+                          cmpmc_sim_stats* total, cudaStream_t s, int* launches) {
+    k_scan<<<1, kScanThreads, 0, s>>>(a.ev_nhits, a.n_events, offsets);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    *launches += 1;
+    if (a.keep_hits) {
+        k_scatter<<<4 * 148, 256, 0, s>>>(a.hit_stage, a.hit_key, a.hit_count, a.hit_cap, offsets, hits_out,
+                                          out_cap);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        *launches += 1;
+    }
+    k_reduce_stats<<<1, kReduceThreads, 0, s>>>(a.ev_stats, a.n_events, total);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+}  // namespace cmpmc_gpu

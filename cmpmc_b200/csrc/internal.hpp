@@ -1,0 +1,32 @@
+// internal.hpp -- host-side types shared by the library's translation units.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/cmpmc_gpu.h"
+#include "transport.cuh"
+
+struct cmpmc_lattice {
+    cmpmc_crystal_config cfg;
+    std::vector<cmpmc_gpu::OctEntry> oct;  // [3][256][256]
+    std::vector<double> cdf_lt, cdf_tt;    // [1024] each
+    std::vector<double> hv;                // flattened HV tensors (see cmpmc_lattice_tables)
+    cmpmc_gpu::Lattice view;               // host pointers into the vectors above
+};
+
+namespace cmpmc_gpu {
+
+// Checks a detector / crystal pair against what the device path supports and applies the
+// reference's guards (engine.hpp:165-168, 197-199, 407-409). Returns a CMPMC_* status.
+int validate_config(const cmpmc_crystal_config& cfg, const cmpmc_detector& det, bool has_charges,
+                    std::string& err);
+Detector detector_view(const cmpmc_detector& det);
+
+// Record conversion between the reference layouts and the register-state structs.
+Track track_from_record(const cmpmc_phonon_track& r);
+void track_to_record(const Track& t, cmpmc_phonon_track& r);
+Charge charge_from_record(const cmpmc_charge_track& r);
+void charge_to_record(const Charge& c, cmpmc_charge_track& r);
+
+}  // namespace cmpmc_gpu

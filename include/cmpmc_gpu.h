@@ -1,0 +1,297 @@
+/*
+ * cmpmc_gpu.h -- C ABI of the B200 (sm_100a) transport path for CMPMC.
+ *
+ * This is the drop-in boundary behind CMPMC's run_events / SimulationEngine API.
+ * Every entry point takes plain pointers and sizes; no C++ or torch type crosses it.
+ * Status codes are int (0 = OK, see CMPMC_* below); no exception crosses the ABI.
+ *
+ * Reference interfaces replaced (paths within the CMPMC project):
+ *   run_events(engine, n, generate, options)   include/cmpmc/transport/parallel.hpp:76-148
+ *   SimulationEngine::transport                include/cmpmc/transport/engine.hpp:403-582
+ *   SimulationEngine::transport_charges        include/cmpmc/transport/engine.hpp:192-380
+ *   SimulationEngine::make_track               include/cmpmc/transport/engine.hpp:171-187
+ *   CrystalLattice(cfg) (host table build)     include/cmpmc/lattice/crystal_lattice.hpp:45-55
+ *   Rng::for_stream                            include/cmpmc/core/rng.hpp:34-36
+ *
+ * Records (cmpmc_phonon_track, cmpmc_charge_track, cmpmc_sensor_hit, cmpmc_sim_stats)
+ * are byte-compatible with the reference's PhononTrack, ChargeTrack, SensorHit and
+ * SimStats (include/cmpmc/core/track.hpp:62-108, transport/engine.hpp:29-93), so a
+ * caller can pass std::vector<PhononTrack>::data() directly.
+ *
+ * Threading: a context is bound to one device and one stream; calls on one context
+ * must be serialized by the caller. Different contexts may run concurrently.
+ */
+#ifndef CMPMC_GPU_H
+#define CMPMC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CMPMC_GPU_ABI_VERSION 1
+
+/* ---- status codes -------------------------------------------------------------- */
+#define CMPMC_OK                 0
+#define CMPMC_ERR_INVALID        1  /* bad argument / unsupported configuration        */
+#define CMPMC_ERR_CUDA           2  /* a CUDA runtime call failed                       */
+#define CMPMC_ERR_UNVALIDATED    3  /* guarded module used without allow_unvalidated
+                                       (reference: UnvalidatedModuleError,
+                                       core/validation.hpp:20-29)                      */
+#define CMPMC_ERR_CAPACITY       4  /* a device buffer (stack, hits) overflowed         */
+#define CMPMC_ERR_DEVICE         5  /* a kernel reported an error status word           */
+#define CMPMC_ERR_NO_DEVICE      6  /* no CUDA device / extension cannot run            */
+
+/* ---- records (byte layout of the reference types) ------------------------------ */
+enum { CMPMC_MODE_L = 0, CMPMC_MODE_FT = 1, CMPMC_MODE_ST = 2 };
+enum { CMPMC_SURF_TOP = 0, CMPMC_SURF_BOTTOM = 1, CMPMC_SURF_SIDE = 2 };
+enum { CMPMC_EXC_PHONON = 0, CMPMC_EXC_ELECTRON = 1, CMPMC_EXC_HOLE = 2 };
+
+/* PhononTrack (track.hpp:62-72): 128 B, 64-byte aligned */
+typedef struct cmpmc_phonon_track {
+    double pos[3];
+    double k_dir[3];
+    double vg_dir[3];
+    double energy;
+    double vg_mag;
+    double time;
+    double weight;
+    uint32_t bounces;
+    uint8_t mode;
+    uint8_t _pad[19];
+} cmpmc_phonon_track;
+
+/* ChargeTrack (track.hpp:75-84): 128 B, 64-byte aligned */
+typedef struct cmpmc_charge_track {
+    double pos[3];
+    double p_eV[3];
+    double ekin;
+    double time;
+    double weight;
+    uint16_t valley;
+    uint8_t type;
+    uint8_t alive;
+    uint8_t _pad[52];
+} cmpmc_charge_track;
+
+/* SensorHit (track.hpp:99-108): 56 B */
+typedef struct cmpmc_sensor_hit {
+    double pos[3];
+    double time;
+    double edep;
+    double incident_energy;
+    uint8_t surface_id;
+    uint8_t excitation;
+    uint8_t mode;
+    uint8_t _pad;
+    int32_t channel_id;
+} cmpmc_sensor_hit;
+
+/* SimStats (engine.hpp:29-93): 208 B, same field order */
+typedef struct cmpmc_sim_stats {
+    uint64_t total_steps, isotope_scatters, polycrystal_scatters, decays_L_to_TT, decays_L_to_LT,
+             surface_refls, surface_downconversions, sensor_hits, killed_tracks;
+    uint64_t charge_steps, luke_phonons_emitted, intervalley_scatters, charges_trapped,
+             trap_ionizations, charge_surface_refls, charges_collected;
+    double total_luke_phonon_eV, charge_recomb_edep_eV;
+    uint64_t sc_pair_breakings, qp_diffusion_steps, qp_phonons_radiated, qp_recombinations,
+             qp_local_traps;
+    double total_injected_eV, total_deposited_eV, escaped_or_killed_eV;
+} cmpmc_sim_stats;
+
+/* ---- configuration (plain data mirrors of the reference structs) ---------------- */
+#define CMPMC_MAX_VALLEYS 8
+#define CMPMC_MAX_IV 4
+#define CMPMC_MAX_POLY 8
+
+/* CrystalConfig (materials/crystal_config.hpp:43-226); fields in SI / eV as there. */
+typedef struct cmpmc_crystal_config {
+    int32_t group;                 /* BravaisGroup */
+    int32_t has_custom_C;
+    double density;
+    double C11, C12, C13, C14, C16, C33, C44, C66;
+    double C_custom[6][6];
+    double beta, gamma, lambda, mu;
+    double B_iso, A_anh, fTT_frac, polycrystal_mfp_m;
+    double fLDOS, fSTDOS, fFTDOS;
+    double debye_freq, v_sound, v_trans;
+    double bandgap, pair_energy, fano_factor, epsilon_rel, neutral_impurity_cm3, alpha_nonparabolic;
+    double h_mass_ratio;
+    double e_mass_tensor[3];
+    int32_t n_valleys;
+    int32_t iv_model;              /* IVRateModel: 0 Quadratic, 1 Linear, 2 Matrix */
+    double valley_dirs[CMPMC_MAX_VALLEYS][3];
+    double ac_deform_e, ac_deform_h;
+    int32_t n_iv;
+    int32_t _pad0;
+    double iv_deform_eV_m[CMPMC_MAX_IV], iv_energy_eV[CMPMC_MAX_IV];
+    double iv_min_energy, iv_quad_rate, iv_quad_field, iv_quad_power, iv_lin_rate0, iv_lin_rate1, iv_lin_power;
+    double e_trapping_mfp_m, h_trapping_mfp_m, e_trap_ion_d0_mfp_m, e_trap_ion_a_mfp_m,
+           h_trap_ion_d_mfp_m, h_trap_ion_a0_mfp_m;
+    double orient[3][3];           /* crystal -> detector rotation */
+} cmpmc_crystal_config;
+
+/* SuperconductorFilmConfig (crystal_config.hpp:240-257) */
+typedef struct cmpmc_film_config {
+    double film_absorption, film_thickness, v_sound, gap_energy, phonon_lifetime,
+           phonon_lifetime_slope, low_qp_limit, high_qp_limit, subgap_absorption, absorber_gap,
+           absorber_eff, absorber_eff_slope, temperature;
+    int32_t keep_all_phonons;
+    int32_t loss_model;            /* FilmLossModel: 0 MeanFreePath, 1 KaplanRateCompetition */
+    double phonon_loss_time;
+} cmpmc_film_config;
+
+/* SurfaceProperty (geometry/surface_property.hpp:23-45) */
+typedef struct cmpmc_surface {
+    double prob_abs, prob_refl, refl_cutoff, anh_cutoff;
+    double prob_charge_abs, prob_charge_spec, min_k_elec, min_k_hole;
+    double spec_prob_const;
+    int32_t n_spec, n_diff, n_anh;
+    int32_t demo_values;
+    double spec_coeffs[CMPMC_MAX_POLY], diff_coeffs[CMPMC_MAX_POLY], anh_coeffs[CMPMC_MAX_POLY];
+    int32_t has_film;
+    int32_t has_amm;               /* interface model: not supported on the device (must be 0) */
+    int32_t has_mask;              /* electrode mask: not supported on the device (must be 0) */
+    int32_t _pad0;
+    cmpmc_film_config film;
+} cmpmc_surface;
+
+/* DetectorModel (transport/engine.hpp:96-156) with a CylinderSolid */
+typedef struct cmpmc_detector {
+    double radius, half_z;
+    double e_field[3];             /* UniformElectricField::field_Vm */
+    cmpmc_surface surfaces[3];     /* TopFace, BottomFace, SideWall */
+    uint32_t max_bounces;
+    uint32_t russian_roulette_bounces;
+    double russian_roulette_survival;
+    double min_phonon_eV;
+    double luke_sample_fraction;
+    double charge_max_dk_frac, charge_dt_cap_s, charge_sampling_dk_frac;
+    int32_t charge_stepping;       /* 0 FirstOrderDkCap, 1 LemanSecondOrder */
+    int32_t charge_release;        /* 0 RecordOnly (others unsupported on the device) */
+    double fermi_level_above_Ev_eV;
+    double electrode_seed_max_gap;
+    int32_t allow_unvalidated;
+    int32_t jump_to_ballistic;     /* experimental; must be 0 */
+    int32_t kinematics_mode;       /* CrystalLattice::KinematicsMode: 0 Octahedral (only) */
+    int32_t _pad0;
+} cmpmc_detector;
+
+/* Germanium preset (materials/presets.hpp:18-25) and the default detector
+ * (engine.hpp:96-156: Al Kaplan films on both faces, bare diffuse side wall). */
+void cmpmc_crystal_config_germanium(cmpmc_crystal_config* cfg);
+void cmpmc_detector_default(cmpmc_detector* det);
+void cmpmc_film_aluminum(cmpmc_film_config* film);
+
+/* ---- host lattice (replaces the CrystalLattice constructor) -------------------- */
+typedef struct cmpmc_lattice cmpmc_lattice;
+
+/* Builds the octahedral FP32 group-velocity table (3x256x256 {vx,vy,vz,|v|}), the
+ * decay inverse-CDF tables (2x1024 FP64) and the Herring-Vogt valley tensors on the
+ * host, with the reference's arithmetic (crystal_lattice.hpp:340-477). */
+int cmpmc_lattice_create(const cmpmc_crystal_config* cfg, cmpmc_lattice** out);
+void cmpmc_lattice_destroy(cmpmc_lattice* lat);
+/* Read-only views of the tables (owned by the lattice). hv: 16 + 9*n_valleys doubles
+ * in the order e_cond_mass, h_mass, mass_ratio[3], hv_sqrt[3], hv_sqrt_inv[3], l0_e,
+ * l0_h, k_sound_e, k_sound_h, n_valleys, valley_rot[n][3][3]. */
+int cmpmc_lattice_tables(const cmpmc_lattice* lat, const float** oct_lut, const double** cdf_lt,
+                         const double** cdf_tt, const double** hv, size_t* n_hv);
+/* CrystalLattice::map_k_to_vg_oct (crystal_lattice.hpp:144-176), on the host. */
+int cmpmc_lattice_map_k_to_vg(const cmpmc_lattice* lat, int mode, const double k_det[3],
+                              double vg_dir[3], double* vg_mag);
+/* SimulationEngine::make_track (engine.hpp:171-187), on the host. */
+int cmpmc_make_track(const cmpmc_lattice* lat, const double pos[3], const double k_dir[3], int mode,
+                     double energy_eV, double time_s, double weight, cmpmc_phonon_track* out);
+/* ChargePhysics::make_charge (charge/charge_transport.hpp:49-70), on the host. */
+int cmpmc_make_charge(const cmpmc_lattice* lat, int type, const double pos[3], const double dir[3],
+                      double ekin_eV, int valley, double time_s, cmpmc_charge_track* out);
+
+/* ---- random streams (core/rng.hpp) --------------------------------------------- */
+void cmpmc_rng_for_stream(uint64_t seed, uint64_t stream, uint64_t state[4]);
+uint64_t cmpmc_rng_next_u64(uint64_t state[4]);
+double cmpmc_rng_uniform(uint64_t state[4]);
+
+/* ---- canonical workload generators (host) --------------------------------------- */
+enum {
+    CMPMC_WL_SINGLE_L_ORIGIN = 0,  /* one L phonon, 7.5 meV, at the origin, isotropic          */
+    CMPMC_WL_MIXED_ENERGY    = 1,  /* 100 phonons/event, log-uniform 1-30 meV, L/ST/FT mix      */
+    CMPMC_WL_PAIR_DRIFT      = 2,  /* one e-/h+ pair per event, uniform origin                  */
+    CMPMC_WL_SINGLE_L_VOLUME = 4,  /* one L phonon, 7.5 meV, uniform origin, isotropic          */
+    CMPMC_WL_TEST_PARALLEL   = 5   /* reference tests/test_parallel.cpp:110-125 generator        */
+};
+/* Runs the workload's generator for events [first_event, first_event + n_events) from
+ * Rng::for_stream(seed, ev) and writes, per event, the RNG state after the generator
+ * (4 u64), the injected energy and the CSR-packed initial tracks. Capacities are in
+ * records; *n_phonons / *n_charges receive the totals (CMPMC_ERR_CAPACITY if short). */
+int cmpmc_generate(const cmpmc_lattice* lat, const cmpmc_detector* det, int workload, uint64_t seed,
+                   uint64_t first_event, uint64_t n_events, int n_threads,
+                   uint64_t* rng_state, double* injected_eV,
+                   uint64_t* phonon_offsets, cmpmc_phonon_track* phonons, uint64_t phonon_cap,
+                   uint64_t* n_phonons,
+                   uint64_t* charge_offsets, cmpmc_charge_track* charges, uint64_t charge_cap,
+                   uint64_t* n_charges);
+
+/* ---- device context and run ---------------------------------------------------- */
+typedef struct cmpmc_gpu_ctx cmpmc_gpu_ctx;
+
+enum {
+    CMPMC_FORM_PLAIN_FP64   = 0,   /* bit-exact event streams, one event per device thread   */
+    CMPMC_FORM_BATCHED_FP32 = 1    /* per-primary substreams, FP32 geometry, FP64 ledger/time */
+};
+
+typedef struct cmpmc_run_desc {
+    uint64_t n_events;
+    uint64_t first_event;          /* event id of record 0 (event ids feed the substreams)  */
+    const uint64_t* rng_state;     /* [n_events][4] post-generator state                    */
+    const double* injected_eV;     /* [n_events]                                            */
+    const uint64_t* phonon_offsets;/* [n_events + 1]                                        */
+    const cmpmc_phonon_track* phonons;
+    const uint64_t* charge_offsets;/* [n_events + 1], or NULL when there are no charges     */
+    const cmpmc_charge_track* charges;
+    int32_t keep_hits;             /* RunOptions::keep_hits                                  */
+    int32_t form;                  /* CMPMC_FORM_*                                           */
+    int32_t inputs_on_device;      /* 1: the pointers above are device pointers             */
+    int32_t outputs_on_device;     /* 1: leave hits / offsets / event stats on the device   */
+    uint64_t seed;                 /* batched form: substream seed                          */
+    int32_t want_event_stats;      /* 1: also return per-event SimStats                     */
+    int32_t _pad0;
+} cmpmc_run_desc;
+
+typedef struct cmpmc_run_out {
+    cmpmc_sim_stats stats;         /* summed over all events                                 */
+    uint64_t n_hits;
+    const cmpmc_sensor_hit* hits;  /* [n_hits], event order; owned by the context            */
+    const uint64_t* hit_offsets;   /* [n_events + 1]; owned by the context                   */
+    const cmpmc_sim_stats* event_stats; /* [n_events] if requested; owned by the context     */
+    double kernel_ms;              /* device time of the transport kernel(s)                 */
+    double total_ms;               /* device time of the whole call incl. copies            */
+    uint32_t device_error;         /* error word written by the kernels (0 = none)           */
+    uint32_t kernel_launches;      /* kernels this call launched                             */
+} cmpmc_run_out;
+
+int cmpmc_gpu_create(const cmpmc_lattice* lat, const cmpmc_detector* det, int device,
+                     cmpmc_gpu_ctx** out);
+void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx);
+/* run_events on the device for pre-generated events (the generator ran on the host). */
+int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* desc, cmpmc_run_out* out);
+/* Copies the message of the last failed call on ctx (or of a failed create when ctx is
+ * NULL) into buf. Returns the status of that call. */
+int cmpmc_gpu_last_error(const cmpmc_gpu_ctx* ctx, char* buf, size_t size);
+/* Device-side tuning: threads per block and blocks per SM of the transport kernels,
+ * stack capacity (tracks per device thread), hit staging capacity (records). 0 keeps
+ * the current value. */
+int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_per_sm,
+                        uint64_t stack_capacity, uint64_t hit_capacity);
+int cmpmc_gpu_device_count(int* count);
+
+/* Layout self-check for bindings: writes sizeof of the ABI structs in the order
+ * phonon_track, charge_track, sensor_hit, sim_stats, crystal_config, film_config,
+ * surface, detector, run_desc, run_out (at most n values). Returns the ABI version. */
+int cmpmc_abi_sizes(size_t* out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CMPMC_GPU_H */

@@ -1,0 +1,288 @@
+// Test infrastructure only (the checker): drives the unmodified reference CMPMC
+// library, compiled from its own headers, on the canonical workloads and writes
+// its per-event results as raw binary records. Nothing in the product links or
+// runs this program; tests/golden/make_golden.py and bench.py's CPU-baseline leg
+// call it.
+//
+// Usage:
+//   cmpmc_ref dump <workload> <first_event> <n_events> <threads> <out_prefix>
+//       Runs events [first, first+n) one by one (each from Rng::for_stream(seed, ev),
+//       as run_events does, parallel.hpp:102-114) and writes
+//         <prefix>.init   per event: u64 rng_state[4] after the generator, f64 injected,
+//                         u64 n_phonons, u64 n_charges, then the PhononTrack /
+//                         ChargeTrack records (128 B each)
+//         <prefix>.events per event: u64 n_hits, SimStats (208 B)
+//         <prefix>.hits   SensorHit records (56 B each), in event order
+//   cmpmc_ref time <workload> <first_event> <n_events> <threads>
+//       Times the reference's own run_events (parallel.hpp:76-148) on the workload
+//       and prints one JSON line (wall seconds from RunResult::wall_seconds).
+//   cmpmc_ref rng <seed> <stream> <count>
+//       Prints next_u64 / uniform / isotropic_dir / lambertian_dir vectors.
+//
+// Workloads (seeds and draw orders are the canonical generators of this project):
+//   c0  default Ge detector; one L phonon, 7.5 meV, at the origin, isotropic; seed 42
+//   c1  default detector; 100 phonons per event: E = 1 meV*exp(ln30*u), mode L/ST/FT
+//       at u < 0.10 / < 0.46 / else, origin uniform in the cylinder (rejection in x,y
+//       then z), direction isotropic; seed 7
+//   c2  uniform field 4 V over 2.54 cm, luke_sample_fraction 0; one e-/h+ pair per
+//       event: origin as c1, valley = next_u64() % 4, e- isotropic, h+ isotropic,
+//       1 ueV each; seed 11; events_per_chunk 1
+//   c4  default detector; one L phonon, 7.5 meV, origin as c1, isotropic; seed 17
+//   tp  the mixed workload of the reference's own tests/test_parallel.cpp:110-125
+//       (even events: FT 7.5 meV phonon at the origin; odd events: e-/h+ pair),
+//       field 2 V over 2.54 cm, luke_sample_fraction 0.02; seed 77
+//   tpl same as tp with luke_sample_fraction 1 (every Luke phonon tracked)
+#include "cmpmc/cmpmc.hpp"
+
+#include <chrono>
+#include <cinttypes>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace cmpmc;
+
+namespace {
+
+struct Workload {
+    std::string name;
+    uint64_t seed = 1;
+    uint32_t events_per_chunk = 16;
+};
+
+Workload make_workload(const std::string& w) {
+    Workload wl;
+    wl.name = w;
+    if (w == "c0") wl.seed = 42;
+    else if (w == "c1") wl.seed = 7;
+    else if (w == "c2") { wl.seed = 11; wl.events_per_chunk = 1; }
+    else if (w == "c4") wl.seed = 17;
+    else if (w == "tp" || w == "tpl") wl.seed = 77;
+    else { std::fprintf(stderr, "unknown workload %s\n", w.c_str()); std::exit(2); }
+    return wl;
+}
+
+void setup_detector(const std::string& w, DetectorModel& det) {
+    if (w == "c2") {
+        det.e_field = UniformElectricField::from_bias(4.0, 2.54 * units::cm);
+        det.luke_sample_fraction = 0.0;
+    } else if (w == "tp" || w == "tpl") {
+        det.e_field = UniformElectricField::from_bias(2.0, 2.54 * units::cm);
+        det.luke_sample_fraction = (w == "tp") ? 0.02 : 1.0;
+    }
+}
+
+Vec3 uniform_origin(const CylinderSolid& s, Rng& rng) {
+    double x, y;
+    do {
+        x = (2.0 * rng.uniform() - 1.0) * s.radius;
+        y = (2.0 * rng.uniform() - 1.0) * s.radius;
+    } while (x * x + y * y > s.radius * s.radius);
+    const double z = (2.0 * rng.uniform() - 1.0) * s.half_z;
+    return {x, y, z};
+}
+
+struct Generator {
+    std::string w;
+    const SimulationEngine* engine;
+    const ChargePhysics* charges;
+    const DetectorModel* det;
+    size_t n_valleys;
+
+    void operator()(EventInput& in) const {
+        if (w == "c0") {
+            in.phonons.push_back(engine->make_track({0, 0, 0}, in.rng.isotropic_dir(), PhononMode::L, 7.5e-3));
+            in.injected_eV += 7.5e-3;
+        } else if (w == "c1") {
+            for (int j = 0; j < 100; ++j) {
+                const double E = 1e-3 * std::exp(std::log(30.0) * in.rng.uniform());
+                const double um = in.rng.uniform();
+                const PhononMode m = um < 0.10 ? PhononMode::L : (um < 0.46 ? PhononMode::ST : PhononMode::FT);
+                const Vec3 p = uniform_origin(det->solid, in.rng);
+                const Vec3 d = in.rng.isotropic_dir();
+                in.phonons.push_back(engine->make_track(p, d, m, E));
+                in.injected_eV += E;
+            }
+        } else if (w == "c2") {
+            const Vec3 p = uniform_origin(det->solid, in.rng);
+            const uint16_t v = static_cast<uint16_t>(in.rng.next_u64() % 4);
+            const Vec3 de = in.rng.isotropic_dir();
+            in.charges.push_back(charges->make_charge(ExcitationType::Electron, p, de, 1e-6, v));
+            const Vec3 dh = in.rng.isotropic_dir();
+            in.charges.push_back(charges->make_charge(ExcitationType::Hole, p, dh, 1e-6, 0));
+        } else if (w == "c4") {
+            const Vec3 p = uniform_origin(det->solid, in.rng);
+            const Vec3 d = in.rng.isotropic_dir();
+            in.phonons.push_back(engine->make_track(p, d, PhononMode::L, 7.5e-3));
+            in.injected_eV += 7.5e-3;
+        } else {  // tp, tpl: tests/test_parallel.cpp:110-125
+            if (in.event_id % 2 == 0) {
+                in.phonons.push_back(engine->make_track({0, 0, 0}, in.rng.isotropic_dir(), PhononMode::FT, 7.5e-3));
+                in.injected_eV += 7.5e-3;
+            } else {
+                const auto v = static_cast<uint16_t>(in.rng.uniform() * n_valleys) % n_valleys;
+                in.charges.push_back(charges->make_charge(ExcitationType::Electron, {0, 0, 0}, in.rng.isotropic_dir(), 1e-6, v));
+                in.charges.push_back(charges->make_charge(ExcitationType::Hole, {0, 0, 0}, in.rng.isotropic_dir(), 1e-6, 0));
+            }
+        }
+    }
+};
+
+struct EventRecord {
+    uint64_t rng_after_gen[4];
+    double injected;
+    std::vector<PhononTrack> phonons;
+    std::vector<ChargeTrack> charges;
+    SimStats stats;
+    std::vector<SensorHit> hits;
+};
+
+FILE* open_or_die(const std::string& path) {
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) { std::perror(path.c_str()); std::exit(1); }
+    return f;
+}
+
+int cmd_dump(const std::string& w, uint64_t first, uint64_t n, unsigned threads, const std::string& prefix) {
+    const Workload wl = make_workload(w);
+    const CrystalLattice lattice(materials::Germanium());
+    DetectorModel det;
+    setup_detector(w, det);
+    const SimulationEngine engine(lattice, det);
+    const ChargePhysics cp(lattice);
+    const Generator gen{w, &engine, &cp, &det, lattice.config().valley_dirs.size()};
+
+    std::vector<EventRecord> rec(n);
+    std::atomic<uint64_t> next{0};
+    auto worker = [&]() {
+        std::vector<PhononTrack> ph;
+        std::vector<ChargeTrack> ch;
+        for (;;) {
+            const uint64_t i = next.fetch_add(1);
+            if (i >= n) return;
+            const uint64_t ev = first + i;
+            EventRecord& r = rec[i];
+            Rng rng = Rng::for_stream(wl.seed, ev);
+            ph.clear();
+            ch.clear();
+            EventInput in{ev, rng, ph, ch, 0.0};
+            gen(in);
+            std::memcpy(r.rng_after_gen, rng.s, sizeof(r.rng_after_gen));
+            r.injected = in.injected_eV;
+            r.phonons = ph;
+            r.charges = ch;
+            r.stats.total_injected_eV += in.injected_eV;
+            if (!ch.empty()) engine.transport_charges(ch, ph, r.hits, r.stats, rng);
+            if (!ph.empty()) engine.transport(ph, r.hits, r.stats, rng);
+        }
+    };
+    const unsigned nt = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; ++t) pool.emplace_back(worker);
+    for (auto& t : pool) t.join();
+
+    FILE* fi = open_or_die(prefix + ".init");
+    FILE* fe = open_or_die(prefix + ".events");
+    FILE* fh = open_or_die(prefix + ".hits");
+    static_assert(sizeof(PhononTrack) == 128 && sizeof(ChargeTrack) == 128 && sizeof(SensorHit) == 56 &&
+                  sizeof(SimStats) == 208, "record layout");
+    for (const EventRecord& r : rec) {
+        const uint64_t np = r.phonons.size(), nc = r.charges.size(), nh = r.hits.size();
+        std::fwrite(r.rng_after_gen, 8, 4, fi);
+        std::fwrite(&r.injected, 8, 1, fi);
+        std::fwrite(&np, 8, 1, fi);
+        std::fwrite(&nc, 8, 1, fi);
+        if (np) std::fwrite(r.phonons.data(), sizeof(PhononTrack), np, fi);
+        if (nc) std::fwrite(r.charges.data(), sizeof(ChargeTrack), nc, fi);
+        std::fwrite(&nh, 8, 1, fe);
+        std::fwrite(&r.stats, sizeof(SimStats), 1, fe);
+        if (nh) std::fwrite(r.hits.data(), sizeof(SensorHit), nh, fh);
+    }
+    std::fclose(fi);
+    std::fclose(fe);
+    std::fclose(fh);
+    return 0;
+}
+
+int cmd_time(const std::string& w, uint64_t first, uint64_t n, unsigned threads) {
+    const Workload wl = make_workload(w);
+    const auto t0 = std::chrono::steady_clock::now();
+    const CrystalLattice lattice(materials::Germanium());
+    DetectorModel det;
+    setup_detector(w, det);
+    const SimulationEngine engine(lattice, det);
+    const ChargePhysics cp(lattice);
+    const Generator gen{w, &engine, &cp, &det, lattice.config().valley_dirs.size()};
+    const double init_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    // run_events numbers events from 0; an offset range runs through a shifted generator
+    // whose streams are Rng::for_stream(seed, first + i), exactly as in the full run.
+    RunOptions opt;
+    opt.threads = threads;
+    opt.seed = wl.seed;
+    opt.events_per_chunk = wl.events_per_chunk;
+    opt.keep_hits = true;
+    RunResult r;
+    if (first == 0) {
+        r = run_events(engine, n, gen, opt);
+    } else {
+        auto shifted = [&](EventInput& in) {
+            in.rng = Rng::for_stream(wl.seed, first + in.event_id);
+            EventInput sh{first + in.event_id, in.rng, in.phonons, in.charges, 0.0};
+            gen(sh);
+            in.injected_eV = sh.injected_eV;
+        };
+        r = run_events(engine, n, shifted, opt);
+    }
+    uint64_t n_primary = 0;
+    if (w == "c1") n_primary = 100 * n; else n_primary = n;
+    std::printf("{\"workload\": \"%s\", \"first_event\": %" PRIu64 ", \"n_events\": %" PRIu64
+                ", \"threads\": %u, \"wall_seconds\": %.6f, \"init_seconds\": %.6f, \"primaries\": %" PRIu64
+                ", \"total_steps\": %" PRIu64 ", \"charge_steps\": %" PRIu64 ", \"sensor_hits\": %" PRIu64
+                ", \"n_hits\": %zu, \"injected_eV\": %.17g, \"deposited_eV\": %.17g, \"escaped_eV\": %.17g}\n",
+                w.c_str(), first, n, r.threads_used, r.wall_seconds, init_s, n_primary,
+                r.stats.total_steps, r.stats.charge_steps, r.stats.sensor_hits, r.hits.size(),
+                r.stats.total_injected_eV, r.stats.total_deposited_eV, r.stats.escaped_or_killed_eV);
+    return 0;
+}
+
+int cmd_rng(uint64_t seed, uint64_t stream, int count) {
+    Rng a = Rng::for_stream(seed, stream);
+    std::printf("state %" PRIu64 " %" PRIu64 " %" PRIu64 " %" PRIu64 "\n", a.s[0], a.s[1], a.s[2], a.s[3]);
+    for (int i = 0; i < count; ++i) std::printf("u64 %" PRIu64 "\n", a.next_u64());
+    for (int i = 0; i < count; ++i) std::printf("uniform %.17g\n", a.uniform());
+    for (int i = 0; i < count; ++i) {
+        const Vec3 d = a.isotropic_dir();
+        std::printf("iso %.17g %.17g %.17g\n", d.x, d.y, d.z);
+    }
+    const Vec3 normals[3] = {{0, 0, -1}, {0, 0, 1}, {-0.6, -0.8, 0}};
+    for (int i = 0; i < count; ++i) {
+        const Vec3 d = a.lambertian_dir(normals[i % 3]);
+        std::printf("lamb %.17g %.17g %.17g\n", d.x, d.y, d.z);
+    }
+    Rng b(12345);
+    std::printf("seeded %" PRIu64 " %" PRIu64 " %" PRIu64 " %" PRIu64 "\n", b.s[0], b.s[1], b.s[2], b.s[3]);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2) {
+        std::fprintf(stderr, "usage: %s dump|time|rng ...\n", argv[0]);
+        return 2;
+    }
+    const std::string cmd = argv[1];
+    if (cmd == "dump" && argc == 7)
+        return cmd_dump(argv[2], std::strtoull(argv[3], nullptr, 10), std::strtoull(argv[4], nullptr, 10),
+                        static_cast<unsigned>(std::atoi(argv[5])), argv[6]);
+    if (cmd == "time" && argc == 6)
+        return cmd_time(argv[2], std::strtoull(argv[3], nullptr, 10), std::strtoull(argv[4], nullptr, 10),
+                        static_cast<unsigned>(std::atoi(argv[5])));
+    if (cmd == "rng" && argc == 5)
+        return cmd_rng(std::strtoull(argv[2], nullptr, 10), std::strtoull(argv[3], nullptr, 10), std::atoi(argv[4]));
+    std::fprintf(stderr, "bad arguments\n");
+    return 2;
+}

@@ -1,0 +1,110 @@
+"""Regenerates the golden fixtures in this directory from the reference CMPMC build.
+
+Runs oracle/_ref/cmpmc_ref and oracle/_ref/cmpmc_ref_tables (the unmodified reference,
+compiled from its own headers by `make -C oracle ref`) and stores compact records:
+
+  rng.json              Rng::for_stream / next_u64 / uniform / isotropic_dir / lambertian_dir vectors
+  lattice_ge.npz        sha256 of the reference's octahedral table, its CDF tables and
+                        Herring-Vogt tensors, and a sample of table entries
+  <workload>_full.npz   per-event records for a few events: post-generator Rng state,
+                        initial tracks, per-event SimStats and every SensorHit
+  <workload>_summary.npz per-event summaries for many events (hit count, integer counters,
+                        sums over the hits, hash of the discrete hit fields)
+
+Usage: python tests/golden/make_golden.py   (needs the reference build; takes ~1 min)
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from tests.golden.records import (EVENT_DTYPE, SUMMARY_DTYPE, read_dump, summarize)  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref", "cmpmc_ref")
+REF_TABLES = os.path.join(ROOT, "oracle", "_ref", "cmpmc_ref_tables")
+
+# workload -> (full events, summary events)
+PLAN = {
+    "c0": (64, 10000),
+    "c4": (0, 2000),
+    "c1": (3, 40),
+    "c2": (64, 2000),
+    "tp": (32, 203),
+    "tpl": (2, 21),
+}
+
+
+def dump(workload: str, first: int, n: int, tmp: str):
+    prefix = os.path.join(tmp, f"{workload}_{first}_{n}")
+    subprocess.run([REF, "dump", workload, str(first), str(n), "0", prefix], check=True)
+    return read_dump(prefix, n)
+
+
+def main() -> None:
+    if not (os.path.exists(REF) and os.path.exists(REF_TABLES)):
+        sys.exit("build the reference first: make -C oracle ref")
+    with tempfile.TemporaryDirectory() as tmp:
+        # RNG vectors
+        rng = {}
+        for seed, stream in ((42, 0), (7, 12345), (17, 999999)):
+            out = subprocess.run([REF, "rng", str(seed), str(stream), "8"], check=True, capture_output=True,
+                                 text=True).stdout.split("\n")
+            rec = {"state": [], "u64": [], "uniform": [], "iso": [], "lamb": [], "seeded_12345": []}
+            for line in out:
+                if not line:
+                    continue
+                k, *v = line.split()
+                if k == "state":
+                    rec["state"] = [int(x) for x in v]
+                elif k == "seeded":
+                    rec["seeded_12345"] = [int(x) for x in v]
+                elif k == "u64":
+                    rec["u64"].append(int(v[0]))
+                elif k == "uniform":
+                    rec["uniform"].append(float.hex(float(v[0])))
+                else:
+                    rec[k].append([float.hex(float(x)) for x in v])
+            rng[f"{seed}:{stream}"] = rec
+        with open(os.path.join(HERE, "rng.json"), "w") as f:
+            json.dump(rng, f, indent=1)
+
+        # lattice tables
+        prefix = os.path.join(tmp, "ge")
+        subprocess.run([REF_TABLES, prefix], check=True)
+        oct_b = open(prefix + ".oct", "rb").read()
+        cdf = np.fromfile(prefix + ".cdf", dtype=np.float64)
+        hv = np.fromfile(prefix + ".hv", dtype=np.float64)
+        octa = np.frombuffer(oct_b, dtype=np.float32).reshape(3, 256, 256, 4)
+        idx = np.random.default_rng(0).integers(0, 256, size=(64, 2))
+        np.savez_compressed(os.path.join(HERE, "lattice_ge.npz"), oct_sha256=np.array(hashlib.sha256(oct_b).hexdigest()),
+                            cdf_lt=cdf[:1024], cdf_tt=cdf[1024:], hv=hv, sample_idx=idx,
+                            sample=octa[:, idx[:, 0], idx[:, 1], :])
+
+        # workloads
+        for wl, (n_full, n_sum) in PLAN.items():
+            if n_full:
+                d = dump(wl, 0, n_full, tmp)
+                np.savez_compressed(os.path.join(HERE, f"{wl}_full.npz"), **d)
+            d = dump(wl, 0, n_sum, tmp)
+            s = summarize(d["events"], d["hit_offsets"], d["hits"])
+            np.savez_compressed(os.path.join(HERE, f"{wl}_summary.npz"), summary=s,
+                                injected=d["injected"], rng_state=d["rng_state"])
+            print(wl, n_full, n_sum, int(d["hit_offsets"][-1]), "hits")
+    gl = subprocess.run(["ldd", "--version"], capture_output=True, text=True).stdout.split("\n")[0]
+    with open(os.path.join(HERE, "PROVENANCE.txt"), "w") as f:
+        f.write("Generated by tests/golden/make_golden.py from the unmodified reference CMPMC\n"
+                "(oracle/_ref, g++ -O3 -std=c++20, no -march=native).\n"
+                f"host libm: {gl}\n")
+
+
+if __name__ == "__main__":
+    main()

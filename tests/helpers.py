@@ -1,0 +1,48 @@
+"""Shared helpers of the test suite: fixture paths and the canonical workloads."""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def golden(name: str):
+    return np.load(os.path.join(GOLDEN, name), allow_pickle=False)
+
+
+def detector_for(workload: str):
+    """The canonical detector of each fixture workload (mirrors oracle/ref_driver.cpp)."""
+    import cmpmc_b200 as cm
+    det = cm.DetectorModel()
+    if workload == "c2":
+        det.e_field = cm.UniformElectricField.from_bias(4.0, 2.54 * cm.units.cm)
+        det.luke_sample_fraction = 0.0
+    elif workload in ("tp", "tpl"):
+        det.e_field = cm.UniformElectricField.from_bias(2.0, 2.54 * cm.units.cm)
+        det.luke_sample_fraction = 0.02 if workload == "tp" else 1.0
+    return det
+
+
+WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77}
+
+
+def workload_of(name: str):
+    import cmpmc_b200 as cm
+    return {"c0": cm.workloads.single_l_origin, "c1": cm.workloads.mixed_energy, "c2": cm.workloads.pair_drift,
+            "c4": cm.workloads.single_l_volume, "tp": cm.workloads.test_parallel,
+            "tpl": cm.workloads.test_parallel}[name]
+
+
+def has_gpu() -> bool:
+    try:
+        from cmpmc_b200 import _ffi
+        import ctypes
+        n = ctypes.c_int32(0)
+        return _ffi.load().cmpmc_gpu_device_count(ctypes.byref(n)) == 0 and n.value > 0
+    except Exception:
+        return False

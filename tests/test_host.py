@@ -1,0 +1,142 @@
+"""CPU tests of the host side: library load and exports, RNG streams, lattice tables,
+generators and guards, all against the reference's golden records. No device needed."""
+import ctypes
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+from tests.helpers import GOLDEN, ROOT, WORKLOAD_SEED, detector_for, golden, workload_of
+
+
+def test_library_exports_every_declared_symbol(lib):
+    header = open(os.path.join(ROOT, "include", "cmpmc_gpu.h")).read()
+    declared = set(re.findall(r"^\s*(?:[a-z_0-9]+\s*\*?\s+)+\*?(cmpmc_[a-z_0-9]+)\s*\(", header, re.M))
+    assert len(declared) >= 20
+    for name in sorted(declared):
+        assert hasattr(lib, name), name
+    from cmpmc_b200 import _ffi
+    assert set(_ffi.EXPORTED) <= declared
+
+
+def test_rng_streams_match_reference():
+    from cmpmc_b200 import Rng
+    from cmpmc_b200 import _ffi
+    lib = _ffi.load()
+    ref = json.load(open(os.path.join(GOLDEN, "rng.json")))
+    for key, rec in ref.items():
+        seed, stream = (int(x) for x in key.split(":"))
+        r = Rng.for_stream(seed, stream)
+        assert r.s == rec["state"]
+        st = (ctypes.c_uint64 * 4)()
+        lib.cmpmc_rng_for_stream(seed, stream, st)
+        assert list(st) == rec["state"]
+        assert [r.next_u64() for _ in range(8)] == rec["u64"]
+        for want in rec["uniform"]:
+            assert r.uniform() == float.fromhex(want)
+        for want in rec["iso"]:
+            assert r.isotropic_dir() == tuple(float.fromhex(x) for x in want)
+        normals = [(0, 0, -1), (0, 0, 1), (-0.6, -0.8, 0)]
+        for i, want in enumerate(rec["lamb"]):
+            assert r.lambertian_dir(normals[i % 3]) == tuple(float.fromhex(x) for x in want)
+        assert Rng(12345).s == rec["seeded_12345"]
+        # the native stream continues identically
+        r2 = Rng.for_stream(seed, stream)
+        st2 = (ctypes.c_uint64 * 4)(*r2.s)
+        assert [lib.cmpmc_rng_next_u64(st2) for _ in range(8)] == rec["u64"]
+
+
+def test_lattice_tables_bit_identical_to_reference(ge_lattice):
+    import hashlib
+    g = golden("lattice_ge.npz")
+    t = ge_lattice.tables()
+    assert hashlib.sha256(t["oct"].tobytes()).hexdigest() == str(g["oct_sha256"])
+    assert np.array_equal(t["cdf_lt"], g["cdf_lt"])
+    assert np.array_equal(t["cdf_tt"], g["cdf_tt"])
+    assert np.array_equal(t["hv"], g["hv"])
+    idx = g["sample_idx"]
+    assert np.array_equal(t["oct"][:, idx[:, 0], idx[:, 1], :], g["sample"])
+
+
+@pytest.mark.parametrize("wl", ["c0", "c1", "c2", "tp", "tpl"])
+def test_native_generators_match_reference(ge_lattice, wl):
+    import cmpmc_b200 as cm
+    g = golden(f"{wl}_full.npz")
+    n = len(g["rng_state"])
+    eng = cm.SimulationEngine(ge_lattice, detector_for(wl))
+    ev = eng.generate(workload_of(wl), n, WORKLOAD_SEED[wl], threads=2)
+    assert np.array_equal(ev.rng_state, g["rng_state"])
+    assert np.array_equal(ev.injected_eV, g["injected"])
+    assert np.array_equal(ev.phonon_offsets, g["phonon_offsets"])
+    assert np.array_equal(ev.charge_offsets, g["charge_offsets"])
+    assert ev.phonons.tobytes() == g["phonons"].tobytes()
+    assert ev.charges.tobytes() == g["charges"].tobytes()
+
+
+def test_native_generator_summary_streams(ge_lattice):
+    """Post-generator Rng states of all 10,000 single-phonon events (the event-stream
+    handoff to the device)."""
+    import cmpmc_b200 as cm
+    s = golden("c0_summary.npz")
+    eng = cm.SimulationEngine(ge_lattice, detector_for("c0"))
+    ev = eng.generate(cm.workloads.single_l_origin, len(s["rng_state"]), 42)
+    assert np.array_equal(ev.rng_state, s["rng_state"])
+    assert np.array_equal(ev.injected_eV, s["injected"])
+
+
+def test_python_generator_matches_native(ge_lattice):
+    import cmpmc_b200 as cm
+    det = detector_for("tp")
+    eng = cm.SimulationEngine(ge_lattice, det)
+    n_val = 4
+
+    def gen(inp):  # tests/test_parallel.cpp:110-125 of the reference
+        if inp.event_id % 2 == 0:
+            inp.phonons.append(eng.make_track((0, 0, 0), inp.rng.isotropic_dir(), cm.PhononMode.FT, 7.5e-3))
+            inp.injected_eV += 7.5e-3
+        else:
+            v = int(inp.rng.uniform() * n_val) % n_val
+            inp.charges.append(eng.make_charge(cm.ExcitationType.Electron, (0, 0, 0), inp.rng.isotropic_dir(), 1e-6, v))
+            inp.charges.append(eng.make_charge(cm.ExcitationType.Hole, (0, 0, 0), inp.rng.isotropic_dir(), 1e-6, 0))
+
+    a = eng.generate_python(gen, 32, 77)
+    g = golden("tp_full.npz")
+    assert np.array_equal(a.rng_state, g["rng_state"])
+    assert a.phonons.tobytes() == g["phonons"].tobytes()
+    assert a.charges.tobytes() == g["charges"].tobytes()
+
+
+def test_map_k_to_vg_host_closed_form(ge_lattice):
+    """Along [100] of a cubic crystal the L group velocity is sqrt(C11/rho) and parallel to k
+    (the table blend reproduces it to the table's interpolation error)."""
+    import math
+    import cmpmc_b200 as cm
+    vg, mag = ge_lattice.map_k_to_vg(cm.PhononMode.L, (1.0, 0.0, 0.0))
+    cfg = ge_lattice.config()
+    assert abs(mag - math.sqrt(cfg.C11 / cfg.density)) / mag < 1e-3
+    assert vg[0] > 0.9999  # the [100] direction sits on the octahedral fold (u = 1)
+
+
+def test_demo_surfaces_are_guarded(ge_lattice):
+    import cmpmc_b200 as cm
+    det = cm.DetectorModel()
+    det.surfaces = [cm.SurfaceProperty.demo_polynomial_sensor_surface(),
+                    cm.SurfaceProperty.demo_polynomial_sensor_surface(),
+                    cm.SurfaceProperty.demo_polynomial_bare_surface()]
+    with pytest.raises(cm.UnvalidatedModuleError):
+        cm.SimulationEngine(ge_lattice, det)
+    det.allow_unvalidated = True
+    cm.SimulationEngine(ge_lattice, det)
+
+
+def test_no_device_fails_loudly(ge_lattice):
+    """Without a GPU the device path raises; nothing falls back to a CPU implementation."""
+    from tests.helpers import has_gpu
+    import cmpmc_b200 as cm
+    if has_gpu():
+        pytest.skip("a device is present")
+    eng = cm.SimulationEngine(ge_lattice, cm.DetectorModel())
+    with pytest.raises(cm.CmpmcError):
+        cm.run_events(eng, 4, cm.workloads.single_l_origin, cm.RunOptions(seed=42))
