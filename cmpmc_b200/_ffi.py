@@ -147,6 +147,10 @@ _SIG = {
     "cmpmc_gpu_last_error": (_i32, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "cmpmc_gpu_configure": (_i32, [C.c_void_p, _i32, _i32, _u64, _u64]),
     "cmpmc_gpu_device_count": (_i32, [C.POINTER(_i32)]),
+    "cmpmc_cr_log": (_f64, [_f64]),
+    "cmpmc_cr_sin": (_f64, [_f64]),
+    "cmpmc_cr_cos": (_f64, [_f64]),
+    "cmpmc_gpu_math_check": (_i32, [_i32, _u64, C.c_void_p, C.c_void_p]),
 }
 
 EXPORTED = sorted(_SIG)

@@ -131,6 +131,20 @@ int cmpmc_gpu_device_count(int* count) {
     return (e == cudaSuccess && n > 0) ? CMPMC_OK : CMPMC_ERR_NO_DEVICE;
 }
 
+int cmpmc_gpu_math_check(int device, uint64_t n, const double* x, double* out) {
+    if (!x || !out) return CMPMC_ERR_INVALID;
+    if (cudaSetDevice(device) != cudaSuccess) return CMPMC_ERR_NO_DEVICE;
+    double *dx = nullptr, *dout = nullptr;
+    cudaError_t e = cudaMalloc(&dx, std::max<uint64_t>(n, 1) * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, std::max<uint64_t>(n, 1) * 24);
+    if (e == cudaSuccess) e = cudaMemcpy(dx, x, n * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n) e = launch_math_check(n, dx, dout);
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, n * 24, cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(dout);
+    return e == cudaSuccess ? CMPMC_OK : CMPMC_ERR_CUDA;
+}
+
 int cmpmc_gpu_create(const cmpmc_lattice* lat, const cmpmc_detector* det, int device, cmpmc_gpu_ctx** out) {
     cmpmc_gpu_ctx* ctx = nullptr;
     if (!out) return fail(nullptr, CMPMC_ERR_INVALID, "out is NULL");

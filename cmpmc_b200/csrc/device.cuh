@@ -137,6 +137,7 @@ cudaError_t plain_fp64_occupancy(int block, int* blocks_per_sm);
 cudaError_t launch_batched_fp32(const Lattice& L, const Detector& D, const RunArgs& a, int grid, int block,
                                 cudaStream_t s);
 cudaError_t batched_fp32_occupancy(int block, int* blocks_per_sm);
+cudaError_t launch_math_check(uint64_t n, const double* x, double* out);
 cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
                           cmpmc_sim_stats* total, cudaStream_t s, int* launches);
 

@@ -270,6 +270,10 @@ void gen_event(int wl, const Lattice& L, const cmpmc_detector& det, uint64_t ev,
 
 extern "C" {
 
+double cmpmc_cr_log(double x) { return crmath::log(x); }
+double cmpmc_cr_sin(double x) { return crmath::sin(x); }
+double cmpmc_cr_cos(double x) { return crmath::cos(x); }
+
 int cmpmc_abi_sizes(size_t* out, int n) {
     const size_t sz[] = {sizeof(cmpmc_phonon_track), sizeof(cmpmc_charge_track), sizeof(cmpmc_sensor_hit),
                          sizeof(cmpmc_sim_stats),    sizeof(cmpmc_crystal_config), sizeof(cmpmc_film_config),

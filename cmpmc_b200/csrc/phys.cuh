@@ -4,9 +4,8 @@
 // Every function restates the reference's arithmetic in the reference's operation
 // order, because the plain FP64 form must reproduce the CPU's event streams: the
 // translation units that use it for parity are compiled without FMA contraction, so
-// + - * / and sqrt round exactly as on x86-64 SSE. Transcendentals (log, sin, cos,
-// acos, exp, cbrt, pow, hypot) call the platform's libm (glibc on the host, CUDA's on
-// the device); their last-ulp differences only shift continuous values.
+// + - * / and sqrt round exactly as on x86-64 SSE. Every transcendental is correctly
+// rounded on the device (crmath.cuh, see m_log below).
 #pragma once
 
 #include <math.h>
@@ -18,7 +17,35 @@
 #define CMPMC_HD inline
 #endif
 
+#include "crmath.cuh"
+
 namespace cmpmc_gpu {
+
+// Transcendentals of the transport. On the device, log, sin, cos, acos, exp, pow, hypot
+// and cbrt are the correctly
+// rounded functions of crmath.cuh (path lengths, energies and charge kinematics feed
+// trajectories that are sensitive to the last bit); on the host they are the platform libm,
+// so host-side generators and make_track reproduce the CPU reference. Defining
+// CMPMC_HOST_CRMATH selects the correctly rounded functions on the host as well.
+#if defined(__CUDA_ARCH__) || defined(CMPMC_HOST_CRMATH)
+CMPMC_HD double m_log(double x) { return crmath::log(x); }
+CMPMC_HD double m_sin(double x) { return crmath::sin(x); }
+CMPMC_HD double m_cos(double x) { return crmath::cos(x); }
+CMPMC_HD double m_exp(double x) { return crmath::exp(x); }
+CMPMC_HD double m_pow(double x, double y) { return crmath::pow(x, y); }
+CMPMC_HD double m_hypot(double x, double y) { return crmath::hypot(x, y); }
+CMPMC_HD double m_cbrt(double x) { return crmath::cbrt(x); }
+CMPMC_HD double m_acos(double x) { return crmath::acos(x); }
+#else
+CMPMC_HD double m_log(double x) { return ::log(x); }
+CMPMC_HD double m_sin(double x) { return ::sin(x); }
+CMPMC_HD double m_cos(double x) { return ::cos(x); }
+CMPMC_HD double m_exp(double x) { return ::exp(x); }
+CMPMC_HD double m_pow(double x, double y) { return ::pow(x, y); }
+CMPMC_HD double m_hypot(double x, double y) { return ::hypot(x, y); }
+CMPMC_HD double m_cbrt(double x) { return ::cbrt(x); }
+CMPMC_HD double m_acos(double x) { return ::acos(x); }
+#endif
 
 // ---- constants (core/units.hpp:26-72) ---------------------------------------------
 constexpr double kPi = 3.14159265358979323846;
@@ -130,7 +157,7 @@ struct Rng {
         const double cos_theta = 2.0 * uniform() - 1.0;
         const double sin_theta = sqrt(dmax(0.0, 1.0 - cos_theta * cos_theta));
         const double phi = kTwoPi * uniform();
-        return v3(sin_theta * cos(phi), sin_theta * sin(phi), cos_theta);
+        return v3(sin_theta * m_cos(phi), sin_theta * m_sin(phi), cos_theta);
     }
     // rng.hpp:86-96
     CMPMC_HD V3 lambertian_dir(V3 n) {
@@ -139,7 +166,7 @@ struct Rng {
         const double cos_theta = sqrt(dmax(0.0, 1.0 - sin_theta * sin_theta));
         const V3 u = orthogonal_unit(n);
         const V3 v = cross(n, u);
-        return unit(u * (sin_theta * cos(phi)) + v * (sin_theta * sin(phi)) + n * cos_theta);
+        return unit(u * (sin_theta * m_cos(phi)) + v * (sin_theta * m_sin(phi)) + n * cos_theta);
     }
 };
 
@@ -272,17 +299,17 @@ CMPMC_HD int sample_transverse_mode(const Lattice& L, Rng& rng) {
 CMPMC_HD double decay_angle_L_to_LT(double x, double vl, double vt) {
     const double m = vl / vt;
     const double cos_th = (1.0 + (x * x) * (1.0 - m * m) + 2.0 * x * m * m - m * m) / (2.0 * x);
-    return acos(dclamp(cos_th, -1.0, 1.0));
+    return m_acos(dclamp(cos_th, -1.0, 1.0));
 }
 CMPMC_HD double decay_angle_T_from_LT(double x, double vl, double vt) {
     const double m = vl / vt;
     const double cos_th = (1.0 - x * x + m * m * (1.0 - x) * (1.0 - x)) / (2.0 * m * (1.0 - x));
-    return acos(dclamp(cos_th, -1.0, 1.0));
+    return m_acos(dclamp(cos_th, -1.0, 1.0));
 }
 CMPMC_HD double decay_angle_TT(double x, double vl, double vt) {
     const double m = vl / vt;
     const double cos_th = (1.0 - m * m * (1.0 - x) * (1.0 - x) + m * m * x * x) / (2.0 * m * x);
-    return acos(dclamp(cos_th, -1.0, 1.0));
+    return m_acos(dclamp(cos_th, -1.0, 1.0));
 }
 // crystal_lattice.hpp:200-212
 CMPMC_HD double sample_cdf(const double* cdf, Rng& rng) {
@@ -326,7 +353,7 @@ CMPMC_HD BHit intersect_exit(double radius, double half_z, V3 p, V3 v) {
         h.n_in = v3(0.0, 0.0, 1.0);
     } else {
         const V3 hp = p + v * t_min;
-        const double r_xy = hypot(hp.x, hp.y);
+        const double r_xy = m_hypot(hp.x, hp.y);
         h.n_in = (r_xy > 1e-15) ? v3(-hp.x / r_xy, -hp.y / r_xy, 0.0) : v3(-1.0, 0.0, 0.0);
     }
     return h;
@@ -398,7 +425,7 @@ CMPMC_HD bool film_is_subgap(const Film& f, double e) { return e < 2.0 * f.gap_e
 CMPMC_HD bool film_is_thermalized(const Film& f, double e, Rng& rng) {
     if (f.temperature <= 0.0) return false;
     const double kT = kBoltzmann * f.temperature;
-    return e < kT * (-log(rng.uniform()));
+    return e < kT * (-m_log(rng.uniform()));
 }
 CMPMC_HD double film_escape_probability(const Film& f, double e, double thickness_frac) {
     if (f.gap_energy <= 0.0) return 1.0;
@@ -406,7 +433,7 @@ CMPMC_HD double film_escape_probability(const Film& f, double e, double thicknes
     if (denom <= 0.0) return 1.0;
     const double mfp = (f.v_sound * f.phonon_lifetime) / denom;
     const double path = thickness_frac * f.film_thickness;
-    return exp(-path / mfp);
+    return m_exp(-path / mfp);
 }
 CMPMC_HD double film_pb_integral(const Film& f, double omega) {
     const double d = f.gap_energy;
@@ -415,7 +442,7 @@ CMPMC_HD double film_pb_integral(const Film& f, double omega) {
     double acc = 0.0;
     for (int i = 0; i < 48; ++i) {
         const double t = kPi * (i + 0.5) / 48;
-        const double E = d + 0.5 * s * (1.0 - cos(t));
+        const double E = d + 0.5 * s * (1.0 - m_cos(t));
         acc += (E * (omega - E) + d * d) / sqrt((E + d) * (omega - E + d));
     }
     return acc * kPi / 48;
@@ -468,7 +495,7 @@ CMPMC_HD double film_sample_qp_energy(const Film& f, double E, Rng& rng) {
     const double w_max = dmax(qp_weight(E, d, d), qp_weight(E, d, 0.5 * E));
     for (;;) {
         const double u = rng.uniform();
-        const double s = sin(kHalfPi * u);
+        const double s = m_sin(kHalfPi * u);
         const double x = d + span * (s * s);
         if (rng.uniform() * w_max <= qp_weight(E, d, x)) return x;
     }
@@ -559,7 +586,7 @@ CMPMC_HD double film_absorb_phonon(const Film& f, double energy, KBuf& refl, dou
                 // (kaplan_film.hpp:193-194); its GCC build takes the left one first.
                 const double u_side = rng.uniform();
                 const double u_angle = rng.uniform();
-                const double frac = ((u_side < 0.5) ? 0.5 : 1.5) / cos(u_angle * 1.47);
+                const double frac = ((u_side < 0.5) ? 0.5 : 1.5) / m_cos(u_angle * 1.47);
                 if (rng.uniform() < film_escape_probability(f, E, frac)) {
                     refl.push(E);
                 } else if (f.keep_all_phonons || !film_is_subgap(f, E)) {

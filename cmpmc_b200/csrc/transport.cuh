@@ -97,15 +97,15 @@ CMPMC_HD void anharmonic_decay(const Lattice& L, Track& trk, C& ctx, EvStats& st
     const V3 dir1 = trk.k;
     const V3 perp = orthogonal_unit(dir1);
     const double phi = kTwoPi * rng.uniform();
-    const double c_phi = cos(phi);
-    const double s_phi = sin(phi);
+    const double c_phi = m_cos(phi);
+    const double s_phi = m_sin(phi);
     if (rng.uniform() < L.fTT_frac) {
         st.decays_TT++;
         const double x = sample_cdf(L.cdf_tt, rng);
         const double th1 = decay_angle_TT(x, L.v_sound, L.v_trans);
         const double th2 = decay_angle_TT(1.0 - x, L.v_sound, L.v_trans);
-        const V3 k1 = unit(rotate_around(rotate_around(dir1, perp, cos(th1), sin(th1)), dir1, c_phi, s_phi));
-        const V3 k2 = unit(rotate_around(rotate_around(dir1, perp, cos(-th2), sin(-th2)), dir1, c_phi, s_phi));
+        const V3 k1 = unit(rotate_around(rotate_around(dir1, perp, m_cos(th1), m_sin(th1)), dir1, c_phi, s_phi));
+        const V3 k2 = unit(rotate_around(rotate_around(dir1, perp, m_cos(-th2), m_sin(-th2)), dir1, c_phi, s_phi));
         const int m1 = sample_transverse_mode(L, rng);
         const int m2 = sample_transverse_mode(L, rng);
         ctx.push(make_track(L, trk.pos, k2, m2, (1.0 - x) * trk.E, trk.t, trk.w));
@@ -118,8 +118,8 @@ CMPMC_HD void anharmonic_decay(const Lattice& L, Track& trk, C& ctx, EvStats& st
         const double x = sample_cdf(L.cdf_lt, rng);
         const double thL = decay_angle_L_to_LT(x, L.v_sound, L.v_trans);
         const double thT = decay_angle_T_from_LT(x, L.v_sound, L.v_trans);
-        const V3 kL = unit(rotate_around(rotate_around(dir1, perp, cos(thL), sin(thL)), dir1, c_phi, s_phi));
-        const V3 kT = unit(rotate_around(rotate_around(dir1, perp, cos(-thT), sin(-thT)), dir1, c_phi, s_phi));
+        const V3 kL = unit(rotate_around(rotate_around(dir1, perp, m_cos(thL), m_sin(thL)), dir1, c_phi, s_phi));
+        const V3 kT = unit(rotate_around(rotate_around(dir1, perp, m_cos(-thT), m_sin(-thT)), dir1, c_phi, s_phi));
         const int mT = sample_transverse_mode(L, rng);
         ctx.push(make_track(L, trk.pos, kT, mT, (1.0 - x) * trk.E, trk.t, trk.w));
         trk.E = x * trk.E;
@@ -157,7 +157,7 @@ CMPMC_HD void transport_phonons(const Lattice& L, const Detector& D, C& ctx, EvS
             const double rate_poly = polycrystal_rate(L, trk.vmag);
             const double rate_down = downconversion_rate(L, trk.mode, trk.E);
             const double rate_tot = rate_iso + rate_poly + rate_down;
-            const double d_phys = (rate_tot > 1e-12) ? (-log(rng.uniform()) * (trk.vmag / rate_tot)) : kInf;
+            const double d_phys = (rate_tot > 1e-12) ? (-m_log(rng.uniform()) * (trk.vmag / rate_tot)) : kInf;
             const BHit bh = intersect_exit(D.radius, D.half_z, trk.pos, trk.vg);
 
             if (d_phys < bh.distance) {
@@ -339,10 +339,10 @@ CMPMC_HD double intervalley_rate(const Lattice& L, double ek, V3 E) {
     if (ek < L.iv_min_energy) return 0.0;
     if (L.iv_model == 0) {
         const double e0 = L.iv_quad_field;
-        return L.iv_quad_rate * pow(e0 * e0 + norm2(E), 0.5 * L.iv_quad_power);
+        return L.iv_quad_rate * m_pow(e0 * e0 + norm2(E), 0.5 * L.iv_quad_power);
     }
     const double e_vcm = norm(E) * 0.01;
-    return L.iv_lin_rate0 + L.iv_lin_rate1 * pow(e_vcm, L.iv_lin_power);
+    return L.iv_lin_rate0 + L.iv_lin_rate1 * m_pow(e_vcm, L.iv_lin_power);
 }
 CMPMC_HD double mfp_rate(double v, double mfp) { return (mfp > 0.0 && mfp < 1e20) ? (v / mfp) : 0.0; }
 
@@ -386,13 +386,13 @@ CMPMC_HD LukeEmit emit_luke(const Lattice& L, Charge& c, Rng& rng) {
     const V3 k_dir = vdiv(k_trk, k_mag);
     const double v = k_sound / k_mag;
     const double u = rng.uniform();
-    const double cos_th = dclamp(v + (1.0 - v) * cbrt(1.0 - u), v, 1.0);
+    const double cos_th = dclamp(v + (1.0 - v) * m_cbrt(1.0 - u), v, 1.0);
     const double sin_th = sqrt(dmax(0.0, 1.0 - cos_th * cos_th));
     const double phi = kTwoPi * rng.uniform();
     const double q = 2.0 * (k_mag * cos_th - k_sound);
     if (q <= 0.0) return none;
     const V3 perp = orthogonal_unit(k_dir);
-    const V3 q_vec = rotate_around(rotate_around(k_dir * q, perp, cos_th, sin_th), k_dir, cos(phi), sin(phi));
+    const V3 q_vec = rotate_around(rotate_around(k_dir * q, perp, cos_th, sin_th), k_dir, m_cos(phi), m_sin(phi));
     const V3 k_recoil = k_trk - q_vec;
     const double e_ph = norm(q_vec) * L.v_sound * kHbar;
     if (e_ph >= c.ekin || e_ph <= 0.0) return none;
@@ -511,7 +511,7 @@ CMPMC_HD void transport_charges(const Lattice& L, const Detector& D, C& ctx, EvS
                 trial.ekin = charge_ekin(L, trial);
                 const double a0 = R0.tot;
                 const double a1 = (charge_rates(L, trial, E).tot - a0) / dt_max;
-                const double lnu = log(rng.uniform());
+                const double lnu = m_log(rng.uniform());
                 if (fabs(a1) * dt_max <= 1e-9 * dmax(a0, 1e-300)) {
                     dt_phys = (a0 > 0.0) ? (-lnu / a0) : kInf;
                 } else {
@@ -520,7 +520,7 @@ CMPMC_HD void transport_charges(const Lattice& L, const Detector& D, C& ctx, EvS
                     if (!(dt_phys >= 0.0)) dt_phys = kInf;
                 }
             } else {
-                dt_phys = (r_tot > 1.0) ? (-log(rng.uniform()) / r_tot) : kInf;
+                dt_phys = (r_tot > 1.0) ? (-m_log(rng.uniform()) / r_tot) : kInf;
             }
             const double dt = dmin(dt_phys, dt_max);
             const V3 dp = E * (q_sign * kCLight * dt);

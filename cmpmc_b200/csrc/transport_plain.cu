@@ -158,6 +158,20 @@ __global__ void __launch_bounds__(128) k_plain_fp64(const Lattice L, const Detec
 
 }  // namespace
 
+__global__ void k_math_check(uint64_t n, const double* __restrict__ x, double* __restrict__ out) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        out[3 * i + 0] = crmath::log(x[i]);
+        out[3 * i + 1] = crmath::sin(x[i]);
+        out[3 * i + 2] = crmath::cos(x[i]);
+    }
+}
+
+cudaError_t launch_math_check(uint64_t n, const double* x, double* out) {
+    k_math_check<<<148, 256>>>(n, x, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_plain_fp64(const Lattice& L, const Detector& D, const RunArgs& a, int grid, int block,
                               cudaStream_t s) {
     k_plain_fp64<<<grid, block, 0, s>>>(L, D, a);

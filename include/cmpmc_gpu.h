@@ -286,6 +286,15 @@ int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_pe
                         uint64_t stack_capacity, uint64_t hit_capacity);
 int cmpmc_gpu_device_count(int* count);
 
+/* Correctly rounded log / sin / cos of the device transport (crmath), evaluated on the
+ * host; the device computes bit-identical values. */
+double cmpmc_cr_log(double x);
+double cmpmc_cr_sin(double x);
+double cmpmc_cr_cos(double x);
+/* Evaluates the device's log, sin and cos on n host inputs and writes out[3*i+{0,1,2}]
+ * (for checking that device and host agree bit for bit). */
+int cmpmc_gpu_math_check(int device, uint64_t n, const double* x, double* out);
+
 /* Layout self-check for bindings: writes sizeof of the ABI structs in the order
  * phonon_track, charge_track, sensor_hit, sim_stats, crystal_config, film_config,
  * surface, detector, run_desc, run_out (at most n values). Returns the ABI version. */

@@ -32,6 +32,16 @@
 //       (even events: FT 7.5 meV phonon at the origin; odd events: e-/h+ pair),
 //       field 2 V over 2.54 cm, luke_sample_fraction 0.02; seed 77
 //   tpl same as tp with luke_sample_fraction 1 (every Luke phonon tracked)
+//
+// Built with -DCMPMC_ORACLE_CRLIBM (as cmpmc_ref_crlibm) the transport uses a correctly
+// rounded libm (ref_crlibm.hpp); the generators and the lattice build keep the
+// platform libm, as they do in the device path (they run on the host there).
+#ifdef CMPMC_ORACLE_CRLIBM
+#include "ref_crlibm.hpp"
+#define CMPMC_SET_CRLIBM(v) (cmpmc_oracle::g_crlibm = (v))
+#else
+#define CMPMC_SET_CRLIBM(v) ((void)0)
+#endif
 #include "cmpmc/cmpmc.hpp"
 
 #include <chrono>
@@ -92,7 +102,14 @@ struct Generator {
     const DetectorModel* det;
     size_t n_valleys;
 
+    // the generator runs on the host with the platform libm in every build
     void operator()(EventInput& in) const {
+        CMPMC_SET_CRLIBM(false);
+        generate(in);
+        CMPMC_SET_CRLIBM(true);
+    }
+
+    void generate(EventInput& in) const {
         if (w == "c0") {
             in.phonons.push_back(engine->make_track({0, 0, 0}, in.rng.isotropic_dir(), PhononMode::L, 7.5e-3));
             in.injected_eV += 7.5e-3;

@@ -10,6 +10,9 @@ compiled from its own headers by `make -C oracle ref`) and stores compact record
                         initial tracks, per-event SimStats and every SensorHit
   <workload>_summary.npz per-event summaries for many events (hit count, integer counters,
                         sums over the hits, hash of the discrete hit fields)
+  <workload>_cr_*.npz   the same from oracle/_ref/cmpmc_ref_crlibm: the reference whose
+                        transport uses a correctly rounded libm (oracle/ref_crlibm.hpp);
+                        `floor` = fraction of events on which it agrees with the glibc build
 
 Usage: python tests/golden/make_golden.py   (needs the reference build; takes ~1 min)
 """
@@ -27,10 +30,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-from tests.golden.records import (EVENT_DTYPE, SUMMARY_DTYPE, read_dump, summarize)  # noqa: E402
+from tests.golden.records import compare_summaries, read_dump, summarize  # noqa: E402
 
 REF = os.path.join(ROOT, "oracle", "_ref", "cmpmc_ref")
 REF_TABLES = os.path.join(ROOT, "oracle", "_ref", "cmpmc_ref_tables")
+REF_CR = os.path.join(ROOT, "oracle", "_ref", "cmpmc_ref_crlibm")
 
 # workload -> (full events, summary events)
 PLAN = {
@@ -43,9 +47,9 @@ PLAN = {
 }
 
 
-def dump(workload: str, first: int, n: int, tmp: str):
-    prefix = os.path.join(tmp, f"{workload}_{first}_{n}")
-    subprocess.run([REF, "dump", workload, str(first), str(n), "0", prefix], check=True)
+def dump(workload: str, first: int, n: int, tmp: str, exe: str = REF):
+    prefix = os.path.join(tmp, f"{workload}_{first}_{n}_{os.path.basename(exe)}")
+    subprocess.run([exe, "dump", workload, str(first), str(n), "0", prefix], check=True)
     return read_dump(prefix, n)
 
 
@@ -89,16 +93,26 @@ def main() -> None:
                             cdf_lt=cdf[:1024], cdf_tt=cdf[1024:], hv=hv, sample_idx=idx,
                             sample=octa[:, idx[:, 0], idx[:, 1], :])
 
-        # workloads
+        # workloads: the reference (glibc libm) and the reference with a correctly rounded
+        # libm in the transport (cmpmc_ref_crlibm); "floor" is the fraction of events on
+        # which the two agree (the device's transcendentals are correctly rounded)
         for wl, (n_full, n_sum) in PLAN.items():
             if n_full:
                 d = dump(wl, 0, n_full, tmp)
                 np.savez_compressed(os.path.join(HERE, f"{wl}_full.npz"), **d)
+                dc = dump(wl, 0, n_full, tmp, REF_CR)
+                np.savez_compressed(os.path.join(HERE, f"{wl}_cr_full.npz"), **dc)
             d = dump(wl, 0, n_sum, tmp)
             s = summarize(d["events"], d["hit_offsets"], d["hits"])
             np.savez_compressed(os.path.join(HERE, f"{wl}_summary.npz"), summary=s,
                                 injected=d["injected"], rng_state=d["rng_state"])
-            print(wl, n_full, n_sum, int(d["hit_offsets"][-1]), "hits")
+            dc = dump(wl, 0, n_sum, tmp, REF_CR)
+            sc = summarize(dc["events"], dc["hit_offsets"], dc["hits"])
+            floor = compare_summaries(s, sc)
+            np.savez_compressed(os.path.join(HERE, f"{wl}_cr_summary.npz"), summary=sc,
+                                floor_mask=floor["agree_mask"], floor=np.array(floor["frac"]))
+            print(wl, n_full, n_sum, int(d["hit_offsets"][-1]), "hits; glibc vs correctly rounded agree on",
+                  f"{100 * floor['frac']:.2f}% of events")
     gl = subprocess.run(["ldd", "--version"], capture_output=True, text=True).stdout.split("\n")[0]
     with open(os.path.join(HERE, "PROVENANCE.txt"), "w") as f:
         f.write("Generated by tests/golden/make_golden.py from the unmodified reference CMPMC\n"
