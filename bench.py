@@ -1,0 +1,355 @@
+"""Benchmark of the transport hot path (run_events over phonon tracks) on B200.
+
+Workload (the mixed-energy phonon batch): 10,000 events x 100 phonons = 1,000,000 primary
+tracks per GPU, energies log-uniform on [1, 30] meV, modes L/ST/FT 0.10/0.36/0.54, origins
+uniform in the Ge cylinder (R 3.81 cm, half height 1.27 cm), isotropic directions, seed 7;
+default Ge lattice and detector (Al Kaplan films on both faces). One step = one run_events
+pass over the whole batch in the batched FP32 form (FP32 geometry, FP64 energy ledger and
+time of flight), hits kept.
+
+  value  primary phonon tracks / s, inputs resident on the device, device-timed (CUDA
+         events on the library's stream), max over ranks
+  e2e    the same through the public API with host buffers: pinned host inputs copied in
+         and every hit, the hit offsets and the statistics copied back, each step
+  plain_fp64  the plain FP64 form (bit-exact event streams) on the same workload, one step
+
+Multi-GPU (torchrun): every rank runs its own 10,000 events (events rank*10000 + i), no
+collective on the data path (weak scaling); barrier and max-over-ranks timing through
+torch.distributed.
+
+`--impl reference` times the reference's own CPU run_events (oracle/_ref/cmpmc_ref, the
+unmodified reference built from its headers) on all host cores, on a bounded sample of the
+same workload per step, and prints the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "phonon tracks/s, 1 B200: batched FP32 vs plain FP64 at matched hit stats"
+UNIT = "primary phonon tracks/s"
+EVENTS = 10000
+PER_EVENT = 100
+SEED = 7
+BYTES_PER_STEP = 192  # algorithmic FP32 track-state traffic per transport step
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per transport step of the batched kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "batched_fp32_mixed_energy.json")) as f:
+            return float(json.load(f)["dram_bytes_per_step"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        sms, maxs, reasons = [], [], set()
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                sms.append(float(p[1]))
+                maxs.append(float(p[2]))
+                for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                                   p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        except Exception:
+            pass
+        if not sms:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxs), "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def reference_arm(args) -> None:
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    exe = os.path.join(ROOT, "oracle", "_ref", "cmpmc_ref")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cmpmc_ref is not built (make -C oracle ref)"}))
+        return
+    sample_events = args.ref_events
+    cores = os.cpu_count() or 1
+
+    def one(first):
+        out = subprocess.run([exe, "time", "c1", str(first), str(sample_events), "0"], check=True,
+                             capture_output=True, text=True).stdout
+        return json.loads(out.strip().splitlines()[-1])
+
+    for w in range(args.warmup):
+        one(w * sample_events)
+    walls, prim, steps = 0.0, 0, 0
+    for k in range(args.steps):
+        r = one((args.warmup + k) * sample_events)
+        walls += r["wall_seconds"]
+        prim += r["primaries"]
+        steps += r["total_steps"]
+    value = prim / walls
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * walls / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "mixed_energy_phonons", "events_per_step": sample_events, "primaries_per_event": PER_EVENT,
+                   "seed": SEED, "threads": cores},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{sample_events} events x {PER_EVENT} primaries per step (events advance "
+                                   f"through the seed-{SEED} stream), reference run_events on all cores",
+                         "steps_per_s": steps / walls},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(sample_events: int):
+    exe = os.path.join(ROOT, "oracle", "_ref", "cmpmc_ref")
+    if not os.path.exists(exe):
+        return None
+    out = subprocess.run([exe, "time", "c1", "0", str(sample_events), "0"], check=True, capture_output=True,
+                         text=True).stdout
+    r = json.loads(out.strip().splitlines()[-1])
+    return {"value": r["primaries"] / r["wall_seconds"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
+            "sample": f"events 0-{sample_events - 1} of the workload ({r['primaries']} primaries), reference "
+                      f"run_events (oracle/_ref/cmpmc_ref, unmodified reference) on {r['threads']} threads",
+            "steps_per_s": r["total_steps"] / r["wall_seconds"], "wall_seconds": r["wall_seconds"]}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--events", type=int, default=EVENTS)
+    ap.add_argument("--ref-events", type=int, default=400)
+    ap.add_argument("--cpu-events", type=int, default=1000)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import cmpmc_b200 as cm
+    from cmpmc_b200 import _ffi
+
+    rank, world, local = dist_env()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = local
+    torch.cuda.set_device(dev)
+
+    lat = cm.CrystalLattice(cm.materials.Germanium())
+    det = cm.DetectorModel()
+    eng = cm.SimulationEngine(lat, det)
+    first = rank * args.events
+    t_gen = time.perf_counter()
+    packed = eng.generate(cm.workloads.mixed_energy, args.events, SEED, first_event=first)
+    t_gen = time.perf_counter() - t_gen
+    n_prim = int(packed.phonon_offsets[-1])
+    lib = _ffi.load()
+    h = eng.context(dev)
+
+    # device-resident inputs (torch owns the memory)
+    def to_dev(a):
+        t = torch.from_numpy(a.view(np.uint8).reshape(-1).copy()).to(f"cuda:{dev}")
+        return t
+    d_rng, d_inj = to_dev(packed.rng_state), to_dev(packed.injected_eV)
+    d_off, d_ph = to_dev(packed.phonon_offsets), to_dev(packed.phonons)
+    torch.cuda.synchronize(dev)
+
+    def desc(on_device: bool, host=None):
+        d = _ffi.RunDescC()
+        d.n_events = args.events
+        d.first_event = first
+        d.keep_hits = 1
+        d.form = _ffi.FORM_BATCHED_FP32
+        d.seed = SEED
+        if on_device:
+            d.rng_state, d.injected_eV = d_rng.data_ptr(), d_inj.data_ptr()
+            d.phonon_offsets, d.phonons = d_off.data_ptr(), d_ph.data_ptr()
+            d.inputs_on_device = 1
+            d.outputs_on_device = 1
+        else:
+            d.rng_state, d.injected_eV, d.phonon_offsets, d.phonons = host
+        return d
+
+    def run(d):
+        out = _ffi.RunOutC()
+        st = lib.cmpmc_gpu_run_events(h, C.byref(d), C.byref(out))
+        if st != 0:
+            buf = C.create_string_buffer(512)
+            lib.cmpmc_gpu_last_error(h, buf, 512)
+            raise RuntimeError(buf.value.decode())
+        return out
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")  # 256 MiB > 126 MB L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    dd = desc(True)
+    for _ in range(args.warmup):
+        flush.zero_()
+        run(dd)
+    barrier()
+    ms, kms, launches, steps_total, hits_total = [], [], 0, 0, 0
+    with ClockSampler(dev) as clocks:
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            o = run(dd)
+            ms.append(o.total_ms)
+            kms.append(o.kernel_ms)
+            launches += o.kernel_launches
+            steps_total += o.stats.total_steps
+            hits_total += o.n_hits
+        barrier()
+        wall = time.perf_counter() - t0
+    step_ms = max_over_ranks(sum(ms) / args.steps)
+    kernel_ms = max_over_ranks(sum(kms) / args.steps)
+    value = world * n_prim / (step_ms * 1e-3)
+
+    # e2e: host buffers (pinned), H2D of the inputs and D2H of every output inside the call
+    def pinned(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        t.numpy()[:] = a.view(np.uint8).reshape(-1)
+        return t
+    hp = [pinned(packed.rng_state), pinned(packed.injected_eV), pinned(packed.phonon_offsets), pinned(packed.phonons)]
+    hd = desc(False, tuple(t.data_ptr() for t in hp))
+    run(hd)
+    barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        barrier()
+        t1 = time.perf_counter()
+        o = run(hd)
+        e2e_ms.append(1e3 * (time.perf_counter() - t1))
+    e2e_step = max_over_ranks(sum(e2e_ms) / args.steps)
+    h2d = sum(t.numel() for t in hp)
+    d2h = int(o.n_hits) * 56 + (args.events + 1) * 8 + 208
+
+    # plain FP64 form on the same workload (bit-exact event streams), one step
+    plain = None
+    if not args.no_plain:
+        dp = desc(True)
+        dp.form = _ffi.FORM_PLAIN_FP64
+        o = run(dp)
+        p_ms = max_over_ranks(o.total_ms)
+        plain = {"value": world * n_prim / (p_ms * 1e-3), "unit": UNIT, "ms_per_step": p_ms,
+                 "steps_per_s": o.stats.total_steps / (o.kernel_ms * 1e-3)}
+
+    peak, peak_kind = measured_peaks()
+    steps_per_launch = steps_total / args.steps
+    achieved = steps_per_launch * BYTES_PER_STEP / (sum(kms) / args.steps * 1e-3) / 1e9
+    tps = profile_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "mixed_energy_phonons", "events": args.events * world, "primaries_per_event": PER_EVENT,
+                   "primaries": n_prim * world, "form": "batched_fp32", "seed": SEED,
+                   "energy": "log-uniform 1-30 meV", "modes": "L/ST/FT 0.10/0.36/0.54",
+                   "l2": "256 MiB buffer written between timed steps (L2 126 MB); inputs 128 MB, hits ~1.5 GB per step"},
+        "kernel_ms_per_step": kernel_ms,
+        "steps_per_s": world * steps_per_launch / (kernel_ms * 1e-3),
+        "hits_per_step": hits_total / args.steps,
+        "e2e": {"value": world * n_prim / (e2e_step * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "bytes_per_step": BYTES_PER_STEP,
+                     "traffic": (tps * steps_per_launch if tps else None)},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+        "wall_s_timed": wall,
+        "generator_s": t_gen,
+    }
+    if plain is not None:
+        line["plain_fp64"] = plain
+        line["batched_over_plain"] = value / plain["value"]
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_events)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -91,6 +91,8 @@ struct cmpmc_gpu_ctx {
     uint64_t hit_cap = 0;
     DevBuf in_rng, in_inj, in_phoff, in_ph, in_choff, in_ch;
     DevBuf stack, cstack, hit_stage, hit_key, counters, ev_stats, ev_nhits, offsets, hits_out, total;
+    DevBuf unit_event, ev_offsets, ev_stats2;  // batched form: unit -> event map, event offsets / stats
+    const float* cdf_f = nullptr;              // FP32 copies of the decay tables (in `tables`)
     HostBuf h_hits, h_offsets, h_evstats, h_total, h_counters;
     cudaEvent_t e_start = nullptr, e_k0 = nullptr, e_k1 = nullptr, e_end = nullptr;
     std::string last_error;
@@ -171,7 +173,16 @@ int cmpmc_gpu_create(const cmpmc_lattice* lat, const cmpmc_detector* det, int de
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->e_end);
     const size_t oct_bytes = lat->oct.size() * sizeof(OctEntry);
     const size_t cdf_bytes = 2 * kNCdf * sizeof(double);
-    if (e == cudaSuccess) e = ctx->tables.ensure(oct_bytes + cdf_bytes);
+    const size_t cdf_f_bytes = 2 * kNCdf * sizeof(float);
+    float cdf_f[2 * kNCdf];
+    for (int i = 0; i < kNCdf; ++i) {
+        cdf_f[i] = static_cast<float>(lat->cdf_lt[i]);
+        cdf_f[kNCdf + i] = static_cast<float>(lat->cdf_tt[i]);
+    }
+    if (e == cudaSuccess) e = ctx->tables.ensure(oct_bytes + cdf_bytes + cdf_f_bytes);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(static_cast<char*>(ctx->tables.p) + oct_bytes + cdf_bytes, cdf_f, cdf_f_bytes,
+                       cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(ctx->tables.p, lat->oct.data(), oct_bytes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
@@ -189,6 +200,7 @@ int cmpmc_gpu_create(const cmpmc_lattice* lat, const cmpmc_detector* det, int de
     ctx->L.oct = static_cast<const OctEntry*>(ctx->tables.p);
     ctx->L.cdf_lt = reinterpret_cast<const double*>(static_cast<char*>(ctx->tables.p) + oct_bytes);
     ctx->L.cdf_tt = ctx->L.cdf_lt + kNCdf;
+    ctx->cdf_f = reinterpret_cast<const float*>(static_cast<char*>(ctx->tables.p) + oct_bytes + cdf_bytes);
     ctx->D = detector_view(*det);
     // Keep the 3 MiB group-velocity table resident in L2 (it is gathered on every step).
     cudaStreamAttrValue attr;
@@ -210,7 +222,8 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf* b : {&ctx->tables, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
-                      &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total})
+                      &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
+                      &ctx->unit_event, &ctx->ev_offsets, &ctx->ev_stats2})
         b->release();
     for (HostBuf* b : {&ctx->h_hits, &ctx->h_offsets, &ctx->h_evstats, &ctx->h_total, &ctx->h_counters})
         b->release();
@@ -254,6 +267,7 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     if (n > (1ull << 31)) return fail(ctx, CMPMC_ERR_INVALID, "too many events in one call");
     if (n > 0 && (!d->rng_state || !d->injected_eV || !d->phonon_offsets))
         return fail(ctx, CMPMC_ERR_INVALID, "rng_state, injected_eV and phonon_offsets are required");
+    const bool batched = d->form == CMPMC_FORM_BATCHED_FP32;
     const bool has_charges = d->charge_offsets != nullptr;
     std::string err;
     const int vst = validate_config(ctx->cfg, ctx->det, has_charges, err);
@@ -266,7 +280,6 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     // ---- inputs ------------------------------------------------------------------
     RunArgs a;
     std::memset(&a, 0, sizeof(a));
-    a.n_events = n;
     a.first_event = d->first_event;
     a.keep_hits = d->keep_hits;
     a.seed = d->seed;
@@ -278,6 +291,12 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
         a.ph = d->phonons;
         a.ch_off = d->charge_offsets;
         a.ch = d->charges;
+        if (n > 0) {
+            CK(cudaMemcpyAsync(&n_ph, d->phonon_offsets + n, 8, cudaMemcpyDeviceToHost, s), "read track count");
+            if (has_charges)
+                CK(cudaMemcpyAsync(&n_ch, d->charge_offsets + n, 8, cudaMemcpyDeviceToHost, s), "read charge count");
+            CK(cudaStreamSynchronize(s), "read track count");
+        }
     } else if (n > 0) {
         n_ph = d->phonon_offsets[n];
         n_ch = has_charges ? d->charge_offsets[n] : 0;
@@ -289,7 +308,8 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
         CK(ctx->in_ph.ensure(std::max<uint64_t>(n_ph, 1) * sizeof(cmpmc_phonon_track)), "alloc phonons");
         CK(cudaMemcpyAsync(ctx->in_rng.p, d->rng_state, n * 32, cudaMemcpyHostToDevice, s), "copy rng");
         CK(cudaMemcpyAsync(ctx->in_inj.p, d->injected_eV, n * 8, cudaMemcpyHostToDevice, s), "copy injected");
-        CK(cudaMemcpyAsync(ctx->in_phoff.p, d->phonon_offsets, (n + 1) * 8, cudaMemcpyHostToDevice, s), "copy offsets");
+        CK(cudaMemcpyAsync(ctx->in_phoff.p, d->phonon_offsets, (n + 1) * 8, cudaMemcpyHostToDevice, s),
+           "copy offsets");
         if (n_ph)
             CK(cudaMemcpyAsync(ctx->in_ph.p, d->phonons, n_ph * sizeof(cmpmc_phonon_track), cudaMemcpyHostToDevice, s),
                "copy phonons");
@@ -303,34 +323,47 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
             CK(cudaMemcpyAsync(ctx->in_choff.p, d->charge_offsets, (n + 1) * 8, cudaMemcpyHostToDevice, s),
                "copy charge offsets");
             if (n_ch)
-                CK(cudaMemcpyAsync(ctx->in_ch.p, d->charges, n_ch * sizeof(cmpmc_charge_track),
-                                   cudaMemcpyHostToDevice, s),
+                CK(cudaMemcpyAsync(ctx->in_ch.p, d->charges, n_ch * sizeof(cmpmc_charge_track), cudaMemcpyHostToDevice,
+                                   s),
                    "copy charges");
             a.ch_off = ctx->in_choff.as<uint64_t>();
             a.ch = ctx->in_ch.as<cmpmc_charge_track>();
         }
     }
+    if (batched && n_ch > 0)
+        return fail(ctx, CMPMC_ERR_INVALID, "the batched FP32 form transports phonons only (charges: plain form)");
 
-    // ---- launch geometry and work buffers ------------------------------------------
-    const bool batched = d->form == CMPMC_FORM_BATCHED_FP32;
+    // ---- work units: events (plain form) or primary phonons (batched form) ---------
+    const uint64_t units = batched ? n_ph : n;
+    a.n_events = units;
     int bps = ctx->bps;
     if (!bps) {
         CK(batched ? batched_fp32_occupancy(ctx->tpb, &bps) : plain_fp64_occupancy(ctx->tpb, &bps), "occupancy");
         bps = std::max(bps, 1);
     }
     uint64_t grid = static_cast<uint64_t>(ctx->num_sms) * bps;
-    const uint64_t per_thread_units = std::max<uint64_t>(n, 1);
-    grid = std::min<uint64_t>(grid, (per_thread_units + ctx->tpb - 1) / ctx->tpb);
+    grid = std::min<uint64_t>(grid, (std::max<uint64_t>(units, 1) + ctx->tpb - 1) / ctx->tpb);
     grid = std::max<uint64_t>(grid, 1);
     const uint64_t slots = grid * ctx->tpb;
+    const size_t stack_entry = batched ? batched_stack_entry_bytes() : sizeof(GTrack);
 
-    CK(ctx->ev_stats.ensure(std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats)), "alloc event stats");
-    CK(ctx->ev_nhits.ensure(std::max<uint64_t>(n, 1) * 8), "alloc event hit counts");
-    CK(ctx->offsets.ensure((n + 1) * 8), "alloc hit offsets");
+    CK(ctx->ev_stats.ensure(std::max<uint64_t>(units, 1) * sizeof(cmpmc_sim_stats)), "alloc unit stats");
+    CK(ctx->ev_nhits.ensure(std::max<uint64_t>(units, 1) * 8), "alloc unit hit counts");
+    CK(ctx->offsets.ensure((units + 1) * 8), "alloc unit offsets");
     CK(ctx->counters.ensure(sizeof(Counters)), "alloc counters");
     CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
     CK(ctx->h_counters.ensure(sizeof(Counters)), "alloc host counters");
     CK(ctx->cstack.ensure(slots * ctx->cstack_cap * sizeof(GCharge)), "alloc charge stacks");
+    if (batched) {
+        CK(ctx->unit_event.ensure(std::max<uint64_t>(units, 1) * 4), "alloc unit map");
+        CK(ctx->ev_offsets.ensure((n + 1) * 8), "alloc event offsets");
+        if (d->want_event_stats) CK(ctx->ev_stats2.ensure(std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats)),
+                                    "alloc event stats");
+        if (n > 0) {
+            CK(launch_unit_event(a.ph_off, n, ctx->unit_event.as<uint32_t>(), s), "unit map");
+            ++launches;
+        }
+    }
     a.cstack = ctx->cstack.as<GCharge>();
     a.cstack_cap = ctx->cstack_cap;
     a.ev_stats = ctx->ev_stats.as<cmpmc_sim_stats>();
@@ -341,15 +374,12 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     a.err = &dc->err;
 
     uint64_t hit_cap = ctx->hit_cap;
-    if (!hit_cap) {
-        const uint64_t units = d->inputs_on_device ? n : std::max<uint64_t>(n, n_ph + n_ch);
-        hit_cap = std::max<uint64_t>(4096, units * 32);
-    }
+    if (!hit_cap) hit_cap = std::max<uint64_t>(4096, std::max<uint64_t>(n, n_ph + n_ch) * 32);
     Counters hc{};
     float kms = 0.0f;
     for (int attempt = 0;; ++attempt) {
         if (!d->keep_hits) hit_cap = 1;
-        CK(ctx->stack.ensure(slots * ctx->stack_cap * sizeof(GTrack)), "alloc phonon stacks");
+        CK(ctx->stack.ensure(slots * ctx->stack_cap * stack_entry), "alloc phonon stacks");
         CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
         CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
         a.stack = ctx->stack.as<GTrack>();
@@ -359,8 +389,9 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
         a.hit_cap = hit_cap;
         CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s), "memset counters");
         CK(cudaEventRecord(ctx->e_k0, s), "event");
-        if (n > 0) {
-            CK(batched ? launch_batched_fp32(ctx->L, ctx->D, a, static_cast<int>(grid), ctx->tpb, s)
+        if (units > 0) {
+            CK(batched ? launch_batched_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->unit_event.as<uint32_t>(),
+                                             static_cast<int>(grid), ctx->tpb, s)
                        : launch_plain_fp64(ctx->L, ctx->D, a, static_cast<int>(grid), ctx->tpb, s),
                "transport launch");
             ++launches;
@@ -374,10 +405,10 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
         const bool stack_over = (hc.err & (kErrPhononStack | kErrChargeStack)) != 0;
         const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
         if (!stack_over && !hits_over) break;
-        if (attempt >= 6) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack or hit buffer overflow persists");
-        if (hc.err & kErrPhononStack) ctx->stack_cap = std::min<uint32_t>(ctx->stack_cap * 4, 1u << 24);
+        if (attempt >= 10) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack or hit buffer overflow persists");
+        if (hc.err & kErrPhononStack) ctx->stack_cap = std::min<uint32_t>(ctx->stack_cap * 8, 1u << 24);
         if (hc.err & kErrChargeStack) {
-            ctx->cstack_cap *= 4;
+            ctx->cstack_cap = std::min<uint32_t>(ctx->cstack_cap * 8, 1u << 20);
             CK(ctx->cstack.ensure(slots * ctx->cstack_cap * sizeof(GCharge)), "alloc charge stacks");
             a.cstack = ctx->cstack.as<GCharge>();
             a.cstack_cap = ctx->cstack_cap;
@@ -390,12 +421,19 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     // ---- merge ------------------------------------------------------------------------
     const uint64_t n_hits = d->keep_hits ? hc.hit_count : 0;
     CK(ctx->hits_out.ensure(std::max<uint64_t>(n_hits, 1) * sizeof(cmpmc_sensor_hit)), "alloc hits");
-    if (n > 0) {
+    uint64_t* ev_offsets = batched ? ctx->ev_offsets.as<uint64_t>() : ctx->offsets.as<uint64_t>();
+    cmpmc_sim_stats* ev_stats = batched ? ctx->ev_stats2.as<cmpmc_sim_stats>() : ctx->ev_stats.as<cmpmc_sim_stats>();
+    if (n > 0 && batched) {
+        CK(launch_batched_finish(a, n, a.ph_off, a.injected, ctx->offsets.as<uint64_t>(), ev_offsets,
+                                 ctx->hits_out.as<cmpmc_sensor_hit>(), n_hits, ctx->total.as<cmpmc_sim_stats>(),
+                                 d->want_event_stats ? ev_stats : nullptr, s, &launches),
+           "merge kernels");
+    } else if (n > 0) {
         CK(launch_finish(a, ctx->offsets.as<uint64_t>(), ctx->hits_out.as<cmpmc_sensor_hit>(), n_hits,
                          ctx->total.as<cmpmc_sim_stats>(), s, &launches),
            "merge kernels");
     } else {
-        CK(cudaMemsetAsync(ctx->offsets.p, 0, 8, s), "memset offsets");
+        CK(cudaMemsetAsync(ev_offsets, 0, 8, s), "memset offsets");
         CK(cudaMemsetAsync(ctx->total.p, 0, sizeof(cmpmc_sim_stats), s), "memset totals");
     }
     CK(ctx->h_total.ensure(sizeof(cmpmc_sim_stats)), "alloc host totals");
@@ -403,8 +441,8 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
        "copy totals");
     if (d->outputs_on_device) {
         out->hits = ctx->hits_out.as<cmpmc_sensor_hit>();
-        out->hit_offsets = ctx->offsets.as<uint64_t>();
-        out->event_stats = d->want_event_stats ? ctx->ev_stats.as<cmpmc_sim_stats>() : nullptr;
+        out->hit_offsets = ev_offsets;
+        out->event_stats = d->want_event_stats ? ev_stats : nullptr;
     } else {
         CK(ctx->h_hits.ensure(std::max<uint64_t>(n_hits, 1) * sizeof(cmpmc_sensor_hit)), "alloc host hits");
         CK(ctx->h_offsets.ensure((n + 1) * 8), "alloc host offsets");
@@ -412,11 +450,10 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
             CK(cudaMemcpyAsync(ctx->h_hits.p, ctx->hits_out.p, n_hits * sizeof(cmpmc_sensor_hit),
                                cudaMemcpyDeviceToHost, s),
                "copy hits");
-        CK(cudaMemcpyAsync(ctx->h_offsets.p, ctx->offsets.p, (n + 1) * 8, cudaMemcpyDeviceToHost, s), "copy offsets");
+        CK(cudaMemcpyAsync(ctx->h_offsets.p, ev_offsets, (n + 1) * 8, cudaMemcpyDeviceToHost, s), "copy offsets");
         if (d->want_event_stats && n > 0) {
             CK(ctx->h_evstats.ensure(n * sizeof(cmpmc_sim_stats)), "alloc host event stats");
-            CK(cudaMemcpyAsync(ctx->h_evstats.p, ctx->ev_stats.p, n * sizeof(cmpmc_sim_stats),
-                               cudaMemcpyDeviceToHost, s),
+            CK(cudaMemcpyAsync(ctx->h_evstats.p, ev_stats, n * sizeof(cmpmc_sim_stats), cudaMemcpyDeviceToHost, s),
                "copy event stats");
         }
         out->hits = ctx->h_hits.as<cmpmc_sensor_hit>();

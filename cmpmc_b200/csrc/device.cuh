@@ -134,9 +134,16 @@ CMPMC_HD void stats_from_event(const EvStats& e, double injected, cmpmc_sim_stat
 cudaError_t launch_plain_fp64(const Lattice& L, const Detector& D, const RunArgs& a, int grid, int block,
                               cudaStream_t s);
 cudaError_t plain_fp64_occupancy(int block, int* blocks_per_sm);
-cudaError_t launch_batched_fp32(const Lattice& L, const Detector& D, const RunArgs& a, int grid, int block,
-                                cudaStream_t s);
+cudaError_t launch_batched_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
+                                const uint32_t* unit_event, int grid, int block, cudaStream_t s);
 cudaError_t batched_fp32_occupancy(int block, int* blocks_per_sm);
+cudaError_t launch_unit_event(const uint64_t* ph_off, uint64_t n_events, uint32_t* unit_event, cudaStream_t s);
+size_t batched_stack_entry_bytes();
+// merge of the batched form: units are primaries; event offsets / stats derive from them
+cudaError_t launch_batched_finish(const RunArgs& a, uint64_t n_events, const uint64_t* ph_off,
+                                  const double* injected, uint64_t* unit_offsets, uint64_t* ev_offsets,
+                                  cmpmc_sensor_hit* hits_out, uint64_t out_cap, cmpmc_sim_stats* total,
+                                  cmpmc_sim_stats* ev_stats_out, cudaStream_t s, int* launches);
 cudaError_t launch_math_check(uint64_t n, const double* x, double* out);
 cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
                           cmpmc_sim_stats* total, cudaStream_t s, int* launches);

@@ -98,7 +98,74 @@ __global__ void __launch_bounds__(kReduceThreads) k_reduce_stats(const cmpmc_sim
     if (t < kStatsWords) reinterpret_cast<uint64_t*>(total)[t] = acc[0][t];
 }
 
+__global__ void k_event_offsets(const uint64_t* __restrict__ unit_offsets, const uint64_t* __restrict__ ph_off,
+                                uint64_t n_events, uint64_t* __restrict__ ev_offsets) {
+    for (uint64_t ev = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; ev <= n_events;
+         ev += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        ev_offsets[ev] = unit_offsets[ph_off[ev]];
+}
+
+// per-event SimStats of the batched form: the event's primaries summed in order
+__global__ void k_event_stats(const cmpmc_sim_stats* __restrict__ unit_stats, const uint64_t* __restrict__ ph_off,
+                              const double* __restrict__ injected, uint64_t n_events,
+                              cmpmc_sim_stats* __restrict__ out) {
+    for (uint64_t ev = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; ev < n_events;
+         ev += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t u[kStatsWords];
+        double d[kStatsWords];
+        for (int w = 0; w < kStatsWords; ++w) {
+            u[w] = 0;
+            d[w] = 0.0;
+        }
+        for (uint64_t j = ph_off[ev]; j < ph_off[ev + 1]; ++j) {
+            const uint64_t* src = reinterpret_cast<const uint64_t*>(unit_stats + j);
+            for (int w = 0; w < kStatsWords; ++w) {
+                if (stats_word_is_double(w)) d[w] += __longlong_as_double(static_cast<long long>(src[w]));
+                else u[w] += src[w];
+            }
+        }
+        d[23] = injected[ev];
+        uint64_t* dst = reinterpret_cast<uint64_t*>(out + ev);
+        for (int w = 0; w < kStatsWords; ++w)
+            dst[w] = stats_word_is_double(w) ? static_cast<uint64_t>(__double_as_longlong(d[w])) : u[w];
+    }
+}
+
+// total injected energy (deterministic single-block sum) into total->total_injected_eV
+__global__ void __launch_bounds__(kReduceThreads) k_sum_injected(const double* __restrict__ injected, uint64_t n,
+                                                                 cmpmc_sim_stats* total) {
+    __shared__ double acc[kReduceThreads];
+    const int t = threadIdx.x;
+    const uint64_t chunk = (n + kReduceThreads - 1) / kReduceThreads;
+    const uint64_t lo = min(n, t * chunk), hi = min(n, lo + chunk);
+    double s = 0.0;
+    for (uint64_t i = lo; i < hi; ++i) s += injected[i];
+    acc[t] = s;
+    __syncthreads();
+    for (int stride = kReduceThreads / 2; stride > 0; stride >>= 1) {
+        if (t < stride) acc[t] += acc[t + stride];
+        __syncthreads();
+    }
+    if (t == 0) total->total_injected_eV = acc[0];
+}
+
 }  // namespace
+
+cudaError_t launch_batched_finish(const RunArgs& a, uint64_t n_events, const uint64_t* ph_off,
+                                  const double* injected, uint64_t* unit_offsets, uint64_t* ev_offsets,
+                                  cmpmc_sensor_hit* hits_out, uint64_t out_cap, cmpmc_sim_stats* total,
+                                  cmpmc_sim_stats* ev_stats_out, cudaStream_t s, int* launches) {
+    cudaError_t e = launch_finish(a, unit_offsets, hits_out, out_cap, total, s, launches);
+    if (e != cudaSuccess) return e;
+    k_event_offsets<<<148, 256, 0, s>>>(unit_offsets, ph_off, n_events, ev_offsets);
+    k_sum_injected<<<1, kReduceThreads, 0, s>>>(injected, n_events, total);
+    *launches += 2;
+    if (ev_stats_out) {
+        k_event_stats<<<148, 128, 0, s>>>(a.ev_stats, ph_off, injected, n_events, ev_stats_out);
+        *launches += 1;
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
                           cmpmc_sim_stats* total, cudaStream_t s, int* launches) {

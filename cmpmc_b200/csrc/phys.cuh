@@ -27,7 +27,8 @@ namespace cmpmc_gpu {
 // trajectories that are sensitive to the last bit); on the host they are the platform libm,
 // so host-side generators and make_track reproduce the CPU reference. Defining
 // CMPMC_HOST_CRMATH selects the correctly rounded functions on the host as well.
-#if defined(__CUDA_ARCH__) || defined(CMPMC_HOST_CRMATH)
+// CMPMC_DEVICE_FAST_MATH (the batched FP32 form) keeps CUDA's libm on the device.
+#if (defined(__CUDA_ARCH__) && !defined(CMPMC_DEVICE_FAST_MATH)) || defined(CMPMC_HOST_CRMATH)
 CMPMC_HD double m_log(double x) { return crmath::log(x); }
 CMPMC_HD double m_sin(double x) { return crmath::sin(x); }
 CMPMC_HD double m_cos(double x) { return crmath::cos(x); }

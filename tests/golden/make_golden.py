@@ -10,6 +10,8 @@ compiled from its own headers by `make -C oracle ref`) and stores compact record
                         initial tracks, per-event SimStats and every SensorHit
   <workload>_summary.npz per-event summaries for many events (hit count, integer counters,
                         sums over the hits, hash of the discrete hit fields)
+  c1_hist.npz           per-event hit histograms (time, radius, energy) of 2000 mixed-energy
+                        events (200,000 primaries), for the batched FP32 form's chi^2 tests
   <workload>_cr_*.npz   the same from oracle/_ref/cmpmc_ref_crlibm: the reference whose
                         transport uses a correctly rounded libm (oracle/ref_crlibm.hpp);
                         `floor` = fraction of events on which it agrees with the glibc build
@@ -30,7 +32,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-from tests.golden.records import compare_summaries, read_dump, summarize  # noqa: E402
+from tests.golden.records import compare_summaries, event_histograms, read_dump, summarize  # noqa: E402
 
 REF = os.path.join(ROOT, "oracle", "_ref", "cmpmc_ref")
 REF_TABLES = os.path.join(ROOT, "oracle", "_ref", "cmpmc_ref_tables")
@@ -113,6 +115,17 @@ def main() -> None:
                                 floor_mask=floor["agree_mask"], floor=np.array(floor["frac"]))
             print(wl, n_full, n_sum, int(d["hit_offsets"][-1]), "hits; glibc vs correctly rounded agree on",
                   f"{100 * floor['frac']:.2f}% of events")
+        # mixed-energy batch: per-event hit histograms of the reference (2000 events,
+        # 200,000 primaries) for the statistical parity of the batched FP32 form
+        d = dump("c1", 0, 2000, tmp)
+        lo, hi = float(d["hits"]["edep"].min()), float(d["hits"]["edep"].max())
+        h = event_histograms(d["hit_offsets"], d["hits"], (lo, hi * (1 + 1e-9)))
+        st = d["events"]["stats"]
+        np.savez_compressed(os.path.join(HERE, "c1_hist.npz"), **h,
+                            injected=d["injected"].sum(), deposited=st["total_deposited_eV"].sum(),
+                            escaped=st["escaped_or_killed_eV"].sum(), steps=st["total_steps"].sum(),
+                            n_hits=len(d["hits"]))
+        print("c1 histograms from", len(d["hits"]), "hits")
     gl = subprocess.run(["ldd", "--version"], capture_output=True, text=True).stdout.split("\n")[0]
     with open(os.path.join(HERE, "PROVENANCE.txt"), "w") as f:
         f.write("Generated by tests/golden/make_golden.py from the unmodified reference CMPMC\n"

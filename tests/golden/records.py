@@ -117,3 +117,49 @@ def compare_summaries(ref: np.ndarray, got: np.ndarray, rel_tol: float = 1e-9) -
     return {"n": int(len(ref)), "agree": int(agree.sum()), "frac": float(agree.mean()) if len(ref) else 1.0,
             "same_n_hits": int(same_n.sum()), "same_hash": int(same_hash.sum()), "same_ints": int(same_ints.sum()),
             "cont_close": int(cont.sum()), "agree_mask": agree}
+
+
+# ---- histogram statistics (hit time, radial position, energy) ---------------------------
+HIST_SPEC = {
+    "time": (256, 0.0, 2e-3),          # s
+    "radius": (64, 0.0, 3.81e-2),      # m
+    "edep": (64, None, None),          # eV, range from the reference sample
+}
+
+
+def event_histograms(hit_offsets: np.ndarray, hits: np.ndarray, edep_range: tuple) -> dict:
+    """Per-bin sum and sum of squares over events of the per-event hit histograms.
+
+    Hits of one event are correlated, so comparisons treat the event as the independent
+    unit: the mean per-event count in a bin and its variance across events."""
+    n = len(hit_offsets) - 1
+    ev = np.repeat(np.arange(n), np.diff(hit_offsets.astype(np.int64)))
+    out = {"n_events": n}
+    values = {"time": hits["time"], "radius": np.hypot(hits["pos"][:, 0], hits["pos"][:, 1]), "edep": hits["edep"]}
+    for name, (nb, lo, hi) in HIST_SPEC.items():
+        if name == "edep":
+            lo, hi = edep_range
+        b = np.floor((values[name] - lo) / (hi - lo) * nb).astype(np.int64)
+        ok = (b >= 0) & (b < nb)
+        counts = np.zeros((n, nb), dtype=np.float64)
+        np.add.at(counts, (ev[ok], b[ok]), 1.0)
+        out[name + "_sum"] = counts.sum(axis=0)
+        out[name + "_sumsq"] = (counts * counts).sum(axis=0)
+    out["edep_range"] = np.array(edep_range, dtype=np.float64)
+    return out
+
+
+def hist_chi2(a: dict, b: dict, name: str, min_count: float = 20.0):
+    """chi^2 of the difference of mean per-event histograms, with per-bin variances
+    estimated from the spread across events. Returns (chi2, dof, p)."""
+    from scipy.stats import chi2 as chi2_dist
+    na, nb = a["n_events"], b["n_events"]
+    sa, qa = a[name + "_sum"], a[name + "_sumsq"]
+    sb, qb = b[name + "_sum"], b[name + "_sumsq"]
+    ma, mb = sa / na, sb / nb
+    va = np.maximum(qa / na - ma * ma, 0.0) / na
+    vb = np.maximum(qb / nb - mb * mb, 0.0) / nb
+    use = (sa + sb >= min_count) & (va + vb > 0)
+    c2 = float(np.sum((ma[use] - mb[use]) ** 2 / (va[use] + vb[use])))
+    dof = int(use.sum())
+    return c2, dof, float(chi2_dist.sf(c2, dof))

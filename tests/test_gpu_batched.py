@@ -1,0 +1,112 @@
+"""The batched FP32 form: statistical parity with the FP64 reference.
+
+The batched form gives every primary phonon its own random substream, so its events are
+not the reference's events; what must agree are the distributions. Bar: chi^2 p > 0.01 for
+the hit time (256 bins, 0-2 ms), radial position (64 bins) and energy (64 bins) histograms
+against the reference (mixed-energy workload, 200,000 primaries) and against the plain
+FP64 device form, and energy-ledger closure |injected - deposited - escaped| / injected
+<= 1e-6. The chi^2 treats an event as the independent unit (tests/golden/records.py).
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import WORKLOAD_SEED, detector_for, golden, workload_of
+from tests.golden.records import event_histograms, hist_chi2
+
+pytestmark = pytest.mark.gpu
+
+P_MIN = 0.01
+LEDGER_TOL = 1e-6
+
+
+def _engine(ge_lattice, wl):
+    import cmpmc_b200 as cm
+    return cm.SimulationEngine(ge_lattice, detector_for(wl))
+
+
+def _batched(eng, wl, n, seed=None, want_event_stats=False):
+    import cmpmc_b200 as cm
+    opt = cm.RunOptions(seed=WORKLOAD_SEED[wl], form="batched_fp32", want_event_stats=want_event_stats)
+    packed = eng.generate(workload_of(wl), n, WORKLOAD_SEED[wl])
+    if seed is not None:
+        opt.seed = seed
+    return eng.run_packed(packed, opt)
+
+
+@pytest.fixture(scope="module")
+def c1_batched(ge_lattice):
+    eng = _engine(ge_lattice, "c1")
+    return _batched(eng, "c1", 2000, want_event_stats=True)
+
+
+def test_batched_histograms_match_reference(c1_batched):
+    ref = dict(golden("c1_hist.npz"))
+    got = event_histograms(c1_batched.hit_offsets, c1_batched.hits, tuple(ref["edep_range"]))
+    for name in ("time", "radius", "edep"):
+        c2, dof, p = hist_chi2(ref, got, name)
+        print(f"{name}: chi2 {c2:.1f} dof {dof} p {p:.3f}")
+        assert p > P_MIN, (name, c2, dof, p)
+    n_ref, n_got = int(ref["n_hits"]), len(c1_batched.hits)
+    assert abs(n_got - n_ref) / n_ref < 0.01
+
+
+def test_batched_ledger_closes(c1_batched):
+    st = c1_batched.stats
+    inj = st.total_injected_eV
+    assert abs(inj - st.total_deposited_eV - st.escaped_or_killed_eV) / inj <= LEDGER_TOL
+    ref = golden("c1_hist.npz")
+    assert abs(inj - float(ref["injected"])) / inj < 1e-12  # same generator, same primaries
+    # deposited fraction agrees with the reference at the 1% level
+    assert abs(st.total_deposited_eV / inj - float(ref["deposited"]) / float(ref["injected"])) < 0.01
+
+
+def test_batched_event_bookkeeping(c1_batched):
+    r = c1_batched
+    assert len(r.hit_offsets) == 2001
+    assert int(r.hit_offsets[-1]) == len(r.hits)
+    assert np.all(np.diff(r.hit_offsets.astype(np.int64)) >= 0)
+    ev = r.event_stats
+    assert int(ev["total_steps"].sum()) == r.stats.total_steps
+    assert int(ev["sensor_hits"].sum()) == len(r.hits)
+    assert np.array_equal(np.diff(r.hit_offsets.astype(np.int64)), ev["sensor_hits"].astype(np.int64))
+    np.testing.assert_allclose(ev["total_injected_eV"].sum(), r.stats.total_injected_eV, rtol=1e-12)
+
+
+def test_batched_matches_plain_fp64_statistics(ge_lattice):
+    """Single 7.5 meV L phonons in the volume: batched FP32 vs plain FP64 on the device."""
+    import cmpmc_b200 as cm
+    eng = _engine(ge_lattice, "c4")
+    n = 20000
+    plain = cm.run_events(eng, n, workload_of("c4"), cm.RunOptions(seed=17))
+    batched = _batched(eng, "c4", n)
+    lo = min(plain.hits["edep"].min(), batched.hits["edep"].min())
+    hi = max(plain.hits["edep"].max(), batched.hits["edep"].max()) * (1 + 1e-9)
+    a = event_histograms(plain.hit_offsets, plain.hits, (lo, hi))
+    b = event_histograms(batched.hit_offsets, batched.hits, (lo, hi))
+    for name in ("time", "radius", "edep"):
+        c2, dof, p = hist_chi2(a, b, name)
+        print(f"{name}: chi2 {c2:.1f} dof {dof} p {p:.3f}")
+        assert p > P_MIN, (name, c2, dof, p)
+    sp, sb = plain.stats, batched.stats
+    for st in (sp, sb):
+        assert abs(st.total_injected_eV - st.total_deposited_eV - st.escaped_or_killed_eV) / st.total_injected_eV < 1e-9
+    # mean steps per primary within 2 %
+    assert abs(sb.total_steps / sp.total_steps - 1.0) < 0.02
+
+
+def test_batched_deterministic(ge_lattice):
+    eng = _engine(ge_lattice, "c1")
+    a = _batched(eng, "c1", 100)
+    eng.configure(threads_per_block=64, blocks_per_sm=2)
+    b = _batched(eng, "c1", 100)
+    assert a.hits.tobytes() == b.hits.tobytes()
+    assert a.stats.record().tobytes() == b.stats.record().tobytes()
+    c = _batched(eng, "c1", 100, seed=12345)
+    assert a.hits.tobytes() != c.hits.tobytes()
+
+
+def test_batched_rejects_charges(ge_lattice):
+    import cmpmc_b200 as cm
+    eng = _engine(ge_lattice, "c2")
+    with pytest.raises(cm.CmpmcError):
+        cm.run_events(eng, 4, workload_of("c2"), cm.RunOptions(seed=11, form="batched_fp32"))

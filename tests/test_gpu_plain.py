@@ -93,7 +93,7 @@ def test_full_hit_records_match(ge_lattice, wl):
 def test_run_totals_and_closure(ge_lattice):
     """Totals equal the sum of the per-event records; energy closes (tests/test_parallel.cpp:126-137
     and tests/test_engine_energy_closure.cpp:14-21 of the reference, closure 1e-9)."""
-    ref = golden("c0_summary.npz")["summary"]
+    ref = golden("c0_cr_summary.npz")["summary"]
     _, res = _run(ge_lattice, "c0", 2000)
     st = res.stats
     assert st.total_steps == int(ref["ints"][:2000, 0].sum())
