@@ -1,0 +1,259 @@
+// run_events_gpu.hpp -- header-only C++ adapter from CMPMC's API to the B200 C ABI.
+//
+// Include this next to the reference's own headers ("cmpmc/cmpmc.hpp"), build one
+// cmpmc_b200::GpuEngine(lattice.config(), detector) and call gpu.run_events(n_events,
+// generate, options) where the reference code calls cmpmc::run_events(engine, n_events,
+// generate, options) (include/cmpmc/transport/parallel.hpp:76-148). The generator is the same user callback:
+// it runs on the host, once per event, from Rng::for_stream(options.seed, i), with the
+// reference's EventInput, Rng and SimulationEngine::make_track, so the initial stacks and
+// the post-generator random state are exactly the reference's. Transport runs on the
+// device; the RunResult is rebuilt from the device output (SensorHit and SimStats records
+// are byte-identical, include/cmpmc_gpu.h).
+//
+// The device needs the crystal's configuration (it rebuilds the CrystalLattice tables with
+// the same arithmetic) and the DetectorModel. Guarded modules raise the reference's
+// UnvalidatedModuleError; configurations the device does not support (interface
+// transmission, electrode masks, charge release other than RecordOnly, bilinear / exact
+// kinematics, mesh fields) raise std::invalid_argument.
+#pragma once
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <exception>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../cmpmc_gpu.h"
+
+namespace cmpmc_b200 {
+
+enum class Form { PlainFP64 = CMPMC_FORM_PLAIN_FP64, BatchedFP32 = CMPMC_FORM_BATCHED_FP32 };
+
+struct GpuRunOptions {
+    int device = 0;
+    Form form = Form::PlainFP64;
+};
+
+namespace detail {
+
+inline void check(int status, const cmpmc_gpu_ctx* ctx, const char* what) {
+    if (status == CMPMC_OK) return;
+    char buf[1024];
+    cmpmc_gpu_last_error(ctx, buf, sizeof(buf));
+    const std::string msg = std::string(what) + ": " + buf;
+    if (status == CMPMC_ERR_UNVALIDATED) throw cmpmc::UnvalidatedModuleError(msg);
+    if (status == CMPMC_ERR_INVALID) throw std::invalid_argument(msg);
+    throw std::runtime_error(msg);
+}
+
+inline cmpmc_crystal_config to_c(const cmpmc::CrystalConfig& c) {
+    cmpmc_crystal_config o;
+    std::memset(&o, 0, sizeof(o));
+    o.group = static_cast<int32_t>(c.group);
+    o.has_custom_C = c.has_custom_C ? 1 : 0;
+    o.density = c.density;
+    o.C11 = c.C11; o.C12 = c.C12; o.C13 = c.C13; o.C14 = c.C14; o.C16 = c.C16; o.C33 = c.C33;
+    o.C44 = c.C44; o.C66 = c.C66;
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) o.C_custom[i][j] = c.C_custom[i][j];
+    o.beta = c.beta; o.gamma = c.gamma; o.lambda = c.lambda; o.mu = c.mu;
+    o.B_iso = c.B_iso; o.A_anh = c.A_anh; o.fTT_frac = c.fTT_frac; o.polycrystal_mfp_m = c.polycrystal_mfp_m;
+    o.fLDOS = c.fLDOS; o.fSTDOS = c.fSTDOS; o.fFTDOS = c.fFTDOS;
+    o.debye_freq = c.debye_freq; o.v_sound = c.v_sound; o.v_trans = c.v_trans;
+    o.bandgap = c.bandgap; o.pair_energy = c.pair_energy; o.fano_factor = c.fano_factor;
+    o.epsilon_rel = c.epsilon_rel; o.neutral_impurity_cm3 = c.neutral_impurity_cm3;
+    o.alpha_nonparabolic = c.alpha_nonparabolic; o.h_mass_ratio = c.h_mass_ratio;
+    o.e_mass_tensor[0] = c.e_mass_tensor.x; o.e_mass_tensor[1] = c.e_mass_tensor.y;
+    o.e_mass_tensor[2] = c.e_mass_tensor.z;
+    if (c.valley_dirs.size() > CMPMC_MAX_VALLEYS) throw std::invalid_argument("too many valleys");
+    o.n_valleys = static_cast<int32_t>(c.valley_dirs.size());
+    for (size_t k = 0; k < c.valley_dirs.size(); ++k) {
+        o.valley_dirs[k][0] = c.valley_dirs[k].x;
+        o.valley_dirs[k][1] = c.valley_dirs[k].y;
+        o.valley_dirs[k][2] = c.valley_dirs[k].z;
+    }
+    o.ac_deform_e = c.ac_deform_e; o.ac_deform_h = c.ac_deform_h;
+    const size_t n_iv = std::min<size_t>({c.iv_deform_eV_m.size(), c.iv_energy_eV.size(), CMPMC_MAX_IV});
+    o.n_iv = static_cast<int32_t>(n_iv);
+    for (size_t i = 0; i < n_iv; ++i) {
+        o.iv_deform_eV_m[i] = c.iv_deform_eV_m[i];
+        o.iv_energy_eV[i] = c.iv_energy_eV[i];
+    }
+    o.iv_min_energy = c.iv_min_energy;
+    o.iv_model = static_cast<int32_t>(c.iv_model);
+    o.iv_quad_rate = c.iv_quad_rate; o.iv_quad_field = c.iv_quad_field; o.iv_quad_power = c.iv_quad_power;
+    o.iv_lin_rate0 = c.iv_lin_rate0; o.iv_lin_rate1 = c.iv_lin_rate1; o.iv_lin_power = c.iv_lin_power;
+    o.e_trapping_mfp_m = c.e_trapping_mfp_m; o.h_trapping_mfp_m = c.h_trapping_mfp_m;
+    o.e_trap_ion_d0_mfp_m = c.e_trap_ion_d0_mfp_m; o.e_trap_ion_a_mfp_m = c.e_trap_ion_a_mfp_m;
+    o.h_trap_ion_d_mfp_m = c.h_trap_ion_d_mfp_m; o.h_trap_ion_a0_mfp_m = c.h_trap_ion_a0_mfp_m;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) o.orient[i][j] = c.orient.m[i][j];
+    return o;
+}
+
+inline void poly(const std::vector<double>& v, double* dst, int32_t& n) {
+    if (v.size() > CMPMC_MAX_POLY) throw std::invalid_argument("surface polynomial longer than CMPMC_MAX_POLY");
+    n = static_cast<int32_t>(v.size());
+    for (size_t i = 0; i < v.size(); ++i) dst[i] = v[i];
+}
+
+inline cmpmc_detector to_c(const cmpmc::DetectorModel& d) {
+    if (d.mesh_field_3d.has_value() || d.mesh_field_2d.has_value())
+        throw std::invalid_argument("mesh fields are not available through this adapter");
+    cmpmc_detector o;
+    std::memset(&o, 0, sizeof(o));
+    o.radius = d.solid.radius;
+    o.half_z = d.solid.half_z;
+    o.e_field[0] = d.e_field.field_Vm.x;
+    o.e_field[1] = d.e_field.field_Vm.y;
+    o.e_field[2] = d.e_field.field_Vm.z;
+    for (int i = 0; i < 3; ++i) {
+        const cmpmc::SurfaceProperty& s = d.surfaces[i];
+        cmpmc_surface& t = o.surfaces[i];
+        t.prob_abs = s.prob_abs; t.prob_refl = s.prob_refl; t.refl_cutoff = s.refl_cutoff; t.anh_cutoff = s.anh_cutoff;
+        t.prob_charge_abs = s.prob_charge_abs; t.prob_charge_spec = s.prob_charge_spec;
+        t.min_k_elec = s.min_k_elec; t.min_k_hole = s.min_k_hole; t.spec_prob_const = s.spec_prob_const;
+        poly(s.spec_coeffs, t.spec_coeffs, t.n_spec);
+        poly(s.diff_coeffs, t.diff_coeffs, t.n_diff);
+        poly(s.anh_coeffs, t.anh_coeffs, t.n_anh);
+        t.demo_values = s.demo_values ? 1 : 0;
+        t.has_amm = s.amm_interface.has_value() ? 1 : 0;
+        t.has_mask = s.electrode_mask.has_value() ? 1 : 0;
+        if (s.kaplan_sensor.has_value()) {
+            const cmpmc::KaplanFilm& f = *s.kaplan_sensor;
+            t.has_film = 1;
+            t.film.film_absorption = f.film_absorption; t.film.film_thickness = f.film_thickness;
+            t.film.v_sound = f.v_sound; t.film.gap_energy = f.gap_energy; t.film.phonon_lifetime = f.phonon_lifetime;
+            t.film.phonon_lifetime_slope = f.phonon_lifetime_slope; t.film.low_qp_limit = f.low_qp_limit;
+            t.film.high_qp_limit = f.high_qp_limit; t.film.subgap_absorption = f.subgap_absorption;
+            t.film.absorber_gap = f.absorber_gap; t.film.absorber_eff = f.absorber_eff;
+            t.film.absorber_eff_slope = f.absorber_eff_slope; t.film.temperature = f.temperature;
+            t.film.keep_all_phonons = f.keep_all_phonons ? 1 : 0;
+            t.film.loss_model = static_cast<int32_t>(f.loss_model);
+            t.film.phonon_loss_time = f.phonon_loss_time;
+        }
+    }
+    o.max_bounces = d.max_bounces;
+    o.russian_roulette_bounces = d.russian_roulette_bounces;
+    o.russian_roulette_survival = d.russian_roulette_survival;
+    o.min_phonon_eV = d.min_phonon_eV;
+    o.luke_sample_fraction = d.luke_sample_fraction;
+    o.charge_max_dk_frac = d.charge_max_dk_frac;
+    o.charge_dt_cap_s = d.charge_dt_cap_s;
+    o.charge_sampling_dk_frac = d.charge_sampling_dk_frac;
+    o.charge_stepping = static_cast<int32_t>(d.charge_stepping);
+    o.charge_release = static_cast<int32_t>(d.charge_release);
+    o.fermi_level_above_Ev_eV = d.fermi_level_above_Ev_eV;
+    o.electrode_seed_max_gap = d.electrode_seed_max_gap;
+    o.allow_unvalidated = d.allow_unvalidated ? 1 : 0;
+    o.jump_to_ballistic = d.jump_to_ballistic.enabled ? 1 : 0;
+    return o;
+}
+
+}  // namespace detail
+
+// A device context for one crystal and detector (create once, run many times).
+class GpuEngine {
+public:
+    GpuEngine(const cmpmc::CrystalConfig& cfg, const cmpmc::DetectorModel& det, int device = 0)
+        : ccfg_(detail::to_c(cfg)), cdet_(detail::to_c(det)) {
+        detail::check(cmpmc_lattice_create(&ccfg_, &lat_), nullptr, "lattice");
+        const int st = cmpmc_gpu_create(lat_, &cdet_, device, &ctx_);
+        if (st != CMPMC_OK) {
+            cmpmc_lattice_destroy(lat_);
+            detail::check(st, nullptr, "device context");
+        }
+    }
+    ~GpuEngine() {
+        cmpmc_gpu_destroy(ctx_);
+        cmpmc_lattice_destroy(lat_);
+    }
+    GpuEngine(const GpuEngine&) = delete;
+    GpuEngine& operator=(const GpuEngine&) = delete;
+
+    // run_events on the device; `engine` is the reference engine built from the same
+    // lattice and detector (the generator calls its make_track).
+    template <class Generator>
+    cmpmc::RunResult run_events(uint64_t n_events, Generator&& generate, const cmpmc::RunOptions& options = {},
+                                const GpuRunOptions& gpu = {}) {
+        const auto t0 = std::chrono::steady_clock::now();
+        std::vector<uint64_t> rng(4 * n_events), ph_off(n_events + 1, 0), ch_off(n_events + 1, 0);
+        std::vector<double> injected(n_events, 0.0);
+        std::vector<std::vector<cmpmc::PhononTrack>> ph(n_events);
+        std::vector<std::vector<cmpmc::ChargeTrack>> ch(n_events);
+        // generator on the host thread pool, one stream per event (parallel.hpp:102-109)
+        const unsigned nt = options.threads ? options.threads : std::max(1u, std::thread::hardware_concurrency());
+        std::atomic<uint64_t> next{0};
+        std::exception_ptr error;
+        std::mutex error_mutex;
+        auto worker = [&]() {
+            try {
+                for (;;) {
+                    const uint64_t ev = next.fetch_add(1);
+                    if (ev >= n_events) return;
+                    cmpmc::Rng r = cmpmc::Rng::for_stream(options.seed, ev);
+                    cmpmc::EventInput in{ev, r, ph[ev], ch[ev], 0.0};
+                    generate(in);
+                    injected[ev] = in.injected_eV;
+                    std::memcpy(&rng[4 * ev], r.s, 32);
+                }
+            } catch (...) {
+                std::lock_guard<std::mutex> lock(error_mutex);
+                if (!error) error = std::current_exception();
+            }
+        };
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nt; ++t) pool.emplace_back(worker);
+        for (auto& t : pool) t.join();
+        if (error) std::rethrow_exception(error);
+        std::vector<cmpmc::PhononTrack> phonons;
+        std::vector<cmpmc::ChargeTrack> charges;
+        for (uint64_t ev = 0; ev < n_events; ++ev) {
+            phonons.insert(phonons.end(), ph[ev].begin(), ph[ev].end());
+            charges.insert(charges.end(), ch[ev].begin(), ch[ev].end());
+            ph_off[ev + 1] = phonons.size();
+            ch_off[ev + 1] = charges.size();
+        }
+        static_assert(sizeof(cmpmc::PhononTrack) == sizeof(cmpmc_phonon_track), "PhononTrack layout");
+        static_assert(sizeof(cmpmc::ChargeTrack) == sizeof(cmpmc_charge_track), "ChargeTrack layout");
+        static_assert(sizeof(cmpmc::SensorHit) == sizeof(cmpmc_sensor_hit), "SensorHit layout");
+        static_assert(sizeof(cmpmc::SimStats) == sizeof(cmpmc_sim_stats), "SimStats layout");
+        cmpmc_run_desc d;
+        std::memset(&d, 0, sizeof(d));
+        d.n_events = n_events;
+        d.rng_state = rng.data();
+        d.injected_eV = injected.data();
+        d.phonon_offsets = ph_off.data();
+        d.phonons = reinterpret_cast<const cmpmc_phonon_track*>(phonons.data());
+        if (!charges.empty()) {
+            d.charge_offsets = ch_off.data();
+            d.charges = reinterpret_cast<const cmpmc_charge_track*>(charges.data());
+        }
+        d.keep_hits = options.keep_hits ? 1 : 0;
+        d.form = static_cast<int32_t>(gpu.form);
+        d.seed = options.seed;
+        cmpmc_run_out out;
+        detail::check(cmpmc_gpu_run_events(ctx_, &d, &out), ctx_, "run_events");
+        cmpmc::RunResult r;
+        std::memcpy(&r.stats, &out.stats, sizeof(r.stats));
+        r.hits.resize(out.n_hits);
+        if (out.n_hits) std::memcpy(r.hits.data(), out.hits, out.n_hits * sizeof(cmpmc_sensor_hit));
+        r.hit_offsets.assign(out.hit_offsets, out.hit_offsets + n_events + 1);
+        r.threads_used = nt;
+        r.wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return r;
+    }
+
+private:
+    cmpmc_crystal_config ccfg_;
+    cmpmc_detector cdet_;
+    cmpmc_lattice* lat_ = nullptr;
+    cmpmc_gpu_ctx* ctx_ = nullptr;
+};
+
+}  // namespace cmpmc_b200

@@ -1,0 +1,40 @@
+// Compiled by tests/test_shim.py against the reference's headers: the reference's own
+// generator code (tests/test_parallel.cpp:110-125) unchanged, run through the device adapter.
+#include "cmpmc/cmpmc.hpp"
+#include "cmpmc_b200/run_events_gpu.hpp"
+
+#include <cstdio>
+
+int main() {
+    using namespace cmpmc;
+    const CrystalLattice lattice(materials::Germanium());
+    DetectorModel det;
+    det.e_field = UniformElectricField::from_bias(2.0, 2.54 * units::cm);
+    det.luke_sample_fraction = 0.02;
+    const SimulationEngine engine(lattice, det);
+    const ChargePhysics charges(lattice);
+    const size_t n_valleys = lattice.config().valley_dirs.size();
+    auto gen = [&](EventInput& in) {
+        if (in.event_id % 2 == 0) {
+            in.phonons.push_back(engine.make_track({0, 0, 0}, in.rng.isotropic_dir(), PhononMode::FT, 7.5e-3));
+            in.injected_eV += 7.5e-3;
+        } else {
+            const auto v = static_cast<uint16_t>(in.rng.uniform() * n_valleys) % n_valleys;
+            in.charges.push_back(charges.make_charge(ExcitationType::Electron, {0, 0, 0}, in.rng.isotropic_dir(), 1e-6, v));
+            in.charges.push_back(charges.make_charge(ExcitationType::Hole, {0, 0, 0}, in.rng.isotropic_dir(), 1e-6, 0));
+        }
+    };
+    RunOptions opt;
+    opt.seed = 77;
+    try {
+        cmpmc_b200::GpuEngine gpu(lattice.config(), det);
+        const RunResult r = gpu.run_events(203, gen, opt);
+        const RunResult c = run_events(engine, 203, gen, opt);
+        std::printf("device hits %zu cpu hits %zu steps %llu vs %llu\n", r.hits.size(), c.hits.size(),
+                    (unsigned long long)r.stats.total_steps, (unsigned long long)c.stats.total_steps);
+        return 0;
+    } catch (const std::runtime_error& e) {
+        std::printf("device unavailable: %s\n", e.what());
+        return 3;
+    }
+}
