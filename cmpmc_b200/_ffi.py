@@ -151,6 +151,9 @@ _SIG = {
     "cmpmc_cr_sin": (_f64, [_f64]),
     "cmpmc_cr_cos": (_f64, [_f64]),
     "cmpmc_gpu_math_check": (_i32, [_i32, _u64, C.c_void_p, C.c_void_p]),
+    "cmpmc_gpu_run_events_noalloc": (_i32, [C.c_void_p, C.POINTER(DetectorC), _i32, _u64, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _u64,
+                                            C.c_void_p, C.POINTER(SimStatsC), C.POINTER(_u64)]),
 }
 
 EXPORTED = sorted(_SIG)

@@ -286,6 +286,30 @@ int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_pe
                         uint64_t stack_capacity, uint64_t hit_capacity);
 int cmpmc_gpu_device_count(int* count);
 
+/* Allocation-free run of the plain FP64 form (phonon-only events). No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc -- code running inside a
+ * framework whose caching allocator owns the device memory, code with a fixed memory
+ * budget, or latency-critical loops where an allocation may block or fail. It allocates
+ * no device memory: every input and output below is caller-owned device memory, and the
+ * per-thread stacks and counters live in a fixed array of the library (about 29 MiB, plus
+ * 3 MiB of lattice tables), which every GPU that loads the library holds until exit.
+ *   inputs : rng_state [n][4], injected_eV [n], phonon_offsets [n+1], phonons
+ *   outputs: event_stats [n], hit_offsets [n+1], hits [hit_capacity] (event order)
+ *   host   : *total (run SimStats), *n_hits (hits the run produced, also when they do not fit)
+ * At most 64 tracks may sit on one event's stack at a time (CMPMC_ERR_CAPACITY otherwise);
+ * CMPMC_ERR_CAPACITY is also returned when *n_hits > hit_capacity (nothing is written).
+ * The transport runs twice (count, then write), so a call costs about two plain runs.
+ * The first call on a device resolves the array's device address and uploads the tables:
+ * make it before any stream capture. Calls share the array and clear what they use, so
+ * calls whose work overlaps on the GPU race: serialize them. `stream` is a cudaStream_t
+ * (NULL: the default stream). */
+int cmpmc_gpu_run_events_noalloc(const cmpmc_lattice* lat, const cmpmc_detector* det, int device,
+                                 uint64_t n_events, const uint64_t* rng_state, const double* injected_eV,
+                                 const uint64_t* phonon_offsets, const cmpmc_phonon_track* phonons,
+                                 cmpmc_sim_stats* event_stats, uint64_t* hit_offsets,
+                                 cmpmc_sensor_hit* hits, uint64_t hit_capacity, void* stream,
+                                 cmpmc_sim_stats* total, uint64_t* n_hits);
+
 /* Correctly rounded log / sin / cos of the device transport (crmath), evaluated on the
  * host; the device computes bit-identical values. */
 double cmpmc_cr_log(double x);
