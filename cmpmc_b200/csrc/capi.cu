@@ -91,7 +91,7 @@ struct cmpmc_gpu_ctx {
     uint64_t hit_cap = 0;
     DevBuf in_rng, in_inj, in_phoff, in_ph, in_choff, in_ch;
     DevBuf stack, cstack, hit_stage, hit_key, counters, ev_stats, ev_nhits, offsets, hits_out, total;
-    DevBuf unit_event, ev_offsets, ev_stats2;  // batched form: unit -> event map, event offsets / stats
+    DevBuf unit_event, ev_offsets, ev_stats2, partials;  // batched form: unit -> event map, event offsets / stats
     const float* cdf_f = nullptr;              // FP32 copies of the decay tables (in `tables`)
     HostBuf h_hits, h_offsets, h_evstats, h_total, h_counters;
     cudaEvent_t e_start = nullptr, e_k0 = nullptr, e_k1 = nullptr, e_end = nullptr;
@@ -223,7 +223,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     for (DevBuf* b : {&ctx->tables, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
-                      &ctx->unit_event, &ctx->ev_offsets, &ctx->ev_stats2})
+                      &ctx->unit_event, &ctx->ev_offsets, &ctx->ev_stats2, &ctx->partials})
         b->release();
     for (HostBuf* b : {&ctx->h_hits, &ctx->h_offsets, &ctx->h_evstats, &ctx->h_total, &ctx->h_counters})
         b->release();
@@ -352,6 +352,7 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     CK(ctx->offsets.ensure((units + 1) * 8), "alloc unit offsets");
     CK(ctx->counters.ensure(sizeof(Counters)), "alloc counters");
     CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
+    CK(ctx->partials.ensure(kReducePartials * sizeof(cmpmc_sim_stats)), "alloc partial totals");
     CK(ctx->h_counters.ensure(sizeof(Counters)), "alloc host counters");
     CK(ctx->cstack.ensure(slots * ctx->cstack_cap * sizeof(GCharge)), "alloc charge stacks");
     if (batched) {
@@ -426,11 +427,12 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     if (n > 0 && batched) {
         CK(launch_batched_finish(a, n, a.ph_off, a.injected, ctx->offsets.as<uint64_t>(), ev_offsets,
                                  ctx->hits_out.as<cmpmc_sensor_hit>(), n_hits, ctx->total.as<cmpmc_sim_stats>(),
-                                 d->want_event_stats ? ev_stats : nullptr, s, &launches),
+                                 ctx->partials.as<cmpmc_sim_stats>(), d->want_event_stats ? ev_stats : nullptr, s,
+                                 &launches),
            "merge kernels");
     } else if (n > 0) {
         CK(launch_finish(a, ctx->offsets.as<uint64_t>(), ctx->hits_out.as<cmpmc_sensor_hit>(), n_hits,
-                         ctx->total.as<cmpmc_sim_stats>(), s, &launches),
+                         ctx->total.as<cmpmc_sim_stats>(), ctx->partials.as<cmpmc_sim_stats>(), s, &launches),
            "merge kernels");
     } else {
         CK(cudaMemsetAsync(ev_offsets, 0, 8, s), "memset offsets");

@@ -143,9 +143,11 @@ size_t batched_stack_entry_bytes();
 cudaError_t launch_batched_finish(const RunArgs& a, uint64_t n_events, const uint64_t* ph_off,
                                   const double* injected, uint64_t* unit_offsets, uint64_t* ev_offsets,
                                   cmpmc_sensor_hit* hits_out, uint64_t out_cap, cmpmc_sim_stats* total,
-                                  cmpmc_sim_stats* ev_stats_out, cudaStream_t s, int* launches);
+                                  cmpmc_sim_stats* partials, cmpmc_sim_stats* ev_stats_out, cudaStream_t s,
+                                  int* launches);
 cudaError_t launch_math_check(uint64_t n, const double* x, double* out);
+constexpr int kReducePartials = 592;  // blocks of the first reduction level
 cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
-                          cmpmc_sim_stats* total, cudaStream_t s, int* launches);
+                          cmpmc_sim_stats* total, cmpmc_sim_stats* partials, cudaStream_t s, int* launches);
 
 }  // namespace cmpmc_gpu

@@ -10,6 +10,7 @@ namespace {
 constexpr int kScanThreads = 1024;
 constexpr int kReduceThreads = 128;
 constexpr int kStatsWords = sizeof(cmpmc_sim_stats) / 8;
+constexpr uint64_t kReduceTwoLevel = 65536;  // above this many records, reduce in two levels
 
 // SimStats word kinds: doubles at 16, 17, 23, 24, 25 (engine.hpp:49-50, 60-62)
 __host__ __device__ constexpr bool stats_word_is_double(int i) {
@@ -55,9 +56,15 @@ __global__ void k_scatter(const cmpmc_sensor_hit* __restrict__ stage, const uint
     }
 }
 
-__global__ void __launch_bounds__(kReduceThreads) k_reduce_stats(const cmpmc_sim_stats* __restrict__ ev,
-                                                                 uint64_t n, cmpmc_sim_stats* total) {
+// Block b reduces records [b n / B, (b + 1) n / B) into total[b] in a fixed order (each
+// thread a contiguous slice, then a tree over the threads).
+__global__ void __launch_bounds__(kReduceThreads) k_reduce_stats(const cmpmc_sim_stats* __restrict__ ev_all,
+                                                                 uint64_t n_all, cmpmc_sim_stats* total_all) {
     __shared__ uint64_t acc[kReduceThreads][kStatsWords];
+    const uint64_t b0 = n_all * blockIdx.x / gridDim.x, b1 = n_all * (blockIdx.x + 1) / gridDim.x;
+    const cmpmc_sim_stats* ev = ev_all + b0;
+    const uint64_t n = b1 - b0;
+    cmpmc_sim_stats* total = total_all + blockIdx.x;
     const int t = threadIdx.x;
     const uint64_t chunk = (n + kReduceThreads - 1) / kReduceThreads;
     const uint64_t lo = min(n, t * chunk), hi = min(n, lo + chunk);
@@ -154,8 +161,9 @@ __global__ void __launch_bounds__(kReduceThreads) k_sum_injected(const double* _
 cudaError_t launch_batched_finish(const RunArgs& a, uint64_t n_events, const uint64_t* ph_off,
                                   const double* injected, uint64_t* unit_offsets, uint64_t* ev_offsets,
                                   cmpmc_sensor_hit* hits_out, uint64_t out_cap, cmpmc_sim_stats* total,
-                                  cmpmc_sim_stats* ev_stats_out, cudaStream_t s, int* launches) {
-    cudaError_t e = launch_finish(a, unit_offsets, hits_out, out_cap, total, s, launches);
+                                  cmpmc_sim_stats* partials, cmpmc_sim_stats* ev_stats_out, cudaStream_t s,
+                                  int* launches) {
+    cudaError_t e = launch_finish(a, unit_offsets, hits_out, out_cap, total, partials, s, launches);
     if (e != cudaSuccess) return e;
     k_event_offsets<<<148, 256, 0, s>>>(unit_offsets, ph_off, n_events, ev_offsets);
     k_sum_injected<<<1, kReduceThreads, 0, s>>>(injected, n_events, total);
@@ -168,7 +176,7 @@ cudaError_t launch_batched_finish(const RunArgs& a, uint64_t n_events, const uin
 }
 
 cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
-                          cmpmc_sim_stats* total, cudaStream_t s, int* launches) {
+                          cmpmc_sim_stats* total, cmpmc_sim_stats* partials, cudaStream_t s, int* launches) {
     k_scan<<<1, kScanThreads, 0, s>>>(a.ev_nhits, a.n_events, offsets);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -180,8 +188,14 @@ cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit*
         if (e != cudaSuccess) return e;
         *launches += 1;
     }
-    k_reduce_stats<<<1, kReduceThreads, 0, s>>>(a.ev_stats, a.n_events, total);
-    *launches += 1;
+    if (a.n_events > kReduceTwoLevel && partials) {
+        k_reduce_stats<<<kReducePartials, kReduceThreads, 0, s>>>(a.ev_stats, a.n_events, partials);
+        k_reduce_stats<<<1, kReduceThreads, 0, s>>>(partials, kReducePartials, total);
+        *launches += 2;
+    } else {
+        k_reduce_stats<<<1, kReduceThreads, 0, s>>>(a.ev_stats, a.n_events, total);
+        *launches += 1;
+    }
     return cudaGetLastError();
 }
 

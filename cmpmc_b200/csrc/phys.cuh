@@ -423,7 +423,8 @@ struct KBuf {
 
 // KaplanFilm (superconductor/kaplan_film.hpp:39-323)
 CMPMC_HD bool film_is_subgap(const Film& f, double e) { return e < 2.0 * f.gap_energy; }
-CMPMC_HD bool film_is_thermalized(const Film& f, double e, Rng& rng) {
+template <class G>
+CMPMC_HD bool film_is_thermalized(const Film& f, double e, G& rng) {
     if (f.temperature <= 0.0) return false;
     const double kT = kBoltzmann * f.temperature;
     return e < kT * (-m_log(rng.uniform()));
@@ -461,11 +462,13 @@ CMPMC_HD double film_loss_probability(const Film& f, double e, double thickness_
     }
     return film_escape_probability(f, e, thickness_frac);
 }
-CMPMC_HD bool film_direct_absorption(const Film& f, double e, Rng& rng) {
+template <class G>
+CMPMC_HD bool film_direct_absorption(const Film& f, double e, G& rng) {
     if (e < 2.0 * f.absorber_gap) return false;
     return rng.uniform() < f.subgap_absorption;
 }
-CMPMC_HD double film_calc_direct_absorption(const Film& f, double e, KBuf& keep, Rng& rng) {
+template <class G>
+CMPMC_HD double film_calc_direct_absorption(const Film& f, double e, KBuf& keep, G& rng) {
     if (film_direct_absorption(f, e, rng)) return e;
     keep.push(e);
     return 0.0;
@@ -474,7 +477,8 @@ CMPMC_HD double film_qp_efficiency(const Film& f, double qpE) {
     const double eff = (f.gap_energy > 0.0) ? (f.absorber_eff + f.absorber_eff_slope * (qpE / f.gap_energy)) : 1.0;
     return dclamp(eff, 0.0, 1.0);
 }
-CMPMC_HD double film_calc_qp_absorption(const Film& f, double qpE, KBuf& phon, KBuf& qp, Rng& rng) {
+template <class G>
+CMPMC_HD double film_calc_qp_absorption(const Film& f, double qpE, KBuf& phon, KBuf& qp, G& rng) {
     if (rng.uniform() > film_qp_efficiency(f, qpE)) return 0.0;
     if (qpE >= f.low_qp_limit * f.gap_energy) {
         qp.push(qpE);
@@ -489,7 +493,8 @@ CMPMC_HD double qp_weight(double E, double d, double x) {
     return (x * (E - x) + d * d) / sqrt((x + d) * (E - x + d));
 }
 // kaplan_film.hpp:209-227
-CMPMC_HD double film_sample_qp_energy(const Film& f, double E, Rng& rng) {
+template <class G>
+CMPMC_HD double film_sample_qp_energy(const Film& f, double E, G& rng) {
     const double d = f.gap_energy;
     const double span = E - 2.0 * d;
     if (span <= 1e-16) return 0.5 * E;
@@ -506,7 +511,8 @@ CMPMC_HD double ph_weight(double E, double d, double d2E, double x) {
     return (diff * diff) * (x - d2E) / sqrt(x + d);
 }
 // kaplan_film.hpp:269-289
-CMPMC_HD double film_sample_phonon_energy(const Film& f, double E, Rng& rng) {
+template <class G>
+CMPMC_HD double film_sample_phonon_energy(const Film& f, double E, G& rng) {
     const double d = f.gap_energy;
     const double span = E - d;
     if (span <= 1e-16) return 0.0;
@@ -524,7 +530,8 @@ CMPMC_HD double film_sample_phonon_energy(const Film& f, double E, Rng& rng) {
 // generation buffers of the reference are value-copied at the end of each stage; here
 // the same buffers are swapped, which leaves identical contents. `work` must hold
 // 4 * kKaplanCap doubles; `refl` receives the re-emitted phonon energies.
-CMPMC_HD double film_absorb_phonon(const Film& f, double energy, KBuf& refl, double* work, Rng& rng) {
+template <class G>
+CMPMC_HD double film_absorb_phonon(const Film& f, double energy, KBuf& refl, double* work, G& rng) {
     refl.clear();
     if (film_direct_absorption(f, energy, rng)) return energy;
     if (film_is_subgap(f, energy) || rng.uniform() <= film_loss_probability(f, energy, 4.0)) {

@@ -1,19 +1,24 @@
 // transport_batched.cu -- the batched FP32 form: one device thread per primary track.
 //
 // The plain form keeps each event's single random stream, so an event's tracks run one
-// after another on one thread. Here every primary phonon owns its own xoshiro256**
-// substream, Rng::for_stream(seed, (event << 20) | index within the event), so all
+// after another on one thread. Here every primary phonon owns its own random substream
+// (xoshiro128**, seeded from (run seed, event << 20 | index within the event)), so all
 // primaries of a batch run concurrently and the result does not depend on how the device
-// schedules them. A thread transports its primary and every daughter of it (decay,
-// film re-emission, surface down-conversion) from a per-thread LIFO in global memory.
+// schedules them. A thread transports its primary and every daughter of it (decay, film
+// re-emission, surface down-conversion) from a per-thread LIFO in global memory.
+//
+// The physics follows SimulationEngine::transport (transport/engine.hpp:403-582); the draw
+// order differs (each substream is private, so any order of independent draws samples
+// the same distributions). The step is arranged so the lanes of a warp stay converged:
+// bulk scatter (isotropic) and diffuse reflection (Lambertian about the inward normal)
+// share one direction-sampling and table-lookup path; decays, film entries, specular and
+// down-converting reflections are the rare branches, and the Kaplan cascade is an
+// out-of-line call so the step loop keeps few registers.
 //
 // Precision: position, directions, group velocity, the octahedral table blend, rates and
-// sampling are FP32 (fast CUDA intrinsics); the phonon energy, time of flight, weight and
-// the energy ledger are FP64, as is the Kaplan film cascade (so the ledger closes to
-// rounding). The physics and its random-draw structure follow SimulationEngine::transport
-// (transport/engine.hpp:403-582); only the stream assignment and the precision differ.
-// A reflected track is moved 10 nm inward (the reference moves it 1e-11 m, below FP32
-// resolution at the cylinder wall).
+// sampling are FP32; the phonon energy, time of flight and the energy ledger are FP64, as
+// is the Kaplan film cascade (so the ledger closes to rounding). A reflected track is
+// moved 10 nm inward (the reference moves it 1e-11 m, below FP32 resolution at the wall).
 #define CMPMC_DEVICE_FAST_MATH 1
 #include "device.cuh"
 
@@ -22,6 +27,7 @@ namespace cmpmc_gpu {
 namespace {
 
 constexpr float kNudge = 1e-8f;  // inward displacement after a boundary event (m)
+constexpr float kTwoPiF = 6.28318530717958648f;
 
 struct F3 {
     float x, y, z;
@@ -47,29 +53,36 @@ __device__ __forceinline__ F3 forth(F3 v) {
     return funit(fcross(v, a));
 }
 
-// per-primary stream: xoshiro256** with a 24-bit FP32 uniform in (0, 1)
-struct FRng {
-    Rng r;
+// xoshiro128** (Blackman and Vigna) per substream; FP32 uniforms in (0, 1) with 24 bits and
+// FP64 uniforms with 53 bits for the Kaplan cascade
+struct R128 {
+    uint32_t s0, s1, s2, s3;
+    __device__ __forceinline__ void seed(uint64_t key) {
+        uint64_t z = key;
+        const uint64_t a = splitmix_step(z += 0x9e3779b97f4a7c15ULL);
+        const uint64_t b = splitmix_step(z += 0x9e3779b97f4a7c15ULL);
+        s0 = static_cast<uint32_t>(a);
+        s1 = static_cast<uint32_t>(a >> 32);
+        s2 = static_cast<uint32_t>(b);
+        s3 = static_cast<uint32_t>(b >> 32) | 1u;  // never all zero
+    }
+    __device__ __forceinline__ uint32_t next() {
+        const uint32_t r = __funnelshift_l(s1 * 5u, s1 * 5u, 7) * 9u;
+        const uint32_t t = s1 << 9;
+        s2 ^= s0;
+        s3 ^= s1;
+        s1 ^= s2;
+        s0 ^= s3;
+        s2 ^= t;
+        s3 = __funnelshift_l(s3, s3, 11);
+        return r;
+    }
     __device__ __forceinline__ float u() {
-        const uint32_t m = static_cast<uint32_t>(r.next_u64() >> 41);  // 23 bits
-        return __uint2float_rn(2u * m + 1u) * 5.9604644775390625e-8f;  // (2m+1) / 2^24
+        return __uint2float_rn(((next() >> 9) << 1) | 1u) * 5.9604644775390625e-8f;  // (2m+1) / 2^24
     }
-    __device__ __forceinline__ F3 iso() {
-        const float ct = 2.0f * u() - 1.0f;
-        const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
-        float s, c;
-        __sincosf(6.28318530717958648f * u(), &s, &c);
-        return f3(st * c, st * s, ct);
-    }
-    __device__ __forceinline__ F3 lambert(F3 n) {
-        const float phi = 6.28318530717958648f * u();
-        const float st = sqrtf(u());
-        const float ct = sqrtf(fmaxf(0.0f, 1.0f - st * st));
-        const F3 a = forth(n);
-        const F3 b = fcross(n, a);
-        float s, c;
-        __sincosf(phi, &s, &c);
-        return funit(a * (st * c) + b * (st * s) + n * ct);
+    __device__ __forceinline__ double uniform() {  // 53-bit, for the FP64 cascade
+        const uint64_t x = (static_cast<uint64_t>(next()) << 21) ^ (next() >> 11);
+        return static_cast<double>(x | 1ULL) * (1.0 / 9007199254740992.0);
     }
 };
 
@@ -84,6 +97,9 @@ struct FLat {
     float poly_inv;   // 1 / polycrystal mfp (0 disables)
     float fL, fLST, p_st_trans, fTT;
     float m_ratio;    // v_L / v_T
+    // per surface: constant reflection split (1 when the polynomials do not depend on energy)
+    int split_const[3];
+    float p_anh[3], p_anh_spec[3];
 };
 
 struct FKin {
@@ -124,12 +140,9 @@ __device__ __forceinline__ FKin fmap(const FLat& L, int mode, F3 k) {
     return r;
 }
 
-__device__ __forceinline__ int fdos(const FLat& L, FRng& g) {
-    const float u = g.u();
-    return (u < L.fL) ? 0 : ((u < L.fLST) ? 2 : 1);
-}
-__device__ __forceinline__ int ftrans(const FLat& L, FRng& g) { return (g.u() < L.p_st_trans) ? 2 : 1; }
-__device__ __forceinline__ float fcdf(const float* cdf, FRng& g) {
+__device__ __forceinline__ int fdos(const FLat& L, float u) { return (u < L.fL) ? 0 : ((u < L.fLST) ? 2 : 1); }
+__device__ __forceinline__ int ftrans(const FLat& L, R128& g) { return (g.u() < L.p_st_trans) ? 2 : 1; }
+__device__ __forceinline__ float fcdf(const float* cdf, R128& g) {
     const float u = g.u() * (kNCdf - 1);
     const int i = min(static_cast<int>(u), kNCdf - 2);
     const float f = u - i;
@@ -140,22 +153,29 @@ __device__ __forceinline__ float facos_clamped(float c) { return acosf(fminf(fma
 struct FTrack {
     F3 pos, k, vg;
     float vmag;
-    double E, t, w;
+    double E, t;
+    float w;
     uint32_t bounces;
     int mode;
 };
 
 struct alignas(16) GFTrack {
-    float px, py, pz, kx, ky, kz, vx, vy, vz, vmag;
-    uint32_t bounces;
-    int mode;
-    double E, t, w;
+    float px, py, pz, kx, ky, kz, vx, vy, vz, vmag, w;
+    uint32_t bounces_mode;  // bounces << 2 | mode
+    double E, t;
 };
 
 // inward Lambertian wavevector whose group velocity points inward (engine.hpp:927-936)
-__device__ __forceinline__ F3 finward(const FLat& L, int mode, F3 n, FRng& g, FKin& kin) {
+__device__ __forceinline__ F3 finward(const FLat& L, int mode, F3 n, R128& g, FKin& kin) {
+    const F3 a = forth(n);
+    const F3 b = fcross(n, a);
     for (int trial = 0; trial < 16; ++trial) {
-        const F3 kd = g.lambert(n);
+        const float phi = kTwoPiF * g.u();
+        const float st = sqrtf(g.u());
+        const float ct = sqrtf(fmaxf(0.0f, 1.0f - st * st));
+        float s, c;
+        __sincosf(phi, &s, &c);
+        const F3 kd = funit(a * (st * c) + b * (st * s) + n * ct);
         kin = fmap(L, mode, kd);
         if (fdot(kin.dir, n) > 1e-6f) return kd;
     }
@@ -200,50 +220,103 @@ __device__ __forceinline__ FBHit fexit(float R, float H, F3 p, F3 v) {
     return h;
 }
 
-struct BatchCtx {
-    GFTrack* stk;
-    uint32_t n_stk, cap;
-    unsigned err;
-    __device__ __forceinline__ void push(const FTrack& t) {
-        if (n_stk >= cap) {
-            err |= kErrPhononStack;
-            return;
-        }
-        GFTrack g;
-        g.px = t.pos.x; g.py = t.pos.y; g.pz = t.pos.z;
-        g.kx = t.k.x; g.ky = t.k.y; g.kz = t.k.z;
-        g.vx = t.vg.x; g.vy = t.vg.y; g.vz = t.vg.z;
-        g.vmag = t.vmag;
-        g.bounces = t.bounces;
-        g.mode = t.mode;
-        g.E = t.E; g.t = t.t; g.w = t.w;
-        stk[n_stk++] = g;
+__device__ __forceinline__ void push_track(GFTrack* stk, uint32_t& n, uint32_t cap, unsigned& err, const FTrack& t) {
+    if (n >= cap) {
+        err |= kErrPhononStack;
+        return;
     }
-    __device__ __forceinline__ void pop(FTrack& t) {
-        const GFTrack g = stk[--n_stk];
-        t.pos = f3(g.px, g.py, g.pz);
-        t.k = f3(g.kx, g.ky, g.kz);
-        t.vg = f3(g.vx, g.vy, g.vz);
-        t.vmag = g.vmag;
-        t.bounces = g.bounces;
-        t.mode = g.mode;
-        t.E = g.E; t.t = g.t; t.w = g.w;
-    }
+    GFTrack g;
+    g.px = t.pos.x; g.py = t.pos.y; g.pz = t.pos.z;
+    g.kx = t.k.x; g.ky = t.k.y; g.kz = t.k.z;
+    g.vx = t.vg.x; g.vy = t.vg.y; g.vz = t.vg.z;
+    g.vmag = t.vmag;
+    g.w = t.w;
+    g.bounces_mode = (t.bounces << 2) | static_cast<uint32_t>(t.mode);
+    g.E = t.E;
+    g.t = t.t;
+    stk[n++] = g;
+}
+__device__ __forceinline__ void pop_track(const GFTrack* stk, uint32_t& n, FTrack& t) {
+    const GFTrack g = stk[--n];
+    t.pos = f3(g.px, g.py, g.pz);
+    t.k = f3(g.kx, g.ky, g.kz);
+    t.vg = f3(g.vx, g.vy, g.vz);
+    t.vmag = g.vmag;
+    t.w = g.w;
+    t.bounces = g.bounces_mode >> 2;
+    t.mode = static_cast<int>(g.bounces_mode & 3u);
+    t.E = g.E;
+    t.t = g.t;
+}
+
+// compact per-primary counters (a primary's lineage stays far below 2^32 steps)
+struct UStats {
+    uint32_t steps, iso, poly, tt, lt, refl, down, hits, killed;
+    double dep, esc;
 };
 
-__device__ __forceinline__ FTrack fmake(const FLat& L, F3 pos, F3 k, int mode, double E, double t, double w) {
-    FTrack r;
-    r.pos = pos;
-    r.k = funit(k);
-    const FKin kin = fmap(L, mode, r.k);
-    r.vg = kin.dir;
-    r.vmag = kin.mag;
-    r.E = E;
-    r.t = t;
-    r.w = w;
-    r.bounces = 0;
-    r.mode = mode;
-    return r;
+// Kaplan cascade out of line: its FP64 registers stay out of the step loop
+__device__ __noinline__ double kaplan_call(const Film* f, double E, double* refl, int* n_refl, double* work,
+                                           R128* g) {
+    KBuf r{refl, 0};
+    const double edep = film_absorb_phonon(*f, E, r, work, *g);
+    *n_refl = r.n;
+    return edep;
+}
+
+// anharmonic decay of an L phonon (engine.hpp:938-988), FP32 angles
+__device__ __noinline__ void decay_call(const FLat* Lp, FTrack* tp, GFTrack* stk, uint32_t* n_stk, uint32_t cap,
+                                        unsigned* err, UStats* st, R128* gp) {
+    const FLat& L = *Lp;
+    FTrack& trk = *tp;
+    R128& g = *gp;
+    const F3 d1 = trk.k;
+    const F3 perp = forth(d1);
+    float sp, cp;
+    __sincosf(kTwoPiF * g.u(), &sp, &cp);
+    float x, th1, th2;
+    int m1, m2;
+    const float m = L.m_ratio, mm = m * m;
+    if (g.u() < L.fTT) {
+        st->tt++;
+        x = fcdf(L.cdf_tt, g);
+        const float y = 1.0f - x;
+        th1 = facos_clamped((1.0f - mm * y * y + mm * x * x) / (2.0f * m * x));
+        th2 = facos_clamped((1.0f - mm * x * x + mm * y * y) / (2.0f * m * y));
+        m1 = ftrans(L, g);
+        m2 = ftrans(L, g);
+    } else {
+        st->lt++;
+        x = fcdf(L.cdf_lt, g);
+        th1 = facos_clamped((1.0f + x * x * (1.0f - mm) + 2.0f * x * mm - mm) / (2.0f * x));
+        th2 = facos_clamped((1.0f - x * x + mm * (1.0f - x) * (1.0f - x)) / (2.0f * m * (1.0f - x)));
+        m1 = 0;
+        m2 = ftrans(L, g);
+    }
+    float s1, c1, s2, c2;
+    __sincosf(th1, &s1, &c1);
+    __sincosf(-th2, &s2, &c2);
+    const F3 k1 = funit(frotate(frotate(d1, perp, c1, s1), d1, cp, sp));
+    const F3 k2 = funit(frotate(frotate(d1, perp, c2, s2), d1, cp, sp));
+    const double xd = static_cast<double>(x);
+    FTrack d;
+    d.pos = trk.pos;
+    d.k = k2;
+    const FKin kin2 = fmap(L, m2, k2);
+    d.vg = kin2.dir;
+    d.vmag = kin2.mag;
+    d.E = (1.0 - xd) * trk.E;
+    d.t = trk.t;
+    d.w = trk.w;
+    d.bounces = 0;
+    d.mode = m2;
+    push_track(stk, *n_stk, cap, *err, d);
+    trk.E = xd * trk.E;
+    trk.mode = m1;
+    trk.k = k1;
+    const FKin kin = fmap(L, m1, k1);
+    trk.vg = kin.dir;
+    trk.vmag = kin.mag;
 }
 
 __global__ void __launch_bounds__(128) k_unit_event(const uint64_t* __restrict__ ph_off, uint64_t n_events,
@@ -253,200 +326,214 @@ __global__ void __launch_bounds__(128) k_unit_event(const uint64_t* __restrict__
         for (uint64_t j = ph_off[ev]; j < ph_off[ev + 1]; ++j) unit_event[j] = static_cast<uint32_t>(ev);
 }
 
-__global__ void __launch_bounds__(128) k_batched_fp32(const FLat L, const Detector D, const RunArgs a,
-                                                      const uint32_t* __restrict__ unit_event) {
+__device__ __forceinline__ void write_unit(const RunArgs& a, uint64_t unit, const UStats& st, uint32_t n_hits) {
+    cmpmc_sim_stats& o = a.ev_stats[unit];
+    o.total_steps = st.steps;
+    o.isotope_scatters = st.iso;
+    o.polycrystal_scatters = st.poly;
+    o.decays_L_to_TT = st.tt;
+    o.decays_L_to_LT = st.lt;
+    o.surface_refls = st.refl;
+    o.surface_downconversions = st.down;
+    o.sensor_hits = st.hits;
+    o.killed_tracks = st.killed;
+    o.charge_steps = 0; o.luke_phonons_emitted = 0; o.intervalley_scatters = 0; o.charges_trapped = 0;
+    o.trap_ionizations = 0; o.charge_surface_refls = 0; o.charges_collected = 0;
+    o.total_luke_phonon_eV = 0.0; o.charge_recomb_edep_eV = 0.0;
+    o.sc_pair_breakings = 0; o.qp_diffusion_steps = 0; o.qp_phonons_radiated = 0; o.qp_recombinations = 0;
+    o.qp_local_traps = 0;
+    o.total_injected_eV = 0.0;
+    o.total_deposited_eV = st.dep;
+    o.escaped_or_killed_eV = st.esc;
+    a.ev_nhits[unit] = a.keep_hits ? n_hits : 0;
+}
+
+__global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__ FLat L,
+                                                         const __grid_constant__ Detector D,
+                                                         const __grid_constant__ RunArgs a,
+                                                         const uint32_t* __restrict__ unit_event) {
     const uint64_t slot = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     double refl_buf[kKaplanCap];
     double kwork[4 * kKaplanCap];
-    KBuf refl{refl_buf, 0};
-    BatchCtx ctx;
-    ctx.stk = reinterpret_cast<GFTrack*>(a.stack) + slot * a.stack_cap;
-    ctx.cap = a.stack_cap;
-    ctx.err = 0;
+    GFTrack* stk = reinterpret_cast<GFTrack*>(a.stack) + slot * a.stack_cap;
+    uint32_t n_stk = 0;
+    unsigned err = 0;
     const float R = static_cast<float>(D.radius), H = static_cast<float>(D.half_z);
+    const double min_E = D.min_phonon_eV;
+    const uint64_t seed_key = mix64(a.seed ^ 0x5851f42d4c957f2dULL);
+
+    FTrack trk;
+    R128 g;
+    UStats st;
+    uint32_t n_hits = 0;
+    uint64_t unit = ~0ull;
+    bool live = false;  // trk holds a track in flight
     for (;;) {
-        const unsigned long long unit = atomicAdd(a.next_work, 1ull);
-        if (unit >= a.n_events) break;
-        const uint32_t ev = unit_event[unit];
-        const uint64_t j = unit - a.ph_off[ev];
-        FRng g;
-        g.r = Rng::for_stream(a.seed, ((a.first_event + ev) << 20) | j);
-        const cmpmc_phonon_track& in = a.ph[unit];
-        FTrack trk;
-        trk.pos = f3(static_cast<float>(in.pos[0]), static_cast<float>(in.pos[1]), static_cast<float>(in.pos[2]));
-        trk.k = f3(static_cast<float>(in.k_dir[0]), static_cast<float>(in.k_dir[1]), static_cast<float>(in.k_dir[2]));
-        trk.vg = f3(static_cast<float>(in.vg_dir[0]), static_cast<float>(in.vg_dir[1]),
-                    static_cast<float>(in.vg_dir[2]));
-        trk.vmag = static_cast<float>(in.vg_mag);
-        trk.E = in.energy;
-        trk.t = in.time;
-        trk.w = in.weight;
-        trk.bounces = in.bounces;
-        trk.mode = in.mode;
-        ctx.n_stk = 0;
-        EvStats st;
-        memset(&st, 0, sizeof(st));
-        uint32_t n_hits = 0;
-        for (bool have = true; have; have = (ctx.n_stk > 0) ? (ctx.pop(trk), true) : false) {
-            for (;;) {
-                if (trk.E < D.min_phonon_eV || trk.bounces >= D.max_bounces) {
-                    st.killed_tracks++;
-                    st.escaped_eV += trk.E * trk.w;
-                    break;
-                }
-                if (D.rr_bounces != 0 && trk.bounces > D.rr_bounces && (trk.bounces - D.rr_bounces) % 32 == 0) {
-                    if (g.u() < static_cast<float>(D.rr_survival)) {
-                        trk.w /= D.rr_survival;
-                    } else {
-                        st.killed_tracks++;
-                        break;
-                    }
-                }
-                st.total_steps++;
-                const float nu = static_cast<float>(trk.E) * L.inv_h_thz;
-                const float nu2 = nu * nu;
-                const float r_iso = L.b4 * (nu2 * nu2);
-                const float r_poly = trk.vmag * L.poly_inv;
-                const float r_down = (trk.mode == 0) ? L.a5 * (nu2 * nu2 * nu) : 0.0f;
-                const float r_tot = r_iso + r_poly + r_down;
-                const float d_phys = (r_tot > 1e-12f) ? (-__logf(g.u()) * trk.vmag / r_tot)
-                                                      : __int_as_float(0x7f800000);
-                const FBHit bh = fexit(R, H, trk.pos, trk.vg);
-                if (d_phys < bh.d) {
-                    trk.pos = trk.pos + trk.vg * d_phys;
-                    trk.t += static_cast<double>(d_phys / trk.vmag);
-                    const float u_proc = g.u() * r_tot;
-                    if (r_down > 0.0f && u_proc < r_down) {
-                        // anharmonic decay (engine.hpp:938-988)
-                        const F3 d1 = trk.k;
-                        const F3 perp = forth(d1);
-                        float sp, cp;
-                        __sincosf(6.28318530717958648f * g.u(), &sp, &cp);
-                        float x, th1, th2;
-                        int m1, m2;
-                        const float m = L.m_ratio, mm = m * m;
-                        if (g.u() < L.fTT) {
-                            st.decays_TT++;
-                            x = fcdf(L.cdf_tt, g);
-                            const float y = 1.0f - x;
-                            th1 = facos_clamped((1.0f - mm * y * y + mm * x * x) / (2.0f * m * x));
-                            th2 = facos_clamped((1.0f - mm * x * x + mm * y * y) / (2.0f * m * y));
-                            m1 = ftrans(L, g);
-                            m2 = ftrans(L, g);
-                        } else {
-                            st.decays_LT++;
-                            x = fcdf(L.cdf_lt, g);
-                            th1 = facos_clamped((1.0f + x * x * (1.0f - mm) + 2.0f * x * mm - mm) / (2.0f * x));
-                            th2 = facos_clamped((1.0f - x * x + mm * (1.0f - x) * (1.0f - x)) / (2.0f * m * (1.0f - x)));
-                            m1 = 0;
-                            m2 = ftrans(L, g);
+        if (!live) {
+            if (n_stk > 0) {
+                pop_track(stk, n_stk, trk);
+                live = true;
+            } else {
+                if (unit != ~0ull) write_unit(a, unit, st, n_hits);
+                unit = atomicAdd(a.next_work, 1ull);
+                if (unit >= a.n_events) break;
+                const uint32_t ev = unit_event[unit];
+                const uint64_t j = unit - a.ph_off[ev];
+                g.seed(seed_key ^ mix64(((a.first_event + ev) << 20) | j));
+                const cmpmc_phonon_track& in = a.ph[unit];
+                trk.pos = f3(static_cast<float>(in.pos[0]), static_cast<float>(in.pos[1]),
+                             static_cast<float>(in.pos[2]));
+                trk.k = f3(static_cast<float>(in.k_dir[0]), static_cast<float>(in.k_dir[1]),
+                           static_cast<float>(in.k_dir[2]));
+                trk.vg = f3(static_cast<float>(in.vg_dir[0]), static_cast<float>(in.vg_dir[1]),
+                            static_cast<float>(in.vg_dir[2]));
+                trk.vmag = static_cast<float>(in.vg_mag);
+                trk.E = in.energy;
+                trk.t = in.time;
+                trk.w = static_cast<float>(in.weight);
+                trk.bounces = in.bounces;
+                trk.mode = in.mode;
+                st = UStats{0, 0, 0, 0, 0, 0, 0, 0, 0, 0.0, 0.0};
+                n_hits = 0;
+                live = true;
+            }
+        }
+        if (trk.E < min_E || trk.bounces >= D.max_bounces) {
+            st.killed++;
+            st.esc += trk.E * trk.w;
+            live = false;
+            continue;
+        }
+        if (D.rr_bounces != 0 && trk.bounces > D.rr_bounces && (trk.bounces - D.rr_bounces) % 32 == 0) {
+            if (g.u() < static_cast<float>(D.rr_survival)) {
+                trk.w /= static_cast<float>(D.rr_survival);
+            } else {
+                st.killed++;
+                live = false;
+                continue;
+            }
+        }
+        st.steps++;
+        const float nu = static_cast<float>(trk.E) * L.inv_h_thz;
+        const float nu2 = nu * nu;
+        const float r_iso = L.b4 * (nu2 * nu2);
+        const float r_poly = trk.vmag * L.poly_inv;
+        const float r_down = (trk.mode == 0) ? L.a5 * (nu2 * nu2 * nu) : 0.0f;
+        const float r_tot = r_iso + r_poly + r_down;
+        const float d_phys = (r_tot > 1e-12f) ? (-logf(g.u()) * trk.vmag / r_tot) : __int_as_float(0x7f800000);
+        const FBHit bh = fexit(R, H, trk.pos, trk.vg);
+        const bool bulk = d_phys < bh.d;
+        const float d = bulk ? d_phys : bh.d;
+        trk.pos = trk.pos + trk.vg * d;
+        trk.t += static_cast<double>(d / trk.vmag);
+        // 0: new isotropic direction (bulk scatter), 1: Lambertian about bh.n, 2: nothing more
+        int sample = 2;
+        if (bulk) {
+            const float u_proc = g.u() * r_tot;
+            if (r_down > 0.0f && u_proc < r_down) {
+                decay_call(&L, &trk, stk, &n_stk, a.stack_cap, &err, &st, &g);
+            } else {
+                if (u_proc < r_down + r_iso) st.iso++;
+                else st.poly++;
+                trk.mode = fdos(L, g.u());
+                sample = 0;
+            }
+        } else {
+            trk.bounces++;
+            const Surface& s = D.surf[bh.surf];
+            if (s.has_film && g.u() < static_cast<float>(s.prob_abs) &&
+                g.u() < static_cast<float>(s.film.film_absorption)) {
+                int n_refl = 0;
+                const double edep = kaplan_call(&s.film, trk.E, refl_buf, &n_refl, kwork, &g);
+                if (edep > 0.0) {
+                    const double wedep = edep * trk.w;
+                    st.hits++;
+                    st.dep += wedep;
+                    const uint32_t local = n_hits++;
+                    if (a.keep_hits) {
+                        const unsigned long long idx = atomicAdd(a.hit_count, 1ull);
+                        if (idx < a.hit_cap) {
+                            cmpmc_sensor_hit r;
+                            r.pos[0] = trk.pos.x; r.pos[1] = trk.pos.y; r.pos[2] = trk.pos.z;
+                            r.time = trk.t;
+                            r.edep = wedep;
+                            r.incident_energy = trk.E;
+                            r.surface_id = static_cast<uint8_t>(bh.surf);
+                            r.excitation = 0;
+                            r.mode = static_cast<uint8_t>(trk.mode);
+                            r._pad = 0;
+                            r.channel_id = -1;
+                            a.hit_stage[idx] = r;
+                            a.hit_key[idx] = (unit << 32) | local;
                         }
-                        float s1, c1, s2, c2;
-                        __sincosf(th1, &s1, &c1);
-                        __sincosf(-th2, &s2, &c2);
-                        const F3 k1 = funit(frotate(frotate(d1, perp, c1, s1), d1, cp, sp));
-                        const F3 k2 = funit(frotate(frotate(d1, perp, c2, s2), d1, cp, sp));
-                        const double xd = static_cast<double>(x);
-                        ctx.push(fmake(L, trk.pos, k2, m2, (1.0 - xd) * trk.E, trk.t, trk.w));
-                        trk.E = xd * trk.E;
-                        trk.mode = m1;
-                        trk.k = k1;
-                        const FKin kin = fmap(L, m1, k1);
-                        trk.vg = kin.dir;
-                        trk.vmag = kin.mag;
-                    } else {
-                        if (u_proc < r_down + r_iso) st.isotope_scatters++;
-                        else st.polycrystal_scatters++;
-                        trk.mode = fdos(L, g);
-                        trk.k = g.iso();
-                        const FKin kin = fmap(L, trk.mode, trk.k);
-                        trk.vg = kin.dir;
-                        trk.vmag = kin.mag;
                     }
+                }
+                double sum_refl = 0.0;
+                for (int i = 0; i < n_refl; ++i) sum_refl += refl_buf[i];
+                st.esc += dmax(0.0, trk.E - edep - sum_refl) * trk.w;
+                if (n_refl == 0) {
+                    live = false;
                     continue;
                 }
-                trk.pos = trk.pos + trk.vg * bh.d;
-                trk.t += static_cast<double>(bh.d / trk.vmag);
-                trk.bounces++;
-                const Surface& s = D.surf[bh.surf];
-                if (s.has_film && g.u() < static_cast<float>(s.prob_abs) &&
-                    g.u() < static_cast<float>(s.film.film_absorption)) {
-                    // Kaplan cascade in FP64 (CUDA libm); a substream-local Rng drives it
-                    const double edep = film_absorb_phonon(s.film, trk.E, refl, kwork, g.r);
-                    if (edep > 0.0) {
-                        const double wedep = edep * trk.w;
-                        st.sensor_hits++;
-                        st.deposited_eV += wedep;
-                        const uint32_t local = n_hits++;
-                        if (a.keep_hits) {
-                            const unsigned long long idx = atomicAdd(a.hit_count, 1ull);
-                            if (idx < a.hit_cap) {
-                                cmpmc_sensor_hit r;
-                                r.pos[0] = trk.pos.x; r.pos[1] = trk.pos.y; r.pos[2] = trk.pos.z;
-                                r.time = trk.t;
-                                r.edep = wedep;
-                                r.incident_energy = trk.E;
-                                r.surface_id = static_cast<uint8_t>(bh.surf);
-                                r.excitation = 0;
-                                r.mode = static_cast<uint8_t>(trk.mode);
-                                r._pad = 0;
-                                r.channel_id = -1;
-                                a.hit_stage[idx] = r;
-                                a.hit_key[idx] = (static_cast<uint64_t>(unit) << 32) | local;
-                            }
-                        }
-                    }
-                    double sum_refl = 0.0;
-                    for (int i = 0; i < refl.n; ++i) sum_refl += refl.d[i];
-                    st.escaped_eV += dmax(0.0, trk.E - edep - sum_refl) * trk.w;
-                    if (refl.n == 0) break;
-                    const F3 re = trk.pos + bh.n * kNudge;
-                    for (int i = 1; i < refl.n; ++i) {
-                        const int m = fdos(L, g);
-                        FKin kin;
-                        const F3 kd = finward(L, m, bh.n, g, kin);
-                        FTrack d;
-                        d.pos = re; d.k = kd; d.vg = kin.dir; d.vmag = kin.mag;
-                        d.E = refl.d[i]; d.t = trk.t; d.w = trk.w; d.bounces = 0; d.mode = m;
-                        ctx.push(d);
-                    }
-                    trk.pos = re;
-                    trk.E = refl.d[0];
-                    trk.mode = fdos(L, g);
+                const F3 re = trk.pos + bh.n * kNudge;
+                for (int i = 1; i < n_refl; ++i) {
+                    FTrack dtr;
+                    dtr.mode = fdos(L, g.u());
                     FKin kin;
-                    trk.k = finward(L, trk.mode, bh.n, g, kin);
-                    trk.vg = kin.dir;
-                    trk.vmag = kin.mag;
-                    continue;
+                    dtr.k = finward(L, dtr.mode, bh.n, g, kin);
+                    dtr.pos = re;
+                    dtr.vg = kin.dir;
+                    dtr.vmag = kin.mag;
+                    dtr.E = refl_buf[i];
+                    dtr.t = trk.t;
+                    dtr.w = trk.w;
+                    dtr.bounces = 0;
+                    push_track(stk, n_stk, a.stack_cap, err, dtr);
                 }
-                if (g.u() > static_cast<float>(s.prob_refl)) {
-                    st.killed_tracks++;
-                    st.escaped_eV += trk.E * trk.w;
-                    break;
-                }
-                st.surface_refls++;
+                trk.pos = re;
+                trk.E = refl_buf[0];
+                trk.mode = fdos(L, g.u());
+                sample = 1;
+            } else if (g.u() > static_cast<float>(s.prob_refl)) {
+                st.killed++;
+                st.esc += trk.E * trk.w;
+                live = false;
+                continue;
+            } else {
+                st.refl++;
                 trk.pos = trk.pos + bh.n * kNudge;
-                const Split sp = reflection_split(s, trk.E);
+                float p_anh, p_anh_spec;
+                if (L.split_const[bh.surf]) {
+                    p_anh = L.p_anh[bh.surf];
+                    p_anh_spec = L.p_anh_spec[bh.surf];
+                } else {
+                    const Split sp = reflection_split(s, trk.E);
+                    p_anh = static_cast<float>(sp.p_anh);
+                    p_anh_spec = static_cast<float>(sp.p_anh + sp.p_spec);
+                }
                 const float u_refl = g.u();
-                if (u_refl < static_cast<float>(sp.p_anh)) {
-                    st.surface_downconversions++;
+                if (u_refl < p_anh) {
+                    st.down++;
                     const bool tt = g.u() < L.fTT;
                     const float x = tt ? fcdf(L.cdf_tt, g) : fcdf(L.cdf_lt, g);
                     const int m1 = tt ? ftrans(L, g) : 0;
                     const int m2 = ftrans(L, g);
+                    FTrack dtr;
                     FKin k2kin;
-                    const F3 k2 = finward(L, m2, bh.n, g, k2kin);
-                    FTrack d;
-                    d.pos = trk.pos; d.k = k2; d.vg = k2kin.dir; d.vmag = k2kin.mag;
-                    d.E = (1.0 - static_cast<double>(x)) * trk.E; d.t = trk.t; d.w = trk.w; d.bounces = 0; d.mode = m2;
-                    ctx.push(d);
+                    dtr.k = finward(L, m2, bh.n, g, k2kin);
+                    dtr.pos = trk.pos;
+                    dtr.vg = k2kin.dir;
+                    dtr.vmag = k2kin.mag;
+                    dtr.E = (1.0 - static_cast<double>(x)) * trk.E;
+                    dtr.t = trk.t;
+                    dtr.w = trk.w;
+                    dtr.bounces = 0;
+                    dtr.mode = m2;
+                    push_track(stk, n_stk, a.stack_cap, err, dtr);
                     trk.E = static_cast<double>(x) * trk.E;
                     trk.mode = m1;
-                    FKin kin;
-                    trk.k = finward(L, m1, bh.n, g, kin);
-                    trk.vg = kin.dir;
-                    trk.vmag = kin.mag;
-                } else if (u_refl < static_cast<float>(sp.p_anh + sp.p_spec)) {
+                    sample = 1;
+                } else if (u_refl < p_anh_spec) {
                     F3 kr = trk.k - bh.n * (2.0f * fdot(trk.k, bh.n));
                     FKin kin = fmap(L, trk.mode, kr);
                     if (fdot(kin.dir, bh.n) <= 1e-6f) kr = finward(L, trk.mode, bh.n, g, kin);
@@ -454,23 +541,48 @@ __global__ void __launch_bounds__(128) k_batched_fp32(const FLat L, const Detect
                     trk.vg = kin.dir;
                     trk.vmag = kin.mag;
                 } else {
-                    FKin kin;
-                    trk.k = finward(L, trk.mode, bh.n, g, kin);
-                    trk.vg = kin.dir;
-                    trk.vmag = kin.mag;
+                    sample = 1;
                 }
             }
         }
-        stats_from_event(st, 0.0, a.ev_stats[unit]);
-        a.ev_nhits[unit] = a.keep_hits ? n_hits : 0;
+        // shared new-direction path: isotropic (bulk scatter) or Lambertian about the
+        // inward normal (diffuse reflection / re-emission), then the table lookup
+        if (sample != 2) {
+            const bool lam = (sample == 1);
+            const F3 e3 = lam ? bh.n : f3(0.0f, 0.0f, 1.0f);
+            const F3 e1 = lam ? forth(bh.n) : f3(1.0f, 0.0f, 0.0f);
+            const F3 e2 = lam ? fcross(bh.n, e1) : f3(0.0f, 1.0f, 0.0f);
+            FKin kin;
+            F3 kd;
+            for (int trial = 0;; ++trial) {
+                const float u1 = g.u();
+                const float u2 = g.u();
+                const float ct = lam ? sqrtf(u1) : 2.0f * u1 - 1.0f;  // Lambertian: cos theta = sqrt(u)
+                const float st_ = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+                float sphi, cphi;
+                __sincosf(kTwoPiF * u2, &sphi, &cphi);
+                kd = e1 * (st_ * cphi) + e2 * (st_ * sphi) + e3 * ct;
+                if (lam) kd = funit(kd);
+                kin = fmap(L, trk.mode, kd);
+                if (!lam || fdot(kin.dir, bh.n) > 1e-6f) break;
+                if (trial == 15) {
+                    kd = bh.n;
+                    kin = fmap(L, trk.mode, kd);
+                    break;
+                }
+            }
+            trk.k = kd;
+            trk.vg = kin.dir;
+            trk.vmag = kin.mag;
+        }
     }
-    if (ctx.err) atomicOr(a.err, ctx.err);
+    if (err) atomicOr(a.err, err);
 }
 
 }  // namespace
 
 // FP32 constants of the crystal derived from the FP64 lattice view
-static FLat make_flat(const Lattice& L, const float* cdf_f) {
+static FLat make_flat(const Lattice& L, const float* cdf_f, const Detector& D) {
     FLat f;
     f.oct = reinterpret_cast<const float4*>(L.oct);
     f.cdf_lt = cdf_f;
@@ -486,6 +598,17 @@ static FLat make_flat(const Lattice& L, const float* cdf_f) {
     f.p_st_trans = static_cast<float>(L.fSTDOS / (L.fSTDOS + L.fFTDOS));
     f.fTT = static_cast<float>(L.fTT_frac);
     f.m_ratio = static_cast<float>(L.v_sound / L.v_trans);
+    for (int i = 0; i < 3; ++i) {
+        const Surface& s = D.surf[i];
+        // the split is energy independent when every polynomial is constant (or absent)
+        const bool cst = s.n_spec <= 1 && s.n_diff <= 1 && s.n_anh <= 1;
+        f.split_const[i] = cst ? 1 : 0;
+        // constant polynomials still switch at the cut-offs; evaluate below and above them
+        const Split lo = reflection_split(s, 1e-6), hi = reflection_split(s, 1.0);
+        if (cst && (lo.p_anh != hi.p_anh || lo.p_spec != hi.p_spec)) f.split_const[i] = 0;
+        f.p_anh[i] = static_cast<float>(lo.p_anh);
+        f.p_anh_spec[i] = static_cast<float>(lo.p_anh + lo.p_spec);
+    }
     return f;
 }
 
@@ -496,7 +619,7 @@ cudaError_t launch_unit_event(const uint64_t* ph_off, uint64_t n_events, uint32_
 
 cudaError_t launch_batched_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                                 const uint32_t* unit_event, int grid, int block, cudaStream_t s) {
-    k_batched_fp32<<<grid, block, 0, s>>>(make_flat(L, cdf_f), D, a, unit_event);
+    k_batched_fp32<<<grid, block, 0, s>>>(make_flat(L, cdf_f, D), D, a, unit_event);
     return cudaGetLastError();
 }
 
