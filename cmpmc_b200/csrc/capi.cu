@@ -86,7 +86,8 @@ struct cmpmc_gpu_ctx {
     DevBuf tables;  // oct LUT + CDF tables
     int tpb = 128;
     int bps = 0;  // 0: occupancy-derived
-    uint32_t stack_cap = 1024;
+    uint32_t stack_cap = 1024;        // plain form: tracks per device thread
+    uint32_t stack_cap_batched = 256;  // batched form: one primary's lineage per thread
     uint32_t cstack_cap = 64;
     uint64_t hit_cap = 0;
     DevBuf in_rng, in_inj, in_phoff, in_ph, in_choff, in_ch;
@@ -251,7 +252,10 @@ int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_pe
         return fail(ctx, CMPMC_ERR_INVALID, "threads_per_block must be a multiple of 32 in [32, 128]");
     if (threads_per_block) ctx->tpb = threads_per_block;
     if (blocks_per_sm) ctx->bps = blocks_per_sm;
-    if (stack_capacity) ctx->stack_cap = static_cast<uint32_t>(std::min<uint64_t>(stack_capacity, 1u << 24));
+    if (stack_capacity) {
+        ctx->stack_cap = static_cast<uint32_t>(std::min<uint64_t>(stack_capacity, 1u << 24));
+        ctx->stack_cap_batched = ctx->stack_cap;
+    }
     if (hit_capacity) ctx->hit_cap = hit_capacity;
     return CMPMC_OK;
 }
@@ -378,13 +382,14 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     if (!hit_cap) hit_cap = std::max<uint64_t>(4096, std::max<uint64_t>(n, n_ph + n_ch) * 32);
     Counters hc{};
     float kms = 0.0f;
+    uint32_t& stack_cap = batched ? ctx->stack_cap_batched : ctx->stack_cap;
     for (int attempt = 0;; ++attempt) {
         if (!d->keep_hits) hit_cap = 1;
-        CK(ctx->stack.ensure(slots * ctx->stack_cap * stack_entry), "alloc phonon stacks");
+        CK(ctx->stack.ensure(slots * stack_cap * stack_entry), "alloc phonon stacks");
         CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
         CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
         a.stack = ctx->stack.as<GTrack>();
-        a.stack_cap = ctx->stack_cap;
+        a.stack_cap = stack_cap;
         a.hit_stage = ctx->hit_stage.as<cmpmc_sensor_hit>();
         a.hit_key = ctx->hit_key.as<uint64_t>();
         a.hit_cap = hit_cap;
@@ -407,7 +412,7 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
         const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
         if (!stack_over && !hits_over) break;
         if (attempt >= 10) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack or hit buffer overflow persists");
-        if (hc.err & kErrPhononStack) ctx->stack_cap = std::min<uint32_t>(ctx->stack_cap * 8, 1u << 24);
+        if (hc.err & kErrPhononStack) stack_cap = std::min<uint32_t>(stack_cap * 8, 1u << 24);
         if (hc.err & kErrChargeStack) {
             ctx->cstack_cap = std::min<uint32_t>(ctx->cstack_cap * 8, 1u << 20);
             CK(ctx->cstack.ensure(slots * ctx->cstack_cap * sizeof(GCharge)), "alloc charge stacks");
