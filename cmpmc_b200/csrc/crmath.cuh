@@ -42,6 +42,13 @@
 #endif
 #endif
 
+// rare slow paths are kept out of line so the hot kernels stay small
+#ifdef __CUDACC__
+#define CMPMC_CR_COLD static __host__ __device__ __noinline__
+#else
+#define CMPMC_CR_COLD static inline
+#endif
+
 namespace cmpmc_gpu {
 namespace crmath {
 
@@ -123,7 +130,7 @@ CMPMC_HD DD dd_div(DD x, DD y) {
 CMPMC_HD DD dd_tab(const double (*t)[2], int i) { return DD{t[i][0], t[i][1]}; }
 
 // log(x) as a double-double for positive finite normal or subnormal x
-CMPMC_HD DD log_dd(double x) {
+CMPMC_CR_COLD DD log_dd(double x) {
     uint64_t bits;
     memcpy(&bits, &x, 8);
     int e = static_cast<int>((bits >> 52) & 0x7ff);
@@ -157,16 +164,61 @@ CMPMC_HD DD log_dd(double x) {
     return res;
 }
 
+// Ziv's rounding test: (h, l) is normalised (h = RN(h + l)) and the exact value lies within
+// eps |h| of h + l; true when every value in that interval rounds to h, so h is the
+// correctly rounded result (J.-M. Muller et al., Handbook of Floating-Point Arithmetic,
+// "Ziv's strategy"). The margin is inflated slightly to cover the rounding of l +- e.
+CMPMC_HD bool ziv_ok(double h, double l, double eps) {
+    const double e = fabs(h) * (eps * 1.125);
+    return (h + (l + e) == h) && (h + (l - e) == h);
+}
+
 // log(x) correctly rounded for positive finite x; other inputs go to the platform log.
+// Fast path: the same reduction with log1p(r) summed as r - r^2/2 (error-free) plus an
+// FP64 tail, relative error below 2^-64; the double-double path runs only when the
+// rounding test fails (about one call in a thousand).
 CMPMC_HD double log(double x) {
     if (!(x > 0.0) || !(x < __builtin_huge_val())) return ::log(x);
+    uint64_t bits;
+    memcpy(&bits, &x, 8);
+    int e = static_cast<int>((bits >> 52) & 0x7ff);
+    if (e == 0) {
+        const DD r = log_dd(x);
+        return r.hi + r.lo;
+    }
+    e -= 1023;
+    const uint64_t mbits = (bits & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL;
+    double m;
+    memcpy(&m, &mbits, 8);
+    if (m >= 4.0 / 3.0) {
+        m *= 0.5;
+        e += 1;
+    }
+    const int n = static_cast<int>(m * 128.0 + 0.5);
+    const double c = n * (1.0 / 128.0);
+    const double t = m - c;
+    const double q = t / c;
+    const double ql = fma_rn(-q, c, t) / c;  // r = q + ql
+    const DD z = two_prod(q, q);
+    // log1p(q) - q + q^2/2 = q^3 (1/3 - q/4 + q^2/5 - ...), |q| < 2^-7.4, to q^11
+    const double tail = q * z.hi *
+                        (1.0 / 3 + q * (-1.0 / 4 + q * (1.0 / 5 + q * (-1.0 / 6 + q * (1.0 / 7 + q * (-1.0 / 8 +
+                         q * (1.0 / 9 + q * (-1.0 / 10 + q * (1.0 / 11)))))))));
+    const double ed = static_cast<double>(e);
+    const DD A = two_sum(ed * CMPMC_CR_LN2_H42, logc_hi(n - 85));  // ed * head is exact
+    const DD B = two_sum(A.hi, q);
+    const DD C = two_sum(B.hi, -0.5 * z.hi);
+    const double lo = A.lo + B.lo + C.lo + (ql - ql * q) - 0.5 * z.lo + tail +
+                      (ed * CMPMC_CR_LN2_T42 + logc_lo(n - 85));
+    const DD y = fast_two_sum(C.hi, lo);
+    if (ziv_ok(y.hi, y.lo, 0x1p-64)) return y.hi;
     const DD r = log_dd(x);
     return r.hi + r.lo;
 }
 
 // exp of a double-double argument t, |t| < 700: t = k ln2 + r, exp(r) = (exp(r/16))^16
 // with the Taylor series of exp(r/16), |r/16| < 0.022.
-CMPMC_HD DD exp_dd(DD t, int& k_out) {
+CMPMC_CR_COLD DD exp_dd(DD t, int& k_out) {
     const double kd = rint(t.hi * 1.4426950408889634);
     const DD kl = dd_mul_d(DD{CMPMC_CR_LN2_HI, CMPMC_CR_LN2_LO}, kd);
     DD r = dd_add(t, DD{-kl.hi, -kl.lo});
@@ -272,7 +324,66 @@ CMPMC_HD DD cos_kernel(DD z) {
 
 CMPMC_HD bool in_range(double x) { return fabs(x) < 1048576.0; }
 
+// Fast sin / cos of a reduced argument r = rh + rl (|r| <= pi/4 + eps) as unrounded (h, l)
+// with relative error below 2^-64 (sin) and 2^-63 (cos): the leading Taylor terms
+// (r^3/6, r^5/120 and r^2/2, r^4/24) in double-double, the rest in FP64.
+CMPMC_HD DD sin_fast(DD r) {
+    const double rh = r.hi, rl = r.lo;
+    const DD z = two_prod(rh, rh);                                   // rh^2 exactly
+    const DD p3 = two_prod(rh, z.hi);
+    const DD r3 = fast_two_sum(p3.hi, p3.lo + rh * z.lo);            // rh^3
+    const DD t3 = dd_mul(r3, DD{CMPMC_CR_INV6_HI, CMPMC_CR_INV6_LO});
+    const DD t5 = dd_div(dd_mul(r3, z), DD{120.0, 0.0});
+    const double zz = z.hi;
+    const double tail7 = rh * zz * zz * zz *
+                         (-1.0 / 5040 + zz * (1.0 / 362880 + zz * (-1.0 / 39916800 + zz * (1.0 / 6227020800.0 +
+                          zz * (-1.0 / 1307674368000.0 + zz * (1.0 / 355687428096000.0 +
+                          zz * (-1.0 / 121645100408832000.0 + zz * (1.0 / 51090942171709440000.0))))))));
+    const double dcos = 1.0 - 0.5 * zz + zz * zz * (1.0 / 24) - zz * zz * zz * (1.0 / 720);
+    DD s = two_sum(rh, -t3.hi);
+    const DD s2 = two_sum(s.hi, t5.hi);
+    const double lo = s.lo + s2.lo - t3.lo + t5.lo + tail7 + rl * dcos;
+    return fast_two_sum(s2.hi, lo);
+}
+CMPMC_HD DD cos_fast(DD r) {
+    const double rh = r.hi, rl = r.lo;
+    const DD z = two_prod(rh, rh);
+    const double w = z.lo + 2.0 * rh * rl;                            // r^2 = z.hi + w
+    const DD zsq = two_prod(z.hi, z.hi);
+    const DD t4 = dd_mul(DD{zsq.hi, zsq.lo + 2.0 * z.hi * w}, DD{CMPMC_CR_INV24_HI, CMPMC_CR_INV24_LO});
+    const double zz = z.hi;
+    const double tail6 = zz * zz * zz *
+                         (-1.0 / 720 + zz * (1.0 / 40320 + zz * (-1.0 / 3628800 + zz * (1.0 / 479001600.0 +
+                          zz * (-1.0 / 87178291200.0 + zz * (1.0 / 20922789888000.0 +
+                          zz * (-1.0 / 6402373705728000.0 + zz * (1.0 / 2432902008176640000.0))))))));
+    const DD c = two_sum(1.0, -0.5 * z.hi);
+    const DD c2 = two_sum(c.hi, t4.hi);
+    const double lo = c.lo + c2.lo + t4.lo - 0.5 * w + tail6;
+    return fast_two_sum(c2.hi, lo);
+}
+
+CMPMC_CR_COLD double sin_slow(double x);
+CMPMC_CR_COLD double cos_slow(double x);
+
 CMPMC_HD double sin(double x) {
+    if (!in_range(x) || x == 0.0) return sin_slow(x);
+    int q;
+    const DD r = reduce_pio2(x, q);
+    const DD v = (q & 1) ? cos_fast(r) : sin_fast(r);
+    if (!ziv_ok(v.hi, v.lo, 0x1p-62)) return sin_slow(x);
+    return (q & 2) ? -v.hi : v.hi;
+}
+
+CMPMC_HD double cos(double x) {
+    if (!in_range(x)) return cos_slow(x);
+    int q;
+    const DD r = reduce_pio2(x, q);
+    const DD v = (q & 1) ? sin_fast(r) : cos_fast(r);
+    if (!ziv_ok(v.hi, v.lo, 0x1p-62)) return cos_slow(x);
+    return ((q + 1) & 2) ? -v.hi : v.hi;
+}
+
+CMPMC_CR_COLD double sin_slow(double x) {
     if (!in_range(x)) return ::sin(x);
     if (x == 0.0) return x;
     int q;
@@ -285,7 +396,7 @@ CMPMC_HD double sin(double x) {
     return (q & 2) ? -y : y;
 }
 
-CMPMC_HD double cos(double x) {
+CMPMC_CR_COLD double cos_slow(double x) {
     if (!in_range(x)) return ::cos(x);
     int q;
     const DD r = reduce_pio2(x, q);
@@ -298,7 +409,7 @@ CMPMC_HD double cos(double x) {
 }
 
 // sin and cos of x as double-doubles (|x| < 2^20)
-CMPMC_HD void sincos_dd(double x, DD& s, DD& c) {
+CMPMC_CR_COLD void sincos_dd(double x, DD& s, DD& c) {
     int q;
     const DD r = reduce_pio2(x, q);
     const DD z = dd_mul(r, r);
@@ -325,27 +436,10 @@ CMPMC_HD double acos(double x) {
     return y0 + corr;
 }
 
-// both at once, sharing the reduction
+// both at once
 CMPMC_HD void sincos(double x, double& s, double& c) {
-    if (!in_range(x)) {
-        s = ::sin(x);
-        c = ::cos(x);
-        return;
-    }
-    int q;
-    const DD r = reduce_pio2(x, q);
-    const DD z = dd_mul(r, r);
-    const DD vs = sin_kernel(r, z);
-    const DD vc = cos_kernel(z);
-    const double ys = vs.hi + vs.lo;
-    const double yc = vc.hi + vc.lo;
-    switch (q) {
-        case 0: s = ys; c = yc; break;
-        case 1: s = yc; c = -ys; break;
-        case 2: s = -ys; c = -yc; break;
-        default: s = -yc; c = ys; break;
-    }
-    if (x == 0.0) s = x;
+    s = sin(x);
+    c = cos(x);
 }
 
 }  // namespace crmath

@@ -94,6 +94,12 @@
   }
 #define CMPMC_CR_LN2_HI 0x1.62e42fefa39efp-1
 #define CMPMC_CR_LN2_LO 0x1.abc9e3b39803fp-56
+#define CMPMC_CR_LN2_H42 0x1.62e42fefa3800p-1
+#define CMPMC_CR_LN2_T42 0x1.ef35793c76730p-45
+#define CMPMC_CR_INV6_HI 0x1.5555555555555p-3
+#define CMPMC_CR_INV6_LO 0x1.5555555555555p-57
+#define CMPMC_CR_INV24_HI 0x1.5555555555555p-5
+#define CMPMC_CR_INV24_LO 0x1.5555555555555p-59
 // 1 / (2k + 1)
 #define CMPMC_CR_INVODD { \
     {0x1.0000000000000p+0, 0x0.0p+0}, \

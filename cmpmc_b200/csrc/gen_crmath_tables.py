@@ -52,6 +52,14 @@ def main() -> None:
     out.append("  }")
     hi, lo = dd(Decimal(2).ln())
     out.append(f"#define CMPMC_CR_LN2_HI {h(hi)}\n#define CMPMC_CR_LN2_LO {h(lo)}")
+    # log 2 split for the fast path: a 42-bit head (e * head exact for |e| < 2^11) and a tail
+    l2 = Decimal(2).ln()
+    h42 = trunc_bits(l2, 42)
+    out.append(f"#define CMPMC_CR_LN2_H42 {h(h42)}\n#define CMPMC_CR_LN2_T42 {h(float(l2 - Decimal(h42)))}")
+    # 1/6 and 1/24 as double-doubles (leading Taylor terms of the fast sin / cos paths)
+    for name, v in (("INV6", Decimal(1) / 6), ("INV24", Decimal(1) / 24)):
+        a, b = dd(v)
+        out.append(f"#define CMPMC_CR_{name}_HI {h(a)}\n#define CMPMC_CR_{name}_LO {h(b)}")
     out.append("// 1 / (2k + 1)")
     out.append("#define CMPMC_CR_INVODD { \\")
     for k in range(12):

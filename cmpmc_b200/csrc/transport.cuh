@@ -160,6 +160,11 @@ CMPMC_HD void transport_phonons(const Lattice& L, const Detector& D, C& ctx, EvS
             const double d_phys = (rate_tot > 1e-12) ? (-m_log(rng.uniform()) * (trk.vmag / rate_tot)) : kInf;
             const BHit bh = intersect_exit(D.radius, D.half_z, trk.pos, trk.vg);
 
+            // new direction drawn after the branches below: 1 isotropic (Rng::isotropic_dir,
+            // rng.hpp:78-83), 2 Lambertian about the inward normal with the inward check of
+            // sample_inward_wavevector (engine.hpp:927-936). The two share one block so the
+            // lanes of a warp stay together; each lane computes exactly the reference's values.
+            int new_dir = 0;
             if (d_phys < bh.distance) {
                 trk.pos = trk.pos + trk.vg * d_phys;
                 trk.t += d_phys / trk.vmag;
@@ -170,89 +175,124 @@ CMPMC_HD void transport_phonons(const Lattice& L, const Detector& D, C& ctx, EvS
                     if (u_proc < rate_down + rate_iso) st.isotope_scatters++;
                     else st.polycrystal_scatters++;
                     trk.mode = sample_dos_mode(L, rng);
-                    trk.k = rng.isotropic_dir();
-                    set_kin(trk, map_k_to_vg(L, trk.mode, trk.k));
+                    new_dir = 1;
                 }
-                continue;
-            }
-
-            trk.pos = trk.pos + trk.vg * bh.distance;
-            trk.t += bh.distance / trk.vmag;
-            trk.bounces++;
-            const Surface& s = D.surf[bh.surf];
-            const int ch_id = -1;  // no electrode mask on the device: every pad is active
-
-            if (s.has_film && rng.uniform() < s.prob_abs) {
-                const Film& film = s.film;
-                const double p_enter = film.film_absorption;
-                if (rng.uniform() < p_enter) {
-                    const double edep = film_absorb_phonon(film, trk.E, ctx.refl, ctx.kwork, rng);
-                    if (edep > 0.0) {
-                        const double wedep = edep * trk.w;
-                        st.sensor_hits++;
-                        st.deposited_eV += wedep;
-                        Hit h;
-                        h.pos = trk.pos;
-                        h.t = trk.t;
-                        h.edep = wedep;
-                        h.incident = trk.E;
-                        h.surf = bh.surf;
-                        h.excitation = 0;
-                        h.mode = trk.mode;
-                        ctx.hit(h, ch_id);
-                    }
-                    double sum_refl = 0.0;
-                    for (int i = 0; i < ctx.refl.n; ++i) sum_refl += ctx.refl.d[i];
-                    st.escaped_eV += dmax(0.0, trk.E - edep - sum_refl) * trk.w;
-                    if (ctx.refl.n == 0) break;
-                    const V3 reemit = trk.pos + bh.n_in * 1e-11;
-                    for (int i = 1; i < ctx.refl.n; ++i) {
-                        const int m = sample_dos_mode(L, rng);
-                        const V3 kd = sample_inward(L, m, bh.n_in, rng);
-                        ctx.push(make_track(L, reemit, kd, m, ctx.refl.d[i], trk.t, trk.w));
-                    }
-                    trk.pos = reemit;
-                    trk.E = ctx.refl.d[0];
-                    trk.mode = sample_dos_mode(L, rng);
-                    trk.k = sample_inward(L, trk.mode, bh.n_in, rng);
-                    set_kin(trk, map_k_to_vg(L, trk.mode, trk.k));
-                    continue;
-                }
-            }
-
-            if (rng.uniform() > s.prob_refl) {
-                st.killed_tracks++;
-                st.escaped_eV += trk.E * trk.w;
-                break;
-            }
-            st.surface_refls++;
-            trk.pos = trk.pos + bh.n_in * 1e-11;
-            const Split split = reflection_split(s, trk.E);
-            const double u_refl = rng.uniform();
-            if (u_refl < split.p_anh) {
-                st.surface_downconversions++;
-                const bool tt = rng.uniform() < L.fTT_frac;
-                const double x = tt ? sample_cdf(L.cdf_tt, rng) : sample_cdf(L.cdf_lt, rng);
-                const int m1 = tt ? sample_transverse_mode(L, rng) : 0;
-                const int m2 = sample_transverse_mode(L, rng);
-                const V3 k2 = sample_inward(L, m2, bh.n_in, rng);
-                ctx.push(make_track(L, trk.pos, k2, m2, (1.0 - x) * trk.E, trk.t, trk.w));
-                trk.E = x * trk.E;
-                trk.mode = m1;
-                trk.k = sample_inward(L, m1, bh.n_in, rng);
-                set_kin(trk, map_k_to_vg(L, m1, trk.k));
-            } else if (u_refl < split.p_anh + split.p_spec) {
-                V3 k_refl = trk.k - bh.n_in * (2.0 * dot(trk.k, bh.n_in));
-                Kin kin = map_k_to_vg(L, trk.mode, k_refl);
-                if (dot(kin.vg_dir, bh.n_in) <= 1e-6) {
-                    k_refl = sample_inward(L, trk.mode, bh.n_in, rng);
-                    kin = map_k_to_vg(L, trk.mode, k_refl);
-                }
-                trk.k = k_refl;
-                set_kin(trk, kin);
             } else {
-                trk.k = sample_inward(L, trk.mode, bh.n_in, rng);
-                set_kin(trk, map_k_to_vg(L, trk.mode, trk.k));
+
+                trk.pos = trk.pos + trk.vg * bh.distance;
+                trk.t += bh.distance / trk.vmag;
+                trk.bounces++;
+                const Surface& s = D.surf[bh.surf];
+                const int ch_id = -1;  // no electrode mask on the device: every pad is active
+
+                if (s.has_film && rng.uniform() < s.prob_abs) {
+                    const Film& film = s.film;
+                    const double p_enter = film.film_absorption;
+                    if (rng.uniform() < p_enter) {
+                        const double edep = film_absorb_phonon(film, trk.E, ctx.refl, ctx.kwork, rng);
+                        if (edep > 0.0) {
+                            const double wedep = edep * trk.w;
+                            st.sensor_hits++;
+                            st.deposited_eV += wedep;
+                            Hit h;
+                            h.pos = trk.pos;
+                            h.t = trk.t;
+                            h.edep = wedep;
+                            h.incident = trk.E;
+                            h.surf = bh.surf;
+                            h.excitation = 0;
+                            h.mode = trk.mode;
+                            ctx.hit(h, ch_id);
+                        }
+                        double sum_refl = 0.0;
+                        for (int i = 0; i < ctx.refl.n; ++i) sum_refl += ctx.refl.d[i];
+                        st.escaped_eV += dmax(0.0, trk.E - edep - sum_refl) * trk.w;
+                        if (ctx.refl.n == 0) break;
+                        const V3 reemit = trk.pos + bh.n_in * 1e-11;
+                        for (int i = 1; i < ctx.refl.n; ++i) {
+                            const int m = sample_dos_mode(L, rng);
+                            const V3 kd = sample_inward(L, m, bh.n_in, rng);
+                            ctx.push(make_track(L, reemit, kd, m, ctx.refl.d[i], trk.t, trk.w));
+                        }
+                        trk.pos = reemit;
+                        trk.E = ctx.refl.d[0];
+                        trk.mode = sample_dos_mode(L, rng);
+                        trk.k = sample_inward(L, trk.mode, bh.n_in, rng);
+                        set_kin(trk, map_k_to_vg(L, trk.mode, trk.k));
+                        continue;
+                    }
+                }
+
+                if (rng.uniform() > s.prob_refl) {
+                    st.killed_tracks++;
+                    st.escaped_eV += trk.E * trk.w;
+                    break;
+                }
+                st.surface_refls++;
+                trk.pos = trk.pos + bh.n_in * 1e-11;
+                const Split split = reflection_split(s, trk.E);
+                const double u_refl = rng.uniform();
+                if (u_refl < split.p_anh) {
+                    st.surface_downconversions++;
+                    const bool tt = rng.uniform() < L.fTT_frac;
+                    const double x = tt ? sample_cdf(L.cdf_tt, rng) : sample_cdf(L.cdf_lt, rng);
+                    const int m1 = tt ? sample_transverse_mode(L, rng) : 0;
+                    const int m2 = sample_transverse_mode(L, rng);
+                    const V3 k2 = sample_inward(L, m2, bh.n_in, rng);
+                    ctx.push(make_track(L, trk.pos, k2, m2, (1.0 - x) * trk.E, trk.t, trk.w));
+                    trk.E = x * trk.E;
+                    trk.mode = m1;
+                    trk.k = sample_inward(L, m1, bh.n_in, rng);
+                    set_kin(trk, map_k_to_vg(L, m1, trk.k));
+                } else if (u_refl < split.p_anh + split.p_spec) {
+                    V3 k_refl = trk.k - bh.n_in * (2.0 * dot(trk.k, bh.n_in));
+                    Kin kin = map_k_to_vg(L, trk.mode, k_refl);
+                    if (dot(kin.vg_dir, bh.n_in) <= 1e-6) {
+                        k_refl = sample_inward(L, trk.mode, bh.n_in, rng);
+                        kin = map_k_to_vg(L, trk.mode, k_refl);
+                    }
+                    trk.k = k_refl;
+                    set_kin(trk, kin);
+                } else {
+                    new_dir = 2;
+                }
+            }
+            if (new_dir != 0) {
+                const bool iso = (new_dir == 1);
+                V3 ou = v3(1.0, 0.0, 0.0), ov = ou;
+                if (!iso) {
+                    ou = orthogonal_unit(bh.n_in);
+                    ov = cross(bh.n_in, ou);
+                }
+                V3 kd;
+                Kin kin;
+                for (int trial = 0;; ++trial) {
+                    const double u1 = rng.uniform();
+                    const double u2 = rng.uniform();
+                    double st_, ct_, phi;
+                    if (iso) {
+                        ct_ = 2.0 * u1 - 1.0;
+                        st_ = sqrt(dmax(0.0, 1.0 - ct_ * ct_));
+                        phi = kTwoPi * u2;
+                    } else {
+                        phi = kTwoPi * u1;
+                        st_ = sqrt(u2);
+                        ct_ = sqrt(dmax(0.0, 1.0 - st_ * st_));
+                    }
+                    const double cphi = m_cos(phi);
+                    const double sphi = m_sin(phi);
+                    kd = iso ? v3(st_ * cphi, st_ * sphi, ct_)
+                             : unit(ou * (st_ * cphi) + ov * (st_ * sphi) + bh.n_in * ct_);
+                    kin = map_k_to_vg(L, trk.mode, kd);
+                    if (iso || dot(kin.vg_dir, bh.n_in) > 1e-6) break;
+                    if (trial == 15) {
+                        kd = bh.n_in;
+                        kin = map_k_to_vg(L, trk.mode, kd);
+                        break;
+                    }
+                }
+                trk.k = kd;
+                set_kin(trk, kin);
             }
         }
     }
