@@ -348,117 +348,7 @@ __device__ __forceinline__ void write_unit(const RunArgs& a, uint64_t unit, cons
     a.ev_nhits[unit] = a.keep_hits ? n_hits : 0;
 }
 
-// Film entry of one track: Kaplan cascade, hit record, re-emission (engine.hpp:490-533).
-// Returns true when the track continues (as the first re-emitted phonon).
-__device__ __noinline__ bool film_call(const Surface* s, int surf, F3 n, FTrack* tp, const FLat* Lp, const RunArgs* ap,
-                                       uint64_t unit, uint32_t* n_hits, UStats* st, GFTrack* stk, uint32_t* n_stk,
-                                       unsigned* err, double* refl_buf, double* kwork, R128* gp) {
-    FTrack& trk = *tp;
-    const RunArgs& a = *ap;
-    const FLat& L = *Lp;
-    R128& g = *gp;
-    int n_refl = 0;
-    const double edep = kaplan_call(&s->film, trk.E, refl_buf, &n_refl, kwork, &g);
-    if (edep > 0.0) {
-        const double wedep = edep * trk.w;
-        st->hits++;
-        st->dep += wedep;
-        const uint32_t local = (*n_hits)++;
-        if (a.keep_hits) {
-            const unsigned long long idx = atomicAdd(a.hit_count, 1ull);
-            if (idx < a.hit_cap) {
-                cmpmc_sensor_hit r;
-                r.pos[0] = trk.pos.x; r.pos[1] = trk.pos.y; r.pos[2] = trk.pos.z;
-                r.time = trk.t;
-                r.edep = wedep;
-                r.incident_energy = trk.E;
-                r.surface_id = static_cast<uint8_t>(surf);
-                r.excitation = 0;
-                r.mode = static_cast<uint8_t>(trk.mode);
-                r._pad = 0;
-                r.channel_id = -1;
-                a.hit_stage[idx] = r;
-                a.hit_key[idx] = (unit << 32) | local;
-            }
-        }
-    }
-    double sum_refl = 0.0;
-    for (int i = 0; i < n_refl; ++i) sum_refl += refl_buf[i];
-    st->esc += dmax(0.0, trk.E - edep - sum_refl) * trk.w;
-    if (n_refl == 0) return false;
-    const F3 re = trk.pos + n * kNudge;
-    for (int i = 1; i < n_refl; ++i) {
-        FTrack dtr;
-        dtr.mode = fdos(L, g.u());
-        FKin kin;
-        dtr.k = finward(L, dtr.mode, n, g, kin);
-        dtr.pos = re;
-        dtr.vg = kin.dir;
-        dtr.vmag = kin.mag;
-        dtr.E = refl_buf[i];
-        dtr.t = trk.t;
-        dtr.w = trk.w;
-        dtr.bounces = 0;
-        push_track(stk, *n_stk, a.stack_cap, *err, dtr);
-    }
-    trk.pos = re;
-    trk.E = refl_buf[0];
-    trk.mode = fdos(L, g.u());
-    FKin kin;
-    trk.k = finward(L, trk.mode, n, g, kin);
-    trk.vg = kin.dir;
-    trk.vmag = kin.mag;
-    return true;
-}
-
-// surface down-conversion or specular reflection (the rare reflection branches)
-__device__ __noinline__ void rare_reflection(bool anh, F3 n, FTrack* tp, const FLat* Lp, const RunArgs* ap,
-                                             UStats* st, GFTrack* stk, uint32_t* n_stk, unsigned* err, R128* gp) {
-    FTrack& trk = *tp;
-    const FLat& L = *Lp;
-    R128& g = *gp;
-    if (anh) {
-        st->down++;
-        const bool tt = g.u() < L.fTT;
-        const float x = tt ? fcdf(L.cdf_tt, g) : fcdf(L.cdf_lt, g);
-        const int m1 = tt ? ftrans(L, g) : 0;
-        const int m2 = ftrans(L, g);
-        FTrack dtr;
-        FKin k2kin;
-        dtr.k = finward(L, m2, n, g, k2kin);
-        dtr.pos = trk.pos;
-        dtr.vg = k2kin.dir;
-        dtr.vmag = k2kin.mag;
-        dtr.E = (1.0 - static_cast<double>(x)) * trk.E;
-        dtr.t = trk.t;
-        dtr.w = trk.w;
-        dtr.bounces = 0;
-        dtr.mode = m2;
-        push_track(stk, *n_stk, ap->stack_cap, *err, dtr);
-        trk.E = static_cast<double>(x) * trk.E;
-        trk.mode = m1;
-        FKin kin;
-        trk.k = finward(L, m1, n, g, kin);
-        trk.vg = kin.dir;
-        trk.vmag = kin.mag;
-    } else {
-        F3 kr = trk.k - n * (2.0f * fdot(trk.k, n));
-        FKin kin = fmap(L, trk.mode, kr);
-        if (fdot(kin.dir, n) <= 1e-6f) kr = finward(L, trk.mode, n, g, kin);
-        trk.k = kr;
-        trk.vg = kin.dir;
-        trk.vmag = kin.mag;
-    }
-}
-
-// Warp-synchronous step loop. Every iteration each lane either fetches work, takes one
-// transport step, or waits at a film entry; the warp runs the waiting lanes' Kaplan
-// cascades together once kFilmBatch lanes wait (or no lane can step), so the long FP64
-// cascade is not executed by one lane while 31 idle. A waiting lane keeps its track and
-// its substream, so results do not depend on when the cascade runs.
-constexpr int kFilmBatch = 8;
-
-__global__ void __launch_bounds__(128, 6) k_batched_fp32(const __grid_constant__ FLat L,
+__global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__ FLat L,
                                                          const __grid_constant__ Detector D,
                                                          const __grid_constant__ RunArgs a,
                                                          const uint32_t* __restrict__ unit_event) {
@@ -477,101 +367,139 @@ __global__ void __launch_bounds__(128, 6) k_batched_fp32(const __grid_constant__
     UStats st;
     uint32_t n_hits = 0;
     uint64_t unit = ~0ull;
-    bool live = false;     // trk holds a track in flight
-    bool done = false;     // no work left for this lane
-    bool waiting = false;  // trk stopped at a film entry, cascade pending
-    int w_surf = 0;
-    F3 w_n = f3(0.0f, 0.0f, 0.0f);
+    bool live = false;  // trk holds a track in flight
     for (;;) {
-        if (!done && !waiting && !live) {
+        if (!live) {
             if (n_stk > 0) {
                 pop_track(stk, n_stk, trk);
                 live = true;
             } else {
                 if (unit != ~0ull) write_unit(a, unit, st, n_hits);
                 unit = atomicAdd(a.next_work, 1ull);
-                if (unit >= a.n_events) {
-                    done = true;
-                } else {
-                    const uint32_t ev = unit_event[unit];
-                    const uint64_t j = unit - a.ph_off[ev];
-                    g.seed(seed_key ^ mix64(((a.first_event + ev) << 20) | j));
-                    const cmpmc_phonon_track& in = a.ph[unit];
-                    trk.pos = f3(static_cast<float>(in.pos[0]), static_cast<float>(in.pos[1]),
-                                 static_cast<float>(in.pos[2]));
-                    trk.k = f3(static_cast<float>(in.k_dir[0]), static_cast<float>(in.k_dir[1]),
-                               static_cast<float>(in.k_dir[2]));
-                    trk.vg = f3(static_cast<float>(in.vg_dir[0]), static_cast<float>(in.vg_dir[1]),
-                                static_cast<float>(in.vg_dir[2]));
-                    trk.vmag = static_cast<float>(in.vg_mag);
-                    trk.E = in.energy;
-                    trk.t = in.time;
-                    trk.w = static_cast<float>(in.weight);
-                    trk.bounces = in.bounces;
-                    trk.mode = in.mode;
-                    st = UStats{0, 0, 0, 0, 0, 0, 0, 0, 0, 0.0, 0.0};
-                    n_hits = 0;
-                    live = true;
-                }
+                if (unit >= a.n_events) break;
+                const uint32_t ev = unit_event[unit];
+                const uint64_t j = unit - a.ph_off[ev];
+                g.seed(seed_key ^ mix64(((a.first_event + ev) << 20) | j));
+                const cmpmc_phonon_track& in = a.ph[unit];
+                trk.pos = f3(static_cast<float>(in.pos[0]), static_cast<float>(in.pos[1]),
+                             static_cast<float>(in.pos[2]));
+                trk.k = f3(static_cast<float>(in.k_dir[0]), static_cast<float>(in.k_dir[1]),
+                           static_cast<float>(in.k_dir[2]));
+                trk.vg = f3(static_cast<float>(in.vg_dir[0]), static_cast<float>(in.vg_dir[1]),
+                            static_cast<float>(in.vg_dir[2]));
+                trk.vmag = static_cast<float>(in.vg_mag);
+                trk.E = in.energy;
+                trk.t = in.time;
+                trk.w = static_cast<float>(in.weight);
+                trk.bounces = in.bounces;
+                trk.mode = in.mode;
+                st = UStats{0, 0, 0, 0, 0, 0, 0, 0, 0, 0.0, 0.0};
+                n_hits = 0;
+                live = true;
             }
         }
-        if (live && !waiting) do {
-            if (trk.E < min_E || trk.bounces >= D.max_bounces) {
+        if (trk.E < min_E || trk.bounces >= D.max_bounces) {
+            st.killed++;
+            st.esc += trk.E * trk.w;
+            live = false;
+            continue;
+        }
+        if (D.rr_bounces != 0 && trk.bounces > D.rr_bounces && (trk.bounces - D.rr_bounces) % 32 == 0) {
+            if (g.u() < static_cast<float>(D.rr_survival)) {
+                trk.w /= static_cast<float>(D.rr_survival);
+            } else {
+                st.killed++;
+                live = false;
+                continue;
+            }
+        }
+        st.steps++;
+        const float nu = static_cast<float>(trk.E) * L.inv_h_thz;
+        const float nu2 = nu * nu;
+        const float r_iso = L.b4 * (nu2 * nu2);
+        const float r_poly = trk.vmag * L.poly_inv;
+        const float r_down = (trk.mode == 0) ? L.a5 * (nu2 * nu2 * nu) : 0.0f;
+        const float r_tot = r_iso + r_poly + r_down;
+        const float d_phys = (r_tot > 1e-12f) ? (-logf(g.u()) * trk.vmag / r_tot) : __int_as_float(0x7f800000);
+        const FBHit bh = fexit(R, H, trk.pos, trk.vg);
+        const bool bulk = d_phys < bh.d;
+        const float d = bulk ? d_phys : bh.d;
+        trk.pos = trk.pos + trk.vg * d;
+        trk.t += static_cast<double>(d / trk.vmag);
+        // 0: new isotropic direction (bulk scatter), 1: Lambertian about bh.n, 2: nothing more
+        int sample = 2;
+        if (bulk) {
+            const float u_proc = g.u() * r_tot;
+            if (r_down > 0.0f && u_proc < r_down) {
+                decay_call(&L, &trk, stk, &n_stk, a.stack_cap, &err, &st, &g);
+            } else {
+                if (u_proc < r_down + r_iso) st.iso++;
+                else st.poly++;
+                trk.mode = fdos(L, g.u());
+                sample = 0;
+            }
+        } else {
+            trk.bounces++;
+            const Surface& s = D.surf[bh.surf];
+            if (s.has_film && g.u() < static_cast<float>(s.prob_abs) &&
+                g.u() < static_cast<float>(s.film.film_absorption)) {
+                int n_refl = 0;
+                const double edep = kaplan_call(&s.film, trk.E, refl_buf, &n_refl, kwork, &g);
+                if (edep > 0.0) {
+                    const double wedep = edep * trk.w;
+                    st.hits++;
+                    st.dep += wedep;
+                    const uint32_t local = n_hits++;
+                    if (a.keep_hits) {
+                        const unsigned long long idx = atomicAdd(a.hit_count, 1ull);
+                        if (idx < a.hit_cap) {
+                            cmpmc_sensor_hit r;
+                            r.pos[0] = trk.pos.x; r.pos[1] = trk.pos.y; r.pos[2] = trk.pos.z;
+                            r.time = trk.t;
+                            r.edep = wedep;
+                            r.incident_energy = trk.E;
+                            r.surface_id = static_cast<uint8_t>(bh.surf);
+                            r.excitation = 0;
+                            r.mode = static_cast<uint8_t>(trk.mode);
+                            r._pad = 0;
+                            r.channel_id = -1;
+                            a.hit_stage[idx] = r;
+                            a.hit_key[idx] = (unit << 32) | local;
+                        }
+                    }
+                }
+                double sum_refl = 0.0;
+                for (int i = 0; i < n_refl; ++i) sum_refl += refl_buf[i];
+                st.esc += dmax(0.0, trk.E - edep - sum_refl) * trk.w;
+                if (n_refl == 0) {
+                    live = false;
+                    continue;
+                }
+                const F3 re = trk.pos + bh.n * kNudge;
+                for (int i = 1; i < n_refl; ++i) {
+                    FTrack dtr;
+                    dtr.mode = fdos(L, g.u());
+                    FKin kin;
+                    dtr.k = finward(L, dtr.mode, bh.n, g, kin);
+                    dtr.pos = re;
+                    dtr.vg = kin.dir;
+                    dtr.vmag = kin.mag;
+                    dtr.E = refl_buf[i];
+                    dtr.t = trk.t;
+                    dtr.w = trk.w;
+                    dtr.bounces = 0;
+                    push_track(stk, n_stk, a.stack_cap, err, dtr);
+                }
+                trk.pos = re;
+                trk.E = refl_buf[0];
+                trk.mode = fdos(L, g.u());
+                sample = 1;
+            } else if (g.u() > static_cast<float>(s.prob_refl)) {
                 st.killed++;
                 st.esc += trk.E * trk.w;
                 live = false;
-                break;
-            }
-            if (D.rr_bounces != 0 && trk.bounces > D.rr_bounces && (trk.bounces - D.rr_bounces) % 32 == 0) {
-                if (g.u() < static_cast<float>(D.rr_survival)) {
-                    trk.w /= static_cast<float>(D.rr_survival);
-                } else {
-                    st.killed++;
-                    live = false;
-                    break;
-                }
-            }
-            st.steps++;
-            const float nu = static_cast<float>(trk.E) * L.inv_h_thz;
-            const float nu2 = nu * nu;
-            const float r_iso = L.b4 * (nu2 * nu2);
-            const float r_poly = trk.vmag * L.poly_inv;
-            const float r_down = (trk.mode == 0) ? L.a5 * (nu2 * nu2 * nu) : 0.0f;
-            const float r_tot = r_iso + r_poly + r_down;
-            const float d_phys = (r_tot > 1e-12f) ? (-logf(g.u()) * trk.vmag / r_tot) : __int_as_float(0x7f800000);
-            const FBHit bh = fexit(R, H, trk.pos, trk.vg);
-            const bool bulk = d_phys < bh.d;
-            const float d = bulk ? d_phys : bh.d;
-            trk.pos = trk.pos + trk.vg * d;
-            trk.t += static_cast<double>(d / trk.vmag);
-            // 0: new isotropic direction (bulk scatter), 1: Lambertian about bh.n, 2: done
-            int sample = 2;
-            if (bulk) {
-                const float u_proc = g.u() * r_tot;
-                if (r_down > 0.0f && u_proc < r_down) {
-                    decay_call(&L, &trk, stk, &n_stk, a.stack_cap, &err, &st, &g);
-                } else {
-                    if (u_proc < r_down + r_iso) st.iso++;
-                    else st.poly++;
-                    trk.mode = fdos(L, g.u());
-                    sample = 0;
-                }
+                continue;
             } else {
-                trk.bounces++;
-                const Surface& s = D.surf[bh.surf];
-                if (s.has_film && g.u() < static_cast<float>(s.prob_abs) &&
-                    g.u() < static_cast<float>(s.film.film_absorption)) {
-                    waiting = true;  // the cascade runs with the warp's other waiting lanes
-                    w_surf = bh.surf;
-                    w_n = bh.n;
-                    break;
-                }
-                if (g.u() > static_cast<float>(s.prob_refl)) {
-                    st.killed++;
-                    st.esc += trk.E * trk.w;
-                    live = false;
-                    break;
-                }
                 st.refl++;
                 trk.pos = trk.pos + bh.n * kNudge;
                 float p_anh, p_anh_spec;
@@ -584,50 +512,68 @@ __global__ void __launch_bounds__(128, 6) k_batched_fp32(const __grid_constant__
                     p_anh_spec = static_cast<float>(sp.p_anh + sp.p_spec);
                 }
                 const float u_refl = g.u();
-                if (u_refl < p_anh_spec) rare_reflection(u_refl < p_anh, bh.n, &trk, &L, &a, &st, stk, &n_stk, &err, &g);
-                else sample = 1;
-            }
-            // shared new-direction path: isotropic (bulk scatter) or Lambertian about the
-            // inward normal (diffuse reflection), then the table lookup
-            if (sample != 2) {
-                const bool lam = (sample == 1);
-                const F3 e3 = lam ? bh.n : f3(0.0f, 0.0f, 1.0f);
-                const F3 e1 = lam ? forth(bh.n) : f3(1.0f, 0.0f, 0.0f);
-                const F3 e2 = lam ? fcross(bh.n, e1) : f3(0.0f, 1.0f, 0.0f);
-                FKin kin;
-                F3 kd;
-                for (int trial = 0;; ++trial) {
-                    const float u1 = g.u();
-                    const float u2 = g.u();
-                    const float ct = lam ? sqrtf(u1) : 2.0f * u1 - 1.0f;  // Lambertian: cos theta = sqrt(u)
-                    const float st_ = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
-                    float sphi, cphi;
-                    __sincosf(kTwoPiF * u2, &sphi, &cphi);
-                    kd = e1 * (st_ * cphi) + e2 * (st_ * sphi) + e3 * ct;
-                    if (lam) kd = funit(kd);
-                    kin = fmap(L, trk.mode, kd);
-                    if (!lam || fdot(kin.dir, bh.n) > 1e-6f) break;
-                    if (trial == 15) {
-                        kd = bh.n;
-                        kin = fmap(L, trk.mode, kd);
-                        break;
-                    }
+                if (u_refl < p_anh) {
+                    st.down++;
+                    const bool tt = g.u() < L.fTT;
+                    const float x = tt ? fcdf(L.cdf_tt, g) : fcdf(L.cdf_lt, g);
+                    const int m1 = tt ? ftrans(L, g) : 0;
+                    const int m2 = ftrans(L, g);
+                    FTrack dtr;
+                    FKin k2kin;
+                    dtr.k = finward(L, m2, bh.n, g, k2kin);
+                    dtr.pos = trk.pos;
+                    dtr.vg = k2kin.dir;
+                    dtr.vmag = k2kin.mag;
+                    dtr.E = (1.0 - static_cast<double>(x)) * trk.E;
+                    dtr.t = trk.t;
+                    dtr.w = trk.w;
+                    dtr.bounces = 0;
+                    dtr.mode = m2;
+                    push_track(stk, n_stk, a.stack_cap, err, dtr);
+                    trk.E = static_cast<double>(x) * trk.E;
+                    trk.mode = m1;
+                    sample = 1;
+                } else if (u_refl < p_anh_spec) {
+                    F3 kr = trk.k - bh.n * (2.0f * fdot(trk.k, bh.n));
+                    FKin kin = fmap(L, trk.mode, kr);
+                    if (fdot(kin.dir, bh.n) <= 1e-6f) kr = finward(L, trk.mode, bh.n, g, kin);
+                    trk.k = kr;
+                    trk.vg = kin.dir;
+                    trk.vmag = kin.mag;
+                } else {
+                    sample = 1;
                 }
-                trk.k = kd;
-                trk.vg = kin.dir;
-                trk.vmag = kin.mag;
             }
-        } while (false);
-        // warp-level schedule of the film cascades
-        const unsigned m_wait = __ballot_sync(0xffffffffu, waiting);
-        const unsigned m_run = __ballot_sync(0xffffffffu, !done && !waiting);
-        if (m_wait == 0 && m_run == 0) break;
-        if (m_wait != 0 && (__popc(m_wait) >= kFilmBatch || m_run == 0)) {
-            if (waiting) {
-                live = film_call(&D.surf[w_surf], w_surf, w_n, &trk, &L, &a, unit, &n_hits, &st, stk, &n_stk, &err,
-                                 refl_buf, kwork, &g);
-                waiting = false;
+        }
+        // shared new-direction path: isotropic (bulk scatter) or Lambertian about the
+        // inward normal (diffuse reflection / re-emission), then the table lookup
+        if (sample != 2) {
+            const bool lam = (sample == 1);
+            const F3 e3 = lam ? bh.n : f3(0.0f, 0.0f, 1.0f);
+            const F3 e1 = lam ? forth(bh.n) : f3(1.0f, 0.0f, 0.0f);
+            const F3 e2 = lam ? fcross(bh.n, e1) : f3(0.0f, 1.0f, 0.0f);
+            FKin kin;
+            F3 kd;
+            for (int trial = 0;; ++trial) {
+                const float u1 = g.u();
+                const float u2 = g.u();
+                const float ct = lam ? sqrtf(u1) : 2.0f * u1 - 1.0f;  // Lambertian: cos theta = sqrt(u)
+                const float st_ = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+                float sphi, cphi;
+                __sincosf(kTwoPiF * u2, &sphi, &cphi);
+                kd = e1 * (st_ * cphi) + e2 * (st_ * sphi) + e3 * ct;
+                if (lam) kd = funit(kd);
+                kin = fmap(L, trk.mode, kd);
+                if (!lam || fdot(kin.dir, bh.n) > 1e-6f) break;
+                if (trial == 15) {
+                    kd = bh.n;
+                    kin = fmap(L, trk.mode, kd);
+                    break;
+                }
             }
+            trk.k = kd;
+            trk.vg = kin.dir;
+            trk.vmag = kin.mag;
         }
     }
     if (err) atomicOr(a.err, err);
