@@ -30,6 +30,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -42,7 +43,7 @@ UNIT = "primary phonon tracks/s"
 EVENTS = 10000
 PER_EVENT = 100
 SEED = 7
-BYTES_PER_STEP = 192  # algorithmic FP32 track-state traffic per transport step
+BYTES_PER_STEP = 192  # algorithmic FP32 track state read + written per transport step: 2 x 96 B
 
 
 def dist_env():
@@ -73,10 +74,10 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        fd, self.path = tempfile.mkstemp(prefix=f"cmpmc_clocks{index}_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
