@@ -8,10 +8,12 @@ from .api import (AluminumFilm, CmpmcError, CrystalConfig, CrystalLattice, Cylin
                   EventInput, ExcitationType, KaplanFilm, PackedEvents, PhononMode, Rng, RunOptions, RunResult,
                   SimStats, SimulationEngine, SuperconductorFilmConfig, SurfaceId, SurfaceProperty,
                   UniformElectricField, UnvalidatedModuleError, Workload, materials, run_events, units, workloads)
+from .adjoint import AdjointResult, HistogramAdjoint, THETA_NAMES, default_theta
 
 __all__ = [
-    "AluminumFilm", "CmpmcError", "CrystalConfig", "CrystalLattice", "CylinderSolid", "DetectorModel", "EventInput",
+    "AdjointResult", "AluminumFilm", "CmpmcError", "CrystalConfig", "CrystalLattice", "CylinderSolid", "DetectorModel", "EventInput",
     "ExcitationType", "KaplanFilm", "PackedEvents", "PhononMode", "Rng", "RunOptions", "RunResult", "SimStats",
     "SimulationEngine", "SuperconductorFilmConfig", "SurfaceId", "SurfaceProperty", "UniformElectricField",
-    "UnvalidatedModuleError", "Workload", "materials", "run_events", "units", "workloads",
+    "UnvalidatedModuleError", "Workload", "materials", "run_events", "units", "workloads", "HistogramAdjoint",
+    "THETA_NAMES", "default_theta",
 ]

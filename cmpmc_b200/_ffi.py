@@ -122,6 +122,26 @@ class RunOutC(C.Structure):
     ]
 
 
+ADJ_MAX_BINS = 256
+
+
+class AdjointDescC(C.Structure):
+    _fields_ = [
+        ("n_events", _u64), ("first_event", _u64), ("seed", _u64), ("phonon_offsets", C.c_void_p),
+        ("phonons", C.c_void_p), ("inputs_on_device", _i32), ("n_bins", _i32), ("t_min", _f64), ("t_max", _f64),
+        ("theta", _f64 * 4), ("bin_weight", C.c_void_p), ("per_primary", C.c_void_p),
+        ("per_primary_on_device", _i32), ("_pad0", _i32),
+    ]
+
+
+class AdjointOutC(C.Structure):
+    _fields_ = [
+        ("hist", _f64 * ADJ_MAX_BINS), ("value", _f64), ("grad", _f64 * 4), ("value_var", _f64),
+        ("grad_var", _f64 * 4), ("stats", SimStatsC), ("n_primaries", _u64), ("kernel_ms", _f64),
+        ("total_ms", _f64), ("device_error", _u32), ("kernel_launches", _u32),
+    ]
+
+
 _SIG = {
     "cmpmc_abi_sizes": (_i32, [C.POINTER(C.c_size_t), _i32]),
     "cmpmc_crystal_config_germanium": (None, [C.POINTER(CrystalConfigC)]),
@@ -144,6 +164,7 @@ _SIG = {
     "cmpmc_gpu_create": (_i32, [C.c_void_p, C.POINTER(DetectorC), _i32, C.POINTER(C.c_void_p)]),
     "cmpmc_gpu_destroy": (None, [C.c_void_p]),
     "cmpmc_gpu_run_events": (_i32, [C.c_void_p, C.POINTER(RunDescC), C.POINTER(RunOutC)]),
+    "cmpmc_gpu_adjoint": (_i32, [C.c_void_p, C.POINTER(AdjointDescC), C.POINTER(AdjointOutC)]),
     "cmpmc_gpu_last_error": (_i32, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "cmpmc_gpu_configure": (_i32, [C.c_void_p, _i32, _i32, _u64, _u64]),
     "cmpmc_gpu_device_count": (_i32, [C.POINTER(_i32)]),
@@ -174,10 +195,11 @@ def load() -> C.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    sizes = (C.c_size_t * 10)()
-    ver = lib.cmpmc_abi_sizes(sizes, 10)
+    sizes = (C.c_size_t * 12)()
+    ver = lib.cmpmc_abi_sizes(sizes, 12)
     want = [128, 128, 56, 208, C.sizeof(CrystalConfigC), C.sizeof(FilmConfigC), C.sizeof(SurfaceC),
-            C.sizeof(DetectorC), C.sizeof(RunDescC), C.sizeof(RunOutC)]
+            C.sizeof(DetectorC), C.sizeof(RunDescC), C.sizeof(RunOutC), C.sizeof(AdjointDescC),
+            C.sizeof(AdjointOutC)]
     if ver != ABI_VERSION or list(sizes) != want:
         raise ImportError(f"ABI mismatch: library v{ver} sizes {list(sizes)} vs binding {want}")
     assert PHONON_DTYPE.itemsize == 128 and CHARGE_DTYPE.itemsize == 128 and HIT_DTYPE.itemsize == 56

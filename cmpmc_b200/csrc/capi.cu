@@ -93,6 +93,7 @@ struct cmpmc_gpu_ctx {
     DevBuf in_rng, in_inj, in_phoff, in_ph, in_choff, in_ch;
     DevBuf stack, cstack, hit_stage, hit_key, counters, ev_stats, ev_nhits, offsets, hits_out, total;
     DevBuf unit_event, ev_offsets, ev_stats2, partials;  // batched form: unit -> event map, event offsets / stats
+    DevBuf adj_prim, adj_hist, adj_w, adj_partials, adj_sums;  // adjoint: per-primary rows, bins, reductions
     const float* cdf_f = nullptr;              // FP32 copies of the decay tables (in `tables`)
     HostBuf h_hits, h_offsets, h_evstats, h_total, h_counters;
     cudaEvent_t e_start = nullptr, e_k0 = nullptr, e_k1 = nullptr, e_end = nullptr;
@@ -224,7 +225,8 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     for (DevBuf* b : {&ctx->tables, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
-                      &ctx->unit_event, &ctx->ev_offsets, &ctx->ev_stats2, &ctx->partials})
+                      &ctx->unit_event, &ctx->ev_offsets, &ctx->ev_stats2, &ctx->partials, &ctx->adj_prim,
+                      &ctx->adj_hist, &ctx->adj_w, &ctx->adj_partials, &ctx->adj_sums})
         b->release();
     for (HostBuf* b : {&ctx->h_hits, &ctx->h_offsets, &ctx->h_evstats, &ctx->h_total, &ctx->h_counters})
         b->release();
@@ -473,6 +475,208 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     CK(cudaEventElapsedTime(&tms, ctx->e_start, ctx->e_end), "event time");
     out->stats = *ctx->h_total.as<cmpmc_sim_stats>();
     out->n_hits = n_hits;
+    out->kernel_ms = kms;
+    out->total_ms = tms;
+    out->device_error = hc.err;
+    out->kernel_launches = static_cast<uint32_t>(launches);
+    return CMPMC_OK;
+}
+
+// Adjoint of the hit-time histogram (batched FP32 form with per-track scores). theta
+// replaces the context's isotope and anharmonic coefficients, the reflection split of every
+// surface and the absorption of every film for this call only.
+int cmpmc_gpu_adjoint(cmpmc_gpu_ctx* ctx, const cmpmc_adjoint_desc* d, cmpmc_adjoint_out* out) {
+    if (!ctx || !d || !out) return CMPMC_ERR_INVALID;
+    std::memset(out, 0, sizeof(*out));
+    ctx->last_status = CMPMC_OK;
+    ctx->last_error.clear();
+    const uint64_t n = d->n_events;
+    if (n > (1ull << 31)) return fail(ctx, CMPMC_ERR_INVALID, "too many events in one call");
+    if (n > 0 && !d->phonon_offsets) return fail(ctx, CMPMC_ERR_INVALID, "phonon_offsets is required");
+    if (d->n_bins < 1 || d->n_bins > CMPMC_ADJ_MAX_BINS) return fail(ctx, CMPMC_ERR_INVALID, "n_bins out of range");
+    if (!(d->t_max > d->t_min)) return fail(ctx, CMPMC_ERR_INVALID, "t_max must exceed t_min");
+    const double* th = d->theta;
+    if (!(th[0] > 0.0) || !(th[1] > 0.0) || !(th[2] > 0.0 && th[2] <= 1.0) || !(th[3] > 0.0 && th[3] <= 1.0))
+        return fail(ctx, CMPMC_ERR_INVALID, "theta: B_iso > 0, A_anh > 0, diffuse fraction and film absorption in (0, 1]");
+    std::string err;
+    const int vst = validate_config(ctx->cfg, ctx->det, false, err);
+    if (vst != CMPMC_OK) return fail(ctx, vst, err);
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = ctx->stream;
+    int launches = 0;
+    CK(cudaEventRecord(ctx->e_start, s), "event");
+
+    // ---- parameters ------------------------------------------------------------------
+    Lattice L = ctx->L;
+    L.B_iso = th[0];
+    L.A_anh = th[1];
+    Detector D = ctx->D;
+    for (int i = 0; i < 3; ++i) {
+        Surface& sf = D.surf[i];
+        sf.n_spec = 1;
+        sf.spec[0] = 1.0 - th[2];
+        sf.n_diff = 1;
+        sf.diff[0] = th[2];
+        sf.n_anh = 0;
+        sf.spec_prob_const = 1.0 - th[2];
+        if (sf.has_film) sf.film.film_absorption = th[3];
+    }
+
+    // ---- inputs --------------------------------------------------------------------
+    RunArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.first_event = d->first_event;
+    a.keep_hits = 0;
+    a.seed = d->seed;
+    uint64_t n_ph = 0;
+    if (d->inputs_on_device) {
+        a.ph_off = d->phonon_offsets;
+        a.ph = d->phonons;
+        if (n > 0) {
+            CK(cudaMemcpyAsync(&n_ph, d->phonon_offsets + n, 8, cudaMemcpyDeviceToHost, s), "read track count");
+            CK(cudaStreamSynchronize(s), "read track count");
+        }
+    } else if (n > 0) {
+        n_ph = d->phonon_offsets[n];
+        if (n_ph && !d->phonons) return fail(ctx, CMPMC_ERR_INVALID, "phonons are required for non-empty stacks");
+        CK(ctx->in_phoff.ensure((n + 1) * 8), "alloc offsets");
+        CK(ctx->in_ph.ensure(std::max<uint64_t>(n_ph, 1) * sizeof(cmpmc_phonon_track)), "alloc phonons");
+        CK(cudaMemcpyAsync(ctx->in_phoff.p, d->phonon_offsets, (n + 1) * 8, cudaMemcpyHostToDevice, s),
+           "copy offsets");
+        if (n_ph)
+            CK(cudaMemcpyAsync(ctx->in_ph.p, d->phonons, n_ph * sizeof(cmpmc_phonon_track), cudaMemcpyHostToDevice, s),
+               "copy phonons");
+        a.ph_off = ctx->in_phoff.as<uint64_t>();
+        a.ph = ctx->in_ph.as<cmpmc_phonon_track>();
+    }
+    if (n_ph >= (1ull << 32)) return fail(ctx, CMPMC_ERR_INVALID, "too many primaries in one call");
+    const uint64_t units = n_ph;
+    a.n_events = units;
+
+    int bps = ctx->bps;
+    if (!bps) {
+        CK(adjoint_fp32_occupancy(ctx->tpb, &bps), "occupancy");
+        bps = std::max(bps, 1);
+    }
+    uint64_t grid = static_cast<uint64_t>(ctx->num_sms) * bps;
+    grid = std::min<uint64_t>(grid, (std::max<uint64_t>(units, 1) + ctx->tpb - 1) / ctx->tpb);
+    grid = std::max<uint64_t>(grid, 1);
+    const uint64_t slots = grid * ctx->tpb;
+
+    CK(ctx->ev_stats.ensure(std::max<uint64_t>(units, 1) * sizeof(cmpmc_sim_stats)), "alloc unit stats");
+    CK(ctx->ev_nhits.ensure(std::max<uint64_t>(units, 1) * 8), "alloc unit hit counts");
+    CK(ctx->counters.ensure(sizeof(Counters)), "alloc counters");
+    CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
+    CK(ctx->partials.ensure(kReducePartials * sizeof(cmpmc_sim_stats)), "alloc partial totals");
+    CK(ctx->h_counters.ensure(sizeof(Counters)), "alloc host counters");
+    CK(ctx->unit_event.ensure(std::max<uint64_t>(units, 1) * 4), "alloc unit map");
+    CK(ctx->adj_prim.ensure(std::max<uint64_t>(units, 1) * kAdjCols * 8), "alloc per-primary rows");
+    CK(ctx->adj_hist.ensure(CMPMC_ADJ_MAX_BINS * 8), "alloc histogram");
+    CK(ctx->adj_w.ensure(CMPMC_ADJ_MAX_BINS * 4), "alloc bin weights");
+    CK(ctx->adj_partials.ensure(kColPartials * 2 * kAdjCols * 8), "alloc partial sums");
+    CK(ctx->adj_sums.ensure(2 * kAdjCols * 8), "alloc sums");
+    CK(ctx->h_total.ensure(sizeof(cmpmc_sim_stats) + (CMPMC_ADJ_MAX_BINS + 2 * kAdjCols) * 8), "alloc host totals");
+    float w[CMPMC_ADJ_MAX_BINS];
+    for (int b = 0; b < d->n_bins; ++b) w[b] = d->bin_weight ? static_cast<float>(d->bin_weight[b]) : 0.0f;
+    CK(cudaMemcpyAsync(ctx->adj_w.p, w, d->n_bins * 4, cudaMemcpyHostToDevice, s), "copy bin weights");
+    CK(cudaStreamSynchronize(s), "copy bin weights");  // w lives on this stack frame
+    if (n > 0) {
+        CK(launch_unit_event(a.ph_off, n, ctx->unit_event.as<uint32_t>(), s), "unit map");
+        ++launches;
+    }
+    a.ev_stats = ctx->ev_stats.as<cmpmc_sim_stats>();
+    a.ev_nhits = ctx->ev_nhits.as<uint64_t>();
+    Counters* dc = ctx->counters.as<Counters>();
+    a.hit_count = &dc->hit_count;
+    a.next_work = &dc->next_work;
+    a.err = &dc->err;
+    a.hit_cap = 0;
+
+    AdjArgs adj;
+    std::memset(&adj, 0, sizeof(adj));
+    adj.n_bins = d->n_bins;
+    adj.t0 = d->t_min;
+    adj.inv_dt = d->n_bins / (d->t_max - d->t_min);
+    adj.bin_w = ctx->adj_w.as<float>();
+    adj.hist = ctx->adj_hist.as<double>();
+    adj.prim = ctx->adj_prim.as<double>();
+    adj.spec_score = th[2] < 1.0 ? static_cast<float>(-th[2] / (1.0 - th[2])) : 0.0f;
+    adj.film_miss_score = th[3] < 1.0 ? static_cast<float>(-th[3] / (1.0 - th[3])) : 0.0f;
+    for (int k = 0; k < 4; ++k) adj.inv_theta[k] = 1.0 / th[k];
+
+    Counters hc{};
+    float kms = 0.0f;
+    uint32_t& stack_cap = ctx->stack_cap_batched;
+    for (int attempt = 0;; ++attempt) {
+        CK(ctx->stack.ensure(slots * stack_cap * adjoint_stack_entry_bytes()), "alloc phonon stacks");
+        a.stack = ctx->stack.as<GTrack>();
+        a.stack_cap = stack_cap;
+        CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s), "memset counters");
+        CK(cudaMemsetAsync(ctx->adj_hist.p, 0, CMPMC_ADJ_MAX_BINS * 8, s), "memset histogram");
+        CK(cudaEventRecord(ctx->e_k0, s), "event");
+        if (units > 0) {
+            CK(launch_adjoint_fp32(L, ctx->cdf_f, D, a, adj, ctx->unit_event.as<uint32_t>(), static_cast<int>(grid),
+                                   ctx->tpb, s),
+               "adjoint launch");
+            ++launches;
+        }
+        CK(cudaEventRecord(ctx->e_k1, s), "event");
+        CK(cudaMemcpyAsync(ctx->h_counters.p, ctx->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s),
+           "copy counters");
+        CK(cudaStreamSynchronize(s), "adjoint kernel");
+        hc = *ctx->h_counters.as<Counters>();
+        CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
+        if (!(hc.err & kErrPhononStack)) break;
+        if (attempt >= 10) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack overflow persists");
+        stack_cap = std::min<uint32_t>(stack_cap * 8, 1u << 24);
+    }
+    if (hc.err) return fail(ctx, CMPMC_ERR_DEVICE, "adjoint kernel reported error word " + std::to_string(hc.err));
+
+    // ---- reductions (fixed order) and outputs -------------------------------------------
+    char* hbuf = static_cast<char*>(ctx->h_total.p);
+    if (units > 0) {
+        CK(launch_reduce_cols(adj.prim, units, kAdjCols, ctx->adj_partials.as<double>(), ctx->adj_sums.as<double>(), s,
+                              &launches),
+           "reduce per-primary rows");
+        CK(launch_reduce_stats(a.ev_stats, units, ctx->partials.as<cmpmc_sim_stats>(), ctx->total.as<cmpmc_sim_stats>(),
+                               s, &launches),
+           "reduce stats");
+    } else {
+        CK(cudaMemsetAsync(ctx->adj_sums.p, 0, 2 * kAdjCols * 8, s), "memset sums");
+        CK(cudaMemsetAsync(ctx->total.p, 0, sizeof(cmpmc_sim_stats), s), "memset totals");
+    }
+    CK(cudaMemcpyAsync(hbuf, ctx->total.p, sizeof(cmpmc_sim_stats), cudaMemcpyDeviceToHost, s), "copy totals");
+    CK(cudaMemcpyAsync(hbuf + sizeof(cmpmc_sim_stats), ctx->adj_hist.p, CMPMC_ADJ_MAX_BINS * 8,
+                       cudaMemcpyDeviceToHost, s),
+       "copy histogram");
+    CK(cudaMemcpyAsync(hbuf + sizeof(cmpmc_sim_stats) + CMPMC_ADJ_MAX_BINS * 8, ctx->adj_sums.p, 2 * kAdjCols * 8,
+                       cudaMemcpyDeviceToHost, s),
+       "copy sums");
+    if (d->per_primary && units > 0)
+        CK(cudaMemcpyAsync(d->per_primary, adj.prim, units * kAdjCols * 8,
+                           d->per_primary_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s),
+           "copy per-primary rows");
+    CK(cudaEventRecord(ctx->e_end, s), "event");
+    CK(cudaStreamSynchronize(s), "adjoint outputs");
+    float tms = 0.0f;
+    CK(cudaEventElapsedTime(&tms, ctx->e_start, ctx->e_end), "event time");
+    std::memcpy(&out->stats, hbuf, sizeof(cmpmc_sim_stats));
+    const double* hist = reinterpret_cast<const double*>(hbuf + sizeof(cmpmc_sim_stats));
+    const double* sums = hist + CMPMC_ADJ_MAX_BINS;
+    for (int b = 0; b < d->n_bins; ++b) out->hist[b] = hist[b];
+    const double nu = static_cast<double>(units);
+    auto var_of_sum = [&](int c) {  // n / (n - 1) * (sum x^2 - (sum x)^2 / n)
+        if (units < 2) return 0.0;
+        const double v = sums[kAdjCols + c] - sums[c] * sums[c] / nu;
+        return std::max(0.0, v) * nu / (nu - 1.0);
+    };
+    out->value = sums[0];
+    out->value_var = var_of_sum(0);
+    for (int k = 0; k < 4; ++k) {
+        out->grad[k] = sums[1 + k];
+        out->grad_var[k] = var_of_sum(1 + k);
+    }
+    out->n_primaries = units;
     out->kernel_ms = kms;
     out->total_ms = tms;
     out->device_error = hc.err;

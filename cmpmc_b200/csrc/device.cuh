@@ -61,6 +61,20 @@ struct RunArgs {
     unsigned* err;
 };
 
+// Adjoint of a binned hit-time histogram (batched FP32 form, k_adjoint_fp32)
+constexpr int kAdjMaxBins = 256;
+constexpr int kAdjCols = 5;  // per primary: value, d value / d theta_0..3
+struct AdjArgs {
+    int n_bins;
+    double t0, inv_dt;        // bin b covers [t0 + b / inv_dt, t0 + (b + 1) / inv_dt)
+    const float* bin_w;       // [n_bins] dLoss/dh_b
+    double* hist;             // [n_bins] weighted hit counts (accumulated)
+    double* prim;             // [units][kAdjCols]
+    float spec_score;         // d log(1 - p_d) / d log p_d = -p_d / (1 - p_d)
+    float film_miss_score;    // d log(1 - f) / d log f = -f / (1 - f)
+    double inv_theta[4];      // log-derivatives -> derivatives
+};
+
 CMPMC_HD GTrack pack_track(const Track& t) {
     GTrack g;
     g.px = t.pos.x; g.py = t.pos.y; g.pz = t.pos.z;
@@ -139,6 +153,18 @@ cudaError_t launch_batched_fp32(const Lattice& L, const float* cdf_f, const Dete
 cudaError_t batched_fp32_occupancy(int block, int* blocks_per_sm);
 cudaError_t launch_unit_event(const uint64_t* ph_off, uint64_t n_events, uint32_t* unit_event, cudaStream_t s);
 size_t batched_stack_entry_bytes();
+cudaError_t launch_adjoint_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
+                                const AdjArgs& adj, const uint32_t* unit_event, int grid, int block, cudaStream_t s);
+cudaError_t adjoint_fp32_occupancy(int block, int* blocks_per_sm);
+size_t adjoint_stack_entry_bytes();
+// fixed-order column sums and sums of squares of a row-major [rows][cols] FP64 array
+// (cols <= 8): out[c] = sum, out[cols + c] = sum of squares
+cudaError_t launch_reduce_cols(const double* x, uint64_t rows, int cols, double* partials, double* out,
+                               cudaStream_t s, int* launches);
+constexpr int kColPartials = 296;
+// fixed-order SimStats sum of n records (two levels through `partials` above 65,536 records)
+cudaError_t launch_reduce_stats(const cmpmc_sim_stats* rec, uint64_t n, cmpmc_sim_stats* partials,
+                                cmpmc_sim_stats* total, cudaStream_t s, int* launches);
 // merge of the batched form: units are primaries; event offsets / stats derive from them
 cudaError_t launch_batched_finish(const RunArgs& a, uint64_t n_events, const uint64_t* ph_off,
                                   const double* injected, uint64_t* unit_offsets, uint64_t* ev_offsets,

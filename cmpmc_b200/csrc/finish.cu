@@ -156,7 +156,58 @@ __global__ void __launch_bounds__(kReduceThreads) k_sum_injected(const double* _
     if (t == 0) total->total_injected_eV = acc[0];
 }
 
+// Column sums (and sums of squares when `squares`) of rows [b n / B, (b + 1) n / B) of a
+// row-major [n][cols] array into out[b][2 cols]: each thread a contiguous slice, then a
+// fixed tree over the threads, so the result does not depend on scheduling.
+constexpr int kMaxCols = 8;
+__global__ void __launch_bounds__(kReduceThreads) k_reduce_cols(const double* __restrict__ x_all, uint64_t n_all,
+                                                                int cols, int in_stride, bool squares,
+                                                                double* __restrict__ out_all) {
+    __shared__ double acc[kReduceThreads][2 * kMaxCols];
+    const uint64_t b0 = n_all * blockIdx.x / gridDim.x, b1 = n_all * (blockIdx.x + 1) / gridDim.x;
+    const uint64_t n = b1 - b0;
+    const int t = threadIdx.x;
+    const uint64_t chunk = (n + kReduceThreads - 1) / kReduceThreads;
+    const uint64_t lo = min(n, t * chunk), hi = min(n, lo + chunk);
+    double sum[2 * kMaxCols];
+#pragma unroll
+    for (int c = 0; c < 2 * kMaxCols; ++c) sum[c] = 0.0;
+    for (uint64_t i = lo; i < hi; ++i) {
+        const double* row = x_all + (b0 + i) * in_stride;
+#pragma unroll
+        for (int c = 0; c < kMaxCols; ++c) {
+            if (c < cols) {
+                const double v = row[c];
+                sum[c] += v;
+                sum[kMaxCols + c] += squares ? v * v : row[cols + c];
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 2 * kMaxCols; ++c) acc[t][c] = sum[c];
+    __syncthreads();
+    for (int stride = kReduceThreads / 2; stride > 0; stride >>= 1) {
+        if (t < stride)
+            for (int c = 0; c < 2 * kMaxCols; ++c) acc[t][c] += acc[t + stride][c];
+        __syncthreads();
+    }
+    if (t < cols) {
+        out_all[blockIdx.x * 2 * cols + t] = acc[0][t];
+        out_all[blockIdx.x * 2 * cols + cols + t] = acc[0][kMaxCols + t];
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_reduce_cols(const double* x, uint64_t rows, int cols, double* partials, double* out,
+                               cudaStream_t s, int* launches) {
+    if (cols < 1 || cols > kMaxCols) return cudaErrorInvalidValue;
+    // level 1: row blocks -> [kColPartials][sum, sum of squares]; level 2: one block over them
+    k_reduce_cols<<<kColPartials, kReduceThreads, 0, s>>>(x, rows, cols, cols, true, partials);
+    k_reduce_cols<<<1, kReduceThreads, 0, s>>>(partials, kColPartials, cols, 2 * cols, false, out);
+    *launches += 2;
+    return cudaGetLastError();
+}
 
 cudaError_t launch_batched_finish(const RunArgs& a, uint64_t n_events, const uint64_t* ph_off,
                                   const double* injected, uint64_t* unit_offsets, uint64_t* ev_offsets,
@@ -188,12 +239,17 @@ cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit*
         if (e != cudaSuccess) return e;
         *launches += 1;
     }
-    if (a.n_events > kReduceTwoLevel && partials) {
-        k_reduce_stats<<<kReducePartials, kReduceThreads, 0, s>>>(a.ev_stats, a.n_events, partials);
+    return launch_reduce_stats(a.ev_stats, a.n_events, partials, total, s, launches);
+}
+
+cudaError_t launch_reduce_stats(const cmpmc_sim_stats* rec, uint64_t n, cmpmc_sim_stats* partials,
+                                cmpmc_sim_stats* total, cudaStream_t s, int* launches) {
+    if (n > kReduceTwoLevel && partials) {
+        k_reduce_stats<<<kReducePartials, kReduceThreads, 0, s>>>(rec, n, partials);
         k_reduce_stats<<<1, kReduceThreads, 0, s>>>(partials, kReducePartials, total);
         *launches += 2;
     } else {
-        k_reduce_stats<<<1, kReduceThreads, 0, s>>>(a.ev_stats, a.n_events, total);
+        k_reduce_stats<<<1, kReduceThreads, 0, s>>>(rec, n, total);
         *launches += 1;
     }
     return cudaGetLastError();

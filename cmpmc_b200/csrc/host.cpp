@@ -278,7 +278,7 @@ int cmpmc_abi_sizes(size_t* out, int n) {
     const size_t sz[] = {sizeof(cmpmc_phonon_track), sizeof(cmpmc_charge_track), sizeof(cmpmc_sensor_hit),
                          sizeof(cmpmc_sim_stats),    sizeof(cmpmc_crystal_config), sizeof(cmpmc_film_config),
                          sizeof(cmpmc_surface),      sizeof(cmpmc_detector),      sizeof(cmpmc_run_desc),
-                         sizeof(cmpmc_run_out)};
+                         sizeof(cmpmc_run_out),      sizeof(cmpmc_adjoint_desc), sizeof(cmpmc_adjoint_out)};
     for (int i = 0; i < n && i < static_cast<int>(sizeof(sz) / sizeof(sz[0])); ++i) out[i] = sz[i];
     return CMPMC_GPU_ABI_VERSION;
 }

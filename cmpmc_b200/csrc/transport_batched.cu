@@ -20,6 +20,8 @@
 // is the Kaplan film cascade (so the ledger closes to rounding). A reflected track is
 // moved 10 nm inward (the reference moves it 1e-11 m, below FP32 resolution at the wall).
 #define CMPMC_DEVICE_FAST_MATH 1
+#include <type_traits>
+
 #include "device.cuh"
 
 namespace cmpmc_gpu {
@@ -159,11 +161,36 @@ struct FTrack {
     int mode;
 };
 
+// A track of the adjoint kernel also carries its score: the derivative of the log density
+// of every random decision of its lineage so far with respect to log theta_k (k = isotope
+// coefficient, anharmonic coefficient, diffuse fraction, film absorption).
+struct FTrackA : FTrack {
+    float s[4];
+};
+
+template <bool kAdj>
+using TrackOf = typename std::conditional<kAdj, FTrackA, FTrack>::type;
+
 struct alignas(16) GFTrack {
     float px, py, pz, kx, ky, kz, vx, vy, vz, vmag, w;
     uint32_t bounces_mode;  // bounces << 2 | mode
     double E, t;
 };
+struct alignas(16) GFTrackA {
+    GFTrack g;
+    float4 s;
+};
+template <bool kAdj>
+using EntryOf = typename std::conditional<kAdj, GFTrackA, GFTrack>::type;
+
+// a daughter starts with its parent's score (the decisions that made it)
+template <bool kAdj>
+__device__ __forceinline__ void inherit(TrackOf<kAdj>& d, const TrackOf<kAdj>& parent) {
+    if constexpr (kAdj) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) d.s[i] = parent.s[i];
+    }
+}
 
 // inward Lambertian wavevector whose group velocity points inward (engine.hpp:927-936)
 __device__ __forceinline__ F3 finward(const FLat& L, int mode, F3 n, R128& g, FKin& kin) {
@@ -220,7 +247,9 @@ __device__ __forceinline__ FBHit fexit(float R, float H, F3 p, F3 v) {
     return h;
 }
 
-__device__ __forceinline__ void push_track(GFTrack* stk, uint32_t& n, uint32_t cap, unsigned& err, const FTrack& t) {
+template <bool kAdj>
+__device__ __forceinline__ void push_track(EntryOf<kAdj>* stk, uint32_t& n, uint32_t cap, unsigned& err,
+                                           const TrackOf<kAdj>& t) {
     if (n >= cap) {
         err |= kErrPhononStack;
         return;
@@ -234,10 +263,26 @@ __device__ __forceinline__ void push_track(GFTrack* stk, uint32_t& n, uint32_t c
     g.bounces_mode = (t.bounces << 2) | static_cast<uint32_t>(t.mode);
     g.E = t.E;
     g.t = t.t;
-    stk[n++] = g;
+    if constexpr (kAdj) {
+        GFTrackA e;
+        e.g = g;
+        e.s = make_float4(t.s[0], t.s[1], t.s[2], t.s[3]);
+        stk[n++] = e;
+    } else {
+        stk[n++] = g;
+    }
 }
-__device__ __forceinline__ void pop_track(const GFTrack* stk, uint32_t& n, FTrack& t) {
-    const GFTrack g = stk[--n];
+template <bool kAdj>
+__device__ __forceinline__ void pop_track(const EntryOf<kAdj>* stk, uint32_t& n, TrackOf<kAdj>& t) {
+    --n;
+    GFTrack g;
+    if constexpr (kAdj) {
+        const GFTrackA e = stk[n];
+        g = e.g;
+        t.s[0] = e.s.x; t.s[1] = e.s.y; t.s[2] = e.s.z; t.s[3] = e.s.w;
+    } else {
+        g = stk[n];
+    }
     t.pos = f3(g.px, g.py, g.pz);
     t.k = f3(g.kx, g.ky, g.kz);
     t.vg = f3(g.vx, g.vy, g.vz);
@@ -265,10 +310,11 @@ __device__ __noinline__ double kaplan_call(const Film* f, double E, double* refl
 }
 
 // anharmonic decay of an L phonon (engine.hpp:938-988), FP32 angles
-__device__ __noinline__ void decay_call(const FLat* Lp, FTrack* tp, GFTrack* stk, uint32_t* n_stk, uint32_t cap,
-                                        unsigned* err, UStats* st, R128* gp) {
+template <bool kAdj>
+__device__ __noinline__ void decay_call(const FLat* Lp, TrackOf<kAdj>* tp, EntryOf<kAdj>* stk, uint32_t* n_stk,
+                                        uint32_t cap, unsigned* err, UStats* st, R128* gp) {
     const FLat& L = *Lp;
-    FTrack& trk = *tp;
+    TrackOf<kAdj>& trk = *tp;
     R128& g = *gp;
     const F3 d1 = trk.k;
     const F3 perp = forth(d1);
@@ -299,7 +345,7 @@ __device__ __noinline__ void decay_call(const FLat* Lp, FTrack* tp, GFTrack* stk
     const F3 k1 = funit(frotate(frotate(d1, perp, c1, s1), d1, cp, sp));
     const F3 k2 = funit(frotate(frotate(d1, perp, c2, s2), d1, cp, sp));
     const double xd = static_cast<double>(x);
-    FTrack d;
+    TrackOf<kAdj> d;
     d.pos = trk.pos;
     d.k = k2;
     const FKin kin2 = fmap(L, m2, k2);
@@ -310,7 +356,8 @@ __device__ __noinline__ void decay_call(const FLat* Lp, FTrack* tp, GFTrack* stk
     d.w = trk.w;
     d.bounces = 0;
     d.mode = m2;
-    push_track(stk, *n_stk, cap, *err, d);
+    inherit<kAdj>(d, trk);
+    push_track<kAdj>(stk, *n_stk, cap, *err, d);
     trk.E = xd * trk.E;
     trk.mode = m1;
     trk.k = k1;
@@ -348,21 +395,24 @@ __device__ __forceinline__ void write_unit(const RunArgs& a, uint64_t unit, cons
     a.ev_nhits[unit] = a.keep_hits ? n_hits : 0;
 }
 
-__global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__ FLat L,
-                                                         const __grid_constant__ Detector D,
-                                                         const __grid_constant__ RunArgs a,
-                                                         const uint32_t* __restrict__ unit_event) {
+// The step loop of both batched kernels. kAdj adds the score bookkeeping of the adjoint
+// (every decision's d log p / d log theta, carried per track and inherited by daughters)
+// and bins hits into the time histogram instead of writing hit records.
+template <bool kAdj>
+__device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, const RunArgs& a,
+                                             const uint32_t* __restrict__ unit_event, const AdjArgs& adj,
+                                             float* s_w, float* s_hist) {
     const uint64_t slot = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     double refl_buf[kKaplanCap];
     double kwork[4 * kKaplanCap];
-    GFTrack* stk = reinterpret_cast<GFTrack*>(a.stack) + slot * a.stack_cap;
+    EntryOf<kAdj>* stk = reinterpret_cast<EntryOf<kAdj>*>(a.stack) + slot * a.stack_cap;
     uint32_t n_stk = 0;
     unsigned err = 0;
     const float R = static_cast<float>(D.radius), H = static_cast<float>(D.half_z);
     const double min_E = D.min_phonon_eV;
     const uint64_t seed_key = mix64(a.seed ^ 0x5851f42d4c957f2dULL);
 
-    FTrack trk;
+    TrackOf<kAdj> trk;
     R128 g;
     UStats st;
     uint32_t n_hits = 0;
@@ -371,7 +421,7 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
     for (;;) {
         if (!live) {
             if (n_stk > 0) {
-                pop_track(stk, n_stk, trk);
+                pop_track<kAdj>(stk, n_stk, trk);
                 live = true;
             } else {
                 if (unit != ~0ull) write_unit(a, unit, st, n_hits);
@@ -393,6 +443,12 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
                 trk.w = static_cast<float>(in.weight);
                 trk.bounces = in.bounces;
                 trk.mode = in.mode;
+                if constexpr (kAdj) {
+                    trk.s[0] = trk.s[1] = trk.s[2] = trk.s[3] = 0.0f;
+                    double* row = adj.prim + unit * kAdjCols;
+#pragma unroll
+                    for (int c = 0; c < kAdjCols; ++c) row[c] = 0.0;
+                }
                 st = UStats{0, 0, 0, 0, 0, 0, 0, 0, 0, 0.0, 0.0};
                 n_hits = 0;
                 live = true;
@@ -426,23 +482,38 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
         const float d = bulk ? d_phys : bh.d;
         trk.pos = trk.pos + trk.vg * d;
         trk.t += static_cast<double>(d / trk.vmag);
+        if constexpr (kAdj) {
+            // free flight: survival exp(-r t) of each theta-dependent channel over the segment
+            const float seg = d / trk.vmag;
+            trk.s[0] -= r_iso * seg;
+            trk.s[1] -= r_down * seg;
+        }
         // 0: new isotropic direction (bulk scatter), 1: Lambertian about bh.n, 2: nothing more
         int sample = 2;
         if (bulk) {
             const float u_proc = g.u() * r_tot;
             if (r_down > 0.0f && u_proc < r_down) {
-                decay_call(&L, &trk, stk, &n_stk, a.stack_cap, &err, &st, &g);
+                if constexpr (kAdj) trk.s[1] += 1.0f;  // density of a decay: r_down exp(-r_tot t)
+                decay_call<kAdj>(&L, &trk, stk, &n_stk, a.stack_cap, &err, &st, &g);
             } else {
-                if (u_proc < r_down + r_iso) st.iso++;
-                else st.poly++;
+                if (u_proc < r_down + r_iso) {
+                    st.iso++;
+                    if constexpr (kAdj) trk.s[0] += 1.0f;
+                } else {
+                    st.poly++;
+                }
                 trk.mode = fdos(L, g.u());
                 sample = 0;
             }
         } else {
             trk.bounces++;
             const Surface& s = D.surf[bh.surf];
-            if (s.has_film && g.u() < static_cast<float>(s.prob_abs) &&
-                g.u() < static_cast<float>(s.film.film_absorption)) {
+            bool enter = false;
+            if (s.has_film && g.u() < static_cast<float>(s.prob_abs)) {
+                enter = g.u() < static_cast<float>(s.film.film_absorption);
+                if constexpr (kAdj) trk.s[3] += enter ? 1.0f : adj.film_miss_score;
+            }
+            if (enter) {
                 int n_refl = 0;
                 const double edep = kaplan_call(&s.film, trk.E, refl_buf, &n_refl, kwork, &g);
                 if (edep > 0.0) {
@@ -450,7 +521,20 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
                     st.hits++;
                     st.dep += wedep;
                     const uint32_t local = n_hits++;
-                    if (a.keep_hits) {
+                    if constexpr (kAdj) {
+                        const double tb = (trk.t - adj.t0) * adj.inv_dt;
+                        if (tb >= 0.0 && tb < static_cast<double>(adj.n_bins)) {
+                            const int b = static_cast<int>(tb);
+                            atomicAdd(s_hist + b, trk.w);
+                            const double gw = static_cast<double>(s_w[b]) * trk.w;
+                            if (gw != 0.0) {
+                                double* row = adj.prim + unit * kAdjCols;
+                                row[0] += gw;
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) row[1 + c] += gw * trk.s[c] * adj.inv_theta[c];
+                            }
+                        }
+                    } else if (a.keep_hits) {
                         const unsigned long long idx = atomicAdd(a.hit_count, 1ull);
                         if (idx < a.hit_cap) {
                             cmpmc_sensor_hit r;
@@ -477,7 +561,7 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
                 }
                 const F3 re = trk.pos + bh.n * kNudge;
                 for (int i = 1; i < n_refl; ++i) {
-                    FTrack dtr;
+                    TrackOf<kAdj> dtr;
                     dtr.mode = fdos(L, g.u());
                     FKin kin;
                     dtr.k = finward(L, dtr.mode, bh.n, g, kin);
@@ -488,7 +572,8 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
                     dtr.t = trk.t;
                     dtr.w = trk.w;
                     dtr.bounces = 0;
-                    push_track(stk, n_stk, a.stack_cap, err, dtr);
+                    inherit<kAdj>(dtr, trk);
+                    push_track<kAdj>(stk, n_stk, a.stack_cap, err, dtr);
                 }
                 trk.pos = re;
                 trk.E = refl_buf[0];
@@ -518,7 +603,7 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
                     const float x = tt ? fcdf(L.cdf_tt, g) : fcdf(L.cdf_lt, g);
                     const int m1 = tt ? ftrans(L, g) : 0;
                     const int m2 = ftrans(L, g);
-                    FTrack dtr;
+                    TrackOf<kAdj> dtr;
                     FKin k2kin;
                     dtr.k = finward(L, m2, bh.n, g, k2kin);
                     dtr.pos = trk.pos;
@@ -529,11 +614,13 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
                     dtr.w = trk.w;
                     dtr.bounces = 0;
                     dtr.mode = m2;
-                    push_track(stk, n_stk, a.stack_cap, err, dtr);
+                    inherit<kAdj>(dtr, trk);
+                    push_track<kAdj>(stk, n_stk, a.stack_cap, err, dtr);
                     trk.E = static_cast<double>(x) * trk.E;
                     trk.mode = m1;
                     sample = 1;
                 } else if (u_refl < p_anh_spec) {
+                    if constexpr (kAdj) trk.s[2] += adj.spec_score;  // d log(1 - p_d) / d log p_d
                     F3 kr = trk.k - bh.n * (2.0f * fdot(trk.k, bh.n));
                     FKin kin = fmap(L, trk.mode, kr);
                     if (fdot(kin.dir, bh.n) <= 1e-6f) kr = finward(L, trk.mode, bh.n, g, kin);
@@ -541,6 +628,7 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
                     trk.vg = kin.dir;
                     trk.vmag = kin.mag;
                 } else {
+                    if constexpr (kAdj) trk.s[2] += 1.0f;  // d log p_d / d log p_d
                     sample = 1;
                 }
             }
@@ -577,6 +665,35 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
         }
     }
     if (err) atomicOr(a.err, err);
+}
+
+__global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__ FLat L,
+                                                         const __grid_constant__ Detector D,
+                                                         const __grid_constant__ RunArgs a,
+                                                         const uint32_t* __restrict__ unit_event) {
+    const AdjArgs none{};
+    batched_loop<false>(L, D, a, unit_event, none, nullptr, nullptr);
+}
+
+// Adjoint of the hit-time histogram: the batched transport with per-track scores. Bin
+// weights (dLoss/dh_b) and the block's histogram live in shared memory; the histogram is
+// added to the global FP64 bins once per block.
+__global__ void __launch_bounds__(128, 6) k_adjoint_fp32(const __grid_constant__ FLat L,
+                                                         const __grid_constant__ Detector D,
+                                                         const __grid_constant__ RunArgs a,
+                                                         const __grid_constant__ AdjArgs adj,
+                                                         const uint32_t* __restrict__ unit_event) {
+    __shared__ float s_w[kAdjMaxBins];
+    __shared__ float s_hist[kAdjMaxBins];
+    for (int b = threadIdx.x; b < kAdjMaxBins; b += blockDim.x) {
+        s_w[b] = (b < adj.n_bins) ? adj.bin_w[b] : 0.0f;
+        s_hist[b] = 0.0f;
+    }
+    __syncthreads();
+    batched_loop<true>(L, D, a, unit_event, adj, s_w, s_hist);
+    __syncthreads();
+    for (int b = threadIdx.x; b < adj.n_bins; b += blockDim.x)
+        if (s_hist[b] != 0.0f) atomicAdd(adj.hist + b, static_cast<double>(s_hist[b]));
 }
 
 }  // namespace
@@ -628,5 +745,17 @@ cudaError_t batched_fp32_occupancy(int block, int* blocks_per_sm) {
 }
 
 size_t batched_stack_entry_bytes() { return sizeof(GFTrack); }
+
+cudaError_t launch_adjoint_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
+                                const AdjArgs& adj, const uint32_t* unit_event, int grid, int block, cudaStream_t s) {
+    k_adjoint_fp32<<<grid, block, 0, s>>>(make_flat(L, cdf_f, D), D, a, adj, unit_event);
+    return cudaGetLastError();
+}
+
+cudaError_t adjoint_fp32_occupancy(int block, int* blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_adjoint_fp32, block, 0);
+}
+
+size_t adjoint_stack_entry_bytes() { return sizeof(GFTrackA); }
 
 }  // namespace cmpmc_gpu

@@ -310,6 +310,56 @@ int cmpmc_gpu_run_events_noalloc(const cmpmc_lattice* lat, const cmpmc_detector*
                                  cmpmc_sensor_hit* hits, uint64_t hit_capacity, void* stream,
                                  cmpmc_sim_stats* total, uint64_t* n_hits);
 
+/* ---- adjoint of the sensor-arrival histogram ---------------------------------------------
+ * No function of the reference computes it; the forward quantity is the reference's own
+ * transport (engine.hpp:403-582) observed through a binned histogram of SensorHit::time.
+ * Parameters theta (absolute values):
+ *   theta[0] isotope coefficient B_iso (CrystalConfig::B_iso, s^3)
+ *   theta[1] anharmonic coefficient A_anh (CrystalConfig::A_anh, s^4)
+ *   theta[2] diffuse fraction p_d of every surface: reflection_split gives p_spec = 1 - p_d,
+ *            p_diff = p_d, p_anh = 0 at every frequency (spec_coeffs {1-p_d}, diff_coeffs {p_d},
+ *            anh_coeffs {}, spec_prob_const 1-p_d in the reference's SurfaceProperty)
+ *   theta[3] film absorption (SuperconductorFilmConfig::film_absorption of every film)
+ * The transport is the batched FP32 form (each primary its own substream of `seed`); the
+ * call returns the weighted hit counts per time bin h_b(theta) and, given bin weights
+ * w_b = dLoss/dh_b, value = sum_b w_b h_b and its gradient d value / d theta estimated by
+ * the score function: every theta-dependent random decision (the exponential free flights
+ * with their isotope and anharmonic channels, the specular/diffuse choice, film entry)
+ * adds d log p / d theta to the score of its track, daughters inherit their parent's score,
+ * and every binned hit adds w_b * score. Tracks are recomputed from their RNG substreams
+ * (nothing is stored between the forward and the backward call). */
+#define CMPMC_ADJ_MAX_BINS 256
+typedef struct cmpmc_adjoint_desc {
+    uint64_t n_events;
+    uint64_t first_event;
+    uint64_t seed;
+    const uint64_t* phonon_offsets;     /* [n_events + 1]                                    */
+    const cmpmc_phonon_track* phonons;  /* initial phonons                                   */
+    int inputs_on_device;
+    int n_bins;                         /* 1 .. CMPMC_ADJ_MAX_BINS                            */
+    double t_min, t_max;                /* histogram range of hit times (s)                  */
+    double theta[4];
+    const double* bin_weight;           /* host [n_bins]; NULL: histogram only               */
+    double* per_primary;                /* optional [n_primaries][5]: value and d value /
+                                           d theta_k of each primary's lineage               */
+    int per_primary_on_device;          /* per_primary is device memory                      */
+} cmpmc_adjoint_desc;
+
+typedef struct cmpmc_adjoint_out {
+    double hist[CMPMC_ADJ_MAX_BINS];    /* weighted hit counts per bin (FP64 sums)           */
+    double value;                       /* sum_b bin_weight_b hist_b                          */
+    double grad[4];                     /* d value / d theta_k                               */
+    double value_var;                   /* variance estimates of value and grad from the      */
+    double grad_var[4];                 /* spread over primaries (independent substreams)   */
+    cmpmc_sim_stats stats;              /* summed over all primaries (no hit records kept)   */
+    uint64_t n_primaries;
+    double kernel_ms, total_ms;
+    uint32_t device_error;
+    uint32_t kernel_launches;
+} cmpmc_adjoint_out;
+
+int cmpmc_gpu_adjoint(cmpmc_gpu_ctx* ctx, const cmpmc_adjoint_desc* desc, cmpmc_adjoint_out* out);
+
 /* Correctly rounded log / sin / cos of the device transport (crmath), evaluated on the
  * host; the device computes bit-identical values. */
 double cmpmc_cr_log(double x);
@@ -321,7 +371,8 @@ int cmpmc_gpu_math_check(int device, uint64_t n, const double* x, double* out);
 
 /* Layout self-check for bindings: writes sizeof of the ABI structs in the order
  * phonon_track, charge_track, sensor_hit, sim_stats, crystal_config, film_config,
- * surface, detector, run_desc, run_out (at most n values). Returns the ABI version. */
+ * surface, detector, run_desc, run_out, adjoint_desc, adjoint_out (at most n values).
+ * Returns the ABI version. */
 int cmpmc_abi_sizes(size_t* out, int n);
 
 #ifdef __cplusplus

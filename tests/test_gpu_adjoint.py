@@ -1,0 +1,149 @@
+"""Adjoint of the sensor-arrival histogram on the device (cmpmc_gpu_adjoint).
+
+Workload: 1,000,000 L phonons of 7.5 meV, one per event, origins uniform in the Ge cylinder,
+isotropic, seed 17. Loss = sum_b (h_b(theta) - h_b(1.1 theta0))^2 with h the hit-time
+histogram (64 bins over [0, 1 ms]); theta = (B_iso, A_anh, p_d, f_abs) around
+theta0 = (3.67e-41, 6.43e-55, 0.9, 0.2).
+
+Bars: the device gradient is within 3 sigma of (a) central finite differences with common
+random numbers (relative step 1e-3) on the device, sigma from the per-primary spread of
+both estimates, and (b) the same estimator and finite differences run on the reference's
+CPU transport (tests/golden/adjoint_c4.npz). The torch.autograd.Function wrapper lives
+here in the test harness only.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import golden
+
+pytestmark = pytest.mark.gpu
+
+N_FULL = 1_000_000
+SEED = 17
+FD_STEP = 1e-3
+Z_MAX = 3.0
+
+
+@pytest.fixture(scope="module")
+def setup(ge_lattice):
+    import cmpmc_b200 as cm
+    eng = cm.SimulationEngine(ge_lattice, cm.DetectorModel())
+    packed = eng.generate(cm.workloads.single_l_volume, N_FULL, SEED)
+    adj = cm.HistogramAdjoint(eng, packed, SEED, n_bins=64, t_range=(0.0, 1e-3))
+    theta0 = cm.default_theta(eng, diffuse_fraction=0.9)
+    return eng, packed, adj, theta0
+
+
+def _small(setup, n):
+    import cmpmc_b200 as cm
+    eng, _, _, theta0 = setup
+    packed = eng.generate(cm.workloads.single_l_volume, n, SEED)
+    return cm.HistogramAdjoint(eng, packed, SEED, n_bins=64, t_range=(0.0, 1e-3)), theta0
+
+
+def test_histogram_equals_binned_batched_run(setup):
+    """At p_d = 1 the theta surfaces equal the default ones: the adjoint kernel's histogram
+    must equal the binned hits of the batched form on the same substreams."""
+    import cmpmc_b200 as cm
+    eng, _, _, theta0 = setup
+    adj, _ = _small(setup, 50_000)
+    th = theta0.copy()
+    th[2] = 1.0
+    res = adj.run(th)
+    run = eng.run_packed(adj.packed, cm.RunOptions(seed=SEED, form="batched_fp32"))
+    t = run.hits["time"]
+    want = np.histogram(t[(t >= 0) & (t < 1e-3)], bins=64, range=(0.0, 1e-3))[0].astype(np.float64)
+    assert res.stats.total_steps == run.stats.total_steps
+    assert res.stats.sensor_hits == run.stats.sensor_hits
+    assert np.array_equal(res.hist, want), np.abs(res.hist - want).max()
+
+
+def test_adjoint_deterministic(setup):
+    adj, theta0 = _small(setup, 100_000)
+    w = np.linspace(-1.0, 1.0, 64)
+    a = adj.run(theta0, w)
+    b = adj.run(theta0, w)
+    assert np.array_equal(a.hist, b.hist)
+    assert a.value == b.value and np.array_equal(a.grad, b.grad)
+
+
+def test_adjoint_matches_finite_differences(setup):
+    _, _, adj, theta0 = setup
+    h0 = adj.histogram(theta0)
+    ht = adj.histogram(theta0 * 1.1)
+    w = 2.0 * (h0 - ht)
+    res = adj.run(theta0, w, per_primary=True)
+    assert np.array_equal(res.hist, h0)
+    n = res.n_primaries
+    assert n == N_FULL
+    # the per-primary rows sum to the reduced totals
+    np.testing.assert_allclose(res.per_primary.sum(axis=0), np.r_[res.value, res.grad], rtol=1e-9)
+    loss0 = np.sum((h0 - ht) ** 2)
+    for k in range(4):
+        tp, tm = theta0.copy(), theta0.copy()
+        tp[k] *= 1.0 + FD_STEP
+        tm[k] *= 1.0 - FD_STEP
+        rp = adj.run(tp, w, per_primary=True)
+        rm = adj.run(tm, w, per_primary=True)
+        c = (rp.per_primary[:, 0] - rm.per_primary[:, 0]) / (2.0 * FD_STEP * theta0[k])
+        fd = c.sum()
+        se_fd = c.std(ddof=1) * np.sqrt(n)
+        se_adj = np.sqrt(res.grad_var[k])
+        z = (res.grad[k] - fd) / np.hypot(se_adj, se_fd)
+        # the full loss difference (not linearised around theta0)
+        fd_loss = (np.sum((rp.hist - ht) ** 2) - np.sum((rm.hist - ht) ** 2)) / (2.0 * FD_STEP * theta0[k])
+        print(f"theta_{k}: adjoint {res.grad[k]:.5g} +- {se_adj:.3g}  FD {fd:.5g} +- {se_fd:.3g}  "
+              f"FD(loss) {fd_loss:.5g}  z {z:.2f}  loss {loss0:.4g}")
+        assert abs(z) < Z_MAX, (k, z)
+
+
+def test_adjoint_matches_reference_cpu(setup):
+    """Per-primary means against the score-function estimator run on the reference's
+    transport (restated loop pinned bit-exact to it) and against finite differences on the
+    unmodified reference, both from the fixture."""
+    ref = dict(golden("adjoint_c4.npz"))
+    _, _, adj, theta0 = setup
+    assert int(ref["check_mismatched"]) == 0
+    np.testing.assert_array_equal(ref["theta0"], theta0)
+    res = adj.run(theta0, ref["w"])
+    n = res.n_primaries
+    mean = np.r_[res.value, res.grad] / n
+    se = np.sqrt(np.r_[res.value_var, res.grad_var]) / n
+    for c in range(5):
+        z = (mean[c] - ref["est_mean"][c]) / np.hypot(se[c], ref["est_se"][c])
+        print(f"col {c}: device {mean[c]:.5g} +- {se[c]:.3g}   reference estimator "
+              f"{ref['est_mean'][c]:.5g} +- {ref['est_se'][c]:.3g}  z {z:.2f}")
+        assert abs(z) < Z_MAX, (c, z)
+    for k in range(4):
+        z = (mean[1 + k] - ref["fd_mean"][k]) / np.hypot(se[1 + k], ref["fd_se"][k])
+        print(f"theta_{k}: device {mean[1 + k]:.5g}   reference FD {ref['fd_mean'][k]:.5g} +- "
+              f"{ref['fd_se'][k]:.3g}  z {z:.2f}")
+        assert abs(z) < Z_MAX, (k, z)
+    # hits in the window per primary: FP32 device vs FP64 reference within 1 %
+    per_dev = res.hist.sum() / n
+    per_ref = ref["hist0"].sum() / float(ref["n"])
+    assert abs(per_dev / per_ref - 1.0) < 0.01, (per_dev, per_ref)
+
+
+def test_autograd_function_wrapper(setup):
+    torch = pytest.importorskip("torch")
+    adj, theta0 = _small(setup, 100_000)
+
+    class HistogramFn(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, theta):
+            ctx.theta = theta.detach().numpy().copy()
+            return torch.from_numpy(adj.histogram(ctx.theta))
+
+        @staticmethod
+        def backward(ctx, grad_h):
+            res = adj.run(ctx.theta, grad_h.detach().numpy())
+            return torch.from_numpy(res.grad)
+
+    target = torch.from_numpy(adj.histogram(theta0 * 1.1))
+    theta = torch.tensor(theta0, dtype=torch.float64, requires_grad=True)
+    loss = ((HistogramFn.apply(theta) - target) ** 2).sum()
+    loss.backward()
+    want_loss, want_grad, _ = adj.loss_and_grad(theta0, target.numpy())
+    assert float(loss) == want_loss
+    np.testing.assert_array_equal(theta.grad.numpy(), want_grad)
