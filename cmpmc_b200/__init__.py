@@ -7,13 +7,14 @@ the C ABI in include/cmpmc_gpu.h.
 from .api import (AluminumFilm, CmpmcError, CrystalConfig, CrystalLattice, CylinderSolid, DetectorModel,
                   EventInput, ExcitationType, KaplanFilm, PackedEvents, PhononMode, Rng, RunOptions, RunResult,
                   SimStats, SimulationEngine, SuperconductorFilmConfig, SurfaceId, SurfaceProperty,
-                  UniformElectricField, UnvalidatedModuleError, Workload, materials, run_events, units, workloads)
+                  TriLinearMesh3D, UniformElectricField, UnvalidatedModuleError, Workload, materials, run_events, units, workloads)
 from .adjoint import AdjointResult, HistogramAdjoint, THETA_NAMES, default_theta
 
 __all__ = [
     "AdjointResult", "AluminumFilm", "CmpmcError", "CrystalConfig", "CrystalLattice", "CylinderSolid", "DetectorModel", "EventInput",
     "ExcitationType", "KaplanFilm", "PackedEvents", "PhononMode", "Rng", "RunOptions", "RunResult", "SimStats",
-    "SimulationEngine", "SuperconductorFilmConfig", "SurfaceId", "SurfaceProperty", "UniformElectricField",
+    "SimulationEngine", "SuperconductorFilmConfig", "SurfaceId", "SurfaceProperty", "TriLinearMesh3D",
+    "UniformElectricField",
     "UnvalidatedModuleError", "Workload", "materials", "run_events", "units", "workloads", "HistogramAdjoint",
     "THETA_NAMES", "default_theta",
 ]

@@ -19,6 +19,7 @@ ABI_VERSION = 1
 OK, ERR_INVALID, ERR_CUDA, ERR_UNVALIDATED, ERR_CAPACITY, ERR_DEVICE, ERR_NO_DEVICE = range(7)
 FORM_PLAIN_FP64, FORM_BATCHED_FP32 = 0, 1
 WL_SINGLE_L_ORIGIN, WL_MIXED_ENERGY, WL_PAIR_DRIFT, WL_SINGLE_L_VOLUME, WL_TEST_PARALLEL = 0, 1, 2, 4, 5
+WL_RECOIL, WL_RECOIL_LIGHT = 3, 6
 
 MAX_VALLEYS, MAX_IV, MAX_POLY = 8, 4, 8
 
@@ -70,7 +71,7 @@ class CrystalConfigC(C.Structure):
         ("iv_lin_rate0", _f64), ("iv_lin_rate1", _f64), ("iv_lin_power", _f64),
         ("e_trapping_mfp_m", _f64), ("h_trapping_mfp_m", _f64), ("e_trap_ion_d0_mfp_m", _f64),
         ("e_trap_ion_a_mfp_m", _f64), ("h_trap_ion_d_mfp_m", _f64), ("h_trap_ion_a0_mfp_m", _f64),
-        ("orient", (_f64 * 3) * 3),
+        ("orient", (_f64 * 3) * 3), ("atomic_Z", _f64), ("atomic_A", _f64),
     ]
 
 
@@ -142,6 +143,9 @@ class AdjointOutC(C.Structure):
     ]
 
 
+# double (*)(const double p[3], void* user): node potential of cmpmc_mesh_build_cartesian
+POTENTIAL_FN = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p)
+
 _SIG = {
     "cmpmc_abi_sizes": (_i32, [C.POINTER(C.c_size_t), _i32]),
     "cmpmc_crystal_config_germanium": (None, [C.POINTER(CrystalConfigC)]),
@@ -172,6 +176,17 @@ _SIG = {
     "cmpmc_cr_sin": (_f64, [_f64]),
     "cmpmc_cr_cos": (_f64, [_f64]),
     "cmpmc_gpu_math_check": (_i32, [_i32, _u64, C.c_void_p, C.c_void_p]),
+    "cmpmc_mesh_create": (_i32, [C.c_void_p, C.c_void_p, _u64, C.c_void_p, _u64, _f64, _f64,
+                                 C.POINTER(C.c_void_p)]),
+    "cmpmc_mesh_build_cartesian": (_i32, [_f64, _f64, _f64, _i32, _i32, _i32, C.c_void_p, C.c_void_p,
+                                          C.POINTER(C.c_void_p)]),
+    "cmpmc_recoil_potential": (_f64, [C.POINTER(_f64), C.c_void_p]),
+    "cmpmc_recoil_mesh": (_i32, [C.POINTER(DetectorC), C.POINTER(C.c_void_p)]),
+    "cmpmc_mesh_destroy": (None, [C.c_void_p]),
+    "cmpmc_mesh_info": (_i32, [C.c_void_p, C.POINTER(_u64), C.POINTER(_u64)]),
+    "cmpmc_mesh_field_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
+    "cmpmc_mesh_potential_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
+    "cmpmc_gpu_set_mesh": (_i32, [C.c_void_p, C.c_void_p]),
     "cmpmc_gpu_run_events_noalloc": (_i32, [C.c_void_p, C.POINTER(DetectorC), _i32, _u64, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _u64,
                                             C.c_void_p, C.POINTER(SimStatsC), C.POINTER(_u64)]),

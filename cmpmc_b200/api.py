@@ -233,6 +233,8 @@ class CrystalConfig:
     h_trap_ion_d_mfp_m: float = 0.0
     h_trap_ion_a0_mfp_m: float = 0.0
     orient: tuple = ((1.0, 0.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0))
+    atomic_Z: float = 32.0
+    atomic_A: float = 72.63
 
     def to_c(self) -> _ffi.CrystalConfigC:
         c = _ffi.CrystalConfigC()
@@ -395,11 +397,98 @@ def _default_surfaces():
             SurfaceProperty.diffuse_bare_surface()]
 
 
+class TriLinearMesh3D:
+    """TriLinearMesh3D (geometry/mesh_field.hpp:40-345): a tetrahedral mesh of node
+    potentials whose field is constant inside each tetrahedron. Built on the host by the
+    native library (face neighbours, inverse edge matrices and fields with the reference's
+    arithmetic); attached to a DetectorModel as mesh_field_3d it is copied to the device and
+    walked there by every charge step."""
+
+    def __init__(self, vertices=None, potentials=None, tetrahedra=None, V_min_clamp: float = -1e30,
+                 V_max_clamp: float = 1e30, _handle=None):
+        self._lib = _ffi.load()
+        self._hint = C.c_int32(0)
+        if _handle is not None:
+            self._h = _handle
+            return
+        x = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+        v = np.ascontiguousarray(potentials, dtype=np.float64).reshape(-1)
+        t = np.ascontiguousarray(tetrahedra, dtype=np.int32).reshape(-1, 4)
+        if len(v) != len(x):
+            raise ValueError("one potential per vertex")
+        h = C.c_void_p()
+        _check(self._lib.cmpmc_mesh_create(x.ctypes.data, v.ctypes.data, len(x), t.ctypes.data, len(t),
+                                           float(V_min_clamp), float(V_max_clamp), C.byref(h)), what="mesh")
+        self._h = h
+
+    @staticmethod
+    def build_cartesian_grid(half_x: float, half_y: float, half_z: float, nx: int, ny: int, nz: int,
+                             potential_fn: Callable) -> "TriLinearMesh3D":
+        """Kuhn-triangulated box, 6 tetrahedra per cell (mesh_field.hpp:131-189);
+        potential_fn((x, y, z)) gives the node potential in volts."""
+        lib = _ffi.load()
+        cb = _ffi.POTENTIAL_FN(lambda p, _u: float(potential_fn((p[0], p[1], p[2]))))
+        h = C.c_void_p()
+        _check(lib.cmpmc_mesh_build_cartesian(half_x, half_y, half_z, nx, ny, nz, cb, None, C.byref(h)),
+               what="mesh")
+        return TriLinearMesh3D(_handle=h)
+
+    @staticmethod
+    def recoil_mesh(detector: "DetectorModel") -> "TriLinearMesh3D":
+        """The recoil workloads' mesh: build_cartesian_grid(R, R, h, 58, 58, 57) with
+        V = 4 V (z + h) / 2h + 0.2 V (r / R)^2 sin(pi z / 2h), built natively."""
+        lib = _ffi.load()
+        cdet = detector.to_c()
+        h = C.c_void_p()
+        _check(lib.cmpmc_recoil_mesh(C.byref(cdet), C.byref(h)), what="mesh")
+        return TriLinearMesh3D(_handle=h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.cmpmc_mesh_destroy(h)
+            self._h = None
+
+    def _info(self):
+        nv, nt = C.c_uint64(), C.c_uint64()
+        _check(self._lib.cmpmc_mesh_info(self._h, C.byref(nv), C.byref(nt)))
+        return nv.value, nt.value
+
+    def num_vertices(self) -> int:
+        return self._info()[0]
+
+    def num_tetrahedra(self) -> int:
+        return self._info()[1]
+
+    def empty(self) -> bool:
+        return self.num_tetrahedra() == 0
+
+    def field_at(self, p, tet_hint: Optional[C.c_int32] = None):
+        """E(p) in V/m from the containing tetrahedron (zero outside); the walk starts from
+        and updates tet_hint (a ctypes int32), or the mesh's own hint (as at())."""
+        hint = self._hint if tet_hint is None else tet_hint
+        q = (C.c_double * 3)(*p)
+        e = (C.c_double * 3)()
+        _check(self._lib.cmpmc_mesh_field_at(self._h, q, C.byref(hint), e))
+        return (e[0], e[1], e[2])
+
+    def potential_at(self, p, tet_hint: Optional[C.c_int32] = None) -> float:
+        hint = self._hint if tet_hint is None else tet_hint
+        q = (C.c_double * 3)(*p)
+        v = C.c_double()
+        _check(self._lib.cmpmc_mesh_potential_at(self._h, q, C.byref(hint), C.byref(v)))
+        return v.value
+
+    def at(self, p):
+        return self.field_at(p)
+
+
 @dataclass
 class DetectorModel:
     """DetectorModel (transport/engine.hpp:96-156)."""
     solid: CylinderSolid = field(default_factory=CylinderSolid)
     e_field: UniformElectricField = field(default_factory=lambda: UniformElectricField.from_bias(0.0, 2.54 * units.cm))
+    mesh_field_3d: Optional[TriLinearMesh3D] = None
     surfaces: list = field(default_factory=_default_surfaces)
     max_bounces: int = 5000
     min_phonon_eV: float = 10.0 * units.ueV
@@ -558,6 +647,11 @@ class workloads:
     pair_drift = Workload(_ffi.WL_PAIR_DRIFT, 2, "pair_drift")
     single_l_volume = Workload(_ffi.WL_SINGLE_L_VOLUME, 1, "single_L_7.5meV_volume")
     test_parallel = Workload(_ffi.WL_TEST_PARALLEL, 1, "test_parallel_mixed")
+    # electron recoils split by EnergyPartition::partition_deposit; the detector needs
+    # TriLinearMesh3D.recoil_mesh as mesh_field_3d and luke_sample_fraction 1 (recoil) or
+    # 0.05 (recoil_light)
+    recoil = Workload(_ffi.WL_RECOIL, 1, "electron_recoil_10eV_10keV")
+    recoil_light = Workload(_ffi.WL_RECOIL_LIGHT, 1, "electron_recoil_10eV_100eV_light")
 
 
 @dataclass
@@ -601,6 +695,8 @@ class SimulationEngine:
             _check(self._lib.cmpmc_gpu_create(self.lattice._h, C.byref(self._cdet), int(device), C.byref(h)),
                    what="device context")
             self._ctx[device] = h
+            if self.detector.mesh_field_3d is not None:
+                _check(self._lib.cmpmc_gpu_set_mesh(h, self.detector.mesh_field_3d._h), h)
         return h
 
     def configure(self, device: int = 0, threads_per_block: int = 0, blocks_per_sm: int = 0,

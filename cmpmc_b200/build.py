@@ -33,6 +33,7 @@ CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
 SOURCES = {
     "lattice_host.cpp": [],
     "host.cpp": [],
+    "mesh_host.cpp": [],
     "transport_plain.cu": ["--fmad=false"],
     "transport_batched.cu": [],
     "finish.cu": [],

@@ -84,6 +84,7 @@ struct cmpmc_gpu_ctx {
     Lattice L{};
     Detector D{};
     DevBuf tables;  // oct LUT + CDF tables
+    DevBuf mesh;    // MeshTet records of the attached field mesh
     int tpb = 128;
     int bps = 0;  // 0: occupancy-derived
     uint32_t stack_cap = 1024;        // plain form: tracks per device thread
@@ -222,7 +223,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->tables, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
+    for (DevBuf* b : {&ctx->tables, &ctx->mesh, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
                       &ctx->unit_event, &ctx->ev_offsets, &ctx->ev_stats2, &ctx->partials, &ctx->adj_prim,
@@ -259,6 +260,23 @@ int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_pe
         ctx->stack_cap_batched = ctx->stack_cap;
     }
     if (hit_capacity) ctx->hit_cap = hit_capacity;
+    return CMPMC_OK;
+}
+
+int cmpmc_gpu_set_mesh(cmpmc_gpu_ctx* ctx, const cmpmc_mesh* mesh) {
+    if (!ctx) return CMPMC_ERR_INVALID;
+    ctx->last_status = CMPMC_OK;
+    ctx->last_error.clear();
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    ctx->D.mesh.tet = nullptr;
+    ctx->D.mesh.n_tets = 0;
+    if (!mesh || mesh->rec.empty()) return CMPMC_OK;
+    const size_t bytes = mesh->rec.size() * sizeof(MeshTet);
+    CK(ctx->mesh.ensure(bytes), "alloc mesh");
+    CK(cudaMemcpy(ctx->mesh.p, mesh->rec.data(), bytes, cudaMemcpyHostToDevice), "copy mesh");
+    ctx->D.mesh.tet = ctx->mesh.as<MeshTet>();
+    ctx->D.mesh.n_tets = static_cast<int32_t>(mesh->rec.size());
     return CMPMC_OK;
 }
 

@@ -1,10 +1,12 @@
 // internal.hpp -- host-side types shared by the library's translation units.
 #pragma once
 
+#include <array>
 #include <string>
 #include <vector>
 
 #include "../../include/cmpmc_gpu.h"
+#include "mesh.cuh"
 #include "transport.cuh"
 
 struct cmpmc_lattice {
@@ -13,6 +15,15 @@ struct cmpmc_lattice {
     std::vector<double> cdf_lt, cdf_tt;    // [1024] each
     std::vector<double> hv;                // flattened HV tensors (see cmpmc_lattice_tables)
     cmpmc_gpu::Lattice view;               // host pointers into the vectors above
+};
+
+// TriLinearMesh3D (geometry/mesh_field.hpp:40-345): node table, potentials, sorted
+// tetrahedra and the per-tetrahedron records the device walks (mesh.cuh).
+struct cmpmc_mesh {
+    std::vector<double> X;                   // [n_vertices][3]
+    std::vector<double> V;                   // [n_vertices], clamped
+    std::vector<std::array<int32_t, 4>> tets;
+    std::vector<cmpmc_gpu::MeshTet> rec;     // [n_tets]
 };
 
 namespace cmpmc_gpu {

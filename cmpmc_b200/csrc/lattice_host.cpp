@@ -420,6 +420,8 @@ void cmpmc_crystal_config_germanium(cmpmc_crystal_config* c) {
     c->iv_lin_rate1 = 1.5;
     c->iv_lin_power = 4.0;
     c->orient[0][0] = c->orient[1][1] = c->orient[2][2] = 1.0;
+    c->atomic_Z = 32.0;
+    c->atomic_A = 72.63;
 }
 
 int cmpmc_lattice_create(const cmpmc_crystal_config* cfg, cmpmc_lattice** out) {

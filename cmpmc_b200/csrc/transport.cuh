@@ -9,6 +9,7 @@
 // hit sink; the device kernels supply global-memory stacks (transport_plain.cu).
 #pragma once
 
+#include "mesh.cuh"
 #include "phys.cuh"
 
 namespace cmpmc_gpu {
@@ -26,6 +27,7 @@ struct Detector {
     double charge_max_dk_frac, charge_dt_cap_s, charge_sampling_dk_frac;
     int charge_stepping;
     double fermi_level_above_Ev_eV;
+    MeshView mesh;  // DetectorModel::mesh_field_3d on the device (tet == nullptr: uniform field)
 };
 
 // Phonon state held in registers (PhononTrack, track.hpp:62-72)

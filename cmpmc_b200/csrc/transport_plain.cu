@@ -43,6 +43,8 @@ struct PlainCtx {
     uint64_t ev;
     uint32_t n_hits;
     V3 field_value;
+    MeshView mesh;
+    int32_t tet_hint;  // walk hint of this device thread, kept across carriers and events
     unsigned err;
     KBuf refl;
     double* kwork;
@@ -91,7 +93,11 @@ struct PlainCtx {
             err |= kErrChargeStack;
         }
     }
-    __device__ V3 field(V3, Charge&) { return field_value; }
+    // DetectorModel::electric_field_at (engine.hpp:151-155)
+    __device__ V3 field(V3 p, Charge&) {
+        if (mesh.tet) return mesh_field(mesh, p, tet_hint);
+        return field_value;
+    }
     __device__ void hit(const Hit& h, int channel) {
         const uint32_t local = n_hits++;
         if (!keep_hits) return;
@@ -130,6 +136,8 @@ __global__ void __launch_bounds__(128) k_plain_fp64(const Lattice L, const Detec
     ctx.refl.n = 0;
     ctx.kwork = kwork;
     ctx.field_value = D.e_field;
+    ctx.mesh = D.mesh;
+    ctx.tet_hint = 0;
     for (;;) {
         const unsigned long long ev = atomicAdd(a.next_work, 1ull);
         if (ev >= a.n_events) break;

@@ -93,6 +93,8 @@ inline cmpmc_crystal_config to_c(const cmpmc::CrystalConfig& c) {
     o.h_trap_ion_d_mfp_m = c.h_trap_ion_d_mfp_m; o.h_trap_ion_a0_mfp_m = c.h_trap_ion_a0_mfp_m;
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) o.orient[i][j] = c.orient.m[i][j];
+    o.atomic_Z = c.atomic_Z;
+    o.atomic_A = c.atomic_A;
     return o;
 }
 

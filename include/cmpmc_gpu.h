@@ -131,6 +131,7 @@ typedef struct cmpmc_crystal_config {
     double e_trapping_mfp_m, h_trapping_mfp_m, e_trap_ion_d0_mfp_m, e_trap_ion_a_mfp_m,
            h_trap_ion_d_mfp_m, h_trap_ion_a0_mfp_m;
     double orient[3][3];           /* crystal -> detector rotation */
+    double atomic_Z, atomic_A;     /* for NIEL and the charge-cloud radius (crystal_config.hpp:46-47) */
 } cmpmc_crystal_config;
 
 /* SuperconductorFilmConfig (crystal_config.hpp:240-257) */
@@ -208,6 +209,30 @@ int cmpmc_make_track(const cmpmc_lattice* lat, const double pos[3], const double
 int cmpmc_make_charge(const cmpmc_lattice* lat, int type, const double pos[3], const double dir[3],
                       double ekin_eV, int valley, double time_s, cmpmc_charge_track* out);
 
+/* ---- tetrahedral field mesh (replaces TriLinearMesh3D, geometry/mesh_field.hpp:40-345) -- */
+typedef struct cmpmc_mesh cmpmc_mesh;
+/* TriLinearMesh3D(vertices, potentials, tetrahedra, V_min_clamp, V_max_clamp)
+ * (mesh_field.hpp:47-58): vertices [n][3] (m), potentials [n] (V), tets [m][4] (0-based
+ * node indices). Face neighbours, inverse edge matrices and the per-tetrahedron field
+ * are computed on the host with the reference's arithmetic. */
+int cmpmc_mesh_create(const double* vertices, const double* potentials, uint64_t n_vertices, const int32_t* tets,
+                      uint64_t n_tets, double v_min_clamp, double v_max_clamp, cmpmc_mesh** out);
+/* TriLinearMesh3D::build_cartesian_grid (mesh_field.hpp:131-189): a Kuhn-triangulated
+ * box (6 tetrahedra per cell) over [-hx,hx] x [-hy,hy] x [-hz,hz]; potential(p, user)
+ * gives the node potentials. */
+typedef double (*cmpmc_potential_fn)(const double p[3], void* user);
+int cmpmc_mesh_build_cartesian(double half_x, double half_y, double half_z, int nx, int ny, int nz,
+                               cmpmc_potential_fn potential, void* user, cmpmc_mesh** out);
+/* The node potential of the recoil workloads (user = const cmpmc_detector*):
+ * V = 4 V (z + h) / 2h + 0.2 V (r / R)^2 sin(pi z / 2h). */
+double cmpmc_recoil_potential(const double p[3], void* detector);
+void cmpmc_mesh_destroy(cmpmc_mesh* mesh);
+int cmpmc_mesh_info(const cmpmc_mesh* mesh, uint64_t* n_vertices, uint64_t* n_tets);
+/* field_at / potential_at with a caller-held walk hint (mesh_field.hpp:66-116); zero
+ * outside the mesh. */
+int cmpmc_mesh_field_at(const cmpmc_mesh* mesh, const double p[3], int32_t* hint, double E[3]);
+int cmpmc_mesh_potential_at(const cmpmc_mesh* mesh, const double p[3], int32_t* hint, double* V);
+
 /* ---- random streams (core/rng.hpp) --------------------------------------------- */
 void cmpmc_rng_for_stream(uint64_t seed, uint64_t stream, uint64_t state[4]);
 uint64_t cmpmc_rng_next_u64(uint64_t state[4]);
@@ -218,13 +243,22 @@ enum {
     CMPMC_WL_SINGLE_L_ORIGIN = 0,  /* one L phonon, 7.5 meV, at the origin, isotropic          */
     CMPMC_WL_MIXED_ENERGY    = 1,  /* 100 phonons/event, log-uniform 1-30 meV, L/ST/FT mix      */
     CMPMC_WL_PAIR_DRIFT      = 2,  /* one e-/h+ pair per event, uniform origin                  */
+    CMPMC_WL_RECOIL          = 3,  /* electron recoil 10 eV-10 keV (log-uniform), uniform origin,
+                                      split by EnergyPartition::partition_deposit (pairs capped
+                                      at 4096); all Luke phonons tracked; mesh field          */
     CMPMC_WL_SINGLE_L_VOLUME = 4,  /* one L phonon, 7.5 meV, uniform origin, isotropic          */
-    CMPMC_WL_TEST_PARALLEL   = 5   /* reference tests/test_parallel.cpp:110-125 generator        */
+    CMPMC_WL_TEST_PARALLEL   = 5,  /* reference tests/test_parallel.cpp:110-125 generator        */
+    CMPMC_WL_RECOIL_LIGHT    = 6   /* as RECOIL with deposits 10-100 eV (log-uniform), at most 20
+                                      prompt phonons (weighted) and 5 % of the Luke phonons
+                                      tracked (weight 20): the parity case                   */
 };
 /* Runs the workload's generator for events [first_event, first_event + n_events) from
  * Rng::for_stream(seed, ev) and writes, per event, the RNG state after the generator
  * (4 u64), the injected energy and the CSR-packed initial tracks. Capacities are in
- * records; *n_phonons / *n_charges receive the totals (CMPMC_ERR_CAPACITY if short). */
+ * records; *n_phonons / *n_charges receive the totals (CMPMC_ERR_CAPACITY if short; the
+ * offsets are written either way, so a call with zero capacities sizes the buffers).
+ * The recoil workloads expect det->luke_sample_fraction as they define it (1 or 0.05);
+ * their field mesh is built by cmpmc_recoil_mesh. */
 int cmpmc_generate(const cmpmc_lattice* lat, const cmpmc_detector* det, int workload, uint64_t seed,
                    uint64_t first_event, uint64_t n_events, int n_threads,
                    uint64_t* rng_state, double* injected_eV,
@@ -232,6 +266,11 @@ int cmpmc_generate(const cmpmc_lattice* lat, const cmpmc_detector* det, int work
                    uint64_t* n_phonons,
                    uint64_t* charge_offsets, cmpmc_charge_track* charges, uint64_t charge_cap,
                    uint64_t* n_charges);
+
+/* The field mesh of the recoil workloads: build_cartesian_grid(R, R, h, 58, 58, 57) of the
+ * detector's cylinder (59 x 59 x 58 = 201,898 nodes, 1,150,488 tetrahedra) with node
+ * potentials cmpmc_recoil_potential. */
+int cmpmc_recoil_mesh(const cmpmc_detector* det, cmpmc_mesh** out);
 
 /* ---- device context and run ---------------------------------------------------- */
 typedef struct cmpmc_gpu_ctx cmpmc_gpu_ctx;
@@ -285,6 +324,12 @@ int cmpmc_gpu_last_error(const cmpmc_gpu_ctx* ctx, char* buf, size_t size);
 int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_per_sm,
                         uint64_t stack_capacity, uint64_t hit_capacity);
 int cmpmc_gpu_device_count(int* count);
+/* DetectorModel::mesh_field_3d (engine.hpp:99, looked up by electric_field_at,
+ * engine.hpp:151-155): copies the mesh to the context's device; the charge transport then
+ * takes its field from the mesh instead of the uniform e_field. NULL detaches it. Each
+ * device thread keeps its own walk hint across carriers and events, like the reference's
+ * thread_local hint (mesh_field.hpp:119-122). */
+int cmpmc_gpu_set_mesh(cmpmc_gpu_ctx* ctx, const cmpmc_mesh* mesh);
 
 /* Allocation-free run of the plain FP64 form (phonon-only events). No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc -- code running inside a

@@ -18,6 +18,10 @@
 //       and prints one JSON line (wall seconds from RunResult::wall_seconds).
 //   cmpmc_ref rng <seed> <stream> <count>
 //       Prints next_u64 / uniform / isotropic_dir / lambertian_dir vectors.
+//   cmpmc_ref mesh <n_points> <out>
+//       Builds the c3 field mesh and writes, for n points drawn in the cylinder
+//       (Rng::for_stream(5, 0)), the point, field_at and potential_at (each with one
+//       walk hint carried from point to point) as 7 doubles per point.
 //
 // Workloads (seeds and draw orders are the canonical generators of this project):
 //   c0  default Ge detector; one L phonon, 7.5 meV, at the origin, isotropic; seed 42
@@ -32,6 +36,13 @@
 //       (even events: FT 7.5 meV phonon at the origin; odd events: e-/h+ pair),
 //       field 2 V over 2.54 cm, luke_sample_fraction 0.02; seed 77
 //   tpl same as tp with luke_sample_fraction 1 (every Luke phonon tracked)
+//   c3  electron recoils: E = 10 eV * 10^(3u), origin as c1, split by the reference's
+//       EnergyPartition::partition_deposit (max_sampled_pairs 4096, other options at their
+//       defaults); field from TriLinearMesh3D::build_cartesian_grid(R, R, h, 58, 58, 57)
+//       with V = 4 (z + h) / 2h + 0.2 ((x^2 + y^2) / R^2) sin(pi z / 2h); all Luke phonons
+//       tracked; seed 13; events_per_chunk 1
+//   c3s the same with E = 10 eV * 10^u, max_sampled_phonons 20 (prompt phonons carry the
+//       weight n_true / 20) and luke_sample_fraction 0.05
 //
 // Built with -DCMPMC_ORACLE_CRLIBM (as cmpmc_ref_crlibm) the transport uses a correctly
 // rounded libm (ref_crlibm.hpp); the generators and the lattice build keep the
@@ -71,12 +82,27 @@ Workload make_workload(const std::string& w) {
     else if (w == "c2") { wl.seed = 11; wl.events_per_chunk = 1; }
     else if (w == "c4") wl.seed = 17;
     else if (w == "tp" || w == "tpl") wl.seed = 77;
+    else if (w == "c3" || w == "c3s") { wl.seed = 13; wl.events_per_chunk = 1; }
     else { std::fprintf(stderr, "unknown workload %s\n", w.c_str()); std::exit(2); }
     return wl;
 }
 
+double recoil_potential(const Vec3& p, double R, double h) {
+    const double rr = (p.x * p.x + p.y * p.y) / (R * R);
+    return 4.0 * (p.z + h) / (2.0 * h) + 0.2 * rr * std::sin(units::pi * p.z / (2.0 * h));
+}
+
+geometry::TriLinearMesh3D recoil_mesh(const CylinderSolid& s) {
+    const double R = s.radius, h = s.half_z;
+    return geometry::TriLinearMesh3D::build_cartesian_grid(
+        R, R, h, 58, 58, 57, [R, h](const Vec3& p) { return recoil_potential(p, R, h); });
+}
+
 void setup_detector(const std::string& w, DetectorModel& det) {
-    if (w == "c2") {
+    if (w == "c3" || w == "c3s") {
+        det.mesh_field_3d = recoil_mesh(det.solid);
+        det.luke_sample_fraction = (w == "c3") ? 1.0 : 0.05;
+    } else if (w == "c2") {
         det.e_field = UniformElectricField::from_bias(4.0, 2.54 * units::cm);
         det.luke_sample_fraction = 0.0;
     } else if (w == "tp" || w == "tpl") {
@@ -101,6 +127,7 @@ struct Generator {
     const ChargePhysics* charges;
     const DetectorModel* det;
     size_t n_valleys;
+    const EnergyPartition* partition;
 
     // the generator runs on the host with the platform libm in every build
     void operator()(EventInput& in) const {
@@ -130,6 +157,15 @@ struct Generator {
             in.charges.push_back(charges->make_charge(ExcitationType::Electron, p, de, 1e-6, v));
             const Vec3 dh = in.rng.isotropic_dir();
             in.charges.push_back(charges->make_charge(ExcitationType::Hole, p, dh, 1e-6, 0));
+        } else if (w == "c3" || w == "c3s") {
+            const double u = in.rng.uniform();
+            const double E = (w == "c3") ? 10.0 * std::pow(10.0, 3.0 * u) : 10.0 * std::pow(10.0, u);
+            const Vec3 p = uniform_origin(det->solid, in.rng);
+            PartitionOptions opts;
+            opts.max_sampled_pairs = 4096;
+            if (w == "c3s") opts.max_sampled_phonons = 20;
+            partition->partition_deposit(p, 0.0, E, false, in.charges, in.phonons, in.rng, opts);
+            in.injected_eV += E;
         } else if (w == "c4") {
             const Vec3 p = uniform_origin(det->solid, in.rng);
             const Vec3 d = in.rng.isotropic_dir();
@@ -170,7 +206,8 @@ int cmd_dump(const std::string& w, uint64_t first, uint64_t n, unsigned threads,
     setup_detector(w, det);
     const SimulationEngine engine(lattice, det);
     const ChargePhysics cp(lattice);
-    const Generator gen{w, &engine, &cp, &det, lattice.config().valley_dirs.size()};
+    const EnergyPartition part(lattice);
+    const Generator gen{w, &engine, &cp, &det, lattice.config().valley_dirs.size(), &part};
 
     std::vector<EventRecord> rec(n);
     std::atomic<uint64_t> next{0};
@@ -232,7 +269,8 @@ int cmd_time(const std::string& w, uint64_t first, uint64_t n, unsigned threads)
     setup_detector(w, det);
     const SimulationEngine engine(lattice, det);
     const ChargePhysics cp(lattice);
-    const Generator gen{w, &engine, &cp, &det, lattice.config().valley_dirs.size()};
+    const EnergyPartition part(lattice);
+    const Generator gen{w, &engine, &cp, &det, lattice.config().valley_dirs.size(), &part};
     const double init_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     // run_events numbers events from 0; an offset range runs through a shifted generator
     // whose streams are Rng::for_stream(seed, first + i), exactly as in the full run.
@@ -284,6 +322,24 @@ int cmd_rng(uint64_t seed, uint64_t stream, int count) {
     return 0;
 }
 
+int cmd_mesh(uint64_t n, const std::string& out) {
+    const DetectorModel det;
+    const geometry::TriLinearMesh3D mesh = recoil_mesh(det.solid);
+    Rng rng = Rng::for_stream(5, 0);
+    int hint_e = 0, hint_v = 0;
+    FILE* f = open_or_die(out);
+    for (uint64_t i = 0; i < n; ++i) {
+        const Vec3 p = uniform_origin(det.solid, rng);
+        const Vec3 E = mesh.field_at(p, hint_e);
+        const double V = mesh.potential_at(p, hint_v);
+        const double rec[7] = {p.x, p.y, p.z, E.x, E.y, E.z, V};
+        std::fwrite(rec, 8, 7, f);
+    }
+    std::fclose(f);
+    std::printf("{\"vertices\": %zu, \"tetrahedra\": %zu}\n", mesh.num_vertices(), mesh.num_tetrahedra());
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -298,6 +354,7 @@ int main(int argc, char** argv) {
     if (cmd == "time" && argc == 6)
         return cmd_time(argv[2], std::strtoull(argv[3], nullptr, 10), std::strtoull(argv[4], nullptr, 10),
                         static_cast<unsigned>(std::atoi(argv[5])));
+    if (cmd == "mesh" && argc == 4) return cmd_mesh(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "rng" && argc == 5)
         return cmd_rng(std::strtoull(argv[2], nullptr, 10), std::strtoull(argv[3], nullptr, 10), std::atoi(argv[4]));
     std::fprintf(stderr, "bad arguments\n");

@@ -15,8 +15,11 @@ compiled from its own headers by `make -C oracle ref`) and stores compact record
   <workload>_cr_*.npz   the same from oracle/_ref/cmpmc_ref_crlibm: the reference whose
                         transport uses a correctly rounded libm (oracle/ref_crlibm.hpp);
                         `floor` = fraction of events on which it agrees with the glibc build
+  mesh_c3.npz           the recoil workloads' field mesh (TriLinearMesh3D::build_cartesian_grid,
+                        201,898 nodes): field_at and potential_at at 4096 points in the cylinder
 
-Usage: python tests/golden/make_golden.py   (needs the reference build; takes ~1 min)
+Usage: python tests/golden/make_golden.py [--only NAME,...]   (needs the reference build;
+       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist or mesh)
 """
 from __future__ import annotations
 
@@ -46,6 +49,7 @@ PLAN = {
     "c2": (64, 2000),
     "tp": (32, 203),
     "tpl": (2, 21),
+    "c3s": (1, 64),
 }
 
 
@@ -58,79 +62,110 @@ def dump(workload: str, first: int, n: int, tmp: str, exe: str = REF):
 def main() -> None:
     if not (os.path.exists(REF) and os.path.exists(REF_TABLES)):
         sys.exit("build the reference first: make -C oracle ref")
+    only = None
+    if len(sys.argv) > 2 and sys.argv[1] == "--only":
+        only = set(sys.argv[2].split(","))
+
+    def want(name: str) -> bool:
+        return only is None or name in only
+
     with tempfile.TemporaryDirectory() as tmp:
-        # RNG vectors
-        rng = {}
-        for seed, stream in ((42, 0), (7, 12345), (17, 999999)):
-            out = subprocess.run([REF, "rng", str(seed), str(stream), "8"], check=True, capture_output=True,
-                                 text=True).stdout.split("\n")
-            rec = {"state": [], "u64": [], "uniform": [], "iso": [], "lamb": [], "seeded_12345": []}
-            for line in out:
-                if not line:
-                    continue
-                k, *v = line.split()
-                if k == "state":
-                    rec["state"] = [int(x) for x in v]
-                elif k == "seeded":
-                    rec["seeded_12345"] = [int(x) for x in v]
-                elif k == "u64":
-                    rec["u64"].append(int(v[0]))
-                elif k == "uniform":
-                    rec["uniform"].append(float.hex(float(v[0])))
-                else:
-                    rec[k].append([float.hex(float(x)) for x in v])
-            rng[f"{seed}:{stream}"] = rec
-        with open(os.path.join(HERE, "rng.json"), "w") as f:
-            json.dump(rng, f, indent=1)
-
-        # lattice tables
-        prefix = os.path.join(tmp, "ge")
-        subprocess.run([REF_TABLES, prefix], check=True)
-        oct_b = open(prefix + ".oct", "rb").read()
-        cdf = np.fromfile(prefix + ".cdf", dtype=np.float64)
-        hv = np.fromfile(prefix + ".hv", dtype=np.float64)
-        octa = np.frombuffer(oct_b, dtype=np.float32).reshape(3, 256, 256, 4)
-        idx = np.random.default_rng(0).integers(0, 256, size=(64, 2))
-        np.savez_compressed(os.path.join(HERE, "lattice_ge.npz"), oct_sha256=np.array(hashlib.sha256(oct_b).hexdigest()),
-                            cdf_lt=cdf[:1024], cdf_tt=cdf[1024:], hv=hv, sample_idx=idx,
-                            sample=octa[:, idx[:, 0], idx[:, 1], :])
-
-        # workloads: the reference (glibc libm) and the reference with a correctly rounded
-        # libm in the transport (cmpmc_ref_crlibm); "floor" is the fraction of events on
-        # which the two agree (the device's transcendentals are correctly rounded)
-        for wl, (n_full, n_sum) in PLAN.items():
-            if n_full:
-                d = dump(wl, 0, n_full, tmp)
-                np.savez_compressed(os.path.join(HERE, f"{wl}_full.npz"), **d)
-                dc = dump(wl, 0, n_full, tmp, REF_CR)
-                np.savez_compressed(os.path.join(HERE, f"{wl}_cr_full.npz"), **dc)
-            d = dump(wl, 0, n_sum, tmp)
-            s = summarize(d["events"], d["hit_offsets"], d["hits"])
-            np.savez_compressed(os.path.join(HERE, f"{wl}_summary.npz"), summary=s,
-                                injected=d["injected"], rng_state=d["rng_state"])
-            dc = dump(wl, 0, n_sum, tmp, REF_CR)
-            sc = summarize(dc["events"], dc["hit_offsets"], dc["hits"])
-            floor = compare_summaries(s, sc)
-            np.savez_compressed(os.path.join(HERE, f"{wl}_cr_summary.npz"), summary=sc,
-                                floor_mask=floor["agree_mask"], floor=np.array(floor["frac"]))
-            print(wl, n_full, n_sum, int(d["hit_offsets"][-1]), "hits; glibc vs correctly rounded agree on",
-                  f"{100 * floor['frac']:.2f}% of events")
-        # mixed-energy batch: per-event hit histograms of the reference (2000 events,
-        # 200,000 primaries) for the statistical parity of the batched FP32 form
-        d = dump("c1", 0, 2000, tmp)
-        lo, hi = float(d["hits"]["edep"].min()), float(d["hits"]["edep"].max())
-        h = event_histograms(d["hit_offsets"], d["hits"], (lo, hi * (1 + 1e-9)))
-        st = d["events"]["stats"]
-        np.savez_compressed(os.path.join(HERE, "c1_hist.npz"), **h,
-                            injected=d["injected"].sum(), deposited=st["total_deposited_eV"].sum(),
-                            escaped=st["escaped_or_killed_eV"].sum(), steps=st["total_steps"].sum(),
-                            n_hits=len(d["hits"]))
-        print("c1 histograms from", len(d["hits"]), "hits")
+        if want("mesh"):
+            path = os.path.join(tmp, "mesh.bin")
+            info = json.loads(subprocess.run([REF, "mesh", "4096", path], check=True, capture_output=True,
+                                             text=True).stdout)
+            rec = np.fromfile(path, dtype=np.float64).reshape(-1, 7)
+            np.savez_compressed(os.path.join(HERE, "mesh_c3.npz"), points=rec[:, 0:3], field=rec[:, 3:6],
+                                potential=rec[:, 6], n_vertices=info["vertices"], n_tets=info["tetrahedra"])
+        if want("rng"):
+            _rng_vectors()
+        if want("lattice"):
+            _lattice(tmp)
+        _workloads(tmp, want)
+        if want("hist"):
+            _hist(tmp)
     gl = subprocess.run(["ldd", "--version"], capture_output=True, text=True).stdout.split("\n")[0]
     with open(os.path.join(HERE, "PROVENANCE.txt"), "w") as f:
         f.write("Generated by tests/golden/make_golden.py from the unmodified reference CMPMC\n"
                 "(oracle/_ref, g++ -O3 -std=c++20, no -march=native).\n"
                 f"host libm: {gl}\n")
+
+
+def _rng_vectors() -> None:
+    rng = {}
+    for seed, stream in ((42, 0), (7, 12345), (17, 999999)):
+        out = subprocess.run([REF, "rng", str(seed), str(stream), "8"], check=True, capture_output=True,
+                             text=True).stdout.split("\n")
+        rec = {"state": [], "u64": [], "uniform": [], "iso": [], "lamb": [], "seeded_12345": []}
+        for line in out:
+            if not line:
+                continue
+            k, *v = line.split()
+            if k == "state":
+                rec["state"] = [int(x) for x in v]
+            elif k == "seeded":
+                rec["seeded_12345"] = [int(x) for x in v]
+            elif k == "u64":
+                rec["u64"].append(int(v[0]))
+            elif k == "uniform":
+                rec["uniform"].append(float.hex(float(v[0])))
+            else:
+                rec[k].append([float.hex(float(x)) for x in v])
+        rng[f"{seed}:{stream}"] = rec
+    with open(os.path.join(HERE, "rng.json"), "w") as f:
+        json.dump(rng, f, indent=1)
+
+
+def _lattice(tmp: str) -> None:
+    prefix = os.path.join(tmp, "ge")
+    subprocess.run([REF_TABLES, prefix], check=True)
+    oct_b = open(prefix + ".oct", "rb").read()
+    cdf = np.fromfile(prefix + ".cdf", dtype=np.float64)
+    hv = np.fromfile(prefix + ".hv", dtype=np.float64)
+    octa = np.frombuffer(oct_b, dtype=np.float32).reshape(3, 256, 256, 4)
+    idx = np.random.default_rng(0).integers(0, 256, size=(64, 2))
+    np.savez_compressed(os.path.join(HERE, "lattice_ge.npz"), oct_sha256=np.array(hashlib.sha256(oct_b).hexdigest()),
+                        cdf_lt=cdf[:1024], cdf_tt=cdf[1024:], hv=hv, sample_idx=idx,
+                        sample=octa[:, idx[:, 0], idx[:, 1], :])
+
+
+def _workloads(tmp: str, want) -> None:
+    # workloads: the reference (glibc libm) and the reference with a correctly rounded
+    # libm in the transport (cmpmc_ref_crlibm); "floor" is the fraction of events on
+    # which the two agree (the device's transcendentals are correctly rounded)
+    for wl, (n_full, n_sum) in PLAN.items():
+        if not want(wl):
+            continue
+        if n_full:
+            d = dump(wl, 0, n_full, tmp)
+            np.savez_compressed(os.path.join(HERE, f"{wl}_full.npz"), **d)
+            dc = dump(wl, 0, n_full, tmp, REF_CR)
+            np.savez_compressed(os.path.join(HERE, f"{wl}_cr_full.npz"), **dc)
+        d = dump(wl, 0, n_sum, tmp)
+        s = summarize(d["events"], d["hit_offsets"], d["hits"])
+        np.savez_compressed(os.path.join(HERE, f"{wl}_summary.npz"), summary=s,
+                            injected=d["injected"], rng_state=d["rng_state"])
+        dc = dump(wl, 0, n_sum, tmp, REF_CR)
+        sc = summarize(dc["events"], dc["hit_offsets"], dc["hits"])
+        floor = compare_summaries(s, sc)
+        np.savez_compressed(os.path.join(HERE, f"{wl}_cr_summary.npz"), summary=sc,
+                            floor_mask=floor["agree_mask"], floor=np.array(floor["frac"]))
+        print(wl, n_full, n_sum, int(d["hit_offsets"][-1]), "hits; glibc vs correctly rounded agree on",
+              f"{100 * floor['frac']:.2f}% of events")
+
+
+def _hist(tmp: str) -> None:
+    # mixed-energy batch: per-event hit histograms of the reference (2000 events,
+    # 200,000 primaries) for the statistical parity of the batched FP32 form
+    d = dump("c1", 0, 2000, tmp)
+    lo, hi = float(d["hits"]["edep"].min()), float(d["hits"]["edep"].max())
+    h = event_histograms(d["hit_offsets"], d["hits"], (lo, hi * (1 + 1e-9)))
+    st = d["events"]["stats"]
+    np.savez_compressed(os.path.join(HERE, "c1_hist.npz"), **h,
+                        injected=d["injected"].sum(), deposited=st["total_deposited_eV"].sum(),
+                        escaped=st["escaped_or_killed_eV"].sum(), steps=st["total_steps"].sum(),
+                        n_hits=len(d["hits"]))
+    print("c1 histograms from", len(d["hits"]), "hits")
 
 
 if __name__ == "__main__":

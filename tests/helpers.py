@@ -22,20 +22,34 @@ def detector_for(workload: str):
     if workload == "c2":
         det.e_field = cm.UniformElectricField.from_bias(4.0, 2.54 * cm.units.cm)
         det.luke_sample_fraction = 0.0
+    elif workload == "c3s":
+        det.mesh_field_3d = recoil_mesh()
+        det.luke_sample_fraction = 0.05
     elif workload in ("tp", "tpl"):
         det.e_field = cm.UniformElectricField.from_bias(2.0, 2.54 * cm.units.cm)
         det.luke_sample_fraction = 0.02 if workload == "tp" else 1.0
     return det
 
 
-WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77}
+_MESH = []
+
+
+def recoil_mesh():
+    """The recoil workloads' field mesh (built once per test process)."""
+    import cmpmc_b200 as cm
+    if not _MESH:
+        _MESH.append(cm.TriLinearMesh3D.recoil_mesh(cm.DetectorModel()))
+    return _MESH[0]
+
+
+WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13}
 
 
 def workload_of(name: str):
     import cmpmc_b200 as cm
     return {"c0": cm.workloads.single_l_origin, "c1": cm.workloads.mixed_energy, "c2": cm.workloads.pair_drift,
             "c4": cm.workloads.single_l_volume, "tp": cm.workloads.test_parallel,
-            "tpl": cm.workloads.test_parallel}[name]
+            "tpl": cm.workloads.test_parallel, "c3s": cm.workloads.recoil_light}[name]
 
 
 def has_gpu() -> bool:

@@ -60,7 +60,7 @@ def test_lattice_tables_bit_identical_to_reference(ge_lattice):
     assert np.array_equal(t["oct"][:, idx[:, 0], idx[:, 1], :], g["sample"])
 
 
-@pytest.mark.parametrize("wl", ["c0", "c1", "c2", "tp", "tpl"])
+@pytest.mark.parametrize("wl", ["c0", "c1", "c2", "tp", "tpl", "c3s"])
 def test_native_generators_match_reference(ge_lattice, wl):
     import cmpmc_b200 as cm
     g = golden(f"{wl}_full.npz")
@@ -84,6 +84,84 @@ def test_native_generator_summary_streams(ge_lattice):
     ev = eng.generate(cm.workloads.single_l_origin, len(s["rng_state"]), 42)
     assert np.array_equal(ev.rng_state, s["rng_state"])
     assert np.array_equal(ev.injected_eV, s["injected"])
+
+
+def test_recoil_generator_streams(ge_lattice):
+    """EnergyPartition::partition_deposit restated on the host: the post-generator Rng
+    state and deposit of all 64 light-recoil events equal the reference's."""
+    import cmpmc_b200 as cm
+    s = golden("c3s_summary.npz")
+    eng = cm.SimulationEngine(ge_lattice, detector_for("c3s"))
+    ev = eng.generate(cm.workloads.recoil_light, len(s["rng_state"]), 13)
+    assert np.array_equal(ev.rng_state, s["rng_state"])
+    assert np.array_equal(ev.injected_eV, s["injected"])
+    # pairs: electron then hole at the same point, charge weight n_true / n_sampled >= 1
+    ch = ev.charges
+    assert len(ch) % 2 == 0 and np.all(ch["type"][0::2] == 1) and np.all(ch["type"][1::2] == 2)
+    assert np.array_equal(ch["pos"][0::2], ch["pos"][1::2])
+    assert np.all(ev.phonons["weight"] >= 1.0)
+
+
+def test_recoil_generator_full_range_counts(ge_lattice):
+    """Deposits up to 10 keV: pair counts within [1, 4096] sampled per event (weights
+    above the cap), at most 5000 prompt phonons, offsets consistent, sizing call first."""
+    import cmpmc_b200 as cm
+    eng = cm.SimulationEngine(ge_lattice, cm.DetectorModel())
+    ev = eng.generate(cm.workloads.recoil, 256, 13)
+    n_ch = np.diff(ev.charge_offsets)
+    n_ph = np.diff(ev.phonon_offsets)
+    assert n_ch.max() <= 2 * 4096 and n_ph.max() <= 5000 and n_ph.min() >= 1
+    pair_e = ev.injected_eV / np.maximum(n_ch // 2, 1)
+    assert 0.5 < np.median(pair_e) < 6.0  # ~2.96 eV per pair in Ge
+    # prompt phonon energy: deposit minus n_true pairs x (gap + 10 meV)
+    w = ev.phonons["weight"]
+    assert np.all(w >= 1.0)
+
+
+def test_mesh_field_bit_identical_to_reference():
+    """TriLinearMesh3D::build_cartesian_grid + field_at / potential_at of the recoil
+    workloads' mesh: every field and potential at 4096 points equals the reference's,
+    with the walk hint carried from point to point."""
+    import ctypes as C
+    from tests.helpers import recoil_mesh
+    g = golden("mesh_c3.npz")
+    m = recoil_mesh()
+    assert m.num_vertices() == int(g["n_vertices"]) and m.num_tetrahedra() == int(g["n_tets"])
+    he, hv = C.c_int32(0), C.c_int32(0)
+    for i, p in enumerate(g["points"]):
+        assert m.field_at(p, he) == tuple(g["field"][i]), i
+        assert m.potential_at(p, hv) == g["potential"][i], i
+
+
+def test_mesh_from_arrays_and_cartesian_builder_agree():
+    """A user mesh given as arrays (the TriLinearMesh3D constructor) equals the Cartesian
+    builder's; outside the hull the field is zero; a linear potential gives its exact
+    gradient."""
+    import cmpmc_b200 as cm
+    n = 3
+    xs = np.linspace(-1.0, 1.0, n + 1)
+    fn = lambda p: 2.0 * p[0] - 3.0 * p[1] + 0.5 * p[2]  # noqa: E731
+    a = cm.TriLinearMesh3D.build_cartesian_grid(1.0, 1.0, 1.0, n, n, n, fn)
+    verts = np.array([(x, y, z) for x in xs for y in xs for z in xs])
+    pots = np.array([fn(v) for v in verts])
+    vid = lambda i, j, k: (i * (n + 1) + j) * (n + 1) + k  # noqa: E731
+    tets = []
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                c = [vid(i + di, j + dj, k + dk) for di in (0, 1) for dj in (0, 1) for dk in (0, 1)]
+                v000, v001, v010, v011, v100, v101, v110, v111 = c
+                tets += [(v111, v000, v100, v110), (v000, v100, v101, v111), (v000, v010, v110, v111),
+                         (v000, v010, v011, v111), (v000, v001, v101, v111), (v000, v001, v011, v111)]
+    b = cm.TriLinearMesh3D(verts, pots, tets)
+    assert a.num_tetrahedra() == b.num_tetrahedra() == 6 * n ** 3
+    rng = np.random.default_rng(1)
+    for p in rng.uniform(-0.99, 0.99, size=(200, 3)):
+        ea, eb = a.field_at(p), b.field_at(p)
+        assert ea == eb
+        np.testing.assert_allclose(ea, (-2.0, 3.0, -0.5), rtol=1e-12, atol=1e-12)
+        assert a.potential_at(p) == pytest.approx(fn(p), rel=1e-12, abs=1e-12)
+    assert a.field_at((3.0, 0.0, 0.0)) == (0.0, 0.0, 0.0)
 
 
 def test_python_generator_matches_native(ge_lattice):
