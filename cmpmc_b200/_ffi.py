@@ -187,6 +187,7 @@ _SIG = {
     "cmpmc_mesh_field_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
     "cmpmc_mesh_potential_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
     "cmpmc_gpu_set_mesh": (_i32, [C.c_void_p, C.c_void_p]),
+    "cmpmc_gpu_configure_queue": (_i32, [C.c_void_p, _u64]),
     "cmpmc_gpu_run_events_noalloc": (_i32, [C.c_void_p, C.POINTER(DetectorC), _i32, _u64, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _u64,
                                             C.c_void_p, C.POINTER(SimStatsC), C.POINTER(_u64)]),

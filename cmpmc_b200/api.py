@@ -700,9 +700,11 @@ class SimulationEngine:
         return h
 
     def configure(self, device: int = 0, threads_per_block: int = 0, blocks_per_sm: int = 0,
-                  stack_capacity: int = 0, hit_capacity: int = 0) -> None:
+                  stack_capacity: int = 0, hit_capacity: int = 0, queue_capacity: int = 0) -> None:
         h = self.context(device)
         _check(self._lib.cmpmc_gpu_configure(h, threads_per_block, blocks_per_sm, stack_capacity, hit_capacity), h)
+        if queue_capacity:
+            _check(self._lib.cmpmc_gpu_configure_queue(h, int(queue_capacity)), h)
 
     def make_track(self, pos, k_dir, mode, energy_eV, time_s=0.0, weight=1.0) -> np.ndarray:
         out = np.zeros((), dtype=_ffi.PHONON_DTYPE)

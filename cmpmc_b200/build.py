@@ -36,6 +36,7 @@ SOURCES = {
     "mesh_host.cpp": [],
     "transport_plain.cu": ["--fmad=false"],
     "transport_batched.cu": [],
+    "charges_batched.cu": [],
     "finish.cu": [],
     "capi.cu": [],
 }

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "device.cuh"
 #include "internal.hpp"
@@ -95,6 +96,9 @@ struct cmpmc_gpu_ctx {
     DevBuf stack, cstack, hit_stage, hit_key, counters, ev_stats, ev_nhits, offsets, hits_out, total;
     DevBuf unit_event, ev_offsets, ev_stats2, partials;  // batched form: unit -> event map, event offsets / stats
     DevBuf adj_prim, adj_hist, adj_w, adj_partials, adj_sums;  // adjoint: per-primary rows, bins, reductions
+    DevBuf mesh32;                                      // FP32 mesh records (batched charge form)
+    DevBuf queue, resume_a, resume_b, ccounters, carrier_event, cursor;  // batched charge form
+    uint64_t queue_cap = 1ull << 24;                    // Luke-phonon queue entries (64 B each)
     const float* cdf_f = nullptr;              // FP32 copies of the decay tables (in `tables`)
     HostBuf h_hits, h_offsets, h_evstats, h_total, h_counters;
     cudaEvent_t e_start = nullptr, e_k0 = nullptr, e_k1 = nullptr, e_end = nullptr;
@@ -124,6 +128,169 @@ int cuda_fail(cmpmc_gpu_ctx* ctx, cudaError_t e, const char* what) {
         cudaError_t _e = (call);                           \
         if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); \
     } while (0)
+
+// Device counters of the batched charge form (reset per phase except next_carrier)
+struct ChargeCounters {
+    unsigned long long q_tail, resume_next, n_resume_out, next_carrier;
+};
+
+// The batched FP32 form of events with charges: phase 0 transports the generator's
+// phonons; then charge phases (carriers drift and queue their Luke phonons) alternate
+// with queue phases (the queued phonons are transported) until every carrier is done.
+// All units add their counters and hits to per-event sinks, merged at the end. A stack
+// or hit-staging overflow reruns the whole call with more room (every unit owns its
+// substream, so the rerun reproduces the same hits).
+int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, uint64_t n, uint64_t n_ph,
+                        uint64_t n_ch, int& launches, Counters& hc, float& kms, uint64_t& n_hits,
+                        uint64_t*& ev_offsets, cmpmc_sim_stats*& ev_stats) {
+    cudaStream_t s = ctx->stream;
+    const int tpb = ctx->tpb;
+    int bps_ph = ctx->bps, bps_ch = ctx->bps;
+    if (!bps_ph) {
+        CK(batched_fp32_occupancy(tpb, &bps_ph), "occupancy");
+        bps_ph = std::max(bps_ph, 1);
+    }
+    if (!bps_ch) {
+        CK(charges_fp32_occupancy(tpb, &bps_ch), "occupancy");
+        bps_ch = std::max(bps_ch, 1);
+    }
+    const uint64_t grid_ph = static_cast<uint64_t>(ctx->num_sms) * bps_ph;
+    const uint64_t grid_ch = std::max<uint64_t>(
+        1, std::min<uint64_t>(static_cast<uint64_t>(ctx->num_sms) * bps_ch, (n_ch + tpb - 1) / tpb));
+    const uint64_t resume_cap = grid_ch * tpb * 9;  // a carrier and up to 8 knock-ons per thread
+    const uint64_t q_cap = std::max<uint64_t>(ctx->queue_cap, 64);
+
+    CK(ctx->ev_stats2.ensure(std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats)), "alloc event stats");
+    CK(ctx->ev_nhits.ensure(std::max<uint64_t>(n, 1) * 8), "alloc event hit counts");
+    CK(ctx->ev_offsets.ensure((n + 1) * 8), "alloc event offsets");
+    CK(ctx->cursor.ensure(std::max<uint64_t>(n, 1) * 8), "alloc event cursors");
+    CK(ctx->counters.ensure(sizeof(Counters)), "alloc counters");
+    CK(ctx->ccounters.ensure(sizeof(ChargeCounters)), "alloc charge counters");
+    CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
+    CK(ctx->partials.ensure(kReducePartials * sizeof(cmpmc_sim_stats)), "alloc partial totals");
+    CK(ctx->h_counters.ensure(sizeof(Counters) + sizeof(ChargeCounters)), "alloc host counters");
+    CK(ctx->queue.ensure(q_cap * sizeof(QPhonon)), "alloc Luke-phonon queue");
+    CK(ctx->resume_a.ensure(resume_cap * sizeof(QCharge)), "alloc parked carriers");
+    CK(ctx->resume_b.ensure(resume_cap * sizeof(QCharge)), "alloc parked carriers");
+    CK(ctx->carrier_event.ensure(std::max<uint64_t>(n_ch, 1) * 4), "alloc carrier map");
+    if (n_ph) CK(ctx->unit_event.ensure(n_ph * 4), "alloc unit map");
+    CK(launch_carrier_event(a.ch_off, n, ctx->carrier_event.as<uint32_t>(), s), "carrier map");
+    ++launches;
+    if (n_ph) {
+        CK(launch_unit_event(a.ph_off, n, ctx->unit_event.as<uint32_t>(), s), "unit map");
+        ++launches;
+    }
+    a.ev_sink = 1;
+    a.ev_stats = ctx->ev_stats2.as<cmpmc_sim_stats>();
+    a.ev_nhits = ctx->ev_nhits.as<uint64_t>();
+    Counters* dc = ctx->counters.as<Counters>();
+    a.hit_count = &dc->hit_count;
+    a.next_work = &dc->next_work;
+    a.err = &dc->err;
+    ChargeCounters* cc = ctx->ccounters.as<ChargeCounters>();
+    ChargeArgs ca;
+    std::memset(&ca, 0, sizeof(ca));
+    ca.n_carriers = n_ch;
+    ca.carrier_event = ctx->carrier_event.as<uint32_t>();
+    ca.carrier_seed = mix64(d->seed ^ 0x2545f4914f6cdd1dULL);
+    ca.queue = ctx->queue.as<QPhonon>();
+    ca.q_cap = q_cap;
+    ca.q_tail = &cc->q_tail;
+    ca.resume_next = &cc->resume_next;
+    ca.n_resume_out = &cc->n_resume_out;
+    ca.next_carrier = &cc->next_carrier;
+    ca.resume_cap = resume_cap;
+
+    uint64_t hit_cap = ctx->hit_cap;
+    if (!hit_cap) hit_cap = std::max<uint64_t>(1u << 20, (n_ph + n_ch) * 64);
+    uint32_t& stack_cap = ctx->stack_cap_batched;
+    const uint64_t slots = grid_ph * tpb;
+    char* hbuf = ctx->h_counters.as<char>();
+    for (int attempt = 0;; ++attempt) {
+        if (!d->keep_hits) hit_cap = 1;
+        CK(ctx->stack.ensure(slots * stack_cap * batched_stack_entry_bytes()), "alloc phonon stacks");
+        CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
+        CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
+        a.stack = ctx->stack.as<GTrack>();
+        a.stack_cap = stack_cap;
+        a.hit_stage = ctx->hit_stage.as<cmpmc_sensor_hit>();
+        a.hit_key = ctx->hit_key.as<uint64_t>();
+        a.hit_cap = hit_cap;
+        CK(cudaMemsetAsync(ctx->ev_stats2.p, 0, std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats), s), "memset");
+        CK(cudaMemsetAsync(ctx->ev_nhits.p, 0, std::max<uint64_t>(n, 1) * 8, s), "memset");
+        CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s), "memset counters");
+        CK(cudaMemsetAsync(ctx->ccounters.p, 0, sizeof(ChargeCounters), s), "memset counters");
+        CK(cudaEventRecord(ctx->e_k0, s), "event");
+        // phase 0: the generator's phonons
+        if (n_ph) {
+            a.n_events = n_ph;
+            CK(launch_batched_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->unit_event.as<uint32_t>(),
+                                   static_cast<int>(std::min<uint64_t>(grid_ph, (n_ph + tpb - 1) / tpb)), tpb, s),
+               "phonon launch");
+            ++launches;
+        }
+        // charge / queue phases
+        QCharge* r_in = ctx->resume_a.as<QCharge>();
+        QCharge* r_out = ctx->resume_b.as<QCharge>();
+        uint64_t n_resume = 0, carriers_started = 0;
+        for (int round = 0;; ++round) {
+            CK(cudaMemsetAsync(ctx->queue.p, 0xff, q_cap * sizeof(QPhonon), s), "memset queue");
+            CK(cudaMemsetAsync(&cc->q_tail, 0, 3 * sizeof(unsigned long long), s), "memset counters");
+            ca.resume_in = r_in;
+            ca.n_resume_in = n_resume;
+            ca.resume_out = r_out;
+            CK(launch_charges_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ca, static_cast<int>(grid_ch), tpb, s),
+               "charge launch");
+            ++launches;
+            CK(cudaMemcpyAsync(hbuf + sizeof(Counters), cc, sizeof(ChargeCounters), cudaMemcpyDeviceToHost, s),
+               "copy counters");
+            CK(cudaStreamSynchronize(s), "charge kernel");
+            const ChargeCounters hcc = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
+            const uint64_t n_q = std::min<uint64_t>(hcc.q_tail, q_cap);
+            if (n_q) {
+                CK(cudaMemsetAsync(&dc->next_work, 0, sizeof(unsigned long long), s), "memset work counter");
+                a.n_events = n_q;
+                CK(launch_queue_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ca.queue,
+                                     static_cast<int>(std::min<uint64_t>(grid_ph, (n_q + tpb - 1) / tpb)), tpb, s),
+                   "queue launch");
+                ++launches;
+            }
+            const uint64_t started = std::min<uint64_t>(hcc.next_carrier, n_ch);
+            const uint64_t parked = hcc.n_resume_out;
+            if (parked > resume_cap) return fail(ctx, CMPMC_ERR_CAPACITY, "parked-carrier buffer overflow");
+            if (parked == 0 && started >= n_ch) break;
+            if (n_q == 0 && parked >= n_resume && started == carriers_started)
+                return fail(ctx, CMPMC_ERR_DEVICE, "charge phases make no progress (queue too small)");
+            n_resume = parked;
+            carriers_started = started;
+            std::swap(r_in, r_out);
+        }
+        CK(cudaEventRecord(ctx->e_k1, s), "event");
+        CK(cudaMemcpyAsync(hbuf, ctx->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "copy counters");
+        CK(cudaStreamSynchronize(s), "transport kernels");
+        hc = *reinterpret_cast<const Counters*>(hbuf);
+        CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
+        const bool stack_over = (hc.err & kErrPhononStack) != 0;
+        const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
+        if (!stack_over && !hits_over) break;
+        if (attempt >= 6) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack or hit buffer overflow persists");
+        if (stack_over) stack_cap = std::min<uint32_t>(stack_cap * 8, 1u << 20);
+        if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
+        hc.err = 0;
+    }
+    if (d->keep_hits) ctx->hit_cap = std::max<uint64_t>(ctx->hit_cap, hit_cap);
+    if (hc.err) return fail(ctx, CMPMC_ERR_DEVICE, "transport kernels reported error word " + std::to_string(hc.err));
+    n_hits = d->keep_hits ? hc.hit_count : 0;
+    CK(ctx->hits_out.ensure(std::max<uint64_t>(n_hits, 1) * sizeof(cmpmc_sensor_hit)), "alloc hits");
+    CK(cudaMemsetAsync(ctx->cursor.p, 0, std::max<uint64_t>(n, 1) * 8, s), "memset cursors");
+    ev_offsets = ctx->ev_offsets.as<uint64_t>();
+    ev_stats = ctx->ev_stats2.as<cmpmc_sim_stats>();
+    a.n_events = n;
+    CK(launch_sink_finish(a, n, ev_offsets, ctx->cursor.as<unsigned long long>(), ctx->hits_out.as<cmpmc_sensor_hit>(),
+                          n_hits, ctx->total.as<cmpmc_sim_stats>(), ctx->partials.as<cmpmc_sim_stats>(), s, &launches),
+       "merge kernels");
+    return CMPMC_OK;
+}
 
 }  // namespace
 
@@ -223,7 +390,8 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->tables, &ctx->mesh, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
+    for (DevBuf* b : {&ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
+                      &ctx->ccounters, &ctx->carrier_event, &ctx->cursor, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
                       &ctx->unit_event, &ctx->ev_offsets, &ctx->ev_stats2, &ctx->partials, &ctx->adj_prim,
@@ -263,6 +431,12 @@ int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_pe
     return CMPMC_OK;
 }
 
+int cmpmc_gpu_configure_queue(cmpmc_gpu_ctx* ctx, uint64_t queue_capacity) {
+    if (!ctx) return CMPMC_ERR_INVALID;
+    if (queue_capacity) ctx->queue_cap = std::max<uint64_t>(queue_capacity, 64);
+    return CMPMC_OK;
+}
+
 int cmpmc_gpu_set_mesh(cmpmc_gpu_ctx* ctx, const cmpmc_mesh* mesh) {
     if (!ctx) return CMPMC_ERR_INVALID;
     ctx->last_status = CMPMC_OK;
@@ -271,12 +445,31 @@ int cmpmc_gpu_set_mesh(cmpmc_gpu_ctx* ctx, const cmpmc_mesh* mesh) {
     CK(cudaStreamSynchronize(ctx->stream), "sync");
     ctx->D.mesh.tet = nullptr;
     ctx->D.mesh.n_tets = 0;
+    ctx->D.mesh32.tet = nullptr;
+    ctx->D.mesh32.n_tets = 0;
     if (!mesh || mesh->rec.empty()) return CMPMC_OK;
     const size_t bytes = mesh->rec.size() * sizeof(MeshTet);
     CK(ctx->mesh.ensure(bytes), "alloc mesh");
     CK(cudaMemcpy(ctx->mesh.p, mesh->rec.data(), bytes, cudaMemcpyHostToDevice), "copy mesh");
+    std::vector<MeshTet32> r32(mesh->rec.size());
+    for (size_t i = 0; i < r32.size(); ++i) {
+        const MeshTet& t = mesh->rec[i];
+        MeshTet32& o = r32[i];
+        for (int j = 0; j < 9; ++j) o.tinv[j] = static_cast<float>(t.tinv[j]);
+        for (int j = 0; j < 3; ++j) {
+            o.x3[j] = static_cast<float>(t.x3[j]);
+            o.e[j] = static_cast<float>(t.e[j]);
+        }
+        for (int j = 0; j < 4; ++j) o.nb[j] = t.nb[j];
+        o.pad = 0.0f;
+    }
+    CK(ctx->mesh32.ensure(r32.size() * sizeof(MeshTet32)), "alloc FP32 mesh");
+    CK(cudaMemcpy(ctx->mesh32.p, r32.data(), r32.size() * sizeof(MeshTet32), cudaMemcpyHostToDevice),
+       "copy FP32 mesh");
     ctx->D.mesh.tet = ctx->mesh.as<MeshTet>();
     ctx->D.mesh.n_tets = static_cast<int32_t>(mesh->rec.size());
+    ctx->D.mesh32.tet = ctx->mesh32.as<MeshTet32>();
+    ctx->D.mesh32.n_tets = static_cast<int32_t>(mesh->rec.size());
     return CMPMC_OK;
 }
 
@@ -354,114 +547,121 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
             a.ch = ctx->in_ch.as<cmpmc_charge_track>();
         }
     }
-    if (batched && n_ch > 0)
-        return fail(ctx, CMPMC_ERR_INVALID, "the batched FP32 form transports phonons only (charges: plain form)");
-
-    // ---- work units: events (plain form) or primary phonons (batched form) ---------
-    const uint64_t units = batched ? n_ph : n;
-    a.n_events = units;
-    int bps = ctx->bps;
-    if (!bps) {
-        CK(batched ? batched_fp32_occupancy(ctx->tpb, &bps) : plain_fp64_occupancy(ctx->tpb, &bps), "occupancy");
-        bps = std::max(bps, 1);
-    }
-    uint64_t grid = static_cast<uint64_t>(ctx->num_sms) * bps;
-    grid = std::min<uint64_t>(grid, (std::max<uint64_t>(units, 1) + ctx->tpb - 1) / ctx->tpb);
-    grid = std::max<uint64_t>(grid, 1);
-    const uint64_t slots = grid * ctx->tpb;
-    const size_t stack_entry = batched ? batched_stack_entry_bytes() : sizeof(GTrack);
-
-    CK(ctx->ev_stats.ensure(std::max<uint64_t>(units, 1) * sizeof(cmpmc_sim_stats)), "alloc unit stats");
-    CK(ctx->ev_nhits.ensure(std::max<uint64_t>(units, 1) * 8), "alloc unit hit counts");
-    CK(ctx->offsets.ensure((units + 1) * 8), "alloc unit offsets");
-    CK(ctx->counters.ensure(sizeof(Counters)), "alloc counters");
-    CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
-    CK(ctx->partials.ensure(kReducePartials * sizeof(cmpmc_sim_stats)), "alloc partial totals");
-    CK(ctx->h_counters.ensure(sizeof(Counters)), "alloc host counters");
-    CK(ctx->cstack.ensure(slots * ctx->cstack_cap * sizeof(GCharge)), "alloc charge stacks");
-    if (batched) {
-        CK(ctx->unit_event.ensure(std::max<uint64_t>(units, 1) * 4), "alloc unit map");
-        CK(ctx->ev_offsets.ensure((n + 1) * 8), "alloc event offsets");
-        if (d->want_event_stats) CK(ctx->ev_stats2.ensure(std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats)),
-                                    "alloc event stats");
-        if (n > 0) {
-            CK(launch_unit_event(a.ph_off, n, ctx->unit_event.as<uint32_t>(), s), "unit map");
-            ++launches;
-        }
-    }
-    a.cstack = ctx->cstack.as<GCharge>();
-    a.cstack_cap = ctx->cstack_cap;
-    a.ev_stats = ctx->ev_stats.as<cmpmc_sim_stats>();
-    a.ev_nhits = ctx->ev_nhits.as<uint64_t>();
-    Counters* dc = ctx->counters.as<Counters>();
-    a.hit_count = &dc->hit_count;
-    a.next_work = &dc->next_work;
-    a.err = &dc->err;
-
-    uint64_t hit_cap = ctx->hit_cap;
-    if (!hit_cap) hit_cap = std::max<uint64_t>(4096, std::max<uint64_t>(n, n_ph + n_ch) * 32);
     Counters hc{};
     float kms = 0.0f;
-    uint32_t& stack_cap = batched ? ctx->stack_cap_batched : ctx->stack_cap;
-    for (int attempt = 0;; ++attempt) {
-        if (!d->keep_hits) hit_cap = 1;
-        CK(ctx->stack.ensure(slots * stack_cap * stack_entry), "alloc phonon stacks");
-        CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
-        CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
-        a.stack = ctx->stack.as<GTrack>();
-        a.stack_cap = stack_cap;
-        a.hit_stage = ctx->hit_stage.as<cmpmc_sensor_hit>();
-        a.hit_key = ctx->hit_key.as<uint64_t>();
-        a.hit_cap = hit_cap;
-        CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s), "memset counters");
-        CK(cudaEventRecord(ctx->e_k0, s), "event");
-        if (units > 0) {
-            CK(batched ? launch_batched_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->unit_event.as<uint32_t>(),
-                                             static_cast<int>(grid), ctx->tpb, s)
-                       : launch_plain_fp64(ctx->L, ctx->D, a, static_cast<int>(grid), ctx->tpb, s),
-               "transport launch");
-            ++launches;
-        }
-        CK(cudaEventRecord(ctx->e_k1, s), "event");
-        CK(cudaMemcpyAsync(ctx->h_counters.p, ctx->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s),
-           "copy counters");
-        CK(cudaStreamSynchronize(s), "transport kernel");
-        hc = *ctx->h_counters.as<Counters>();
-        CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
-        const bool stack_over = (hc.err & (kErrPhononStack | kErrChargeStack)) != 0;
-        const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
-        if (!stack_over && !hits_over) break;
-        if (attempt >= 10) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack or hit buffer overflow persists");
-        if (hc.err & kErrPhononStack) stack_cap = std::min<uint32_t>(stack_cap * 8, 1u << 24);
-        if (hc.err & kErrChargeStack) {
-            ctx->cstack_cap = std::min<uint32_t>(ctx->cstack_cap * 8, 1u << 20);
-            CK(ctx->cstack.ensure(slots * ctx->cstack_cap * sizeof(GCharge)), "alloc charge stacks");
-            a.cstack = ctx->cstack.as<GCharge>();
-            a.cstack_cap = ctx->cstack_cap;
-        }
-        if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
-    }
-    if (d->keep_hits) ctx->hit_cap = std::max<uint64_t>(ctx->hit_cap, hit_cap);
-    if (hc.err) return fail(ctx, CMPMC_ERR_DEVICE, "transport kernel reported error word " + std::to_string(hc.err));
-
-    // ---- merge ------------------------------------------------------------------------
-    const uint64_t n_hits = d->keep_hits ? hc.hit_count : 0;
-    CK(ctx->hits_out.ensure(std::max<uint64_t>(n_hits, 1) * sizeof(cmpmc_sensor_hit)), "alloc hits");
-    uint64_t* ev_offsets = batched ? ctx->ev_offsets.as<uint64_t>() : ctx->offsets.as<uint64_t>();
-    cmpmc_sim_stats* ev_stats = batched ? ctx->ev_stats2.as<cmpmc_sim_stats>() : ctx->ev_stats.as<cmpmc_sim_stats>();
-    if (n > 0 && batched) {
-        CK(launch_batched_finish(a, n, a.ph_off, a.injected, ctx->offsets.as<uint64_t>(), ev_offsets,
-                                 ctx->hits_out.as<cmpmc_sensor_hit>(), n_hits, ctx->total.as<cmpmc_sim_stats>(),
-                                 ctx->partials.as<cmpmc_sim_stats>(), d->want_event_stats ? ev_stats : nullptr, s,
-                                 &launches),
-           "merge kernels");
-    } else if (n > 0) {
-        CK(launch_finish(a, ctx->offsets.as<uint64_t>(), ctx->hits_out.as<cmpmc_sensor_hit>(), n_hits,
-                         ctx->total.as<cmpmc_sim_stats>(), ctx->partials.as<cmpmc_sim_stats>(), s, &launches),
-           "merge kernels");
+    uint64_t n_hits = 0;
+    uint64_t* ev_offsets = nullptr;
+    cmpmc_sim_stats* ev_stats = nullptr;
+    if (batched && n_ch > 0) {
+        // carriers and their Luke phonons: alternating charge / queue phases, event sinks
+        const int st = run_charges_batched(ctx, d, a, n, n_ph, n_ch, launches, hc, kms, n_hits, ev_offsets, ev_stats);
+        if (st != CMPMC_OK) return st;
     } else {
-        CK(cudaMemsetAsync(ev_offsets, 0, 8, s), "memset offsets");
-        CK(cudaMemsetAsync(ctx->total.p, 0, sizeof(cmpmc_sim_stats), s), "memset totals");
+
+        // ---- work units: events (plain form) or primary phonons (batched form) ---------
+        const uint64_t units = batched ? n_ph : n;
+        a.n_events = units;
+        int bps = ctx->bps;
+        if (!bps) {
+            CK(batched ? batched_fp32_occupancy(ctx->tpb, &bps) : plain_fp64_occupancy(ctx->tpb, &bps), "occupancy");
+            bps = std::max(bps, 1);
+        }
+        uint64_t grid = static_cast<uint64_t>(ctx->num_sms) * bps;
+        grid = std::min<uint64_t>(grid, (std::max<uint64_t>(units, 1) + ctx->tpb - 1) / ctx->tpb);
+        grid = std::max<uint64_t>(grid, 1);
+        const uint64_t slots = grid * ctx->tpb;
+        const size_t stack_entry = batched ? batched_stack_entry_bytes() : sizeof(GTrack);
+
+        CK(ctx->ev_stats.ensure(std::max<uint64_t>(units, 1) * sizeof(cmpmc_sim_stats)), "alloc unit stats");
+        CK(ctx->ev_nhits.ensure(std::max<uint64_t>(units, 1) * 8), "alloc unit hit counts");
+        CK(ctx->offsets.ensure((units + 1) * 8), "alloc unit offsets");
+        CK(ctx->counters.ensure(sizeof(Counters)), "alloc counters");
+        CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
+        CK(ctx->partials.ensure(kReducePartials * sizeof(cmpmc_sim_stats)), "alloc partial totals");
+        CK(ctx->h_counters.ensure(sizeof(Counters)), "alloc host counters");
+        CK(ctx->cstack.ensure(slots * ctx->cstack_cap * sizeof(GCharge)), "alloc charge stacks");
+        if (batched) {
+            CK(ctx->unit_event.ensure(std::max<uint64_t>(units, 1) * 4), "alloc unit map");
+            CK(ctx->ev_offsets.ensure((n + 1) * 8), "alloc event offsets");
+            if (d->want_event_stats) CK(ctx->ev_stats2.ensure(std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats)),
+                                        "alloc event stats");
+            if (n > 0) {
+                CK(launch_unit_event(a.ph_off, n, ctx->unit_event.as<uint32_t>(), s), "unit map");
+                ++launches;
+            }
+        }
+        a.cstack = ctx->cstack.as<GCharge>();
+        a.cstack_cap = ctx->cstack_cap;
+        a.ev_stats = ctx->ev_stats.as<cmpmc_sim_stats>();
+        a.ev_nhits = ctx->ev_nhits.as<uint64_t>();
+        Counters* dc = ctx->counters.as<Counters>();
+        a.hit_count = &dc->hit_count;
+        a.next_work = &dc->next_work;
+        a.err = &dc->err;
+
+        uint64_t hit_cap = ctx->hit_cap;
+        if (!hit_cap) hit_cap = std::max<uint64_t>(4096, std::max<uint64_t>(n, n_ph + n_ch) * 32);
+        uint32_t& stack_cap = batched ? ctx->stack_cap_batched : ctx->stack_cap;
+        for (int attempt = 0;; ++attempt) {
+            if (!d->keep_hits) hit_cap = 1;
+            CK(ctx->stack.ensure(slots * stack_cap * stack_entry), "alloc phonon stacks");
+            CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
+            CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
+            a.stack = ctx->stack.as<GTrack>();
+            a.stack_cap = stack_cap;
+            a.hit_stage = ctx->hit_stage.as<cmpmc_sensor_hit>();
+            a.hit_key = ctx->hit_key.as<uint64_t>();
+            a.hit_cap = hit_cap;
+            CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s), "memset counters");
+            CK(cudaEventRecord(ctx->e_k0, s), "event");
+            if (units > 0) {
+                CK(batched ? launch_batched_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->unit_event.as<uint32_t>(),
+                                                 static_cast<int>(grid), ctx->tpb, s)
+                           : launch_plain_fp64(ctx->L, ctx->D, a, static_cast<int>(grid), ctx->tpb, s),
+                   "transport launch");
+                ++launches;
+            }
+            CK(cudaEventRecord(ctx->e_k1, s), "event");
+            CK(cudaMemcpyAsync(ctx->h_counters.p, ctx->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s),
+               "copy counters");
+            CK(cudaStreamSynchronize(s), "transport kernel");
+            hc = *ctx->h_counters.as<Counters>();
+            CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
+            const bool stack_over = (hc.err & (kErrPhononStack | kErrChargeStack)) != 0;
+            const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
+            if (!stack_over && !hits_over) break;
+            if (attempt >= 10) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack or hit buffer overflow persists");
+            if (hc.err & kErrPhononStack) stack_cap = std::min<uint32_t>(stack_cap * 8, 1u << 24);
+            if (hc.err & kErrChargeStack) {
+                ctx->cstack_cap = std::min<uint32_t>(ctx->cstack_cap * 8, 1u << 20);
+                CK(ctx->cstack.ensure(slots * ctx->cstack_cap * sizeof(GCharge)), "alloc charge stacks");
+                a.cstack = ctx->cstack.as<GCharge>();
+                a.cstack_cap = ctx->cstack_cap;
+            }
+            if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
+        }
+        if (d->keep_hits) ctx->hit_cap = std::max<uint64_t>(ctx->hit_cap, hit_cap);
+        if (hc.err) return fail(ctx, CMPMC_ERR_DEVICE, "transport kernel reported error word " + std::to_string(hc.err));
+
+        // ---- merge ------------------------------------------------------------------------
+        n_hits = d->keep_hits ? hc.hit_count : 0;
+        CK(ctx->hits_out.ensure(std::max<uint64_t>(n_hits, 1) * sizeof(cmpmc_sensor_hit)), "alloc hits");
+        ev_offsets = batched ? ctx->ev_offsets.as<uint64_t>() : ctx->offsets.as<uint64_t>();
+        ev_stats = batched ? ctx->ev_stats2.as<cmpmc_sim_stats>() : ctx->ev_stats.as<cmpmc_sim_stats>();
+        if (n > 0 && batched) {
+            CK(launch_batched_finish(a, n, a.ph_off, a.injected, ctx->offsets.as<uint64_t>(), ev_offsets,
+                                     ctx->hits_out.as<cmpmc_sensor_hit>(), n_hits, ctx->total.as<cmpmc_sim_stats>(),
+                                     ctx->partials.as<cmpmc_sim_stats>(), d->want_event_stats ? ev_stats : nullptr, s,
+                                     &launches),
+               "merge kernels");
+        } else if (n > 0) {
+            CK(launch_finish(a, ctx->offsets.as<uint64_t>(), ctx->hits_out.as<cmpmc_sensor_hit>(), n_hits,
+                             ctx->total.as<cmpmc_sim_stats>(), ctx->partials.as<cmpmc_sim_stats>(), s, &launches),
+               "merge kernels");
+        } else {
+            CK(cudaMemsetAsync(ev_offsets, 0, 8, s), "memset offsets");
+            CK(cudaMemsetAsync(ctx->total.p, 0, sizeof(cmpmc_sim_stats), s), "memset totals");
+        }
     }
     CK(ctx->h_total.ensure(sizeof(cmpmc_sim_stats)), "alloc host totals");
     CK(cudaMemcpyAsync(ctx->h_total.p, ctx->total.p, sizeof(cmpmc_sim_stats), cudaMemcpyDeviceToHost, s),

@@ -13,6 +13,7 @@ enum : unsigned {
     kErrPhononStack = 1u,
     kErrChargeStack = 2u,
     kErrQueue = 4u,
+    kErrResume = 8u,
 };
 
 // A pushed phonon in a per-thread global-memory LIFO (112 B, 16-byte aligned)
@@ -59,6 +60,51 @@ struct RunArgs {
     cmpmc_sim_stats* ev_stats;        // [n]
     uint64_t* ev_nhits;               // [n]
     unsigned* err;
+    // event sink (batched form with charges): units add their counters to ev_stats[event]
+    // and their hit counts to ev_nhits[event]; staged hits carry the event as key
+    int ev_sink;
+};
+
+// Luke-phonon queue entry of the batched charge form (64 B). ev == kQEmpty marks a slot
+// that was reserved but not filled.
+constexpr uint32_t kQEmpty = 0xffffffffu;
+struct alignas(16) QPhonon {
+    float px, py, pz, kx, ky, kz;
+    float w;
+    uint32_t mode;
+    double E, t;
+    uint64_t key;  // substream key of this phonon
+    uint32_t ev;   // event index within the call
+    uint32_t pad;
+};
+
+// A carrier of the batched charge form between phases (96 B): a carrier whose queue
+// reservation failed is parked here with its generator state and resumed next phase.
+struct alignas(16) QCharge {
+    float px, py, pz, qx, qy, qz, ekin, w;
+    double t;
+    uint64_t ckey;      // lineage key: Luke phonon i of this carrier uses mix(ckey, i)
+    uint32_t rng[4];
+    uint32_t ev, luke_idx, n_knock;
+    int32_t hint;       // mesh walk hint
+    uint32_t valley_type;  // valley | type << 16
+    uint32_t pad[3];
+};
+
+struct ChargeArgs {
+    uint64_t n_carriers;              // initial carriers (RunArgs::ch)
+    const uint32_t* carrier_event;    // [n_carriers]
+    uint64_t carrier_seed;            // substream seed of the carriers
+    QPhonon* queue;
+    uint64_t q_cap;
+    unsigned long long* q_tail;
+    const QCharge* resume_in;
+    uint64_t n_resume_in;
+    unsigned long long* resume_next;
+    QCharge* resume_out;
+    uint64_t resume_cap;
+    unsigned long long* n_resume_out;
+    unsigned long long* next_carrier;
 };
 
 // Adjoint of a binned hit-time histogram (batched FP32 form, k_adjoint_fp32)
@@ -172,6 +218,20 @@ cudaError_t launch_batched_finish(const RunArgs& a, uint64_t n_events, const uin
                                   cmpmc_sim_stats* partials, cmpmc_sim_stats* ev_stats_out, cudaStream_t s,
                                   int* launches);
 cudaError_t launch_math_check(uint64_t n, const double* x, double* out);
+// batched charge form: carriers (FP32 drift) filling the Luke-phonon queue, then the
+// phonon kernel over the queue entries; both add to per-event sinks
+cudaError_t launch_charges_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
+                                const ChargeArgs& c, int grid, int block, cudaStream_t s);
+cudaError_t charges_fp32_occupancy(int block, int* blocks_per_sm);
+cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
+                              const QPhonon* queue, int grid, int block, cudaStream_t s);
+cudaError_t launch_carrier_event(const uint64_t* ch_off, uint64_t n_events, uint32_t* carrier_event,
+                                 cudaStream_t s);
+// merge of the event-sink runs: injected energies, hit offsets, hits into event order
+// (order within an event follows staging), run totals
+cudaError_t launch_sink_finish(const RunArgs& a, uint64_t n_events, uint64_t* ev_offsets,
+                               unsigned long long* cursor, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
+                               cmpmc_sim_stats* total, cmpmc_sim_stats* partials, cudaStream_t s, int* launches);
 constexpr int kReducePartials = 592;  // blocks of the first reduction level
 cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
                           cmpmc_sim_stats* total, cmpmc_sim_stats* partials, cudaStream_t s, int* launches);

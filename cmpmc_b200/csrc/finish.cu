@@ -56,6 +56,28 @@ __global__ void k_scatter(const cmpmc_sensor_hit* __restrict__ stage, const uint
     }
 }
 
+// event-sink runs: staged hits carry their event; each lands at the event's offset plus a
+// per-event cursor (within an event the order is the staging order)
+__global__ void k_scatter_sink(const cmpmc_sensor_hit* __restrict__ stage, const uint64_t* __restrict__ key,
+                               const unsigned long long* __restrict__ count, uint64_t stage_cap,
+                               const uint64_t* __restrict__ offsets, unsigned long long* __restrict__ cursor,
+                               cmpmc_sensor_hit* __restrict__ out, uint64_t out_cap) {
+    const uint64_t n = min(static_cast<uint64_t>(*count), stage_cap);
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t ev = key[i];
+        const uint64_t dst = offsets[ev] + atomicAdd(cursor + ev, 1ull);
+        if (dst < out_cap) out[dst] = stage[i];
+    }
+}
+
+__global__ void k_set_injected(cmpmc_sim_stats* __restrict__ ev_stats, const double* __restrict__ injected,
+                               uint64_t n) {
+    for (uint64_t ev = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; ev < n;
+         ev += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        ev_stats[ev].total_injected_eV = injected[ev];
+}
+
 // Block b reduces records [b n / B, (b + 1) n / B) into total[b] in a fixed order (each
 // thread a contiguous slice, then a tree over the threads).
 __global__ void __launch_bounds__(kReduceThreads) k_reduce_stats(const cmpmc_sim_stats* __restrict__ ev_all,
@@ -240,6 +262,29 @@ cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit*
         *launches += 1;
     }
     return launch_reduce_stats(a.ev_stats, a.n_events, partials, total, s, launches);
+}
+
+cudaError_t launch_sink_finish(const RunArgs& a, uint64_t n_events, uint64_t* ev_offsets,
+                               unsigned long long* cursor, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
+                               cmpmc_sim_stats* total, cmpmc_sim_stats* partials, cudaStream_t s, int* launches) {
+    if (n_events == 0) {
+        cudaError_t e = cudaMemsetAsync(ev_offsets, 0, 8, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(total, 0, sizeof(cmpmc_sim_stats), s);
+        return e;
+    }
+    k_set_injected<<<148, 256, 0, s>>>(a.ev_stats, a.injected, n_events);
+    k_scan<<<1, kScanThreads, 0, s>>>(a.ev_nhits, n_events, ev_offsets);
+    *launches += 2;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (a.keep_hits) {
+        k_scatter_sink<<<4 * 148, 256, 0, s>>>(a.hit_stage, a.hit_key, a.hit_count, a.hit_cap, ev_offsets, cursor,
+                                               hits_out, out_cap);
+        *launches += 1;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return launch_reduce_stats(a.ev_stats, n_events, partials, total, s, launches);
 }
 
 cudaError_t launch_reduce_stats(const cmpmc_sim_stats* rec, uint64_t n, cmpmc_sim_stats* partials,

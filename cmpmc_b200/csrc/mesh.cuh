@@ -35,6 +35,22 @@ struct MeshView {
     int32_t n_tets;
 };
 
+// FP32 copy of a record for the batched charge form (80 B): the same fields rounded to
+// float, laid out so the walk reads them as four float4 loads.
+struct alignas(16) MeshTet32 {
+    float tinv[9];
+    float x3[3];
+    float e[3];
+    int32_t nb[4];
+    float pad;
+};
+static_assert(sizeof(MeshTet32) == 80, "FP32 mesh record layout");
+
+struct MeshView32 {
+    const MeshTet32* tet;
+    int32_t n_tets;
+};
+
 // TriLinearMesh3D::bary_coord (mesh_field.hpp:239-246)
 CMPMC_HD void mesh_bary(const MeshTet& t, V3 p, double b[4]) {
     const double dx = p.x - t.x3[0];

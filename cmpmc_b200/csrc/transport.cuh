@@ -27,7 +27,8 @@ struct Detector {
     double charge_max_dk_frac, charge_dt_cap_s, charge_sampling_dk_frac;
     int charge_stepping;
     double fermi_level_above_Ev_eV;
-    MeshView mesh;  // DetectorModel::mesh_field_3d on the device (tet == nullptr: uniform field)
+    MeshView mesh;      // DetectorModel::mesh_field_3d on the device (tet == nullptr: uniform field)
+    MeshView32 mesh32;  // the same mesh in FP32 (batched charge form)
 };
 
 // Phonon state held in registers (PhononTrack, track.hpp:62-72)

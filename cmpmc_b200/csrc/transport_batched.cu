@@ -23,134 +23,11 @@
 #include <type_traits>
 
 #include "device.cuh"
+#include "fp32.cuh"
 
 namespace cmpmc_gpu {
 
 namespace {
-
-constexpr float kNudge = 1e-8f;  // inward displacement after a boundary event (m)
-constexpr float kTwoPiF = 6.28318530717958648f;
-
-struct F3 {
-    float x, y, z;
-};
-__device__ __forceinline__ F3 f3(float x, float y, float z) { return F3{x, y, z}; }
-__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
-__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
-__device__ __forceinline__ F3 operator*(F3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
-__device__ __forceinline__ float fdot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ F3 fcross(F3 a, F3 b) {
-    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
-}
-__device__ __forceinline__ F3 funit(F3 a) {
-    const float n2 = fdot(a, a);
-    if (n2 <= 0.0f) return f3(0.0f, 0.0f, 1.0f);
-    return a * rsqrtf(n2);
-}
-__device__ __forceinline__ F3 frotate(F3 v, F3 k, float c, float s) {
-    return v * c + fcross(k, v) * s + k * (fdot(k, v) * (1.0f - c));
-}
-__device__ __forceinline__ F3 forth(F3 v) {
-    const F3 a = (fabsf(v.x) < 0.9f) ? f3(1.0f, 0.0f, 0.0f) : f3(0.0f, 1.0f, 0.0f);
-    return funit(fcross(v, a));
-}
-
-// xoshiro128** (Blackman and Vigna) per substream; FP32 uniforms in (0, 1) with 24 bits and
-// FP64 uniforms with 53 bits for the Kaplan cascade
-struct R128 {
-    uint32_t s0, s1, s2, s3;
-    __device__ __forceinline__ void seed(uint64_t key) {
-        uint64_t z = key;
-        const uint64_t a = splitmix_step(z += 0x9e3779b97f4a7c15ULL);
-        const uint64_t b = splitmix_step(z += 0x9e3779b97f4a7c15ULL);
-        s0 = static_cast<uint32_t>(a);
-        s1 = static_cast<uint32_t>(a >> 32);
-        s2 = static_cast<uint32_t>(b);
-        s3 = static_cast<uint32_t>(b >> 32) | 1u;  // never all zero
-    }
-    __device__ __forceinline__ uint32_t next() {
-        const uint32_t r = __funnelshift_l(s1 * 5u, s1 * 5u, 7) * 9u;
-        const uint32_t t = s1 << 9;
-        s2 ^= s0;
-        s3 ^= s1;
-        s1 ^= s2;
-        s0 ^= s3;
-        s2 ^= t;
-        s3 = __funnelshift_l(s3, s3, 11);
-        return r;
-    }
-    __device__ __forceinline__ float u() {
-        return __uint2float_rn(((next() >> 9) << 1) | 1u) * 5.9604644775390625e-8f;  // (2m+1) / 2^24
-    }
-    __device__ __forceinline__ double uniform() {  // 53-bit, for the FP64 cascade
-        const uint64_t x = (static_cast<uint64_t>(next()) << 21) ^ (next() >> 11);
-        return static_cast<double>(x | 1ULL) * (1.0 / 9007199254740992.0);
-    }
-};
-
-// FP32 view of the crystal (scaled so that rates stay in FP32 range)
-struct FLat {
-    const float4* oct;
-    const float* cdf_lt;
-    const float* cdf_tt;
-    float o[9];
-    float inv_h_thz;  // E[eV] -> nu[THz]
-    float b4, a5;     // B_iso * 1e48, A_anh * 1e60 (nu in THz)
-    float poly_inv;   // 1 / polycrystal mfp (0 disables)
-    float fL, fLST, p_st_trans, fTT;
-    float m_ratio;    // v_L / v_T
-    // per surface: constant reflection split (1 when the polynomials do not depend on energy)
-    int split_const[3];
-    float p_anh[3], p_anh_spec[3];
-};
-
-struct FKin {
-    F3 dir;
-    float mag;
-};
-
-__device__ __forceinline__ FKin fmap(const FLat& L, int mode, F3 k) {
-    const F3 kc = f3(L.o[0] * k.x + L.o[3] * k.y + L.o[6] * k.z, L.o[1] * k.x + L.o[4] * k.y + L.o[7] * k.z,
-                     L.o[2] * k.x + L.o[5] * k.y + L.o[8] * k.z);
-    const float l1 = fabsf(kc.x) + fabsf(kc.y) + fabsf(kc.z);
-    const float inv = (l1 > 1e-18f) ? __frcp_rn(l1) : 1.0f;
-    float px = kc.x * inv, py = kc.y * inv;
-    if (kc.z < 0.0f) {
-        const float ox = (1.0f - fabsf(py)) * (px >= 0.0f ? 1.0f : -1.0f);
-        const float oy = (1.0f - fabsf(px)) * (py >= 0.0f ? 1.0f : -1.0f);
-        px = ox;
-        py = oy;
-    }
-    const float u = (fminf(fmaxf(px, -1.0f), 1.0f) + 1.0f) * 127.5f;
-    const float v = (fminf(fmaxf(py, -1.0f), 1.0f) + 1.0f) * 127.5f;
-    const int i0 = min(max(static_cast<int>(u), 0), kNOct - 2);
-    const int j0 = min(max(static_cast<int>(v), 0), kNOct - 2);
-    const float du = u - i0, dv = v - j0;
-    const int base = (mode * kNOct + i0) * kNOct + j0;
-    const float4 e00 = __ldg(L.oct + base), e01 = __ldg(L.oct + base + 1);
-    const float4 e10 = __ldg(L.oct + base + kNOct), e11 = __ldg(L.oct + base + kNOct + 1);
-    const float w00 = (1.0f - du) * (1.0f - dv), w10 = du * (1.0f - dv), w01 = (1.0f - du) * dv, w11 = du * dv;
-    const F3 vc = f3(e00.x * w00 + e10.x * w10 + e01.x * w01 + e11.x * w11,
-                     e00.y * w00 + e10.y * w10 + e01.y * w01 + e11.y * w11,
-                     e00.z * w00 + e10.z * w10 + e01.z * w01 + e11.z * w11);
-    const float mag = sqrtf(fdot(vc, vc));
-    const F3 vn = vc * __frcp_rn(fmaxf(mag, 1e-12f));
-    FKin r;
-    r.dir = f3(L.o[0] * vn.x + L.o[1] * vn.y + L.o[2] * vn.z, L.o[3] * vn.x + L.o[4] * vn.y + L.o[5] * vn.z,
-               L.o[6] * vn.x + L.o[7] * vn.y + L.o[8] * vn.z);
-    r.mag = mag;
-    return r;
-}
-
-__device__ __forceinline__ int fdos(const FLat& L, float u) { return (u < L.fL) ? 0 : ((u < L.fLST) ? 2 : 1); }
-__device__ __forceinline__ int ftrans(const FLat& L, R128& g) { return (g.u() < L.p_st_trans) ? 2 : 1; }
-__device__ __forceinline__ float fcdf(const float* cdf, R128& g) {
-    const float u = g.u() * (kNCdf - 1);
-    const int i = min(static_cast<int>(u), kNCdf - 2);
-    const float f = u - i;
-    return __ldg(cdf + i) * (1.0f - f) + __ldg(cdf + i + 1) * f;
-}
-__device__ __forceinline__ float facos_clamped(float c) { return acosf(fminf(fmaxf(c, -1.0f), 1.0f)); }
 
 struct FTrack {
     F3 pos, k, vg;
@@ -190,61 +67,6 @@ __device__ __forceinline__ void inherit(TrackOf<kAdj>& d, const TrackOf<kAdj>& p
 #pragma unroll
         for (int i = 0; i < 4; ++i) d.s[i] = parent.s[i];
     }
-}
-
-// inward Lambertian wavevector whose group velocity points inward (engine.hpp:927-936)
-__device__ __forceinline__ F3 finward(const FLat& L, int mode, F3 n, R128& g, FKin& kin) {
-    const F3 a = forth(n);
-    const F3 b = fcross(n, a);
-    for (int trial = 0; trial < 16; ++trial) {
-        const float phi = kTwoPiF * g.u();
-        const float st = sqrtf(g.u());
-        const float ct = sqrtf(fmaxf(0.0f, 1.0f - st * st));
-        float s, c;
-        __sincosf(phi, &s, &c);
-        const F3 kd = funit(a * (st * c) + b * (st * s) + n * ct);
-        kin = fmap(L, mode, kd);
-        if (fdot(kin.dir, n) > 1e-6f) return kd;
-    }
-    kin = fmap(L, mode, n);
-    return n;
-}
-
-struct FBHit {
-    float d;
-    F3 n;
-    int surf;
-};
-
-__device__ __forceinline__ FBHit fexit(float R, float H, F3 p, F3 v) {
-    float t = __int_as_float(0x7f800000);
-    int surf = 2;
-    if (v.z > 1e-15f) {
-        const float tz = (H - p.z) / v.z;
-        if (tz >= 0.0f && tz < t) { t = tz; surf = 0; }
-    } else if (v.z < -1e-15f) {
-        const float tz = (-H - p.z) / v.z;
-        if (tz >= 0.0f && tz < t) { t = tz; surf = 1; }
-    }
-    const float a = v.x * v.x + v.y * v.y;
-    if (a > 1e-18f) {
-        const float b = p.x * v.x + p.y * v.y;
-        const float c = p.x * p.x + p.y * p.y - R * R;
-        const float disc = fmaxf(0.0f, b * b - a * c);
-        const float tr = (-b + sqrtf(disc)) / a;
-        if (tr >= 0.0f && tr < t) { t = tr; surf = 2; }
-    }
-    FBHit h;
-    h.d = fmaxf(0.0f, t);
-    h.surf = surf;
-    if (surf == 0) h.n = f3(0.0f, 0.0f, -1.0f);
-    else if (surf == 1) h.n = f3(0.0f, 0.0f, 1.0f);
-    else {
-        const F3 hp = p + v * h.d;
-        const float r = sqrtf(hp.x * hp.x + hp.y * hp.y);
-        h.n = (r > 1e-15f) ? f3(-hp.x / r, -hp.y / r, 0.0f) : f3(-1.0f, 0.0f, 0.0f);
-    }
-    return h;
 }
 
 template <bool kAdj>
@@ -395,12 +217,42 @@ __device__ __forceinline__ void write_unit(const RunArgs& a, uint64_t unit, cons
     a.ev_nhits[unit] = a.keep_hits ? n_hits : 0;
 }
 
+// event sink: a finished unit adds its counters to its event (units of one event run on
+// many threads; the doubles are FP64 atomics, so their last bits depend on the order)
+__device__ __forceinline__ void add_u64(unsigned long long* p, uint32_t v) {
+    if (v) atomicAdd(p, static_cast<unsigned long long>(v));
+}
+__device__ __forceinline__ void add_f64(double* p, double v) {
+    if (v != 0.0) atomicAdd(p, v);
+}
+__device__ __noinline__ void sink_unit(const RunArgs* a, uint32_t ev, const UStats* stp) {
+    const UStats& st = *stp;
+    cmpmc_sim_stats& o = a->ev_stats[ev];
+    add_u64(reinterpret_cast<unsigned long long*>(&o.total_steps), st.steps);
+    add_u64(reinterpret_cast<unsigned long long*>(&o.isotope_scatters), st.iso);
+    add_u64(reinterpret_cast<unsigned long long*>(&o.polycrystal_scatters), st.poly);
+    add_u64(reinterpret_cast<unsigned long long*>(&o.decays_L_to_TT), st.tt);
+    add_u64(reinterpret_cast<unsigned long long*>(&o.decays_L_to_LT), st.lt);
+    add_u64(reinterpret_cast<unsigned long long*>(&o.surface_refls), st.refl);
+    add_u64(reinterpret_cast<unsigned long long*>(&o.surface_downconversions), st.down);
+    add_u64(reinterpret_cast<unsigned long long*>(&o.sensor_hits), st.hits);
+    add_u64(reinterpret_cast<unsigned long long*>(&o.killed_tracks), st.killed);
+    add_f64(&o.total_deposited_eV, st.dep);
+    add_f64(&o.escaped_or_killed_eV, st.esc);
+}
+
+enum { kSrcInput = 0, kSrcQueue = 1 };
+
 // The step loop of both batched kernels. kAdj adds the score bookkeeping of the adjoint
 // (every decision's d log p / d log theta, carried per track and inherited by daughters)
 // and bins hits into the time histogram instead of writing hit records.
-template <bool kAdj>
+// kSrc selects where units come from: the caller's primary phonon records (kSrcInput,
+// substream (event << 20 | index)) or the Luke-phonon queue of the charge form
+// (kSrcQueue, the entry's own substream key; empty slots are skipped).
+template <bool kAdj, int kSrc = kSrcInput>
 __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, const RunArgs& a,
-                                             const uint32_t* __restrict__ unit_event, const AdjArgs& adj,
+                                             const uint32_t* __restrict__ unit_event,
+                                             const QPhonon* __restrict__ queue, const AdjArgs& adj,
                                              float* s_w, float* s_hist) {
     const uint64_t slot = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     double refl_buf[kKaplanCap];
@@ -417,6 +269,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
     UStats st;
     uint32_t n_hits = 0;
     uint64_t unit = ~0ull;
+    uint32_t ev_cur = 0;  // event of the unit in flight
     bool live = false;  // trk holds a track in flight
     for (;;) {
         if (!live) {
@@ -424,10 +277,37 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 pop_track<kAdj>(stk, n_stk, trk);
                 live = true;
             } else {
-                if (unit != ~0ull) write_unit(a, unit, st, n_hits);
+                if (unit != ~0ull) {
+                    if (a.ev_sink) sink_unit(&a, ev_cur, &st);
+                    else write_unit(a, unit, st, n_hits);
+                }
                 unit = atomicAdd(a.next_work, 1ull);
                 if (unit >= a.n_events) break;
+                if constexpr (kSrc == kSrcQueue) {
+                    const QPhonon q = queue[unit];
+                    if (q.ev == kQEmpty) {
+                        unit = ~0ull;
+                        continue;
+                    }
+                    ev_cur = q.ev;
+                    g.seed(q.key);
+                    trk.pos = f3(q.px, q.py, q.pz);
+                    trk.k = f3(q.kx, q.ky, q.kz);
+                    trk.mode = static_cast<int>(q.mode);
+                    const FKin kin = fmap(L, trk.mode, trk.k);
+                    trk.vg = kin.dir;
+                    trk.vmag = kin.mag;
+                    trk.E = q.E;
+                    trk.t = q.t;
+                    trk.w = q.w;
+                    trk.bounces = 0;
+                    st = UStats{0, 0, 0, 0, 0, 0, 0, 0, 0, 0.0, 0.0};
+                    n_hits = 0;
+                    live = true;
+                    continue;
+                }
                 const uint32_t ev = unit_event[unit];
+                ev_cur = ev;
                 const uint64_t j = unit - a.ph_off[ev];
                 g.seed(seed_key ^ mix64(((a.first_event + ev) << 20) | j));
                 const cmpmc_phonon_track& in = a.ph[unit];
@@ -535,6 +415,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                             }
                         }
                     } else if (a.keep_hits) {
+                        if (a.ev_sink) atomicAdd(reinterpret_cast<unsigned long long*>(a.ev_nhits + ev_cur), 1ull);
                         const unsigned long long idx = atomicAdd(a.hit_count, 1ull);
                         if (idx < a.hit_cap) {
                             cmpmc_sensor_hit r;
@@ -548,7 +429,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                             r._pad = 0;
                             r.channel_id = -1;
                             a.hit_stage[idx] = r;
-                            a.hit_key[idx] = (unit << 32) | local;
+                            a.hit_key[idx] = a.ev_sink ? static_cast<uint64_t>(ev_cur) : ((unit << 32) | local);
                         }
                     }
                 }
@@ -672,7 +553,16 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
                                                          const __grid_constant__ RunArgs a,
                                                          const uint32_t* __restrict__ unit_event) {
     const AdjArgs none{};
-    batched_loop<false>(L, D, a, unit_event, none, nullptr, nullptr);
+    batched_loop<false>(L, D, a, unit_event, nullptr, none, nullptr, nullptr);
+}
+
+// The Luke-phonon queue of the batched charge form: one unit per queue entry
+__global__ void __launch_bounds__(128, 8) k_queue_fp32(const __grid_constant__ FLat L,
+                                                       const __grid_constant__ Detector D,
+                                                       const __grid_constant__ RunArgs a,
+                                                       const QPhonon* __restrict__ queue) {
+    const AdjArgs none{};
+    batched_loop<false, kSrcQueue>(L, D, a, nullptr, queue, none, nullptr, nullptr);
 }
 
 // Adjoint of the hit-time histogram: the batched transport with per-track scores. Bin
@@ -690,44 +580,13 @@ __global__ void __launch_bounds__(128, 6) k_adjoint_fp32(const __grid_constant__
         s_hist[b] = 0.0f;
     }
     __syncthreads();
-    batched_loop<true>(L, D, a, unit_event, adj, s_w, s_hist);
+    batched_loop<true>(L, D, a, unit_event, nullptr, adj, s_w, s_hist);
     __syncthreads();
     for (int b = threadIdx.x; b < adj.n_bins; b += blockDim.x)
         if (s_hist[b] != 0.0f) atomicAdd(adj.hist + b, static_cast<double>(s_hist[b]));
 }
 
 }  // namespace
-
-// FP32 constants of the crystal derived from the FP64 lattice view
-static FLat make_flat(const Lattice& L, const float* cdf_f, const Detector& D) {
-    FLat f;
-    f.oct = reinterpret_cast<const float4*>(L.oct);
-    f.cdf_lt = cdf_f;
-    f.cdf_tt = cdf_f + kNCdf;
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) f.o[3 * i + j] = static_cast<float>(L.orient.m[i][j]);
-    f.inv_h_thz = static_cast<float>(1.0 / (kHPlanck * 1e12));
-    f.b4 = static_cast<float>(L.B_iso * 1e48);
-    f.a5 = static_cast<float>(L.A_anh * 1e60);
-    f.poly_inv = (L.poly_mfp > 0.0) ? static_cast<float>(1.0 / L.poly_mfp) : 0.0f;
-    f.fL = static_cast<float>(L.fLDOS);
-    f.fLST = static_cast<float>(L.fLDOS + L.fSTDOS);
-    f.p_st_trans = static_cast<float>(L.fSTDOS / (L.fSTDOS + L.fFTDOS));
-    f.fTT = static_cast<float>(L.fTT_frac);
-    f.m_ratio = static_cast<float>(L.v_sound / L.v_trans);
-    for (int i = 0; i < 3; ++i) {
-        const Surface& s = D.surf[i];
-        // the split is energy independent when every polynomial is constant (or absent)
-        const bool cst = s.n_spec <= 1 && s.n_diff <= 1 && s.n_anh <= 1;
-        f.split_const[i] = cst ? 1 : 0;
-        // constant polynomials still switch at the cut-offs; evaluate below and above them
-        const Split lo = reflection_split(s, 1e-6), hi = reflection_split(s, 1.0);
-        if (cst && (lo.p_anh != hi.p_anh || lo.p_spec != hi.p_spec)) f.split_const[i] = 0;
-        f.p_anh[i] = static_cast<float>(lo.p_anh);
-        f.p_anh_spec[i] = static_cast<float>(lo.p_anh + lo.p_spec);
-    }
-    return f;
-}
 
 cudaError_t launch_unit_event(const uint64_t* ph_off, uint64_t n_events, uint32_t* unit_event, cudaStream_t s) {
     k_unit_event<<<4 * 148, 128, 0, s>>>(ph_off, n_events, unit_event);
@@ -745,6 +604,12 @@ cudaError_t batched_fp32_occupancy(int block, int* blocks_per_sm) {
 }
 
 size_t batched_stack_entry_bytes() { return sizeof(GFTrack); }
+
+cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
+                              const QPhonon* queue, int grid, int block, cudaStream_t s) {
+    k_queue_fp32<<<grid, block, 0, s>>>(make_flat(L, cdf_f, D), D, a, queue);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_adjoint_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                                 const AdjArgs& adj, const uint32_t* unit_event, int grid, int block, cudaStream_t s) {

@@ -277,7 +277,10 @@ typedef struct cmpmc_gpu_ctx cmpmc_gpu_ctx;
 
 enum {
     CMPMC_FORM_PLAIN_FP64   = 0,   /* bit-exact event streams, one event per device thread   */
-    CMPMC_FORM_BATCHED_FP32 = 1    /* per-primary substreams, FP32 geometry, FP64 ledger/time */
+    CMPMC_FORM_BATCHED_FP32 = 1    /* per-primary substreams, FP32 geometry, FP64 ledger/time;
+                                      with charges: per-carrier substreams, FP32 drift, Luke
+                                      phonons through a device queue (hits of an event in
+                                      no fixed order, FP64 event sums by atomics)           */
 };
 
 typedef struct cmpmc_run_desc {
@@ -324,6 +327,11 @@ int cmpmc_gpu_last_error(const cmpmc_gpu_ctx* ctx, char* buf, size_t size);
 int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_per_sm,
                         uint64_t stack_capacity, uint64_t hit_capacity);
 int cmpmc_gpu_device_count(int* count);
+/* Batched FP32 form with charges: capacity of the device Luke-phonon queue in entries
+ * (64 B each, default 2^24). Carriers queue their tracked Luke phonons there; when it is
+ * full they are parked and resumed after the queued phonons have been transported, so a
+ * small queue only adds phases. 0 keeps the current value. */
+int cmpmc_gpu_configure_queue(cmpmc_gpu_ctx* ctx, uint64_t queue_capacity);
 /* DetectorModel::mesh_field_3d (engine.hpp:99, looked up by electric_field_at,
  * engine.hpp:151-155): copies the mesh to the context's device; the charge transport then
  * takes its field from the mesh instead of the uniform e_field. NULL detaches it. Each

@@ -103,10 +103,3 @@ def test_batched_deterministic(ge_lattice):
     assert a.stats.record().tobytes() == b.stats.record().tobytes()
     c = _batched(eng, "c1", 100, seed=12345)
     assert a.hits.tobytes() != c.hits.tobytes()
-
-
-def test_batched_rejects_charges(ge_lattice):
-    import cmpmc_b200 as cm
-    eng = _engine(ge_lattice, "c2")
-    with pytest.raises(cm.CmpmcError):
-        cm.run_events(eng, 4, workload_of("c2"), cm.RunOptions(seed=11, form="batched_fp32"))
