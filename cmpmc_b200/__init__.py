@@ -4,14 +4,14 @@ The public API mirrors the reference's C++ API (run_events, SimulationEngine,
 CrystalLattice, DetectorModel, ...); the work runs in hand-written CUDA kernels behind
 the C ABI in include/cmpmc_gpu.h.
 """
-from .api import (AluminumFilm, CmpmcError, CrystalConfig, CrystalLattice, CylinderSolid, DetectorModel,
+from .api import (AluminumFilm, CmpmcError, ElectrodePad, ElectrodePatternMask, CrystalConfig, CrystalLattice, CylinderSolid, DetectorModel,
                   EventInput, ExcitationType, KaplanFilm, PackedEvents, PhononMode, Rng, RunOptions, RunResult,
                   SimStats, SimulationEngine, SuperconductorFilmConfig, SurfaceId, SurfaceProperty,
                   TriLinearMesh3D, UniformElectricField, UnvalidatedModuleError, Workload, materials, run_events, units, workloads)
 from .adjoint import AdjointResult, HistogramAdjoint, THETA_NAMES, default_theta
 
 __all__ = [
-    "AdjointResult", "AluminumFilm", "CmpmcError", "CrystalConfig", "CrystalLattice", "CylinderSolid", "DetectorModel", "EventInput",
+    "AdjointResult", "AluminumFilm", "CmpmcError", "ElectrodePad", "ElectrodePatternMask", "CrystalConfig", "CrystalLattice", "CylinderSolid", "DetectorModel", "EventInput",
     "ExcitationType", "KaplanFilm", "PackedEvents", "PhononMode", "Rng", "RunOptions", "RunResult", "SimStats",
     "SimulationEngine", "SuperconductorFilmConfig", "SurfaceId", "SurfaceProperty", "TriLinearMesh3D",
     "UniformElectricField",

@@ -75,6 +75,11 @@ class CrystalConfigC(C.Structure):
     ]
 
 
+class ElectrodePadC(C.Structure):
+    _fields_ = [("shape", _i32), ("channel_id", _i32), ("cx", _f64), ("cy", _f64), ("r_min", _f64), ("r_max", _f64),
+                ("phi_min", _f64), ("phi_max", _f64), ("fill_fraction", _f64)]
+
+
 class FilmConfigC(C.Structure):
     _fields_ = [
         ("film_absorption", _f64), ("film_thickness", _f64), ("v_sound", _f64), ("gap_energy", _f64),
@@ -188,6 +193,11 @@ _SIG = {
     "cmpmc_mesh_potential_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
     "cmpmc_gpu_set_mesh": (_i32, [C.c_void_p, C.c_void_p]),
     "cmpmc_gpu_configure_queue": (_i32, [C.c_void_p, _u64]),
+    "cmpmc_gpu_set_electrode_mask": (_i32, [C.c_void_p, _i32, C.c_void_p, _u64]),
+    "cmpmc_mask_supercdms_qet": (_i32, [_f64, _f64, C.c_void_p]),
+    "cmpmc_mask_rectangular_grid": (_i32, [_i32, _i32, _f64, _f64, _f64, _f64, _f64, C.c_void_p, _u64,
+                                           C.POINTER(_u64)]),
+    "cmpmc_mask_find_channel": (_i32, [C.c_void_p, _u64, C.POINTER(_f64), C.POINTER(_u64), C.POINTER(_i32)]),
     "cmpmc_gpu_run_events_noalloc": (_i32, [C.c_void_p, C.POINTER(DetectorC), _i32, _u64, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _u64,
                                             C.c_void_p, C.POINTER(SimStatsC), C.POINTER(_u64)]),

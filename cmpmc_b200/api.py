@@ -310,9 +310,83 @@ def AluminumFilm() -> SuperconductorFilmConfig:
 
 
 @dataclass
+class ElectrodePad:
+    """ElectrodePad (geometry/electrode_pattern.hpp:23-63). shape: 0 disk, 1 annular sector,
+    2 rectangle (r_min / r_max are then the half-width / half-height)."""
+    shape: int = 0
+    channel_id: int = 0
+    cx: float = 0.0
+    cy: float = 0.0
+    r_min: float = 0.0
+    r_max: float = 0.0
+    phi_min: float = 0.0
+    phi_max: float = units.two_pi
+    fill_fraction: float = 1.0
+
+    Disk, AnnularSector, Rectangle = 0, 1, 2
+
+    def to_c(self) -> _ffi.ElectrodePadC:
+        return _ffi.ElectrodePadC(int(self.shape), int(self.channel_id), self.cx, self.cy, self.r_min, self.r_max,
+                                  self.phi_min, self.phi_max, self.fill_fraction)
+
+
+class ElectrodePatternMask:
+    """ElectrodePatternMask (geometry/electrode_pattern.hpp:65-187): readout pads on a face;
+    attached to a SurfaceProperty as electrode_mask and evaluated on the device."""
+
+    def __init__(self, pads=None):
+        self.pads = list(pads or [])
+
+    def empty(self) -> bool:
+        return not self.pads
+
+    def num_pads(self) -> int:
+        return len(self.pads)
+
+    def add_pad(self, pad: ElectrodePad) -> None:
+        self.pads.append(pad)
+
+    def to_c(self):
+        arr = (_ffi.ElectrodePadC * max(len(self.pads), 1))()
+        for i, p in enumerate(self.pads):
+            arr[i] = p.to_c()
+        return arr
+
+    @staticmethod
+    def _from_c(arr, n) -> "ElectrodePatternMask":
+        return ElectrodePatternMask([ElectrodePad(a.shape, a.channel_id, a.cx, a.cy, a.r_min, a.r_max, a.phi_min,
+                                                  a.phi_max, a.fill_fraction) for a in arr[:n]])
+
+    @staticmethod
+    def supercdms_qet_mask(crystal_radius_m: float, fill_fraction: float = 1.0) -> "ElectrodePatternMask":
+        arr = (_ffi.ElectrodePadC * 5)()
+        _check(_ffi.load().cmpmc_mask_supercdms_qet(crystal_radius_m, fill_fraction, arr))
+        return ElectrodePatternMask._from_c(arr, 5)
+
+    @staticmethod
+    def rectangular_grid_mask(nx: int, ny: int, pitch_x: float, pitch_y: float, pad_half_w: float,
+                              pad_half_h: float, fill_fraction: float = 1.0) -> "ElectrodePatternMask":
+        n = max(nx * ny, 1)
+        arr = (_ffi.ElectrodePadC * n)()
+        cnt = C.c_uint64()
+        _check(_ffi.load().cmpmc_mask_rectangular_grid(nx, ny, pitch_x, pitch_y, pad_half_w, pad_half_h,
+                                                       fill_fraction, arr, n, C.byref(cnt)))
+        return ElectrodePatternMask._from_c(arr, cnt.value)
+
+    def find_channel(self, pos, rng: "Rng") -> int:
+        """The channel at (pos.x, pos.y), drawing from rng like the reference (host)."""
+        st = (C.c_uint64 * 4)(*rng.s)
+        ch = C.c_int32()
+        q = (C.c_double * 3)(*pos)
+        _check(_ffi.load().cmpmc_mask_find_channel(self.to_c(), len(self.pads), q, st, C.byref(ch)))
+        rng.s = list(st)
+        return ch.value
+
+
+@dataclass
 class SurfaceProperty:
-    """SurfaceProperty (geometry/surface_property.hpp:23-45); interface models and electrode
-    masks are not available on the device."""
+    """SurfaceProperty (geometry/surface_property.hpp:23-45); interface models are not
+    available on the device."""
     prob_abs: float = 0.0
     prob_refl: float = 1.0
     refl_cutoff: float = 350.0
@@ -327,6 +401,7 @@ class SurfaceProperty:
     kaplan_sensor: Optional[SuperconductorFilmConfig] = None
     spec_prob_const: float = 0.0
     demo_values: bool = False
+    electrode_mask: Optional[ElectrodePatternMask] = None
 
     @staticmethod
     def diffuse_bare_surface() -> "SurfaceProperty":
@@ -697,6 +772,10 @@ class SimulationEngine:
             self._ctx[device] = h
             if self.detector.mesh_field_3d is not None:
                 _check(self._lib.cmpmc_gpu_set_mesh(h, self.detector.mesh_field_3d._h), h)
+            for i, sp in enumerate(self.detector.surfaces):
+                if sp.electrode_mask is not None and not sp.electrode_mask.empty():
+                    m = sp.electrode_mask
+                    _check(self._lib.cmpmc_gpu_set_electrode_mask(h, i, m.to_c(), m.num_pads()), h)
         return h
 
     def configure(self, device: int = 0, threads_per_block: int = 0, blocks_per_sm: int = 0,

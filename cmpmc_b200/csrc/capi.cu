@@ -97,6 +97,7 @@ struct cmpmc_gpu_ctx {
     DevBuf unit_event, ev_offsets, ev_stats2, partials;  // batched form: unit -> event map, event offsets / stats
     DevBuf adj_prim, adj_hist, adj_w, adj_partials, adj_sums;  // adjoint: per-primary rows, bins, reductions
     DevBuf mesh32;                                      // FP32 mesh records (batched charge form)
+    DevBuf pads[3];                                     // electrode masks of the three surfaces
     DevBuf queue, resume_a, resume_b, ccounters, carrier_event, cursor;  // batched charge form
     uint64_t queue_cap = 1ull << 24;                    // Luke-phonon queue entries (64 B each)
     const float* cdf_f = nullptr;              // FP32 copies of the decay tables (in `tables`)
@@ -390,7 +391,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
+    for (DevBuf* b : {&ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
                       &ctx->ccounters, &ctx->carrier_event, &ctx->cursor, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
@@ -428,6 +429,31 @@ int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_pe
         ctx->stack_cap_batched = ctx->stack_cap;
     }
     if (hit_capacity) ctx->hit_cap = hit_capacity;
+    return CMPMC_OK;
+}
+
+int cmpmc_gpu_set_electrode_mask(cmpmc_gpu_ctx* ctx, int surface, const cmpmc_electrode_pad* pads, uint64_t n) {
+    if (!ctx) return CMPMC_ERR_INVALID;
+    ctx->last_status = CMPMC_OK;
+    ctx->last_error.clear();
+    if (surface < 0 || surface > 2) return fail(ctx, CMPMC_ERR_INVALID, "surface must be 0 (top), 1 (bottom) or 2 (side)");
+    if (n && !pads) return fail(ctx, CMPMC_ERR_INVALID, "pads is NULL");
+    if (n > 4096) return fail(ctx, CMPMC_ERR_INVALID, "at most 4096 pads per surface");
+    std::vector<Pad> p(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        if (pads[i].shape < 0 || pads[i].shape > 2)
+            return fail(ctx, CMPMC_ERR_INVALID, "pad shape must be disk, annular sector or rectangle");
+        p[i] = pad_view(pads[i]);
+    }
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    ctx->D.surf[surface].pads = nullptr;
+    ctx->D.surf[surface].n_pads = 0;
+    if (n == 0) return CMPMC_OK;
+    CK(ctx->pads[surface].ensure(n * sizeof(Pad)), "alloc pads");
+    CK(cudaMemcpy(ctx->pads[surface].p, p.data(), n * sizeof(Pad), cudaMemcpyHostToDevice), "copy pads");
+    ctx->D.surf[surface].pads = ctx->pads[surface].as<Pad>();
+    ctx->D.surf[surface].n_pads = static_cast<int>(n);
     return CMPMC_OK;
 }
 

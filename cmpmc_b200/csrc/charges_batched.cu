@@ -57,6 +57,8 @@ struct FCLat {
 
 struct FCSurf {
     float prob_abs, prob_spec, min_k_e, min_k_h;
+    int n_pads;
+    const Pad* pads;  // electrode mask
 };
 
 struct FCDet {
@@ -407,10 +409,16 @@ __global__ void __launch_bounds__(128, 4) k_charges_fp32(const __grid_constant__
                 c.p = c.p + E * (q_sign * kCLightF * dt_b);
                 c.ekin = ekin_of(L, c);
                 const FCSurf& s = D.surf[bh.surf];
-                // ChargePhysics::should_absorb_boundary (charge_transport.hpp:187-199)
+                // electrode mask (engine.hpp:284-289), then ChargePhysics::should_absorb_boundary
+                // (charge_transport.hpp:187-199)
+                int ch_id = -1;
+                bool absorb = true;
+                if (s.n_pads > 0) {
+                    ch_id = find_channel(s.pads, s.n_pads, static_cast<double>(c.pos.x), static_cast<double>(c.pos.y), k.g);
+                    absorb = ch_id >= 0;
+                }
                 const float k_perp = -fdot(c.p * (1.0f / kHbarCF), bh.n);
-                bool absorb = false;
-                if (k_perp > ((c.type == 1) ? s.min_k_e : s.min_k_h)) absorb = k.g.u() < s.prob_abs;
+                if (absorb) absorb = k_perp > ((c.type == 1) ? s.min_k_e : s.min_k_h) && k.g.u() < s.prob_abs;
                 if (!absorb) {
                     ++st.crefl;
                     c.pos = c.pos + bh.n * kNudge;
@@ -479,7 +487,7 @@ __global__ void __launch_bounds__(128, 4) k_charges_fp32(const __grid_constant__
                         h.excitation = static_cast<uint8_t>(c.type);
                         h.mode = 0;
                         h._pad = 0;
-                        h.channel_id = -1;
+                        h.channel_id = ch_id;
                         a.hit_stage[idx] = h;
                         a.hit_key[idx] = k.ev;
                     }
@@ -654,6 +662,8 @@ FCDet make_fcdet(const Detector& D, const MeshView32& mesh, const Lattice& L) {
         f.surf[i].prob_spec = static_cast<float>(D.surf[i].prob_charge_spec);
         f.surf[i].min_k_e = static_cast<float>(D.surf[i].min_k_elec);
         f.surf[i].min_k_h = static_cast<float>(D.surf[i].min_k_hole);
+        f.surf[i].n_pads = D.surf[i].n_pads;
+        f.surf[i].pads = D.surf[i].pads;
     }
     f.dt_cap = static_cast<float>(D.charge_dt_cap_s);
     const bool second = (D.charge_stepping == 1);

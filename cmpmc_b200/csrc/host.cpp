@@ -65,6 +65,20 @@ void charge_to_record(const Charge& c, cmpmc_charge_track& r) {
     r.alive = 1;
 }
 
+Pad pad_view(const cmpmc_electrode_pad& p) {
+    Pad o;
+    o.shape = p.shape;
+    o.channel = p.channel_id;
+    o.cx = p.cx;
+    o.cy = p.cy;
+    o.r_min = p.r_min;
+    o.r_max = p.r_max;
+    o.phi_min = p.phi_min;
+    o.phi_max = p.phi_max;
+    o.fill = p.fill_fraction;
+    return o;
+}
+
 Detector detector_view(const cmpmc_detector& d) {
     Detector D;
     std::memset(&D, 0, sizeof(D));
@@ -598,6 +612,50 @@ int cmpmc_generate(const cmpmc_lattice* lat, const cmpmc_detector* det, int work
             for (int k = 0; k < 4; ++k) rng_state[4 * i + k] = rng.s[k];
         }
     });
+    return CMPMC_OK;
+}
+
+int cmpmc_mask_supercdms_qet(double R, double fill, cmpmc_electrode_pad out[5]) {
+    if (!out) return CMPMC_ERR_INVALID;
+    std::memset(out, 0, 5 * sizeof(cmpmc_electrode_pad));
+    out[0] = {CMPMC_PAD_DISK, 0, 0.0, 0.0, 0.0, 0.55 * R, 0.0, kTwoPi, fill};
+    const double gap = 2.0 * (kPi / 180.0);
+    const double span = kTwoPi / 3.0;
+    for (int s = 0; s < 3; ++s)
+        out[1 + s] = {CMPMC_PAD_ANNULAR_SECTOR, s + 1, 0.0, 0.0, 0.57 * R, 0.90 * R, s * span + 0.5 * gap,
+                      (s + 1) * span - 0.5 * gap, fill};
+    out[4] = {CMPMC_PAD_ANNULAR_SECTOR, 4, 0.0, 0.0, 0.92 * R, 0.98 * R, 0.0, kTwoPi, fill};
+    return CMPMC_OK;
+}
+
+int cmpmc_mask_rectangular_grid(int nx, int ny, double pitch_x, double pitch_y, double hw, double hh, double fill,
+                                cmpmc_electrode_pad* out, uint64_t cap, uint64_t* n) {
+    if (nx < 0 || ny < 0) return CMPMC_ERR_INVALID;
+    const uint64_t total = static_cast<uint64_t>(nx) * static_cast<uint64_t>(ny);
+    if (n) *n = total;
+    if (total > cap) return CMPMC_ERR_CAPACITY;
+    if (total && !out) return CMPMC_ERR_INVALID;
+    int32_t ch = 0;
+    for (int ix = 0; ix < nx; ++ix) {
+        const double cx = (ix - 0.5 * (nx - 1)) * pitch_x;
+        for (int iy = 0; iy < ny; ++iy) {
+            const double cy = (iy - 0.5 * (ny - 1)) * pitch_y;
+            out[ch] = {CMPMC_PAD_RECTANGLE, ch, cx, cy, hw, hh, 0.0, 0.0, fill};
+            ++ch;
+        }
+    }
+    return CMPMC_OK;
+}
+
+int cmpmc_mask_find_channel(const cmpmc_electrode_pad* pads, uint64_t n, const double pos[3], uint64_t rng_state[4],
+                            int32_t* channel) {
+    if ((n && !pads) || !pos || !rng_state || !channel) return CMPMC_ERR_INVALID;
+    std::vector<Pad> p(n);
+    for (uint64_t i = 0; i < n; ++i) p[i] = pad_view(pads[i]);
+    Rng rng;
+    for (int k = 0; k < 4; ++k) rng.s[k] = rng_state[k];
+    *channel = find_channel(p.data(), static_cast<int>(n), pos[0], pos[1], rng);
+    for (int k = 0; k < 4; ++k) rng_state[k] = rng.s[k];
     return CMPMC_OK;
 }
 

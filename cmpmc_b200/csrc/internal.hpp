@@ -33,6 +33,7 @@ namespace cmpmc_gpu {
 int validate_config(const cmpmc_crystal_config& cfg, const cmpmc_detector& det, bool has_charges,
                     std::string& err);
 Detector detector_view(const cmpmc_detector& det);
+Pad pad_view(const cmpmc_electrode_pad& p);
 
 // Record conversion between the reference layouts and the register-state structs.
 Track track_from_record(const cmpmc_phonon_track& r);

@@ -370,6 +370,34 @@ struct Film {
     double phonon_loss_time;
 };
 
+// ElectrodePad (geometry/electrode_pattern.hpp:23-63): a readout pad on a face
+struct Pad {
+    int shape;  // 0 disk, 1 annular sector, 2 rectangle
+    int channel;
+    double cx, cy, r_min, r_max, phi_min, phi_max, fill;
+};
+
+// ElectrodePad::contains (electrode_pattern.hpp:37-62). The sector test takes atan2 of the
+// offset: CUDA's atan2 on the device (a last-ulp difference to the host's only matters
+// for a point within ~1e-16 rad of a sector edge).
+CMPMC_HD bool pad_contains(const Pad& p, double x, double y) {
+    if (p.shape == 0) {
+        const double dx = x - p.cx, dy = y - p.cy;
+        return (dx * dx + dy * dy) <= (p.r_max * p.r_max);
+    }
+    if (p.shape == 1) {
+        const double dx = x - p.cx, dy = y - p.cy;
+        const double r2 = dx * dx + dy * dy;
+        if (r2 < p.r_min * p.r_min || r2 > p.r_max * p.r_max) return false;
+        double phi = atan2(dy, dx);
+        if (phi < 0.0) phi += kTwoPi;
+        if (p.phi_min <= p.phi_max) return phi >= p.phi_min && phi <= p.phi_max;
+        return phi >= p.phi_min || phi <= p.phi_max;
+    }
+    if (p.shape == 2) return (fabs(x - p.cx) <= p.r_min) && (fabs(y - p.cy) <= p.r_max);
+    return false;
+}
+
 struct Surface {
     double prob_abs, prob_refl, refl_cutoff, anh_cutoff;
     double prob_charge_abs, prob_charge_spec, min_k_elec, min_k_hole;
@@ -378,7 +406,25 @@ struct Surface {
     int has_film;
     double spec[8], diff[8], anh[8];
     Film film;
+    // SurfaceProperty::electrode_mask (surface_property.hpp:45): n_pads > 0 when present
+    const Pad* pads;
+    int n_pads;
 };
+
+// ElectrodePatternMask::find_channel (electrode_pattern.hpp:82-92): the first pad that
+// contains (x, y) gives the channel, drawing once when its fill fraction is below 1;
+// -1 for bare crystal. `U` is the generator (FP64 uniform()).
+template <class U>
+CMPMC_HD int find_channel(const Pad* pads, int n_pads, double x, double y, U& rng) {
+    for (int i = 0; i < n_pads; ++i) {
+        const Pad& p = pads[i];
+        if (pad_contains(p, x, y)) {
+            if (p.fill >= 1.0 || rng.uniform() < p.fill) return p.channel;
+            return -1;
+        }
+    }
+    return -1;
+}
 
 // SurfaceProperty::eval_poly (surface_property.hpp:48-55): Horner from the top
 CMPMC_HD double eval_poly(const double* c, int n, double f) {

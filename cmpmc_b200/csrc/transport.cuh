@@ -186,9 +186,11 @@ CMPMC_HD void transport_phonons(const Lattice& L, const Detector& D, C& ctx, EvS
                 trk.t += bh.distance / trk.vmag;
                 trk.bounces++;
                 const Surface& s = D.surf[bh.surf];
-                const int ch_id = -1;  // no electrode mask on the device: every pad is active
+                // electrode mask (engine.hpp:483-488): bare crystal between pads reflects
+                const int ch_id = (s.n_pads > 0) ? find_channel(s.pads, s.n_pads, trk.pos.x, trk.pos.y, rng) : -1;
+                const bool active_pad = (s.n_pads == 0) || ch_id >= 0;
 
-                if (s.has_film && rng.uniform() < s.prob_abs) {
+                if (active_pad && s.has_film && rng.uniform() < s.prob_abs) {
                     const Film& film = s.film;
                     const double p_enter = film.film_absorption;
                     if (rng.uniform() < p_enter) {
@@ -582,8 +584,11 @@ CMPMC_HD void transport_charges(const Lattice& L, const Detector& D, C& ctx, EvS
                     c.p = c.p + E * (q_sign * kCLight * dt_b);
                     c.ekin = charge_ekin(L, c);
                     const Surface& s = D.surf[bh.surf];
-                    const int ch_id = -1;
-                    if (!should_absorb_boundary(c, bh.n_in, s.prob_charge_abs, s.min_k_elec, s.min_k_hole, rng)) {
+                    // electrode mask (engine.hpp:284-289)
+                    const int ch_id = (s.n_pads > 0) ? find_channel(s.pads, s.n_pads, c.pos.x, c.pos.y, rng) : -1;
+                    const bool active_pad = (s.n_pads == 0) || ch_id >= 0;
+                    if (!active_pad ||
+                        !should_absorb_boundary(c, bh.n_in, s.prob_charge_abs, s.min_k_elec, s.min_k_hole, rng)) {
                         st.charge_surface_refls++;
                         c.pos = c.pos + bh.n_in * 1e-11;
                         reflect_at_boundary(L, c, bh.n_in, s.prob_charge_spec, rng);

@@ -389,7 +389,13 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
             trk.bounces++;
             const Surface& s = D.surf[bh.surf];
             bool enter = false;
-            if (s.has_film && g.u() < static_cast<float>(s.prob_abs)) {
+            int ch_id = -1;
+            bool active_pad = true;
+            if (s.n_pads > 0) {  // electrode mask (engine.hpp:483-488)
+                ch_id = find_channel(s.pads, s.n_pads, static_cast<double>(trk.pos.x), static_cast<double>(trk.pos.y), g);
+                active_pad = ch_id >= 0;
+            }
+            if (active_pad && s.has_film && g.u() < static_cast<float>(s.prob_abs)) {
                 enter = g.u() < static_cast<float>(s.film.film_absorption);
                 if constexpr (kAdj) trk.s[3] += enter ? 1.0f : adj.film_miss_score;
             }
@@ -427,7 +433,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                             r.excitation = 0;
                             r.mode = static_cast<uint8_t>(trk.mode);
                             r._pad = 0;
-                            r.channel_id = -1;
+                            r.channel_id = ch_id;
                             a.hit_stage[idx] = r;
                             a.hit_key[idx] = a.ev_sink ? static_cast<uint64_t>(ev_cur) : ((unit << 32) | local);
                         }

@@ -154,7 +154,7 @@ typedef struct cmpmc_surface {
     double spec_coeffs[CMPMC_MAX_POLY], diff_coeffs[CMPMC_MAX_POLY], anh_coeffs[CMPMC_MAX_POLY];
     int32_t has_film;
     int32_t has_amm;               /* interface model: not supported on the device (must be 0) */
-    int32_t has_mask;              /* electrode mask: not supported on the device (must be 0) */
+    int32_t has_mask;              /* must be 0: masks are attached with cmpmc_gpu_set_electrode_mask */
     int32_t _pad0;
     cmpmc_film_config film;
 } cmpmc_surface;
@@ -185,6 +185,32 @@ typedef struct cmpmc_detector {
 void cmpmc_crystal_config_germanium(cmpmc_crystal_config* cfg);
 void cmpmc_detector_default(cmpmc_detector* det);
 void cmpmc_film_aluminum(cmpmc_film_config* film);
+
+/* ---- electrode masks (replaces ElectrodePatternMask, geometry/electrode_pattern.hpp) -- */
+enum { CMPMC_PAD_DISK = 0, CMPMC_PAD_ANNULAR_SECTOR = 1, CMPMC_PAD_RECTANGLE = 2 };
+/* ElectrodePad (electrode_pattern.hpp:23-35): 64 B */
+typedef struct cmpmc_electrode_pad {
+    int32_t shape;                 /* CMPMC_PAD_*                                          */
+    int32_t channel_id;
+    double cx, cy;                 /* centre (m) of a disk or rectangle                    */
+    double r_min;                  /* inner radius, or half-width hx of a rectangle (m)    */
+    double r_max;                  /* outer radius, or half-height hy of a rectangle (m)   */
+    double phi_min, phi_max;       /* azimuth range in [0, 2 pi] of an annular sector      */
+    double fill_fraction;          /* active metal fraction in (0, 1]                      */
+} cmpmc_electrode_pad;
+/* ElectrodePatternMask::supercdms_qet_mask (electrode_pattern.hpp:99-148): inner disk,
+ * three 120-degree sectors and a guard ring; writes 5 pads. */
+int cmpmc_mask_supercdms_qet(double crystal_radius_m, double fill_fraction, cmpmc_electrode_pad out[5]);
+/* ElectrodePatternMask::rectangular_grid_mask (electrode_pattern.hpp:151-178): nx * ny
+ * rectangles; *n receives nx * ny (CMPMC_ERR_CAPACITY when cap is smaller). */
+int cmpmc_mask_rectangular_grid(int nx, int ny, double pitch_x, double pitch_y, double pad_half_w,
+                                double pad_half_h, double fill_fraction, cmpmc_electrode_pad* out, uint64_t cap,
+                                uint64_t* n);
+/* ElectrodePatternMask::find_channel (electrode_pattern.hpp:82-92) on the host: the first
+ * pad containing (pos[0], pos[1]); one draw from rng_state when its fill fraction is below
+ * 1; -1 for bare crystal. */
+int cmpmc_mask_find_channel(const cmpmc_electrode_pad* pads, uint64_t n, const double pos[3], uint64_t rng_state[4],
+                            int32_t* channel);
 
 /* ---- host lattice (replaces the CrystalLattice constructor) -------------------- */
 typedef struct cmpmc_lattice cmpmc_lattice;
@@ -332,6 +358,11 @@ int cmpmc_gpu_device_count(int* count);
  * full they are parked and resumed after the queued phonons have been transported, so a
  * small queue only adds phases. 0 keeps the current value. */
 int cmpmc_gpu_configure_queue(cmpmc_gpu_ctx* ctx, uint64_t queue_capacity);
+/* SurfaceProperty::electrode_mask (surface_property.hpp:45, evaluated at engine.hpp:284-289
+ * and 483-488): attaches n pads to surface `surface` (CMPMC_SURF_*) of the context's
+ * detector and copies them to the device; n = 0 removes the mask. A phonon or carrier
+ * reaching bare crystal between pads reflects; a hit on a pad records its channel_id. */
+int cmpmc_gpu_set_electrode_mask(cmpmc_gpu_ctx* ctx, int surface, const cmpmc_electrode_pad* pads, uint64_t n);
 /* DetectorModel::mesh_field_3d (engine.hpp:99, looked up by electric_field_at,
  * engine.hpp:151-155): copies the mesh to the context's device; the charge transport then
  * takes its field from the mesh instead of the uniform e_field. NULL detaches it. Each

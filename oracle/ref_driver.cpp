@@ -18,6 +18,11 @@
 //       and prints one JSON line (wall seconds from RunResult::wall_seconds).
 //   cmpmc_ref rng <seed> <stream> <count>
 //       Prints next_u64 / uniform / isotropic_dir / lambertian_dir vectors.
+//   cmpmc_ref mask <n_points> <out>
+//       For n points uniform in [-R, R]^2 (Rng::for_stream(9, 0)): the channel of the
+//       SuperCDMS QET mask (fill 0.8, find_channel drawing from the same stream after each
+//       point) and of a 4 x 4 rectangular grid (find_geometric_channel); x, y as doubles,
+//       then the two channels as int32.
 //   cmpmc_ref mesh <n_points> <out>
 //       Builds the c3 field mesh and writes, for n points drawn in the cylinder
 //       (Rng::for_stream(5, 0)), the point, field_at and potential_at (each with one
@@ -41,6 +46,8 @@
 //       defaults); field from TriLinearMesh3D::build_cartesian_grid(R, R, h, 58, 58, 57)
 //       with V = 4 (z + h) / 2h + 0.2 ((x^2 + y^2) / R^2) sin(pi z / 2h); all Luke phonons
 //       tracked; seed 13; events_per_chunk 1
+//   c0m c0 with the SuperCDMS QET electrode mask (fill fraction 0.8) on both faces; seed 42
+//   tpm tp with the same masks on both faces; seed 77
 //   c3s the same with E = 10 eV * 10^u, max_sampled_phonons 20 (prompt phonons carry the
 //       weight n_true / 20) and luke_sample_fraction 0.05
 //
@@ -77,11 +84,11 @@ struct Workload {
 Workload make_workload(const std::string& w) {
     Workload wl;
     wl.name = w;
-    if (w == "c0") wl.seed = 42;
+    if (w == "c0" || w == "c0m") wl.seed = 42;
     else if (w == "c1") wl.seed = 7;
     else if (w == "c2") { wl.seed = 11; wl.events_per_chunk = 1; }
     else if (w == "c4") wl.seed = 17;
-    else if (w == "tp" || w == "tpl") wl.seed = 77;
+    else if (w == "tp" || w == "tpl" || w == "tpm") wl.seed = 77;
     else if (w == "c3" || w == "c3s") { wl.seed = 13; wl.events_per_chunk = 1; }
     else { std::fprintf(stderr, "unknown workload %s\n", w.c_str()); std::exit(2); }
     return wl;
@@ -105,10 +112,14 @@ void setup_detector(const std::string& w, DetectorModel& det) {
     } else if (w == "c2") {
         det.e_field = UniformElectricField::from_bias(4.0, 2.54 * units::cm);
         det.luke_sample_fraction = 0.0;
-    } else if (w == "tp" || w == "tpl") {
+    } else if (w == "tp" || w == "tpl" || w == "tpm") {
         det.e_field = UniformElectricField::from_bias(2.0, 2.54 * units::cm);
-        det.luke_sample_fraction = (w == "tp") ? 0.02 : 1.0;
+        det.luke_sample_fraction = (w == "tpl") ? 1.0 : 0.02;
     }
+    if (w == "c0m" || w == "tpm")
+        for (int f = 0; f < 2; ++f)
+            det.surfaces[f].electrode_mask =
+                geometry::ElectrodePatternMask::supercdms_qet_mask(det.solid.radius, 0.8);
 }
 
 Vec3 uniform_origin(const CylinderSolid& s, Rng& rng) {
@@ -137,7 +148,7 @@ struct Generator {
     }
 
     void generate(EventInput& in) const {
-        if (w == "c0") {
+        if (w == "c0" || w == "c0m") {
             in.phonons.push_back(engine->make_track({0, 0, 0}, in.rng.isotropic_dir(), PhononMode::L, 7.5e-3));
             in.injected_eV += 7.5e-3;
         } else if (w == "c1") {
@@ -322,6 +333,27 @@ int cmd_rng(uint64_t seed, uint64_t stream, int count) {
     return 0;
 }
 
+int cmd_mask(uint64_t n, const std::string& out) {
+    const DetectorModel det;
+    const double R = det.solid.radius;
+    const auto qet = geometry::ElectrodePatternMask::supercdms_qet_mask(R, 0.8);
+    const auto grid = geometry::ElectrodePatternMask::rectangular_grid_mask(4, 4, 1.5e-2, 1.5e-2, 0.6e-2, 0.5e-2);
+    Rng rng = Rng::for_stream(9, 0);
+    FILE* f = open_or_die(out);
+    for (uint64_t i = 0; i < n; ++i) {
+        const double x = (2.0 * rng.uniform() - 1.0) * R;
+        const double y = (2.0 * rng.uniform() - 1.0) * R;
+        const int32_t cq = qet.find_channel({x, y, 0.0}, rng);
+        const int32_t cg = grid.find_geometric_channel(x, y);
+        std::fwrite(&x, 8, 1, f);
+        std::fwrite(&y, 8, 1, f);
+        std::fwrite(&cq, 4, 1, f);
+        std::fwrite(&cg, 4, 1, f);
+    }
+    std::fclose(f);
+    return 0;
+}
+
 int cmd_mesh(uint64_t n, const std::string& out) {
     const DetectorModel det;
     const geometry::TriLinearMesh3D mesh = recoil_mesh(det.solid);
@@ -354,6 +386,7 @@ int main(int argc, char** argv) {
     if (cmd == "time" && argc == 6)
         return cmd_time(argv[2], std::strtoull(argv[3], nullptr, 10), std::strtoull(argv[4], nullptr, 10),
                         static_cast<unsigned>(std::atoi(argv[5])));
+    if (cmd == "mask" && argc == 4) return cmd_mask(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mesh" && argc == 4) return cmd_mesh(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "rng" && argc == 5)
         return cmd_rng(std::strtoull(argv[2], nullptr, 10), std::strtoull(argv[3], nullptr, 10), std::atoi(argv[4]));

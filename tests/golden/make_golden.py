@@ -15,11 +15,13 @@ compiled from its own headers by `make -C oracle ref`) and stores compact record
   <workload>_cr_*.npz   the same from oracle/_ref/cmpmc_ref_crlibm: the reference whose
                         transport uses a correctly rounded libm (oracle/ref_crlibm.hpp);
                         `floor` = fraction of events on which it agrees with the glibc build
+  mask_channels.npz     channels of the SuperCDMS QET mask (fill 0.8, with its draws) and of
+                        a 4 x 4 pad grid at 4096 points of a face
   mesh_c3.npz           the recoil workloads' field mesh (TriLinearMesh3D::build_cartesian_grid,
                         201,898 nodes): field_at and potential_at at 4096 points in the cylinder
 
 Usage: python tests/golden/make_golden.py [--only NAME,...]   (needs the reference build;
-       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist or mesh)
+       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist, mask or mesh)
 """
 from __future__ import annotations
 
@@ -50,6 +52,8 @@ PLAN = {
     "tp": (32, 203),
     "tpl": (2, 21),
     "c3s": (1, 64),
+    "c0m": (16, 2000),
+    "tpm": (8, 203),
 }
 
 
@@ -77,6 +81,12 @@ def main() -> None:
             rec = np.fromfile(path, dtype=np.float64).reshape(-1, 7)
             np.savez_compressed(os.path.join(HERE, "mesh_c3.npz"), points=rec[:, 0:3], field=rec[:, 3:6],
                                 potential=rec[:, 6], n_vertices=info["vertices"], n_tets=info["tetrahedra"])
+        if want("mask"):
+            path = os.path.join(tmp, "mask.bin")
+            subprocess.run([REF, "mask", "4096", path], check=True)
+            rec = np.fromfile(path, dtype=np.dtype([("x", "<f8"), ("y", "<f8"), ("qet", "<i4"), ("grid", "<i4")]))
+            np.savez_compressed(os.path.join(HERE, "mask_channels.npz"), x=rec["x"], y=rec["y"], qet=rec["qet"],
+                                grid=rec["grid"])
         if want("rng"):
             _rng_vectors()
         if want("lattice"):

@@ -25,9 +25,12 @@ def detector_for(workload: str):
     elif workload == "c3s":
         det.mesh_field_3d = recoil_mesh()
         det.luke_sample_fraction = 0.05
-    elif workload in ("tp", "tpl"):
+    elif workload in ("tp", "tpl", "tpm"):
         det.e_field = cm.UniformElectricField.from_bias(2.0, 2.54 * cm.units.cm)
-        det.luke_sample_fraction = 0.02 if workload == "tp" else 1.0
+        det.luke_sample_fraction = 1.0 if workload == "tpl" else 0.02
+    if workload in ("c0m", "tpm"):
+        for f in (0, 1):
+            det.surfaces[f].electrode_mask = cm.ElectrodePatternMask.supercdms_qet_mask(det.solid.radius, 0.8)
     return det
 
 
@@ -42,14 +45,15 @@ def recoil_mesh():
     return _MESH[0]
 
 
-WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13}
+WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13, "c0m": 42, "tpm": 77}
 
 
 def workload_of(name: str):
     import cmpmc_b200 as cm
     return {"c0": cm.workloads.single_l_origin, "c1": cm.workloads.mixed_energy, "c2": cm.workloads.pair_drift,
             "c4": cm.workloads.single_l_volume, "tp": cm.workloads.test_parallel,
-            "tpl": cm.workloads.test_parallel, "c3s": cm.workloads.recoil_light}[name]
+            "tpl": cm.workloads.test_parallel, "c3s": cm.workloads.recoil_light,
+            "c0m": cm.workloads.single_l_origin, "tpm": cm.workloads.test_parallel}[name]
 
 
 def has_gpu() -> bool:

@@ -103,3 +103,26 @@ def test_batched_deterministic(ge_lattice):
     assert a.stats.record().tobytes() == b.stats.record().tobytes()
     c = _batched(eng, "c1", 100, seed=12345)
     assert a.hits.tobytes() != c.hits.tobytes()
+
+
+def test_batched_electrode_mask_channels(ge_lattice):
+    """SuperCDMS QET masks (fill 0.8) on both faces: the per-event channel histogram of the
+    batched form against the plain FP64 form (itself identical to the reference event by
+    event), chi^2 p > 0.01; bare crystal between pads records no film hit."""
+    import cmpmc_b200 as cm
+    eng = _engine(ge_lattice, "c0m")
+    n = 4000
+    plain = cm.run_events(eng, n, workload_of("c0m"), cm.RunOptions(seed=42))
+    batched = _batched(eng, "c0m", n)
+
+    def per_event(res):
+        ev = np.repeat(np.arange(n), np.diff(res.hit_offsets.astype(np.int64)))
+        ch = res.hits["channel_id"].astype(np.int64)
+        assert ch.min() >= 0 and ch.max() <= 4  # film hits only on pads
+        counts = np.zeros((n, 5))
+        np.add.at(counts, (ev, ch), 1.0)
+        return {"n_events": n, "ch_sum": counts.sum(axis=0), "ch_sumsq": (counts ** 2).sum(axis=0)}
+
+    c2, dof, p = hist_chi2(per_event(plain), per_event(batched), "ch")
+    print(f"channels: chi2 {c2:.1f} dof {dof} p {p:.3f}")
+    assert p > P_MIN

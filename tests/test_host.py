@@ -164,6 +164,26 @@ def test_mesh_from_arrays_and_cartesian_builder_agree():
     assert a.field_at((3.0, 0.0, 0.0)) == (0.0, 0.0, 0.0)
 
 
+def test_electrode_masks_match_reference():
+    """SuperCDMS QET preset with fill fraction 0.8 (find_channel drawing from the same
+    stream as the reference) and a 4 x 4 rectangular pad grid at 4096 points of a face."""
+    import cmpmc_b200 as cm
+    g = golden("mask_channels.npz")
+    R = cm.DetectorModel().solid.radius
+    qet = cm.ElectrodePatternMask.supercdms_qet_mask(R, 0.8)
+    grid = cm.ElectrodePatternMask.rectangular_grid_mask(4, 4, 1.5e-2, 1.5e-2, 0.6e-2, 0.5e-2)
+    assert qet.num_pads() == 5 and grid.num_pads() == 16
+    rng = cm.Rng.for_stream(9, 0)
+    for i in range(len(g["x"])):
+        x = (2.0 * rng.uniform() - 1.0) * R
+        y = (2.0 * rng.uniform() - 1.0) * R
+        assert (x, y) == (g["x"][i], g["y"][i])
+        assert qet.find_channel((x, y, 0.0), rng) == g["qet"][i], i
+        one = cm.Rng(1)
+        assert grid.find_channel((x, y, 0.0), one) == g["grid"][i], i
+    assert set(np.unique(g["qet"])) == {-1, 0, 1, 2, 3, 4}
+
+
 def test_python_generator_matches_native(ge_lattice):
     import cmpmc_b200 as cm
     det = detector_for("tp")
