@@ -116,7 +116,7 @@ class RunDescC(C.Structure):
         ("n_events", _u64), ("first_event", _u64), ("rng_state", C.c_void_p), ("injected_eV", C.c_void_p),
         ("phonon_offsets", C.c_void_p), ("phonons", C.c_void_p), ("charge_offsets", C.c_void_p),
         ("charges", C.c_void_p), ("keep_hits", _i32), ("form", _i32), ("inputs_on_device", _i32),
-        ("outputs_on_device", _i32), ("seed", _u64), ("want_event_stats", _i32), ("_pad0", _i32),
+        ("outputs_on_device", _i32), ("seed", _u64), ("want_event_stats", _i32), ("kaplan_surrogate", _i32),
     ]
 
 
@@ -193,6 +193,11 @@ _SIG = {
     "cmpmc_mesh_potential_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
     "cmpmc_gpu_set_mesh": (_i32, [C.c_void_p, C.c_void_p]),
     "cmpmc_gpu_configure_queue": (_i32, [C.c_void_p, _u64]),
+    "cmpmc_kaplan_surrogate_create": (_i32, [C.POINTER(FilmConfigC), _u64, C.POINTER(C.c_void_p)]),
+    "cmpmc_kaplan_surrogate_destroy": (None, [C.c_void_p]),
+    "cmpmc_kaplan_surrogate_info": (_i32, [C.c_void_p, C.POINTER(_u64), C.POINTER(_u64)]),
+    "cmpmc_kaplan_surrogate_absorb": (_i32, [C.c_void_p, _f64, C.POINTER(_u64), C.c_void_p, _u64, C.POINTER(_u64),
+                                             C.POINTER(_f64)]),
     "cmpmc_gpu_set_electrode_mask": (_i32, [C.c_void_p, _i32, C.c_void_p, _u64]),
     "cmpmc_mask_supercdms_qet": (_i32, [_f64, _f64, C.c_void_p]),
     "cmpmc_mask_rectangular_grid": (_i32, [_i32, _i32, _f64, _f64, _f64, _f64, _f64, C.c_void_p, _u64,

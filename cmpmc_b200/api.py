@@ -309,6 +309,33 @@ def AluminumFilm() -> SuperconductorFilmConfig:
     return SuperconductorFilmConfig()
 
 
+class KaplanSurrogateLUT:
+    """KaplanSurrogateLUT (superconductor/kaplan_film.hpp:336-383), built natively on the
+    host; the batched form uses the same table on the device (RunOptions.kaplan_surrogate)."""
+
+    def __init__(self, film: "SuperconductorFilmConfig", seed: int = 1337):
+        self._lib = _ffi.load()
+        self._film = film.to_c()
+        h = C.c_void_p()
+        _check(self._lib.cmpmc_kaplan_surrogate_create(C.byref(self._film), int(seed), C.byref(h)), what="surrogate")
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.cmpmc_kaplan_surrogate_destroy(h)
+            self._h = None
+
+    def absorb_phonon_fast(self, energy: float, rng: "Rng"):
+        """(absorbed energy, re-emitted energies), drawing from rng like the reference."""
+        st = (C.c_uint64 * 4)(*rng.s)
+        buf = (C.c_double * 256)()
+        n, e = C.c_uint64(), C.c_double()
+        _check(self._lib.cmpmc_kaplan_surrogate_absorb(self._h, float(energy), st, buf, 256, C.byref(n), C.byref(e)))
+        rng.s = list(st)
+        return e.value, list(buf[:n.value])
+
+
 @dataclass
 class ElectrodePad:
     """ElectrodePad (geometry/electrode_pattern.hpp:23-63). shape: 0 disk, 1 annular sector,
@@ -668,6 +695,8 @@ class RunOptions:
     device: int = 0
     want_event_stats: bool = False
     first_event: int = 0
+    # batched form: film cascades from the KaplanSurrogateLUT table (kaplan_film.hpp:336-383)
+    kaplan_surrogate: bool = False
 
 
 class SimStats:
@@ -867,6 +896,7 @@ class SimulationEngine:
         d.form = _ffi.FORM_BATCHED_FP32 if options.form == "batched_fp32" else _ffi.FORM_PLAIN_FP64
         d.seed = options.seed
         d.want_event_stats = int(options.want_event_stats)
+        d.kaplan_surrogate = int(options.kaplan_surrogate)
         out = _ffi.RunOutC()
         _check(self._lib.cmpmc_gpu_run_events(h, C.byref(d), C.byref(out)), h)
         nh = int(out.n_hits)

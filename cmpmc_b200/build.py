@@ -34,6 +34,7 @@ SOURCES = {
     "lattice_host.cpp": [],
     "host.cpp": [],
     "mesh_host.cpp": [],
+    "kaplan_lut.cpp": [],
     "transport_plain.cu": ["--fmad=false"],
     "transport_batched.cu": [],
     "charges_batched.cu": [],

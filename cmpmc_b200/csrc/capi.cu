@@ -98,6 +98,8 @@ struct cmpmc_gpu_ctx {
     DevBuf adj_prim, adj_hist, adj_w, adj_partials, adj_sums;  // adjoint: per-primary rows, bins, reductions
     DevBuf mesh32;                                      // FP32 mesh records (batched charge form)
     DevBuf pads[3];                                     // electrode masks of the three surfaces
+    DevBuf lut[3];                                      // Kaplan surrogate tables of the films
+    bool lut_ready = false;
     DevBuf queue, resume_a, resume_b, ccounters, carrier_event, cursor;  // batched charge form
     uint64_t queue_cap = 1ull << 24;                    // Luke-phonon queue entries (64 B each)
     const float* cdf_f = nullptr;              // FP32 copies of the decay tables (in `tables`)
@@ -129,6 +131,37 @@ int cuda_fail(cmpmc_gpu_ctx* ctx, cudaError_t e, const char* what) {
         cudaError_t _e = (call);                           \
         if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); \
     } while (0)
+
+// Builds (once per context) the Kaplan surrogate table of every film on the host
+// (KaplanSurrogateLUT, reference seed 1337) and copies it to the device
+int ensure_surrogate(cmpmc_gpu_ctx* ctx) {
+    if (ctx->lut_ready) return CMPMC_OK;
+    for (int i = 0; i < 3; ++i) {
+        Surface& sf = ctx->D.surf[i];
+        sf.lut_abs = nullptr;
+        sf.lut_off = nullptr;
+        sf.lut_refl = nullptr;
+        if (!ctx->det.surfaces[i].has_film) continue;
+        cmpmc_kaplan_lut* t = nullptr;
+        const int st = cmpmc_kaplan_surrogate_create(&ctx->det.surfaces[i].film, 1337ull, &t);
+        if (st != CMPMC_OK) return fail(ctx, st, "surrogate table");
+        const size_t b_abs = t->abs.size() * 4, b_off = t->off.size() * 4, b_refl = std::max<size_t>(t->refl.size(), 1) * 4;
+        const size_t o_off = (b_abs + 255) / 256 * 256, o_refl = o_off + (b_off + 255) / 256 * 256;
+        cudaError_t e = ctx->lut[i].ensure(o_refl + b_refl);
+        char* base = ctx->lut[i].as<char>();
+        if (e == cudaSuccess) e = cudaMemcpy(base, t->abs.data(), b_abs, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(base + o_off, t->off.data(), b_off, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !t->refl.empty())
+            e = cudaMemcpy(base + o_refl, t->refl.data(), t->refl.size() * 4, cudaMemcpyHostToDevice);
+        cmpmc_kaplan_surrogate_destroy(t);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "copy surrogate table");
+        sf.lut_abs = reinterpret_cast<const float*>(base);
+        sf.lut_off = reinterpret_cast<const uint32_t*>(base + o_off);
+        sf.lut_refl = reinterpret_cast<const float*>(base + o_refl);
+    }
+    ctx->lut_ready = true;
+    return CMPMC_OK;
+}
 
 // Device counters of the batched charge form (reset per phase except next_carrier)
 struct ChargeCounters {
@@ -391,7 +424,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
+    for (DevBuf* b : {&ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
                       &ctx->ccounters, &ctx->carrier_event, &ctx->cursor, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
@@ -526,6 +559,11 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     a.first_event = d->first_event;
     a.keep_hits = d->keep_hits;
     a.seed = d->seed;
+    if (d->kaplan_surrogate && batched) {
+        const int st = ensure_surrogate(ctx);
+        if (st != CMPMC_OK) return st;
+        a.surrogate = 1;
+    }
     uint64_t n_ph = 0, n_ch = 0;
     if (d->inputs_on_device) {
         a.rng_state = d->rng_state;

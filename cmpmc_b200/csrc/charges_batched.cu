@@ -140,6 +140,11 @@ __device__ FCharge make_charge_f(const FCLat& L, int type, F3 pos, F3 dir, float
     return c;
 }
 
+// electrode mask lookup out of line (keeps atan2 out of the step loop)
+__device__ __noinline__ int mask_call(const Pad* pads, int n_pads, float x, float y, R128* g) {
+    return find_channel(pads, n_pads, static_cast<double>(x), static_cast<double>(y), *g);
+}
+
 struct FRates {
     float luke, iv, trap, ion_e, ion_h, tot;
 };
@@ -414,7 +419,7 @@ __global__ void __launch_bounds__(128, 4) k_charges_fp32(const __grid_constant__
                 int ch_id = -1;
                 bool absorb = true;
                 if (s.n_pads > 0) {
-                    ch_id = find_channel(s.pads, s.n_pads, static_cast<double>(c.pos.x), static_cast<double>(c.pos.y), k.g);
+                    ch_id = mask_call(s.pads, s.n_pads, c.pos.x, c.pos.y, &k.g);
                     absorb = ch_id >= 0;
                 }
                 const float k_perp = -fdot(c.p * (1.0f / kHbarCF), bh.n);

@@ -63,6 +63,8 @@ struct RunArgs {
     // event sink (batched form with charges): units add their counters to ev_stats[event]
     // and their hit counts to ev_nhits[event]; staged hits carry the event as key
     int ev_sink;
+    // batched form: film cascades from the surfaces' surrogate tables (Surface::lut_*)
+    int surrogate;
 };
 
 // Luke-phonon queue entry of the batched charge form (64 B). ev == kQEmpty marks a slot

@@ -65,6 +65,27 @@ void charge_to_record(const Charge& c, cmpmc_charge_track& r) {
     r.alive = 1;
 }
 
+Film film_view(const cmpmc_film_config& f) {
+    Film o;
+    o.film_absorption = f.film_absorption;
+    o.film_thickness = f.film_thickness;
+    o.v_sound = f.v_sound;
+    o.gap_energy = f.gap_energy;
+    o.phonon_lifetime = f.phonon_lifetime;
+    o.phonon_lifetime_slope = f.phonon_lifetime_slope;
+    o.low_qp_limit = f.low_qp_limit;
+    o.high_qp_limit = f.high_qp_limit;
+    o.subgap_absorption = f.subgap_absorption;
+    o.absorber_gap = f.absorber_gap;
+    o.absorber_eff = f.absorber_eff;
+    o.absorber_eff_slope = f.absorber_eff_slope;
+    o.temperature = f.temperature;
+    o.keep_all_phonons = f.keep_all_phonons;
+    o.loss_model = f.loss_model;
+    o.phonon_loss_time = f.phonon_loss_time;
+    return o;
+}
+
 Pad pad_view(const cmpmc_electrode_pad& p) {
     Pad o;
     o.shape = p.shape;
@@ -106,23 +127,7 @@ Detector detector_view(const cmpmc_detector& d) {
             o.diff[k] = s.diff_coeffs[k];
             o.anh[k] = s.anh_coeffs[k];
         }
-        const cmpmc_film_config& f = s.film;
-        o.film.film_absorption = f.film_absorption;
-        o.film.film_thickness = f.film_thickness;
-        o.film.v_sound = f.v_sound;
-        o.film.gap_energy = f.gap_energy;
-        o.film.phonon_lifetime = f.phonon_lifetime;
-        o.film.phonon_lifetime_slope = f.phonon_lifetime_slope;
-        o.film.low_qp_limit = f.low_qp_limit;
-        o.film.high_qp_limit = f.high_qp_limit;
-        o.film.subgap_absorption = f.subgap_absorption;
-        o.film.absorber_gap = f.absorber_gap;
-        o.film.absorber_eff = f.absorber_eff;
-        o.film.absorber_eff_slope = f.absorber_eff_slope;
-        o.film.temperature = f.temperature;
-        o.film.keep_all_phonons = f.keep_all_phonons;
-        o.film.loss_model = f.loss_model;
-        o.film.phonon_loss_time = f.phonon_loss_time;
+        o.film = film_view(s.film);
     }
     D.max_bounces = d.max_bounces;
     D.rr_bounces = d.russian_roulette_bounces;

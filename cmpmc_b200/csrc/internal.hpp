@@ -17,6 +17,13 @@ struct cmpmc_lattice {
     cmpmc_gpu::Lattice view;               // host pointers into the vectors above
 };
 
+struct cmpmc_kaplan_lut {
+    cmpmc_gpu::Film film;
+    std::vector<float> abs;        // [kLutNE * kLutNS]
+    std::vector<uint32_t> off;     // [kLutNE * kLutNS + 1]
+    std::vector<float> refl;
+};
+
 // TriLinearMesh3D (geometry/mesh_field.hpp:40-345): node table, potentials, sorted
 // tetrahedra and the per-tetrahedron records the device walks (mesh.cuh).
 struct cmpmc_mesh {
@@ -34,6 +41,14 @@ int validate_config(const cmpmc_crystal_config& cfg, const cmpmc_detector& det, 
                     std::string& err);
 Detector detector_view(const cmpmc_detector& det);
 Pad pad_view(const cmpmc_electrode_pad& p);
+Film film_view(const cmpmc_film_config& f);
+
+// KaplanSurrogateLUT (superconductor/kaplan_film.hpp:336-383) tables: 128 energy nodes on
+// [2 Delta, 40 Delta] x 512 pre-sampled cascade outcomes (absorbed fraction and the
+// re-emitted energies as fractions of the incident energy)
+constexpr int kLutNE = 128;
+constexpr int kLutNS = 512;
+constexpr double kLutEMaxDiv2Gap = 20.0;
 
 // Record conversion between the reference layouts and the register-state structs.
 Track track_from_record(const cmpmc_phonon_track& r);

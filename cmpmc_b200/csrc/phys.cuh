@@ -409,6 +409,11 @@ struct Surface {
     // SurfaceProperty::electrode_mask (surface_property.hpp:45): n_pads > 0 when present
     const Pad* pads;
     int n_pads;
+    // KaplanSurrogateLUT tables of the film (batched form, when requested): absorbed
+    // fractions [128 * 512], offsets into the re-emitted fractions [128 * 512 + 1]
+    const float* lut_abs;
+    const uint32_t* lut_off;
+    const float* lut_refl;
 };
 
 // ElectrodePatternMask::find_channel (electrode_pattern.hpp:82-92): the first pad that

@@ -131,6 +131,29 @@ __device__ __noinline__ double kaplan_call(const Film* f, double E, double* refl
     return edep;
 }
 
+// electrode mask lookup out of line: the sector test's atan2 stays out of the step loop's
+// instruction stream
+__device__ __noinline__ int mask_call(const Pad* pads, int n_pads, float x, float y, R128* g) {
+    return find_channel(pads, n_pads, static_cast<double>(x), static_cast<double>(y), *g);
+}
+
+// KaplanSurrogateLUT::absorb_phonon_fast (kaplan_film.hpp:361-374): one stored cascade
+// outcome of a bracketing energy node, rescaled; the full cascade outside the table
+__device__ __noinline__ double surrogate_call(const Surface* s, double E, double* refl, int* n_refl, double* work,
+                                              R128* g) {
+    const double two_delta = 2.0 * dmax(s->film.gap_energy, 1e-12);
+    const double u = (E / two_delta - 1.0) / (20.0 - 1.0) * 127.0;
+    if (film_is_subgap(s->film, E) || u < 0.0 || u > 127.0) return kaplan_call(&s->film, E, refl, n_refl, work, g);
+    int ie = min(static_cast<int>(u), 126);
+    if (g->uniform() < (u - ie)) ++ie;
+    const int k = ie * 512 + min(511, static_cast<int>(g->uniform() * 512.0));
+    const uint32_t r0 = __ldg(s->lut_off + k), r1 = __ldg(s->lut_off + k + 1);
+    const int n = min(static_cast<int>(r1 - r0), kKaplanCap);
+    for (int i = 0; i < n; ++i) refl[i] = E * static_cast<double>(__ldg(s->lut_refl + r0 + i));
+    *n_refl = n;
+    return E * static_cast<double>(__ldg(s->lut_abs + k));
+}
+
 // anharmonic decay of an L phonon (engine.hpp:938-988), FP32 angles
 template <bool kAdj>
 __device__ __noinline__ void decay_call(const FLat* Lp, TrackOf<kAdj>* tp, EntryOf<kAdj>* stk, uint32_t* n_stk,
@@ -249,7 +272,9 @@ enum { kSrcInput = 0, kSrcQueue = 1 };
 // kSrc selects where units come from: the caller's primary phonon records (kSrcInput,
 // substream (event << 20 | index)) or the Luke-phonon queue of the charge form
 // (kSrcQueue, the entry's own substream key; empty slots are skipped).
-template <bool kAdj, int kSrc = kSrcInput>
+// kSink: units add to per-event sinks (runs with charges); kSur: film cascades from the
+// surrogate tables. Both are compile-time so the default kernel carries neither branch.
+template <bool kAdj, int kSrc = kSrcInput, bool kSink = false, bool kSur = false>
 __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, const RunArgs& a,
                                              const uint32_t* __restrict__ unit_event,
                                              const QPhonon* __restrict__ queue, const AdjArgs& adj,
@@ -278,7 +303,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 live = true;
             } else {
                 if (unit != ~0ull) {
-                    if (a.ev_sink) sink_unit(&a, ev_cur, &st);
+                    if constexpr (kSink) sink_unit(&a, ev_cur, &st);
                     else write_unit(a, unit, st, n_hits);
                 }
                 unit = atomicAdd(a.next_work, 1ull);
@@ -392,7 +417,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
             int ch_id = -1;
             bool active_pad = true;
             if (s.n_pads > 0) {  // electrode mask (engine.hpp:483-488)
-                ch_id = find_channel(s.pads, s.n_pads, static_cast<double>(trk.pos.x), static_cast<double>(trk.pos.y), g);
+                ch_id = mask_call(s.pads, s.n_pads, trk.pos.x, trk.pos.y, &g);
                 active_pad = ch_id >= 0;
             }
             if (active_pad && s.has_film && g.u() < static_cast<float>(s.prob_abs)) {
@@ -401,7 +426,13 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
             }
             if (enter) {
                 int n_refl = 0;
-                const double edep = kaplan_call(&s.film, trk.E, refl_buf, &n_refl, kwork, &g);
+                double edep;
+                if constexpr (kSur) {
+                    edep = s.lut_abs ? surrogate_call(&s, trk.E, refl_buf, &n_refl, kwork, &g)
+                                     : kaplan_call(&s.film, trk.E, refl_buf, &n_refl, kwork, &g);
+                } else {
+                    edep = kaplan_call(&s.film, trk.E, refl_buf, &n_refl, kwork, &g);
+                }
                 if (edep > 0.0) {
                     const double wedep = edep * trk.w;
                     st.hits++;
@@ -421,7 +452,8 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                             }
                         }
                     } else if (a.keep_hits) {
-                        if (a.ev_sink) atomicAdd(reinterpret_cast<unsigned long long*>(a.ev_nhits + ev_cur), 1ull);
+                        if constexpr (kSink)
+                            atomicAdd(reinterpret_cast<unsigned long long*>(a.ev_nhits + ev_cur), 1ull);
                         const unsigned long long idx = atomicAdd(a.hit_count, 1ull);
                         if (idx < a.hit_cap) {
                             cmpmc_sensor_hit r;
@@ -435,7 +467,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                             r._pad = 0;
                             r.channel_id = ch_id;
                             a.hit_stage[idx] = r;
-                            a.hit_key[idx] = a.ev_sink ? static_cast<uint64_t>(ev_cur) : ((unit << 32) | local);
+                            a.hit_key[idx] = kSink ? static_cast<uint64_t>(ev_cur) : ((unit << 32) | local);
                         }
                     }
                 }
@@ -554,21 +586,23 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
     if (err) atomicOr(a.err, err);
 }
 
+template <bool kSink, bool kSur>
 __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__ FLat L,
                                                          const __grid_constant__ Detector D,
                                                          const __grid_constant__ RunArgs a,
                                                          const uint32_t* __restrict__ unit_event) {
     const AdjArgs none{};
-    batched_loop<false>(L, D, a, unit_event, nullptr, none, nullptr, nullptr);
+    batched_loop<false, kSrcInput, kSink, kSur>(L, D, a, unit_event, nullptr, none, nullptr, nullptr);
 }
 
 // The Luke-phonon queue of the batched charge form: one unit per queue entry
+template <bool kSur>
 __global__ void __launch_bounds__(128, 8) k_queue_fp32(const __grid_constant__ FLat L,
                                                        const __grid_constant__ Detector D,
                                                        const __grid_constant__ RunArgs a,
                                                        const QPhonon* __restrict__ queue) {
     const AdjArgs none{};
-    batched_loop<false, kSrcQueue>(L, D, a, nullptr, queue, none, nullptr, nullptr);
+    batched_loop<false, kSrcQueue, true, kSur>(L, D, a, nullptr, queue, none, nullptr, nullptr);
 }
 
 // Adjoint of the hit-time histogram: the batched transport with per-track scores. Bin
@@ -601,19 +635,27 @@ cudaError_t launch_unit_event(const uint64_t* ph_off, uint64_t n_events, uint32_
 
 cudaError_t launch_batched_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                                 const uint32_t* unit_event, int grid, int block, cudaStream_t s) {
-    k_batched_fp32<<<grid, block, 0, s>>>(make_flat(L, cdf_f, D), D, a, unit_event);
+    const FLat f = make_flat(L, cdf_f, D);
+    if (a.ev_sink) {
+        if (a.surrogate) k_batched_fp32<true, true><<<grid, block, 0, s>>>(f, D, a, unit_event);
+        else k_batched_fp32<true, false><<<grid, block, 0, s>>>(f, D, a, unit_event);
+    } else {
+        if (a.surrogate) k_batched_fp32<false, true><<<grid, block, 0, s>>>(f, D, a, unit_event);
+        else k_batched_fp32<false, false><<<grid, block, 0, s>>>(f, D, a, unit_event);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t batched_fp32_occupancy(int block, int* blocks_per_sm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_batched_fp32, block, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_batched_fp32<false, false>, block, 0);
 }
 
 size_t batched_stack_entry_bytes() { return sizeof(GFTrack); }
 
 cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                               const QPhonon* queue, int grid, int block, cudaStream_t s) {
-    k_queue_fp32<<<grid, block, 0, s>>>(make_flat(L, cdf_f, D), D, a, queue);
+    if (a.surrogate) k_queue_fp32<true><<<grid, block, 0, s>>>(make_flat(L, cdf_f, D), D, a, queue);
+    else k_queue_fp32<false><<<grid, block, 0, s>>>(make_flat(L, cdf_f, D), D, a, queue);
     return cudaGetLastError();
 }
 

@@ -50,6 +50,7 @@ struct PlainCtx {
     double* kwork;
 
     __device__ bool pop(Track& t) {
+        if (err) return false;  // a stack overflowed: the event is rerun with more room
         if (n_stk > 0) {
             t = unpack_track(stk[--n_stk]);
             return true;
@@ -65,6 +66,7 @@ struct PlainCtx {
         else err |= kErrPhononStack;
     }
     __device__ bool pop_charge(Charge& c) {
+        if (err) return false;
         if (n_cstk > 0) {
             const GCharge& g = cstk[--n_cstk];
             c.pos = v3(g.px, g.py, g.pz);

@@ -212,6 +212,20 @@ int cmpmc_mask_rectangular_grid(int nx, int ny, double pitch_x, double pitch_y, 
 int cmpmc_mask_find_channel(const cmpmc_electrode_pad* pads, uint64_t n, const double pos[3], uint64_t rng_state[4],
                             int32_t* channel);
 
+/* ---- Kaplan-cascade surrogate (replaces KaplanSurrogateLUT, kaplan_film.hpp:336-383) ---- */
+typedef struct cmpmc_kaplan_lut cmpmc_kaplan_lut;
+/* KaplanSurrogateLUT(film, seed) (kaplan_film.hpp:344-358): 128 energy nodes on
+ * [2 Delta, 40 Delta] x 512 cascade outcomes drawn from Rng(seed) (the reference's
+ * default seed is 1337). */
+int cmpmc_kaplan_surrogate_create(const cmpmc_film_config* film, uint64_t seed, cmpmc_kaplan_lut** out);
+void cmpmc_kaplan_surrogate_destroy(cmpmc_kaplan_lut* lut);
+int cmpmc_kaplan_surrogate_info(const cmpmc_kaplan_lut* lut, uint64_t* n_outcomes, uint64_t* n_reflected);
+/* KaplanSurrogateLUT::absorb_phonon_fast (kaplan_film.hpp:361-374) on the host: returns the
+ * absorbed energy in *edep and the re-emitted energies in refl[0 .. *n_refl); draws from
+ * rng_state. */
+int cmpmc_kaplan_surrogate_absorb(const cmpmc_kaplan_lut* lut, double energy, uint64_t rng_state[4], double* refl,
+                                  uint64_t cap, uint64_t* n_refl, double* edep);
+
 /* ---- host lattice (replaces the CrystalLattice constructor) -------------------- */
 typedef struct cmpmc_lattice cmpmc_lattice;
 
@@ -324,7 +338,9 @@ typedef struct cmpmc_run_desc {
     int32_t outputs_on_device;     /* 1: leave hits / offsets / event stats on the device   */
     uint64_t seed;                 /* batched form: substream seed                          */
     int32_t want_event_stats;      /* 1: also return per-event SimStats                     */
-    int32_t _pad0;
+    int32_t kaplan_surrogate;      /* batched form: 1 = film cascades from the surrogate
+                                      table (KaplanSurrogateLUT, seed 1337) inside its
+                                      energy range, the full cascade outside it            */
 } cmpmc_run_desc;
 
 typedef struct cmpmc_run_out {

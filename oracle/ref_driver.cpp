@@ -23,6 +23,11 @@
 //       SuperCDMS QET mask (fill 0.8, find_channel drawing from the same stream after each
 //       point) and of a 4 x 4 rectangular grid (find_geometric_channel); x, y as doubles,
 //       then the two channels as int32.
+//   cmpmc_ref kaplan <n> <out>
+//       KaplanSurrogateLUT of the default Al film (seed 1337): for n energies
+//       E = Delta (1 + 45 u) (Rng::for_stream(3, 0), sub-gap, in-table and above-table),
+//       absorb_phonon_fast(E) with the same stream; per record E, edep (f64), the count
+//       (u32) and the re-emitted energies (f64).
 //   cmpmc_ref mesh <n_points> <out>
 //       Builds the c3 field mesh and writes, for n points drawn in the cylinder
 //       (Rng::for_stream(5, 0)), the point, field_at and potential_at (each with one
@@ -354,6 +359,26 @@ int cmd_mask(uint64_t n, const std::string& out) {
     return 0;
 }
 
+int cmd_kaplan(uint64_t n, const std::string& out) {
+    const DetectorModel det;
+    const KaplanFilm& film = *det.surfaces[0].kaplan_sensor;
+    const KaplanSurrogateLUT lut(film);
+    Rng rng = Rng::for_stream(3, 0);
+    KaplanBuffer refl;
+    FILE* f = open_or_die(out);
+    for (uint64_t i = 0; i < n; ++i) {
+        const double E = film.gap_energy * (1.0 + 45.0 * rng.uniform());
+        const double edep = lut.absorb_phonon_fast(E, refl, rng);
+        const uint32_t cnt = static_cast<uint32_t>(refl.size());
+        std::fwrite(&E, 8, 1, f);
+        std::fwrite(&edep, 8, 1, f);
+        std::fwrite(&cnt, 4, 1, f);
+        for (double r : refl) std::fwrite(&r, 8, 1, f);
+    }
+    std::fclose(f);
+    return 0;
+}
+
 int cmd_mesh(uint64_t n, const std::string& out) {
     const DetectorModel det;
     const geometry::TriLinearMesh3D mesh = recoil_mesh(det.solid);
@@ -386,6 +411,7 @@ int main(int argc, char** argv) {
     if (cmd == "time" && argc == 6)
         return cmd_time(argv[2], std::strtoull(argv[3], nullptr, 10), std::strtoull(argv[4], nullptr, 10),
                         static_cast<unsigned>(std::atoi(argv[5])));
+    if (cmd == "kaplan" && argc == 4) return cmd_kaplan(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mask" && argc == 4) return cmd_mask(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mesh" && argc == 4) return cmd_mesh(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "rng" && argc == 5)

@@ -17,11 +17,13 @@ compiled from its own headers by `make -C oracle ref`) and stores compact record
                         `floor` = fraction of events on which it agrees with the glibc build
   mask_channels.npz     channels of the SuperCDMS QET mask (fill 0.8, with its draws) and of
                         a 4 x 4 pad grid at 4096 points of a face
+  kaplan_surrogate.npz  KaplanSurrogateLUT (default Al film, seed 1337) lookups at 2000 energies
+                        on [Delta, 46 Delta] with the reference's draws
   mesh_c3.npz           the recoil workloads' field mesh (TriLinearMesh3D::build_cartesian_grid,
                         201,898 nodes): field_at and potential_at at 4096 points in the cylinder
 
 Usage: python tests/golden/make_golden.py [--only NAME,...]   (needs the reference build;
-       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist, mask or mesh)
+       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist, kaplan, mask or mesh)
 """
 from __future__ import annotations
 
@@ -87,6 +89,23 @@ def main() -> None:
             rec = np.fromfile(path, dtype=np.dtype([("x", "<f8"), ("y", "<f8"), ("qet", "<i4"), ("grid", "<i4")]))
             np.savez_compressed(os.path.join(HERE, "mask_channels.npz"), x=rec["x"], y=rec["y"], qet=rec["qet"],
                                 grid=rec["grid"])
+        if want("kaplan"):
+            path = os.path.join(tmp, "kaplan.bin")
+            subprocess.run([REF, "kaplan", "2000", path], check=True)
+            raw = open(path, "rb").read()
+            E, edep, cnt, refl = [], [], [], []
+            off = 0
+            while off < len(raw):
+                e, d = np.frombuffer(raw, dtype="<f8", count=2, offset=off)
+                c = int(np.frombuffer(raw, dtype="<u4", count=1, offset=off + 16)[0])
+                off += 20
+                refl.append(np.frombuffer(raw, dtype="<f8", count=c, offset=off))
+                off += 8 * c
+                E.append(e)
+                edep.append(d)
+                cnt.append(c)
+            np.savez_compressed(os.path.join(HERE, "kaplan_surrogate.npz"), energy=np.array(E), edep=np.array(edep),
+                                n_refl=np.array(cnt, dtype=np.uint32), refl=np.concatenate(refl))
         if want("rng"):
             _rng_vectors()
         if want("lattice"):

@@ -126,3 +126,28 @@ def test_batched_electrode_mask_channels(ge_lattice):
     c2, dof, p = hist_chi2(per_event(plain), per_event(batched), "ch")
     print(f"channels: chi2 {c2:.1f} dof {dof} p {p:.3f}")
     assert p > P_MIN
+
+
+def test_batched_kaplan_surrogate_statistics(ge_lattice):
+    """Film cascades from the KaplanSurrogateLUT table (kaplan_film.hpp:336-383) in the
+    batched form against the reference's full-cascade transport: hit time and radius
+    histograms chi^2 p > 0.01, deposited fraction within 3 % (the reference's own bar for
+    the surrogate, tests/test_kaplan.cpp:95-107), and the ledger still closes. The per-hit
+    energy spectrum is not compared: a stored outcome is rescaled from the nearest of 128
+    energy nodes, which reshapes the edep histogram by design."""
+    import cmpmc_b200 as cm
+    eng = _engine(ge_lattice, "c1")
+    packed = eng.generate(workload_of("c1"), 2000, WORKLOAD_SEED["c1"])
+    res = eng.run_packed(packed, cm.RunOptions(seed=7, form="batched_fp32", kaplan_surrogate=True))
+    ref = dict(golden("c1_hist.npz"))
+    got = event_histograms(res.hit_offsets, res.hits, tuple(ref["edep_range"]))
+    for name in ("time", "radius"):
+        c2, dof, p = hist_chi2(ref, got, name)
+        print(f"surrogate {name}: chi2 {c2:.1f} dof {dof} p {p:.3f}")
+        assert p > P_MIN, (name, c2, dof, p)
+    st = res.stats
+    inj = st.total_injected_eV
+    assert abs(inj - st.total_deposited_eV - st.escaped_or_killed_eV) / inj <= LEDGER_TOL
+    frac_ref = float(ref["deposited"]) / float(ref["injected"])
+    print(f"deposited fraction: surrogate {st.total_deposited_eV / inj:.5f} reference {frac_ref:.5f}")
+    assert abs(st.total_deposited_eV / inj / frac_ref - 1.0) < 0.03

@@ -184,6 +184,26 @@ def test_electrode_masks_match_reference():
     assert set(np.unique(g["qet"])) == {-1, 0, 1, 2, 3, 4}
 
 
+def test_kaplan_surrogate_matches_reference():
+    """KaplanSurrogateLUT of the default Al film (seed 1337): 2000 lookups over sub-gap,
+    in-table and above-table energies equal the reference's (absorbed energy and every
+    re-emitted energy), drawing from the same stream."""
+    import cmpmc_b200 as cm
+    g = golden("kaplan_surrogate.npz")
+    film = cm.AluminumFilm()
+    lut = cm.KaplanSurrogateLUT(film)
+    rng = cm.Rng.for_stream(3, 0)
+    off = 0
+    for i in range(len(g["energy"])):
+        E = film.gap_energy * (1.0 + 45.0 * rng.uniform())
+        assert E == g["energy"][i]
+        edep, refl = lut.absorb_phonon_fast(E, rng)
+        k = int(g["n_refl"][i])
+        assert edep == g["edep"][i], i
+        assert refl == list(g["refl"][off:off + k]), i
+        off += k
+
+
 def test_python_generator_matches_native(ge_lattice):
     import cmpmc_b200 as cm
     det = detector_for("tp")
