@@ -11,13 +11,18 @@
 // are byte-identical, include/cmpmc_gpu.h).
 //
 // The device needs the crystal's configuration (it rebuilds the CrystalLattice tables with
-// the same arithmetic) and the DetectorModel. Guarded modules raise the reference's
-// UnvalidatedModuleError; configurations the device does not support (interface
-// transmission, electrode masks, charge release other than RecordOnly, bilinear / exact
-// kinematics, mesh fields) raise std::invalid_argument.
+// the same arithmetic) and the DetectorModel. Electrode masks are copied from the
+// surfaces' ElectrodePatternMask pads. A TriLinearMesh3D field keeps its nodes private in
+// the reference, so a detector with mesh_field_3d needs the same mesh handed over once with
+// GpuEngine::set_mesh (its node coordinates, potentials and tetrahedra) or
+// set_cartesian_mesh (the build_cartesian_grid arguments and the potential function).
+// Guarded modules raise the reference's UnvalidatedModuleError; configurations the device
+// does not support (interface transmission, charge release other than RecordOnly, bilinear /
+// exact kinematics, 2D meshes) raise std::invalid_argument.
 #pragma once
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cstring>
@@ -26,6 +31,7 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../cmpmc_gpu.h"
@@ -37,6 +43,7 @@ enum class Form { PlainFP64 = CMPMC_FORM_PLAIN_FP64, BatchedFP32 = CMPMC_FORM_BA
 struct GpuRunOptions {
     int device = 0;
     Form form = Form::PlainFP64;
+    bool kaplan_surrogate = false;  // batched form: film cascades from the KaplanSurrogateLUT table
 };
 
 namespace detail {
@@ -104,9 +111,23 @@ inline void poly(const std::vector<double>& v, double* dst, int32_t& n) {
     for (size_t i = 0; i < v.size(); ++i) dst[i] = v[i];
 }
 
+inline std::vector<cmpmc_electrode_pad> pads_of(const cmpmc::geometry::ElectrodePatternMask& m) {
+    std::vector<cmpmc_electrode_pad> out;
+    for (const auto& p : m.pads()) {
+        cmpmc_electrode_pad q;
+        std::memset(&q, 0, sizeof(q));
+        q.shape = static_cast<int32_t>(p.shape);
+        q.channel_id = p.channel_id;
+        q.cx = p.cx; q.cy = p.cy; q.r_min = p.r_min; q.r_max = p.r_max;
+        q.phi_min = p.phi_min; q.phi_max = p.phi_max; q.fill_fraction = p.fill_fraction;
+        out.push_back(q);
+    }
+    return out;
+}
+
 inline cmpmc_detector to_c(const cmpmc::DetectorModel& d) {
-    if (d.mesh_field_3d.has_value() || d.mesh_field_2d.has_value())
-        throw std::invalid_argument("mesh fields are not available through this adapter");
+    if (d.mesh_field_2d.has_value())
+        throw std::invalid_argument("2D mesh fields are not available on the device");
     cmpmc_detector o;
     std::memset(&o, 0, sizeof(o));
     o.radius = d.solid.radius;
@@ -125,7 +146,7 @@ inline cmpmc_detector to_c(const cmpmc::DetectorModel& d) {
         poly(s.anh_coeffs, t.anh_coeffs, t.n_anh);
         t.demo_values = s.demo_values ? 1 : 0;
         t.has_amm = s.amm_interface.has_value() ? 1 : 0;
-        t.has_mask = s.electrode_mask.has_value() ? 1 : 0;
+        t.has_mask = 0;  // the pads are attached to the context (GpuEngine constructor)
         if (s.kaplan_sensor.has_value()) {
             const cmpmc::KaplanFilm& f = *s.kaplan_sensor;
             t.has_film = 1;
@@ -163,17 +184,51 @@ inline cmpmc_detector to_c(const cmpmc::DetectorModel& d) {
 class GpuEngine {
 public:
     GpuEngine(const cmpmc::CrystalConfig& cfg, const cmpmc::DetectorModel& det, int device = 0)
-        : ccfg_(detail::to_c(cfg)), cdet_(detail::to_c(det)) {
+        : ccfg_(detail::to_c(cfg)), cdet_(detail::to_c(det)), needs_mesh_(det.mesh_field_3d.has_value()) {
         detail::check(cmpmc_lattice_create(&ccfg_, &lat_), nullptr, "lattice");
         const int st = cmpmc_gpu_create(lat_, &cdet_, device, &ctx_);
         if (st != CMPMC_OK) {
             cmpmc_lattice_destroy(lat_);
             detail::check(st, nullptr, "device context");
         }
+        for (int i = 0; i < 3; ++i) {
+            if (!det.surfaces[i].electrode_mask.has_value()) continue;
+            const auto pads = detail::pads_of(*det.surfaces[i].electrode_mask);
+            detail::check(cmpmc_gpu_set_electrode_mask(ctx_, i, pads.data(), pads.size()), ctx_, "electrode mask");
+        }
     }
     ~GpuEngine() {
         cmpmc_gpu_destroy(ctx_);
         cmpmc_lattice_destroy(lat_);
+        cmpmc_mesh_destroy(mesh_);
+    }
+
+    // DetectorModel::mesh_field_3d: the TriLinearMesh3D(vertices, potentials, tetrahedra)
+    // the detector was built with (mesh_field.hpp:47-58).
+    void set_mesh(const std::vector<cmpmc::Vec3>& vertices, const std::vector<double>& potentials,
+                  const std::vector<std::array<int, 4>>& tets, double v_min_clamp = -1e30, double v_max_clamp = 1e30) {
+        static_assert(sizeof(cmpmc::Vec3) == 3 * sizeof(double), "Vec3 layout");
+        std::vector<int32_t> t(4 * tets.size());
+        for (size_t i = 0; i < tets.size(); ++i)
+            for (int j = 0; j < 4; ++j) t[4 * i + j] = tets[i][j];
+        cmpmc_mesh* m = nullptr;
+        detail::check(cmpmc_mesh_create(reinterpret_cast<const double*>(vertices.data()), potentials.data(),
+                                        potentials.size(), t.data(), tets.size(), v_min_clamp, v_max_clamp, &m),
+                      nullptr, "mesh");
+        attach(m);
+    }
+    // The same for a mesh made by TriLinearMesh3D::build_cartesian_grid (mesh_field.hpp:131-189).
+    template <class PotentialFn>
+    void set_cartesian_mesh(double half_x, double half_y, double half_z, int nx, int ny, int nz, PotentialFn&& fn) {
+        using Fn = std::remove_reference_t<PotentialFn>;
+        auto thunk = [](const double p[3], void* user) -> double {
+            return (*static_cast<Fn*>(user))(cmpmc::Vec3{p[0], p[1], p[2]});
+        };
+        cmpmc_mesh* m = nullptr;
+        detail::check(cmpmc_mesh_build_cartesian(half_x, half_y, half_z, nx, ny, nz, thunk,
+                                                 const_cast<void*>(static_cast<const void*>(&fn)), &m),
+                      nullptr, "mesh");
+        attach(m);
     }
     GpuEngine(const GpuEngine&) = delete;
     GpuEngine& operator=(const GpuEngine&) = delete;
@@ -183,6 +238,8 @@ public:
     template <class Generator>
     cmpmc::RunResult run_events(uint64_t n_events, Generator&& generate, const cmpmc::RunOptions& options = {},
                                 const GpuRunOptions& gpu = {}) {
+        if (needs_mesh_ && !mesh_)
+            throw std::invalid_argument("the detector has a mesh field: hand it over with set_mesh or set_cartesian_mesh");
         const auto t0 = std::chrono::steady_clock::now();
         std::vector<uint64_t> rng(4 * n_events), ph_off(n_events + 1, 0), ch_off(n_events + 1, 0);
         std::vector<double> injected(n_events, 0.0);
@@ -238,6 +295,7 @@ public:
         }
         d.keep_hits = options.keep_hits ? 1 : 0;
         d.form = static_cast<int32_t>(gpu.form);
+        d.kaplan_surrogate = gpu.kaplan_surrogate ? 1 : 0;
         d.seed = options.seed;
         cmpmc_run_out out;
         detail::check(cmpmc_gpu_run_events(ctx_, &d, &out), ctx_, "run_events");
@@ -252,10 +310,22 @@ public:
     }
 
 private:
+    void attach(cmpmc_mesh* m) {
+        const int st = cmpmc_gpu_set_mesh(ctx_, m);
+        if (st != CMPMC_OK) {
+            cmpmc_mesh_destroy(m);
+            detail::check(st, ctx_, "mesh");
+        }
+        cmpmc_mesh_destroy(mesh_);
+        mesh_ = m;
+    }
+
     cmpmc_crystal_config ccfg_;
     cmpmc_detector cdet_;
+    bool needs_mesh_ = false;
     cmpmc_lattice* lat_ = nullptr;
     cmpmc_gpu_ctx* ctx_ = nullptr;
+    cmpmc_mesh* mesh_ = nullptr;
 };
 
 }  // namespace cmpmc_b200

@@ -32,6 +32,22 @@ int main() {
         const RunResult c = run_events(engine, 203, gen, opt);
         std::printf("device hits %zu cpu hits %zu steps %llu vs %llu\n", r.hits.size(), c.hits.size(),
                     (unsigned long long)r.stats.total_steps, (unsigned long long)c.stats.total_steps);
+        // electrode masks (copied from the surfaces) and a mesh field (handed over once)
+        DetectorModel det2 = det;
+        const double R = det.solid.radius, h = det.solid.half_z;
+        auto pot = [h](const Vec3& p) { return 2.0 * (p.z + h) / (2.0 * h); };
+        for (int f = 0; f < 2; ++f)
+            det2.surfaces[f].electrode_mask = geometry::ElectrodePatternMask::supercdms_qet_mask(R, 0.8);
+        det2.mesh_field_3d = geometry::TriLinearMesh3D::build_cartesian_grid(R, R, h, 8, 8, 8, pot);
+        const SimulationEngine engine2(lattice, det2);
+        cmpmc_b200::GpuEngine gpu2(lattice.config(), det2);
+        gpu2.set_cartesian_mesh(R, R, h, 8, 8, 8, pot);
+        const RunResult m = gpu2.run_events(203, gen, opt);
+        const RunResult mc = run_events(engine2, 203, gen, opt);
+        size_t on_pad = 0;
+        for (const SensorHit& x : m.hits) on_pad += (x.channel_id >= 0);
+        std::printf("masked + mesh: device hits %zu (%zu on pads) cpu hits %zu\n", m.hits.size(), on_pad,
+                    mc.hits.size());
         return 0;
     } catch (const std::runtime_error& e) {
         std::printf("device unavailable: %s\n", e.what());
