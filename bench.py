@@ -184,6 +184,8 @@ def main() -> None:
     ap.add_argument("--cpu-events", type=int, default=1000)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-configuration autotuner")
+    ap.add_argument("--no-graph", action="store_true", help="eager launches instead of CUDA-graph replay")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -262,6 +264,20 @@ def main() -> None:
         return float(t.item())
 
     dd = desc(True)
+    # launch configuration from the project's autotuner (results do not depend on it), then
+    # CUDA-graph replay of the device-resident call
+    tune = None
+    if not args.no_tune:
+        tr = _ffi.TuneResultC()
+        if lib.cmpmc_gpu_autotune(h, C.byref(dd), 1, C.byref(tr)) != 0:
+            buf = C.create_string_buffer(512)
+            lib.cmpmc_gpu_last_error(h, buf, 512)
+            raise RuntimeError(buf.value.decode())
+        tune = {"threads_per_block": tr.threads_per_block, "blocks_per_sm": tr.blocks_per_sm,
+                "best_kernel_ms": tr.best_ms, "default_kernel_ms": tr.first_ms,
+                "tried": [[tr.tried_tpb[i], tr.tried_bps[i], round(tr.tried_ms[i], 2)] for i in range(tr.n_tried)]}
+    if not args.no_graph:
+        lib.cmpmc_gpu_configure_graph(h, 1)
     for _ in range(args.warmup):
         flush.zero_()
         run(dd)
@@ -292,6 +308,7 @@ def main() -> None:
         return t
     hp = [pinned(packed.rng_state), pinned(packed.injected_eV), pinned(packed.phonon_offsets), pinned(packed.phonons)]
     hd = desc(False, tuple(t.data_ptr() for t in hp))
+    lib.cmpmc_gpu_configure_graph(h, 0)
     run(hd)
     barrier()
     e2e_ms = []
@@ -336,6 +353,7 @@ def main() -> None:
                      "peak_kind": peak_kind, "bytes_per_step": BYTES_PER_STEP,
                      "traffic": (tps * steps_per_launch if tps else None)},
         "gpu_launches": launches,
+        "launch": {"graph": not args.no_graph, "autotune": tune},
         "clocks": clocks.summary(),
         "wall_s_timed": wall,
         "generator_s": t_gen,

@@ -151,6 +151,17 @@ class AdjointOutC(C.Structure):
 # double (*)(const double p[3], void* user): node potential of cmpmc_mesh_build_cartesian
 POTENTIAL_FN = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p)
 
+TUNE_MAX = 16
+
+
+class TuneResultC(C.Structure):
+    _fields_ = [
+        ("threads_per_block", _i32), ("blocks_per_sm", _i32), ("queue_capacity", _u64), ("best_ms", _f64),
+        ("first_ms", _f64), ("n_tried", _i32), ("_pad0", _i32), ("tried_tpb", _i32 * TUNE_MAX),
+        ("tried_bps", _i32 * TUNE_MAX), ("tried_queue", _u64 * TUNE_MAX), ("tried_ms", _f64 * TUNE_MAX),
+    ]
+
+
 _SIG = {
     "cmpmc_abi_sizes": (_i32, [C.POINTER(C.c_size_t), _i32]),
     "cmpmc_crystal_config_germanium": (None, [C.POINTER(CrystalConfigC)]),
@@ -193,6 +204,9 @@ _SIG = {
     "cmpmc_mesh_potential_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
     "cmpmc_gpu_set_mesh": (_i32, [C.c_void_p, C.c_void_p]),
     "cmpmc_gpu_configure_queue": (_i32, [C.c_void_p, _u64]),
+    "cmpmc_gpu_configure_graph": (_i32, [C.c_void_p, _i32]),
+    "cmpmc_gpu_memcpy": (_i32, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "cmpmc_gpu_autotune": (_i32, [C.c_void_p, C.POINTER(RunDescC), _i32, C.POINTER(TuneResultC)]),
     "cmpmc_kaplan_surrogate_create": (_i32, [C.POINTER(FilmConfigC), _u64, C.POINTER(C.c_void_p)]),
     "cmpmc_kaplan_surrogate_destroy": (None, [C.c_void_p]),
     "cmpmc_kaplan_surrogate_info": (_i32, [C.c_void_p, C.POINTER(_u64), C.POINTER(_u64)]),

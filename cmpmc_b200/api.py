@@ -814,6 +814,24 @@ class SimulationEngine:
         if queue_capacity:
             _check(self._lib.cmpmc_gpu_configure_queue(h, int(queue_capacity)), h)
 
+    def configure_graph(self, enable: bool = True, device: int = 0) -> None:
+        """Replay repeated batched calls on device-resident inputs as one CUDA graph."""
+        h = self.context(device)
+        _check(self._lib.cmpmc_gpu_configure_graph(h, int(enable)), h)
+
+    def autotune(self, ev: "PackedEvents", options: "RunOptions", repeats: int = 2) -> dict:
+        """Times the launch-configuration candidates on this batch and keeps the fastest
+        (cmpmc_gpu_autotune); returns the choice and every candidate's kernel time."""
+        h = self.context(options.device)
+        keep = []
+        d = self._desc(ev, options, keep)
+        r = _ffi.TuneResultC()
+        _check(self._lib.cmpmc_gpu_autotune(h, C.byref(d), int(repeats), C.byref(r)), h, "autotune")
+        tried = [{"threads_per_block": r.tried_tpb[i], "blocks_per_sm": r.tried_bps[i],
+                  "queue_capacity": r.tried_queue[i], "kernel_ms": r.tried_ms[i]} for i in range(r.n_tried)]
+        return {"threads_per_block": r.threads_per_block, "blocks_per_sm": r.blocks_per_sm,
+                "queue_capacity": r.queue_capacity, "best_ms": r.best_ms, "first_ms": r.first_ms, "tried": tried}
+
     def make_track(self, pos, k_dir, mode, energy_eV, time_s=0.0, weight=1.0) -> np.ndarray:
         out = np.zeros((), dtype=_ffi.PHONON_DTYPE)
         p = (C.c_double * 3)(*pos)
@@ -877,19 +895,18 @@ class SimulationEngine:
         return PackedEvents(n, first_event, rng_state, inj, po, ph, co, ch)
 
     # -- device run ----------------------------------------------------------------------------
-    def run_packed(self, ev: PackedEvents, options: RunOptions) -> RunResult:
-        h = self.context(options.device)
-        n = ev.n_events
-        has_charges = ev.charges.size > 0
+    @staticmethod
+    def _desc(ev: PackedEvents, options: RunOptions, keep: list) -> _ffi.RunDescC:
         d = _ffi.RunDescC()
-        d.n_events = n
+        d.n_events = ev.n_events
         d.first_event = ev.first_event
         ph = ev.phonons if ev.phonons.size else np.zeros(1, dtype=_ffi.PHONON_DTYPE)
+        keep.append(ph)
         d.rng_state = ev.rng_state.ctypes.data
         d.injected_eV = ev.injected_eV.ctypes.data
         d.phonon_offsets = ev.phonon_offsets.ctypes.data
         d.phonons = ph.ctypes.data
-        if has_charges:
+        if ev.charges.size > 0:
             d.charge_offsets = ev.charge_offsets.ctypes.data
             d.charges = ev.charges.ctypes.data
         d.keep_hits = int(options.keep_hits)
@@ -897,6 +914,13 @@ class SimulationEngine:
         d.seed = options.seed
         d.want_event_stats = int(options.want_event_stats)
         d.kaplan_surrogate = int(options.kaplan_surrogate)
+        return d
+
+    def run_packed(self, ev: PackedEvents, options: RunOptions) -> RunResult:
+        h = self.context(options.device)
+        n = ev.n_events
+        keep = []
+        d = self._desc(ev, options, keep)
         out = _ffi.RunOutC()
         _check(self._lib.cmpmc_gpu_run_events(h, C.byref(d), C.byref(out)), h)
         nh = int(out.n_hits)

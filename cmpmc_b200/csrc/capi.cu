@@ -102,6 +102,12 @@ struct cmpmc_gpu_ctx {
     bool lut_ready = false;
     DevBuf queue, resume_a, resume_b, ccounters, carrier_event, cursor;  // batched charge form
     uint64_t queue_cap = 1ull << 24;                    // Luke-phonon queue entries (64 B each)
+    // CUDA-graph replay of the batched phonon call (cmpmc_gpu_configure_graph)
+    bool graph_enabled = false;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<uint64_t> graph_key;
+    uint64_t graph_hits_cap = 0;                        // hit records the captured merge can write
+    int graph_launches = 0;
     const float* cdf_f = nullptr;              // FP32 copies of the decay tables (in `tables`)
     HostBuf h_hits, h_offsets, h_evstats, h_total, h_counters;
     cudaEvent_t e_start = nullptr, e_k0 = nullptr, e_k1 = nullptr, e_end = nullptr;
@@ -131,6 +137,23 @@ int cuda_fail(cmpmc_gpu_ctx* ctx, cudaError_t e, const char* what) {
         cudaError_t _e = (call);                           \
         if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); \
     } while (0)
+
+void drop_graph(cmpmc_gpu_ctx* ctx) {
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+    ctx->graph_exec = nullptr;
+    ctx->graph_key.clear();
+}
+
+// The call signature a captured graph is valid for: the descriptor's pointers and sizes
+// and the context's launch configuration (device buffers only move when an eager call
+// grows them, and every eager call recaptures).
+std::vector<uint64_t> graph_key_of(const cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d) {
+    return {d->n_events, d->first_event, reinterpret_cast<uint64_t>(d->rng_state),
+            reinterpret_cast<uint64_t>(d->injected_eV), reinterpret_cast<uint64_t>(d->phonon_offsets),
+            reinterpret_cast<uint64_t>(d->phonons), static_cast<uint64_t>(d->keep_hits), d->seed,
+            static_cast<uint64_t>(d->want_event_stats), static_cast<uint64_t>(d->kaplan_surrogate),
+            static_cast<uint64_t>(ctx->tpb), static_cast<uint64_t>(ctx->bps), ctx->stack_cap_batched, ctx->hit_cap};
+}
 
 // Builds (once per context) the Kaplan surrogate table of every film on the host
 // (KaplanSurrogateLUT, reference seed 1337) and copies it to the device
@@ -337,6 +360,12 @@ int cmpmc_gpu_device_count(int* count) {
     return (e == cudaSuccess && n > 0) ? CMPMC_OK : CMPMC_ERR_NO_DEVICE;
 }
 
+int cmpmc_gpu_memcpy(void* dst, const void* src, size_t bytes) {
+    if (!bytes) return CMPMC_OK;
+    if (!dst || !src) return CMPMC_ERR_INVALID;
+    return cudaMemcpy(dst, src, bytes, cudaMemcpyDefault) == cudaSuccess ? CMPMC_OK : CMPMC_ERR_CUDA;
+}
+
 int cmpmc_gpu_math_check(int device, uint64_t n, const double* x, double* out) {
     if (!x || !out) return CMPMC_ERR_INVALID;
     if (cudaSetDevice(device) != cudaSuccess) return CMPMC_ERR_NO_DEVICE;
@@ -433,6 +462,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
         b->release();
     for (HostBuf* b : {&ctx->h_hits, &ctx->h_offsets, &ctx->h_evstats, &ctx->h_total, &ctx->h_counters})
         b->release();
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     for (cudaEvent_t ev : {ctx->e_start, ctx->e_k0, ctx->e_k1, ctx->e_end})
         if (ev) cudaEventDestroy(ev);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -487,6 +517,101 @@ int cmpmc_gpu_set_electrode_mask(cmpmc_gpu_ctx* ctx, int surface, const cmpmc_el
     CK(cudaMemcpy(ctx->pads[surface].p, p.data(), n * sizeof(Pad), cudaMemcpyHostToDevice), "copy pads");
     ctx->D.surf[surface].pads = ctx->pads[surface].as<Pad>();
     ctx->D.surf[surface].n_pads = static_cast<int>(n);
+    return CMPMC_OK;
+}
+
+int cmpmc_gpu_autotune(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* sample, int repeats, cmpmc_tune_result* out) {
+    if (!ctx || !sample || !out) return CMPMC_ERR_INVALID;
+    std::memset(out, 0, sizeof(*out));
+    repeats = std::max(1, std::min(repeats, 16));
+    const bool batched = sample->form == CMPMC_FORM_BATCHED_FP32;
+    const bool charges = batched && sample->charge_offsets != nullptr;
+    const int tpb0 = ctx->tpb, bps0 = ctx->bps;
+    const uint64_t q0 = ctx->queue_cap;
+    auto time_run = [&](double& best) -> int {
+        best = 1e300;
+        for (int r = 0; r < repeats; ++r) {
+            cmpmc_run_out o;
+            const int st = cmpmc_gpu_run_events(ctx, sample, &o);
+            if (st != CMPMC_OK) return st;
+            best = std::min(best, static_cast<double>(o.kernel_ms));
+        }
+        return CMPMC_OK;
+    };
+    auto record = [&](int tpb, int bps, uint64_t q, double ms) {
+        if (out->n_tried < CMPMC_TUNE_MAX) {
+            out->tried_tpb[out->n_tried] = tpb;
+            out->tried_bps[out->n_tried] = bps;
+            out->tried_queue[out->n_tried] = q;
+            out->tried_ms[out->n_tried] = ms;
+            ++out->n_tried;
+        }
+    };
+    // the configuration in place first (it also sizes every buffer)
+    double ms = 0.0;
+    int st = time_run(ms);
+    if (st != CMPMC_OK) return st;
+    out->first_ms = ms;
+    int best_tpb = tpb0, best_bps = bps0;
+    uint64_t best_q = q0;
+    double best_ms = ms;
+    record(tpb0, bps0, q0, ms);
+    // block shapes: 64 or 128 threads, the occupancy limit and three quarters / half of it
+    for (int tpb : {64, 128}) {
+        int occ = 1;
+        CK(charges ? charges_fp32_occupancy(tpb, &occ)
+                   : (batched ? batched_fp32_occupancy(tpb, &occ) : plain_fp64_occupancy(tpb, &occ)),
+           "occupancy");
+        occ = std::max(occ, 1);
+        int tried[3] = {occ, std::max(1, (3 * occ) / 4), std::max(1, occ / 2)};
+        for (int k = 0; k < 3; ++k) {
+            const int bps = tried[k];
+            if ((k > 0 && bps == tried[k - 1]) || (k > 1 && bps == tried[0])) continue;
+            ctx->tpb = tpb;
+            ctx->bps = bps;
+            st = time_run(ms);
+            if (st != CMPMC_OK) break;
+            record(tpb, bps, ctx->queue_cap, ms);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_tpb = tpb;
+                best_bps = bps;
+            }
+        }
+        if (st != CMPMC_OK) break;
+    }
+    // queue depth of the charge phases, with the best block shape
+    if (st == CMPMC_OK && charges) {
+        ctx->tpb = best_tpb;
+        ctx->bps = best_bps;
+        for (uint64_t q : {1ull << 20, 1ull << 22, 1ull << 24}) {
+            if (q == q0) continue;
+            ctx->queue_cap = q;
+            st = time_run(ms);
+            if (st != CMPMC_OK) break;
+            record(best_tpb, best_bps, q, ms);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_q = q;
+            }
+        }
+    }
+    ctx->tpb = best_tpb;
+    ctx->bps = best_bps;
+    ctx->queue_cap = best_q;
+    drop_graph(ctx);
+    if (st != CMPMC_OK) return st;
+    out->threads_per_block = best_tpb;
+    out->blocks_per_sm = best_bps;
+    out->queue_capacity = best_q;
+    out->best_ms = best_ms;
+    return CMPMC_OK;
+}
+
+int cmpmc_gpu_configure_graph(cmpmc_gpu_ctx* ctx, int enable) {
+    if (!ctx) return CMPMC_ERR_INVALID;
+    ctx->graph_enabled = enable != 0;
+    if (!ctx->graph_enabled) drop_graph(ctx);
     return CMPMC_OK;
 }
 
@@ -621,6 +746,31 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
         const int st = run_charges_batched(ctx, d, a, n, n_ph, n_ch, launches, hc, kms, n_hits, ev_offsets, ev_stats);
         if (st != CMPMC_OK) return st;
     } else {
+        // ---- CUDA-graph replay: the same device-resident batch again ----------------------
+        const bool graph_ok = ctx->graph_enabled && batched && n > 0 && d->inputs_on_device && d->outputs_on_device;
+        if (graph_ok && ctx->graph_exec && ctx->graph_key == graph_key_of(ctx, d)) {
+            CK(cudaGraphLaunch(ctx->graph_exec, s), "graph launch");
+            CK(cudaStreamSynchronize(s), "graph");
+            hc = *ctx->h_counters.as<Counters>();
+            const bool over = hc.err != 0 || (d->keep_hits && (hc.hit_count > ctx->hit_cap ||
+                                                              hc.hit_count > ctx->graph_hits_cap));
+            if (!over) {
+                CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
+                float tms = 0.0f;
+                CK(cudaEventElapsedTime(&tms, ctx->e_start, ctx->e_end), "event time");
+                out->stats = *ctx->h_total.as<cmpmc_sim_stats>();
+                out->n_hits = d->keep_hits ? hc.hit_count : 0;
+                out->hits = ctx->hits_out.as<cmpmc_sensor_hit>();
+                out->hit_offsets = ctx->ev_offsets.as<uint64_t>();
+                out->event_stats = d->want_event_stats ? ctx->ev_stats2.as<cmpmc_sim_stats>() : nullptr;
+                out->kernel_ms = kms;
+                out->total_ms = tms;
+                out->device_error = 0;
+                out->kernel_launches = static_cast<uint32_t>(ctx->graph_launches);
+                return CMPMC_OK;
+            }
+            drop_graph(ctx);  // a buffer overflowed: rerun eagerly with more room (and recapture)
+        }
 
         // ---- work units: events (plain form) or primary phonons (batched form) ---------
         const uint64_t units = batched ? n_ph : n;
@@ -725,6 +875,46 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
         } else {
             CK(cudaMemsetAsync(ev_offsets, 0, 8, s), "memset offsets");
             CK(cudaMemsetAsync(ctx->total.p, 0, sizeof(cmpmc_sim_stats), s), "memset totals");
+        }
+        // ---- capture the clean call for replay: counters, unit map, transport, merge, and
+        // the copies of the counters and totals, as one graph; the timing events are
+        // external event-record nodes, so a replay can be timed like the eager call --------
+        if (graph_ok) {
+            drop_graph(ctx);
+            CK(ctx->h_total.ensure(sizeof(cmpmc_sim_stats)), "alloc host totals");
+            const uint64_t out_cap = ctx->hits_out.cap / sizeof(cmpmc_sensor_hit);
+            int gl = 0;
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+            cudaError_t e = cudaEventRecordWithFlags(ctx->e_start, s, cudaEventRecordExternal);
+            if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s);
+            if (e == cudaSuccess) e = launch_unit_event(a.ph_off, n, ctx->unit_event.as<uint32_t>(), s), ++gl;
+            if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->e_k0, s, cudaEventRecordExternal);
+            if (e == cudaSuccess)
+                e = launch_batched_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->unit_event.as<uint32_t>(),
+                                        static_cast<int>(grid), ctx->tpb, s), ++gl;
+            if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->e_k1, s, cudaEventRecordExternal);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(ctx->h_counters.p, ctx->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess)
+                e = launch_batched_finish(a, n, a.ph_off, a.injected, ctx->offsets.as<uint64_t>(), ev_offsets,
+                                          ctx->hits_out.as<cmpmc_sensor_hit>(), out_cap, ctx->total.as<cmpmc_sim_stats>(),
+                                          ctx->partials.as<cmpmc_sim_stats>(), d->want_event_stats ? ev_stats : nullptr,
+                                          s, &gl);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(ctx->h_total.p, ctx->total.p, sizeof(cmpmc_sim_stats), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->e_end, s, cudaEventRecordExternal);
+            const cudaError_t ec = cudaStreamEndCapture(s, &g);
+            if (e == cudaSuccess) e = ec;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                ctx->graph_exec = nullptr;
+                return cuda_fail(ctx, e, "graph capture");
+            }
+            ctx->graph_key = graph_key_of(ctx, d);
+            ctx->graph_hits_cap = out_cap;
+            ctx->graph_launches = gl;
         }
     }
     CK(ctx->h_total.ensure(sizeof(cmpmc_sim_stats)), "alloc host totals");

@@ -369,11 +369,41 @@ int cmpmc_gpu_last_error(const cmpmc_gpu_ctx* ctx, char* buf, size_t size);
 int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_per_sm,
                         uint64_t stack_capacity, uint64_t hit_capacity);
 int cmpmc_gpu_device_count(int* count);
+/* Synchronous copy between any two pointers (host or device, unified addressing): reads
+ * outputs left on the device (outputs_on_device = 1) without a CUDA binding of your own. */
+int cmpmc_gpu_memcpy(void* dst, const void* src, size_t bytes);
 /* Batched FP32 form with charges: capacity of the device Luke-phonon queue in entries
  * (64 B each, default 2^24). Carriers queue their tracked Luke phonons there; when it is
  * full they are parked and resumed after the queued phonons have been transported, so a
  * small queue only adds phases. 0 keeps the current value. */
 int cmpmc_gpu_configure_queue(cmpmc_gpu_ctx* ctx, uint64_t queue_capacity);
+/* CUDA-graph replay (no counterpart in the reference): with enable = 1, a batched-form call
+ * of phonon events whose inputs and outputs stay on the device is captured after it ran
+ * cleanly (counters, transport, merge and the copies of the counters and totals as one
+ * graph) and replayed by later calls with the same descriptor pointers, sizes and
+ * configuration: one graph launch per call. A replay whose buffers overflow falls back to
+ * the eager call, which grows them and recaptures. */
+int cmpmc_gpu_configure_graph(cmpmc_gpu_ctx* ctx, int enable);
+
+/* Autotuner of the launch configuration (no counterpart in the reference): runs `sample`
+ * (a representative call, outputs discarded) `repeats` times for each candidate, keeps the
+ * fastest transport-kernel time and applies it to the context. Candidates: the current
+ * configuration; 64 and 128 threads per block at the occupancy limit and at 3/4 and 1/2 of
+ * it; for the batched charge form also Luke-phonon queues of 2^20, 2^22 and 2^24 entries.
+ * The batched results do not depend on the configuration (every unit owns its substream). */
+#define CMPMC_TUNE_MAX 16
+typedef struct cmpmc_tune_result {
+    int32_t threads_per_block, blocks_per_sm;   /* chosen */
+    uint64_t queue_capacity;                    /* chosen (charge runs) */
+    double best_ms;                             /* its transport-kernel time */
+    double first_ms;                            /* the configuration in place before tuning */
+    int32_t n_tried, _pad0;
+    int32_t tried_tpb[CMPMC_TUNE_MAX], tried_bps[CMPMC_TUNE_MAX];
+    uint64_t tried_queue[CMPMC_TUNE_MAX];
+    double tried_ms[CMPMC_TUNE_MAX];
+} cmpmc_tune_result;
+int cmpmc_gpu_autotune(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* sample, int repeats, cmpmc_tune_result* out);
+
 /* SurfaceProperty::electrode_mask (surface_property.hpp:45, evaluated at engine.hpp:284-289
  * and 483-488): attaches n pads to surface `surface` (CMPMC_SURF_*) of the context's
  * detector and copies them to the device; n = 0 removes the mask. A phonon or carrier
