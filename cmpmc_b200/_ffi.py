@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libcmpmc_b200.so")
 ABI_VERSION = 1
 
 OK, ERR_INVALID, ERR_CUDA, ERR_UNVALIDATED, ERR_CAPACITY, ERR_DEVICE, ERR_NO_DEVICE = range(7)
-FORM_PLAIN_FP64, FORM_BATCHED_FP32 = 0, 1
+FORM_PLAIN_FP64, FORM_BATCHED_FP32, FORM_BATCHED_FP32_INLINE = 0, 1, 2
 WL_SINGLE_L_ORIGIN, WL_MIXED_ENERGY, WL_PAIR_DRIFT, WL_SINGLE_L_VOLUME, WL_TEST_PARALLEL = 0, 1, 2, 4, 5
 WL_RECOIL, WL_RECOIL_LIGHT = 3, 6
 

@@ -691,7 +691,7 @@ class RunOptions:
     seed: int = 1
     events_per_chunk: int = 16
     keep_hits: bool = True
-    form: str = "plain_fp64"  # or "batched_fp32"
+    form: str = "plain_fp64"  # "batched_fp32" (wavefront split) or "batched_fp32_inline"
     device: int = 0
     want_event_stats: bool = False
     first_event: int = 0
@@ -910,7 +910,11 @@ class SimulationEngine:
             d.charge_offsets = ev.charge_offsets.ctypes.data
             d.charges = ev.charges.ctypes.data
         d.keep_hits = int(options.keep_hits)
-        d.form = _ffi.FORM_BATCHED_FP32 if options.form == "batched_fp32" else _ffi.FORM_PLAIN_FP64
+        forms = {"plain_fp64": _ffi.FORM_PLAIN_FP64, "batched_fp32": _ffi.FORM_BATCHED_FP32,
+                 "batched_fp32_inline": _ffi.FORM_BATCHED_FP32_INLINE}
+        if options.form not in forms:
+            raise ValueError(f"unknown form {options.form!r}: one of {sorted(forms)}")
+        d.form = forms[options.form]
         d.seed = options.seed
         d.want_event_stats = int(options.want_event_stats)
         d.kaplan_surrogate = int(options.kaplan_surrogate)

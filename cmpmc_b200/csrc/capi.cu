@@ -101,6 +101,8 @@ struct cmpmc_gpu_ctx {
     DevBuf lut[3];                                      // Kaplan surrogate tables of the films
     bool lut_ready = false;
     DevBuf queue, resume_a, resume_b, ccounters, carrier_event, cursor;  // batched charge form
+    DevBuf film_a, film_b;                              // film-entry queues of the wavefront split
+    uint64_t film_cap = 1ull << 22;                     // film entries per phase (64 B each)
     uint64_t queue_cap = 1ull << 24;                    // Luke-phonon queue entries (64 B each)
     // CUDA-graph replay of the batched phonon call (cmpmc_gpu_configure_graph)
     bool graph_enabled = false;
@@ -349,6 +351,162 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
     return CMPMC_OK;
 }
 
+// The batched phonon form with the wavefront split: phase 0 transports the generator's
+// phonons until each one dies or reaches an active film (queued as a FilmRec); then film
+// phases (cascades, hits, re-emitted phonons queued as QPhonon) alternate with transport
+// phases over the re-emitted phonons until both queues are empty. Every unit owns its
+// substream, so the phases' order does not change any track; units add to per-event sinks.
+// A queue, stack or hit-staging overflow reruns the whole call with more room.
+int run_split_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, uint64_t n, uint64_t n_ph,
+                      int& launches, Counters& hc, float& kms, uint64_t& n_hits, uint64_t*& ev_offsets,
+                      cmpmc_sim_stats*& ev_stats) {
+    cudaStream_t s = ctx->stream;
+    const int tpb = ctx->tpb;
+    int bps_ph = ctx->bps, bps_f = ctx->bps;
+    if (!bps_ph) {
+        CK(batched_fp32_occupancy(tpb, &bps_ph), "occupancy");
+        bps_ph = std::max(bps_ph, 1);
+    }
+    if (!bps_f) {
+        CK(film_fp32_occupancy(tpb, &bps_f), "occupancy");
+        bps_f = std::max(bps_f, 1);
+    }
+    const uint64_t grid_ph = static_cast<uint64_t>(ctx->num_sms) * bps_ph;
+    const uint64_t grid_f = static_cast<uint64_t>(ctx->num_sms) * bps_f;
+    CK(ctx->ev_stats2.ensure(std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats)), "alloc event stats");
+    CK(ctx->ev_nhits.ensure(std::max<uint64_t>(n, 1) * 8), "alloc event hit counts");
+    CK(ctx->ev_offsets.ensure((n + 1) * 8), "alloc event offsets");
+    CK(ctx->cursor.ensure(std::max<uint64_t>(n, 1) * 8), "alloc event cursors");
+    CK(ctx->counters.ensure(sizeof(Counters)), "alloc counters");
+    CK(ctx->ccounters.ensure(sizeof(ChargeCounters)), "alloc phase counters");
+    CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
+    CK(ctx->partials.ensure(kReducePartials * sizeof(cmpmc_sim_stats)), "alloc partial totals");
+    CK(ctx->h_counters.ensure(sizeof(Counters) + sizeof(ChargeCounters)), "alloc host counters");
+    if (n_ph) CK(ctx->unit_event.ensure(n_ph * 4), "alloc unit map");
+    if (n_ph) {
+        CK(launch_unit_event(a.ph_off, n, ctx->unit_event.as<uint32_t>(), s), "unit map");
+        ++launches;
+    }
+    a.ev_sink = 1;
+    a.ev_stats = ctx->ev_stats2.as<cmpmc_sim_stats>();
+    a.ev_nhits = ctx->ev_nhits.as<uint64_t>();
+    Counters* dc = ctx->counters.as<Counters>();
+    a.hit_count = &dc->hit_count;
+    a.next_work = &dc->next_work;
+    a.err = &dc->err;
+    ChargeCounters* pc = ctx->ccounters.as<ChargeCounters>();  // q_tail: re-emissions, resume_next: film entries
+    a.reemit_tail = &pc->q_tail;
+    a.film_tail = &pc->resume_next;
+    char* hbuf = ctx->h_counters.as<char>();
+
+    uint64_t hit_cap = ctx->hit_cap;
+    if (!hit_cap) hit_cap = std::max<uint64_t>(1u << 20, n_ph * 32);
+    uint32_t& stack_cap = ctx->stack_cap_batched;
+    const uint64_t slots = grid_ph * tpb;
+    for (int attempt = 0;; ++attempt) {
+        if (!d->keep_hits) hit_cap = 1;
+        // a primary's lineage (decay daughters included) reaches a film a few times per round
+        ctx->film_cap = std::max<uint64_t>(ctx->film_cap, std::min<uint64_t>(8 * n_ph, 1ull << 26));
+        const uint64_t q_cap = std::max<uint64_t>(ctx->queue_cap, 64), f_cap = std::max<uint64_t>(ctx->film_cap, 64);
+        CK(ctx->queue.ensure(q_cap * sizeof(QPhonon)), "alloc phonon queue");
+        CK(ctx->film_a.ensure(f_cap * sizeof(FilmRec)), "alloc film queue");
+        CK(ctx->film_b.ensure(f_cap * sizeof(FilmRec)), "alloc film queue");
+        CK(ctx->stack.ensure(slots * stack_cap * batched_stack_entry_bytes()), "alloc phonon stacks");
+        CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
+        CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
+        a.stack = ctx->stack.as<GTrack>();
+        a.stack_cap = stack_cap;
+        a.hit_stage = ctx->hit_stage.as<cmpmc_sensor_hit>();
+        a.hit_key = ctx->hit_key.as<uint64_t>();
+        a.hit_cap = hit_cap;
+        a.reemit = ctx->queue.as<QPhonon>();
+        a.reemit_cap = q_cap;
+        a.film_cap = f_cap;
+        FilmRec* f_in = ctx->film_a.as<FilmRec>();
+        FilmRec* f_out = ctx->film_b.as<FilmRec>();
+        CK(cudaMemsetAsync(ctx->ev_stats2.p, 0, std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats), s), "memset");
+        CK(cudaMemsetAsync(ctx->ev_nhits.p, 0, std::max<uint64_t>(n, 1) * 8, s), "memset");
+        CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s), "memset counters");
+        CK(cudaMemsetAsync(ctx->ccounters.p, 0, sizeof(ChargeCounters), s), "memset counters");
+        CK(cudaEventRecord(ctx->e_k0, s), "event");
+        // phase 0: the generator's phonons, film entries into f_in
+        a.film = f_in;
+        if (n_ph) {
+            a.n_events = n_ph;
+            CK(launch_batched_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->unit_event.as<uint32_t>(),
+                                   static_cast<int>(std::min<uint64_t>(grid_ph, (n_ph + tpb - 1) / tpb)), tpb, s),
+               "phonon launch");
+            ++launches;
+        }
+        bool overflow = false;
+        for (int round = 0;; ++round) {
+            CK(cudaMemcpyAsync(hbuf + sizeof(Counters), pc, sizeof(ChargeCounters), cudaMemcpyDeviceToHost, s),
+               "copy counters");
+            CK(cudaStreamSynchronize(s), "transport phase");
+            const ChargeCounters h1 = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
+            if (h1.resume_next > f_cap) overflow = true;
+            const uint64_t n_f = std::min<uint64_t>(h1.resume_next, f_cap);
+            if (n_f == 0 || overflow) break;
+            // film phase: cascades of f_in, re-emissions into the phonon queue
+            CK(cudaMemsetAsync(&pc->q_tail, 0, sizeof(unsigned long long), s), "memset counters");
+            CK(launch_film_fp32(ctx->L, ctx->cdf_f, ctx->D, a, f_in, n_f,
+                                static_cast<int>(std::min<uint64_t>(grid_f, (n_f + tpb - 1) / tpb)), tpb, s),
+               "film launch");
+            ++launches;
+            CK(cudaMemcpyAsync(hbuf + sizeof(Counters), pc, sizeof(ChargeCounters), cudaMemcpyDeviceToHost, s),
+               "copy counters");
+            CK(cudaStreamSynchronize(s), "film phase");
+            const ChargeCounters h2 = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
+            if (h2.q_tail > q_cap) {
+                overflow = true;
+                break;
+            }
+            const uint64_t n_q = h2.q_tail;
+            if (n_q == 0) break;
+            // transport phase over the re-emitted phonons, film entries into the other buffer
+            std::swap(f_in, f_out);
+            a.film = f_in;
+            CK(cudaMemsetAsync(&pc->resume_next, 0, sizeof(unsigned long long), s), "memset counters");
+            CK(cudaMemsetAsync(&dc->next_work, 0, sizeof(unsigned long long), s), "memset work counter");
+            a.n_events = n_q;
+            CK(launch_queue_fp32(ctx->L, ctx->cdf_f, ctx->D, a, a.reemit,
+                                 static_cast<int>(std::min<uint64_t>(grid_ph, (n_q + tpb - 1) / tpb)), tpb, s),
+               "queue launch");
+            ++launches;
+        }
+        CK(cudaEventRecord(ctx->e_k1, s), "event");
+        CK(cudaMemcpyAsync(hbuf, ctx->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "copy counters");
+        CK(cudaStreamSynchronize(s), "transport kernels");
+        hc = *reinterpret_cast<const Counters*>(hbuf);
+        CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
+        const bool stack_over = (hc.err & kErrPhononStack) != 0;
+        const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
+        overflow = overflow || (hc.err & (kErrQueue | kErrFilmQueue)) != 0;
+        if (!stack_over && !hits_over && !overflow) break;
+        if (attempt >= 6) return fail(ctx, CMPMC_ERR_CAPACITY, "device queue, stack or hit buffer overflow persists");
+        if (stack_over) stack_cap = std::min<uint32_t>(stack_cap * 8, 1u << 20);
+        if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
+        if (overflow) {
+            ctx->queue_cap *= 2;
+            ctx->film_cap *= 2;
+        }
+        hc.err = 0;
+    }
+    a.film = nullptr;
+    if (d->keep_hits) ctx->hit_cap = std::max<uint64_t>(ctx->hit_cap, hit_cap);
+    if (hc.err) return fail(ctx, CMPMC_ERR_DEVICE, "transport kernels reported error word " + std::to_string(hc.err));
+    n_hits = d->keep_hits ? hc.hit_count : 0;
+    CK(ctx->hits_out.ensure(std::max<uint64_t>(n_hits, 1) * sizeof(cmpmc_sensor_hit)), "alloc hits");
+    CK(cudaMemsetAsync(ctx->cursor.p, 0, std::max<uint64_t>(n, 1) * 8, s), "memset cursors");
+    ev_offsets = ctx->ev_offsets.as<uint64_t>();
+    ev_stats = ctx->ev_stats2.as<cmpmc_sim_stats>();
+    a.n_events = n;
+    CK(launch_sink_finish(a, n, ev_offsets, ctx->cursor.as<unsigned long long>(), ctx->hits_out.as<cmpmc_sensor_hit>(),
+                          n_hits, ctx->total.as<cmpmc_sim_stats>(), ctx->partials.as<cmpmc_sim_stats>(), s, &launches),
+       "merge kernels");
+    return CMPMC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -453,7 +611,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
+    for (DevBuf* b : {&ctx->film_a, &ctx->film_b, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
                       &ctx->ccounters, &ctx->carrier_event, &ctx->cursor, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
@@ -663,12 +821,14 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     ctx->last_status = CMPMC_OK;
     ctx->last_error.clear();
     const uint64_t n = d->n_events;
-    if (d->form != CMPMC_FORM_PLAIN_FP64 && d->form != CMPMC_FORM_BATCHED_FP32)
+    if (d->form != CMPMC_FORM_PLAIN_FP64 && d->form != CMPMC_FORM_BATCHED_FP32 &&
+        d->form != CMPMC_FORM_BATCHED_FP32_INLINE)
         return fail(ctx, CMPMC_ERR_INVALID, "unknown transport form");
     if (n > (1ull << 31)) return fail(ctx, CMPMC_ERR_INVALID, "too many events in one call");
     if (n > 0 && (!d->rng_state || !d->injected_eV || !d->phonon_offsets))
         return fail(ctx, CMPMC_ERR_INVALID, "rng_state, injected_eV and phonon_offsets are required");
-    const bool batched = d->form == CMPMC_FORM_BATCHED_FP32;
+    const bool batched = d->form == CMPMC_FORM_BATCHED_FP32 || d->form == CMPMC_FORM_BATCHED_FP32_INLINE;
+    const bool split = d->form == CMPMC_FORM_BATCHED_FP32;
     const bool has_charges = d->charge_offsets != nullptr;
     std::string err;
     const int vst = validate_config(ctx->cfg, ctx->det, has_charges, err);
@@ -744,6 +904,10 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     if (batched && n_ch > 0) {
         // carriers and their Luke phonons: alternating charge / queue phases, event sinks
         const int st = run_charges_batched(ctx, d, a, n, n_ph, n_ch, launches, hc, kms, n_hits, ev_offsets, ev_stats);
+        if (st != CMPMC_OK) return st;
+    } else if (split) {
+        // phonons, wavefront split: transport phases and film phases, event sinks
+        const int st = run_split_batched(ctx, d, a, n, n_ph, launches, hc, kms, n_hits, ev_offsets, ev_stats);
         if (st != CMPMC_OK) return st;
     } else {
         // ---- CUDA-graph replay: the same device-resident batch again ----------------------

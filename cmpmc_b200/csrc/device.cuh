@@ -14,6 +14,7 @@ enum : unsigned {
     kErrChargeStack = 2u,
     kErrQueue = 4u,
     kErrResume = 8u,
+    kErrFilmQueue = 16u,
 };
 
 // A pushed phonon in a per-thread global-memory LIFO (112 B, 16-byte aligned)
@@ -65,10 +66,19 @@ struct RunArgs {
     int ev_sink;
     // batched form: film cascades from the surfaces' surrogate tables (Surface::lut_*)
     int surrogate;
+    // wavefront split of the batched form: film entries are queued (film, film_tail, up to
+    // film_cap) for the film kernel, which queues the re-emitted phonons (reemit, ...)
+    struct FilmRec* film;
+    uint64_t film_cap;
+    unsigned long long* film_tail;
+    struct QPhonon* reemit;
+    uint64_t reemit_cap;
+    unsigned long long* reemit_tail;
 };
 
-// Luke-phonon queue entry of the batched charge form (64 B). ev == kQEmpty marks a slot
-// that was reserved but not filled.
+// Phonon queue entry of the batched forms (64 B): Luke phonons of the charge form and
+// film re-emissions of the wavefront split. ev == kQEmpty marks a slot that was reserved
+// but not filled; `pad` carries the bounce count of a continuing track.
 constexpr uint32_t kQEmpty = 0xffffffffu;
 struct alignas(16) QPhonon {
     float px, py, pz, kx, ky, kz;
@@ -78,6 +88,19 @@ struct alignas(16) QPhonon {
     uint64_t key;  // substream key of this phonon
     uint32_t ev;   // event index within the call
     uint32_t pad;
+};
+
+// A film entry of the wavefront-split batched form (64 B): the phonon that reached an
+// active film, waiting for the film kernel. `key` seeds the cascade and the re-emissions.
+struct alignas(16) FilmRec {
+    float px, py, pz;
+    float w;
+    double E, t;
+    uint64_t key;
+    uint32_t ev;
+    int32_t ch_id;
+    uint32_t bounces;
+    uint8_t surf, mode, pad0, pad1;
 };
 
 // A carrier of the batched charge form between phases (96 B): a carrier whose queue
@@ -227,6 +250,12 @@ cudaError_t launch_charges_fp32(const Lattice& L, const float* cdf_f, const Dete
 cudaError_t charges_fp32_occupancy(int block, int* blocks_per_sm);
 cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                               const QPhonon* queue, int grid, int block, cudaStream_t s);
+// wavefront split of the batched form: the phonon kernels with a.film set stop a track at
+// film entry and queue it; the film kernel runs the queued cascades and queues the
+// re-emitted phonons in a.reemit
+cudaError_t launch_film_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
+                             const FilmRec* film, uint64_t n_film, int grid, int block, cudaStream_t s);
+cudaError_t film_fp32_occupancy(int block, int* blocks_per_sm);
 cudaError_t launch_carrier_event(const uint64_t* ch_off, uint64_t n_events, uint32_t* carrier_event,
                                  cudaStream_t s);
 // merge of the event-sink runs: injected energies, hit offsets, hits into event order

@@ -272,9 +272,11 @@ enum { kSrcInput = 0, kSrcQueue = 1 };
 // kSrc selects where units come from: the caller's primary phonon records (kSrcInput,
 // substream (event << 20 | index)) or the Luke-phonon queue of the charge form
 // (kSrcQueue, the entry's own substream key; empty slots are skipped).
-// kSink: units add to per-event sinks (runs with charges); kSur: film cascades from the
-// surrogate tables. Both are compile-time so the default kernel carries neither branch.
-template <bool kAdj, int kSrc = kSrcInput, bool kSink = false, bool kSur = false>
+// kSink: units add to per-event sinks (runs with charges, wavefront split); kSur: film
+// cascades from the surrogate tables; kSplit: a track that enters a film is queued for the
+// film kernel and ends here (wavefront split). All are compile-time, so the default kernel
+// carries none of their branches.
+template <bool kAdj, int kSrc = kSrcInput, bool kSink = false, bool kSur = false, bool kSplit = false>
 __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, const RunArgs& a,
                                              const uint32_t* __restrict__ unit_event,
                                              const QPhonon* __restrict__ queue, const AdjArgs& adj,
@@ -325,7 +327,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                     trk.E = q.E;
                     trk.t = q.t;
                     trk.w = q.w;
-                    trk.bounces = 0;
+                    trk.bounces = q.pad;
                     st = UStats{0, 0, 0, 0, 0, 0, 0, 0, 0, 0.0, 0.0};
                     n_hits = 0;
                     live = true;
@@ -423,6 +425,32 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
             if (active_pad && s.has_film && g.u() < static_cast<float>(s.prob_abs)) {
                 enter = g.u() < static_cast<float>(s.film.film_absorption);
                 if constexpr (kAdj) trk.s[3] += enter ? 1.0f : adj.film_miss_score;
+            }
+            if constexpr (kSplit) {
+                if (enter) {
+                    // film entry: hand the phonon to the film kernel and end the track here
+                    const unsigned long long slot = atomicAdd(a.film_tail, 1ull);
+                    if (slot < a.film_cap) {
+                        FilmRec r;
+                        r.px = trk.pos.x; r.py = trk.pos.y; r.pz = trk.pos.z;
+                        r.w = trk.w;
+                        r.E = trk.E;
+                        r.t = trk.t;
+                        const uint64_t hi = g.next();
+                        r.key = (hi << 32) | g.next();
+                        r.ev = ev_cur;
+                        r.ch_id = ch_id;
+                        r.bounces = trk.bounces;
+                        r.surf = static_cast<uint8_t>(bh.surf);
+                        r.mode = static_cast<uint8_t>(trk.mode);
+                        r.pad0 = r.pad1 = 0;
+                        a.film[slot] = r;
+                    } else {
+                        err |= kErrFilmQueue;
+                    }
+                    live = false;
+                    continue;
+                }
             }
             if (enter) {
                 int n_refl = 0;
@@ -586,23 +614,112 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
     if (err) atomicOr(a.err, err);
 }
 
-template <bool kSink, bool kSur>
+template <bool kSink, bool kSur, bool kSplit = false>
 __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__ FLat L,
                                                          const __grid_constant__ Detector D,
                                                          const __grid_constant__ RunArgs a,
                                                          const uint32_t* __restrict__ unit_event) {
     const AdjArgs none{};
-    batched_loop<false, kSrcInput, kSink, kSur>(L, D, a, unit_event, nullptr, none, nullptr, nullptr);
+    batched_loop<false, kSrcInput, kSink, kSur, kSplit>(L, D, a, unit_event, nullptr, none, nullptr, nullptr);
 }
 
-// The Luke-phonon queue of the batched charge form: one unit per queue entry
-template <bool kSur>
+// A phonon queue (Luke phonons, film re-emissions): one unit per queue entry
+template <bool kSur, bool kSplit = false>
 __global__ void __launch_bounds__(128, 8) k_queue_fp32(const __grid_constant__ FLat L,
                                                        const __grid_constant__ Detector D,
                                                        const __grid_constant__ RunArgs a,
                                                        const QPhonon* __restrict__ queue) {
     const AdjArgs none{};
-    batched_loop<false, kSrcQueue, true, kSur>(L, D, a, nullptr, queue, none, nullptr, nullptr);
+    batched_loop<false, kSrcQueue, true, kSur, kSplit>(L, D, a, nullptr, queue, none, nullptr, nullptr);
+}
+
+// The film kernel of the wavefront split: one queued film entry per thread. It runs the
+// Kaplan cascade (or the surrogate lookup) from the entry's own substream, records the hit
+// and the ledger in the entry's event, and queues the re-emitted phonons, each inward
+// Lambertian with a DOS mode and its own substream (the first keeps the bounce count).
+template <bool kSur>
+__global__ void __launch_bounds__(128, 8) k_film_fp32(const __grid_constant__ FLat L,
+                                                      const __grid_constant__ Detector D,
+                                                      const __grid_constant__ RunArgs a,
+                                                      const FilmRec* __restrict__ film, uint64_t n_film) {
+    double refl_buf[kKaplanCap];
+    double kwork[4 * kKaplanCap];
+    unsigned err = 0;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n_film;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const FilmRec r = film[i];
+        const Surface& s = D.surf[r.surf];
+        R128 g;
+        g.seed(r.key);
+        int n_refl = 0;
+        double edep;
+        if constexpr (kSur) {
+            edep = s.lut_abs ? surrogate_call(&s, r.E, refl_buf, &n_refl, kwork, &g)
+                             : kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g);
+        } else {
+            edep = kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g);
+        }
+        cmpmc_sim_stats& o = a.ev_stats[r.ev];
+        if (edep > 0.0) {
+            const double wedep = edep * static_cast<double>(r.w);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&o.sensor_hits), 1ull);
+            atomicAdd(&o.total_deposited_eV, wedep);
+            if (a.keep_hits) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(a.ev_nhits + r.ev), 1ull);
+                const unsigned long long idx = atomicAdd(a.hit_count, 1ull);
+                if (idx < a.hit_cap) {
+                    cmpmc_sensor_hit h;
+                    h.pos[0] = r.px; h.pos[1] = r.py; h.pos[2] = r.pz;
+                    h.time = r.t;
+                    h.edep = wedep;
+                    h.incident_energy = r.E;
+                    h.surface_id = r.surf;
+                    h.excitation = 0;
+                    h.mode = r.mode;
+                    h._pad = 0;
+                    h.channel_id = r.ch_id;
+                    a.hit_stage[idx] = h;
+                    a.hit_key[idx] = r.ev;
+                }
+            }
+        }
+        double sum_refl = 0.0;
+        for (int j = 0; j < n_refl; ++j) sum_refl += refl_buf[j];
+        const double esc = dmax(0.0, r.E - edep - sum_refl) * static_cast<double>(r.w);
+        if (esc != 0.0) atomicAdd(&o.escaped_or_killed_eV, esc);
+        if (n_refl == 0) continue;
+        const unsigned long long base = atomicAdd(a.reemit_tail, static_cast<unsigned long long>(n_refl));
+        if (base + n_refl > a.reemit_cap) {
+            err |= kErrQueue;
+            continue;
+        }
+        // inward normal of the face at the entry point (CylinderSolid, solids.hpp:46-93)
+        F3 n;
+        if (r.surf == 0) n = f3(0.0f, 0.0f, -1.0f);
+        else if (r.surf == 1) n = f3(0.0f, 0.0f, 1.0f);
+        else {
+            const float rr = sqrtf(r.px * r.px + r.py * r.py);
+            n = (rr > 1e-15f) ? f3(-r.px / rr, -r.py / rr, 0.0f) : f3(-1.0f, 0.0f, 0.0f);
+        }
+        const F3 re = f3(r.px, r.py, r.pz) + n * kNudge;
+        for (int j = 0; j < n_refl; ++j) {
+            const int mode = fdos(L, g.u());
+            FKin kin;
+            const F3 k = finward(L, mode, n, g, kin);
+            QPhonon q;
+            q.px = re.x; q.py = re.y; q.pz = re.z;
+            q.kx = k.x; q.ky = k.y; q.kz = k.z;
+            q.w = r.w;
+            q.mode = static_cast<uint32_t>(mode);
+            q.E = refl_buf[j];
+            q.t = r.t;
+            q.key = mix64(r.key ^ (0x9e3779b97f4a7c15ULL * static_cast<uint64_t>(j + 1)));
+            q.ev = r.ev;
+            q.pad = (j == 0) ? r.bounces : 0u;
+            a.reemit[base + j] = q;
+        }
+    }
+    if (err) atomicOr(a.err, err);
 }
 
 // Adjoint of the hit-time histogram: the batched transport with per-track scores. Bin
@@ -636,7 +753,10 @@ cudaError_t launch_unit_event(const uint64_t* ph_off, uint64_t n_events, uint32_
 cudaError_t launch_batched_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                                 const uint32_t* unit_event, int grid, int block, cudaStream_t s) {
     const FLat f = make_flat(L, cdf_f, D);
-    if (a.ev_sink) {
+    if (a.film) {
+        if (a.surrogate) k_batched_fp32<true, true, true><<<grid, block, 0, s>>>(f, D, a, unit_event);
+        else k_batched_fp32<true, false, true><<<grid, block, 0, s>>>(f, D, a, unit_event);
+    } else if (a.ev_sink) {
         if (a.surrogate) k_batched_fp32<true, true><<<grid, block, 0, s>>>(f, D, a, unit_event);
         else k_batched_fp32<true, false><<<grid, block, 0, s>>>(f, D, a, unit_event);
     } else {
@@ -652,10 +772,28 @@ cudaError_t batched_fp32_occupancy(int block, int* blocks_per_sm) {
 
 size_t batched_stack_entry_bytes() { return sizeof(GFTrack); }
 
+cudaError_t launch_film_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
+                             const FilmRec* film, uint64_t n_film, int grid, int block, cudaStream_t s) {
+    const FLat f = make_flat(L, cdf_f, D);
+    if (a.surrogate) k_film_fp32<true><<<grid, block, 0, s>>>(f, D, a, film, n_film);
+    else k_film_fp32<false><<<grid, block, 0, s>>>(f, D, a, film, n_film);
+    return cudaGetLastError();
+}
+
+cudaError_t film_fp32_occupancy(int block, int* blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_film_fp32<false>, block, 0);
+}
+
 cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                               const QPhonon* queue, int grid, int block, cudaStream_t s) {
-    if (a.surrogate) k_queue_fp32<true><<<grid, block, 0, s>>>(make_flat(L, cdf_f, D), D, a, queue);
-    else k_queue_fp32<false><<<grid, block, 0, s>>>(make_flat(L, cdf_f, D), D, a, queue);
+    const FLat f = make_flat(L, cdf_f, D);
+    if (a.film) {
+        if (a.surrogate) k_queue_fp32<true, true><<<grid, block, 0, s>>>(f, D, a, queue);
+        else k_queue_fp32<false, true><<<grid, block, 0, s>>>(f, D, a, queue);
+    } else {
+        if (a.surrogate) k_queue_fp32<true><<<grid, block, 0, s>>>(f, D, a, queue);
+        else k_queue_fp32<false><<<grid, block, 0, s>>>(f, D, a, queue);
+    }
     return cudaGetLastError();
 }
 

@@ -316,11 +316,17 @@ int cmpmc_recoil_mesh(const cmpmc_detector* det, cmpmc_mesh** out);
 typedef struct cmpmc_gpu_ctx cmpmc_gpu_ctx;
 
 enum {
-    CMPMC_FORM_PLAIN_FP64   = 0,   /* bit-exact event streams, one event per device thread   */
-    CMPMC_FORM_BATCHED_FP32 = 1    /* per-primary substreams, FP32 geometry, FP64 ledger/time;
-                                      with charges: per-carrier substreams, FP32 drift, Luke
-                                      phonons through a device queue (hits of an event in
-                                      no fixed order, FP64 event sums by atomics)           */
+    CMPMC_FORM_PLAIN_FP64          = 0,  /* bit-exact event streams, one event per device thread */
+    CMPMC_FORM_BATCHED_FP32        = 1,  /* own substreams per primary, FP32 geometry, FP64
+                                            ledger and time of flight; wavefront split: film
+                                            entries run in a film kernel and their re-emitted
+                                            phonons re-enter through a device queue (hits of an
+                                            event in no fixed order, FP64 event sums by
+                                            atomics); with charges: per-carrier substreams, FP32
+                                            drift, Luke phonons through the queue             */
+    CMPMC_FORM_BATCHED_FP32_INLINE = 2   /* the batched form with each primary's whole lineage on
+                                            one thread (film cascades inline): hits in a fixed
+                                            order, the forward of cmpmc_gpu_adjoint           */
 };
 
 typedef struct cmpmc_run_desc {

@@ -43,14 +43,15 @@ def _small(setup, n):
 
 def test_histogram_equals_binned_batched_run(setup):
     """At p_d = 1 the theta surfaces equal the default ones: the adjoint kernel's histogram
-    must equal the binned hits of the batched form on the same substreams."""
+    must equal the binned hits of the batched form (its inline variant, the adjoint's
+    forward) on the same substreams."""
     import cmpmc_b200 as cm
     eng, _, _, theta0 = setup
     adj, _ = _small(setup, 50_000)
     th = theta0.copy()
     th[2] = 1.0
     res = adj.run(th)
-    run = eng.run_packed(adj.packed, cm.RunOptions(seed=SEED, form="batched_fp32"))
+    run = eng.run_packed(adj.packed, cm.RunOptions(seed=SEED, form="batched_fp32_inline"))
     t = run.hits["time"]
     want = np.histogram(t[(t >= 0) & (t < 1e-3)], bins=64, range=(0.0, 1e-3))[0].astype(np.float64)
     assert res.stats.total_steps == run.stats.total_steps

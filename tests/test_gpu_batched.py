@@ -94,15 +94,57 @@ def test_batched_matches_plain_fp64_statistics(ge_lattice):
     assert abs(sb.total_steps / sp.total_steps - 1.0) < 0.02
 
 
+def _sorted_event_hits(res):
+    out = []
+    for i in range(len(res.hit_offsets) - 1):
+        lo, hi = int(res.hit_offsets[i]), int(res.hit_offsets[i + 1])
+        out.append(np.sort(res.hits[lo:hi], order=["time", "edep", "incident_energy"]).tobytes())
+    return out
+
+
 def test_batched_deterministic(ge_lattice):
+    """The wavefront-split form: every unit owns its substream, so the hits of each event (as
+    a set) and every integer counter are the same for any launch shape and queue size; the
+    inline form also keeps the hit order."""
+    import cmpmc_b200 as cm
     eng = _engine(ge_lattice, "c1")
-    a = _batched(eng, "c1", 100)
-    eng.configure(threads_per_block=64, blocks_per_sm=2)
-    b = _batched(eng, "c1", 100)
-    assert a.hits.tobytes() == b.hits.tobytes()
-    assert a.stats.record().tobytes() == b.stats.record().tobytes()
+    a = _batched(eng, "c1", 100, want_event_stats=True)
+    eng2 = _engine(ge_lattice, "c1")
+    eng2.configure(threads_per_block=64, blocks_per_sm=2, queue_capacity=4096)
+    b = _batched(eng2, "c1", 100, want_event_stats=True)
+    assert np.array_equal(a.hit_offsets, b.hit_offsets)
+    assert _sorted_event_hits(a) == _sorted_event_hits(b)
+    for name in a.event_stats.dtype.names:
+        if a.event_stats.dtype[name].kind == "u":
+            assert np.array_equal(a.event_stats[name], b.event_stats[name]), name
+        else:
+            np.testing.assert_allclose(a.event_stats[name], b.event_stats[name], rtol=1e-12, atol=1e-300)
     c = _batched(eng, "c1", 100, seed=12345)
-    assert a.hits.tobytes() != c.hits.tobytes()
+    assert _sorted_event_hits(a) != _sorted_event_hits(c)
+    packed = eng.generate(workload_of("c1"), 100, 7)
+    i1 = eng.run_packed(packed, cm.RunOptions(seed=7, form="batched_fp32_inline"))
+    i2 = eng2.run_packed(packed, cm.RunOptions(seed=7, form="batched_fp32_inline"))
+    assert i1.hits.tobytes() == i2.hits.tobytes()
+    assert i1.stats.record().tobytes() == i2.stats.record().tobytes()
+
+
+def test_batched_inline_and_split_forms_agree(ge_lattice):
+    """The two batched forms sample the same physics with different substream layouts:
+    hit histograms chi^2 p > 0.01, both ledgers close."""
+    import cmpmc_b200 as cm
+    eng = _engine(ge_lattice, "c1")
+    packed = eng.generate(workload_of("c1"), 2000, 7)
+    s = eng.run_packed(packed, cm.RunOptions(seed=7, form="batched_fp32"))
+    i = eng.run_packed(packed, cm.RunOptions(seed=7, form="batched_fp32_inline"))
+    lo = min(s.hits["edep"].min(), i.hits["edep"].min())
+    hi = max(s.hits["edep"].max(), i.hits["edep"].max()) * (1 + 1e-9)
+    hs, hi_ = event_histograms(s.hit_offsets, s.hits, (lo, hi)), event_histograms(i.hit_offsets, i.hits, (lo, hi))
+    for name in ("time", "radius", "edep"):
+        c2, dof, p = hist_chi2(hs, hi_, name)
+        print(f"split vs inline {name}: chi2 {c2:.1f} dof {dof} p {p:.3f}")
+        assert p > P_MIN, (name, c2, dof, p)
+    for st in (s.stats, i.stats):
+        assert abs(st.total_injected_eV - st.total_deposited_eV - st.escaped_or_killed_eV) / st.total_injected_eV <= LEDGER_TOL
 
 
 def test_batched_electrode_mask_channels(ge_lattice):
