@@ -5,7 +5,9 @@ tracks per GPU, energies log-uniform on [1, 30] meV, modes L/ST/FT 0.10/0.36/0.5
 uniform in the Ge cylinder (R 3.81 cm, half height 1.27 cm), isotropic directions, seed 7;
 default Ge lattice and detector (Al Kaplan films on both faces). One step = one run_events
 pass over the whole batch in the batched FP32 form (FP32 geometry, FP64 energy ledger and
-time of flight), hits kept.
+time of flight; wavefront split: transport phases and film-cascade phases alternate until
+every track is absorbed or lost), hits kept. The launch shape comes from the library's
+autotuner (results do not depend on it).
 
   value  primary phonon tracks / s, inputs resident on the device, device-timed (CUDA
          events on the library's stream), max over ranks
@@ -186,6 +188,9 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-configuration autotuner")
     ap.add_argument("--no-graph", action="store_true", help="eager launches instead of CUDA-graph replay")
+    ap.add_argument("--form", default="batched_fp32", choices=["batched_fp32", "batched_fp32_inline"])
+    ap.add_argument("--queue-capacity", type=int, default=0, help="phonon queue entries (0: library default)")
+    ap.add_argument("--stack-capacity", type=int, default=0, help="tracks per device thread (0: library default)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -215,6 +220,9 @@ def main() -> None:
     n_prim = int(packed.phonon_offsets[-1])
     lib = _ffi.load()
     h = eng.context(dev)
+    if args.queue_capacity or args.stack_capacity:
+        eng.configure(dev, stack_capacity=args.stack_capacity, queue_capacity=args.queue_capacity)
+    form_id = _ffi.FORM_BATCHED_FP32 if args.form == "batched_fp32" else _ffi.FORM_BATCHED_FP32_INLINE
 
     # device-resident inputs (torch owns the memory)
     def to_dev(a):
@@ -229,7 +237,7 @@ def main() -> None:
         d.n_events = args.events
         d.first_event = first
         d.keep_hits = 1
-        d.form = _ffi.FORM_BATCHED_FP32
+        d.form = form_id
         d.seed = SEED
         if on_device:
             d.rng_state, d.injected_eV = d_rng.data_ptr(), d_inj.data_ptr()
@@ -274,6 +282,7 @@ def main() -> None:
             lib.cmpmc_gpu_last_error(h, buf, 512)
             raise RuntimeError(buf.value.decode())
         tune = {"threads_per_block": tr.threads_per_block, "blocks_per_sm": tr.blocks_per_sm,
+                "phase_steps": tr.phase_steps,
                 "best_kernel_ms": tr.best_ms, "default_kernel_ms": tr.first_ms,
                 "tried": [[tr.tried_tpb[i], tr.tried_bps[i], round(tr.tried_ms[i], 2)] for i in range(tr.n_tried)]}
     if not args.no_graph:
@@ -341,7 +350,7 @@ def main() -> None:
         "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": "mixed_energy_phonons", "events": args.events * world, "primaries_per_event": PER_EVENT,
-                   "primaries": n_prim * world, "form": "batched_fp32", "seed": SEED,
+                   "primaries": n_prim * world, "form": args.form, "seed": SEED,
                    "energy": "log-uniform 1-30 meV", "modes": "L/ST/FT 0.10/0.36/0.54",
                    "l2": "256 MiB buffer written between timed steps (L2 126 MB); inputs 128 MB, hits ~1.5 GB per step"},
         "kernel_ms_per_step": kernel_ms,

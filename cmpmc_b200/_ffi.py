@@ -156,7 +156,8 @@ TUNE_MAX = 16
 
 class TuneResultC(C.Structure):
     _fields_ = [
-        ("threads_per_block", _i32), ("blocks_per_sm", _i32), ("queue_capacity", _u64), ("best_ms", _f64),
+        ("threads_per_block", _i32), ("blocks_per_sm", _i32), ("queue_capacity", _u64), ("phase_steps", _u32),
+        ("_pad1", _u32), ("best_ms", _f64),
         ("first_ms", _f64), ("n_tried", _i32), ("_pad0", _i32), ("tried_tpb", _i32 * TUNE_MAX),
         ("tried_bps", _i32 * TUNE_MAX), ("tried_queue", _u64 * TUNE_MAX), ("tried_ms", _f64 * TUNE_MAX),
     ]
@@ -205,6 +206,7 @@ _SIG = {
     "cmpmc_gpu_set_mesh": (_i32, [C.c_void_p, C.c_void_p]),
     "cmpmc_gpu_configure_queue": (_i32, [C.c_void_p, _u64]),
     "cmpmc_gpu_configure_graph": (_i32, [C.c_void_p, _i32]),
+    "cmpmc_gpu_configure_phases": (_i32, [C.c_void_p, _u32]),
     "cmpmc_gpu_memcpy": (_i32, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "cmpmc_gpu_autotune": (_i32, [C.c_void_p, C.POINTER(RunDescC), _i32, C.POINTER(TuneResultC)]),
     "cmpmc_kaplan_surrogate_create": (_i32, [C.POINTER(FilmConfigC), _u64, C.POINTER(C.c_void_p)]),

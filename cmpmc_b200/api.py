@@ -830,7 +830,8 @@ class SimulationEngine:
         tried = [{"threads_per_block": r.tried_tpb[i], "blocks_per_sm": r.tried_bps[i],
                   "queue_capacity": r.tried_queue[i], "kernel_ms": r.tried_ms[i]} for i in range(r.n_tried)]
         return {"threads_per_block": r.threads_per_block, "blocks_per_sm": r.blocks_per_sm,
-                "queue_capacity": r.queue_capacity, "best_ms": r.best_ms, "first_ms": r.first_ms, "tried": tried}
+                "queue_capacity": r.queue_capacity, "phase_steps": r.phase_steps, "best_ms": r.best_ms,
+                "first_ms": r.first_ms, "tried": tried}
 
     def make_track(self, pos, k_dir, mode, energy_eV, time_s=0.0, weight=1.0) -> np.ndarray:
         out = np.zeros((), dtype=_ffi.PHONON_DTYPE)

@@ -101,8 +101,9 @@ struct cmpmc_gpu_ctx {
     DevBuf lut[3];                                      // Kaplan surrogate tables of the films
     bool lut_ready = false;
     DevBuf queue, resume_a, resume_b, ccounters, carrier_event, cursor;  // batched charge form
-    DevBuf film_a, film_b;                              // film-entry queues of the wavefront split
+    DevBuf film_a, queue_b;                             // wavefront split: film entries, second phonon queue
     uint64_t film_cap = 1ull << 22;                     // film entries per phase (64 B each)
+    uint32_t phase_steps = 0;                           // steps a track takes per transport phase (0: any)
     uint64_t queue_cap = 1ull << 24;                    // Luke-phonon queue entries (64 B each)
     // CUDA-graph replay of the batched phonon call (cmpmc_gpu_configure_graph)
     bool graph_enabled = false;
@@ -409,8 +410,8 @@ int run_split_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, u
         ctx->film_cap = std::max<uint64_t>(ctx->film_cap, std::min<uint64_t>(8 * n_ph, 1ull << 26));
         const uint64_t q_cap = std::max<uint64_t>(ctx->queue_cap, 64), f_cap = std::max<uint64_t>(ctx->film_cap, 64);
         CK(ctx->queue.ensure(q_cap * sizeof(QPhonon)), "alloc phonon queue");
+        CK(ctx->queue_b.ensure(q_cap * sizeof(QPhonon)), "alloc phonon queue");
         CK(ctx->film_a.ensure(f_cap * sizeof(FilmRec)), "alloc film queue");
-        CK(ctx->film_b.ensure(f_cap * sizeof(FilmRec)), "alloc film queue");
         CK(ctx->stack.ensure(slots * stack_cap * batched_stack_entry_bytes()), "alloc phonon stacks");
         CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
         CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
@@ -419,18 +420,21 @@ int run_split_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, u
         a.hit_stage = ctx->hit_stage.as<cmpmc_sensor_hit>();
         a.hit_key = ctx->hit_key.as<uint64_t>();
         a.hit_cap = hit_cap;
-        a.reemit = ctx->queue.as<QPhonon>();
         a.reemit_cap = q_cap;
         a.film_cap = f_cap;
-        FilmRec* f_in = ctx->film_a.as<FilmRec>();
-        FilmRec* f_out = ctx->film_b.as<FilmRec>();
+        a.film = ctx->film_a.as<FilmRec>();
+        a.phase_steps = ctx->phase_steps;
+        // the transport phase reads q_in and parks long tracks in q_out; the film phase
+        // appends its re-emissions to q_out; then the queues swap
+        QPhonon* q_in = ctx->queue.as<QPhonon>();
+        QPhonon* q_out = ctx->queue_b.as<QPhonon>();
         CK(cudaMemsetAsync(ctx->ev_stats2.p, 0, std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats), s), "memset");
         CK(cudaMemsetAsync(ctx->ev_nhits.p, 0, std::max<uint64_t>(n, 1) * 8, s), "memset");
         CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s), "memset counters");
         CK(cudaMemsetAsync(ctx->ccounters.p, 0, sizeof(ChargeCounters), s), "memset counters");
         CK(cudaEventRecord(ctx->e_k0, s), "event");
-        // phase 0: the generator's phonons, film entries into f_in
-        a.film = f_in;
+        // phase 0: the generator's phonons
+        a.reemit = q_out;
         if (n_ph) {
             a.n_events = n_ph;
             CK(launch_batched_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->unit_event.as<uint32_t>(),
@@ -444,18 +448,21 @@ int run_split_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, u
                "copy counters");
             CK(cudaStreamSynchronize(s), "transport phase");
             const ChargeCounters h1 = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
-            if (h1.resume_next > f_cap) overflow = true;
-            const uint64_t n_f = std::min<uint64_t>(h1.resume_next, f_cap);
-            if (n_f == 0 || overflow) break;
-            // film phase: cascades of f_in, re-emissions into the phonon queue
-            CK(cudaMemsetAsync(&pc->q_tail, 0, sizeof(unsigned long long), s), "memset counters");
-            CK(launch_film_fp32(ctx->L, ctx->cdf_f, ctx->D, a, f_in, n_f,
-                                static_cast<int>(std::min<uint64_t>(grid_f, (n_f + tpb - 1) / tpb)), tpb, s),
-               "film launch");
-            ++launches;
-            CK(cudaMemcpyAsync(hbuf + sizeof(Counters), pc, sizeof(ChargeCounters), cudaMemcpyDeviceToHost, s),
-               "copy counters");
-            CK(cudaStreamSynchronize(s), "film phase");
+            if (h1.resume_next > f_cap || h1.q_tail > q_cap) {
+                overflow = true;
+                break;
+            }
+            const uint64_t n_f = h1.resume_next;
+            if (n_f > 0) {
+                // film phase: cascades of the queued film entries, re-emissions appended to q_out
+                CK(launch_film_fp32(ctx->L, ctx->cdf_f, ctx->D, a, a.film, n_f,
+                                    static_cast<int>(std::min<uint64_t>(grid_f, (n_f + tpb - 1) / tpb)), tpb, s),
+                   "film launch");
+                ++launches;
+                CK(cudaMemcpyAsync(hbuf + sizeof(Counters), pc, sizeof(ChargeCounters), cudaMemcpyDeviceToHost, s),
+                   "copy counters");
+                CK(cudaStreamSynchronize(s), "film phase");
+            }
             const ChargeCounters h2 = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
             if (h2.q_tail > q_cap) {
                 overflow = true;
@@ -463,13 +470,13 @@ int run_split_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, u
             }
             const uint64_t n_q = h2.q_tail;
             if (n_q == 0) break;
-            // transport phase over the re-emitted phonons, film entries into the other buffer
-            std::swap(f_in, f_out);
-            a.film = f_in;
-            CK(cudaMemsetAsync(&pc->resume_next, 0, sizeof(unsigned long long), s), "memset counters");
+            // transport phase over q_out (parked tracks and re-emissions)
+            std::swap(q_in, q_out);
+            a.reemit = q_out;
+            CK(cudaMemsetAsync(&pc->q_tail, 0, 2 * sizeof(unsigned long long), s), "memset counters");
             CK(cudaMemsetAsync(&dc->next_work, 0, sizeof(unsigned long long), s), "memset work counter");
             a.n_events = n_q;
-            CK(launch_queue_fp32(ctx->L, ctx->cdf_f, ctx->D, a, a.reemit,
+            CK(launch_queue_fp32(ctx->L, ctx->cdf_f, ctx->D, a, q_in,
                                  static_cast<int>(std::min<uint64_t>(grid_ph, (n_q + tpb - 1) / tpb)), tpb, s),
                "queue launch");
             ++launches;
@@ -611,7 +618,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->film_a, &ctx->film_b, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
+    for (DevBuf* b : {&ctx->film_a, &ctx->queue_b, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
                       &ctx->ccounters, &ctx->carrier_event, &ctx->cursor, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
@@ -738,6 +745,7 @@ int cmpmc_gpu_autotune(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* sample, int rep
         }
         if (st != CMPMC_OK) break;
     }
+    const uint32_t best_ps = ctx->phase_steps;  // not tuned: it changes the substream layout
     // queue depth of the charge phases, with the best block shape
     if (st == CMPMC_OK && charges) {
         ctx->tpb = best_tpb;
@@ -762,7 +770,14 @@ int cmpmc_gpu_autotune(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* sample, int rep
     out->threads_per_block = best_tpb;
     out->blocks_per_sm = best_bps;
     out->queue_capacity = best_q;
+    out->phase_steps = best_ps;
     out->best_ms = best_ms;
+    return CMPMC_OK;
+}
+
+int cmpmc_gpu_configure_phases(cmpmc_gpu_ctx* ctx, uint32_t phase_steps) {
+    if (!ctx) return CMPMC_ERR_INVALID;
+    ctx->phase_steps = phase_steps;
     return CMPMC_OK;
 }
 

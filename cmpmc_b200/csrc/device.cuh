@@ -74,6 +74,9 @@ struct RunArgs {
     struct QPhonon* reemit;
     uint64_t reemit_cap;
     unsigned long long* reemit_tail;
+    // wavefront split: a track that has taken this many steps in the current phase is parked
+    // in `reemit` (next phase) on a substream derived from its own (0: no limit)
+    uint32_t phase_steps;
 };
 
 // Phonon queue entry of the batched forms (64 B): Luke phonons of the charge form and

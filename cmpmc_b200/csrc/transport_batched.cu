@@ -297,9 +297,11 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
     uint32_t n_hits = 0;
     uint64_t unit = ~0ull;
     uint32_t ev_cur = 0;  // event of the unit in flight
+    uint32_t n_phase = 0;  // steps of the track in flight in this phase (wavefront split)
     bool live = false;  // trk holds a track in flight
     for (;;) {
         if (!live) {
+            n_phase = 0;
             if (n_stk > 0) {
                 pop_track<kAdj>(stk, n_stk, trk);
                 live = true;
@@ -372,6 +374,30 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 trk.w /= static_cast<float>(D.rr_survival);
             } else {
                 st.killed++;
+                live = false;
+                continue;
+            }
+        }
+        if constexpr (kSplit) {
+            if (a.phase_steps && ++n_phase > a.phase_steps) {
+                // park the track for the next phase on a substream derived from its own
+                const unsigned long long slot = atomicAdd(a.reemit_tail, 1ull);
+                if (slot < a.reemit_cap) {
+                    QPhonon q;
+                    q.px = trk.pos.x; q.py = trk.pos.y; q.pz = trk.pos.z;
+                    q.kx = trk.k.x; q.ky = trk.k.y; q.kz = trk.k.z;
+                    q.w = trk.w;
+                    q.mode = static_cast<uint32_t>(trk.mode);
+                    q.E = trk.E;
+                    q.t = trk.t;
+                    const uint64_t hi = g.next();
+                    q.key = (hi << 32) | g.next();
+                    q.ev = ev_cur;
+                    q.pad = trk.bounces;
+                    a.reemit[slot] = q;
+                } else {
+                    err |= kErrQueue;
+                }
                 live = false;
                 continue;
             }

@@ -391,6 +391,13 @@ int cmpmc_gpu_configure_queue(cmpmc_gpu_ctx* ctx, uint64_t queue_capacity);
  * the eager call, which grows them and recaptures. */
 int cmpmc_gpu_configure_graph(cmpmc_gpu_ctx* ctx, int enable);
 
+/* Wavefront split of the batched form (no counterpart in the reference): a track that has
+ * taken `phase_steps` steps in one transport phase is parked for the next phase, on a
+ * substream drawn from its own, so long tracks do not hold a phase open (default 0: no
+ * limit). A limit changes which substream a long track continues on: the results are then
+ * statistically, not bitwise, those of the unlimited run; the autotuner leaves it alone. */
+int cmpmc_gpu_configure_phases(cmpmc_gpu_ctx* ctx, uint32_t phase_steps);
+
 /* Autotuner of the launch configuration (no counterpart in the reference): runs `sample`
  * (a representative call, outputs discarded) `repeats` times for each candidate, keeps the
  * fastest transport-kernel time and applies it to the context. Candidates: the current
@@ -401,6 +408,8 @@ int cmpmc_gpu_configure_graph(cmpmc_gpu_ctx* ctx, int enable);
 typedef struct cmpmc_tune_result {
     int32_t threads_per_block, blocks_per_sm;   /* chosen */
     uint64_t queue_capacity;                    /* chosen (charge runs) */
+    uint32_t phase_steps;                       /* in place (not tuned) */
+    uint32_t _pad1;
     double best_ms;                             /* its transport-kernel time */
     double first_ms;                            /* the configuration in place before tuning */
     int32_t n_tried, _pad0;
