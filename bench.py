@@ -61,10 +61,11 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per transport step of the batched kernel from the committed ncu summary."""
+def profile_traffic(split: bool = True):
+    """DRAM bytes per transport step of the batched kernels from the committed ncu summary."""
+    name = "batched_fp32_split_mixed_energy.json" if split else "batched_fp32_inline_mixed_energy.json"
     try:
-        with open(os.path.join(ROOT, "profiles", "batched_fp32_mixed_energy.json")) as f:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
             return float(json.load(f)["dram_bytes_per_step"])
     except Exception:
         return None
@@ -344,7 +345,7 @@ def main() -> None:
     peak, peak_kind = measured_peaks()
     steps_per_launch = steps_total / args.steps
     achieved = steps_per_launch * BYTES_PER_STEP / (sum(kms) / args.steps * 1e-3) / 1e9
-    tps = profile_traffic()
+    tps = profile_traffic(args.form == "batched_fp32")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
