@@ -5,14 +5,16 @@ CrystalLattice, DetectorModel, ...); the work runs in hand-written CUDA kernels 
 the C ABI in include/cmpmc_gpu.h.
 """
 from .api import (AluminumFilm, CmpmcError, ElectrodePad, ElectrodePatternMask, CrystalConfig, CrystalLattice, CylinderSolid, DetectorModel,
-                  EventInput, ExcitationType, KaplanFilm, KaplanSurrogateLUT, PackedEvents, PhononMode, Rng, RunOptions, RunResult,
+                  EventInput, ExcitationType, IsotropicAMMInterface, IsotropicMedium, KaplanFilm,
+                  KaplanSurrogateLUT, PackedEvents, PhononMode, Rng, RunOptions, RunResult,
                   SimStats, SimulationEngine, SuperconductorFilmConfig, SurfaceId, SurfaceProperty,
                   TriLinearMesh3D, UniformElectricField, UnvalidatedModuleError, Workload, materials, run_events, units, workloads)
 from .adjoint import AdjointResult, HistogramAdjoint, THETA_NAMES, default_theta
 
 __all__ = [
     "AdjointResult", "AluminumFilm", "CmpmcError", "ElectrodePad", "ElectrodePatternMask", "CrystalConfig", "CrystalLattice", "CylinderSolid", "DetectorModel", "EventInput",
-    "ExcitationType", "KaplanFilm", "KaplanSurrogateLUT", "PackedEvents", "PhononMode", "Rng", "RunOptions", "RunResult", "SimStats",
+    "ExcitationType", "IsotropicAMMInterface", "IsotropicMedium", "KaplanFilm",
+    "KaplanSurrogateLUT", "PackedEvents", "PhononMode", "Rng", "RunOptions", "RunResult", "SimStats",
     "SimulationEngine", "SuperconductorFilmConfig", "SurfaceId", "SurfaceProperty", "TriLinearMesh3D",
     "UniformElectricField",
     "UnvalidatedModuleError", "Workload", "materials", "run_events", "units", "workloads", "HistogramAdjoint",

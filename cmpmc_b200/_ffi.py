@@ -97,6 +97,7 @@ class SurfaceC(C.Structure):
         ("spec_prob_const", _f64), ("n_spec", _i32), ("n_diff", _i32), ("n_anh", _i32), ("demo_values", _i32),
         ("spec_coeffs", _f64 * MAX_POLY), ("diff_coeffs", _f64 * MAX_POLY), ("anh_coeffs", _f64 * MAX_POLY),
         ("has_film", _i32), ("has_amm", _i32), ("has_mask", _i32), ("_pad0", _i32), ("film", FilmConfigC),
+        ("amm_substrate", _f64 * 3), ("amm_film", _f64 * 3),
     ]
 
 
@@ -214,6 +215,7 @@ _SIG = {
     "cmpmc_kaplan_surrogate_info": (_i32, [C.c_void_p, C.POINTER(_u64), C.POINTER(_u64)]),
     "cmpmc_kaplan_surrogate_absorb": (_i32, [C.c_void_p, _f64, C.POINTER(_u64), C.c_void_p, _u64, C.POINTER(_u64),
                                              C.POINTER(_f64)]),
+    "cmpmc_amm_transmission": (_f64, [C.POINTER(_f64), C.POINTER(_f64), _i32, _f64]),
     "cmpmc_gpu_set_electrode_mask": (_i32, [C.c_void_p, _i32, C.c_void_p, _u64]),
     "cmpmc_mask_supercdms_qet": (_i32, [_f64, _f64, C.c_void_p]),
     "cmpmc_mask_rectangular_grid": (_i32, [_i32, _i32, _f64, _f64, _f64, _f64, _f64, C.c_void_p, _u64,

@@ -309,6 +309,36 @@ def AluminumFilm() -> SuperconductorFilmConfig:
     return SuperconductorFilmConfig()
 
 
+@dataclass
+class IsotropicMedium:
+    """IsotropicMedium (phonon/interface_transmission.hpp:36-49)."""
+    rho: float = 0.0
+    vL: float = 0.0
+    vT: float = 0.0
+
+    @staticmethod
+    def from_lame(rho: float, lam_Pa: float, mu_Pa: float) -> "IsotropicMedium":
+        return IsotropicMedium(rho, math.sqrt((lam_Pa + 2.0 * mu_Pa) / rho), math.sqrt(mu_Pa / rho))
+
+    @staticmethod
+    def from_bulk_shear(rho: float, K_Pa: float, G_Pa: float) -> "IsotropicMedium":
+        return IsotropicMedium(rho, math.sqrt((K_Pa + 4.0 * G_Pa / 3.0) / rho), math.sqrt(G_Pa / rho))
+
+
+@dataclass
+class IsotropicAMMInterface:
+    """IsotropicAMMInterface (phonon/interface_transmission.hpp:123-140): acoustic-mismatch
+    transmission substrate -> film; on a SurfaceProperty it replaces the film's
+    film_absorption as the film-entry probability."""
+    substrate: IsotropicMedium = field(default_factory=IsotropicMedium)
+    film: IsotropicMedium = field(default_factory=IsotropicMedium)
+
+    def transmission(self, longitudinal: bool, cos_theta: float) -> float:
+        sub = (C.c_double * 3)(self.substrate.rho, self.substrate.vL, self.substrate.vT)
+        fil = (C.c_double * 3)(self.film.rho, self.film.vL, self.film.vT)
+        return _ffi.load().cmpmc_amm_transmission(sub, fil, int(bool(longitudinal)), float(cos_theta))
+
+
 class KaplanSurrogateLUT:
     """KaplanSurrogateLUT (superconductor/kaplan_film.hpp:336-383), built natively on the
     host; the batched form uses the same table on the device (RunOptions.kaplan_surrogate)."""
@@ -429,6 +459,7 @@ class SurfaceProperty:
     spec_prob_const: float = 0.0
     demo_values: bool = False
     electrode_mask: Optional[ElectrodePatternMask] = None
+    amm_interface: Optional[IsotropicAMMInterface] = None
 
     @staticmethod
     def diffuse_bare_surface() -> "SurfaceProperty":
@@ -471,6 +502,13 @@ class SurfaceProperty:
             for i, x in enumerate(v):
                 arr[i] = float(x)
         s.demo_values = int(self.demo_values)
+        if self.amm_interface is not None:
+            s.has_amm = 1
+            m1, m2 = self.amm_interface.substrate, self.amm_interface.film
+            for i, v in enumerate((m1.rho, m1.vL, m1.vT)):
+                s.amm_substrate[i] = float(v)
+            for i, v in enumerate((m2.rho, m2.vL, m2.vT)):
+                s.amm_film[i] = float(v)
         if self.kaplan_sensor is not None:
             s.has_film = 1
             s.film = self.kaplan_sensor.to_c()

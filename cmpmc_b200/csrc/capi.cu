@@ -916,6 +916,9 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     uint64_t n_hits = 0;
     uint64_t* ev_offsets = nullptr;
     cmpmc_sim_stats* ev_stats = nullptr;
+    if (batched && n_ch > 0 && ctx->det.charge_release != 0)
+        return fail(ctx, CMPMC_ERR_INVALID,
+                    "BulkDebye / ElectrodeFilm charge release runs in the plain FP64 form (batched: RecordOnly)");
     if (batched && n_ch > 0) {
         // carriers and their Luke phonons: alternating charge / queue phases, event sinks
         const int st = run_charges_batched(ctx, d, a, n, n_ph, n_ch, launches, hc, kms, n_hits, ev_offsets, ev_stats);
@@ -1152,6 +1155,9 @@ int cmpmc_gpu_adjoint(cmpmc_gpu_ctx* ctx, const cmpmc_adjoint_desc* d, cmpmc_adj
     std::string err;
     const int vst = validate_config(ctx->cfg, ctx->det, false, err);
     if (vst != CMPMC_OK) return fail(ctx, vst, err);
+    for (int i = 0; i < 3; ++i)
+        if (ctx->det.surfaces[i].has_amm)
+            return fail(ctx, CMPMC_ERR_INVALID, "the adjoint's film parameter is film_absorption: no AMM interfaces");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     cudaStream_t s = ctx->stream;
     int launches = 0;

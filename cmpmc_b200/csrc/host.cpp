@@ -122,6 +122,9 @@ Detector detector_view(const cmpmc_detector& d) {
         o.n_diff = s.n_diff;
         o.n_anh = s.n_anh;
         o.has_film = s.has_film;
+        o.has_amm = s.has_amm;
+        o.amm_sub = Medium{s.amm_substrate[0], s.amm_substrate[1], s.amm_substrate[2]};
+        o.amm_film = Medium{s.amm_film[0], s.amm_film[1], s.amm_film[2]};
         for (int k = 0; k < CMPMC_MAX_POLY; ++k) {
             o.spec[k] = s.spec_coeffs[k];
             o.diff[k] = s.diff_coeffs[k];
@@ -139,6 +142,8 @@ Detector detector_view(const cmpmc_detector& d) {
     D.charge_sampling_dk_frac = d.charge_sampling_dk_frac;
     D.charge_stepping = d.charge_stepping;
     D.fermi_level_above_Ev_eV = d.fermi_level_above_Ev_eV;
+    D.charge_release = d.charge_release;
+    D.electrode_seed_max_gap = d.electrode_seed_max_gap;
     return D;
 }
 
@@ -172,8 +177,13 @@ int validate_config(const cmpmc_crystal_config& cfg, const cmpmc_detector& det, 
     }
     for (int i = 0; i < 3; ++i) {
         const cmpmc_surface& s = det.surfaces[i];
-        if (s.has_amm || s.has_mask) {
-            err = "interface-transmission models and electrode masks are not available on the device";
+        if (s.has_mask) {
+            err = "electrode masks are attached with cmpmc_gpu_set_electrode_mask (has_mask must be 0)";
+            return CMPMC_ERR_INVALID;
+        }
+        if (s.has_amm && !(s.amm_substrate[0] > 0.0 && s.amm_substrate[1] > 0.0 && s.amm_substrate[2] > 0.0 &&
+                           s.amm_film[0] > 0.0 && s.amm_film[1] > 0.0 && s.amm_film[2] > 0.0)) {
+            err = "AMM interface: densities and sound speeds must be positive";
             return CMPMC_ERR_INVALID;
         }
         if (s.n_spec < 0 || s.n_spec > CMPMC_MAX_POLY || s.n_diff < 0 || s.n_diff > CMPMC_MAX_POLY ||
@@ -182,8 +192,8 @@ int validate_config(const cmpmc_crystal_config& cfg, const cmpmc_detector& det, 
             return CMPMC_ERR_INVALID;
         }
     }
-    if (det.charge_release != 0) {
-        err = "only ChargeRelease::RecordOnly is available on the device";
+    if (det.charge_release < 0 || det.charge_release > 2) {
+        err = "charge_release must be RecordOnly, BulkDebye or ElectrodeFilm";
         return CMPMC_ERR_INVALID;
     }
     if (det.kinematics_mode != 0) {
@@ -485,6 +495,12 @@ void gen_event(int wl, const Lattice& L, const cmpmc_crystal_config& cfg, const 
 extern "C" {
 
 double cmpmc_cr_log(double x) { return crmath::log(x); }
+
+double cmpmc_amm_transmission(const double sub[3], const double film[3], int longitudinal, double cos_theta) {
+    if (!sub || !film) return 0.0;
+    return amm_transmission(Medium{sub[0], sub[1], sub[2]}, Medium{film[0], film[1], film[2]}, longitudinal != 0,
+                            cos_theta);
+}
 double cmpmc_cr_sin(double x) { return crmath::sin(x); }
 double cmpmc_cr_cos(double x) { return crmath::cos(x); }
 

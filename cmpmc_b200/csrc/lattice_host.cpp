@@ -349,6 +349,7 @@ void build_tables(cmpmc_lattice& lat) {
     L.v_sound = c.v_sound;
     L.v_trans = c.v_trans;
     L.bandgap = c.bandgap;
+    L.debye_energy = c.debye_freq * kHPlanck;
     L.iv_model = c.iv_model;
     L.iv_min_energy = c.iv_min_energy;
     L.iv_quad_rate = c.iv_quad_rate;

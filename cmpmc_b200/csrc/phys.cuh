@@ -188,6 +188,7 @@ struct Lattice {
     double fLDOS, fSTDOS, fFTDOS;
     double v_sound, v_trans;
     double bandgap;
+    double debye_energy;  // CrystalLattice::debye_energy (crystal_lattice.hpp:62)
     // Herring-Vogt (crystal_lattice.hpp:322-331, built 394-438)
     double e_cond_mass, h_mass;
     V3 mass_ratio, hv_sqrt, hv_sqrt_inv;
@@ -398,6 +399,11 @@ CMPMC_HD bool pad_contains(const Pad& p, double x, double y) {
     return false;
 }
 
+// IsotropicMedium (phonon/interface_transmission.hpp:36-49)
+struct Medium {
+    double rho, vL, vT;
+};
+
 struct Surface {
     double prob_abs, prob_refl, refl_cutoff, anh_cutoff;
     double prob_charge_abs, prob_charge_spec, min_k_elec, min_k_hole;
@@ -409,12 +415,120 @@ struct Surface {
     // SurfaceProperty::electrode_mask (surface_property.hpp:45): n_pads > 0 when present
     const Pad* pads;
     int n_pads;
+    // IsotropicAMMInterface (surface_property.hpp:44): substrate -> film transmission
+    // replaces the film's film_absorption (engine.hpp:492-495)
+    int has_amm;
+    Medium amm_sub, amm_film;
     // KaplanSurrogateLUT tables of the film (batched form, when requested): absorbed
     // fractions [128 * 512], offsets into the re-emitted fractions [128 * 512 + 1]
     const float* lut_abs;
     const uint32_t* lut_off;
     const float* lut_refl;
 };
+
+// ---- acoustic mismatch transmission (phonon/interface_transmission.hpp:51-140) ----------
+// Complex numbers for the P-SV boundary solve. Division by Smith's method and the principal
+// square root; a last-ulp difference to the host's complex library only moves the
+// transmission by ~1e-16, which decides a film entry only if the uniform draw lands within
+// that distance of it.
+struct Cx {
+    double re, im;
+};
+CMPMC_HD Cx cx(double re, double im = 0.0) { return Cx{re, im}; }
+CMPMC_HD Cx operator+(Cx a, Cx b) { return cx(a.re + b.re, a.im + b.im); }
+CMPMC_HD Cx operator-(Cx a, Cx b) { return cx(a.re - b.re, a.im - b.im); }
+CMPMC_HD Cx operator*(Cx a, Cx b) { return cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+CMPMC_HD Cx operator*(double s, Cx a) { return cx(s * a.re, s * a.im); }
+CMPMC_HD Cx cneg(Cx a) { return cx(-a.re, -a.im); }
+CMPMC_HD Cx cdiv(Cx a, Cx b) {
+    if (fabs(b.re) >= fabs(b.im)) {
+        const double r = b.im / b.re, den = b.re + b.im * r;
+        return cx((a.re + a.im * r) / den, (a.im - a.re * r) / den);
+    }
+    const double r = b.re / b.im, den = b.re * r + b.im;
+    return cx((a.re * r + a.im) / den, (a.im * r - a.re) / den);
+}
+CMPMC_HD double cabs_(Cx a) { return m_hypot(a.re, a.im); }
+CMPMC_HD double cnorm(Cx a) { return a.re * a.re + a.im * a.im; }
+// sqrt of a real number on the principal branch (the slownesses of amm_psv: Im >= 0)
+CMPMC_HD Cx csqrt_real(double x) { return (x >= 0.0) ? cx(sqrt(x), 0.0) : cx(0.0, sqrt(-x)); }
+
+CMPMC_HD double amm_sh(const Medium& m1, const Medium& m2, double theta1) {
+    const double s2 = m2.vT / m1.vT * m_sin(theta1);
+    if (s2 >= 1.0) return 0.0;
+    const double c1 = m_cos(theta1), c2 = sqrt(1.0 - s2 * s2);
+    const double a = m1.rho * m1.vT * c1, b = m2.rho * m2.vT * c2;
+    return (a + b > 0.0) ? 4.0 * a * b / ((a + b) * (a + b)) : 0.0;
+}
+
+struct AmmWave {
+    Cx dx, dz, txz, tzz;
+};
+CMPMC_HD AmmWave amm_wave(const Medium& m, bool P, Cx s, double p) {
+    const double v = P ? m.vL : m.vT;
+    const Cx dx = P ? cx(v * p) : v * s;
+    const Cx dz = P ? v * s : cx(-v * p);
+    const double mu = m.rho * m.vT * m.vT, la = m.rho * (m.vL * m.vL - 2.0 * m.vT * m.vT);
+    AmmWave w;
+    w.dx = dx;
+    w.dz = dz;
+    w.txz = mu * (s * dx + p * dz);
+    w.tzz = la * (p * dx + s * dz) + ((2.0 * mu) * s) * dz;
+    return w;
+}
+
+// transmitted energy flux T_P + T_S of a P or SV wave (amm_psv, interface_transmission.hpp:74-117)
+CMPMC_HD double amm_psv_transmitted(const Medium& m1, const Medium& m2, bool incident_P, double theta1) {
+    const double v_inc = incident_P ? m1.vL : m1.vT;
+    const double p = m_sin(theta1) / v_inc;
+    const Cx a1 = csqrt_real(1.0 / (m1.vL * m1.vL) - p * p), b1 = csqrt_real(1.0 / (m1.vT * m1.vT) - p * p);
+    const Cx a2 = csqrt_real(1.0 / (m2.vL * m2.vL) - p * p), b2 = csqrt_real(1.0 / (m2.vT * m2.vT) - p * p);
+    const AmmWave inc = amm_wave(m1, incident_P, incident_P ? a1 : b1, p);
+    const AmmWave w[4] = {amm_wave(m1, true, cneg(a1), p), amm_wave(m1, false, cneg(b1), p),
+                          amm_wave(m2, true, a2, p), amm_wave(m2, false, b2, p)};
+    const double sgn[4] = {1.0, 1.0, -1.0, -1.0};
+    Cx M[4][5];
+    for (int j = 0; j < 4; ++j) {
+        M[0][j] = sgn[j] * w[j].dx;
+        M[1][j] = sgn[j] * w[j].dz;
+        M[2][j] = sgn[j] * w[j].txz;
+        M[3][j] = sgn[j] * w[j].tzz;
+    }
+    M[0][4] = cneg(inc.dx);
+    M[1][4] = cneg(inc.dz);
+    M[2][4] = cneg(inc.txz);
+    M[3][4] = cneg(inc.tzz);
+    for (int c = 0; c < 4; ++c) {  // Gauss-Jordan with partial pivoting
+        int piv = c;
+        for (int r = c + 1; r < 4; ++r)
+            if (cabs_(M[r][c]) > cabs_(M[piv][c])) piv = r;
+        if (piv != c)
+            for (int k = 0; k < 5; ++k) {
+                const Cx t = M[c][k];
+                M[c][k] = M[piv][k];
+                M[piv][k] = t;
+            }
+        const Cx d = M[c][c];
+        if (cabs_(d) == 0.0) return 0.0;
+        for (int k = c; k < 5; ++k) M[c][k] = cdiv(M[c][k], d);
+        for (int r = 0; r < 4; ++r)
+            if (r != c) {
+                const Cx f = M[r][c];
+                for (int k = c; k < 5; ++k) M[r][k] = M[r][k] - f * M[c][k];
+            }
+    }
+    const double flux_inc = m1.rho * v_inc * v_inc * (incident_P ? a1 : b1).re;
+    const double tP = m2.rho * m2.vL * m2.vL * fabs(a2.re) * cnorm(M[2][4]) / flux_inc;
+    const double tS = m2.rho * m2.vT * m2.vT * fabs(b2.re) * cnorm(M[3][4]) / flux_inc;
+    return tP + tS;
+}
+
+// IsotropicAMMInterface::transmission (interface_transmission.hpp:125-130)
+CMPMC_HD double amm_transmission(const Medium& sub, const Medium& film, bool longitudinal, double cos_theta) {
+    const double th = m_acos(dclamp(fabs(cos_theta), 0.0, 1.0));
+    if (longitudinal) return amm_psv_transmitted(sub, film, true, th);
+    return 0.5 * (amm_psv_transmitted(sub, film, false, th) + amm_sh(sub, film, th));
+}
 
 // ElectrodePatternMask::find_channel (electrode_pattern.hpp:82-92): the first pad that
 // contains (x, y) gives the channel, drawing once when its fill fraction is below 1;
@@ -543,6 +657,23 @@ CMPMC_HD double film_calc_qp_absorption(const Film& f, double qpE, KBuf& phon, K
 CMPMC_HD double qp_weight(double E, double d, double x) {
     return (x * (E - x) + d * d) / sqrt((x + d) * (E - x + d));
 }
+// Case-II (photon) split weight (kaplan_film.hpp:229-245)
+CMPMC_HD double qp_weight_case2(double E, double d, double x) {
+    return dmax(0.0, x * (E - x) - d * d) / sqrt((x + d) * (E - x + d));
+}
+template <class G>
+CMPMC_HD double film_sample_qp_energy_case2(const Film& f, double E, G& rng) {
+    const double d = f.gap_energy;
+    const double span = E - 2.0 * d;
+    if (span <= 1e-16) return 0.5 * E;
+    const double w_max = dmax(qp_weight_case2(E, d, d), qp_weight_case2(E, d, 0.5 * E)) * 1.0001;
+    for (;;) {
+        const double u = rng.uniform();
+        const double s = m_sin(kHalfPi * u);
+        const double x = d + span * (s * s);
+        if (rng.uniform() * w_max <= qp_weight_case2(E, d, x)) return x;
+    }
+}
 // kaplan_film.hpp:209-227
 template <class G>
 CMPMC_HD double film_sample_qp_energy(const Film& f, double E, G& rng) {
@@ -577,15 +708,16 @@ CMPMC_HD double film_sample_phonon_energy(const Film& f, double E, G& rng) {
     }
 }
 
-// KaplanFilm::absorb_quantum with Seed::Phonon (kaplan_film.hpp:106-206). The four
+// KaplanFilm::absorb_quantum (kaplan_film.hpp:106-206): a phonon seed (photon = false) or a
+// photon seed (an absorbed quantum split into two quasiparticles, no entry step). The four
 // generation buffers of the reference are value-copied at the end of each stage; here
 // the same buffers are swapped, which leaves identical contents. `work` must hold
 // 4 * kKaplanCap doubles; `refl` receives the re-emitted phonon energies.
 template <class G>
-CMPMC_HD double film_absorb_phonon(const Film& f, double energy, KBuf& refl, double* work, G& rng) {
+CMPMC_HD double film_absorb_quantum(const Film& f, double energy, KBuf& refl, double* work, G& rng, bool photon) {
     refl.clear();
-    if (film_direct_absorption(f, energy, rng)) return energy;
-    if (film_is_subgap(f, energy) || rng.uniform() <= film_loss_probability(f, energy, 4.0)) {
+    if (!photon && film_direct_absorption(f, energy, rng)) return energy;
+    if (film_is_subgap(f, energy) || (!photon && rng.uniform() <= film_loss_probability(f, energy, 4.0))) {
         refl.push(energy);
         return 0.0;
     }
@@ -596,7 +728,16 @@ CMPMC_HD double film_absorb_phonon(const Film& f, double energy, KBuf& refl, dou
     KBuf qp{work, 0}, phon{work + kKaplanCap, 0}, next_phon{work + 2 * kKaplanCap, 0},
         next_qp{work + 3 * kKaplanCap, 0};
     const double init_e = energy / n_pairs;
-    for (int i = 0; i < n_pairs; ++i) phon.push(init_e);
+    if (photon) {
+        // case-II split of the absorbed quantum into two quasiparticles (kaplan_film.hpp:134-139)
+        for (int i = 0; i < n_pairs; ++i) {
+            const double qpE = film_sample_qp_energy_case2(f, init_e, rng);
+            edep += film_calc_qp_absorption(f, qpE, phon, qp, rng);
+            edep += film_calc_qp_absorption(f, init_e - qpE, phon, qp, rng);
+        }
+    } else {
+        for (int i = 0; i < n_pairs; ++i) phon.push(init_e);
+    }
 
     while (qp.n != 0 || phon.n != 0) {
         // A. phonons >= 2 Delta break pairs
@@ -656,6 +797,12 @@ CMPMC_HD double film_absorb_phonon(const Film& f, double energy, KBuf& refl, dou
         }
     }
     return edep;
+}
+
+// KaplanFilm::absorb_phonon (kaplan_film.hpp:106-108)
+template <class G>
+CMPMC_HD double film_absorb_phonon(const Film& f, double energy, KBuf& refl, double* work, G& rng) {
+    return film_absorb_quantum(f, energy, refl, work, rng, false);
 }
 
 }  // namespace cmpmc_gpu

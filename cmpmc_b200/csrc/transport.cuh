@@ -27,6 +27,8 @@ struct Detector {
     double charge_max_dk_frac, charge_dt_cap_s, charge_sampling_dk_frac;
     int charge_stepping;
     double fermi_level_above_Ev_eV;
+    int charge_release;            // DetectorModel::ChargeRelease: 0 RecordOnly, 1 BulkDebye, 2 ElectrodeFilm
+    double electrode_seed_max_gap;
     MeshView mesh;      // DetectorModel::mesh_field_3d on the device (tet == nullptr: uniform field)
     MeshView32 mesh32;  // the same mesh in FP32 (batched charge form)
 };
@@ -192,7 +194,9 @@ CMPMC_HD void transport_phonons(const Lattice& L, const Detector& D, C& ctx, EvS
 
                 if (active_pad && s.has_film && rng.uniform() < s.prob_abs) {
                     const Film& film = s.film;
-                    const double p_enter = film.film_absorption;
+                    const double p_enter = s.has_amm ? amm_transmission(s.amm_sub, s.amm_film, trk.mode == 0,
+                                                                        dot(trk.k, bh.n_in))
+                                                     : film.film_absorption;
                     if (rng.uniform() < p_enter) {
                         const double edep = film_absorb_phonon(film, trk.E, ctx.refl, ctx.kwork, rng);
                         if (edep > 0.0) {
@@ -521,6 +525,47 @@ CMPMC_HD double charge_ekin(const Lattice& L, const Charge& c) {
     return (c.type == 1) ? ekin_electron(L, c.valley, c.p) : ekin_hole(L, c.p);
 }
 
+// SimulationEngine::emit_debye_phonons (engine.hpp:894-903): the released energy as
+// Debye-energy phonons at the contact, Lambertian inward
+template <class C>
+CMPMC_HD void emit_debye_phonons(const Lattice& L, double e_rel, V3 pos, V3 n_in, double t, double w, C& ctx,
+                                 Rng& rng) {
+    const double ed = L.debye_energy;
+    const int k = static_cast<int>(round(e_rel / ed));
+    const int n = (k < 1) ? 1 : k;
+    const V3 p0 = pos + n_in * 1e-11;
+    for (int i = 0; i < n; ++i) {
+        const int m = sample_dos_mode(L, rng);
+        const V3 kd = sample_inward(L, m, n_in, rng);
+        ctx.push(make_track(L, p0, kd, m, e_rel / n, t, w));
+    }
+}
+
+// SimulationEngine::electrode_film_release (engine.hpp:906-925): the released energy enters
+// the electrode's film as quanta of at most max(4, electrode_seed_max_gap) Delta (photon
+// seeds); the absorbed part is the hit, escaping phonons re-enter the crystal, the rest is lost
+template <class C>
+CMPMC_HD double electrode_film_release(const Lattice& L, const Detector& D, const Film& film, double e_rel, V3 pos,
+                                       V3 n_in, double t, double w, C& ctx, double& lost, Rng& rng) {
+    const double qmax = dmax(4.0, D.electrode_seed_max_gap) * film.gap_energy;
+    const int k = static_cast<int>(ceil(e_rel / qmax));
+    const int n = (k < 1) ? 1 : k;
+    const double q = e_rel / n;
+    const V3 p0 = pos + n_in * 1e-11;
+    double absorbed = 0.0, emitted = 0.0;
+    for (int i = 0; i < n; ++i) {
+        absorbed += film_absorb_quantum(film, q, ctx.refl, ctx.kwork, rng, true);
+        for (int k = 0; k < ctx.refl.n; ++k) {
+            const int m = sample_dos_mode(L, rng);
+            const V3 kd = sample_inward(L, m, n_in, rng);
+            ctx.push(make_track(L, p0, kd, m, ctx.refl.d[k], t, w));
+            emitted += ctx.refl.d[k];
+        }
+    }
+    lost = dmax(0.0, e_rel - absorbed - emitted);
+    return absorbed;
+}
+
 // SimulationEngine::transport_charges (engine.hpp:192-380). ctx provides
 //   bool pop_charge(Charge&), void push_charge(const Charge&), void push(const Track&),
 //   void hit(const Hit&, int channel), V3 field(V3 pos, Charge&).
@@ -594,11 +639,21 @@ CMPMC_HD void transport_charges(const Lattice& L, const Detector& D, C& ctx, EvS
                         reflect_at_boundary(L, c, bh.n_in, s.prob_charge_spec, rng);
                         continue;
                     }
-                    // collection_release_energy (engine.hpp:889-893), ChargeRelease::RecordOnly
+                    // collection_release_energy (engine.hpp:889-893) and the release mode
+                    // (engine.hpp:302-313)
                     const double muF = (D.fermi_level_above_Ev_eV >= 0.0) ? D.fermi_level_above_Ev_eV : 0.5 * e_gap;
                     const double e_rel = c.ekin + ((c.type == 1) ? (e_gap - muF) : muF);
                     st.charges_collected++;
-                    const double recomb = e_rel * c.w;
+                    double hit_eV = e_rel;
+                    if (D.charge_release == 1) {
+                        hit_eV = 0.0;
+                        emit_debye_phonons(L, e_rel, c.pos, bh.n_in, c.t, c.w, ctx, rng);
+                    } else if (D.charge_release == 2 && s.has_film) {
+                        double lost = 0.0;
+                        hit_eV = electrode_film_release(L, D, s.film, e_rel, c.pos, bh.n_in, c.t, c.w, ctx, lost, rng);
+                        st.escaped_eV += lost * c.w;
+                    }
+                    const double recomb = hit_eV * c.w;
                     st.recomb_eV += recomb;
                     st.deposited_eV += recomb;
                     Hit h;

@@ -137,6 +137,11 @@ __device__ __noinline__ int mask_call(const Pad* pads, int n_pads, float x, floa
     return find_channel(pads, n_pads, static_cast<double>(x), static_cast<double>(y), *g);
 }
 
+// IsotropicAMMInterface::transmission out of line (the complex boundary solve is rare)
+__device__ __noinline__ float amm_call(const Surface* s, bool longitudinal, float cos_theta) {
+    return static_cast<float>(amm_transmission(s->amm_sub, s->amm_film, longitudinal, static_cast<double>(cos_theta)));
+}
+
 // KaplanSurrogateLUT::absorb_phonon_fast (kaplan_film.hpp:361-374): one stored cascade
 // outcome of a bracketing energy node, rescaled; the full cascade outside the table
 __device__ __noinline__ double surrogate_call(const Surface* s, double E, double* refl, int* n_refl, double* work,
@@ -449,7 +454,9 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 active_pad = ch_id >= 0;
             }
             if (active_pad && s.has_film && g.u() < static_cast<float>(s.prob_abs)) {
-                enter = g.u() < static_cast<float>(s.film.film_absorption);
+                const float p_enter = s.has_amm ? amm_call(&s, trk.mode == 0, fdot(trk.k, bh.n))
+                                                : static_cast<float>(s.film.film_absorption);
+                enter = g.u() < p_enter;
                 if constexpr (kAdj) trk.s[3] += enter ? 1.0f : adj.film_miss_score;
             }
             if constexpr (kSplit) {

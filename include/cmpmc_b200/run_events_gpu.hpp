@@ -17,8 +17,8 @@
 // GpuEngine::set_mesh (its node coordinates, potentials and tetrahedra) or
 // set_cartesian_mesh (the build_cartesian_grid arguments and the potential function).
 // Guarded modules raise the reference's UnvalidatedModuleError; configurations the device
-// does not support (interface transmission, charge release other than RecordOnly, bilinear /
-// exact kinematics, 2D meshes) raise std::invalid_argument.
+// does not support (charge release other than RecordOnly, bilinear / exact kinematics, 2D
+// meshes) raise std::invalid_argument.
 #pragma once
 
 #include <algorithm>
@@ -146,6 +146,11 @@ inline cmpmc_detector to_c(const cmpmc::DetectorModel& d) {
         poly(s.anh_coeffs, t.anh_coeffs, t.n_anh);
         t.demo_values = s.demo_values ? 1 : 0;
         t.has_amm = s.amm_interface.has_value() ? 1 : 0;
+        if (s.amm_interface.has_value()) {
+            const auto& a = *s.amm_interface;
+            t.amm_substrate[0] = a.substrate.rho; t.amm_substrate[1] = a.substrate.vL; t.amm_substrate[2] = a.substrate.vT;
+            t.amm_film[0] = a.film.rho; t.amm_film[1] = a.film.vL; t.amm_film[2] = a.film.vT;
+        }
         t.has_mask = 0;  // the pads are attached to the context (GpuEngine constructor)
         if (s.kaplan_sensor.has_value()) {
             const cmpmc::KaplanFilm& f = *s.kaplan_sensor;

@@ -153,10 +153,13 @@ typedef struct cmpmc_surface {
     int32_t demo_values;
     double spec_coeffs[CMPMC_MAX_POLY], diff_coeffs[CMPMC_MAX_POLY], anh_coeffs[CMPMC_MAX_POLY];
     int32_t has_film;
-    int32_t has_amm;               /* interface model: not supported on the device (must be 0) */
+    int32_t has_amm;               /* IsotropicAMMInterface (phonon/interface_transmission.hpp:123-140):
+                                      the substrate -> film transmission replaces film_absorption */
     int32_t has_mask;              /* must be 0: masks are attached with cmpmc_gpu_set_electrode_mask */
     int32_t _pad0;
     cmpmc_film_config film;
+    double amm_substrate[3];       /* IsotropicMedium {rho (kg/m^3), vL, vT (m/s)} of the crystal */
+    double amm_film[3];            /* and of the film                                           */
 } cmpmc_surface;
 
 /* DetectorModel (transport/engine.hpp:96-156) with a CylinderSolid */
@@ -171,7 +174,8 @@ typedef struct cmpmc_detector {
     double luke_sample_fraction;
     double charge_max_dk_frac, charge_dt_cap_s, charge_sampling_dk_frac;
     int32_t charge_stepping;       /* 0 FirstOrderDkCap, 1 LemanSecondOrder */
-    int32_t charge_release;        /* 0 RecordOnly (others unsupported on the device) */
+    int32_t charge_release;        /* DetectorModel::ChargeRelease: 0 RecordOnly, 1 BulkDebye,
+                                      2 ElectrodeFilm (1 and 2: plain FP64 form)            */
     double fermi_level_above_Ev_eV;
     double electrode_seed_max_gap;
     int32_t allow_unvalidated;
@@ -211,6 +215,11 @@ int cmpmc_mask_rectangular_grid(int nx, int ny, double pitch_x, double pitch_y, 
  * 1; -1 for bare crystal. */
 int cmpmc_mask_find_channel(const cmpmc_electrode_pad* pads, uint64_t n, const double pos[3], uint64_t rng_state[4],
                             int32_t* channel);
+
+/* IsotropicAMMInterface::transmission (phonon/interface_transmission.hpp:125-130) on the host:
+ * substrate and film are {rho, vL, vT}; the transmitted energy flux of an L (longitudinal = 1)
+ * or transverse phonon incident at cos_theta. */
+double cmpmc_amm_transmission(const double substrate[3], const double film[3], int longitudinal, double cos_theta);
 
 /* ---- Kaplan-cascade surrogate (replaces KaplanSurrogateLUT, kaplan_film.hpp:336-383) ---- */
 typedef struct cmpmc_kaplan_lut cmpmc_kaplan_lut;

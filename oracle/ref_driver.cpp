@@ -23,6 +23,9 @@
 //       SuperCDMS QET mask (fill 0.8, find_channel drawing from the same stream after each
 //       point) and of a 4 x 4 rectangular grid (find_geometric_channel); x, y as doubles,
 //       then the two channels as int32.
+//   cmpmc_ref amm <n> <out>
+//       IsotropicAMMInterface (the c0a media): transmission of L and transverse phonons at
+//       cos theta = (i + 0.5) / n, i < n; 2n doubles (L then T)
 //   cmpmc_ref kaplan <n> <out>
 //       KaplanSurrogateLUT of the default Al film (seed 1337): for n energies
 //       E = Delta (1 + 45 u) (Rng::for_stream(3, 0), sub-gap, in-table and above-table),
@@ -51,6 +54,9 @@
 //       defaults); field from TriLinearMesh3D::build_cartesian_grid(R, R, h, 58, 58, 57)
 //       with V = 4 (z + h) / 2h + 0.2 ((x^2 + y^2) / R^2) sin(pi z / 2h); all Luke phonons
 //       tracked; seed 13; events_per_chunk 1
+//   c0a c0 with an IsotropicAMMInterface (Ge substrate {5323, 5324.2077, 3258.7879}, Al film
+//       {2700, 6420, 3040}) on both faces; seed 42
+//   tpd tp with ChargeRelease::BulkDebye; tpe tp with ChargeRelease::ElectrodeFilm; seed 77
 //   c0m c0 with the SuperCDMS QET electrode mask (fill fraction 0.8) on both faces; seed 42
 //   tpm tp with the same masks on both faces; seed 77
 //   c3s the same with E = 10 eV * 10^u, max_sampled_phonons 20 (prompt phonons carry the
@@ -89,14 +95,21 @@ struct Workload {
 Workload make_workload(const std::string& w) {
     Workload wl;
     wl.name = w;
-    if (w == "c0" || w == "c0m") wl.seed = 42;
+    if (w == "c0" || w == "c0m" || w == "c0a") wl.seed = 42;
     else if (w == "c1") wl.seed = 7;
     else if (w == "c2") { wl.seed = 11; wl.events_per_chunk = 1; }
     else if (w == "c4") wl.seed = 17;
-    else if (w == "tp" || w == "tpl" || w == "tpm") wl.seed = 77;
+    else if (w == "tp" || w == "tpl" || w == "tpm" || w == "tpd" || w == "tpe") wl.seed = 77;
     else if (w == "c3" || w == "c3s") { wl.seed = 13; wl.events_per_chunk = 1; }
     else { std::fprintf(stderr, "unknown workload %s\n", w.c_str()); std::exit(2); }
     return wl;
+}
+
+physics::IsotropicAMMInterface amm_ge_al() {
+    physics::IsotropicAMMInterface a;
+    a.substrate = {5323.0, 5324.2077, 3258.7879};
+    a.film = {2700.0, 6420.0, 3040.0};
+    return a;
 }
 
 double recoil_potential(const Vec3& p, double R, double h) {
@@ -117,10 +130,14 @@ void setup_detector(const std::string& w, DetectorModel& det) {
     } else if (w == "c2") {
         det.e_field = UniformElectricField::from_bias(4.0, 2.54 * units::cm);
         det.luke_sample_fraction = 0.0;
-    } else if (w == "tp" || w == "tpl" || w == "tpm") {
+    } else if (w == "tp" || w == "tpl" || w == "tpm" || w == "tpd" || w == "tpe") {
         det.e_field = UniformElectricField::from_bias(2.0, 2.54 * units::cm);
         det.luke_sample_fraction = (w == "tpl") ? 1.0 : 0.02;
+        if (w == "tpd") det.charge_release = DetectorModel::ChargeRelease::BulkDebye;
+        if (w == "tpe") det.charge_release = DetectorModel::ChargeRelease::ElectrodeFilm;
     }
+    if (w == "c0a")
+        for (int f = 0; f < 2; ++f) det.surfaces[f].amm_interface = amm_ge_al();
     if (w == "c0m" || w == "tpm")
         for (int f = 0; f < 2; ++f)
             det.surfaces[f].electrode_mask =
@@ -153,7 +170,7 @@ struct Generator {
     }
 
     void generate(EventInput& in) const {
-        if (w == "c0" || w == "c0m") {
+        if (w == "c0" || w == "c0m" || w == "c0a") {
             in.phonons.push_back(engine->make_track({0, 0, 0}, in.rng.isotropic_dir(), PhononMode::L, 7.5e-3));
             in.injected_eV += 7.5e-3;
         } else if (w == "c1") {
@@ -359,6 +376,18 @@ int cmd_mask(uint64_t n, const std::string& out) {
     return 0;
 }
 
+int cmd_amm(uint64_t n, const std::string& out) {
+    const physics::IsotropicAMMInterface a = amm_ge_al();
+    FILE* f = open_or_die(out);
+    for (int lon = 1; lon >= 0; --lon)
+        for (uint64_t i = 0; i < n; ++i) {
+            const double t = a.transmission(lon == 1, (static_cast<double>(i) + 0.5) / static_cast<double>(n));
+            std::fwrite(&t, 8, 1, f);
+        }
+    std::fclose(f);
+    return 0;
+}
+
 int cmd_kaplan(uint64_t n, const std::string& out) {
     const DetectorModel det;
     const KaplanFilm& film = *det.surfaces[0].kaplan_sensor;
@@ -411,6 +440,7 @@ int main(int argc, char** argv) {
     if (cmd == "time" && argc == 6)
         return cmd_time(argv[2], std::strtoull(argv[3], nullptr, 10), std::strtoull(argv[4], nullptr, 10),
                         static_cast<unsigned>(std::atoi(argv[5])));
+    if (cmd == "amm" && argc == 4) return cmd_amm(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "kaplan" && argc == 4) return cmd_kaplan(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mask" && argc == 4) return cmd_mask(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mesh" && argc == 4) return cmd_mesh(std::strtoull(argv[2], nullptr, 10), argv[3]);

@@ -17,13 +17,15 @@ compiled from its own headers by `make -C oracle ref`) and stores compact record
                         `floor` = fraction of events on which it agrees with the glibc build
   mask_channels.npz     channels of the SuperCDMS QET mask (fill 0.8, with its draws) and of
                         a 4 x 4 pad grid at 4096 points of a face
+  amm_transmission.npz  IsotropicAMMInterface (Ge -> Al) transmission of L and transverse
+                        phonons at 400 incidence angles
   kaplan_surrogate.npz  KaplanSurrogateLUT (default Al film, seed 1337) lookups at 2000 energies
                         on [Delta, 46 Delta] with the reference's draws
   mesh_c3.npz           the recoil workloads' field mesh (TriLinearMesh3D::build_cartesian_grid,
                         201,898 nodes): field_at and potential_at at 4096 points in the cylinder
 
 Usage: python tests/golden/make_golden.py [--only NAME,...]   (needs the reference build;
-       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist, kaplan, mask or mesh)
+       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist, amm, kaplan, mask or mesh)
 """
 from __future__ import annotations
 
@@ -56,6 +58,9 @@ PLAN = {
     "c3s": (1, 64),
     "c0m": (16, 2000),
     "tpm": (8, 203),
+    "c0a": (16, 2000),
+    "tpd": (8, 203),
+    "tpe": (8, 203),
 }
 
 
@@ -89,6 +94,11 @@ def main() -> None:
             rec = np.fromfile(path, dtype=np.dtype([("x", "<f8"), ("y", "<f8"), ("qet", "<i4"), ("grid", "<i4")]))
             np.savez_compressed(os.path.join(HERE, "mask_channels.npz"), x=rec["x"], y=rec["y"], qet=rec["qet"],
                                 grid=rec["grid"])
+        if want("amm"):
+            path = os.path.join(tmp, "amm.bin")
+            subprocess.run([REF, "amm", "400", path], check=True)
+            t = np.fromfile(path, dtype=np.float64).reshape(2, -1)
+            np.savez_compressed(os.path.join(HERE, "amm_transmission.npz"), longitudinal=t[0], transverse=t[1])
         if want("kaplan"):
             path = os.path.join(tmp, "kaplan.bin")
             subprocess.run([REF, "kaplan", "2000", path], check=True)

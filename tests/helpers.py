@@ -25,9 +25,15 @@ def detector_for(workload: str):
     elif workload == "c3s":
         det.mesh_field_3d = recoil_mesh()
         det.luke_sample_fraction = 0.05
-    elif workload in ("tp", "tpl", "tpm"):
+    elif workload in ("tp", "tpl", "tpm", "tpd", "tpe"):
         det.e_field = cm.UniformElectricField.from_bias(2.0, 2.54 * cm.units.cm)
         det.luke_sample_fraction = 1.0 if workload == "tpl" else 0.02
+        det.charge_release = {"tpd": 1, "tpe": 2}.get(workload, 0)
+    if workload == "c0a":
+        amm = cm.IsotropicAMMInterface(cm.IsotropicMedium(5323.0, 5324.2077, 3258.7879),
+                                       cm.IsotropicMedium(2700.0, 6420.0, 3040.0))
+        for f in (0, 1):
+            det.surfaces[f].amm_interface = amm
     if workload in ("c0m", "tpm"):
         for f in (0, 1):
             det.surfaces[f].electrode_mask = cm.ElectrodePatternMask.supercdms_qet_mask(det.solid.radius, 0.8)
@@ -45,7 +51,7 @@ def recoil_mesh():
     return _MESH[0]
 
 
-WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13, "c0m": 42, "tpm": 77}
+WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13, "c0m": 42, "tpm": 77, "c0a": 42, "tpd": 77, "tpe": 77}
 
 
 def workload_of(name: str):
@@ -53,7 +59,9 @@ def workload_of(name: str):
     return {"c0": cm.workloads.single_l_origin, "c1": cm.workloads.mixed_energy, "c2": cm.workloads.pair_drift,
             "c4": cm.workloads.single_l_volume, "tp": cm.workloads.test_parallel,
             "tpl": cm.workloads.test_parallel, "c3s": cm.workloads.recoil_light,
-            "c0m": cm.workloads.single_l_origin, "tpm": cm.workloads.test_parallel}[name]
+            "c0m": cm.workloads.single_l_origin, "tpm": cm.workloads.test_parallel,
+            "c0a": cm.workloads.single_l_origin, "tpd": cm.workloads.test_parallel,
+            "tpe": cm.workloads.test_parallel}[name]
 
 
 def has_gpu() -> bool:

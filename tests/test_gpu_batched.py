@@ -193,3 +193,25 @@ def test_batched_kaplan_surrogate_statistics(ge_lattice):
     frac_ref = float(ref["deposited"]) / float(ref["injected"])
     print(f"deposited fraction: surrogate {st.total_deposited_eV / inj:.5f} reference {frac_ref:.5f}")
     assert abs(st.total_deposited_eV / inj / frac_ref - 1.0) < 0.03
+
+
+def test_batched_amm_interface_statistics(ge_lattice):
+    """Ge -> Al acoustic-mismatch film entry (IsotropicAMMInterface) in the batched form
+    against the plain FP64 form (identical to the reference event by event): hit
+    histograms chi^2 p > 0.01 and the same deposited fraction within 1 %."""
+    import cmpmc_b200 as cm
+    eng = _engine(ge_lattice, "c0a")
+    n = 4000
+    plain = cm.run_events(eng, n, workload_of("c0a"), cm.RunOptions(seed=42))
+    batched = _batched(eng, "c0a", n)
+    lo = min(plain.hits["edep"].min(), batched.hits["edep"].min())
+    hi = max(plain.hits["edep"].max(), batched.hits["edep"].max()) * (1 + 1e-9)
+    a = event_histograms(plain.hit_offsets, plain.hits, (lo, hi))
+    b = event_histograms(batched.hit_offsets, batched.hits, (lo, hi))
+    for name in ("time", "radius", "edep"):
+        c2, dof, p = hist_chi2(a, b, name)
+        print(f"AMM {name}: chi2 {c2:.1f} dof {dof} p {p:.3f}")
+        assert p > P_MIN, (name, c2, dof, p)
+    fa = plain.stats.total_deposited_eV / plain.stats.total_injected_eV
+    fb = batched.stats.total_deposited_eV / batched.stats.total_injected_eV
+    assert abs(fb / fa - 1.0) < 0.01

@@ -204,6 +204,22 @@ def test_kaplan_surrogate_matches_reference():
         off += k
 
 
+def test_amm_transmission_matches_reference():
+    """IsotropicAMMInterface (Ge substrate -> Al film): the L and transverse transmission at
+    400 incidence angles equal the reference's (phonon/interface_transmission.hpp:74-130)."""
+    import cmpmc_b200 as cm
+    g = golden("amm_transmission.npz")
+    a = cm.IsotropicAMMInterface(cm.IsotropicMedium(5323.0, 5324.2077, 3258.7879),
+                                 cm.IsotropicMedium(2700.0, 6420.0, 3040.0))
+    n = len(g["longitudinal"])
+    for i in range(n):
+        c = (i + 0.5) / n
+        assert a.transmission(True, c) == g["longitudinal"][i], i
+        assert a.transmission(False, c) == g["transverse"][i], i
+    # flux conservation holds in the reference's model: transmission within [0, 1]
+    assert 0.0 <= g["longitudinal"].min() and g["transverse"].max() <= 1.0
+
+
 def test_python_generator_matches_native(ge_lattice):
     import cmpmc_b200 as cm
     det = detector_for("tp")
