@@ -173,6 +173,8 @@ _SIG = {
     "cmpmc_lattice_destroy": (None, [C.c_void_p]),
     "cmpmc_lattice_tables": (_i32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                     C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "cmpmc_lattice_set_kinematics_mode": (_i32, [C.c_void_p, _i32]),
+    "cmpmc_lattice_kinematics_mode": (_i32, [C.c_void_p]),
     "cmpmc_lattice_map_k_to_vg": (_i32, [C.c_void_p, _i32, C.POINTER(_f64), C.POINTER(_f64), C.POINTER(_f64)]),
     "cmpmc_make_track": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_f64), _i32, _f64, _f64, _f64, C.c_void_p]),
     "cmpmc_make_charge": (_i32, [C.c_void_p, _i32, C.POINTER(_f64), C.POINTER(_f64), _f64, _i32, _f64,

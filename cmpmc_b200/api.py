@@ -704,6 +704,18 @@ class CrystalLattice:
             "hv": np.ctypeslib.as_array(C.cast(hv, C.POINTER(C.c_double)), shape=(n.value,)).copy(),
         }
 
+    # CrystalLattice::KinematicsMode (crystal_lattice.hpp:63-74)
+    Octahedral, Exact, Bilinear = 0, 1, 2
+
+    def set_kinematics_mode(self, mode: int) -> None:
+        """Octahedral (default), Exact (Cardano solve per call) or Bilinear (181 x 361
+        table). Applies to make_track, the generators and every device context created
+        afterwards from this lattice (engines made before keep their contexts)."""
+        _check(self._lib.cmpmc_lattice_set_kinematics_mode(self._h, int(mode)), what="kinematics mode")
+
+    def kinematics_mode(self) -> int:
+        return self._lib.cmpmc_lattice_kinematics_mode(self._h)
+
     def map_k_to_vg(self, mode: int, k_det: Sequence[float]):
         k = (C.c_double * 3)(*k_det)
         vg = (C.c_double * 3)()

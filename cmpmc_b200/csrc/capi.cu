@@ -86,6 +86,7 @@ struct cmpmc_gpu_ctx {
     Detector D{};
     DevBuf tables;  // oct LUT + CDF tables
     DevBuf mesh;    // MeshTet records of the attached field mesh
+    DevBuf kin;     // stiffness tensor and bilinear table of the lattice's kinematics mode
     int tpb = 128;
     int bps = 0;  // 0: occupancy-derived
     uint32_t stack_cap = 1024;        // plain form: tracks per device thread
@@ -595,6 +596,21 @@ int cmpmc_gpu_create(const cmpmc_lattice* lat, const cmpmc_detector* det, int de
         return fail(nullptr, CMPMC_ERR_CUDA, msg);
     }
     ctx->L = lat->view;
+    if (e == cudaSuccess && lat->view.kin_mode != kKinOctahedral) {
+        // the exact and bilinear modes read the stiffness tensor / the bilinear table
+        const size_t b_st = sizeof(Stiffness), b_bil = lat->bil.size() * sizeof(double);
+        e = ctx->kin.ensure(b_st + b_bil);
+        if (e == cudaSuccess) e = cudaMemcpy(ctx->kin.p, &lat->stiff, b_st, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && b_bil)
+            e = cudaMemcpy(static_cast<char*>(ctx->kin.p) + b_st, lat->bil.data(), b_bil, cudaMemcpyHostToDevice);
+        ctx->L.stiff = ctx->kin.as<Stiffness>();
+        ctx->L.bil = b_bil ? reinterpret_cast<const double*>(static_cast<char*>(ctx->kin.p) + b_st) : nullptr;
+        if (e != cudaSuccess) {
+            const std::string msg = std::string("context setup: ") + cudaGetErrorString(e);
+            cmpmc_gpu_destroy(ctx);
+            return fail(nullptr, CMPMC_ERR_CUDA, msg);
+        }
+    }
     ctx->L.oct = static_cast<const OctEntry*>(ctx->tables.p);
     ctx->L.cdf_lt = reinterpret_cast<const double*>(static_cast<char*>(ctx->tables.p) + oct_bytes);
     ctx->L.cdf_tt = ctx->L.cdf_lt + kNCdf;
@@ -618,7 +634,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->film_a, &ctx->queue_b, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
+    for (DevBuf* b : {&ctx->kin, &ctx->film_a, &ctx->queue_b, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
                       &ctx->ccounters, &ctx->carrier_event, &ctx->cursor, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
@@ -916,6 +932,8 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     uint64_t n_hits = 0;
     uint64_t* ev_offsets = nullptr;
     cmpmc_sim_stats* ev_stats = nullptr;
+    if (batched && ctx->L.kin_mode != kKinOctahedral)
+        return fail(ctx, CMPMC_ERR_INVALID, "Exact and Bilinear kinematics run in the plain FP64 form");
     if (batched && n_ch > 0 && ctx->det.charge_release != 0)
         return fail(ctx, CMPMC_ERR_INVALID,
                     "BulkDebye / ElectrodeFilm charge release runs in the plain FP64 form (batched: RecordOnly)");
@@ -1158,6 +1176,8 @@ int cmpmc_gpu_adjoint(cmpmc_gpu_ctx* ctx, const cmpmc_adjoint_desc* d, cmpmc_adj
     for (int i = 0; i < 3; ++i)
         if (ctx->det.surfaces[i].has_amm)
             return fail(ctx, CMPMC_ERR_INVALID, "the adjoint's film parameter is film_absorption: no AMM interfaces");
+    if (ctx->L.kin_mode != kKinOctahedral)
+        return fail(ctx, CMPMC_ERR_INVALID, "the adjoint runs with octahedral kinematics");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     cudaStream_t s = ctx->stream;
     int launches = 0;

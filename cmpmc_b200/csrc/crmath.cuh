@@ -17,9 +17,9 @@
 //    from 80-digit tables (gen_crmath_tables.py).
 //  * exp / pow: reduction by k log 2, then the Taylor series of exp(r/16) squared four
 //    times (pow(x, y) = exp(y log x) with log x kept as a double-double).
-//  * hypot / cbrt / acos: one Newton correction in double-double from sqrt(x^2 + y^2)
-//    rounded and from the platform cbrt / acos (the correction makes the result
-//    independent of the platform's last bit).
+//  * hypot / cbrt / acos / atan2: one Newton correction in double-double from
+//    sqrt(x^2 + y^2) rounded and from the platform cbrt / acos / atan2 (the correction makes
+//    the result independent of the platform's last bit).
 //  * sin / cos: Cody-Waite reduction by pi/2 split into four parts (W. J. Cody and
 //    W. Waite, "Software Manual for the Elementary Functions", 1980), then the Taylor
 //    series of sin and cos on |r| <= pi/4.
@@ -434,6 +434,18 @@ CMPMC_HD double acos(double x) {
     const DD f = dd_add_d(c, -x);  // cos(y0) - x
     const double corr = (f.hi + f.lo) / (s.hi + s.lo);
     return y0 + corr;
+}
+
+// atan2(y, x) correctly rounded: one Newton step on y cos(t) - x sin(t) = 0 in double-double
+// from the platform atan2 (zeros, infinities and NaNs go to the platform atan2).
+CMPMC_HD double atan2(double y, double x) {
+    if (!(fabs(x) < 1.0 / 0.0) || !(fabs(y) < 1.0 / 0.0) || x == 0.0 || y == 0.0) return ::atan2(y, x);
+    const double t0 = ::atan2(y, x);
+    DD s, c;
+    sincos_dd(t0, s, c);
+    const DD f = dd_add(dd_mul_d(c, y), dd_mul_d(s, -x));  // y cos(t0) - x sin(t0)
+    const double g = x * c.hi + y * s.hi;                    // hypot(x, y) near the root
+    return t0 + (f.hi + f.lo) / g;
 }
 
 // both at once

@@ -14,7 +14,9 @@ struct cmpmc_lattice {
     std::vector<cmpmc_gpu::OctEntry> oct;  // [3][256][256]
     std::vector<double> cdf_lt, cdf_tt;    // [1024] each
     std::vector<double> hv;                // flattened HV tensors (see cmpmc_lattice_tables)
-    cmpmc_gpu::Lattice view;               // host pointers into the vectors above
+    cmpmc_gpu::Stiffness stiff;            // C_ijlm (exact kinematics)
+    std::vector<double> bil;               // [3][181][361][3] (bilinear kinematics, built on request)
+    cmpmc_gpu::Lattice view;               // host pointers into the members above
 };
 
 struct cmpmc_kaplan_lut {

@@ -91,98 +91,6 @@ int voigt_index(int i, int j) {
     return 5;
 }
 
-struct Stiffness {
-    double C[3][3][3][3];
-};
-
-double comp(V3 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
-
-// physics::christoffel_modes_from_eigen (phonon/phonon_kernels.hpp:134-175)
-void modes_from_eigen(const Stiffness& S, double density, V3 k, const double evals[3], const V3 evecs[3],
-                      V3 vg_out[3]) {
-    const double inv_rho = 1.0 / density;
-    int long_idx = 0;
-    double max_dot = -1.0;
-    for (int i = 0; i < 3; ++i) {
-        const double d = std::abs(dot(evecs[i], k));
-        if (d > max_dot) {
-            max_dot = d;
-            long_idx = i;
-        }
-    }
-    const int rem1 = (long_idx + 1) % 3;
-    const int rem2 = (long_idx + 2) % 3;
-    const int ft_idx = (evals[rem1] >= evals[rem2]) ? rem1 : rem2;
-    const int st_idx = (evals[rem1] >= evals[rem2]) ? rem2 : rem1;
-    const int mode_indices[3] = {long_idx, ft_idx, st_idx};
-    for (int m = 0; m < 3; ++m) {
-        const int idx = mode_indices[m];
-        const double vp = std::sqrt(std::max(evals[idx], 1.0));
-        const V3 e = evecs[idx];
-        const V3 slow = vdiv(k, vp);
-        double out[3];
-        for (int dim = 0; dim < 3; ++dim) {
-            double sum = 0.0;
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j)
-                    for (int l = 0; l < 3; ++l)
-                        sum += comp(e, i) * S.C[i][j][l][dim] * comp(slow, j) * comp(e, l);
-            out[dim] = sum * inv_rho;
-        }
-        vg_out[m] = v3(out[0], out[1], out[2]);
-    }
-}
-
-// physics::solve_christoffel_exact: cyclic Jacobi on the 3x3 Christoffel matrix
-// (phonon/phonon_kernels.hpp:182-247)
-void solve_christoffel(const Stiffness& S, double density, V3 k, V3 vg_out[3]) {
-    double D[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    const double inv_rho = 1.0 / density;
-    for (int i = 0; i < 3; ++i)
-        for (int l = 0; l < 3; ++l) {
-            double sum = 0.0;
-            for (int j = 0; j < 3; ++j)
-                for (int m = 0; m < 3; ++m) sum += S.C[i][j][l][m] * comp(k, j) * comp(k, m);
-            D[i][l] = sum * inv_rho;
-        }
-    double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
-    for (int sweep = 0; sweep < 12; ++sweep) {
-        const double off = std::abs(D[0][1]) + std::abs(D[0][2]) + std::abs(D[1][2]);
-        if (off < 1e-15 * (std::abs(D[0][0]) + std::abs(D[1][1]) + std::abs(D[2][2]))) break;
-        for (int p = 0; p < 2; ++p)
-            for (int q = p + 1; q < 3; ++q) {
-                if (std::abs(D[p][q]) < 1e-18) continue;
-                const double tau = (D[q][q] - D[p][p]) / (2.0 * D[p][q]);
-                const double t = (tau >= 0.0) ? (1.0 / (tau + std::sqrt(1.0 + tau * tau)))
-                                              : (-1.0 / (-tau + std::sqrt(1.0 + tau * tau)));
-                const double c = 1.0 / std::sqrt(1.0 + t * t);
-                const double s = t * c;
-                const double d_pp = D[p][p];
-                const double d_qq = D[q][q];
-                const double d_pq = D[p][q];
-                D[p][p] = c * c * d_pp - 2.0 * s * c * d_pq + s * s * d_qq;
-                D[q][q] = s * s * d_pp + 2.0 * s * c * d_pq + c * c * d_qq;
-                D[p][q] = D[q][p] = 0.0;
-                for (int r = 0; r < 3; ++r) {
-                    if (r != p && r != q) {
-                        const double d_rp = D[r][p];
-                        const double d_rq = D[r][q];
-                        D[r][p] = D[p][r] = c * d_rp - s * d_rq;
-                        D[r][q] = D[q][r] = s * d_rp + c * d_rq;
-                    }
-                    const double v_rp = V[r][p];
-                    const double v_rq = V[r][q];
-                    V[r][p] = c * v_rp - s * v_rq;
-                    V[r][q] = s * v_rp + c * v_rq;
-                }
-            }
-    }
-    const double evals[3] = {D[0][0], D[1][1], D[2][2]};
-    const V3 evecs[3] = {v3(V[0][0], V[1][0], V[2][0]), v3(V[0][1], V[1][1], V[2][1]),
-                         v3(V[0][2], V[1][2], V[2][2])};
-    modes_from_eigen(S, density, k, evals, evecs, vg_out);
-}
-
 // CrystalLattice::oct_decode (crystal_lattice.hpp:132-141)
 V3 oct_decode(double u, double v) {
     const double kz = 1.0 - std::abs(u) - std::abs(v);
@@ -251,11 +159,34 @@ double tamura_tt_pdf(double x, const cmpmc_crystal_config& c) {
     return t1 * t1 + t2 * t2;
 }
 
+// the 181 x 361 bilinear (cos theta, phi) table (crystal_lattice.hpp:350-368)
+void build_bilinear(cmpmc_lattice& lat) {
+    const cmpmc_crystal_config& c = lat.cfg;
+    lat.bil.assign(static_cast<size_t>(3) * kNCTheta * kNPhi * 3, 0.0);
+    for (int i = 0; i < kNCTheta; ++i) {
+        const double ctheta = -1.0 + 2.0 * (static_cast<double>(i) / (kNCTheta - 1));
+        const double stheta = std::sqrt(std::max(0.0, 1.0 - ctheta * ctheta));
+        for (int j = 0; j < kNPhi; ++j) {
+            const double phi = kTwoPi * (static_cast<double>(j) / (kNPhi - 1));
+            V3 k = v3(stheta * std::cos(phi), stheta * std::sin(phi), ctheta);
+            if (stheta < 1e-7) k = unit(v3(1e-6, 0.0, ctheta));
+            V3 vg[3];
+            solve_christoffel(lat.stiff, c.density, k, vg);
+            for (int m = 0; m < 3; ++m) {
+                double* e = &lat.bil[3 * ((static_cast<size_t>(m) * kNCTheta + i) * kNPhi + j)];
+                e[0] = vg[m].x;
+                e[1] = vg[m].y;
+                e[2] = vg[m].z;
+            }
+        }
+    }
+}
+
 void build_tables(cmpmc_lattice& lat) {
     const cmpmc_crystal_config& c = lat.cfg;
     // stiffness tensor (crystal_lattice.hpp:340-348)
     const Voigt Vt = build_voigt(c);
-    Stiffness S;
+    Stiffness& S = lat.stiff;
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j)
             for (int l = 0; l < 3; ++l)
@@ -336,6 +267,10 @@ void build_tables(cmpmc_lattice& lat) {
 
     // scalar view
     L.oct = lat.oct.data();
+    L.kin_mode = kKinOctahedral;
+    L.density = c.density;
+    L.stiff = &lat.stiff;
+    L.bil = nullptr;
     L.cdf_lt = lat.cdf_lt.data();
     L.cdf_tt = lat.cdf_tt.data();
     L.orient = orient;
@@ -438,6 +373,16 @@ int cmpmc_lattice_create(const cmpmc_crystal_config* cfg, cmpmc_lattice** out) {
 }
 
 void cmpmc_lattice_destroy(cmpmc_lattice* lat) { delete lat; }
+
+int cmpmc_lattice_set_kinematics_mode(cmpmc_lattice* lat, int mode) {
+    if (!lat || mode < kKinOctahedral || mode > kKinBilinear) return CMPMC_ERR_INVALID;
+    if (mode == kKinBilinear && lat->bil.empty()) build_bilinear(*lat);
+    lat->view.bil = lat->bil.empty() ? nullptr : lat->bil.data();
+    lat->view.kin_mode = mode;
+    return CMPMC_OK;
+}
+
+int cmpmc_lattice_kinematics_mode(const cmpmc_lattice* lat) { return lat ? lat->view.kin_mode : -1; }
 
 int cmpmc_lattice_tables(const cmpmc_lattice* lat, const float** oct_lut, const double** cdf_lt,
                          const double** cdf_tt, const double** hv, size_t* n_hv) {

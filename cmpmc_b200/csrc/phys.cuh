@@ -37,6 +37,7 @@ CMPMC_HD double m_pow(double x, double y) { return crmath::pow(x, y); }
 CMPMC_HD double m_hypot(double x, double y) { return crmath::hypot(x, y); }
 CMPMC_HD double m_cbrt(double x) { return crmath::cbrt(x); }
 CMPMC_HD double m_acos(double x) { return crmath::acos(x); }
+CMPMC_HD double m_atan2(double y, double x) { return crmath::atan2(y, x); }
 #else
 CMPMC_HD double m_log(double x) { return ::log(x); }
 CMPMC_HD double m_sin(double x) { return ::sin(x); }
@@ -46,6 +47,7 @@ CMPMC_HD double m_pow(double x, double y) { return ::pow(x, y); }
 CMPMC_HD double m_hypot(double x, double y) { return ::hypot(x, y); }
 CMPMC_HD double m_cbrt(double x) { return ::cbrt(x); }
 CMPMC_HD double m_acos(double x) { return ::acos(x); }
+CMPMC_HD double m_atan2(double y, double x) { return ::atan2(y, x); }
 #endif
 
 // ---- constants (core/units.hpp:26-72) ---------------------------------------------
@@ -179,8 +181,18 @@ struct OctEntry {
     float vx, vy, vz, vmag;
 };
 
+struct Stiffness;
+
+// CrystalLattice::KinematicsMode (crystal_lattice.hpp:63-74)
+enum { kKinOctahedral = 0, kKinExact = 1, kKinBilinear = 2 };
+constexpr int kNCTheta = 181, kNPhi = 361;  // bilinear (cos theta, phi) table (crystal_lattice.hpp:28-29)
+
 struct Lattice {
     const OctEntry* oct;   // [3][256][256]
+    int kin_mode;          // kKin*
+    double density;
+    const Stiffness* stiff;  // C_ijlm (exact mode)
+    const double* bil;       // [3][181][361][3] group velocities (bilinear mode)
     const double* cdf_lt;  // [1024]
     const double* cdf_tt;  // [1024]
     M3 orient;
@@ -267,8 +279,61 @@ CMPMC_HD OctEntry load_oct(const OctEntry* t, int i) {
 CMPMC_HD OctEntry load_oct(const OctEntry* t, int i) { return t[i]; }
 #endif
 
+#ifdef __CUDACC__
+#define CMPMC_HD_COLD static __host__ __device__ __noinline__
+#else
+#define CMPMC_HD_COLD static inline
+#endif
+}  // namespace cmpmc_gpu
+#include "christoffel.cuh"
+namespace cmpmc_gpu {
+
+// CrystalLattice::map_k_to_vg_exact (crystal_lattice.hpp:76-84): the Cardano solve per call
+CMPMC_HD_COLD Kin map_k_to_vg_exact(const Lattice& L, int mode, V3 k_det) {
+    const V3 k = unit(mul_transpose(L.orient, k_det));
+    V3 vg[3];
+    solve_christoffel_cardano(*L.stiff, L.density, k, vg);
+    const V3 v = vg[mode];
+    const double mag = norm(v);
+    Kin r;
+    r.vg_dir = unit(mul(L.orient, vdiv(v, dmax(mag, 1e-12))));
+    r.vg_mag = mag;
+    return r;
+}
+
+// CrystalLattice::map_k_to_vg, bilinear (cos theta, phi) table (crystal_lattice.hpp:86-114)
+CMPMC_HD_COLD Kin map_k_to_vg_bilinear(const Lattice& L, int mode, V3 k_det) {
+    const V3 k = unit(mul_transpose(L.orient, k_det));
+    const double ctheta = dclamp(k.z, -1.0, 1.0);
+    double phi = m_atan2(k.y, k.x);
+    if (phi < 0.0) phi += kTwoPi;
+    const double u = (ctheta + 1.0) * 0.5 * (kNCTheta - 1);
+    const double v = (phi / kTwoPi) * (kNPhi - 1);
+    const int ui = static_cast<int>(u), vi = static_cast<int>(v);
+    const int i0 = (ui < 0) ? 0 : ((ui > kNCTheta - 2) ? kNCTheta - 2 : ui);
+    const int j0 = (vi < 0) ? 0 : ((vi > kNPhi - 2) ? kNPhi - 2 : vi);
+    const double du = u - i0;
+    const double dv = v - j0;
+    auto at = [&](int i, int j) {
+        const double* e = L.bil + 3 * ((static_cast<size_t>(mode) * kNCTheta + i) * kNPhi + j);
+        return v3(e[0], e[1], e[2]);
+    };
+    const V3 vg = at(i0, j0) * ((1.0 - du) * (1.0 - dv)) + at(i0 + 1, j0) * (du * (1.0 - dv)) +
+                  at(i0, j0 + 1) * ((1.0 - du) * dv) + at(i0 + 1, j0 + 1) * (du * dv);
+    const double mag = norm(vg);
+    const V3 vg_det = mul(L.orient, vdiv(vg, dmax(mag, 1e-12)));
+    Kin r;
+    r.vg_dir = unit(vg_det);
+    r.vg_mag = mag;
+    return r;
+}
+
+// CrystalLattice::map_k_to_vg (crystal_lattice.hpp:86-89): dispatch on the kinematics mode
 CMPMC_HD Kin map_k_to_vg(const Lattice& L, int mode, V3 k_det) {
-    return map_k_to_vg_oct_impl(L, mode, k_det, [&](int i) { return load_oct(L.oct, i); });
+    if (L.kin_mode == kKinOctahedral)
+        return map_k_to_vg_oct_impl(L, mode, k_det, [&](int i) { return load_oct(L.oct, i); });
+    if (L.kin_mode == kKinExact) return map_k_to_vg_exact(L, mode, k_det);
+    return map_k_to_vg_bilinear(L, mode, k_det);
 }
 
 // ---- phonon rates and samplers (phonon/phonon_kernels.hpp:29-92) --------------------

@@ -17,8 +17,9 @@
 // GpuEngine::set_mesh (its node coordinates, potentials and tetrahedra) or
 // set_cartesian_mesh (the build_cartesian_grid arguments and the potential function).
 // Guarded modules raise the reference's UnvalidatedModuleError; configurations the device
-// does not support (charge release other than RecordOnly, bilinear / exact kinematics, 2D
-// meshes) raise std::invalid_argument.
+// does not support (2D meshes; in the batched forms, charge release other than RecordOnly
+// and Exact / Bilinear kinematics) raise std::invalid_argument. Build the GpuEngine from the
+// CrystalLattice itself to carry its kinematics mode.
 #pragma once
 
 #include <algorithm>
@@ -189,8 +190,16 @@ inline cmpmc_detector to_c(const cmpmc::DetectorModel& d) {
 class GpuEngine {
 public:
     GpuEngine(const cmpmc::CrystalConfig& cfg, const cmpmc::DetectorModel& det, int device = 0)
+        : GpuEngine(cfg, 0, det, device) {}
+    // The same with the lattice's kinematics mode (CrystalLattice::set_kinematics_mode).
+    GpuEngine(const cmpmc::CrystalLattice& lattice, const cmpmc::DetectorModel& det, int device = 0)
+        : GpuEngine(lattice.config(), static_cast<int>(lattice.kinematics_mode()), det, device) {}
+
+    GpuEngine(const cmpmc::CrystalConfig& cfg, int kinematics_mode, const cmpmc::DetectorModel& det, int device)
         : ccfg_(detail::to_c(cfg)), cdet_(detail::to_c(det)), needs_mesh_(det.mesh_field_3d.has_value()) {
         detail::check(cmpmc_lattice_create(&ccfg_, &lat_), nullptr, "lattice");
+        if (kinematics_mode != 0) detail::check(cmpmc_lattice_set_kinematics_mode(lat_, kinematics_mode), nullptr,
+                                                "kinematics mode");
         const int st = cmpmc_gpu_create(lat_, &cdet_, device, &ctx_);
         if (st != CMPMC_OK) {
             cmpmc_lattice_destroy(lat_);

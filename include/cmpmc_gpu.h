@@ -180,7 +180,7 @@ typedef struct cmpmc_detector {
     double electrode_seed_max_gap;
     int32_t allow_unvalidated;
     int32_t jump_to_ballistic;     /* experimental; must be 0 */
-    int32_t kinematics_mode;       /* CrystalLattice::KinematicsMode: 0 Octahedral (only) */
+    int32_t kinematics_mode;       /* must be 0: the mode is the lattice's (cmpmc_lattice_set_kinematics_mode) */
     int32_t _pad0;
 } cmpmc_detector;
 
@@ -248,7 +248,13 @@ void cmpmc_lattice_destroy(cmpmc_lattice* lat);
  * l0_h, k_sound_e, k_sound_h, n_valleys, valley_rot[n][3][3]. */
 int cmpmc_lattice_tables(const cmpmc_lattice* lat, const float** oct_lut, const double** cdf_lt,
                          const double** cdf_tt, const double** hv, size_t* n_hv);
-/* CrystalLattice::map_k_to_vg_oct (crystal_lattice.hpp:144-176), on the host. */
+/* CrystalLattice::set_kinematics_mode (crystal_lattice.hpp:63-74): 0 Octahedral (default),
+ * 1 Exact (Cardano solve per call), 2 Bilinear (181 x 361 (cos theta, phi) table, built here
+ * on first request). It applies to make_track, the generators and every device context
+ * created afterwards from this lattice; Exact and Bilinear run in the plain FP64 form. */
+int cmpmc_lattice_set_kinematics_mode(cmpmc_lattice* lat, int mode);
+int cmpmc_lattice_kinematics_mode(const cmpmc_lattice* lat);
+/* CrystalLattice::map_k_to_vg (crystal_lattice.hpp:76-176, the lattice's mode), on the host. */
 int cmpmc_lattice_map_k_to_vg(const cmpmc_lattice* lat, int mode, const double k_det[3],
                               double vg_dir[3], double* vg_mag);
 /* SimulationEngine::make_track (engine.hpp:171-187), on the host. */

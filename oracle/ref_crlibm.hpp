@@ -50,8 +50,12 @@ inline double cr_hypot_q(double x, double y) {
 }
 inline double cr_cbrt_q(double x) { return cmpmc_oracle::g_crlibm ? static_cast<double>(cbrtq(x)) : ::cbrt(x); }
 inline double cr_acos_q(double x) { return cmpmc_oracle::g_crlibm ? static_cast<double>(acosq(x)) : ::acos(x); }
+inline double cr_atan2_q(double y, double x) {
+    return cmpmc_oracle::g_crlibm ? static_cast<double>(atan2q(y, x)) : ::atan2(y, x);
+}
 }  // namespace std
 using std::cr_acos_q;
+using std::cr_atan2_q;
 using std::cr_cbrt_q;
 using std::cr_cos_q;
 using std::cr_exp_q;
@@ -68,3 +72,4 @@ using std::cr_sin_q;
 #define hypot cr_hypot_q
 #define cbrt cr_cbrt_q
 #define acos cr_acos_q
+#define atan2 cr_atan2_q

@@ -23,6 +23,10 @@
 //       SuperCDMS QET mask (fill 0.8, find_channel drawing from the same stream after each
 //       point) and of a 4 x 4 rectangular grid (find_geometric_channel); x, y as doubles,
 //       then the two channels as int32.
+//   cmpmc_ref kin <n> <out>
+//       map_k_to_vg of the Ge lattice in the Exact and the Bilinear modes for n directions
+//       (Rng::for_stream(21, 0) isotropic) and the three modes: per direction and mode
+//       (vg_dir[3], vg_mag) for Exact, then for Bilinear (8 doubles)
 //   cmpmc_ref amm <n> <out>
 //       IsotropicAMMInterface (the c0a media): transmission of L and transverse phonons at
 //       cos theta = (i + 0.5) / n, i < n; 2n doubles (L then T)
@@ -57,6 +61,7 @@
 //   c0a c0 with an IsotropicAMMInterface (Ge substrate {5323, 5324.2077, 3258.7879}, Al film
 //       {2700, 6420, 3040}) on both faces; seed 42
 //   tpd tp with ChargeRelease::BulkDebye; tpe tp with ChargeRelease::ElectrodeFilm; seed 77
+//   c0x c0 with KinematicsMode::Exact; c0b c0 with KinematicsMode::Bilinear; seed 42
 //   c0m c0 with the SuperCDMS QET electrode mask (fill fraction 0.8) on both faces; seed 42
 //   tpm tp with the same masks on both faces; seed 77
 //   c3s the same with E = 10 eV * 10^u, max_sampled_phonons 20 (prompt phonons carry the
@@ -95,7 +100,7 @@ struct Workload {
 Workload make_workload(const std::string& w) {
     Workload wl;
     wl.name = w;
-    if (w == "c0" || w == "c0m" || w == "c0a") wl.seed = 42;
+    if (w == "c0" || w == "c0m" || w == "c0a" || w == "c0x" || w == "c0b") wl.seed = 42;
     else if (w == "c1") wl.seed = 7;
     else if (w == "c2") { wl.seed = 11; wl.events_per_chunk = 1; }
     else if (w == "c4") wl.seed = 17;
@@ -121,6 +126,11 @@ geometry::TriLinearMesh3D recoil_mesh(const CylinderSolid& s) {
     const double R = s.radius, h = s.half_z;
     return geometry::TriLinearMesh3D::build_cartesian_grid(
         R, R, h, 58, 58, 57, [R, h](const Vec3& p) { return recoil_potential(p, R, h); });
+}
+
+void setup_lattice(const std::string& w, CrystalLattice& lattice) {
+    if (w == "c0x") lattice.set_kinematics_mode(CrystalLattice::KinematicsMode::Exact);
+    if (w == "c0b") lattice.set_kinematics_mode(CrystalLattice::KinematicsMode::Bilinear);
 }
 
 void setup_detector(const std::string& w, DetectorModel& det) {
@@ -170,7 +180,7 @@ struct Generator {
     }
 
     void generate(EventInput& in) const {
-        if (w == "c0" || w == "c0m" || w == "c0a") {
+        if (w == "c0" || w == "c0m" || w == "c0a" || w == "c0x" || w == "c0b") {
             in.phonons.push_back(engine->make_track({0, 0, 0}, in.rng.isotropic_dir(), PhononMode::L, 7.5e-3));
             in.injected_eV += 7.5e-3;
         } else if (w == "c1") {
@@ -234,7 +244,8 @@ FILE* open_or_die(const std::string& path) {
 
 int cmd_dump(const std::string& w, uint64_t first, uint64_t n, unsigned threads, const std::string& prefix) {
     const Workload wl = make_workload(w);
-    const CrystalLattice lattice(materials::Germanium());
+    CrystalLattice lattice(materials::Germanium());
+    setup_lattice(w, lattice);
     DetectorModel det;
     setup_detector(w, det);
     const SimulationEngine engine(lattice, det);
@@ -297,7 +308,8 @@ int cmd_dump(const std::string& w, uint64_t first, uint64_t n, unsigned threads,
 int cmd_time(const std::string& w, uint64_t first, uint64_t n, unsigned threads) {
     const Workload wl = make_workload(w);
     const auto t0 = std::chrono::steady_clock::now();
-    const CrystalLattice lattice(materials::Germanium());
+    CrystalLattice lattice(materials::Germanium());
+    setup_lattice(w, lattice);
     DetectorModel det;
     setup_detector(w, det);
     const SimulationEngine engine(lattice, det);
@@ -376,6 +388,25 @@ int cmd_mask(uint64_t n, const std::string& out) {
     return 0;
 }
 
+int cmd_kin(uint64_t n, const std::string& out) {
+    CrystalLattice lat(materials::Germanium());
+    Rng rng = Rng::for_stream(21, 0);
+    std::vector<Vec3> ks(n);
+    for (auto& k : ks) k = rng.isotropic_dir();
+    FILE* f = open_or_die(out);
+    for (auto mode : {CrystalLattice::KinematicsMode::Exact, CrystalLattice::KinematicsMode::Bilinear}) {
+        lat.set_kinematics_mode(mode);
+        for (const Vec3& k : ks)
+            for (int m = 0; m < 3; ++m) {
+                const auto kin = lat.map_k_to_vg(static_cast<PhononMode>(m), k);
+                const double rec[4] = {kin.vg_dir.x, kin.vg_dir.y, kin.vg_dir.z, kin.vg_mag};
+                std::fwrite(rec, 8, 4, f);
+            }
+    }
+    std::fclose(f);
+    return 0;
+}
+
 int cmd_amm(uint64_t n, const std::string& out) {
     const physics::IsotropicAMMInterface a = amm_ge_al();
     FILE* f = open_or_die(out);
@@ -440,6 +471,7 @@ int main(int argc, char** argv) {
     if (cmd == "time" && argc == 6)
         return cmd_time(argv[2], std::strtoull(argv[3], nullptr, 10), std::strtoull(argv[4], nullptr, 10),
                         static_cast<unsigned>(std::atoi(argv[5])));
+    if (cmd == "kin" && argc == 4) return cmd_kin(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "amm" && argc == 4) return cmd_amm(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "kaplan" && argc == 4) return cmd_kaplan(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mask" && argc == 4) return cmd_mask(std::strtoull(argv[2], nullptr, 10), argv[3]);

@@ -17,6 +17,7 @@ compiled from its own headers by `make -C oracle ref`) and stores compact record
                         `floor` = fraction of events on which it agrees with the glibc build
   mask_channels.npz     channels of the SuperCDMS QET mask (fill 0.8, with its draws) and of
                         a 4 x 4 pad grid at 4096 points of a face
+  kinematics_modes.npz  map_k_to_vg in the Exact and Bilinear modes (1000 directions x 3 modes)
   amm_transmission.npz  IsotropicAMMInterface (Ge -> Al) transmission of L and transverse
                         phonons at 400 incidence angles
   kaplan_surrogate.npz  KaplanSurrogateLUT (default Al film, seed 1337) lookups at 2000 energies
@@ -25,7 +26,7 @@ compiled from its own headers by `make -C oracle ref`) and stores compact record
                         201,898 nodes): field_at and potential_at at 4096 points in the cylinder
 
 Usage: python tests/golden/make_golden.py [--only NAME,...]   (needs the reference build;
-       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist, amm, kaplan, mask or mesh)
+       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist, kin, amm, kaplan, mask or mesh)
 """
 from __future__ import annotations
 
@@ -61,6 +62,8 @@ PLAN = {
     "c0a": (16, 2000),
     "tpd": (8, 203),
     "tpe": (8, 203),
+    "c0x": (8, 1000),
+    "c0b": (8, 2000),
 }
 
 
@@ -94,6 +97,11 @@ def main() -> None:
             rec = np.fromfile(path, dtype=np.dtype([("x", "<f8"), ("y", "<f8"), ("qet", "<i4"), ("grid", "<i4")]))
             np.savez_compressed(os.path.join(HERE, "mask_channels.npz"), x=rec["x"], y=rec["y"], qet=rec["qet"],
                                 grid=rec["grid"])
+        if want("kin"):
+            path = os.path.join(tmp, "kin.bin")
+            subprocess.run([REF, "kin", "1000", path], check=True)
+            rec = np.fromfile(path, dtype=np.float64).reshape(2, 1000, 3, 4)
+            np.savez_compressed(os.path.join(HERE, "kinematics_modes.npz"), exact=rec[0], bilinear=rec[1])
         if want("amm"):
             path = os.path.join(tmp, "amm.bin")
             subprocess.run([REF, "amm", "400", path], check=True)

@@ -40,6 +40,17 @@ def detector_for(workload: str):
     return det
 
 
+def lattice_for(workload: str, default_lattice):
+    """The lattice of a fixture workload: the shared Ge lattice, or a Ge lattice in the
+    Exact (c0x) or Bilinear (c0b) kinematics mode."""
+    import cmpmc_b200 as cm
+    if workload not in ("c0x", "c0b"):
+        return default_lattice
+    lat = cm.CrystalLattice(cm.materials.Germanium())
+    lat.set_kinematics_mode(cm.CrystalLattice.Exact if workload == "c0x" else cm.CrystalLattice.Bilinear)
+    return lat
+
+
 _MESH = []
 
 
@@ -51,7 +62,7 @@ def recoil_mesh():
     return _MESH[0]
 
 
-WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13, "c0m": 42, "tpm": 77, "c0a": 42, "tpd": 77, "tpe": 77}
+WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13, "c0m": 42, "tpm": 77, "c0a": 42, "tpd": 77, "tpe": 77, "c0x": 42, "c0b": 42}
 
 
 def workload_of(name: str):
@@ -61,7 +72,8 @@ def workload_of(name: str):
             "tpl": cm.workloads.test_parallel, "c3s": cm.workloads.recoil_light,
             "c0m": cm.workloads.single_l_origin, "tpm": cm.workloads.test_parallel,
             "c0a": cm.workloads.single_l_origin, "tpd": cm.workloads.test_parallel,
-            "tpe": cm.workloads.test_parallel}[name]
+            "tpe": cm.workloads.test_parallel, "c0x": cm.workloads.single_l_origin,
+            "c0b": cm.workloads.single_l_origin}[name]
 
 
 def has_gpu() -> bool:

@@ -14,7 +14,7 @@ last-bit difference into a different trajectory on some events).
 import numpy as np
 import pytest
 
-from tests.helpers import WORKLOAD_SEED, detector_for, golden, workload_of
+from tests.helpers import WORKLOAD_SEED, detector_for, golden, lattice_for, workload_of
 from tests.golden.records import FP_STATS, compare_summaries, summarize
 
 pytestmark = pytest.mark.gpu
@@ -24,7 +24,7 @@ REL_TOL = 1e-9
 
 def _run(ge_lattice, wl, n, keep_hits=True, want_event_stats=True, packed=None):
     import cmpmc_b200 as cm
-    eng = cm.SimulationEngine(ge_lattice, detector_for(wl))
+    eng = cm.SimulationEngine(lattice_for(wl, ge_lattice), detector_for(wl))
     opt = cm.RunOptions(seed=WORKLOAD_SEED[wl], keep_hits=keep_hits, want_event_stats=want_event_stats)
     if packed is None:
         return eng, cm.run_events(eng, n, workload_of(wl), opt)
@@ -41,7 +41,7 @@ def _device_summary(ge_lattice, wl, n):
     return _RESULTS[(wl, n)]
 
 
-@pytest.mark.parametrize("wl", ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe"])
+@pytest.mark.parametrize("wl", ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b"])
 def test_event_parity_correctly_rounded_reference(ge_lattice, wl):
     ref = golden(f"{wl}_cr_summary.npz")["summary"]
     got = _device_summary(ge_lattice, wl, len(ref))
@@ -53,7 +53,7 @@ def test_event_parity_correctly_rounded_reference(ge_lattice, wl):
         assert np.all(np.abs(a - b) <= 1e-12 * np.maximum(np.abs(a), 1e-300) + 1e-300), name
 
 
-@pytest.mark.parametrize("wl", ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe"])
+@pytest.mark.parametrize("wl", ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b"])
 def test_event_parity_glibc_reference(ge_lattice, wl):
     ref = golden(f"{wl}_summary.npz")["summary"]
     cr = golden(f"{wl}_cr_summary.npz")
@@ -66,7 +66,7 @@ def test_event_parity_glibc_reference(ge_lattice, wl):
         assert cmp["frac"] >= 0.985
 
 
-@pytest.mark.parametrize("wl", ["c0", "tp", "tpl", "c2", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe"])
+@pytest.mark.parametrize("wl", ["c0", "tp", "tpl", "c2", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b"])
 def test_full_hit_records_match(ge_lattice, wl):
     """Hit-by-hit comparison from the reference's own initial stacks and Rng states."""
     import cmpmc_b200 as cm

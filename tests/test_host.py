@@ -8,7 +8,7 @@ import re
 import numpy as np
 import pytest
 
-from tests.helpers import GOLDEN, ROOT, WORKLOAD_SEED, detector_for, golden, workload_of
+from tests.helpers import GOLDEN, ROOT, WORKLOAD_SEED, detector_for, golden, lattice_for, workload_of
 
 
 def test_library_exports_every_declared_symbol(lib):
@@ -218,6 +218,30 @@ def test_amm_transmission_matches_reference():
         assert a.transmission(False, c) == g["transverse"][i], i
     # flux conservation holds in the reference's model: transmission within [0, 1]
     assert 0.0 <= g["longitudinal"].min() and g["transverse"].max() <= 1.0
+
+
+def test_kinematics_modes_match_reference():
+    """CrystalLattice::map_k_to_vg in the Exact (Cardano per call) and Bilinear (181 x 361
+    table) modes: group-velocity directions and magnitudes of 1000 directions x 3 modes equal
+    the reference's; the native generator's make_track follows the lattice's mode."""
+    import cmpmc_b200 as cm
+    g = golden("kinematics_modes.npz")
+    rng = cm.Rng.for_stream(21, 0)
+    ks = [rng.isotropic_dir() for _ in range(1000)]
+    for mode, key in ((cm.CrystalLattice.Exact, "exact"), (cm.CrystalLattice.Bilinear, "bilinear")):
+        lat = cm.CrystalLattice(cm.materials.Germanium())
+        lat.set_kinematics_mode(mode)
+        assert lat.kinematics_mode() == mode
+        for i, k in enumerate(ks):
+            for m in range(3):
+                d, mag = lat.map_k_to_vg(m, k)
+                assert tuple(d) + (mag,) == tuple(g[key][i, m]), (key, i, m)
+    for wl in ("c0x", "c0b"):
+        full = golden(f"{wl}_full.npz")
+        lat = lattice_for(wl, None)
+        eng = cm.SimulationEngine(lat, detector_for(wl))
+        ev = eng.generate(workload_of(wl), len(full["rng_state"]), WORKLOAD_SEED[wl])
+        assert ev.phonons.tobytes() == full["phonons"].tobytes(), wl
 
 
 def test_python_generator_matches_native(ge_lattice):
