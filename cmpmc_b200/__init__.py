@@ -8,14 +8,14 @@ from .api import (AluminumFilm, CmpmcError, ElectrodePad, ElectrodePatternMask, 
                   EventInput, ExcitationType, IsotropicAMMInterface, IsotropicMedium, KaplanFilm,
                   KaplanSurrogateLUT, PackedEvents, PhononMode, Rng, RunOptions, RunResult,
                   SimStats, SimulationEngine, SuperconductorFilmConfig, SurfaceId, SurfaceProperty,
-                  TriLinearMesh3D, UniformElectricField, UnvalidatedModuleError, Workload, materials, run_events, units, workloads)
+                  TriLinearMesh3D, BiLinearMesh2D, UniformElectricField, UnvalidatedModuleError, Workload, materials, run_events, units, workloads)
 from .adjoint import AdjointResult, HistogramAdjoint, THETA_NAMES, default_theta
 
 __all__ = [
     "AdjointResult", "AluminumFilm", "CmpmcError", "ElectrodePad", "ElectrodePatternMask", "CrystalConfig", "CrystalLattice", "CylinderSolid", "DetectorModel", "EventInput",
     "ExcitationType", "IsotropicAMMInterface", "IsotropicMedium", "KaplanFilm",
     "KaplanSurrogateLUT", "PackedEvents", "PhononMode", "Rng", "RunOptions", "RunResult", "SimStats",
-    "SimulationEngine", "SuperconductorFilmConfig", "SurfaceId", "SurfaceProperty", "TriLinearMesh3D",
+    "SimulationEngine", "SuperconductorFilmConfig", "SurfaceId", "SurfaceProperty", "TriLinearMesh3D", "BiLinearMesh2D",
     "UniformElectricField",
     "UnvalidatedModuleError", "Workload", "materials", "run_events", "units", "workloads", "HistogramAdjoint",
     "THETA_NAMES", "default_theta",

@@ -152,6 +152,9 @@ class AdjointOutC(C.Structure):
 # double (*)(const double p[3], void* user): node potential of cmpmc_mesh_build_cartesian
 POTENTIAL_FN = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p)
 
+# double (*)(double u, double v, void* user): node potential of cmpmc_mesh2d_build_grid
+POTENTIAL2D_FN = C.CFUNCTYPE(C.c_double, C.c_double, C.c_double, C.c_void_p)
+
 TUNE_MAX = 16
 
 
@@ -207,6 +210,14 @@ _SIG = {
     "cmpmc_mesh_field_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
     "cmpmc_mesh_potential_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
     "cmpmc_gpu_set_mesh": (_i32, [C.c_void_p, C.c_void_p]),
+    "cmpmc_mesh2d_create": (_i32, [C.c_void_p, C.c_void_p, _u64, C.c_void_p, _u64, _i32, C.POINTER(C.c_void_p)]),
+    "cmpmc_mesh2d_build_grid": (_i32, [_f64, _f64, _f64, _f64, _i32, _i32, C.c_void_p, C.c_void_p, _i32,
+                                       C.POINTER(C.c_void_p)]),
+    "cmpmc_mesh2d_destroy": (None, [C.c_void_p]),
+    "cmpmc_mesh2d_info": (_i32, [C.c_void_p, C.POINTER(_u64), C.POINTER(_u64)]),
+    "cmpmc_mesh2d_field_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
+    "cmpmc_mesh2d_potential_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
+    "cmpmc_gpu_set_mesh2d": (_i32, [C.c_void_p, C.c_void_p]),
     "cmpmc_gpu_configure_queue": (_i32, [C.c_void_p, _u64]),
     "cmpmc_gpu_configure_graph": (_i32, [C.c_void_p, _i32]),
     "cmpmc_gpu_configure_phases": (_i32, [C.c_void_p, _u32]),

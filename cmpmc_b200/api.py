@@ -623,12 +623,89 @@ class TriLinearMesh3D:
         return self.field_at(p)
 
 
+class BiLinearMesh2D:
+    """BiLinearMesh2D (geometry/mesh_field.hpp:347-582): a triangle mesh in (r, z) for an
+    axisymmetric field (rotated back around the z axis) or in (x, y) for a planar one, the
+    field constant inside each triangle. Built on the host by the native library with the
+    reference's arithmetic; attached to a DetectorModel as mesh_field_2d (and no 3D mesh)
+    it is copied to the device and walked there by every charge step."""
+
+    def __init__(self, vertices=None, potentials=None, triangles=None, axisymmetric_rz: bool = True,
+                 _handle=None):
+        self._lib = _ffi.load()
+        self._hint = C.c_int32(0)
+        if _handle is not None:
+            self._h = _handle
+            return
+        x = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 2)
+        v = np.ascontiguousarray(potentials, dtype=np.float64).reshape(-1)
+        t = np.ascontiguousarray(triangles, dtype=np.int32).reshape(-1, 3)
+        if len(v) != len(x):
+            raise ValueError("one potential per vertex")
+        h = C.c_void_p()
+        _check(self._lib.cmpmc_mesh2d_create(x.ctypes.data, v.ctypes.data, len(x), t.ctypes.data, len(t),
+                                             int(bool(axisymmetric_rz)), C.byref(h)), what="mesh")
+        self._h = h
+
+    @staticmethod
+    def build_grid(u_min: float, u_max: float, v_min: float, v_max: float, nu: int, nv: int,
+                   potential_fn: Callable, axisymmetric_rz: bool = True) -> "BiLinearMesh2D":
+        """nu x nv cells of two triangles each (mesh_field.hpp:438-479); potential_fn(u, v)
+        gives the node potential in volts."""
+        lib = _ffi.load()
+        cb = _ffi.POTENTIAL2D_FN(lambda u, v, _u: float(potential_fn(u, v)))
+        h = C.c_void_p()
+        _check(lib.cmpmc_mesh2d_build_grid(float(u_min), float(u_max), float(v_min), float(v_max), int(nu), int(nv),
+                                           cb, None, int(bool(axisymmetric_rz)), C.byref(h)), what="mesh")
+        return BiLinearMesh2D(_handle=h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.cmpmc_mesh2d_destroy(h)
+            self._h = None
+
+    def _info(self):
+        nv, nt = C.c_uint64(), C.c_uint64()
+        _check(self._lib.cmpmc_mesh2d_info(self._h, C.byref(nv), C.byref(nt)))
+        return nv.value, nt.value
+
+    def num_vertices(self) -> int:
+        return self._info()[0]
+
+    def num_triangles(self) -> int:
+        return self._info()[1]
+
+    def empty(self) -> bool:
+        return self.num_triangles() == 0
+
+    def field_at(self, p, tri_hint: Optional[C.c_int32] = None):
+        """E(p) in V/m from the containing triangle (zero outside); the walk starts from and
+        updates tri_hint (a ctypes int32), or the mesh's own hint (as at())."""
+        hint = self._hint if tri_hint is None else tri_hint
+        q = (C.c_double * 3)(*p)
+        e = (C.c_double * 3)()
+        _check(self._lib.cmpmc_mesh2d_field_at(self._h, q, C.byref(hint), e))
+        return (e[0], e[1], e[2])
+
+    def potential_at(self, p, tri_hint: Optional[C.c_int32] = None) -> float:
+        hint = self._hint if tri_hint is None else tri_hint
+        q = (C.c_double * 3)(*p)
+        v = C.c_double()
+        _check(self._lib.cmpmc_mesh2d_potential_at(self._h, q, C.byref(hint), C.byref(v)))
+        return v.value
+
+    def at(self, p):
+        return self.field_at(p)
+
+
 @dataclass
 class DetectorModel:
     """DetectorModel (transport/engine.hpp:96-156)."""
     solid: CylinderSolid = field(default_factory=CylinderSolid)
     e_field: UniformElectricField = field(default_factory=lambda: UniformElectricField.from_bias(0.0, 2.54 * units.cm))
     mesh_field_3d: Optional[TriLinearMesh3D] = None
+    mesh_field_2d: Optional[BiLinearMesh2D] = None
     surfaces: list = field(default_factory=_default_surfaces)
     max_bounces: int = 5000
     min_phonon_eV: float = 10.0 * units.ueV
@@ -851,6 +928,8 @@ class SimulationEngine:
             self._ctx[device] = h
             if self.detector.mesh_field_3d is not None:
                 _check(self._lib.cmpmc_gpu_set_mesh(h, self.detector.mesh_field_3d._h), h)
+            elif self.detector.mesh_field_2d is not None:
+                _check(self._lib.cmpmc_gpu_set_mesh2d(h, self.detector.mesh_field_2d._h), h)
             for i, sp in enumerate(self.detector.surfaces):
                 if sp.electrode_mask is not None and not sp.electrode_mask.empty():
                     m = sp.electrode_mask

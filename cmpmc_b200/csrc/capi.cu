@@ -98,6 +98,7 @@ struct cmpmc_gpu_ctx {
     DevBuf unit_event, ev_offsets, ev_stats2, partials;  // batched form: unit -> event map, event offsets / stats
     DevBuf adj_prim, adj_hist, adj_w, adj_partials, adj_sums;  // adjoint: per-primary rows, bins, reductions
     DevBuf mesh32;                                      // FP32 mesh records (batched charge form)
+    DevBuf mesh2, mesh2_32;                             // 2D field mesh records, FP64 and FP32
     DevBuf pads[3];                                     // electrode masks of the three surfaces
     DevBuf lut[3];                                      // Kaplan surrogate tables of the films
     bool lut_ready = false;
@@ -634,7 +635,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->kin, &ctx->film_a, &ctx->queue_b, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
+    for (DevBuf* b : {&ctx->kin, &ctx->film_a, &ctx->queue_b, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->mesh2, &ctx->mesh2_32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
                       &ctx->ccounters, &ctx->carrier_event, &ctx->cursor, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
@@ -843,6 +844,37 @@ int cmpmc_gpu_set_mesh(cmpmc_gpu_ctx* ctx, const cmpmc_mesh* mesh) {
     ctx->D.mesh.n_tets = static_cast<int32_t>(mesh->rec.size());
     ctx->D.mesh32.tet = ctx->mesh32.as<MeshTet32>();
     ctx->D.mesh32.n_tets = static_cast<int32_t>(mesh->rec.size());
+    return CMPMC_OK;
+}
+
+int cmpmc_gpu_set_mesh2d(cmpmc_gpu_ctx* ctx, const cmpmc_mesh2d* mesh) {
+    if (!ctx) return CMPMC_ERR_INVALID;
+    ctx->last_status = CMPMC_OK;
+    ctx->last_error.clear();
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    ctx->D.mesh2 = MeshView2{nullptr, 0, 1};
+    ctx->D.mesh2_32 = MeshView2_32{nullptr, 0, 1};
+    if (!mesh || mesh->rec.empty()) return CMPMC_OK;
+    const size_t n = mesh->rec.size();
+    CK(ctx->mesh2.ensure(n * sizeof(MeshTri)), "alloc 2D mesh");
+    CK(cudaMemcpy(ctx->mesh2.p, mesh->rec.data(), n * sizeof(MeshTri), cudaMemcpyHostToDevice), "copy 2D mesh");
+    std::vector<MeshTri32> r32(n);
+    for (size_t i = 0; i < n; ++i) {
+        const MeshTri& t = mesh->rec[i];
+        MeshTri32& o = r32[i];
+        for (int j = 0; j < 4; ++j) o.tinv[j] = static_cast<float>(t.tinv[j]);
+        for (int j = 0; j < 2; ++j) {
+            o.x2[j] = static_cast<float>(t.x2[j]);
+            o.e[j] = static_cast<float>(t.e[j]);
+        }
+        for (int j = 0; j < 3; ++j) o.nb[j] = t.nb[j];
+        o.pad = 0;
+    }
+    CK(ctx->mesh2_32.ensure(n * sizeof(MeshTri32)), "alloc FP32 2D mesh");
+    CK(cudaMemcpy(ctx->mesh2_32.p, r32.data(), n * sizeof(MeshTri32), cudaMemcpyHostToDevice), "copy FP32 2D mesh");
+    ctx->D.mesh2 = MeshView2{ctx->mesh2.as<MeshTri>(), static_cast<int32_t>(n), mesh->axisym};
+    ctx->D.mesh2_32 = MeshView2_32{ctx->mesh2_32.as<MeshTri32>(), static_cast<int32_t>(n), mesh->axisym};
     return CMPMC_OK;
 }
 

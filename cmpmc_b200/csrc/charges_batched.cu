@@ -70,6 +70,7 @@ struct FCDet {
     float luke_prob, luke_wt;
     double muF;
     MeshView32 mesh;
+    MeshView2_32 mesh2;
 };
 
 struct FCharge {
@@ -200,6 +201,39 @@ __device__ __forceinline__ F3 mesh_field_f(const MeshView32& m, F3 p, int32_t& h
         if (mn >= kMeshTol) {
             const float4 e = __ldg(reinterpret_cast<const float4*>(&t) + 3);  // e, nb0
             return f3(e.x, e.y, e.z);
+        }
+        const int32_t next = __ldg(&t.nb[mi]);
+        if (next < 0) break;
+        hint = next;
+    }
+    return f3(0.0f, 0.0f, 0.0f);
+}
+
+// FP32 edge walk (BiLinearMesh2D::find_triangle / field_at, mesh_field.hpp:376-430) with
+// the same FP32 tolerance; the axisymmetric field is rotated back around the z axis
+__device__ __forceinline__ F3 mesh2_field_f(const MeshView2_32& m, F3 p, int32_t& hint) {
+    float u = p.x, v = p.y;
+    if (m.axisym) {
+        u = sqrtf(p.x * p.x + p.y * p.y);
+        v = p.z;
+    }
+    if (hint < 0 || hint >= m.n_tris) hint = m.n_tris / 2;
+    for (int step = 0; step < kMeshMaxSteps; ++step) {
+        const MeshTri32& t = m.tri[hint];
+        const float4 a = __ldg(reinterpret_cast<const float4*>(&t) + 0);  // tinv
+        const float4 b = __ldg(reinterpret_cast<const float4*>(&t) + 1);  // x2, e
+        const float du = u - b.x, dv = v - b.y;
+        const float b0 = a.x * du + a.y * dv;
+        const float b1 = a.z * du + a.w * dv;
+        const float b2 = 1.0f - b0 - b1;
+        float mn = b0;
+        int mi = 0;
+        if (b1 < mn) { mn = b1; mi = 1; }
+        if (b2 < mn) { mn = b2; mi = 2; }
+        if (mn >= kMeshTol) {
+            if (!m.axisym) return f3(b.z, b.w, 0.0f);
+            if (u > 1e-15f) return f3(b.z * (p.x / u), b.z * (p.y / u), b.w);
+            return f3(0.0f, 0.0f, b.w);
         }
         const int32_t next = __ldg(&t.nb[mi]);
         if (next < 0) break;
@@ -364,7 +398,8 @@ __global__ void __launch_bounds__(128, 4) k_charges_fp32(const __grid_constant__
         ++st.steps;
         dirty = true;
         const float q_sign = (c.type == 1) ? -1.0f : 1.0f;
-        const F3 E = D.mesh.tet ? mesh_field_f(D.mesh, c.pos, k.hint) : D.e_field;
+        const F3 E = D.mesh.tet ? mesh_field_f(D.mesh, c.pos, k.hint)
+                                : (D.mesh2.tri ? mesh2_field_f(D.mesh2, c.pos, k.hint) : D.e_field);
         if (E.x != E_last.x || E.y != E_last.y || E.z != E_last.z) {
             E_last = E;
             iv_last = iv_rate_of_field(L, E);
@@ -679,6 +714,7 @@ FCDet make_fcdet(const Detector& D, const MeshView32& mesh, const Lattice& L) {
     f.luke_wt = (lp > 0.0) ? static_cast<float>(1.0 / lp) : 0.0f;
     f.muF = (D.fermi_level_above_Ev_eV >= 0.0) ? D.fermi_level_above_Ev_eV : 0.5 * L.bandgap;
     f.mesh = mesh;
+    f.mesh2 = D.mesh2_32;
     return f;
 }
 

@@ -35,6 +35,15 @@ struct cmpmc_mesh {
     std::vector<cmpmc_gpu::MeshTet> rec;     // [n_tets]
 };
 
+// BiLinearMesh2D (geometry/mesh_field.hpp:347-582)
+struct cmpmc_mesh2d {
+    std::vector<double> X;                   // [n][2] (u, v)
+    std::vector<double> V;
+    std::vector<std::array<int32_t, 3>> tris;
+    std::vector<cmpmc_gpu::MeshTri> rec;
+    int axisym = 1;
+};
+
 namespace cmpmc_gpu {
 
 // Checks a detector / crystal pair against what the device path supports and applies the

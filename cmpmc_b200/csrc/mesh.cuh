@@ -95,4 +95,88 @@ CMPMC_HD V3 mesh_field(const MeshView& m, V3 p, int32_t& hint) {
     return v3(t.e[0], t.e[1], t.e[2]);
 }
 
+// ---- BiLinearMesh2D (geometry/mesh_field.hpp:347-582) -----------------------------------
+// A triangle mesh in (u, v) = (r, z) for an axisymmetric field, or (x, y) for a planar one.
+// One 80-byte record per triangle: the inverse edge matrix, the third vertex, the constant
+// field (E_u, E_v) inside it and the three edge neighbours.
+struct alignas(16) MeshTri {
+    double tinv[4];  // row-major 2x2 inverse of [x0 - x2, x1 - x2] (columns)
+    double x2[2];
+    double e[2];     // (E_u, E_v) = -grad V
+    int32_t nb[3];   // neighbour across the edge opposite vertex i; -1 on the boundary
+    int32_t pad;
+};
+static_assert(sizeof(MeshTri) == 80, "2D mesh record layout");
+
+struct MeshView2 {
+    const MeshTri* tri;  // nullptr: no 2D mesh
+    int32_t n_tris;
+    int32_t axisym;      // 1: (r, z) projection, field rotated back into (x, y, z)
+};
+
+// BiLinearMesh2D::project (mesh_field.hpp:488-493)
+CMPMC_HD void mesh2_project(const MeshView2& m, V3 p, double& u, double& v) {
+    if (m.axisym) {
+        u = m_hypot(p.x, p.y);
+        v = p.z;
+    } else {
+        u = p.x;
+        v = p.y;
+    }
+}
+
+// BiLinearMesh2D::find_triangle (mesh_field.hpp:376-405)
+CMPMC_HD bool mesh2_find(const MeshView2& m, double u, double v, int32_t& hint, double b[3]) {
+    if (m.n_tris <= 0) return false;
+    if (hint < 0 || hint >= m.n_tris) hint = m.n_tris / 2;
+    const int64_t max_steps = static_cast<int64_t>(m.n_tris) + 4;
+    for (int64_t step = 0; step < max_steps; ++step) {
+        const MeshTri& t = m.tri[hint];
+        const double du = u - t.x2[0];
+        const double dv = v - t.x2[1];
+        b[0] = t.tinv[0] * du + t.tinv[1] * dv;
+        b[1] = t.tinv[2] * du + t.tinv[3] * dv;
+        b[2] = 1.0 - b[0] - b[1];
+        double min_b = b[0];
+        int min_i = 0;
+        for (int i = 1; i < 3; ++i)
+            if (b[i] < min_b) {
+                min_b = b[i];
+                min_i = i;
+            }
+        if (min_b >= -1e-10) return true;
+        const int32_t next = t.nb[min_i];
+        if (next < 0) return false;
+        hint = next;
+    }
+    return false;
+}
+
+// BiLinearMesh2D::field_at (mesh_field.hpp:415-430)
+CMPMC_HD V3 mesh2_field(const MeshView2& m, V3 p, int32_t& hint) {
+    double u, v, b[3];
+    mesh2_project(m, p, u, v);
+    if (!mesh2_find(m, u, v, hint, b)) return v3(0.0, 0.0, 0.0);
+    const MeshTri& t = m.tri[hint];
+    if (!m.axisym) return v3(t.e[0], t.e[1], 0.0);
+    if (u > 1e-15) return v3(t.e[0] * (p.x / u), t.e[0] * (p.y / u), t.e[1]);
+    return v3(0.0, 0.0, t.e[1]);
+}
+
+// The 2D mesh in FP32 for the batched charge form: 48 bytes per triangle.
+struct alignas(16) MeshTri32 {
+    float tinv[4];
+    float x2[2];
+    float e[2];
+    int32_t nb[3];
+    int32_t pad;
+};
+static_assert(sizeof(MeshTri32) == 48, "FP32 2D mesh record layout");
+
+struct MeshView2_32 {
+    const MeshTri32* tri;  // nullptr: no 2D mesh
+    int32_t n_tris;
+    int32_t axisym;
+};
+
 }  // namespace cmpmc_gpu

@@ -119,9 +119,179 @@ MeshView host_view(const cmpmc_mesh* m) {
     return v;
 }
 
+struct Edge {
+    std::array<int32_t, 2> nodes;
+    int32_t tri;
+    int32_t slot;
+    bool operator<(const Edge& o) const {
+        if (nodes != o.nodes) return nodes < o.nodes;
+        return tri < o.tri;
+    }
+};
+
+// BiLinearMesh2D::fill_neighbors / fill_tinv_and_grad (mesh_field.hpp:515-580)
+int finish_mesh2d(cmpmc_mesh2d* m) {
+    const size_t nt = m->tris.size(), nv = m->V.size();
+    for (auto& t : m->tris) {
+        std::sort(t.begin(), t.end());
+        for (int i = 0; i < 3; ++i)
+            if (t[i] < 0 || static_cast<size_t>(t[i]) >= nv) return CMPMC_ERR_INVALID;
+    }
+    m->rec.assign(nt, MeshTri{});
+    std::vector<Edge> e;
+    e.reserve(nt * 3);
+    for (size_t it = 0; it < nt; ++it) {
+        const auto& t = m->tris[it];
+        const int32_t id = static_cast<int32_t>(it);
+        e.push_back({{t[1], t[2]}, id, 0});
+        e.push_back({{t[0], t[2]}, id, 1});
+        e.push_back({{t[0], t[1]}, id, 2});
+    }
+    std::sort(e.begin(), e.end());
+    for (size_t it = 0; it < nt; ++it)
+        for (int i = 0; i < 3; ++i) m->rec[it].nb[i] = -1;
+    for (size_t i = 0; i + 1 < e.size(); ++i)
+        if (e[i].nodes == e[i + 1].nodes) {
+            m->rec[e[i].tri].nb[e[i].slot] = e[i + 1].tri;
+            m->rec[e[i + 1].tri].nb[e[i + 1].slot] = e[i].tri;
+            ++i;
+        }
+    for (size_t it = 0; it < nt; ++it) {
+        const auto& t = m->tris[it];
+        MeshTri& r = m->rec[it];
+        const double* x2 = &m->X[2 * static_cast<size_t>(t[2])];
+        r.x2[0] = x2[0];
+        r.x2[1] = x2[1];
+        const double a = m->X[2 * static_cast<size_t>(t[0])] - x2[0];
+        const double b = m->X[2 * static_cast<size_t>(t[1])] - x2[0];
+        const double c = m->X[2 * static_cast<size_t>(t[0]) + 1] - x2[1];
+        const double d = m->X[2 * static_cast<size_t>(t[1]) + 1] - x2[1];
+        const double det = a * d - b * c;
+        if (std::fabs(det) <= 1e-30) {
+            std::memset(r.tinv, 0, sizeof(r.tinv));
+            r.e[0] = r.e[1] = 0.0;
+            continue;
+        }
+        const double inv_det = 1.0 / det;
+        r.tinv[0] = d * inv_det;
+        r.tinv[1] = -b * inv_det;
+        r.tinv[2] = -c * inv_det;
+        r.tinv[3] = a * inv_det;
+        const double dv0 = m->V[t[0]] - m->V[t[2]];
+        const double dv1 = m->V[t[1]] - m->V[t[2]];
+        r.e[0] = -(r.tinv[0] * dv0 + r.tinv[2] * dv1);
+        r.e[1] = -(r.tinv[1] * dv0 + r.tinv[3] * dv1);
+    }
+    return CMPMC_OK;
+}
+
+MeshView2 host_view2(const cmpmc_mesh2d* m) {
+    MeshView2 v;
+    v.tri = m->rec.data();
+    v.n_tris = static_cast<int32_t>(m->rec.size());
+    v.axisym = m->axisym;
+    return v;
+}
+
 }  // namespace
 
 extern "C" {
+
+int cmpmc_mesh2d_create(const double* uv, const double* potentials, uint64_t n_vertices, const int32_t* tris,
+                        uint64_t n_tris, int axisymmetric, cmpmc_mesh2d** out) {
+    if (!out) return CMPMC_ERR_INVALID;
+    *out = nullptr;
+    if ((n_vertices && (!uv || !potentials)) || (n_tris && !tris) || n_tris > 0x7ffffffbull ||
+        n_vertices > 0x7fffffffull)
+        return CMPMC_ERR_INVALID;
+    cmpmc_mesh2d* m = new (std::nothrow) cmpmc_mesh2d();
+    if (!m) return CMPMC_ERR_INVALID;
+    m->X.assign(uv, uv + 2 * n_vertices);
+    m->V.assign(potentials, potentials + n_vertices);
+    m->tris.resize(n_tris);
+    for (uint64_t i = 0; i < n_tris; ++i)
+        for (int j = 0; j < 3; ++j) m->tris[i][j] = tris[3 * i + j];
+    m->axisym = axisymmetric ? 1 : 0;
+    const int st = finish_mesh2d(m);
+    if (st != CMPMC_OK) {
+        delete m;
+        return st;
+    }
+    *out = m;
+    return CMPMC_OK;
+}
+
+int cmpmc_mesh2d_build_grid(double u_min, double u_max, double v_min, double v_max, int nu, int nv,
+                            cmpmc_potential2d_fn potential, void* user, int axisymmetric, cmpmc_mesh2d** out) {
+    if (!out || !potential) return CMPMC_ERR_INVALID;
+    *out = nullptr;
+    nu = std::max(1, nu);
+    nv = std::max(1, nv);
+    const int64_t vu = nu + 1, vv = nv + 1;
+    if (vu * vv > 0x7fffffffll || 2ll * nu * nv > 0x7ffffffbll) return CMPMC_ERR_INVALID;
+    cmpmc_mesh2d* m = new (std::nothrow) cmpmc_mesh2d();
+    if (!m) return CMPMC_ERR_INVALID;
+    m->X.resize(2 * static_cast<size_t>(vu * vv));
+    m->V.resize(static_cast<size_t>(vu * vv));
+    for (int i = 0; i <= nu; ++i) {
+        const double u = u_min + (u_max - u_min) * (static_cast<double>(i) / nu);
+        for (int j = 0; j <= nv; ++j) {
+            const double v = v_min + (v_max - v_min) * (static_cast<double>(j) / nv);
+            const size_t id = static_cast<size_t>(i * vv + j);
+            m->X[2 * id] = u;
+            m->X[2 * id + 1] = v;
+            m->V[id] = potential(u, v, user);
+        }
+    }
+    m->tris.reserve(2 * static_cast<size_t>(nu) * nv);
+    for (int i = 0; i < nu; ++i)
+        for (int j = 0; j < nv; ++j) {
+            const int32_t v00 = static_cast<int32_t>(i * vv + j), v10 = static_cast<int32_t>((i + 1) * vv + j),
+                          v01 = static_cast<int32_t>(i * vv + j + 1), v11 = static_cast<int32_t>((i + 1) * vv + j + 1);
+            m->tris.push_back({v00, v10, v11});
+            m->tris.push_back({v00, v01, v11});
+        }
+    m->axisym = axisymmetric ? 1 : 0;
+    const int st = finish_mesh2d(m);
+    if (st != CMPMC_OK) {
+        delete m;
+        return st;
+    }
+    *out = m;
+    return CMPMC_OK;
+}
+
+void cmpmc_mesh2d_destroy(cmpmc_mesh2d* m) { delete m; }
+
+int cmpmc_mesh2d_info(const cmpmc_mesh2d* m, uint64_t* n_vertices, uint64_t* n_tris) {
+    if (!m) return CMPMC_ERR_INVALID;
+    if (n_vertices) *n_vertices = m->V.size();
+    if (n_tris) *n_tris = m->rec.size();
+    return CMPMC_OK;
+}
+
+int cmpmc_mesh2d_field_at(const cmpmc_mesh2d* m, const double p[3], int32_t* hint, double E[3]) {
+    if (!m || !p || !hint || !E) return CMPMC_ERR_INVALID;
+    const V3 e = mesh2_field(host_view2(m), v3(p[0], p[1], p[2]), *hint);
+    E[0] = e.x;
+    E[1] = e.y;
+    E[2] = e.z;
+    return CMPMC_OK;
+}
+
+int cmpmc_mesh2d_potential_at(const cmpmc_mesh2d* m, const double p[3], int32_t* hint, double* V) {
+    if (!m || !p || !hint || !V) return CMPMC_ERR_INVALID;
+    const MeshView2 v = host_view2(m);
+    double u, w, b[3];
+    mesh2_project(v, v3(p[0], p[1], p[2]), u, w);
+    if (!mesh2_find(v, u, w, *hint, b)) {
+        *V = 0.0;
+        return CMPMC_OK;
+    }
+    const auto& t = m->tris[*hint];
+    *V = b[0] * m->V[t[0]] + b[1] * m->V[t[1]] + b[2] * m->V[t[2]];
+    return CMPMC_OK;
+}
 
 int cmpmc_mesh_create(const double* vertices, const double* potentials, uint64_t n_vertices, const int32_t* tets,
                       uint64_t n_tets, double v_min_clamp, double v_max_clamp, cmpmc_mesh** out) {

@@ -31,6 +31,8 @@ struct Detector {
     double electrode_seed_max_gap;
     MeshView mesh;      // DetectorModel::mesh_field_3d on the device (tet == nullptr: uniform field)
     MeshView32 mesh32;  // the same mesh in FP32 (batched charge form)
+    MeshView2 mesh2;       // DetectorModel::mesh_field_2d, used when there is no 3D mesh
+    MeshView2_32 mesh2_32;  // the 2D mesh in FP32 (batched charge form)
 };
 
 // Phonon state held in registers (PhononTrack, track.hpp:62-72)

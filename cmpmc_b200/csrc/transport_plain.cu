@@ -45,6 +45,8 @@ struct PlainCtx {
     V3 field_value;
     MeshView mesh;
     int32_t tet_hint;  // walk hint of this device thread, kept across carriers and events
+    MeshView2 mesh2;
+    int32_t tri_hint;  // the same for the 2D mesh
     unsigned err;
     KBuf refl;
     double* kwork;
@@ -98,6 +100,7 @@ struct PlainCtx {
     // DetectorModel::electric_field_at (engine.hpp:151-155)
     __device__ V3 field(V3 p, Charge&) {
         if (mesh.tet) return mesh_field(mesh, p, tet_hint);
+        if (mesh2.tri) return mesh2_field(mesh2, p, tri_hint);
         return field_value;
     }
     __device__ void hit(const Hit& h, int channel) {
@@ -140,6 +143,8 @@ __global__ void __launch_bounds__(128) k_plain_fp64(const Lattice L, const Detec
     ctx.field_value = D.e_field;
     ctx.mesh = D.mesh;
     ctx.tet_hint = 0;
+    ctx.mesh2 = D.mesh2;
+    ctx.tri_hint = 0;
     for (;;) {
         const unsigned long long ev = atomicAdd(a.next_work, 1ull);
         if (ev >= a.n_events) break;

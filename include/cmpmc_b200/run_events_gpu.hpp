@@ -15,10 +15,12 @@
 // surfaces' ElectrodePatternMask pads. A TriLinearMesh3D field keeps its nodes private in
 // the reference, so a detector with mesh_field_3d needs the same mesh handed over once with
 // GpuEngine::set_mesh (its node coordinates, potentials and tetrahedra) or
-// set_cartesian_mesh (the build_cartesian_grid arguments and the potential function).
+// set_cartesian_mesh (the build_cartesian_grid arguments and the potential function); a
+// detector with only mesh_field_2d needs its BiLinearMesh2D handed over the same way with
+// set_mesh2d or set_grid_mesh2d.
 // Guarded modules raise the reference's UnvalidatedModuleError; configurations the device
-// does not support (2D meshes; in the batched forms, charge release other than RecordOnly
-// and Exact / Bilinear kinematics) raise std::invalid_argument. Build the GpuEngine from the
+// does not support (in the batched forms, charge release other than RecordOnly and Exact /
+// Bilinear kinematics) raise std::invalid_argument. Build the GpuEngine from the
 // CrystalLattice itself to carry its kinematics mode.
 #pragma once
 
@@ -127,8 +129,6 @@ inline std::vector<cmpmc_electrode_pad> pads_of(const cmpmc::geometry::Electrode
 }
 
 inline cmpmc_detector to_c(const cmpmc::DetectorModel& d) {
-    if (d.mesh_field_2d.has_value())
-        throw std::invalid_argument("2D mesh fields are not available on the device");
     cmpmc_detector o;
     std::memset(&o, 0, sizeof(o));
     o.radius = d.solid.radius;
@@ -196,7 +196,8 @@ public:
         : GpuEngine(lattice.config(), static_cast<int>(lattice.kinematics_mode()), det, device) {}
 
     GpuEngine(const cmpmc::CrystalConfig& cfg, int kinematics_mode, const cmpmc::DetectorModel& det, int device)
-        : ccfg_(detail::to_c(cfg)), cdet_(detail::to_c(det)), needs_mesh_(det.mesh_field_3d.has_value()) {
+        : ccfg_(detail::to_c(cfg)), cdet_(detail::to_c(det)), needs_mesh_(det.mesh_field_3d.has_value()),
+          needs_mesh2_(!det.mesh_field_3d.has_value() && det.mesh_field_2d.has_value()) {
         detail::check(cmpmc_lattice_create(&ccfg_, &lat_), nullptr, "lattice");
         if (kinematics_mode != 0) detail::check(cmpmc_lattice_set_kinematics_mode(lat_, kinematics_mode), nullptr,
                                                 "kinematics mode");
@@ -215,6 +216,7 @@ public:
         cmpmc_gpu_destroy(ctx_);
         cmpmc_lattice_destroy(lat_);
         cmpmc_mesh_destroy(mesh_);
+        cmpmc_mesh2d_destroy(mesh2_);
     }
 
     // DetectorModel::mesh_field_3d: the TriLinearMesh3D(vertices, potentials, tetrahedra)
@@ -244,6 +246,34 @@ public:
                       nullptr, "mesh");
         attach(m);
     }
+    // DetectorModel::mesh_field_2d (used when there is no 3D mesh, engine.hpp:151-155): the
+    // BiLinearMesh2D(vertices, potentials, triangles, axisymmetric_rz) (mesh_field.hpp:356-366).
+    void set_mesh2d(const std::vector<cmpmc::geometry::BiLinearMesh2D::Point2D>& vertices,
+                    const std::vector<double>& potentials, const std::vector<std::array<int, 3>>& triangles,
+                    bool axisymmetric_rz = true) {
+        static_assert(sizeof(cmpmc::geometry::BiLinearMesh2D::Point2D) == 2 * sizeof(double), "Point2D layout");
+        std::vector<int32_t> t(3 * triangles.size());
+        for (size_t i = 0; i < triangles.size(); ++i)
+            for (int j = 0; j < 3; ++j) t[3 * i + j] = triangles[i][j];
+        cmpmc_mesh2d* m = nullptr;
+        detail::check(cmpmc_mesh2d_create(reinterpret_cast<const double*>(vertices.data()), potentials.data(),
+                                          potentials.size(), t.data(), triangles.size(), axisymmetric_rz ? 1 : 0, &m),
+                      nullptr, "2D mesh");
+        attach2(m);
+    }
+    // The same for a mesh made by BiLinearMesh2D::build_grid (mesh_field.hpp:438-479).
+    template <class PotentialFn2D>
+    void set_grid_mesh2d(double u_min, double u_max, double v_min, double v_max, int nu, int nv, PotentialFn2D&& fn,
+                         bool axisymmetric_rz = true) {
+        using Fn = std::remove_reference_t<PotentialFn2D>;
+        auto thunk = [](double u, double v, void* user) -> double { return (*static_cast<Fn*>(user))(u, v); };
+        cmpmc_mesh2d* m = nullptr;
+        detail::check(cmpmc_mesh2d_build_grid(u_min, u_max, v_min, v_max, nu, nv, thunk,
+                                              const_cast<void*>(static_cast<const void*>(&fn)),
+                                              axisymmetric_rz ? 1 : 0, &m),
+                      nullptr, "2D mesh");
+        attach2(m);
+    }
     GpuEngine(const GpuEngine&) = delete;
     GpuEngine& operator=(const GpuEngine&) = delete;
 
@@ -254,6 +284,8 @@ public:
                                 const GpuRunOptions& gpu = {}) {
         if (needs_mesh_ && !mesh_)
             throw std::invalid_argument("the detector has a mesh field: hand it over with set_mesh or set_cartesian_mesh");
+        if (needs_mesh2_ && !mesh2_)
+            throw std::invalid_argument("the detector has a 2D mesh field: hand it over with set_mesh2d or set_grid_mesh2d");
         const auto t0 = std::chrono::steady_clock::now();
         std::vector<uint64_t> rng(4 * n_events), ph_off(n_events + 1, 0), ch_off(n_events + 1, 0);
         std::vector<double> injected(n_events, 0.0);
@@ -334,12 +366,24 @@ private:
         mesh_ = m;
     }
 
+    void attach2(cmpmc_mesh2d* m) {
+        const int st = cmpmc_gpu_set_mesh2d(ctx_, m);
+        if (st != CMPMC_OK) {
+            cmpmc_mesh2d_destroy(m);
+            detail::check(st, ctx_, "2D mesh");
+        }
+        cmpmc_mesh2d_destroy(mesh2_);
+        mesh2_ = m;
+    }
+
     cmpmc_crystal_config ccfg_;
     cmpmc_detector cdet_;
     bool needs_mesh_ = false;
+    bool needs_mesh2_ = false;
     cmpmc_lattice* lat_ = nullptr;
     cmpmc_gpu_ctx* ctx_ = nullptr;
     cmpmc_mesh* mesh_ = nullptr;
+    cmpmc_mesh2d* mesh2_ = nullptr;
 };
 
 }  // namespace cmpmc_b200

@@ -288,6 +288,23 @@ int cmpmc_mesh_info(const cmpmc_mesh* mesh, uint64_t* n_vertices, uint64_t* n_te
 int cmpmc_mesh_field_at(const cmpmc_mesh* mesh, const double p[3], int32_t* hint, double E[3]);
 int cmpmc_mesh_potential_at(const cmpmc_mesh* mesh, const double p[3], int32_t* hint, double* V);
 
+/* ---- 2D triangle field mesh (replaces BiLinearMesh2D, geometry/mesh_field.hpp:347-582) ---- */
+typedef struct cmpmc_mesh2d cmpmc_mesh2d;
+/* BiLinearMesh2D(vertices, potentials, triangles, axisymmetric_rz) (mesh_field.hpp:356-366):
+ * uv [n][2] = (r, z) when axisymmetric (the field is rotated back into x, y, z), else (x, y). */
+int cmpmc_mesh2d_create(const double* uv, const double* potentials, uint64_t n_vertices, const int32_t* tris,
+                        uint64_t n_tris, int axisymmetric, cmpmc_mesh2d** out);
+/* BiLinearMesh2D::build_grid (mesh_field.hpp:438-479): nu x nv cells of two triangles;
+ * potential(u, v, user) gives the node potentials. */
+typedef double (*cmpmc_potential2d_fn)(double u, double v, void* user);
+int cmpmc_mesh2d_build_grid(double u_min, double u_max, double v_min, double v_max, int nu, int nv,
+                            cmpmc_potential2d_fn potential, void* user, int axisymmetric, cmpmc_mesh2d** out);
+void cmpmc_mesh2d_destroy(cmpmc_mesh2d* mesh);
+int cmpmc_mesh2d_info(const cmpmc_mesh2d* mesh, uint64_t* n_vertices, uint64_t* n_tris);
+/* field_at / potential_at with a caller-held walk hint (mesh_field.hpp:376-430); zero outside. */
+int cmpmc_mesh2d_field_at(const cmpmc_mesh2d* mesh, const double p[3], int32_t* hint, double E[3]);
+int cmpmc_mesh2d_potential_at(const cmpmc_mesh2d* mesh, const double p[3], int32_t* hint, double* V);
+
 /* ---- random streams (core/rng.hpp) --------------------------------------------- */
 void cmpmc_rng_for_stream(uint64_t seed, uint64_t stream, uint64_t state[4]);
 uint64_t cmpmc_rng_next_u64(uint64_t state[4]);
@@ -445,6 +462,9 @@ int cmpmc_gpu_set_electrode_mask(cmpmc_gpu_ctx* ctx, int surface, const cmpmc_el
  * device thread keeps its own walk hint across carriers and events, like the reference's
  * thread_local hint (mesh_field.hpp:119-122). */
 int cmpmc_gpu_set_mesh(cmpmc_gpu_ctx* ctx, const cmpmc_mesh* mesh);
+/* DetectorModel::mesh_field_2d (engine.hpp:100, used when there is no 3D mesh,
+ * engine.hpp:151-155): copies the 2D mesh to the context's device; NULL detaches it. */
+int cmpmc_gpu_set_mesh2d(cmpmc_gpu_ctx* ctx, const cmpmc_mesh2d* mesh);
 
 /* Allocation-free run of the plain FP64 form (phonon-only events). No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc -- code running inside a

@@ -35,6 +35,12 @@
 //       E = Delta (1 + 45 u) (Rng::for_stream(3, 0), sub-gap, in-table and above-table),
 //       absorb_phonon_fast(E) with the same stream; per record E, edep (f64), the count
 //       (u32) and the re-emitted energies (f64).
+//   cmpmc_ref mesh2 <n_points> <out>
+//       Builds the tp2 axisymmetric (r, z) mesh and a planar (x, y) mesh
+//       (build_grid(-R, R, -R, R, 32, 32) of V = 3 (x + R) / 2R + 0.5 (y / R)^2) and writes,
+//       for n points (the first 16 on the axis, x = y = 0, the rest drawn in the cylinder,
+//       Rng::for_stream(6, 0)), the point, then field_at and potential_at of each mesh
+//       (one walk hint per mesh and query kind): 11 doubles per point.
 //   cmpmc_ref mesh <n_points> <out>
 //       Builds the c3 field mesh and writes, for n points drawn in the cylinder
 //       (Rng::for_stream(5, 0)), the point, field_at and potential_at (each with one
@@ -62,6 +68,8 @@
 //       {2700, 6420, 3040}) on both faces; seed 42
 //   tpd tp with ChargeRelease::BulkDebye; tpe tp with ChargeRelease::ElectrodeFilm; seed 77
 //   c0x c0 with KinematicsMode::Exact; c0b c0 with KinematicsMode::Bilinear; seed 42
+//   tp2 tp with the field of an axisymmetric BiLinearMesh2D::build_grid(0, R, -h, h, 40, 40)
+//       of V = 2 (z + h) / 2h + 0.3 (r / R)^2 (z / h) (mesh_field_2d; no 3D mesh); seed 77
 //   c0m c0 with the SuperCDMS QET electrode mask (fill fraction 0.8) on both faces; seed 42
 //   tpm tp with the same masks on both faces; seed 77
 //   c3s the same with E = 10 eV * 10^u, max_sampled_phonons 20 (prompt phonons carry the
@@ -104,7 +112,7 @@ Workload make_workload(const std::string& w) {
     else if (w == "c1") wl.seed = 7;
     else if (w == "c2") { wl.seed = 11; wl.events_per_chunk = 1; }
     else if (w == "c4") wl.seed = 17;
-    else if (w == "tp" || w == "tpl" || w == "tpm" || w == "tpd" || w == "tpe") wl.seed = 77;
+    else if (w == "tp" || w == "tpl" || w == "tpm" || w == "tpd" || w == "tpe" || w == "tp2") wl.seed = 77;
     else if (w == "c3" || w == "c3s") { wl.seed = 13; wl.events_per_chunk = 1; }
     else { std::fprintf(stderr, "unknown workload %s\n", w.c_str()); std::exit(2); }
     return wl;
@@ -128,6 +136,23 @@ geometry::TriLinearMesh3D recoil_mesh(const CylinderSolid& s) {
         R, R, h, 58, 58, 57, [R, h](const Vec3& p) { return recoil_potential(p, R, h); });
 }
 
+double axisym_potential(double r, double z, double R, double h) {
+    return 2.0 * (z + h) / (2.0 * h) + 0.3 * (r / R) * (r / R) * (z / h);
+}
+
+geometry::BiLinearMesh2D axisym_mesh(const CylinderSolid& s) {
+    const double R = s.radius, h = s.half_z;
+    return geometry::BiLinearMesh2D::build_grid(
+        0.0, R, -h, h, 40, 40, [R, h](double r, double z) { return axisym_potential(r, z, R, h); }, true);
+}
+
+geometry::BiLinearMesh2D planar_mesh(const CylinderSolid& s) {
+    const double R = s.radius;
+    return geometry::BiLinearMesh2D::build_grid(
+        -R, R, -R, R, 32, 32, [R](double x, double y) { return 3.0 * (x + R) / (2.0 * R) + 0.5 * (y / R) * (y / R); },
+        false);
+}
+
 void setup_lattice(const std::string& w, CrystalLattice& lattice) {
     if (w == "c0x") lattice.set_kinematics_mode(CrystalLattice::KinematicsMode::Exact);
     if (w == "c0b") lattice.set_kinematics_mode(CrystalLattice::KinematicsMode::Bilinear);
@@ -140,8 +165,9 @@ void setup_detector(const std::string& w, DetectorModel& det) {
     } else if (w == "c2") {
         det.e_field = UniformElectricField::from_bias(4.0, 2.54 * units::cm);
         det.luke_sample_fraction = 0.0;
-    } else if (w == "tp" || w == "tpl" || w == "tpm" || w == "tpd" || w == "tpe") {
+    } else if (w == "tp" || w == "tpl" || w == "tpm" || w == "tpd" || w == "tpe" || w == "tp2") {
         det.e_field = UniformElectricField::from_bias(2.0, 2.54 * units::cm);
+        if (w == "tp2") det.mesh_field_2d = axisym_mesh(det.solid);
         det.luke_sample_fraction = (w == "tpl") ? 1.0 : 0.02;
         if (w == "tpd") det.charge_release = DetectorModel::ChargeRelease::BulkDebye;
         if (w == "tpe") det.charge_release = DetectorModel::ChargeRelease::ElectrodeFilm;
@@ -439,6 +465,29 @@ int cmd_kaplan(uint64_t n, const std::string& out) {
     return 0;
 }
 
+int cmd_mesh2(uint64_t n, const std::string& out) {
+    const DetectorModel det;
+    const geometry::BiLinearMesh2D ax = axisym_mesh(det.solid), pl = planar_mesh(det.solid);
+    Rng rng = Rng::for_stream(6, 0);
+    int he_a = 0, hv_a = 0, he_p = 0, hv_p = 0;
+    FILE* f = open_or_die(out);
+    for (uint64_t i = 0; i < n; ++i) {
+        Vec3 p = uniform_origin(det.solid, rng);
+        if (i < 16) p.x = p.y = 0.0;
+        const Vec3 Ea = ax.field_at(p, he_a);
+        const double Va = ax.potential_at(p, hv_a);
+        const Vec3 Ep = pl.field_at(p, he_p);
+        const double Vp = pl.potential_at(p, hv_p);
+        const double rec[11] = {p.x, p.y, p.z, Ea.x, Ea.y, Ea.z, Va, Ep.x, Ep.y, Ep.z, Vp};
+        std::fwrite(rec, 8, 11, f);
+    }
+    std::fclose(f);
+    std::printf("{\"axisym_vertices\": %zu, \"axisym_triangles\": %zu, \"planar_vertices\": %zu, "
+                "\"planar_triangles\": %zu}\n",
+                ax.num_vertices(), ax.num_triangles(), pl.num_vertices(), pl.num_triangles());
+    return 0;
+}
+
 int cmd_mesh(uint64_t n, const std::string& out) {
     const DetectorModel det;
     const geometry::TriLinearMesh3D mesh = recoil_mesh(det.solid);
@@ -475,6 +524,7 @@ int main(int argc, char** argv) {
     if (cmd == "amm" && argc == 4) return cmd_amm(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "kaplan" && argc == 4) return cmd_kaplan(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mask" && argc == 4) return cmd_mask(std::strtoull(argv[2], nullptr, 10), argv[3]);
+    if (cmd == "mesh2" && argc == 4) return cmd_mesh2(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mesh" && argc == 4) return cmd_mesh(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "rng" && argc == 5)
         return cmd_rng(std::strtoull(argv[2], nullptr, 10), std::strtoull(argv[3], nullptr, 10), std::atoi(argv[4]));

@@ -64,6 +64,7 @@ PLAN = {
     "tpe": (8, 203),
     "c0x": (8, 1000),
     "c0b": (8, 2000),
+    "tp2": (8, 1000),
 }
 
 
@@ -91,6 +92,14 @@ def main() -> None:
             rec = np.fromfile(path, dtype=np.float64).reshape(-1, 7)
             np.savez_compressed(os.path.join(HERE, "mesh_c3.npz"), points=rec[:, 0:3], field=rec[:, 3:6],
                                 potential=rec[:, 6], n_vertices=info["vertices"], n_tets=info["tetrahedra"])
+        if want("mesh2"):
+            path = os.path.join(tmp, "mesh2.bin")
+            info = json.loads(subprocess.run([REF, "mesh2", "4096", path], check=True, capture_output=True,
+                                             text=True).stdout)
+            rec = np.fromfile(path, dtype=np.float64).reshape(-1, 11)
+            np.savez_compressed(os.path.join(HERE, "mesh2d.npz"), points=rec[:, 0:3], axisym_field=rec[:, 3:6],
+                                axisym_potential=rec[:, 6], planar_field=rec[:, 7:10], planar_potential=rec[:, 10],
+                                **{k: v for k, v in info.items()})
         if want("mask"):
             path = os.path.join(tmp, "mask.bin")
             subprocess.run([REF, "mask", "4096", path], check=True)

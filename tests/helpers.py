@@ -25,8 +25,10 @@ def detector_for(workload: str):
     elif workload == "c3s":
         det.mesh_field_3d = recoil_mesh()
         det.luke_sample_fraction = 0.05
-    elif workload in ("tp", "tpl", "tpm", "tpd", "tpe"):
+    elif workload in ("tp", "tpl", "tpm", "tpd", "tpe", "tp2"):
         det.e_field = cm.UniformElectricField.from_bias(2.0, 2.54 * cm.units.cm)
+        if workload == "tp2":
+            det.mesh_field_2d = axisym_mesh(det)
         det.luke_sample_fraction = 1.0 if workload == "tpl" else 0.02
         det.charge_release = {"tpd": 1, "tpe": 2}.get(workload, 0)
     if workload == "c0a":
@@ -54,6 +56,25 @@ def lattice_for(workload: str, default_lattice):
 _MESH = []
 
 
+def axisym_mesh(det):
+    """The tp2 field: BiLinearMesh2D.build_grid(0, R, -h, h, 40, 40) in (r, z) of
+    V = 2 (z + h) / 2h + 0.3 (r / R)^2 (z / h)."""
+    import cmpmc_b200 as cm
+    R, h = det.solid.radius, det.solid.half_z
+    return cm.BiLinearMesh2D.build_grid(0.0, R, -h, h, 40, 40,
+                                        lambda r, z: 2.0 * (z + h) / (2.0 * h) + 0.3 * (r / R) * (r / R) * (z / h),
+                                        True)
+
+
+def planar_mesh(det):
+    """A planar (x, y) BiLinearMesh2D.build_grid(-R, R, -R, R, 32, 32) of
+    V = 3 (x + R) / 2R + 0.5 (y / R)^2."""
+    import cmpmc_b200 as cm
+    R = det.solid.radius
+    return cm.BiLinearMesh2D.build_grid(-R, R, -R, R, 32, 32,
+                                        lambda x, y: 3.0 * (x + R) / (2.0 * R) + 0.5 * (y / R) * (y / R), False)
+
+
 def recoil_mesh():
     """The recoil workloads' field mesh (built once per test process)."""
     import cmpmc_b200 as cm
@@ -62,7 +83,7 @@ def recoil_mesh():
     return _MESH[0]
 
 
-WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13, "c0m": 42, "tpm": 77, "c0a": 42, "tpd": 77, "tpe": 77, "c0x": 42, "c0b": 42}
+WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13, "c0m": 42, "tpm": 77, "c0a": 42, "tpd": 77, "tpe": 77, "c0x": 42, "c0b": 42, "tp2": 77}
 
 
 def workload_of(name: str):
@@ -73,7 +94,7 @@ def workload_of(name: str):
             "c0m": cm.workloads.single_l_origin, "tpm": cm.workloads.test_parallel,
             "c0a": cm.workloads.single_l_origin, "tpd": cm.workloads.test_parallel,
             "tpe": cm.workloads.test_parallel, "c0x": cm.workloads.single_l_origin,
-            "c0b": cm.workloads.single_l_origin}[name]
+            "c0b": cm.workloads.single_l_origin, "tp2": cm.workloads.test_parallel}[name]
 
 
 def has_gpu() -> bool:

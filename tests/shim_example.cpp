@@ -48,6 +48,17 @@ int main() {
         for (const SensorHit& x : m.hits) on_pad += (x.channel_id >= 0);
         std::printf("masked + mesh: device hits %zu (%zu on pads) cpu hits %zu\n", m.hits.size(), on_pad,
                     mc.hits.size());
+        // an axisymmetric 2D mesh field (mesh_field_2d, handed over once)
+        DetectorModel det3 = det;
+        auto pot2 = [h](double r, double z) { return 2.0 * (z + h) / (2.0 * h) + 0.1 * r / h; };
+        det3.mesh_field_2d = geometry::BiLinearMesh2D::build_grid(0.0, R, -h, h, 16, 16, pot2, true);
+        const SimulationEngine engine3(lattice, det3);
+        cmpmc_b200::GpuEngine gpu3(lattice.config(), det3);
+        gpu3.set_grid_mesh2d(0.0, R, -h, h, 16, 16, pot2, true);
+        const RunResult a = gpu3.run_events(203, gen, opt);
+        const RunResult ac = run_events(engine3, 203, gen, opt);
+        std::printf("2D mesh: device hits %zu cpu hits %zu charge steps %llu vs %llu\n", a.hits.size(), ac.hits.size(),
+                    (unsigned long long)a.stats.charge_steps, (unsigned long long)ac.stats.charge_steps);
         return 0;
     } catch (const std::runtime_error& e) {
         std::printf("device unavailable: %s\n", e.what());

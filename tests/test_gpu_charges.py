@@ -85,6 +85,29 @@ def test_recoil_batched_matches_reference(ge_lattice):
         assert abs(z) < Z_MAX, (name, z)
 
 
+def test_axisymmetric_mesh_batched_matches_reference(ge_lattice):
+    """The mixed workload in the field of an axisymmetric BiLinearMesh2D (FP32 edge walk,
+    the field rotated back around the axis): per-event differences to the same events of
+    the reference, averaged over four seeds, z < 4."""
+    ref = golden("tp2_cr_summary.npz")["summary"]
+    n = len(ref)
+    runs = []
+    for sd in (77, 1077, 2077, 3077):
+        _, res = _run(ge_lattice, "tp2", n, seed=sd)
+        runs.append(summarize(res.event_stats, res.hit_offsets, res.hits))
+    for name in ("n_hits", "charge_steps", "luke_phonons_emitted", "charges_collected", "total_luke_phonon_eV",
+                 "charge_surface_refls", "sum_time", "sum_edep"):
+        a = _col(ref, name)
+        b = np.mean([_col(r, name) for r in runs], axis=0)
+        d = b - a
+        if d.std(ddof=1) == 0.0:
+            assert d.mean() == 0.0, name
+            continue
+        z = d.mean() / (d.std(ddof=1) / np.sqrt(n))
+        print(f"{name}: reference {a.mean():.6g} batched {b.mean():.6g} z {z:.2f}")
+        assert abs(z) < Z_MAX, (name, z)
+
+
 def test_queue_phases_reproduce_the_same_hits(ge_lattice):
     import cmpmc_b200 as cm
     eng, a = _run(ge_lattice, "c3s", 16)

@@ -41,7 +41,7 @@ def _device_summary(ge_lattice, wl, n):
     return _RESULTS[(wl, n)]
 
 
-@pytest.mark.parametrize("wl", ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b"])
+@pytest.mark.parametrize("wl", ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b", "tp2"])
 def test_event_parity_correctly_rounded_reference(ge_lattice, wl):
     ref = golden(f"{wl}_cr_summary.npz")["summary"]
     got = _device_summary(ge_lattice, wl, len(ref))
@@ -53,7 +53,7 @@ def test_event_parity_correctly_rounded_reference(ge_lattice, wl):
         assert np.all(np.abs(a - b) <= 1e-12 * np.maximum(np.abs(a), 1e-300) + 1e-300), name
 
 
-@pytest.mark.parametrize("wl", ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b"])
+@pytest.mark.parametrize("wl", ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b", "tp2"])
 def test_event_parity_glibc_reference(ge_lattice, wl):
     ref = golden(f"{wl}_summary.npz")["summary"]
     cr = golden(f"{wl}_cr_summary.npz")
@@ -66,7 +66,7 @@ def test_event_parity_glibc_reference(ge_lattice, wl):
         assert cmp["frac"] >= 0.985
 
 
-@pytest.mark.parametrize("wl", ["c0", "tp", "tpl", "c2", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b"])
+@pytest.mark.parametrize("wl", ["c0", "tp", "tpl", "c2", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b", "tp2"])
 def test_full_hit_records_match(ge_lattice, wl):
     """Hit-by-hit comparison from the reference's own initial stacks and Rng states."""
     import cmpmc_b200 as cm

@@ -164,6 +164,55 @@ def test_mesh_from_arrays_and_cartesian_builder_agree():
     assert a.field_at((3.0, 0.0, 0.0)) == (0.0, 0.0, 0.0)
 
 
+def test_mesh2d_field_bit_identical_to_reference():
+    """BiLinearMesh2D::build_grid + field_at / potential_at, axisymmetric (r, z) and planar
+    (x, y): every field and potential at 4096 points (16 on the axis) equals the
+    reference's, with one walk hint per mesh and query kind carried from point to point."""
+    import ctypes as C
+    import cmpmc_b200 as cm
+    from tests.helpers import axisym_mesh, planar_mesh
+    g = golden("mesh2d.npz")
+    det = cm.DetectorModel()
+    ax, pl = axisym_mesh(det), planar_mesh(det)
+    assert ax.num_vertices() == int(g["axisym_vertices"]) and ax.num_triangles() == int(g["axisym_triangles"])
+    assert pl.num_vertices() == int(g["planar_vertices"]) and pl.num_triangles() == int(g["planar_triangles"])
+    h = [C.c_int32(0) for _ in range(4)]
+    for i, p in enumerate(g["points"]):
+        assert ax.field_at(p, h[0]) == tuple(g["axisym_field"][i]), i
+        assert ax.potential_at(p, h[1]) == g["axisym_potential"][i], i
+        assert pl.field_at(p, h[2]) == tuple(g["planar_field"][i]), i
+        assert pl.potential_at(p, h[3]) == g["planar_potential"][i], i
+
+
+def test_mesh2d_from_arrays_matches_grid_builder():
+    """A user mesh given as arrays (the BiLinearMesh2D constructor, triangle nodes in any
+    order) equals the grid builder's; a linear potential gives its exact gradient; the
+    field is zero outside the hull and along the axis only E_z remains."""
+    import cmpmc_b200 as cm
+    n = 4
+    fn = lambda u, v: 2.0 * u - 3.0 * v  # noqa: E731
+    a = cm.BiLinearMesh2D.build_grid(0.0, 1.0, -1.0, 1.0, n, n, fn, True)
+    us, vs = np.linspace(0.0, 1.0, n + 1), np.linspace(-1.0, 1.0, n + 1)
+    verts = np.array([(u, v) for u in us for v in vs])
+    vid = lambda i, j: i * (n + 1) + j  # noqa: E731
+    tris = []
+    for i in range(n):
+        for j in range(n):
+            tris += [(vid(i + 1, j + 1), vid(i + 1, j), vid(i, j)), (vid(i, j + 1), vid(i + 1, j + 1), vid(i, j))]
+    b = cm.BiLinearMesh2D(verts, [fn(u, v) for u, v in verts], tris, axisymmetric_rz=True)
+    assert a.num_triangles() == b.num_triangles() == 2 * n * n
+    rng = np.random.default_rng(3)
+    for p in rng.uniform(-0.7, 0.7, size=(200, 3)):
+        ea, eb = a.field_at(p), b.field_at(p)
+        assert ea == eb
+        r = float(np.hypot(p[0], p[1]))
+        np.testing.assert_allclose(ea, (-2.0 * p[0] / r, -2.0 * p[1] / r, 3.0), rtol=1e-12, atol=1e-12)
+    assert a.field_at((0.0, 0.0, 0.3)) == pytest.approx((0.0, 0.0, 3.0), rel=1e-12)
+    assert a.field_at((2.0, 0.0, 0.0)) == (0.0, 0.0, 0.0)
+    planar = cm.BiLinearMesh2D.build_grid(-1.0, 1.0, -1.0, 1.0, n, n, fn, False)
+    np.testing.assert_allclose(planar.field_at((0.3, -0.2, 5.0)), (-2.0, 3.0, 0.0), rtol=1e-12, atol=1e-12)
+
+
 def test_electrode_masks_match_reference():
     """SuperCDMS QET preset with fill fraction 0.8 (find_channel drawing from the same
     stream as the reference) and a 4 x 4 rectangular pad grid at 4096 points of a face."""
