@@ -203,6 +203,7 @@ _SIG = {
                                  C.POINTER(C.c_void_p)]),
     "cmpmc_mesh_build_cartesian": (_i32, [_f64, _f64, _f64, _i32, _i32, _i32, C.c_void_p, C.c_void_p,
                                           C.POINTER(C.c_void_p)]),
+    "cmpmc_mesh_load_files": (_i32, [C.c_char_p, C.c_char_p, _f64, _f64, C.POINTER(C.c_void_p)]),
     "cmpmc_recoil_potential": (_f64, [C.POINTER(_f64), C.c_void_p]),
     "cmpmc_recoil_mesh": (_i32, [C.POINTER(DetectorC), C.POINTER(C.c_void_p)]),
     "cmpmc_mesh_destroy": (None, [C.c_void_p]),

@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 import time
 from dataclasses import dataclass, field, replace
 from enum import IntEnum
@@ -571,6 +572,18 @@ class TriLinearMesh3D:
         h = C.c_void_p()
         _check(lib.cmpmc_mesh_build_cartesian(half_x, half_y, half_z, nx, ny, nz, cb, None, C.byref(h)),
                what="mesh")
+        return TriLinearMesh3D(_handle=h)
+
+    @staticmethod
+    def load_from_files(coords_file: str, tets_file: str, coord_unit_m: float = 1.0,
+                        potential_unit_V: float = 1.0) -> "TriLinearMesh3D":
+        """G4CMP-style ASCII mesh (mesh_field.hpp:190-231): "x y z V" node lines and
+        "i0 i1 i2 i3" tetrahedron lines, '#' / '%' comments; parsed natively. A file that
+        cannot be opened gives an empty mesh, as in the reference."""
+        lib = _ffi.load()
+        h = C.c_void_p()
+        _check(lib.cmpmc_mesh_load_files(os.fsencode(coords_file), os.fsencode(tets_file), float(coord_unit_m),
+                                         float(potential_unit_V), C.byref(h)), what="mesh")
         return TriLinearMesh3D(_handle=h)
 
     @staticmethod

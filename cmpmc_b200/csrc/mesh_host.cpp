@@ -14,7 +14,10 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <fstream>
 #include <new>
+#include <sstream>
+#include <string>
 #include <vector>
 
 #include "internal.hpp"
@@ -315,6 +318,48 @@ int cmpmc_mesh_create(const double* vertices, const double* potentials, uint64_t
     }
     *out = m;
     return CMPMC_OK;
+}
+
+// TriLinearMesh3D::load_from_files (mesh_field.hpp:190-231): "x y z V" node lines and
+// "i0 i1 i2 i3" tetrahedron lines, '#' / '%' comment lines and lines that do not parse
+// skipped, coordinates and potentials scaled by the units. A file that does not open
+// contributes no lines (an empty mesh, as in the reference).
+int cmpmc_mesh_load_files(const char* coords_file, const char* tets_file, double coord_unit_m,
+                          double potential_unit_V, cmpmc_mesh** out) {
+    if (!out || !coords_file || !tets_file) return CMPMC_ERR_INVALID;
+    *out = nullptr;
+    std::vector<double> X, V;
+    std::vector<int32_t> T;
+    std::string line;
+    {
+        std::ifstream in(coords_file);
+        while (std::getline(in, line)) {
+            if (line.empty() || line[0] == '#' || line[0] == '%') continue;
+            std::istringstream ls(line);
+            double x, y, z, v;
+            if (ls >> x >> y >> z >> v) {
+                X.push_back(x * coord_unit_m);
+                X.push_back(y * coord_unit_m);
+                X.push_back(z * coord_unit_m);
+                V.push_back(v * potential_unit_V);
+            }
+        }
+    }
+    {
+        std::ifstream in(tets_file);
+        while (std::getline(in, line)) {
+            if (line.empty() || line[0] == '#' || line[0] == '%') continue;
+            std::istringstream ls(line);
+            int a, b, c, d;
+            if (ls >> a >> b >> c >> d) {
+                T.push_back(a);
+                T.push_back(b);
+                T.push_back(c);
+                T.push_back(d);
+            }
+        }
+    }
+    return cmpmc_mesh_create(X.data(), V.data(), V.size(), T.data(), T.size() / 4, -1e30, 1e30, out);
 }
 
 int cmpmc_mesh_build_cartesian(double half_x, double half_y, double half_z, int nx, int ny, int nz,

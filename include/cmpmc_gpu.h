@@ -278,6 +278,14 @@ int cmpmc_mesh_create(const double* vertices, const double* potentials, uint64_t
 typedef double (*cmpmc_potential_fn)(const double p[3], void* user);
 int cmpmc_mesh_build_cartesian(double half_x, double half_y, double half_z, int nx, int ny, int nz,
                                cmpmc_potential_fn potential, void* user, cmpmc_mesh** out);
+/* TriLinearMesh3D::load_from_files (mesh_field.hpp:190-231): whitespace-separated ASCII,
+ * one node "x y z V" per line in coords_file and one tetrahedron "i0 i1 i2 i3" (0-based)
+ * per line in tets_file; lines starting with '#' or '%' and lines that do not parse are
+ * skipped; coordinates and potentials are multiplied by the units. A file that cannot be
+ * opened gives no lines (an empty mesh, as in the reference); a node index out of range
+ * returns CMPMC_ERR_INVALID (the reference reads past its node table there). */
+int cmpmc_mesh_load_files(const char* coords_file, const char* tets_file, double coord_unit_m,
+                          double potential_unit_V, cmpmc_mesh** out);
 /* The node potential of the recoil workloads (user = const cmpmc_detector*):
  * V = 4 V (z + h) / 2h + 0.2 V (r / R)^2 sin(pi z / 2h). */
 double cmpmc_recoil_potential(const double p[3], void* detector);

@@ -41,6 +41,9 @@
 //       for n points (the first 16 on the axis, x = y = 0, the rest drawn in the cylinder,
 //       Rng::for_stream(6, 0)), the point, then field_at and potential_at of each mesh
 //       (one walk hint per mesh and query kind): 11 doubles per point.
+//   cmpmc_ref meshfile <coords> <tets> <coord_unit_m> <potential_unit_V> <n_points> <out>
+//       TriLinearMesh3D::load_from_files of the two ASCII files, then as `mesh` for n points
+//       drawn in the default cylinder from Rng::for_stream(7, 0): 7 doubles per point.
 //   cmpmc_ref mesh <n_points> <out>
 //       Builds the c3 field mesh and writes, for n points drawn in the cylinder
 //       (Rng::for_stream(5, 0)), the point, field_at and potential_at (each with one
@@ -488,6 +491,24 @@ int cmd_mesh2(uint64_t n, const std::string& out) {
     return 0;
 }
 
+int cmd_meshfile(const char* coords, const char* tets, double cu, double vu, uint64_t n, const std::string& out) {
+    const DetectorModel det;
+    const geometry::TriLinearMesh3D mesh = geometry::TriLinearMesh3D::load_from_files(coords, tets, cu, vu);
+    Rng rng = Rng::for_stream(7, 0);
+    int hint_e = 0, hint_v = 0;
+    FILE* f = open_or_die(out);
+    for (uint64_t i = 0; i < n; ++i) {
+        const Vec3 p = uniform_origin(det.solid, rng);
+        const Vec3 E = mesh.field_at(p, hint_e);
+        const double V = mesh.potential_at(p, hint_v);
+        const double rec[7] = {p.x, p.y, p.z, E.x, E.y, E.z, V};
+        std::fwrite(rec, 8, 7, f);
+    }
+    std::fclose(f);
+    std::printf("{\"vertices\": %zu, \"tetrahedra\": %zu}\n", mesh.num_vertices(), mesh.num_tetrahedra());
+    return 0;
+}
+
 int cmd_mesh(uint64_t n, const std::string& out) {
     const DetectorModel det;
     const geometry::TriLinearMesh3D mesh = recoil_mesh(det.solid);
@@ -524,6 +545,9 @@ int main(int argc, char** argv) {
     if (cmd == "amm" && argc == 4) return cmd_amm(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "kaplan" && argc == 4) return cmd_kaplan(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mask" && argc == 4) return cmd_mask(std::strtoull(argv[2], nullptr, 10), argv[3]);
+    if (cmd == "meshfile" && argc == 8)
+        return cmd_meshfile(argv[2], argv[3], std::strtod(argv[4], nullptr), std::strtod(argv[5], nullptr),
+                            std::strtoull(argv[6], nullptr, 10), argv[7]);
     if (cmd == "mesh2" && argc == 4) return cmd_mesh2(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mesh" && argc == 4) return cmd_mesh(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "rng" && argc == 5)

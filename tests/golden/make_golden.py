@@ -100,6 +100,8 @@ def main() -> None:
             np.savez_compressed(os.path.join(HERE, "mesh2d.npz"), points=rec[:, 0:3], axisym_field=rec[:, 3:6],
                                 axisym_potential=rec[:, 6], planar_field=rec[:, 7:10], planar_potential=rec[:, 10],
                                 **{k: v for k, v in info.items()})
+        if want("meshfile"):
+            _mesh_files(tmp)
         if want("mask"):
             path = os.path.join(tmp, "mask.bin")
             subprocess.run([REF, "mask", "4096", path], check=True)
@@ -145,6 +147,49 @@ def main() -> None:
         f.write("Generated by tests/golden/make_golden.py from the unmodified reference CMPMC\n"
                 "(oracle/_ref, g++ -O3 -std=c++20, no -march=native).\n"
                 f"host libm: {gl}\n")
+
+
+def _mesh_files(tmp: str) -> None:
+    """A jittered Kuhn mesh of the default cylinder's bounding box written as the ASCII
+    node / tetrahedron files of TriLinearMesh3D::load_from_files (millimetres, millivolts,
+    with comment, blank and malformed lines), and the reference's fields at 2048 points."""
+    d = os.path.join(HERE, "mesh_files")
+    os.makedirs(d, exist_ok=True)
+    R, h = 38.1, 12.7  # mm
+    n = (6, 6, 5)
+    rng = np.random.default_rng(5)
+    xs = [np.linspace(-a, a, k + 1) for a, k in ((R, n[0]), (R, n[1]), (h, n[2]))]
+    vid = lambda i, j, k: (i * (n[1] + 1) + j) * (n[2] + 1) + k  # noqa: E731
+    with open(os.path.join(d, "nodes.txt"), "w") as f:
+        f.write("# x_mm y_mm z_mm V_mV\n% exported node table\n\n")
+        for i in range(n[0] + 1):
+            for j in range(n[1] + 1):
+                for k in range(n[2] + 1):
+                    p = np.array([xs[0][i], xs[1][j], xs[2][k]])
+                    inner = 0 < i < n[0] and 0 < j < n[1] and 0 < k < n[2]
+                    if inner:
+                        p = p + rng.uniform(-0.15, 0.15, 3) * np.array([2 * R / n[0], 2 * R / n[1], 2 * h / n[2]])
+                    v = 4000.0 * (p[2] + h) / (2 * h) + 150.0 * (p[0] / R) ** 2
+                    f.write(" ".join(repr(float(x)) for x in (p[0], p[1], p[2], v)) + "\n")
+        f.write("not a node line\n")
+    with open(os.path.join(d, "tets.txt"), "w") as f:
+        f.write("# i0 i1 i2 i3\n")
+        for i in range(n[0]):
+            for j in range(n[1]):
+                for k in range(n[2]):
+                    c = [vid(i + a, j + b, k + e) for a in (0, 1) for b in (0, 1) for e in (0, 1)]
+                    v000, v001, v010, v011, v100, v101, v110, v111 = c
+                    for t in ((v111, v000, v100, v110), (v000, v100, v101, v111), (v000, v010, v110, v111),
+                              (v000, v010, v011, v111), (v000, v001, v101, v111), (v000, v001, v011, v111)):
+                        f.write(" ".join(str(x) for x in t) + "\n")
+        f.write("%\n")
+    path = os.path.join(tmp, "meshfile.bin")
+    info = json.loads(subprocess.run([REF, "meshfile", os.path.join(d, "nodes.txt"), os.path.join(d, "tets.txt"),
+                                      "1e-3", "1e-3", "2048", path], check=True, capture_output=True,
+                                     text=True).stdout)
+    rec = np.fromfile(path, dtype=np.float64).reshape(-1, 7)
+    np.savez_compressed(os.path.join(HERE, "mesh_files.npz"), points=rec[:, 0:3], field=rec[:, 3:6],
+                        potential=rec[:, 6], n_vertices=info["vertices"], n_tets=info["tetrahedra"])
 
 
 def _rng_vectors() -> None:

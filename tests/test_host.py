@@ -164,6 +164,30 @@ def test_mesh_from_arrays_and_cartesian_builder_agree():
     assert a.field_at((3.0, 0.0, 0.0)) == (0.0, 0.0, 0.0)
 
 
+def test_mesh_load_from_files_matches_reference():
+    """TriLinearMesh3D::load_from_files of an irregular (jittered) mesh in millimetres and
+    millivolts with comment, blank and malformed lines: node and tetrahedron counts, and the
+    field and potential at 2048 points equal the reference's bit for bit. Files that do not
+    open give no lines (an empty mesh, as in the reference); tetrahedra whose nodes are
+    missing are an error (the reference reads past its node table there)."""
+    import ctypes as C
+    import cmpmc_b200 as cm
+    from tests.helpers import GOLDEN
+    g = golden("mesh_files.npz")
+    d = os.path.join(GOLDEN, "mesh_files")
+    m = cm.TriLinearMesh3D.load_from_files(os.path.join(d, "nodes.txt"), os.path.join(d, "tets.txt"), 1e-3, 1e-3)
+    assert m.num_vertices() == int(g["n_vertices"]) and m.num_tetrahedra() == int(g["n_tets"])
+    he, hv = C.c_int32(0), C.c_int32(0)
+    for i, p in enumerate(g["points"]):
+        assert m.field_at(p, he) == tuple(g["field"][i]), i
+        assert m.potential_at(p, hv) == g["potential"][i], i
+    empty = cm.TriLinearMesh3D.load_from_files(os.path.join(d, "missing.txt"), os.path.join(d, "missing.txt"))
+    assert empty.empty() and empty.num_vertices() == 0
+    assert empty.field_at((0.0, 0.0, 0.0)) == (0.0, 0.0, 0.0)
+    with pytest.raises(cm.CmpmcError):
+        cm.TriLinearMesh3D.load_from_files(os.path.join(d, "missing.txt"), os.path.join(d, "tets.txt"))
+
+
 def test_mesh2d_field_bit_identical_to_reference():
     """BiLinearMesh2D::build_grid + field_at / potential_at, axisymmetric (r, z) and planar
     (x, y): every field and potential at 4096 points (16 on the axis) equals the
