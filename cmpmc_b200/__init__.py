@@ -9,6 +9,8 @@ from .api import (AluminumFilm, CmpmcError, ElectrodePad, ElectrodePatternMask, 
                   KaplanSurrogateLUT, PackedEvents, PhononMode, Rng, RunOptions, RunResult,
                   SimStats, SimulationEngine, SuperconductorFilmConfig, SurfaceId, SurfaceProperty,
                   TriLinearMesh3D, BiLinearMesh2D, UniformElectricField, UnvalidatedModuleError, Workload, materials, run_events, units, workloads)
+from .partition import (EmpiricalNIELParams, EnergyPartition, HitMerger, NIELModel, PartitionOptions, PartitionResult,
+                        PrimaryStepInput, physics)
 from .adjoint import AdjointResult, HistogramAdjoint, THETA_NAMES, default_theta
 
 __all__ = [
@@ -18,5 +20,6 @@ __all__ = [
     "SimulationEngine", "SuperconductorFilmConfig", "SurfaceId", "SurfaceProperty", "TriLinearMesh3D", "BiLinearMesh2D",
     "UniformElectricField",
     "UnvalidatedModuleError", "Workload", "materials", "run_events", "units", "workloads", "HistogramAdjoint",
-    "THETA_NAMES", "default_theta",
+    "THETA_NAMES", "default_theta", "EmpiricalNIELParams", "EnergyPartition", "HitMerger", "NIELModel",
+    "PartitionOptions", "PartitionResult", "PrimaryStepInput", "physics",
 ]

@@ -167,6 +167,28 @@ class TuneResultC(C.Structure):
     ]
 
 
+class PartitionOptionsC(C.Structure):
+    _fields_ = [("niel_model", _i32), ("use_fano_fluctuations", _i32), ("use_charge_cloud", _i32),
+                ("max_sampled_pairs", _u32), ("max_sampled_phonons", _u32), ("emp_energy_dependent_k", _i32),
+                ("emp_k_fixed", _f64), ("emp_k_low", _f64), ("emp_k_high", _f64), ("emp_e_low_eV", _f64),
+                ("emp_e_high_eV", _f64)]
+
+
+class PartitionResultC(C.Structure):
+    _fields_ = [("total_edep_eV", _f64), ("ionizing_eV", _f64), ("niel_eV", _f64), ("lindhard_yield", _f64),
+                ("n_pairs_true", _u64), ("n_pairs_sampled", _u64), ("n_phonons_true", _u64),
+                ("n_phonons_sampled", _u64), ("charge_weight", _f64), ("phonon_weight", _f64),
+                ("prompt_phonon_eV", _f64)]
+
+
+class PrimaryStepC(C.Structure):
+    _fields_ = [("track_id", _i32), ("is_charged", _i32), ("start_pos", _f64 * 3), ("end_pos", _f64 * 3),
+                ("time_s", _f64), ("edep_eV", _f64), ("eniel_eV", _f64), ("hit_boundary", _i32),
+                ("track_stopped", _i32)]
+
+
+_U64x4 = _u64 * 4
+
 _SIG = {
     "cmpmc_abi_sizes": (_i32, [C.POINTER(C.c_size_t), _i32]),
     "cmpmc_crystal_config_germanium": (None, [C.POINTER(CrystalConfigC)]),
@@ -211,6 +233,19 @@ _SIG = {
     "cmpmc_mesh_field_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
     "cmpmc_mesh_potential_at": (_i32, [C.c_void_p, C.POINTER(_f64), C.POINTER(_i32), C.POINTER(_f64)]),
     "cmpmc_gpu_set_mesh": (_i32, [C.c_void_p, C.c_void_p]),
+    "cmpmc_partition_options_default": (None, [C.POINTER(PartitionOptionsC)]),
+    "cmpmc_ionization_yield": (_f64, [C.POINTER(CrystalConfigC), _i32, _f64, C.POINTER(PartitionOptionsC)]),
+    "cmpmc_lindhard_yield": (_f64, [C.POINTER(CrystalConfigC), _f64, _f64, _f64]),
+    "cmpmc_sample_fano_binomial": (_u64, [_f64, _f64, _U64x4]),
+    "cmpmc_partition_deposit": (_i32, [C.c_void_p, C.POINTER(_f64), _f64, _f64, _i32, C.POINTER(PartitionOptionsC),
+                                       _U64x4, C.c_void_p, _u64, C.POINTER(_u64), C.c_void_p, _u64,
+                                       C.POINTER(_u64), C.POINTER(PartitionResultC)]),
+    "cmpmc_hit_merger_create": (_i32, [C.c_void_p, _f64, C.POINTER(PartitionOptionsC), C.POINTER(C.c_void_p)]),
+    "cmpmc_hit_merger_destroy": (None, [C.c_void_p]),
+    "cmpmc_hit_merger_process_steps": (_i32, [C.c_void_p, C.POINTER(PrimaryStepC), _u64, _U64x4, C.POINTER(_u64)]),
+    "cmpmc_hit_merger_flush": (_i32, [C.c_void_p, _U64x4, C.POINTER(PartitionResultC)]),
+    "cmpmc_hit_merger_take": (_i32, [C.c_void_p, C.c_void_p, _u64, C.POINTER(_u64), C.c_void_p, _u64,
+                                     C.POINTER(_u64)]),
     "cmpmc_mesh2d_create": (_i32, [C.c_void_p, C.c_void_p, _u64, C.c_void_p, _u64, _i32, C.POINTER(C.c_void_p)]),
     "cmpmc_mesh2d_build_grid": (_i32, [_f64, _f64, _f64, _f64, _i32, _i32, C.c_void_p, C.c_void_p, _i32,
                                        C.POINTER(C.c_void_p)]),

@@ -35,6 +35,7 @@ SOURCES = {
     "lattice_host.cpp": [],
     "host.cpp": [],
     "mesh_host.cpp": [],
+    "partition_host.cpp": [],
     "kaplan_lut.cpp": [],
     "transport_plain.cu": ["--fmad=false"],
     # FP32 intrinsics for the batched phonon kernels (about 3 % faster; the chi^2 parity and

@@ -226,177 +226,8 @@ struct Counts {
     uint64_t phonons, charges;
 };
 
-// ---- recoil workloads: EnergyPartition::partition_deposit (energy_partition.hpp:78-167) ----
-
-// Rng::normal (core/rng.hpp:71-75)
-double rng_normal(Rng& rng) {
-    const double u1 = rng.uniform();
-    const double u2 = rng.uniform();
-    return std::sqrt(-2.0 * std::log(u1)) * std::cos(kTwoPi * u2);
-}
-
-// detail::choose_binom / pdf_binomial (charge/niel_models.hpp:178-198)
-double choose_binom(int64_t n, int64_t x) {
-    if (x > n / 2) x = n - x;
-    if (x < 0) return 0.0;
-    if (x == 0) return 1.0;
-    if (x == 1) return static_cast<double>(n);
-    double c = 1.0;
-    for (int64_t k = 1; k <= x; ++k) c *= static_cast<double>(n - k + 1) / static_cast<double>(k);
-    return c;
-}
-
-double pdf_binomial(int64_t x, int64_t n, double p) {
-    if (x > n || x < 0 || p <= 0.0 || p > 1.0) return 0.0;
-    if (p == 1.0) return (x == n) ? 1.0 : 0.0;
-    const double lnbin = std::log(p) * static_cast<double>(x) + std::log(1.0 - p) * static_cast<double>(n - x);
-    if (lnbin < -708.3) return 0.0;
-    if (lnbin > 709.7) return 1e300;
-    return choose_binom(n, x) * std::exp(lnbin);
-}
-
-// physics::sample_fano_binomial (charge/niel_models.hpp:202-263)
-uint64_t sample_fano_binomial(double mean, double fano, Rng& rng) {
-    if (mean <= 0.0) return 0;
-    if (mean <= 1.0) return 1;
-    if (std::fabs(fano - 1.0) < 1e-9) {
-        if (mean > 30.0)
-            return static_cast<uint64_t>(std::max(0.0, std::round(mean + std::sqrt(mean) * rng_normal(rng))));
-        const double lim = std::exp(-mean);
-        uint64_t k = 0;
-        double p = 1.0;
-        do {
-            ++k;
-            p *= rng.uniform();
-        } while (p > lim);
-        return k - 1;
-    }
-    const double prob = std::clamp(1.0 - fano, 1e-6, 1.0 - 1e-6);
-    const double ntry = mean / prob;
-    if (mean > 9.0 * (fano / prob) && mean > 9.0 * (prob / fano)) {
-        const double sampled = std::round(mean + std::sqrt(mean * fano) * rng_normal(rng));
-        return static_cast<uint64_t>(std::max(1.0, sampled));
-    }
-    const int64_t nlo = static_cast<int64_t>(std::floor(ntry));
-    const int64_t nhi = static_cast<int64_t>(std::ceil(ntry));
-    if (nlo == nhi) {
-        uint64_t hits = 0;
-        for (int64_t i = 0; i < nlo; ++i)
-            if (rng.uniform() < prob) ++hits;
-        return hits;
-    }
-    const double p_lo = std::min(mean / static_cast<double>(nlo), 1.0);
-    const double p_hi = std::min(mean / static_cast<double>(nhi), 1.0);
-    const double dp = (std::fabs(p_hi - p_lo) > 1e-15) ? ((prob - p_lo) / (p_hi - p_lo)) : 0.0;
-    const double pdf_max = std::max(pdf_binomial(static_cast<int64_t>(std::floor(mean)), nlo, p_lo),
-                                    pdf_binomial(static_cast<int64_t>(std::ceil(mean)), nlo, p_lo));
-    if (pdf_max <= 0.0) return static_cast<uint64_t>(std::round(mean));
-    for (int iter = 0; iter < 1000; ++iter) {
-        const int64_t pick = static_cast<int64_t>(rng.uniform() * static_cast<double>(nhi + 1));
-        const double pick_p =
-            (pdf_binomial(pick, nlo, p_lo) * (1.0 - dp) + pdf_binomial(pick, nhi, p_hi) * dp) / pdf_max;
-        if (rng.uniform() <= pick_p) return static_cast<uint64_t>(std::max<int64_t>(0, pick));
-    }
-    return static_cast<uint64_t>(std::round(mean));
-}
-
-// ChargeCloudGenerator::compute_cloud_radius (charge/charge_kernels.hpp:132-143)
-double cloud_radius(uint64_t n_pairs, const cmpmc_crystal_config& cfg) {
-    const double n_avogadro = 6.02214076e23;
-    const double vol_cell = (cfg.density > 0.0 && cfg.atomic_A > 0.0)
-                                ? (8.0 * (cfg.atomic_A * 1e-3) / (n_avogadro * cfg.density))
-                                : std::pow(0.55 * 1e-9, 3.0);
-    const double a0 = std::cbrt(vol_cell);
-    const double r_scale = 0.25 * a0;
-    return std::max(a0, r_scale * std::cbrt(static_cast<double>(n_pairs)));
-}
-
-// ChargeCloudGenerator::sample_offset (charge_kernels.hpp:145-150)
-V3 cloud_offset(double r_max, Rng& rng) {
-    if (r_max <= 0.0) return v3(0.0, 0.0, 0.0);
-    const double u = rng.uniform();
-    const double r = r_max * (1.0 - std::sqrt(std::max(0.0, 1.0 - u * u)));
-    return rng.isotropic_dir() * r;
-}
-
-// The draws of partition_deposit (electron recoil, Fano fluctuations and charge cloud on,
-// the defaults) up to the pair count, and the counts that follow from them.
-struct DepositPlan {
-    double edep;
-    uint64_t pairs_true, pairs_sampled, phonons_true, phonons_sampled;
-    double prompt_eV;
-};
-
-DepositPlan plan_deposit(const cmpmc_crystal_config& cfg, double edep, uint32_t max_pairs, uint32_t max_phonons,
-                         Rng& rng) {
-    DepositPlan d{};
-    d.edep = edep;
-    const double ionizing = edep * 1.0;  // electron recoil: yield 1
-    const double e_gap = cfg.bandgap, e_pair = cfg.pair_energy;
-    if (ionizing >= e_gap && e_pair > 0.0) {
-        const double mean_pairs = ionizing / e_pair;
-        if (mean_pairs < 1.0) {
-            d.pairs_true = static_cast<uint64_t>(std::floor(mean_pairs + rng.uniform()));
-        } else {
-            const uint64_t cap = static_cast<uint64_t>(std::floor(ionizing / e_gap));
-            d.pairs_true = std::min(cap, sample_fano_binomial(mean_pairs, cfg.fano_factor, rng));
-        }
-    }
-    const double init_ekin = 5.0 * 1e-3;
-    const double pair_energy = static_cast<double>(d.pairs_true) * (e_gap + 2.0 * init_ekin);
-    d.prompt_eV = std::max(0.0, edep - pair_energy);
-    d.pairs_sampled = std::min<uint64_t>(d.pairs_true, max_pairs);
-    const double e_debye = cfg.debye_freq * kHPlanck;
-    if (d.prompt_eV > 0.0 && e_debye > 0.0) {
-        d.phonons_true = std::max<uint64_t>(1, static_cast<uint64_t>(std::round(d.prompt_eV / e_debye)));
-        d.phonons_sampled = std::min<uint64_t>(d.phonons_true, max_phonons);
-    }
-    return d;
-}
-
-// The rest of partition_deposit: the sampled pairs (charge cloud, valley, directions) and
-// the prompt Debye phonons, drawn after plan_deposit in the reference's order.
-void fill_deposit(const Lattice& L, const cmpmc_crystal_config& cfg, const DepositPlan& d, V3 pos, double time_s,
-                  Rng& rng, cmpmc_charge_track* ch, cmpmc_phonon_track* ph) {
-    const double init_ekin = 5.0 * 1e-3;
-    if (d.pairs_true > 0) {
-        const double w = static_cast<double>(d.pairs_true) / static_cast<double>(d.pairs_sampled);
-        const uint64_t nv = static_cast<uint64_t>(std::max(1, L.n_valleys));
-        const double r_cloud = cloud_radius(d.pairs_true, cfg);
-        for (uint64_t i = 0; i < d.pairs_sampled; ++i) {
-            const V3 pp = pos + cloud_offset(r_cloud, rng);
-            const int valley = static_cast<int>(static_cast<uint16_t>(rng.next_u64() % nv));
-            const V3 de = rng.isotropic_dir();
-            Charge e = make_charge(L, 1, pp, de, init_ekin, valley, time_s);
-            e.w = w;
-            const V3 dh = rng.isotropic_dir();
-            Charge h = make_charge(L, 2, pp, dh, init_ekin, 0, time_s);
-            h.w = w;
-            charge_to_record(e, ch[2 * i]);
-            charge_to_record(h, ch[2 * i + 1]);
-        }
-    }
-    if (d.phonons_sampled > 0) {
-        const double w = static_cast<double>(d.phonons_true) / static_cast<double>(d.phonons_sampled);
-        const double e_single = d.prompt_eV / static_cast<double>(d.phonons_true);
-        for (uint64_t i = 0; i < d.phonons_sampled; ++i) {
-            const int mode = sample_dos_mode(L, rng);
-            const V3 k = rng.isotropic_dir();
-            const Kin kin = map_k_to_vg(L, mode, k);
-            Track t;
-            t.pos = pos;
-            t.k = k;  // the reference stores the drawn direction as is (no unit())
-            t.vg = kin.vg_dir;
-            t.E = e_single;
-            t.vmag = kin.vg_mag;
-            t.t = time_s;
-            t.w = w;
-            t.bounces = 0;
-            t.mode = mode;
-            track_to_record(t, ph[i]);
-        }
-    }
-}
+// ---- recoil workloads: EnergyPartition::partition_deposit (partition_host.cpp) with the
+// electron-recoil defaults and the pair cap of the recoil batch ----
 
 bool is_recoil(int wl) { return wl == CMPMC_WL_RECOIL || wl == CMPMC_WL_RECOIL_LIGHT; }
 
@@ -404,13 +235,19 @@ constexpr uint32_t kRecoilMaxPairs = 4096;
 constexpr uint32_t kRecoilMaxPhonons = 5000;      // PartitionOptions::max_sampled_phonons default
 constexpr uint32_t kRecoilLightMaxPhonons = 20;
 
+cmpmc_partition_options recoil_options(int wl) {
+    cmpmc_partition_options o = default_partition_options();
+    o.max_sampled_pairs = kRecoilMaxPairs;
+    o.max_sampled_phonons = (wl == CMPMC_WL_RECOIL) ? kRecoilMaxPhonons : kRecoilLightMaxPhonons;
+    return o;
+}
+
 // First draws of a recoil event: deposit energy, origin, then the pair count.
-DepositPlan recoil_plan(int wl, const cmpmc_crystal_config& cfg, const cmpmc_detector& det, Rng& rng, V3& pos) {
+PartitionPlan recoil_plan(int wl, const cmpmc_crystal_config& cfg, const cmpmc_detector& det, Rng& rng, V3& pos) {
     const double u = rng.uniform();
     const double edep = (wl == CMPMC_WL_RECOIL) ? 10.0 * std::pow(10.0, 3.0 * u) : 10.0 * std::pow(10.0, u);
     pos = uniform_origin(det.radius, det.half_z, rng);
-    return plan_deposit(cfg, edep, kRecoilMaxPairs,
-                        (wl == CMPMC_WL_RECOIL) ? kRecoilMaxPhonons : kRecoilLightMaxPhonons, rng);
+    return plan_partition(cfg, edep, false, recoil_options(wl), rng);
 }
 
 Counts counts_of(int wl, uint64_t ev) {
@@ -432,8 +269,8 @@ void gen_event(int wl, const Lattice& L, const cmpmc_crystal_config& cfg, const 
         case CMPMC_WL_RECOIL:
         case CMPMC_WL_RECOIL_LIGHT: {
             V3 pos;
-            const DepositPlan d = recoil_plan(wl, cfg, det, rng, pos);
-            fill_deposit(L, cfg, d, pos, 0.0, rng, ch, ph);
+            const PartitionPlan d = recoil_plan(wl, cfg, det, rng, pos);
+            fill_partition(L, cfg, d, recoil_options(wl), pos, 0.0, rng, ch, ph);
             injected += d.edep;
             break;
         }
@@ -604,7 +441,7 @@ int cmpmc_generate(const cmpmc_lattice* lat, const cmpmc_detector* det, int work
             if (is_recoil(workload)) {
                 Rng rng = Rng::for_stream(seed, first_event + i);
                 V3 pos;
-                const DepositPlan d = recoil_plan(workload, lat->cfg, *det, rng, pos);
+                const PartitionPlan d = recoil_plan(workload, lat->cfg, *det, rng, pos);
                 cnt[i] = {d.phonons_sampled, 2 * d.pairs_sampled};
             } else {
                 cnt[i] = counts_of(workload, first_event + i);

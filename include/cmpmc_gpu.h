@@ -313,6 +313,77 @@ int cmpmc_mesh2d_info(const cmpmc_mesh2d* mesh, uint64_t* n_vertices, uint64_t* 
 int cmpmc_mesh2d_field_at(const cmpmc_mesh2d* mesh, const double p[3], int32_t* hint, double E[3]);
 int cmpmc_mesh2d_potential_at(const cmpmc_mesh2d* mesh, const double p[3], int32_t* hint, double* V);
 
+/* ---- energy partition and primary-step merging (charge/energy_partition.hpp, ----------
+ * ---- charge/niel_models.hpp): the input side of the transport, on the host -------- */
+enum {
+    CMPMC_NIEL_LINDHARD    = 0,  /* NIELModel (niel_models.hpp:28-34) */
+    CMPMC_NIEL_LEWIN_SMITH = 1,
+    CMPMC_NIEL_SARKIS      = 2,
+    CMPMC_NIEL_IMPACT_TUNL = 3,
+    CMPMC_NIEL_EMPIRICAL   = 4
+};
+/* PartitionOptions with EmpiricalNIELParams (energy_partition.hpp:22-29, niel_models.hpp:36-43) */
+typedef struct cmpmc_partition_options {
+    int32_t niel_model;
+    int32_t use_fano_fluctuations;
+    int32_t use_charge_cloud;
+    uint32_t max_sampled_pairs;
+    uint32_t max_sampled_phonons;
+    int32_t emp_energy_dependent_k;
+    double emp_k_fixed, emp_k_low, emp_k_high, emp_e_low_eV, emp_e_high_eV;
+} cmpmc_partition_options;
+/* EnergyPartition::Result (energy_partition.hpp:36-48) */
+typedef struct cmpmc_partition_result {
+    double total_edep_eV, ionizing_eV, niel_eV, lindhard_yield;
+    uint64_t n_pairs_true, n_pairs_sampled, n_phonons_true, n_phonons_sampled;
+    double charge_weight, phonon_weight, prompt_phonon_eV;
+} cmpmc_partition_result;
+void cmpmc_partition_options_default(cmpmc_partition_options* opts);
+/* physics::compute_ionization_yield (niel_models.hpp:161-176); opts supplies the empirical
+ * parameters (NULL: defaults). */
+double cmpmc_ionization_yield(const cmpmc_crystal_config* cfg, int niel_model, double energy_eV,
+                              const cmpmc_partition_options* opts);
+/* EnergyPartition::lindhard_ionization_yield(E, z1, a1) (energy_partition.hpp:53-73) */
+double cmpmc_lindhard_yield(const cmpmc_crystal_config* cfg, double energy_eV, double z1, double a1);
+/* physics::sample_fano_binomial (niel_models.hpp:202-263), drawing from rng_state */
+uint64_t cmpmc_sample_fano_binomial(double mean, double fano, uint64_t rng_state[4]);
+/* EnergyPartition::partition_deposit (energy_partition.hpp:78-167): writes 2 n_pairs_sampled
+ * carriers (e-, h+ interleaved) and n_phonons_sampled prompt phonons, drawing from
+ * rng_state. *n_charges / *n_phonons receive the counts; if a capacity is short the call
+ * returns CMPMC_ERR_CAPACITY and leaves rng_state unchanged (retry with the counts). */
+int cmpmc_partition_deposit(const cmpmc_lattice* lat, const double pos[3], double time_s, double total_edep_eV,
+                            int is_nuclear_recoil, const cmpmc_partition_options* opts, uint64_t rng_state[4],
+                            cmpmc_charge_track* charges, uint64_t charge_cap, uint64_t* n_charges,
+                            cmpmc_phonon_track* phonons, uint64_t phonon_cap, uint64_t* n_phonons,
+                            cmpmc_partition_result* result);
+/* PrimaryStepInput (energy_partition.hpp:182-192) */
+typedef struct cmpmc_primary_step {
+    int32_t track_id;
+    int32_t is_charged;
+    double start_pos[3];
+    double end_pos[3];
+    double time_s, edep_eV, eniel_eV;
+    int32_t hit_boundary, track_stopped;
+} cmpmc_primary_step;
+/* HitMerger (energy_partition.hpp:229-323). The merged secondaries accumulate in the
+ * merger (the reference appends them to the caller's vectors); cmpmc_hit_merger_take
+ * moves them out. The lattice must outlive the merger. */
+typedef struct cmpmc_hit_merger cmpmc_hit_merger;
+int cmpmc_hit_merger_create(const cmpmc_lattice* lat, double combining_step_length_m,
+                            const cmpmc_partition_options* opts, cmpmc_hit_merger** out);
+void cmpmc_hit_merger_destroy(cmpmc_hit_merger* merger);
+/* HitMerger::process_step for each step in order (energy_partition.hpp:236-266);
+ * *n_flushes receives how many of them flushed. */
+int cmpmc_hit_merger_process_steps(cmpmc_hit_merger* merger, const cmpmc_primary_step* steps, uint64_t n_steps,
+                                   uint64_t rng_state[4], uint64_t* n_flushes);
+/* HitMerger::flush (energy_partition.hpp:268-316) */
+int cmpmc_hit_merger_flush(cmpmc_hit_merger* merger, uint64_t rng_state[4], cmpmc_partition_result* result);
+/* Copies the accumulated carriers and phonons out and clears them (CMPMC_ERR_CAPACITY with
+ * the counts set, and nothing cleared, if a capacity is short). */
+int cmpmc_hit_merger_take(cmpmc_hit_merger* merger, cmpmc_charge_track* charges, uint64_t charge_cap,
+                          uint64_t* n_charges, cmpmc_phonon_track* phonons, uint64_t phonon_cap,
+                          uint64_t* n_phonons);
+
 /* ---- random streams (core/rng.hpp) --------------------------------------------- */
 void cmpmc_rng_for_stream(uint64_t seed, uint64_t stream, uint64_t state[4]);
 uint64_t cmpmc_rng_next_u64(uint64_t state[4]);

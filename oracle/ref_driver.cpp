@@ -35,6 +35,22 @@
 //       E = Delta (1 + 45 u) (Rng::for_stream(3, 0), sub-gap, in-table and above-table),
 //       absorb_phonon_fast(E) with the same stream; per record E, edep (f64), the count
 //       (u32) and the re-emitted energies (f64).
+//   cmpmc_ref yield <out>
+//       Ionisation yields at 400 energies 10^(7 i / 399) eV for Germanium() and Silicon():
+//       the five NIEL models (default empirical parameters), Empirical with a fixed k, and
+//       EnergyPartition::lindhard_ionization_yield(E, 2, 4); [2][7][400] doubles.
+//   cmpmc_ref partition <out>
+//       EnergyPartition::partition_deposit on the Germanium lattice for 48 deposits (case i:
+//       E = 10^(1 + 4 i / 47) eV, nuclear recoil when i is odd, pos (i, -2, 3) mm, time
+//       i ns, Rng::for_stream(8, i), at most 100 sampled pairs and 150 sampled phonons,
+//       options by i % 4: defaults / no Fano fluctuations / no charge cloud and 16 sampled
+//       pairs / Empirical yield and 7 sampled phonons);
+//       per case the Result, the record counts, the records and the final Rng state.
+//   cmpmc_ref merge <out>
+//       HitMerger(lattice, 1 mm, 64 pairs / 64 phonons) over three synthetic primary
+//       tracks of 12 steps (charged; neutral; nuclear-recoil-like), Rng::for_stream(9, 0),
+//       then a final flush: per step the process_step flag, then the records, the final
+//       Rng state.
 //   cmpmc_ref mesh2 <n_points> <out>
 //       Builds the tp2 axisymmetric (r, z) mesh and a planar (x, y) mesh
 //       (build_grid(-R, R, -R, R, 32, 32) of V = 3 (x + R) / 2R + 0.5 (y / R)^2) and writes,
@@ -509,6 +525,124 @@ int cmd_meshfile(const char* coords, const char* tets, double cu, double vu, uin
     return 0;
 }
 
+int cmd_yield(const std::string& out) {
+    FILE* f = open_or_die(out);
+    const CrystalConfig cfgs[2] = {materials::Germanium(), materials::Silicon()};
+    for (const CrystalConfig& cfg : cfgs) {
+        const CrystalLattice lat(cfg);
+        const EnergyPartition part(lat);
+        physics::EmpiricalNIELParams fixed;
+        fixed.energy_dependent_k = false;
+        for (int col = 0; col < 7; ++col)
+            for (int i = 0; i < 400; ++i) {
+                const double E = std::pow(10.0, 7.0 * i / 399.0);
+                double y;
+                if (col < 5) y = physics::compute_ionization_yield(static_cast<physics::NIELModel>(col), E, cfg);
+                else if (col == 5) y = physics::compute_ionization_yield(physics::NIELModel::Empirical, E, cfg, fixed);
+                else y = part.lindhard_ionization_yield(E, 2.0, 4.0);
+                std::fwrite(&y, 8, 1, f);
+            }
+    }
+    std::fclose(f);
+    return 0;
+}
+
+void write_result(FILE* f, const EnergyPartition::Result& r) {
+    const double d[4] = {r.total_edep_eV, r.ionizing_eV, r.niel_eV, r.lindhard_yield};
+    const uint64_t n[4] = {r.n_pairs_true, r.n_pairs_sampled, r.n_phonons_true, r.n_phonons_sampled};
+    const double w[3] = {r.charge_weight, r.phonon_weight, r.prompt_phonon_eV};
+    std::fwrite(d, 8, 4, f);
+    std::fwrite(n, 8, 4, f);
+    std::fwrite(w, 8, 3, f);
+}
+
+void write_records(FILE* f, const std::vector<ChargeTrack>& ch, const std::vector<PhononTrack>& ph, const Rng& rng) {
+    const uint64_t n[2] = {ch.size(), ph.size()};
+    std::fwrite(n, 8, 2, f);
+    static_assert(sizeof(ChargeTrack) == 128 && sizeof(PhononTrack) == 128, "record layout");
+    if (!ch.empty()) std::fwrite(ch.data(), sizeof(ChargeTrack), ch.size(), f);
+    if (!ph.empty()) std::fwrite(ph.data(), sizeof(PhononTrack), ph.size(), f);
+    Rng copy = rng;
+    const uint64_t next = copy.next_u64();  // the stream position after the call
+    std::fwrite(&next, 8, 1, f);
+}
+
+int cmd_partition(const std::string& out) {
+    const CrystalLattice lattice(materials::Germanium());
+    const EnergyPartition part(lattice);
+    FILE* f = open_or_die(out);
+    for (int i = 0; i < 48; ++i) {
+        PartitionOptions o;
+        o.max_sampled_pairs = 100;
+        o.max_sampled_phonons = 150;
+        if (i % 4 == 1) o.use_fano_fluctuations = false;
+        if (i % 4 == 2) {
+            o.use_charge_cloud = false;
+            o.max_sampled_pairs = 16;
+        }
+        if (i % 4 == 3) {
+            o.niel_model = physics::NIELModel::Empirical;
+            o.max_sampled_phonons = 7;
+        }
+        const double E = std::pow(10.0, 1.0 + 4.0 * i / 47.0);
+        Rng rng = Rng::for_stream(8, static_cast<uint64_t>(i));
+        std::vector<ChargeTrack> ch;
+        std::vector<PhononTrack> ph;
+        const Vec3 pos{1e-3 * i, -2e-3, 3e-3};
+        const EnergyPartition::Result r = part.partition_deposit(pos, 1e-9 * i, E, (i % 2) == 1, ch, ph, rng, o);
+        write_result(f, r);
+        write_records(f, ch, ph, rng);
+    }
+    std::fclose(f);
+    return 0;
+}
+
+// The synthetic primary tracks of `merge` (also restated by the tests)
+std::vector<PrimaryStepInput> merge_steps() {
+    std::vector<PrimaryStepInput> steps;
+    for (int t = 0; t < 3; ++t) {
+        Vec3 p{-5e-3 + 4e-3 * t, 1e-3 * t, -4e-3};
+        for (int k = 0; k < 12; ++k) {
+            PrimaryStepInput s;
+            s.track_id = t + 1;
+            s.start_pos = p;
+            const double len = 1e-4 * (2 + (k * 7 + t * 3) % 6);
+            p = p + Vec3{0.6 * len, 0.3 * len, 0.74161984870956632 * len};
+            s.end_pos = p;
+            s.time_s = 1e-12 * (10 * t + k);
+            s.edep_eV = (t == 2) ? 20.0 * (k % 3) : 40.0 + 15.0 * ((k * 5 + t) % 7);
+            s.eniel_eV = (t == 2) ? 300.0 + 50.0 * (k % 4) : 0.0;
+            s.is_charged = (t != 1);
+            s.hit_boundary = (k == 7 && t == 0);
+            s.track_stopped = (k == 11);
+            steps.push_back(s);
+        }
+    }
+    return steps;
+}
+
+int cmd_merge(const std::string& out) {
+    const CrystalLattice lattice(materials::Germanium());
+    PartitionOptions o;
+    o.max_sampled_pairs = 64;
+    o.max_sampled_phonons = 64;
+    HitMerger merger(lattice, 1.0 * units::mm, o);
+    Rng rng = Rng::for_stream(9, 0);
+    std::vector<ChargeTrack> ch;
+    std::vector<PhononTrack> ph;
+    FILE* f = open_or_die(out);
+    const std::vector<PrimaryStepInput> steps = merge_steps();
+    for (const PrimaryStepInput& s : steps) {
+        const uint8_t ready = merger.process_step(s, ch, ph, rng) ? 1 : 0;
+        std::fwrite(&ready, 1, 1, f);
+    }
+    const EnergyPartition::Result r = merger.flush(ch, ph, rng);
+    write_result(f, r);
+    write_records(f, ch, ph, rng);
+    std::fclose(f);
+    return 0;
+}
+
 int cmd_mesh(uint64_t n, const std::string& out) {
     const DetectorModel det;
     const geometry::TriLinearMesh3D mesh = recoil_mesh(det.solid);
@@ -548,6 +682,9 @@ int main(int argc, char** argv) {
     if (cmd == "meshfile" && argc == 8)
         return cmd_meshfile(argv[2], argv[3], std::strtod(argv[4], nullptr), std::strtod(argv[5], nullptr),
                             std::strtoull(argv[6], nullptr, 10), argv[7]);
+    if (cmd == "yield" && argc == 3) return cmd_yield(argv[2]);
+    if (cmd == "partition" && argc == 3) return cmd_partition(argv[2]);
+    if (cmd == "merge" && argc == 3) return cmd_merge(argv[2]);
     if (cmd == "mesh2" && argc == 4) return cmd_mesh2(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "mesh" && argc == 4) return cmd_mesh(std::strtoull(argv[2], nullptr, 10), argv[3]);
     if (cmd == "rng" && argc == 5)

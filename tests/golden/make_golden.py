@@ -100,6 +100,8 @@ def main() -> None:
             np.savez_compressed(os.path.join(HERE, "mesh2d.npz"), points=rec[:, 0:3], axisym_field=rec[:, 3:6],
                                 axisym_potential=rec[:, 6], planar_field=rec[:, 7:10], planar_potential=rec[:, 10],
                                 **{k: v for k, v in info.items()})
+        if want("partition"):
+            _partition(tmp)
         if want("meshfile"):
             _mesh_files(tmp)
         if want("mask"):
@@ -147,6 +149,73 @@ def main() -> None:
         f.write("Generated by tests/golden/make_golden.py from the unmodified reference CMPMC\n"
                 "(oracle/_ref, g++ -O3 -std=c++20, no -march=native).\n"
                 f"host libm: {gl}\n")
+
+
+RESULT_DTYPE = np.dtype([("total_edep_eV", "<f8"), ("ionizing_eV", "<f8"), ("niel_eV", "<f8"),
+                         ("lindhard_yield", "<f8"), ("n_pairs_true", "<u8"), ("n_pairs_sampled", "<u8"),
+                         ("n_phonons_true", "<u8"), ("n_phonons_sampled", "<u8"), ("charge_weight", "<f8"),
+                         ("phonon_weight", "<f8"), ("prompt_phonon_eV", "<f8")])
+
+
+def _zero_padding(b: bytes, dtype) -> bytes:
+    """The reference leaves the padding of its records uninitialised: zero it."""
+    a = np.frombuffer(b, dtype=dtype).copy()
+    for name in a.dtype.names:
+        if name.startswith("_pad"):
+            a[name] = 0
+    return a.tobytes()
+
+
+def _read_records(raw: bytes, off: int):
+    from cmpmc_b200._ffi import CHARGE_DTYPE, PHONON_DTYPE
+    nc, nph = np.frombuffer(raw, dtype="<u8", count=2, offset=off)
+    off += 16
+    ch = _zero_padding(raw[off:off + 128 * int(nc)], CHARGE_DTYPE)
+    off += 128 * int(nc)
+    ph = _zero_padding(raw[off:off + 128 * int(nph)], PHONON_DTYPE)
+    off += 128 * int(nph)
+    nxt = int(np.frombuffer(raw, dtype="<u8", count=1, offset=off)[0])
+    return ch, ph, nxt, off + 8
+
+
+def _partition(tmp: str) -> None:
+    """Yields of the five NIEL models (Ge and Si), 48 partition_deposit cases and a
+    HitMerger run of the reference (oracle/ref_driver.cpp `yield`, `partition`, `merge`)."""
+    path = os.path.join(tmp, "yield.bin")
+    subprocess.run([REF, "yield", path], check=True)
+    y = np.fromfile(path, dtype=np.float64).reshape(2, 7, 400)
+    path = os.path.join(tmp, "partition.bin")
+    subprocess.run([REF, "partition", path], check=True)
+    raw = open(path, "rb").read()
+    off = 0
+    res, nc, nph, nxt, h_ch, h_ph, full_ch, full_ph = [], [], [], [], [], [], [], []
+    for i in range(48):
+        res.append(np.frombuffer(raw, dtype=RESULT_DTYPE, count=1, offset=off)[0])
+        off += RESULT_DTYPE.itemsize
+        ch, ph, n, off = _read_records(raw, off)
+        nc.append(len(ch) // 128)
+        nph.append(len(ph) // 128)
+        nxt.append(n)
+        h_ch.append(hashlib.sha256(ch).hexdigest())
+        h_ph.append(hashlib.sha256(ph).hexdigest())
+        if i < 12:
+            full_ch.append(ch)
+            full_ph.append(ph)
+    assert off == len(raw)
+    path = os.path.join(tmp, "merge.bin")
+    subprocess.run([REF, "merge", path], check=True)
+    raw = open(path, "rb").read()
+    flags = np.frombuffer(raw, dtype=np.uint8, count=36)
+    m_res = np.frombuffer(raw, dtype=RESULT_DTYPE, count=1, offset=36)
+    m_ch, m_ph, m_next, off = _read_records(raw, 36 + RESULT_DTYPE.itemsize)
+    assert off == len(raw)
+    np.savez_compressed(os.path.join(HERE, "partition.npz"), yields=y, results=np.array(res, dtype=RESULT_DTYPE),
+                        n_charges=np.array(nc, dtype=np.uint64), n_phonons=np.array(nph, dtype=np.uint64),
+                        next_u64=np.array(nxt, dtype=np.uint64), sha_charges=np.array(h_ch), sha_phonons=np.array(h_ph),
+                        charges_0_11=np.frombuffer(b"".join(full_ch), dtype=np.uint8),
+                        phonons_0_11=np.frombuffer(b"".join(full_ph), dtype=np.uint8),
+                        merge_flags=flags, merge_result=m_res, merge_charges=np.frombuffer(m_ch, dtype=np.uint8),
+                        merge_phonons=np.frombuffer(m_ph, dtype=np.uint8), merge_next_u64=np.uint64(m_next))
 
 
 def _mesh_files(tmp: str) -> None:
