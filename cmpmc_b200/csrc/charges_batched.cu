@@ -454,7 +454,11 @@ __global__ void __launch_bounds__(128, 4) k_charges_fp32(const __grid_constant__
                 int ch_id = -1;
                 bool absorb = true;
                 if (s.n_pads > 0) {
-                    ch_id = mask_call(s.pads, s.n_pads, c.pos.x, c.pos.y, &k.g);
+                    // the out-of-line call gets a copy: only it has its address taken, so
+                    // the carrier state stays in registers
+                    R128 g_c = k.g;
+                    ch_id = mask_call(s.pads, s.n_pads, c.pos.x, c.pos.y, &g_c);
+                    k.g = g_c;
                     absorb = ch_id >= 0;
                 }
                 const float k_perp = -fdot(c.p * (1.0f / kHbarCF), bh.n);

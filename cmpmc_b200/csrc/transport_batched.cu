@@ -116,10 +116,33 @@ __device__ __forceinline__ void pop_track(const EntryOf<kAdj>* stk, uint32_t& n,
     t.t = g.t;
 }
 
-// compact per-primary counters (a primary's lineage stays far below 2^32 steps)
+// Per-unit counters of a thread (a primary's lineage stays far below 2^32 steps). They
+// live in shared memory, one structure of arrays per block (counter c of thread t at
+// [c][t]: consecutive threads hit consecutive banks), so the step loop's registers hold
+// the track state instead of spilling it.
+constexpr int kMaxBlock = 128;  // every kernel running the step loop has __launch_bounds__(128)
+enum { kCSteps = 0, kCIso, kCPoly, kCTT, kCLT, kCRefl, kCDown, kCHits, kCKilled, kNCnt };
 struct UStats {
-    uint32_t steps, iso, poly, tt, lt, refl, down, hits, killed;
-    double dep, esc;
+    uint32_t* c;  // &counters[0][threadIdx.x]
+    double* f;    // &ledger[0][threadIdx.x]: deposited, then escaped or killed
+    __device__ __forceinline__ uint32_t& at(int i) const { return c[i * kMaxBlock]; }
+    __device__ __forceinline__ uint32_t& steps() const { return at(kCSteps); }
+    __device__ __forceinline__ uint32_t& iso() const { return at(kCIso); }
+    __device__ __forceinline__ uint32_t& poly() const { return at(kCPoly); }
+    __device__ __forceinline__ uint32_t& tt() const { return at(kCTT); }
+    __device__ __forceinline__ uint32_t& lt() const { return at(kCLT); }
+    __device__ __forceinline__ uint32_t& refl() const { return at(kCRefl); }
+    __device__ __forceinline__ uint32_t& down() const { return at(kCDown); }
+    __device__ __forceinline__ uint32_t& hits() const { return at(kCHits); }
+    __device__ __forceinline__ uint32_t& killed() const { return at(kCKilled); }
+    __device__ __forceinline__ double& dep() const { return f[0]; }
+    __device__ __forceinline__ double& esc() const { return f[kMaxBlock]; }
+    __device__ __forceinline__ void clear() const {
+#pragma unroll
+        for (int i = 0; i < kNCnt; ++i) at(i) = 0;
+        dep() = 0.0;
+        esc() = 0.0;
+    }
 };
 
 // Kaplan cascade out of line: its FP64 registers stay out of the step loop
@@ -162,7 +185,7 @@ __device__ __noinline__ double surrogate_call(const Surface* s, double E, double
 // anharmonic decay of an L phonon (engine.hpp:938-988), FP32 angles
 template <bool kAdj>
 __device__ __noinline__ void decay_call(const FLat* Lp, TrackOf<kAdj>* tp, EntryOf<kAdj>* stk, uint32_t* n_stk,
-                                        uint32_t cap, unsigned* err, UStats* st, R128* gp) {
+                                        uint32_t cap, unsigned* err, const UStats* st, R128* gp) {
     const FLat& L = *Lp;
     TrackOf<kAdj>& trk = *tp;
     R128& g = *gp;
@@ -174,7 +197,7 @@ __device__ __noinline__ void decay_call(const FLat* Lp, TrackOf<kAdj>* tp, Entry
     int m1, m2;
     const float m = L.m_ratio, mm = m * m;
     if (g.u() < L.fTT) {
-        st->tt++;
+        ++st->tt();
         x = fcdf(L.cdf_tt, g);
         const float y = 1.0f - x;
         th1 = facos_clamped((1.0f - mm * y * y + mm * x * x) / (2.0f * m * x));
@@ -182,7 +205,7 @@ __device__ __noinline__ void decay_call(const FLat* Lp, TrackOf<kAdj>* tp, Entry
         m1 = ftrans(L, g);
         m2 = ftrans(L, g);
     } else {
-        st->lt++;
+        ++st->lt();
         x = fcdf(L.cdf_lt, g);
         th1 = facos_clamped((1.0f + x * x * (1.0f - mm) + 2.0f * x * mm - mm) / (2.0f * x));
         th2 = facos_clamped((1.0f - x * x + mm * (1.0f - x) * (1.0f - x)) / (2.0f * m * (1.0f - x)));
@@ -225,23 +248,23 @@ __global__ void __launch_bounds__(128) k_unit_event(const uint64_t* __restrict__
 
 __device__ __forceinline__ void write_unit(const RunArgs& a, uint64_t unit, const UStats& st, uint32_t n_hits) {
     cmpmc_sim_stats& o = a.ev_stats[unit];
-    o.total_steps = st.steps;
-    o.isotope_scatters = st.iso;
-    o.polycrystal_scatters = st.poly;
-    o.decays_L_to_TT = st.tt;
-    o.decays_L_to_LT = st.lt;
-    o.surface_refls = st.refl;
-    o.surface_downconversions = st.down;
-    o.sensor_hits = st.hits;
-    o.killed_tracks = st.killed;
+    o.total_steps = st.steps();
+    o.isotope_scatters = st.iso();
+    o.polycrystal_scatters = st.poly();
+    o.decays_L_to_TT = st.tt();
+    o.decays_L_to_LT = st.lt();
+    o.surface_refls = st.refl();
+    o.surface_downconversions = st.down();
+    o.sensor_hits = st.hits();
+    o.killed_tracks = st.killed();
     o.charge_steps = 0; o.luke_phonons_emitted = 0; o.intervalley_scatters = 0; o.charges_trapped = 0;
     o.trap_ionizations = 0; o.charge_surface_refls = 0; o.charges_collected = 0;
     o.total_luke_phonon_eV = 0.0; o.charge_recomb_edep_eV = 0.0;
     o.sc_pair_breakings = 0; o.qp_diffusion_steps = 0; o.qp_phonons_radiated = 0; o.qp_recombinations = 0;
     o.qp_local_traps = 0;
     o.total_injected_eV = 0.0;
-    o.total_deposited_eV = st.dep;
-    o.escaped_or_killed_eV = st.esc;
+    o.total_deposited_eV = st.dep();
+    o.escaped_or_killed_eV = st.esc();
     a.ev_nhits[unit] = a.keep_hits ? n_hits : 0;
 }
 
@@ -253,20 +276,19 @@ __device__ __forceinline__ void add_u64(unsigned long long* p, uint32_t v) {
 __device__ __forceinline__ void add_f64(double* p, double v) {
     if (v != 0.0) atomicAdd(p, v);
 }
-__device__ __noinline__ void sink_unit(const RunArgs* a, uint32_t ev, const UStats* stp) {
-    const UStats& st = *stp;
+__device__ __noinline__ void sink_unit(const RunArgs* a, uint32_t ev, const UStats st) {
     cmpmc_sim_stats& o = a->ev_stats[ev];
-    add_u64(reinterpret_cast<unsigned long long*>(&o.total_steps), st.steps);
-    add_u64(reinterpret_cast<unsigned long long*>(&o.isotope_scatters), st.iso);
-    add_u64(reinterpret_cast<unsigned long long*>(&o.polycrystal_scatters), st.poly);
-    add_u64(reinterpret_cast<unsigned long long*>(&o.decays_L_to_TT), st.tt);
-    add_u64(reinterpret_cast<unsigned long long*>(&o.decays_L_to_LT), st.lt);
-    add_u64(reinterpret_cast<unsigned long long*>(&o.surface_refls), st.refl);
-    add_u64(reinterpret_cast<unsigned long long*>(&o.surface_downconversions), st.down);
-    add_u64(reinterpret_cast<unsigned long long*>(&o.sensor_hits), st.hits);
-    add_u64(reinterpret_cast<unsigned long long*>(&o.killed_tracks), st.killed);
-    add_f64(&o.total_deposited_eV, st.dep);
-    add_f64(&o.escaped_or_killed_eV, st.esc);
+    add_u64(reinterpret_cast<unsigned long long*>(&o.total_steps), st.steps());
+    add_u64(reinterpret_cast<unsigned long long*>(&o.isotope_scatters), st.iso());
+    add_u64(reinterpret_cast<unsigned long long*>(&o.polycrystal_scatters), st.poly());
+    add_u64(reinterpret_cast<unsigned long long*>(&o.decays_L_to_TT), st.tt());
+    add_u64(reinterpret_cast<unsigned long long*>(&o.decays_L_to_LT), st.lt());
+    add_u64(reinterpret_cast<unsigned long long*>(&o.surface_refls), st.refl());
+    add_u64(reinterpret_cast<unsigned long long*>(&o.surface_downconversions), st.down());
+    add_u64(reinterpret_cast<unsigned long long*>(&o.sensor_hits), st.hits());
+    add_u64(reinterpret_cast<unsigned long long*>(&o.killed_tracks), st.killed());
+    add_f64(&o.total_deposited_eV, st.dep());
+    add_f64(&o.escaped_or_killed_eV, st.esc());
 }
 
 enum { kSrcInput = 0, kSrcQueue = 1 };
@@ -298,7 +320,9 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
 
     TrackOf<kAdj> trk;
     R128 g;
-    UStats st;
+    __shared__ uint32_t s_cnt[kNCnt][kMaxBlock];
+    __shared__ double s_led[2][kMaxBlock];
+    const UStats st{&s_cnt[0][threadIdx.x], &s_led[0][threadIdx.x]};
     uint32_t n_hits = 0;
     uint64_t unit = ~0ull;
     uint32_t ev_cur = 0;  // event of the unit in flight
@@ -312,7 +336,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 live = true;
             } else {
                 if (unit != ~0ull) {
-                    if constexpr (kSink) sink_unit(&a, ev_cur, &st);
+                    if constexpr (kSink) sink_unit(&a, ev_cur, st);
                     else write_unit(a, unit, st, n_hits);
                 }
                 unit = atomicAdd(a.next_work, 1ull);
@@ -335,7 +359,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                     trk.t = q.t;
                     trk.w = q.w;
                     trk.bounces = q.pad;
-                    st = UStats{0, 0, 0, 0, 0, 0, 0, 0, 0, 0.0, 0.0};
+                    st.clear();
                     n_hits = 0;
                     live = true;
                     continue;
@@ -363,14 +387,14 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
 #pragma unroll
                     for (int c = 0; c < kAdjCols; ++c) row[c] = 0.0;
                 }
-                st = UStats{0, 0, 0, 0, 0, 0, 0, 0, 0, 0.0, 0.0};
+                st.clear();
                 n_hits = 0;
                 live = true;
             }
         }
         if (trk.E < min_E || trk.bounces >= D.max_bounces) {
-            st.killed++;
-            st.esc += trk.E * trk.w;
+            ++st.killed();
+            st.esc() += trk.E * trk.w;
             live = false;
             continue;
         }
@@ -378,7 +402,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
             if (g.u() < static_cast<float>(D.rr_survival)) {
                 trk.w /= static_cast<float>(D.rr_survival);
             } else {
-                st.killed++;
+                ++st.killed();
                 live = false;
                 continue;
             }
@@ -407,7 +431,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 continue;
             }
         }
-        st.steps++;
+        ++st.steps();
         const float nu = static_cast<float>(trk.E) * L.inv_h_thz;
         const float nu2 = nu * nu;
         const float r_iso = L.b4 * (nu2 * nu2);
@@ -432,13 +456,23 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
             const float u_proc = g.u() * r_tot;
             if (r_down > 0.0f && u_proc < r_down) {
                 if constexpr (kAdj) trk.s[1] += 1.0f;  // density of a decay: r_down exp(-r_tot t)
-                decay_call<kAdj>(&L, &trk, stk, &n_stk, a.stack_cap, &err, &st, &g);
+                // the out-of-line call works on copies: only they have their address
+                // taken, so the loop's own track and generator stay in registers
+                TrackOf<kAdj> t_c = trk;
+                R128 g_c = g;
+                uint32_t n_c = n_stk;
+                unsigned e_c = err;
+                decay_call<kAdj>(&L, &t_c, stk, &n_c, a.stack_cap, &e_c, &st, &g_c);
+                trk = t_c;
+                g = g_c;
+                n_stk = n_c;
+                err = e_c;
             } else {
                 if (u_proc < r_down + r_iso) {
-                    st.iso++;
+                    ++st.iso();
                     if constexpr (kAdj) trk.s[0] += 1.0f;
                 } else {
-                    st.poly++;
+                    ++st.poly();
                 }
                 trk.mode = fdos(L, g.u());
                 sample = 0;
@@ -450,7 +484,9 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
             int ch_id = -1;
             bool active_pad = true;
             if (s.n_pads > 0) {  // electrode mask (engine.hpp:483-488)
-                ch_id = mask_call(s.pads, s.n_pads, trk.pos.x, trk.pos.y, &g);
+                R128 g_c = g;
+                ch_id = mask_call(s.pads, s.n_pads, trk.pos.x, trk.pos.y, &g_c);
+                g = g_c;
                 active_pad = ch_id >= 0;
             }
             if (active_pad && s.has_film && g.u() < static_cast<float>(s.prob_abs)) {
@@ -488,16 +524,18 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
             if (enter) {
                 int n_refl = 0;
                 double edep;
+                R128 g_c = g;
                 if constexpr (kSur) {
-                    edep = s.lut_abs ? surrogate_call(&s, trk.E, refl_buf, &n_refl, kwork, &g)
-                                     : kaplan_call(&s.film, trk.E, refl_buf, &n_refl, kwork, &g);
+                    edep = s.lut_abs ? surrogate_call(&s, trk.E, refl_buf, &n_refl, kwork, &g_c)
+                                     : kaplan_call(&s.film, trk.E, refl_buf, &n_refl, kwork, &g_c);
                 } else {
-                    edep = kaplan_call(&s.film, trk.E, refl_buf, &n_refl, kwork, &g);
+                    edep = kaplan_call(&s.film, trk.E, refl_buf, &n_refl, kwork, &g_c);
                 }
+                g = g_c;
                 if (edep > 0.0) {
                     const double wedep = edep * trk.w;
-                    st.hits++;
-                    st.dep += wedep;
+                    ++st.hits();
+                    st.dep() += wedep;
                     const uint32_t local = n_hits++;
                     if constexpr (kAdj) {
                         const double tb = (trk.t - adj.t0) * adj.inv_dt;
@@ -534,7 +572,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 }
                 double sum_refl = 0.0;
                 for (int i = 0; i < n_refl; ++i) sum_refl += refl_buf[i];
-                st.esc += dmax(0.0, trk.E - edep - sum_refl) * trk.w;
+                st.esc() += dmax(0.0, trk.E - edep - sum_refl) * trk.w;
                 if (n_refl == 0) {
                     live = false;
                     continue;
@@ -560,12 +598,12 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 trk.mode = fdos(L, g.u());
                 sample = 1;
             } else if (g.u() > static_cast<float>(s.prob_refl)) {
-                st.killed++;
-                st.esc += trk.E * trk.w;
+                ++st.killed();
+                st.esc() += trk.E * trk.w;
                 live = false;
                 continue;
             } else {
-                st.refl++;
+                ++st.refl();
                 trk.pos = trk.pos + bh.n * kNudge;
                 float p_anh, p_anh_spec;
                 if (L.split_const[bh.surf]) {
@@ -578,7 +616,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 }
                 const float u_refl = g.u();
                 if (u_refl < p_anh) {
-                    st.down++;
+                    ++st.down();
                     const bool tt = g.u() < L.fTT;
                     const float x = tt ? fcdf(L.cdf_tt, g) : fcdf(L.cdf_lt, g);
                     const int m1 = tt ? ftrans(L, g) : 0;
@@ -648,7 +686,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
 }
 
 template <bool kSink, bool kSur, bool kSplit = false>
-__global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__ FLat L,
+__global__ void __launch_bounds__(128, 6) k_batched_fp32(const __grid_constant__ FLat L,
                                                          const __grid_constant__ Detector D,
                                                          const __grid_constant__ RunArgs a,
                                                          const uint32_t* __restrict__ unit_event) {
@@ -658,7 +696,7 @@ __global__ void __launch_bounds__(128, 8) k_batched_fp32(const __grid_constant__
 
 // A phonon queue (Luke phonons, film re-emissions): one unit per queue entry
 template <bool kSur, bool kSplit = false>
-__global__ void __launch_bounds__(128, 8) k_queue_fp32(const __grid_constant__ FLat L,
+__global__ void __launch_bounds__(128, 6) k_queue_fp32(const __grid_constant__ FLat L,
                                                        const __grid_constant__ Detector D,
                                                        const __grid_constant__ RunArgs a,
                                                        const QPhonon* __restrict__ queue) {
@@ -683,14 +721,18 @@ __global__ void __launch_bounds__(128, 8) k_film_fp32(const __grid_constant__ FL
         const FilmRec r = film[i];
         const Surface& s = D.surf[r.surf];
         R128 g;
-        g.seed(r.key);
         int n_refl = 0;
         double edep;
-        if constexpr (kSur) {
-            edep = s.lut_abs ? surrogate_call(&s, r.E, refl_buf, &n_refl, kwork, &g)
-                             : kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g);
-        } else {
-            edep = kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g);
+        {
+            R128 g_c;  // the only generator whose address is taken (see the step loop)
+            g_c.seed(r.key);
+            if constexpr (kSur) {
+                edep = s.lut_abs ? surrogate_call(&s, r.E, refl_buf, &n_refl, kwork, &g_c)
+                                 : kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
+            } else {
+                edep = kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
+            }
+            g = g_c;
         }
         cmpmc_sim_stats& o = a.ev_stats[r.ev];
         if (edep > 0.0) {
