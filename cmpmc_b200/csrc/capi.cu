@@ -103,6 +103,7 @@ struct cmpmc_gpu_ctx {
     DevBuf lut[3];                                      // Kaplan surrogate tables of the films
     bool lut_ready = false;
     DevBuf queue, resume_a, resume_b, ccounters, carrier_event, cursor;  // batched charge form
+    DevBuf rel;                                         // batched charge release records
     DevBuf film_a, queue_b;                             // wavefront split: film entries, second phonon queue
     uint64_t film_cap = 1ull << 22;                     // film entries per phase (64 B each)
     uint32_t phase_steps = 0;                           // steps a track takes per transport phase (0: any)
@@ -193,7 +194,7 @@ int ensure_surrogate(cmpmc_gpu_ctx* ctx) {
 
 // Device counters of the batched charge form (reset per phase except next_carrier)
 struct ChargeCounters {
-    unsigned long long q_tail, resume_next, n_resume_out, next_carrier;
+    unsigned long long q_tail, resume_next, n_resume_out, next_carrier, rel_tail;
 };
 
 // The batched FP32 form of events with charges: phase 0 transports the generator's
@@ -220,7 +221,11 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
     const uint64_t grid_ch = std::max<uint64_t>(
         1, std::min<uint64_t>(static_cast<uint64_t>(ctx->num_sms) * bps_ch, (n_ch + tpb - 1) / tpb));
     const uint64_t resume_cap = grid_ch * tpb * 9;  // a carrier and up to 8 knock-ons per thread
-    const uint64_t q_cap = std::max<uint64_t>(ctx->queue_cap, 64);
+    uint64_t q_cap = std::max<uint64_t>(ctx->queue_cap, 64);
+    // collections with a release mode (BulkDebye / ElectrodeFilm) wait in a record buffer
+    // for the release kernel of their round: at most every carrier and knock-on of the call
+    const bool release = ctx->det.charge_release != 0;
+    const uint64_t rel_cap = release ? std::max<uint64_t>(4 * n_ch, 1024) + resume_cap : 0;
 
     CK(ctx->ev_stats2.ensure(std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats)), "alloc event stats");
     CK(ctx->ev_nhits.ensure(std::max<uint64_t>(n, 1) * 8), "alloc event hit counts");
@@ -231,7 +236,7 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
     CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
     CK(ctx->partials.ensure(kReducePartials * sizeof(cmpmc_sim_stats)), "alloc partial totals");
     CK(ctx->h_counters.ensure(sizeof(Counters) + sizeof(ChargeCounters)), "alloc host counters");
-    CK(ctx->queue.ensure(q_cap * sizeof(QPhonon)), "alloc Luke-phonon queue");
+    if (release) CK(ctx->rel.ensure(rel_cap * sizeof(ReleaseRec)), "alloc release records");
     CK(ctx->resume_a.ensure(resume_cap * sizeof(QCharge)), "alloc parked carriers");
     CK(ctx->resume_b.ensure(resume_cap * sizeof(QCharge)), "alloc parked carriers");
     CK(ctx->carrier_event.ensure(std::max<uint64_t>(n_ch, 1) * 4), "alloc carrier map");
@@ -255,13 +260,14 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
     ca.n_carriers = n_ch;
     ca.carrier_event = ctx->carrier_event.as<uint32_t>();
     ca.carrier_seed = mix64(d->seed ^ 0x2545f4914f6cdd1dULL);
-    ca.queue = ctx->queue.as<QPhonon>();
-    ca.q_cap = q_cap;
     ca.q_tail = &cc->q_tail;
     ca.resume_next = &cc->resume_next;
     ca.n_resume_out = &cc->n_resume_out;
     ca.next_carrier = &cc->next_carrier;
     ca.resume_cap = resume_cap;
+    ca.rel = release ? ctx->rel.as<ReleaseRec>() : nullptr;
+    ca.rel_cap = rel_cap;
+    ca.rel_tail = &cc->rel_tail;
 
     uint64_t hit_cap = ctx->hit_cap;
     if (!hit_cap) hit_cap = std::max<uint64_t>(1u << 20, (n_ph + n_ch) * 64);
@@ -270,6 +276,9 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
     char* hbuf = ctx->h_counters.as<char>();
     for (int attempt = 0;; ++attempt) {
         if (!d->keep_hits) hit_cap = 1;
+        CK(ctx->queue.ensure(q_cap * sizeof(QPhonon)), "alloc Luke-phonon queue");
+        ca.queue = ctx->queue.as<QPhonon>();
+        ca.q_cap = q_cap;
         CK(ctx->stack.ensure(slots * stack_cap * batched_stack_entry_bytes()), "alloc phonon stacks");
         CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
         CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
@@ -298,6 +307,7 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
         for (int round = 0;; ++round) {
             CK(cudaMemsetAsync(ctx->queue.p, 0xff, q_cap * sizeof(QPhonon), s), "memset queue");
             CK(cudaMemsetAsync(&cc->q_tail, 0, 3 * sizeof(unsigned long long), s), "memset counters");
+            CK(cudaMemsetAsync(&cc->rel_tail, 0, sizeof(unsigned long long), s), "memset counters");
             ca.resume_in = r_in;
             ca.n_resume_in = n_resume;
             ca.resume_out = r_out;
@@ -307,7 +317,20 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
             CK(cudaMemcpyAsync(hbuf + sizeof(Counters), cc, sizeof(ChargeCounters), cudaMemcpyDeviceToHost, s),
                "copy counters");
             CK(cudaStreamSynchronize(s), "charge kernel");
-            const ChargeCounters hcc = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
+            ChargeCounters hcc = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
+            if (release && hcc.rel_tail > 0) {
+                // the round's collections release their energy into the phonon queue
+                if (hcc.rel_tail > rel_cap) return fail(ctx, CMPMC_ERR_CAPACITY, "release-record buffer overflow");
+                CK(launch_release_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ca, hcc.rel_tail,
+                                       static_cast<int>(std::min<uint64_t>(grid_ph, (hcc.rel_tail + tpb - 1) / tpb)),
+                                       tpb, s),
+                   "release launch");
+                ++launches;
+                CK(cudaMemcpyAsync(hbuf + sizeof(Counters), cc, sizeof(ChargeCounters), cudaMemcpyDeviceToHost, s),
+                   "copy counters");
+                CK(cudaStreamSynchronize(s), "release kernel");
+                hcc = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
+            }
             const uint64_t n_q = std::min<uint64_t>(hcc.q_tail, q_cap);
             if (n_q) {
                 CK(cudaMemsetAsync(&dc->next_work, 0, sizeof(unsigned long long), s), "memset work counter");
@@ -334,10 +357,15 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
         CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
         const bool stack_over = (hc.err & kErrPhononStack) != 0;
         const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
-        if (!stack_over && !hits_over) break;
-        if (attempt >= 6) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack or hit buffer overflow persists");
+        const bool queue_over = (hc.err & kErrRelease) != 0;  // released phonons did not fit the queue
+        if (!stack_over && !hits_over && !queue_over) break;
+        if (attempt >= 6) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack, hit or queue overflow persists");
         if (stack_over) stack_cap = std::min<uint32_t>(stack_cap * 8, 1u << 20);
         if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
+        if (queue_over) {
+            q_cap *= 4;
+            ctx->queue_cap = std::max<uint64_t>(ctx->queue_cap, q_cap);
+        }
         hc.err = 0;
     }
     if (d->keep_hits) ctx->hit_cap = std::max<uint64_t>(ctx->hit_cap, hit_cap);
@@ -635,7 +663,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->kin, &ctx->film_a, &ctx->queue_b, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->mesh2, &ctx->mesh2_32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
+    for (DevBuf* b : {&ctx->kin, &ctx->film_a, &ctx->queue_b, &ctx->rel, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->mesh2, &ctx->mesh2_32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
                       &ctx->ccounters, &ctx->carrier_event, &ctx->cursor, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
@@ -964,11 +992,9 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     uint64_t n_hits = 0;
     uint64_t* ev_offsets = nullptr;
     cmpmc_sim_stats* ev_stats = nullptr;
-    if (batched && ctx->L.kin_mode != kKinOctahedral)
-        return fail(ctx, CMPMC_ERR_INVALID, "Exact and Bilinear kinematics run in the plain FP64 form");
-    if (batched && n_ch > 0 && ctx->det.charge_release != 0)
+    if (batched && ctx->L.kin_mode != kKinOctahedral && d->kaplan_surrogate)
         return fail(ctx, CMPMC_ERR_INVALID,
-                    "BulkDebye / ElectrodeFilm charge release runs in the plain FP64 form (batched: RecordOnly)");
+                    "the Kaplan surrogate runs with octahedral kinematics (Exact / Bilinear: full cascades)");
     if (batched && n_ch > 0) {
         // carriers and their Luke phonons: alternating charge / queue phases, event sinks
         const int st = run_charges_batched(ctx, d, a, n, n_ph, n_ch, launches, hc, kms, n_hits, ev_offsets, ev_stats);

@@ -59,6 +59,8 @@ struct FCSurf {
     float prob_abs, prob_spec, min_k_e, min_k_h;
     int n_pads;
     const Pad* pads;  // electrode mask
+    int release;      // the collected energy goes to the release kernel (BulkDebye, or
+                      // ElectrodeFilm on a surface with a film)
 };
 
 struct FCDet {
@@ -512,10 +514,36 @@ __global__ void __launch_bounds__(128, 4) k_charges_fp32(const __grid_constant__
                     }
                     continue;
                 }
-                // collection_release_energy (engine.hpp:889-893), ChargeRelease::RecordOnly
+                // collection_release_energy (engine.hpp:889-893)
                 const double e_rel = static_cast<double>(c.ekin) + ((c.type == 1) ? (e_gap - D.muF) : D.muF);
-                const double recomb = e_rel * static_cast<double>(c.w);
                 ++st.collected;
+                if (s.release) {
+                    // BulkDebye / ElectrodeFilm (engine.hpp:302-313): the release kernel emits
+                    // the phonons, runs the film cascades and records the hit
+                    const unsigned long long slot = atomicAdd(ca.rel_tail, 1ull);
+                    if (slot < ca.rel_cap) {
+                        ReleaseRec r;
+                        r.px = c.pos.x; r.py = c.pos.y; r.pz = c.pos.z;
+                        r.w = c.w;
+                        r.e_rel = e_rel;
+                        r.t = c.t;
+                        const uint64_t hi = k.g.next();
+                        r.key = (hi << 32) | k.g.next();
+                        r.ev = k.ev;
+                        r.ch_id = ch_id;
+                        r.surf = static_cast<uint8_t>(bh.surf);
+                        r.type = static_cast<uint8_t>(c.type);
+                        r.pad0 = r.pad1 = 0;
+                        r.pad2 = 0;
+                        ca.rel[slot] = r;
+                    } else {
+                        err |= kErrRelease;
+                    }
+                    live = false;
+                    continue;
+                }
+                // ChargeRelease::RecordOnly
+                const double recomb = e_rel * static_cast<double>(c.w);
                 st.recomb_eV += recomb;
                 st.dep += recomb;
                 if (a.keep_hits) {
@@ -653,6 +681,111 @@ __global__ void k_carrier_event(const uint64_t* __restrict__ ch_off, uint64_t n_
         for (uint64_t j = ch_off[ev]; j < ch_off[ev + 1]; ++j) carrier_event[j] = static_cast<uint32_t>(ev);
 }
 
+// The release phase of the batched charge form (engine.hpp:302-313, 894-925): one collected
+// carrier per thread, from its own substream. BulkDebye emits round(E_rel / E_Debye) (at
+// least one) Debye phonons; ElectrodeFilm sends the energy into the electrode's film as
+// quanta of at most max(4, electrode_seed_max_gap) Delta (photon seeds): the absorbed part
+// is the hit, the escaping phonons re-enter the crystal, the rest is lost. The phonons go,
+// inward Lambertian with a DOS mode and their own substreams, into the phonon queue of
+// the round; the hit and the ledger go to the carrier's event.
+template <int kKin>
+__global__ void __launch_bounds__(128, 8) k_release_fp32(const __grid_constant__ FLat L,
+                                                         const __grid_constant__ Detector D,
+                                                         const __grid_constant__ RunArgs a,
+                                                         const __grid_constant__ ChargeArgs ca,
+                                                         const ReleaseRec* __restrict__ rel, uint64_t n_rel,
+                                                         double debye_energy) {
+    double refl_buf[kKaplanCap];
+    double kwork[4 * kKaplanCap];
+    unsigned err = 0;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n_rel;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const ReleaseRec r = rel[i];
+        R128 g;
+        g.seed(r.key);
+        const F3 hp = f3(r.px, r.py, r.pz);
+        const F3 n_in = fnormal(r.surf, hp);
+        const F3 p0 = hp + n_in * kNudge;
+        uint32_t n_ph = 0;  // phonons queued so far (substream index)
+        auto emit = [&](double e, unsigned long long slot) {
+            const int mode = fdos(L, g.u());
+            FKin kin;
+            const F3 kd = finward<kKin>(L, mode, n_in, g, kin);
+            QPhonon q;
+            q.px = p0.x; q.py = p0.y; q.pz = p0.z;
+            q.kx = kd.x; q.ky = kd.y; q.kz = kd.z;
+            q.w = r.w;
+            q.mode = static_cast<uint32_t>(mode);
+            q.E = e;
+            q.t = r.t;
+            q.key = mix64(r.key ^ (0x9e3779b97f4a7c15ULL * (static_cast<uint64_t>(n_ph++) + 1)));
+            q.ev = r.ev;
+            q.pad = 0;
+            ca.queue[slot] = q;
+        };
+        double hit_eV = 0.0, lost = 0.0;
+        if (D.charge_release == 1) {
+            const int k = static_cast<int>(round(r.e_rel / debye_energy));
+            const int n = (k < 1) ? 1 : k;
+            const unsigned long long base = atomicAdd(ca.q_tail, static_cast<unsigned long long>(n));
+            if (base + n > ca.q_cap) {
+                err |= kErrRelease;
+            } else {
+                for (int j = 0; j < n; ++j) emit(r.e_rel / n, base + j);
+            }
+        } else {
+            const Film& film = D.surf[r.surf].film;
+            const double qmax = dmax(4.0, D.electrode_seed_max_gap) * film.gap_energy;
+            const int k = static_cast<int>(ceil(r.e_rel / qmax));
+            const int n = (k < 1) ? 1 : k;
+            const double q = r.e_rel / n;
+            double absorbed = 0.0, emitted = 0.0;
+            KBuf refl{refl_buf, 0};
+            for (int j = 0; j < n; ++j) {
+                absorbed += film_absorb_quantum(film, q, refl, kwork, g, true);
+                if (refl.n == 0) continue;
+                const unsigned long long base = atomicAdd(ca.q_tail, static_cast<unsigned long long>(refl.n));
+                if (base + refl.n > ca.q_cap) {
+                    err |= kErrRelease;
+                    continue;
+                }
+                for (int m = 0; m < refl.n; ++m) {
+                    emit(refl_buf[m], base + m);
+                    emitted += refl_buf[m];
+                }
+            }
+            lost = dmax(0.0, r.e_rel - absorbed - emitted);
+            hit_eV = absorbed;
+        }
+        const double recomb = hit_eV * static_cast<double>(r.w);
+        cmpmc_sim_stats& o = a.ev_stats[r.ev];
+        if (recomb != 0.0) {
+            atomicAdd(&o.charge_recomb_edep_eV, recomb);
+            atomicAdd(&o.total_deposited_eV, recomb);
+        }
+        if (lost != 0.0) atomicAdd(&o.escaped_or_killed_eV, lost * static_cast<double>(r.w));
+        if (a.keep_hits) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(a.ev_nhits + r.ev), 1ull);
+            const unsigned long long idx = atomicAdd(a.hit_count, 1ull);
+            if (idx < a.hit_cap) {
+                cmpmc_sensor_hit h;
+                h.pos[0] = r.px; h.pos[1] = r.py; h.pos[2] = r.pz;
+                h.time = r.t;
+                h.edep = recomb;
+                h.incident_energy = r.e_rel;
+                h.surface_id = r.surf;
+                h.excitation = r.type;
+                h.mode = 0;
+                h._pad = 0;
+                h.channel_id = r.ch_id;
+                a.hit_stage[idx] = h;
+                a.hit_key[idx] = r.ev;
+            }
+        }
+    }
+    if (err) atomicOr(a.err, err);
+}
+
 FCLat make_fclat(const Lattice& L, const float* cdf_f, const Detector& D) {
     FCLat f{};
     for (int v = 0; v < CMPMC_MAX_VALLEYS && v < L.n_valleys; ++v)
@@ -708,6 +841,7 @@ FCDet make_fcdet(const Detector& D, const MeshView32& mesh, const Lattice& L) {
         f.surf[i].min_k_h = static_cast<float>(D.surf[i].min_k_hole);
         f.surf[i].n_pads = D.surf[i].n_pads;
         f.surf[i].pads = D.surf[i].pads;
+        f.surf[i].release = (D.charge_release == 1 || (D.charge_release == 2 && D.surf[i].has_film)) ? 1 : 0;
     }
     f.dt_cap = static_cast<float>(D.charge_dt_cap_s);
     const bool second = (D.charge_stepping == 1);
@@ -732,6 +866,16 @@ cudaError_t launch_charges_fp32(const Lattice& L, const float* cdf_f, const Dete
 
 cudaError_t charges_fp32_occupancy(int block, int* blocks_per_sm) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_charges_fp32, block, 0);
+}
+
+cudaError_t launch_release_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
+                                const ChargeArgs& c, uint64_t n_rel, int grid, int block, cudaStream_t s) {
+    const FLat f = make_flat(L, cdf_f, D);
+    if (L.kin_mode != kKinOctahedral)
+        k_release_fp32<1><<<grid, block, 0, s>>>(f, D, a, c, c.rel, n_rel, L.debye_energy);
+    else
+        k_release_fp32<0><<<grid, block, 0, s>>>(f, D, a, c, c.rel, n_rel, L.debye_energy);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_carrier_event(const uint64_t* ch_off, uint64_t n_events, uint32_t* carrier_event,

@@ -15,6 +15,7 @@ enum : unsigned {
     kErrQueue = 4u,
     kErrResume = 8u,
     kErrFilmQueue = 16u,
+    kErrRelease = 32u,     // batched charge release: release records or their phonons overflowed
 };
 
 // A pushed phonon in a per-thread global-memory LIFO (112 B, 16-byte aligned)
@@ -119,6 +120,21 @@ struct alignas(16) QCharge {
     uint32_t pad[3];
 };
 
+// A collected carrier whose released energy (DetectorModel::ChargeRelease BulkDebye or
+// ElectrodeFilm, engine.hpp:302-313) is handed from the charge kernel to the release
+// kernel of the batched charge form, with its own substream key.
+struct ReleaseRec {
+    float px, py, pz;  // contact point
+    float w;
+    double e_rel;      // collection_release_energy
+    double t;
+    uint64_t key;
+    uint32_t ev;
+    int32_t ch_id;
+    uint8_t surf, type, pad0, pad1;
+    uint32_t pad2;
+};
+
 struct ChargeArgs {
     uint64_t n_carriers;              // initial carriers (RunArgs::ch)
     const uint32_t* carrier_event;    // [n_carriers]
@@ -133,6 +149,9 @@ struct ChargeArgs {
     uint64_t resume_cap;
     unsigned long long* n_resume_out;
     unsigned long long* next_carrier;
+    ReleaseRec* rel;                  // collections with a release mode (null: RecordOnly)
+    uint64_t rel_cap;
+    unsigned long long* rel_tail;
 };
 
 // Adjoint of a binned hit-time histogram (batched FP32 form, k_adjoint_fp32)
@@ -251,6 +270,9 @@ cudaError_t launch_math_check(uint64_t n, const double* x, double* out);
 cudaError_t launch_charges_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                                 const ChargeArgs& c, int grid, int block, cudaStream_t s);
 cudaError_t charges_fp32_occupancy(int block, int* blocks_per_sm);
+// The release phase of the batched charge form: c.rel[0, n_rel) into c.queue, hits and ledgers
+cudaError_t launch_release_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
+                                const ChargeArgs& c, uint64_t n_rel, int grid, int block, cudaStream_t s);
 cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                               const QPhonon* queue, int grid, int block, cudaStream_t s);
 // wavefront split of the batched form: the phonon kernels with a.film set stop a track at

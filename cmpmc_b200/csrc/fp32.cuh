@@ -84,12 +84,34 @@ struct FLat {
     // per surface: constant reflection split (1 when the polynomials do not depend on energy)
     int split_const[3];
     float p_anh[3], p_anh_spec[3];
+    // KinematicsMode: Octahedral (the table above) or the lattice's Exact / Bilinear map
+    int kin_mode;
+    double density;
+    const Stiffness* stiff;
+    const double* bil;
+    M3 orient64;
 };
 
 struct FKin {
     F3 dir;
     float mag;
 };
+
+// The Exact (Cardano per call) and Bilinear kinematics modes (crystal_lattice.hpp:76-114):
+// the lattice's FP64 maps, out of line, rounded to FP32 at the end
+__device__ __noinline__ FKin fmap_solve(const FLat* Lp, int mode, F3 k) {
+    Lattice l{};
+    l.kin_mode = Lp->kin_mode;
+    l.density = Lp->density;
+    l.stiff = Lp->stiff;
+    l.bil = Lp->bil;
+    l.orient = Lp->orient64;
+    const Kin r = map_k_to_vg(l, mode, v3(k.x, k.y, k.z));
+    FKin f;
+    f.dir = F3{static_cast<float>(r.vg_dir.x), static_cast<float>(r.vg_dir.y), static_cast<float>(r.vg_dir.z)};
+    f.mag = static_cast<float>(r.vg_mag);
+    return f;
+}
 
 __device__ __forceinline__ FKin fmap(const FLat& L, int mode, F3 k) {
     const F3 kc = f3(L.o[0] * k.x + L.o[3] * k.y + L.o[6] * k.z, L.o[1] * k.x + L.o[4] * k.y + L.o[7] * k.z,
@@ -124,6 +146,15 @@ __device__ __forceinline__ FKin fmap(const FLat& L, int mode, F3 k) {
     return r;
 }
 
+// The group-velocity map of the kernel's kinematics: the octahedral table (kKin 0) or the
+// lattice's Exact / Bilinear map (kKin 1, out of line). A compile-time choice: an
+// out-of-line call in the octahedral kernels' step loop would cost them a third.
+template <int kKin>
+__device__ __forceinline__ FKin fmapk(const FLat& L, int mode, F3 k) {
+    if constexpr (kKin != 0) return fmap_solve(&L, mode, k);
+    else return fmap(L, mode, k);
+}
+
 __device__ __forceinline__ int fdos(const FLat& L, float u) { return (u < L.fL) ? 0 : ((u < L.fLST) ? 2 : 1); }
 __device__ __forceinline__ int ftrans(const FLat& L, R128& g) { return (g.u() < L.p_st_trans) ? 2 : 1; }
 __device__ __forceinline__ float fcdf(const float* cdf, R128& g) {
@@ -135,6 +166,7 @@ __device__ __forceinline__ float fcdf(const float* cdf, R128& g) {
 __device__ __forceinline__ float facos_clamped(float c) { return acosf(fminf(fmaxf(c, -1.0f), 1.0f)); }
 
 // inward Lambertian wavevector whose group velocity points inward (engine.hpp:927-936)
+template <int kKin = 0>
 __device__ __forceinline__ F3 finward(const FLat& L, int mode, F3 n, R128& g, FKin& kin) {
     const F3 a = forth(n);
     const F3 b = fcross(n, a);
@@ -145,10 +177,10 @@ __device__ __forceinline__ F3 finward(const FLat& L, int mode, F3 n, R128& g, FK
         float s, c;
         __sincosf(phi, &s, &c);
         const F3 kd = funit(a * (st * c) + b * (st * s) + n * ct);
-        kin = fmap(L, mode, kd);
+        kin = fmapk<kKin>(L, mode, kd);
         if (fdot(kin.dir, n) > 1e-6f) return kd;
     }
-    kin = fmap(L, mode, n);
+    kin = fmapk<kKin>(L, mode, n);
     return n;
 }
 
@@ -189,6 +221,41 @@ __device__ __forceinline__ FBHit fexit(float R, float H, F3 p, F3 v) {
     return h;
 }
 
+// The exit distance and surface only (the phonon step loop): the normal is needed only
+// when the step ends on the boundary, so fnormal computes it there.
+__device__ __forceinline__ FBHit fexit_d(float R, float H, F3 p, F3 v) {
+    float t = __int_as_float(0x7f800000);
+    int surf = 2;
+    if (v.z > 1e-15f) {
+        const float tz = (H - p.z) / v.z;
+        if (tz >= 0.0f && tz < t) { t = tz; surf = 0; }
+    } else if (v.z < -1e-15f) {
+        const float tz = (-H - p.z) / v.z;
+        if (tz >= 0.0f && tz < t) { t = tz; surf = 1; }
+    }
+    const float a = v.x * v.x + v.y * v.y;
+    if (a > 1e-18f) {
+        const float b = p.x * v.x + p.y * v.y;
+        const float c = p.x * p.x + p.y * p.y - R * R;
+        const float disc = fmaxf(0.0f, b * b - a * c);
+        const float tr = (-b + sqrtf(disc)) / a;
+        if (tr >= 0.0f && tr < t) { t = tr; surf = 2; }
+    }
+    FBHit h;
+    h.d = fmaxf(0.0f, t);
+    h.surf = surf;
+    h.n = f3(0.0f, 0.0f, 1.0f);
+    return h;
+}
+
+// inward normal of surface `surf` at the hit point hp (as fexit)
+__device__ __forceinline__ F3 fnormal(int surf, F3 hp) {
+    if (surf == 0) return f3(0.0f, 0.0f, -1.0f);
+    if (surf == 1) return f3(0.0f, 0.0f, 1.0f);
+    const float r = sqrtf(hp.x * hp.x + hp.y * hp.y);
+    return (r > 1e-15f) ? f3(-hp.x / r, -hp.y / r, 0.0f) : f3(-1.0f, 0.0f, 0.0f);
+}
+
 // FP32 constants of the crystal derived from the FP64 lattice view
 inline FLat make_flat(const Lattice& L, const float* cdf_f, const Detector& D) {
     FLat f;
@@ -217,6 +284,11 @@ inline FLat make_flat(const Lattice& L, const float* cdf_f, const Detector& D) {
         f.p_anh[i] = static_cast<float>(lo.p_anh);
         f.p_anh_spec[i] = static_cast<float>(lo.p_anh + lo.p_spec);
     }
+    f.kin_mode = L.kin_mode;
+    f.density = L.density;
+    f.stiff = L.stiff;
+    f.bil = L.bil;
+    f.orient64 = L.orient;
     return f;
 }
 

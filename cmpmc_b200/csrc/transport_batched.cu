@@ -183,7 +183,7 @@ __device__ __noinline__ double surrogate_call(const Surface* s, double E, double
 }
 
 // anharmonic decay of an L phonon (engine.hpp:938-988), FP32 angles
-template <bool kAdj>
+template <bool kAdj, int kKin = 0>
 __device__ __noinline__ void decay_call(const FLat* Lp, TrackOf<kAdj>* tp, EntryOf<kAdj>* stk, uint32_t* n_stk,
                                         uint32_t cap, unsigned* err, const UStats* st, R128* gp) {
     const FLat& L = *Lp;
@@ -221,7 +221,7 @@ __device__ __noinline__ void decay_call(const FLat* Lp, TrackOf<kAdj>* tp, Entry
     TrackOf<kAdj> d;
     d.pos = trk.pos;
     d.k = k2;
-    const FKin kin2 = fmap(L, m2, k2);
+    const FKin kin2 = fmapk<kKin>(L, m2, k2);
     d.vg = kin2.dir;
     d.vmag = kin2.mag;
     d.E = (1.0 - xd) * trk.E;
@@ -234,7 +234,7 @@ __device__ __noinline__ void decay_call(const FLat* Lp, TrackOf<kAdj>* tp, Entry
     trk.E = xd * trk.E;
     trk.mode = m1;
     trk.k = k1;
-    const FKin kin = fmap(L, m1, k1);
+    const FKin kin = fmapk<kKin>(L, m1, k1);
     trk.vg = kin.dir;
     trk.vmag = kin.mag;
 }
@@ -303,7 +303,8 @@ enum { kSrcInput = 0, kSrcQueue = 1 };
 // cascades from the surrogate tables; kSplit: a track that enters a film is queued for the
 // film kernel and ends here (wavefront split). All are compile-time, so the default kernel
 // carries none of their branches.
-template <bool kAdj, int kSrc = kSrcInput, bool kSink = false, bool kSur = false, bool kSplit = false>
+template <bool kAdj, int kSrc = kSrcInput, bool kSink = false, bool kSur = false, bool kSplit = false,
+          int kKin = 0>
 __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, const RunArgs& a,
                                              const uint32_t* __restrict__ unit_event,
                                              const QPhonon* __restrict__ queue, const AdjArgs& adj,
@@ -352,7 +353,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                     trk.pos = f3(q.px, q.py, q.pz);
                     trk.k = f3(q.kx, q.ky, q.kz);
                     trk.mode = static_cast<int>(q.mode);
-                    const FKin kin = fmap(L, trk.mode, trk.k);
+                    const FKin kin = fmapk<kKin>(L, trk.mode, trk.k);
                     trk.vg = kin.dir;
                     trk.vmag = kin.mag;
                     trk.E = q.E;
@@ -439,7 +440,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
         const float r_down = (trk.mode == 0) ? L.a5 * (nu2 * nu2 * nu) : 0.0f;
         const float r_tot = r_iso + r_poly + r_down;
         const float d_phys = (r_tot > 1e-12f) ? (-logf(g.u()) * trk.vmag / r_tot) : __int_as_float(0x7f800000);
-        const FBHit bh = fexit(R, H, trk.pos, trk.vg);
+        FBHit bh = fexit_d(R, H, trk.pos, trk.vg);
         const bool bulk = d_phys < bh.d;
         const float d = bulk ? d_phys : bh.d;
         trk.pos = trk.pos + trk.vg * d;
@@ -462,7 +463,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 R128 g_c = g;
                 uint32_t n_c = n_stk;
                 unsigned e_c = err;
-                decay_call<kAdj>(&L, &t_c, stk, &n_c, a.stack_cap, &e_c, &st, &g_c);
+                decay_call<kAdj, kKin>(&L, &t_c, stk, &n_c, a.stack_cap, &e_c, &st, &g_c);
                 trk = t_c;
                 g = g_c;
                 n_stk = n_c;
@@ -478,6 +479,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 sample = 0;
             }
         } else {
+            bh.n = fnormal(bh.surf, trk.pos);  // trk.pos is the hit point
             trk.bounces++;
             const Surface& s = D.surf[bh.surf];
             bool enter = false;
@@ -582,7 +584,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                     TrackOf<kAdj> dtr;
                     dtr.mode = fdos(L, g.u());
                     FKin kin;
-                    dtr.k = finward(L, dtr.mode, bh.n, g, kin);
+                    dtr.k = finward<kKin>(L, dtr.mode, bh.n, g, kin);
                     dtr.pos = re;
                     dtr.vg = kin.dir;
                     dtr.vmag = kin.mag;
@@ -623,7 +625,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                     const int m2 = ftrans(L, g);
                     TrackOf<kAdj> dtr;
                     FKin k2kin;
-                    dtr.k = finward(L, m2, bh.n, g, k2kin);
+                    dtr.k = finward<kKin>(L, m2, bh.n, g, k2kin);
                     dtr.pos = trk.pos;
                     dtr.vg = k2kin.dir;
                     dtr.vmag = k2kin.mag;
@@ -640,8 +642,8 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 } else if (u_refl < p_anh_spec) {
                     if constexpr (kAdj) trk.s[2] += adj.spec_score;  // d log(1 - p_d) / d log p_d
                     F3 kr = trk.k - bh.n * (2.0f * fdot(trk.k, bh.n));
-                    FKin kin = fmap(L, trk.mode, kr);
-                    if (fdot(kin.dir, bh.n) <= 1e-6f) kr = finward(L, trk.mode, bh.n, g, kin);
+                    FKin kin = fmapk<kKin>(L, trk.mode, kr);
+                    if (fdot(kin.dir, bh.n) <= 1e-6f) kr = finward<kKin>(L, trk.mode, bh.n, g, kin);
                     trk.k = kr;
                     trk.vg = kin.dir;
                     trk.vmag = kin.mag;
@@ -669,11 +671,11 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 __sincosf(kTwoPiF * u2, &sphi, &cphi);
                 kd = e1 * (st_ * cphi) + e2 * (st_ * sphi) + e3 * ct;
                 if (lam) kd = funit(kd);
-                kin = fmap(L, trk.mode, kd);
+                kin = fmapk<kKin>(L, trk.mode, kd);
                 if (!lam || fdot(kin.dir, bh.n) > 1e-6f) break;
                 if (trial == 15) {
                     kd = bh.n;
-                    kin = fmap(L, trk.mode, kd);
+                    kin = fmapk<kKin>(L, trk.mode, kd);
                     break;
                 }
             }
@@ -685,30 +687,30 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
     if (err) atomicOr(a.err, err);
 }
 
-template <bool kSink, bool kSur, bool kSplit = false>
+template <bool kSink, bool kSur, bool kSplit = false, int kKin = 0>
 __global__ void __launch_bounds__(128, 6) k_batched_fp32(const __grid_constant__ FLat L,
                                                          const __grid_constant__ Detector D,
                                                          const __grid_constant__ RunArgs a,
                                                          const uint32_t* __restrict__ unit_event) {
     const AdjArgs none{};
-    batched_loop<false, kSrcInput, kSink, kSur, kSplit>(L, D, a, unit_event, nullptr, none, nullptr, nullptr);
+    batched_loop<false, kSrcInput, kSink, kSur, kSplit, kKin>(L, D, a, unit_event, nullptr, none, nullptr, nullptr);
 }
 
 // A phonon queue (Luke phonons, film re-emissions): one unit per queue entry
-template <bool kSur, bool kSplit = false>
+template <bool kSur, bool kSplit = false, int kKin = 0>
 __global__ void __launch_bounds__(128, 6) k_queue_fp32(const __grid_constant__ FLat L,
                                                        const __grid_constant__ Detector D,
                                                        const __grid_constant__ RunArgs a,
                                                        const QPhonon* __restrict__ queue) {
     const AdjArgs none{};
-    batched_loop<false, kSrcQueue, true, kSur, kSplit>(L, D, a, nullptr, queue, none, nullptr, nullptr);
+    batched_loop<false, kSrcQueue, true, kSur, kSplit, kKin>(L, D, a, nullptr, queue, none, nullptr, nullptr);
 }
 
 // The film kernel of the wavefront split: one queued film entry per thread. It runs the
 // Kaplan cascade (or the surrogate lookup) from the entry's own substream, records the hit
 // and the ledger in the entry's event, and queues the re-emitted phonons, each inward
 // Lambertian with a DOS mode and its own substream (the first keeps the bounce count).
-template <bool kSur>
+template <bool kSur, int kKin = 0>
 __global__ void __launch_bounds__(128, 8) k_film_fp32(const __grid_constant__ FLat L,
                                                       const __grid_constant__ Detector D,
                                                       const __grid_constant__ RunArgs a,
@@ -780,7 +782,7 @@ __global__ void __launch_bounds__(128, 8) k_film_fp32(const __grid_constant__ FL
         for (int j = 0; j < n_refl; ++j) {
             const int mode = fdos(L, g.u());
             FKin kin;
-            const F3 k = finward(L, mode, n, g, kin);
+            const F3 k = finward<kKin>(L, mode, n, g, kin);
             QPhonon q;
             q.px = re.x; q.py = re.y; q.pz = re.z;
             q.kx = k.x; q.ky = k.y; q.kz = k.z;
@@ -828,7 +830,11 @@ cudaError_t launch_unit_event(const uint64_t* ph_off, uint64_t n_events, uint32_
 cudaError_t launch_batched_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                                 const uint32_t* unit_event, int grid, int block, cudaStream_t s) {
     const FLat f = make_flat(L, cdf_f, D);
-    if (a.film) {
+    if (L.kin_mode != kKinOctahedral) {  // Exact / Bilinear kinematics (no surrogate tables)
+        if (a.film) k_batched_fp32<true, false, true, 1><<<grid, block, 0, s>>>(f, D, a, unit_event);
+        else if (a.ev_sink) k_batched_fp32<true, false, false, 1><<<grid, block, 0, s>>>(f, D, a, unit_event);
+        else k_batched_fp32<false, false, false, 1><<<grid, block, 0, s>>>(f, D, a, unit_event);
+    } else if (a.film) {
         if (a.surrogate) k_batched_fp32<true, true, true><<<grid, block, 0, s>>>(f, D, a, unit_event);
         else k_batched_fp32<true, false, true><<<grid, block, 0, s>>>(f, D, a, unit_event);
     } else if (a.ev_sink) {
@@ -850,7 +856,8 @@ size_t batched_stack_entry_bytes() { return sizeof(GFTrack); }
 cudaError_t launch_film_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                              const FilmRec* film, uint64_t n_film, int grid, int block, cudaStream_t s) {
     const FLat f = make_flat(L, cdf_f, D);
-    if (a.surrogate) k_film_fp32<true><<<grid, block, 0, s>>>(f, D, a, film, n_film);
+    if (L.kin_mode != kKinOctahedral) k_film_fp32<false, 1><<<grid, block, 0, s>>>(f, D, a, film, n_film);
+    else if (a.surrogate) k_film_fp32<true><<<grid, block, 0, s>>>(f, D, a, film, n_film);
     else k_film_fp32<false><<<grid, block, 0, s>>>(f, D, a, film, n_film);
     return cudaGetLastError();
 }
@@ -862,7 +869,10 @@ cudaError_t film_fp32_occupancy(int block, int* blocks_per_sm) {
 cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                               const QPhonon* queue, int grid, int block, cudaStream_t s) {
     const FLat f = make_flat(L, cdf_f, D);
-    if (a.film) {
+    if (L.kin_mode != kKinOctahedral) {
+        if (a.film) k_queue_fp32<false, true, 1><<<grid, block, 0, s>>>(f, D, a, queue);
+        else k_queue_fp32<false, false, 1><<<grid, block, 0, s>>>(f, D, a, queue);
+    } else if (a.film) {
         if (a.surrogate) k_queue_fp32<true, true><<<grid, block, 0, s>>>(f, D, a, queue);
         else k_queue_fp32<false, true><<<grid, block, 0, s>>>(f, D, a, queue);
     } else {

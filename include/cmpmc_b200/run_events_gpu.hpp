@@ -19,9 +19,9 @@
 // detector with only mesh_field_2d needs its BiLinearMesh2D handed over the same way with
 // set_mesh2d or set_grid_mesh2d.
 // Guarded modules raise the reference's UnvalidatedModuleError; configurations the device
-// does not support (in the batched forms, charge release other than RecordOnly and Exact /
-// Bilinear kinematics) raise std::invalid_argument. Build the GpuEngine from the
-// CrystalLattice itself to carry its kinematics mode.
+// does not support (in the batched forms, the Kaplan surrogate with Exact / Bilinear
+// kinematics) raise std::invalid_argument. Build the GpuEngine from the CrystalLattice
+// itself to carry its kinematics mode.
 #pragma once
 
 #include <algorithm>

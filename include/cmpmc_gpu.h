@@ -175,7 +175,7 @@ typedef struct cmpmc_detector {
     double charge_max_dk_frac, charge_dt_cap_s, charge_sampling_dk_frac;
     int32_t charge_stepping;       /* 0 FirstOrderDkCap, 1 LemanSecondOrder */
     int32_t charge_release;        /* DetectorModel::ChargeRelease: 0 RecordOnly, 1 BulkDebye,
-                                      2 ElectrodeFilm (1 and 2: plain FP64 form)            */
+                                      2 ElectrodeFilm (batched: a release phase per round) */
     double fermi_level_above_Ev_eV;
     double electrode_seed_max_gap;
     int32_t allow_unvalidated;
@@ -251,7 +251,9 @@ int cmpmc_lattice_tables(const cmpmc_lattice* lat, const float** oct_lut, const 
 /* CrystalLattice::set_kinematics_mode (crystal_lattice.hpp:63-74): 0 Octahedral (default),
  * 1 Exact (Cardano solve per call), 2 Bilinear (181 x 361 (cos theta, phi) table, built here
  * on first request). It applies to make_track, the generators and every device context
- * created afterwards from this lattice; Exact and Bilinear run in the plain FP64 form. */
+ * created afterwards from this lattice. The plain FP64 form evaluates them as the reference
+ * does; the batched FP32 forms call the same FP64 maps out of line and round the group
+ * velocity to FP32 (not with the Kaplan surrogate, and not in the adjoint). */
 int cmpmc_lattice_set_kinematics_mode(cmpmc_lattice* lat, int mode);
 int cmpmc_lattice_kinematics_mode(const cmpmc_lattice* lat);
 /* CrystalLattice::map_k_to_vg (crystal_lattice.hpp:76-176, the lattice's mode), on the host. */

@@ -215,3 +215,34 @@ def test_batched_amm_interface_statistics(ge_lattice):
     fa = plain.stats.total_deposited_eV / plain.stats.total_injected_eV
     fb = batched.stats.total_deposited_eV / batched.stats.total_injected_eV
     assert abs(fb / fa - 1.0) < 0.01
+
+
+@pytest.mark.parametrize("wl,n", [("c0x", 1000), ("c0b", 2000)])
+def test_batched_kinematics_modes_statistics(ge_lattice, wl, n):
+    """Exact (Cardano solve per call) and Bilinear kinematics in the batched form (the FP64
+    maps out of line, rounded to FP32) against the plain FP64 form (identical to the
+    reference event by event): hit histograms chi^2 p > 0.01 and the same deposited fraction
+    within 1 %; the ledger closes."""
+    import cmpmc_b200 as cm
+    from tests.helpers import lattice_for
+    eng = cm.SimulationEngine(lattice_for(wl, ge_lattice), detector_for(wl))
+    plain = cm.run_events(eng, n, workload_of(wl), cm.RunOptions(seed=WORKLOAD_SEED[wl]))
+    batched = _batched(eng, wl, n)
+    lo = min(plain.hits["edep"].min(), batched.hits["edep"].min())
+    hi = max(plain.hits["edep"].max(), batched.hits["edep"].max()) * (1 + 1e-9)
+    a = event_histograms(plain.hit_offsets, plain.hits, (lo, hi))
+    b = event_histograms(batched.hit_offsets, batched.hits, (lo, hi))
+    for name in ("time", "radius", "edep"):
+        c2, dof, p = hist_chi2(a, b, name)
+        print(f"{wl} {name}: chi2 {c2:.1f} dof {dof} p {p:.3f}")
+        assert p > P_MIN, (name, c2, dof, p)
+    fa = plain.stats.total_deposited_eV / plain.stats.total_injected_eV
+    fb = batched.stats.total_deposited_eV / batched.stats.total_injected_eV
+    assert abs(fb / fa - 1.0) < 0.01
+    st = batched.stats
+    assert abs(st.total_injected_eV - st.total_deposited_eV - st.escaped_or_killed_eV) <= \
+        LEDGER_TOL * st.total_injected_eV
+    # the surrogate tables are built for the octahedral kinematics only
+    with pytest.raises(cm.CmpmcError):
+        eng.run_packed(eng.generate(workload_of(wl), 8, WORKLOAD_SEED[wl]),
+                       cm.RunOptions(seed=1, form="batched_fp32", kaplan_surrogate=True))
