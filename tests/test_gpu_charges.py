@@ -132,8 +132,8 @@ def test_charge_release_batched_matches_plain(ge_lattice, wl):
     release phase per round: Debye phonons, or photon-seeded film cascades whose escaping
     phonons re-enter the crystal) against the plain FP64 form, which is identical to the
     reference event by event: per-event means of the hits, the collected carriers, the
-    recombination and deposited energy and the steps agree, z < 4 (independent samples);
-    the ledger closes."""
+    recombination, deposited and escaped energy and the steps agree, z < 4 (independent
+    samples). (The field does work on the carriers, so these events have no closed ledger.)"""
     import cmpmc_b200 as cm
     n = 2000
     eng = cm.SimulationEngine(ge_lattice, detector_for(wl))
@@ -142,8 +142,8 @@ def test_charge_release_batched_matches_plain(ge_lattice, wl):
     _, bat = _run(ge_lattice, wl, n, eng=eng)
     ps = summarize(plain.event_stats, plain.hit_offsets, plain.hits)
     bs = summarize(bat.event_stats, bat.hit_offsets, bat.hits)
-    for name in ("n_hits", "charges_collected", "charge_recomb_edep_eV", "total_deposited_eV", "total_steps",
-                 "luke_phonons_emitted", "sum_edep"):
+    for name in ("n_hits", "charges_collected", "charge_recomb_edep_eV", "total_deposited_eV", "escaped_or_killed_eV",
+                 "total_steps", "luke_phonons_emitted", "sum_edep"):
         a, b = _col(ps, name), _col(bs, name)
         se = np.sqrt(a.var(ddof=1) / len(a) + b.var(ddof=1) / len(b))
         if se == 0.0:
@@ -152,8 +152,6 @@ def test_charge_release_batched_matches_plain(ge_lattice, wl):
         z = (b.mean() - a.mean()) / se
         print(f"{wl} {name}: plain {a.mean():.6g} batched {b.mean():.6g} z {z:.2f}")
         assert abs(z) < Z_MAX, (name, z)
-    st = bat.stats
-    assert abs(st.total_injected_eV - st.total_deposited_eV - st.escaped_or_killed_eV) <= 1e-6 * st.total_injected_eV
     if wl == "tpd":  # every collected carrier's energy becomes phonons: the collection hits carry none
         assert np.all(bat.hits["edep"][bat.hits["excitation"] > 0] == 0.0)
 
