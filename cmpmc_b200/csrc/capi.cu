@@ -195,6 +195,7 @@ int ensure_surrogate(cmpmc_gpu_ctx* ctx) {
 // Device counters of the batched charge form (reset per phase except next_carrier)
 struct ChargeCounters {
     unsigned long long q_tail, resume_next, n_resume_out, next_carrier, rel_tail;
+    unsigned long long film_tail, reemit_tail;  // wavefront split inside the queue phases
 };
 
 // The batched FP32 form of events with charges: phase 0 transports the generator's
@@ -269,6 +270,20 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
     ca.rel_cap = rel_cap;
     ca.rel_tail = &cc->rel_tail;
 
+    // wavefront split (the default batched form): the phonon phases end a track at film
+    // entry; film phases run the cascades and queue the re-emissions, as in the phonon-only
+    // split form, until the round's phonons are done
+    const bool split = d->form == CMPMC_FORM_BATCHED_FP32;
+    int bps_f = ctx->bps;
+    if (split && !bps_f) {
+        CK(film_fp32_occupancy(tpb, &bps_f), "occupancy");
+        bps_f = std::max(bps_f, 1);
+    }
+    const uint64_t grid_f = static_cast<uint64_t>(ctx->num_sms) * std::max(bps_f, 1);
+    a.film_tail = &cc->film_tail;
+    a.reemit_tail = &cc->reemit_tail;
+    a.phase_steps = 0;
+
     uint64_t hit_cap = ctx->hit_cap;
     if (!hit_cap) hit_cap = std::max<uint64_t>(1u << 20, (n_ph + n_ch) * 64);
     uint32_t& stack_cap = ctx->stack_cap_batched;
@@ -279,6 +294,61 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
         CK(ctx->queue.ensure(q_cap * sizeof(QPhonon)), "alloc Luke-phonon queue");
         ca.queue = ctx->queue.as<QPhonon>();
         ca.q_cap = q_cap;
+        uint64_t f_cap = 0;
+        bool split_over = false;
+        if (split) {
+            f_cap = std::max<uint64_t>(ctx->film_cap, std::max<uint64_t>(q_cap, std::min<uint64_t>(8 * n_ph, 1ull << 26)));
+            CK(ctx->queue_b.ensure(q_cap * sizeof(QPhonon)), "alloc re-emission queue");
+            CK(ctx->film_a.ensure(f_cap * sizeof(FilmRec)), "alloc film queue");
+            a.film = ctx->film_a.as<FilmRec>();
+            a.film_cap = f_cap;
+            a.reemit = ctx->queue_b.as<QPhonon>();
+            a.reemit_cap = q_cap;
+        }
+        // After a transport launch that wrote its film entries to a.film and read `q_read`:
+        // film phases and transport phases alternate until no phonon is left. q_read is
+        // free again; a.reemit is where the film phase appends.
+        auto drain = [&](QPhonon* q_read) -> int {
+            QPhonon* q_free = q_read;
+            for (;;) {
+                CK(cudaMemcpyAsync(hbuf + sizeof(Counters), cc, sizeof(ChargeCounters), cudaMemcpyDeviceToHost, s),
+                   "copy counters");
+                CK(cudaStreamSynchronize(s), "transport phase");
+                ChargeCounters h = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
+                if (h.film_tail > f_cap || h.reemit_tail > q_cap) {
+                    split_over = true;
+                    return CMPMC_OK;
+                }
+                if (h.film_tail > 0) {
+                    CK(launch_film_fp32(ctx->L, ctx->cdf_f, ctx->D, a, a.film, h.film_tail,
+                                        static_cast<int>(std::min<uint64_t>(grid_f, (h.film_tail + tpb - 1) / tpb)),
+                                        tpb, s),
+                       "film launch");
+                    ++launches;
+                    CK(cudaMemcpyAsync(hbuf + sizeof(Counters), cc, sizeof(ChargeCounters), cudaMemcpyDeviceToHost,
+                                       s),
+                       "copy counters");
+                    CK(cudaStreamSynchronize(s), "film phase");
+                    h = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
+                    if (h.reemit_tail > q_cap) {
+                        split_over = true;
+                        return CMPMC_OK;
+                    }
+                }
+                const uint64_t n_r = h.reemit_tail;
+                if (n_r == 0) return CMPMC_OK;
+                QPhonon* q_in = a.reemit;
+                a.reemit = q_free;
+                q_free = q_in;
+                CK(cudaMemsetAsync(&cc->film_tail, 0, 2 * sizeof(unsigned long long), s), "memset counters");
+                CK(cudaMemsetAsync(&dc->next_work, 0, sizeof(unsigned long long), s), "memset work counter");
+                a.n_events = n_r;
+                CK(launch_queue_fp32(ctx->L, ctx->cdf_f, ctx->D, a, q_in,
+                                     static_cast<int>(std::min<uint64_t>(grid_ph, (n_r + tpb - 1) / tpb)), tpb, s),
+                   "queue launch");
+                ++launches;
+            }
+        };
         CK(ctx->stack.ensure(slots * stack_cap * batched_stack_entry_bytes()), "alloc phonon stacks");
         CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
         CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
@@ -299,12 +369,16 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
                                    static_cast<int>(std::min<uint64_t>(grid_ph, (n_ph + tpb - 1) / tpb)), tpb, s),
                "phonon launch");
             ++launches;
+            if (split) {
+                const int st = drain(ctx->queue.as<QPhonon>());  // the Luke queue is still free here
+                if (st != CMPMC_OK) return st;
+            }
         }
         // charge / queue phases
         QCharge* r_in = ctx->resume_a.as<QCharge>();
         QCharge* r_out = ctx->resume_b.as<QCharge>();
         uint64_t n_resume = 0, carriers_started = 0;
-        for (int round = 0;; ++round) {
+        for (int round = 0; !split_over; ++round) {
             CK(cudaMemsetAsync(ctx->queue.p, 0xff, q_cap * sizeof(QPhonon), s), "memset queue");
             CK(cudaMemsetAsync(&cc->q_tail, 0, 3 * sizeof(unsigned long long), s), "memset counters");
             CK(cudaMemsetAsync(&cc->rel_tail, 0, sizeof(unsigned long long), s), "memset counters");
@@ -332,14 +406,23 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
                 hcc = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
             }
             const uint64_t n_q = std::min<uint64_t>(hcc.q_tail, q_cap);
-            if (n_q) {
+            if (n_q && !split_over) {
                 CK(cudaMemsetAsync(&dc->next_work, 0, sizeof(unsigned long long), s), "memset work counter");
                 a.n_events = n_q;
+                if (split) {
+                    a.reemit = ctx->queue_b.as<QPhonon>();
+                    CK(cudaMemsetAsync(&cc->film_tail, 0, 2 * sizeof(unsigned long long), s), "memset counters");
+                }
                 CK(launch_queue_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ca.queue,
                                      static_cast<int>(std::min<uint64_t>(grid_ph, (n_q + tpb - 1) / tpb)), tpb, s),
                    "queue launch");
                 ++launches;
+                if (split) {
+                    const int st = drain(ca.queue);
+                    if (st != CMPMC_OK) return st;
+                }
             }
+            if (split_over) break;
             const uint64_t started = std::min<uint64_t>(hcc.next_carrier, n_ch);
             const uint64_t parked = hcc.n_resume_out;
             if (parked > resume_cap) return fail(ctx, CMPMC_ERR_CAPACITY, "parked-carrier buffer overflow");
@@ -358,16 +441,24 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
         const bool stack_over = (hc.err & kErrPhononStack) != 0;
         const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
         const bool queue_over = (hc.err & kErrRelease) != 0;  // released phonons did not fit the queue
-        if (!stack_over && !hits_over && !queue_over) break;
-        if (attempt >= 6) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack, hit or queue overflow persists");
+        split_over = split_over || (hc.err & (kErrQueue | kErrFilmQueue)) != 0;
+        if (!stack_over && !hits_over && !queue_over && !split_over) break;
+        if (attempt >= 8) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack, hit or queue overflow persists");
         if (stack_over) stack_cap = std::min<uint32_t>(stack_cap * 8, 1u << 20);
         if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
         if (queue_over) {
-            q_cap *= 4;
+            q_cap *= 8;
             ctx->queue_cap = std::max<uint64_t>(ctx->queue_cap, q_cap);
+        }
+        if (split_over) {
+            q_cap *= queue_over ? 1 : 4;
+            ctx->queue_cap = std::max<uint64_t>(ctx->queue_cap, q_cap);
+            ctx->film_cap = std::max<uint64_t>(ctx->film_cap, 2 * f_cap);
         }
         hc.err = 0;
     }
+    a.film = nullptr;
+    a.reemit = nullptr;
     if (d->keep_hits) ctx->hit_cap = std::max<uint64_t>(ctx->hit_cap, hit_cap);
     if (hc.err) return fail(ctx, CMPMC_ERR_DEVICE, "transport kernels reported error word " + std::to_string(hc.err));
     n_hits = d->keep_hits ? hc.hit_count : 0;
