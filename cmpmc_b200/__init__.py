@@ -10,7 +10,7 @@ from .api import (AluminumFilm, CmpmcError, ElectrodePad, ElectrodePatternMask, 
                   SimStats, SimulationEngine, SuperconductorFilmConfig, SurfaceId, SurfaceProperty,
                   TriLinearMesh3D, BiLinearMesh2D, UniformElectricField, UnvalidatedModuleError, Workload, materials, run_events, units, workloads)
 from .partition import (EmpiricalNIELParams, EnergyPartition, HitMerger, NIELModel, PartitionOptions, PartitionResult,
-                        PrimaryStepInput, physics)
+                        PrimaryStepInput, partition_deposits_on_device, physics)
 from .adjoint import AdjointResult, HistogramAdjoint, THETA_NAMES, default_theta
 
 __all__ = [
@@ -21,5 +21,5 @@ __all__ = [
     "UniformElectricField",
     "UnvalidatedModuleError", "Workload", "materials", "run_events", "units", "workloads", "HistogramAdjoint",
     "THETA_NAMES", "default_theta", "EmpiricalNIELParams", "EnergyPartition", "HitMerger", "NIELModel",
-    "PartitionOptions", "PartitionResult", "PrimaryStepInput", "physics",
+    "PartitionOptions", "PartitionResult", "PrimaryStepInput", "partition_deposits_on_device", "physics",
 ]

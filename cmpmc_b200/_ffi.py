@@ -167,6 +167,10 @@ class TuneResultC(C.Structure):
     ]
 
 
+DEPOSIT_DTYPE = np.dtype([("pos", "<f8", 3), ("time_s", "<f8"), ("edep_eV", "<f8"), ("is_nuclear_recoil", "<i4"),
+                          ("_pad", "<i4")])
+
+
 class PartitionOptionsC(C.Structure):
     _fields_ = [("niel_model", _i32), ("use_fano_fluctuations", _i32), ("use_charge_cloud", _i32),
                 ("max_sampled_pairs", _u32), ("max_sampled_phonons", _u32), ("emp_energy_dependent_k", _i32),
@@ -240,6 +244,9 @@ _SIG = {
     "cmpmc_partition_deposit": (_i32, [C.c_void_p, C.POINTER(_f64), _f64, _f64, _i32, C.POINTER(PartitionOptionsC),
                                        _U64x4, C.c_void_p, _u64, C.POINTER(_u64), C.c_void_p, _u64,
                                        C.POINTER(_u64), C.POINTER(PartitionResultC)]),
+    "cmpmc_gpu_partition_deposits": (_i32, [C.c_void_p, C.c_void_p, _u64, C.POINTER(PartitionOptionsC), C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, _u64, C.c_void_p, _u64, C.POINTER(_u64),
+                                            C.POINTER(_u64)]),
     "cmpmc_hit_merger_create": (_i32, [C.c_void_p, _f64, C.POINTER(PartitionOptionsC), C.POINTER(C.c_void_p)]),
     "cmpmc_hit_merger_destroy": (None, [C.c_void_p]),
     "cmpmc_hit_merger_process_steps": (_i32, [C.c_void_p, C.POINTER(PrimaryStepC), _u64, _U64x4, C.POINTER(_u64)]),

@@ -38,6 +38,7 @@ SOURCES = {
     "partition_host.cpp": [],
     "kaplan_lut.cpp": [],
     "transport_plain.cu": ["--fmad=false"],
+    "partition_gpu.cu": ["--fmad=false"],
     # FP32 intrinsics for the batched phonon kernels (about 3 % faster; the chi^2 parity and
     # the FP64 ledger are unchanged); the FP64 Kaplan cascade is not affected
     "transport_batched.cu": ["--use_fast_math"],

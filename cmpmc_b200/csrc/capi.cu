@@ -104,6 +104,7 @@ struct cmpmc_gpu_ctx {
     bool lut_ready = false;
     DevBuf queue, resume_a, resume_b, ccounters, carrier_event, cursor;  // batched charge form
     DevBuf rel;                                         // batched charge release records
+    DevBuf part_plans, part_counts;                     // device partition: plans, per-deposit counts
     DevBuf film_a, queue_b;                             // wavefront split: film entries, second phonon queue
     uint64_t film_cap = 1ull << 22;                     // film entries per phase (64 B each)
     uint32_t phase_steps = 0;                           // steps a track takes per transport phase (0: any)
@@ -754,7 +755,7 @@ void cmpmc_gpu_destroy(cmpmc_gpu_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (DevBuf* b : {&ctx->kin, &ctx->film_a, &ctx->queue_b, &ctx->rel, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->mesh2, &ctx->mesh2_32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
+    for (DevBuf* b : {&ctx->kin, &ctx->film_a, &ctx->queue_b, &ctx->rel, &ctx->part_plans, &ctx->part_counts, &ctx->lut[0], &ctx->lut[1], &ctx->lut[2], &ctx->pads[0], &ctx->pads[1], &ctx->pads[2], &ctx->tables, &ctx->mesh, &ctx->mesh32, &ctx->mesh2, &ctx->mesh2_32, &ctx->queue, &ctx->resume_a, &ctx->resume_b,
                       &ctx->ccounters, &ctx->carrier_event, &ctx->cursor, &ctx->in_rng, &ctx->in_inj, &ctx->in_phoff, &ctx->in_ph, &ctx->in_choff,
                       &ctx->in_ch, &ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters,
                       &ctx->ev_stats, &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total,
@@ -994,6 +995,43 @@ int cmpmc_gpu_set_mesh2d(cmpmc_gpu_ctx* ctx, const cmpmc_mesh2d* mesh) {
     CK(cudaMemcpy(ctx->mesh2_32.p, r32.data(), n * sizeof(MeshTri32), cudaMemcpyHostToDevice), "copy FP32 2D mesh");
     ctx->D.mesh2 = MeshView2{ctx->mesh2.as<MeshTri>(), static_cast<int32_t>(n), mesh->axisym};
     ctx->D.mesh2_32 = MeshView2_32{ctx->mesh2_32.as<MeshTri32>(), static_cast<int32_t>(n), mesh->axisym};
+    return CMPMC_OK;
+}
+
+int cmpmc_gpu_partition_deposits(cmpmc_gpu_ctx* ctx, const cmpmc_deposit* deposits, uint64_t n,
+                                 const cmpmc_partition_options* opts, uint64_t* rng_state, uint64_t* charge_offsets,
+                                 uint64_t* phonon_offsets, cmpmc_charge_track* charges, uint64_t charge_cap,
+                                 cmpmc_phonon_track* phonons, uint64_t phonon_cap, uint64_t* n_charges,
+                                 uint64_t* n_phonons) {
+    if (!ctx || !n_charges || !n_phonons || !charge_offsets || !phonon_offsets) return CMPMC_ERR_INVALID;
+    ctx->last_status = CMPMC_OK;
+    ctx->last_error.clear();
+    *n_charges = *n_phonons = 0;
+    const cmpmc_partition_options o = opts ? *opts : default_partition_options();
+    if (o.niel_model < CMPMC_NIEL_LINDHARD || o.niel_model > CMPMC_NIEL_EMPIRICAL || o.max_sampled_pairs == 0 ||
+        o.max_sampled_phonons == 0)
+        return fail(ctx, CMPMC_ERR_INVALID, "partition options");
+    if (n > 0 && (!deposits || !rng_state)) return fail(ctx, CMPMC_ERR_INVALID, "deposits and generator states");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = ctx->stream;
+    CK(ctx->part_plans.ensure(std::max<uint64_t>(n, 1) * partition_plan_bytes()), "alloc partition plans");
+    CK(ctx->part_counts.ensure(std::max<uint64_t>(2 * n, 2) * 8), "alloc partition counts");
+    uint64_t* cnt = ctx->part_counts.as<uint64_t>();
+    CK(launch_partition_plan(ctx->cfg, o, deposits, n, rng_state, ctx->part_plans.p, cnt, cnt + n, s), "plan launch");
+    CK(launch_scan_u64(cnt, n, charge_offsets, s), "scan");
+    CK(launch_scan_u64(cnt + n, n, phonon_offsets, s), "scan");
+    uint64_t tot[2] = {0, 0};
+    CK(cudaMemcpyAsync(&tot[0], charge_offsets + n, 8, cudaMemcpyDeviceToHost, s), "copy totals");
+    CK(cudaMemcpyAsync(&tot[1], phonon_offsets + n, 8, cudaMemcpyDeviceToHost, s), "copy totals");
+    CK(cudaStreamSynchronize(s), "partition plan");
+    *n_charges = tot[0];
+    *n_phonons = tot[1];
+    if (tot[0] > charge_cap || tot[1] > phonon_cap || (tot[0] && !charges) || (tot[1] && !phonons))
+        return fail(ctx, CMPMC_ERR_CAPACITY, "record capacity (the totals are set)");
+    CK(launch_partition_fill(ctx->L, ctx->cfg, o, deposits, n, ctx->part_plans.p, charge_offsets, phonon_offsets,
+                             charges, phonons, rng_state, s),
+       "fill launch");
+    CK(cudaStreamSynchronize(s), "partition fill");
     return CMPMC_OK;
 }
 

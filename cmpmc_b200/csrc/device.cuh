@@ -270,6 +270,21 @@ cudaError_t launch_math_check(uint64_t n, const double* x, double* out);
 cudaError_t launch_charges_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                                 const ChargeArgs& c, int grid, int block, cudaStream_t s);
 cudaError_t charges_fp32_occupancy(int block, int* blocks_per_sm);
+// Exclusive scan of n counts into offsets[0..n] (single block)
+cudaError_t launch_scan_u64(const uint64_t* counts, uint64_t n, uint64_t* offsets, cudaStream_t s);
+
+// EnergyPartition::partition_deposit on the device (partition_gpu.cu): the plan pass writes
+// per-deposit counts and plans, the fill pass the records and the final generator states
+struct PartitionPlanRec;
+cudaError_t launch_partition_plan(const cmpmc_crystal_config& cfg, const cmpmc_partition_options& o,
+                                  const cmpmc_deposit* dep, uint64_t n, const uint64_t* rng, void* plans,
+                                  uint64_t* n_charges, uint64_t* n_phonons, cudaStream_t s);
+cudaError_t launch_partition_fill(const Lattice& L, const cmpmc_crystal_config& cfg, const cmpmc_partition_options& o,
+                                  const cmpmc_deposit* dep, uint64_t n, const void* plans, const uint64_t* ch_off,
+                                  const uint64_t* ph_off, cmpmc_charge_track* ch, cmpmc_phonon_track* ph,
+                                  uint64_t* rng, cudaStream_t s);
+size_t partition_plan_bytes();
+
 // The release phase of the batched charge form: c.rel[0, n_rel) into c.queue, hits and ledgers
 cudaError_t launch_release_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                                 const ChargeArgs& c, uint64_t n_rel, int grid, int block, cudaStream_t s);

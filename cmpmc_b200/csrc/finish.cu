@@ -264,6 +264,11 @@ cudaError_t launch_finish(const RunArgs& a, uint64_t* offsets, cmpmc_sensor_hit*
     return launch_reduce_stats(a.ev_stats, a.n_events, partials, total, s, launches);
 }
 
+cudaError_t launch_scan_u64(const uint64_t* counts, uint64_t n, uint64_t* offsets, cudaStream_t s) {
+    k_scan<<<1, kScanThreads, 0, s>>>(counts, n, offsets);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sink_finish(const RunArgs& a, uint64_t n_events, uint64_t* ev_offsets,
                                unsigned long long* cursor, cmpmc_sensor_hit* hits_out, uint64_t out_cap,
                                cmpmc_sim_stats* total, cmpmc_sim_stats* partials, cudaStream_t s, int* launches) {

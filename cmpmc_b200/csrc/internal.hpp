@@ -7,6 +7,7 @@
 
 #include "../../include/cmpmc_gpu.h"
 #include "mesh.cuh"
+#include "partition.cuh"
 #include "transport.cuh"
 
 struct cmpmc_lattice {
@@ -67,23 +68,7 @@ void track_to_record(const Track& t, cmpmc_phonon_track& r);
 Charge charge_from_record(const cmpmc_charge_track& r);
 void charge_to_record(const Charge& c, cmpmc_charge_track& r);
 
-// EnergyPartition::partition_deposit in two parts (partition_host.cpp): the draws up to the
-// pair count, which fix the output sizes, and the records.
-struct PartitionPlan {
-    double edep, yield, ionizing, niel;
-    uint64_t pairs_true, pairs_sampled, phonons_true, phonons_sampled;
-    double charge_weight, phonon_weight, prompt_eV;
-};
+// EnergyPartition::partition_deposit (partition.cuh) with the reference's default options
 cmpmc_partition_options default_partition_options();
-PartitionPlan plan_partition(const cmpmc_crystal_config& cfg, double edep, bool is_nr,
-                             const cmpmc_partition_options& o, Rng& rng);
-void fill_partition(const Lattice& L, const cmpmc_crystal_config& cfg, const PartitionPlan& d,
-                    const cmpmc_partition_options& o, V3 pos, double time_s, Rng& rng, cmpmc_charge_track* ch,
-                    cmpmc_phonon_track* ph);
-double rng_normal(Rng& rng);
-uint64_t sample_fano_binomial(double mean, double fano, Rng& rng);
-double ionization_yield(int model, double energy_eV, const cmpmc_crystal_config& cfg,
-                        const cmpmc_partition_options& o);
-double lindhard_yield(double energy_eV, const cmpmc_crystal_config& cfg, double z1, double a1);
 
 }  // namespace cmpmc_gpu

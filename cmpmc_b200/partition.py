@@ -230,3 +230,39 @@ class HitMerger:
         _check(self._lib.cmpmc_hit_merger_take(self._h, ch.ctypes.data, len(ch), C.byref(nc), ph.ctypes.data, len(ph),
                                                C.byref(nph)), what="take")
         return ch, ph
+
+
+def partition_deposits_on_device(engine, deposits, rng_state, opts: Optional[PartitionOptions] = None,
+                                 device: int = 0):
+    """EnergyPartition::partition_deposit for every deposit on the engine's device
+    (cmpmc_gpu_partition_deposits): deposit i draws from rng_state[i] (n x 4 uint64).
+    deposits: a DEPOSIT_DTYPE array (pos, time_s, edep_eV, is_nuclear_recoil). Returns the
+    CSR offsets and records of the carriers and phonons per deposit and the advanced
+    generator states, as host arrays. Device buffers come from torch, which this helper
+    imports; C callers pass their own device memory."""
+    import torch
+    lib = _ffi.load()
+    dep = np.ascontiguousarray(deposits, dtype=_ffi.DEPOSIT_DTYPE)
+    n = len(dep)
+    st = np.ascontiguousarray(rng_state, dtype=np.uint64).reshape(n, 4)
+    dev = f"cuda:{device}"
+    t_dep = torch.from_numpy(dep.view(np.uint8).reshape(-1).copy()).to(dev)
+    t_rng = torch.from_numpy(st.view(np.int64).copy()).to(dev)
+    t_coff = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    t_poff = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    h = engine.context(device)
+    o = (opts or PartitionOptions()).to_c()
+    nc, nph = C.c_uint64(0), C.c_uint64(0)
+    args = (h, t_dep.data_ptr(), n, C.byref(o), t_rng.data_ptr(), t_coff.data_ptr(), t_poff.data_ptr())
+    status = lib.cmpmc_gpu_partition_deposits(*args, None, 0, None, 0, C.byref(nc), C.byref(nph))
+    if status not in (0, 4):
+        _check(status, h)
+    t_ch = torch.zeros(max(1, nc.value) * 128, dtype=torch.uint8, device=dev)
+    t_ph = torch.zeros(max(1, nph.value) * 128, dtype=torch.uint8, device=dev)
+    _check(lib.cmpmc_gpu_partition_deposits(*args, t_ch.data_ptr(), nc.value, t_ph.data_ptr(), nph.value,
+                                            C.byref(nc), C.byref(nph)), h)
+    ch = t_ch.cpu().numpy().view(_ffi.CHARGE_DTYPE)[:nc.value].copy()
+    ph = t_ph.cpu().numpy().view(_ffi.PHONON_DTYPE)[:nph.value].copy()
+    return (t_coff.cpu().numpy().view(np.uint64), ch, t_poff.cpu().numpy().view(np.uint64), ph,
+            t_rng.cpu().numpy().view(np.uint64).reshape(n, 4))
+

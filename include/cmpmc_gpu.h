@@ -358,6 +358,16 @@ int cmpmc_partition_deposit(const cmpmc_lattice* lat, const double pos[3], doubl
                             cmpmc_charge_track* charges, uint64_t charge_cap, uint64_t* n_charges,
                             cmpmc_phonon_track* phonons, uint64_t phonon_cap, uint64_t* n_phonons,
                             cmpmc_partition_result* result);
+/* One energy deposit for the device partition: partition_deposit(pos, time_s, edep_eV,
+ * is_nuclear_recoil, ...) (energy_partition.hpp:78-86) */
+typedef struct cmpmc_deposit {
+    double pos[3];
+    double time_s;
+    double edep_eV;
+    int32_t is_nuclear_recoil;
+    int32_t _pad;
+} cmpmc_deposit;
+
 /* PrimaryStepInput (energy_partition.hpp:182-192) */
 typedef struct cmpmc_primary_step {
     int32_t track_id;
@@ -546,6 +556,24 @@ int cmpmc_gpu_set_mesh(cmpmc_gpu_ctx* ctx, const cmpmc_mesh* mesh);
 /* DetectorModel::mesh_field_2d (engine.hpp:100, used when there is no 3D mesh,
  * engine.hpp:151-155): copies the 2D mesh to the context's device; NULL detaches it. */
 int cmpmc_gpu_set_mesh2d(cmpmc_gpu_ctx* ctx, const cmpmc_mesh2d* mesh);
+
+/* EnergyPartition::partition_deposit (energy_partition.hpp:78-167) for n deposits on the
+ * context's device: deposit i draws from rng_state[i] (4 u64, advanced in place, e.g. an
+ * event's state after its generator drew the deposit) with the reference's draw order, and
+ * its 2 n_pairs_sampled carriers (e-, h+ interleaved) and n_phonons_sampled prompt phonons
+ * go to charges[charge_offsets[i] .. charge_offsets[i+1]) and
+ * phonons[phonon_offsets[i] .. phonon_offsets[i+1]): the initial stacks of
+ * cmpmc_gpu_run_events with inputs_on_device. deposits, rng_state, the offsets ([n + 1])
+ * and the records are device memory; *n_charges / *n_phonons (host) receive the totals.
+ * A capacity that is too small returns CMPMC_ERR_CAPACITY with the totals and the offsets
+ * written and rng_state unchanged. The device's transcendentals are correctly rounded, so
+ * a record can differ from the host partition's (cmpmc_partition_deposit, which uses the
+ * platform libm like the reference) in the last bits where the platform libm is not. */
+int cmpmc_gpu_partition_deposits(cmpmc_gpu_ctx* ctx, const cmpmc_deposit* deposits, uint64_t n,
+                                 const cmpmc_partition_options* opts, uint64_t* rng_state, uint64_t* charge_offsets,
+                                 uint64_t* phonon_offsets, cmpmc_charge_track* charges, uint64_t charge_cap,
+                                 cmpmc_phonon_track* phonons, uint64_t phonon_cap, uint64_t* n_charges,
+                                 uint64_t* n_phonons);
 
 /* Allocation-free run of the plain FP64 form (phonon-only events). No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc -- code running inside a
