@@ -292,19 +292,21 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
     char* hbuf = ctx->h_counters.as<char>();
     for (int attempt = 0;; ++attempt) {
         if (!d->keep_hits) hit_cap = 1;
-        CK(ctx->queue.ensure(q_cap * sizeof(QPhonon)), "alloc Luke-phonon queue");
+        // split phases: film entries and re-emissions of one phase get their own capacity
+        // (f_cap entries each); the Luke-queue buffer doubles as a re-emission queue, so it
+        // holds max(q_cap, f_cap) entries while the Luke reservations stay below q_cap
+        const uint64_t f_cap = split ? std::max<uint64_t>(q_cap, ctx->film_cap) : 0;
+        CK(ctx->queue.ensure(std::max(q_cap, f_cap) * sizeof(QPhonon)), "alloc Luke-phonon queue");
         ca.queue = ctx->queue.as<QPhonon>();
         ca.q_cap = q_cap;
-        uint64_t f_cap = 0;
         bool split_over = false;
         if (split) {
-            f_cap = std::max<uint64_t>(ctx->film_cap, std::max<uint64_t>(q_cap, std::min<uint64_t>(8 * n_ph, 1ull << 26)));
-            CK(ctx->queue_b.ensure(q_cap * sizeof(QPhonon)), "alloc re-emission queue");
+            CK(ctx->queue_b.ensure(f_cap * sizeof(QPhonon)), "alloc re-emission queue");
             CK(ctx->film_a.ensure(f_cap * sizeof(FilmRec)), "alloc film queue");
             a.film = ctx->film_a.as<FilmRec>();
             a.film_cap = f_cap;
             a.reemit = ctx->queue_b.as<QPhonon>();
-            a.reemit_cap = q_cap;
+            a.reemit_cap = f_cap;
         }
         // After a transport launch that wrote its film entries to a.film and read `q_read`:
         // film phases and transport phases alternate until no phonon is left. q_read is
@@ -316,7 +318,7 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
                    "copy counters");
                 CK(cudaStreamSynchronize(s), "transport phase");
                 ChargeCounters h = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
-                if (h.film_tail > f_cap || h.reemit_tail > q_cap) {
+                if (h.film_tail > f_cap || h.reemit_tail > f_cap) {
                     split_over = true;
                     return CMPMC_OK;
                 }
@@ -331,7 +333,7 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
                        "copy counters");
                     CK(cudaStreamSynchronize(s), "film phase");
                     h = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
-                    if (h.reemit_tail > q_cap) {
+                    if (h.reemit_tail > f_cap) {
                         split_over = true;
                         return CMPMC_OK;
                     }
@@ -451,10 +453,10 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
             q_cap *= 8;
             ctx->queue_cap = std::max<uint64_t>(ctx->queue_cap, q_cap);
         }
-        if (split_over) {
-            q_cap *= queue_over ? 1 : 4;
-            ctx->queue_cap = std::max<uint64_t>(ctx->queue_cap, q_cap);
-            ctx->film_cap = std::max<uint64_t>(ctx->film_cap, 2 * f_cap);
+        if (split_over) {  // only the split phases' buffers grow (64 B per entry and buffer)
+            if (f_cap >= (1ull << 28))
+                return fail(ctx, CMPMC_ERR_CAPACITY, "film / re-emission phase exceeds 2^28 entries");
+            ctx->film_cap = std::max<uint64_t>(ctx->film_cap, 4 * f_cap);
         }
         hc.err = 0;
     }
