@@ -1017,15 +1017,22 @@ int cmpmc_gpu_partition_deposits(cmpmc_gpu_ctx* ctx, const cmpmc_deposit* deposi
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     cudaStream_t s = ctx->stream;
     CK(ctx->part_plans.ensure(std::max<uint64_t>(n, 1) * partition_plan_bytes()), "alloc partition plans");
-    CK(ctx->part_counts.ensure(std::max<uint64_t>(2 * n, 2) * 8), "alloc partition counts");
+    CK(ctx->part_counts.ensure((2 * n + 1) * 8), "alloc partition counts");
     uint64_t* cnt = ctx->part_counts.as<uint64_t>();
-    CK(launch_partition_plan(ctx->cfg, o, deposits, n, rng_state, ctx->part_plans.p, cnt, cnt + n, s), "plan launch");
+    unsigned long long* bad = reinterpret_cast<unsigned long long*>(cnt + 2 * n);  // non-finite deposits
+    CK(cudaMemsetAsync(bad, 0, 8, s), "memset");
+    CK(launch_partition_plan(ctx->cfg, o, deposits, n, rng_state, ctx->part_plans.p, cnt, cnt + n, bad, s),
+       "plan launch");
     CK(launch_scan_u64(cnt, n, charge_offsets, s), "scan");
     CK(launch_scan_u64(cnt + n, n, phonon_offsets, s), "scan");
-    uint64_t tot[2] = {0, 0};
+    uint64_t tot[3] = {0, 0, 0};
     CK(cudaMemcpyAsync(&tot[0], charge_offsets + n, 8, cudaMemcpyDeviceToHost, s), "copy totals");
     CK(cudaMemcpyAsync(&tot[1], phonon_offsets + n, 8, cudaMemcpyDeviceToHost, s), "copy totals");
+    CK(cudaMemcpyAsync(&tot[2], bad, 8, cudaMemcpyDeviceToHost, s), "copy totals");
     CK(cudaStreamSynchronize(s), "partition plan");
+    if (tot[2] > 0)  // nothing was filled and rng_state is unchanged
+        return fail(ctx, CMPMC_ERR_INVALID,
+                    std::to_string(tot[2]) + " deposit(s) with a non-finite energy, position or time");
     *n_charges = tot[0];
     *n_phonons = tot[1];
     if (tot[0] > charge_cap || tot[1] > phonon_cap || (tot[0] && !charges) || (tot[1] && !phonons))

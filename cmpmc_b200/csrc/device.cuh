@@ -278,7 +278,8 @@ cudaError_t launch_scan_u64(const uint64_t* counts, uint64_t n, uint64_t* offset
 struct PartitionPlanRec;
 cudaError_t launch_partition_plan(const cmpmc_crystal_config& cfg, const cmpmc_partition_options& o,
                                   const cmpmc_deposit* dep, uint64_t n, const uint64_t* rng, void* plans,
-                                  uint64_t* n_charges, uint64_t* n_phonons, cudaStream_t s);
+                                  uint64_t* n_charges, uint64_t* n_phonons, unsigned long long* n_bad,
+                                  cudaStream_t s);
 cudaError_t launch_partition_fill(const Lattice& L, const cmpmc_crystal_config& cfg, const cmpmc_partition_options& o,
                                   const cmpmc_deposit* dep, uint64_t n, const void* plans, const uint64_t* ch_off,
                                   const uint64_t* ph_off, cmpmc_charge_track* ch, cmpmc_phonon_track* ph,

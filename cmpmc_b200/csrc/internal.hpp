@@ -18,6 +18,7 @@ struct cmpmc_lattice {
     cmpmc_gpu::Stiffness stiff;            // C_ijlm (exact kinematics)
     std::vector<double> bil;               // [3][181][361][3] (bilinear kinematics, built on request)
     cmpmc_gpu::Lattice view;               // host pointers into the members above
+    uint64_t id = 0;                       // unique per created lattice (never reused in a process)
 };
 
 struct cmpmc_kaplan_lut {

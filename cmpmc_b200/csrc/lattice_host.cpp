@@ -6,6 +6,7 @@
 // the FP64 inverse-CDF tables are bit-identical to the CPU library's (checked against the
 // reference's own tables by the test suite). Compiled by the host compiler without FMA
 // contraction.
+#include <atomic>
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -368,6 +369,8 @@ int cmpmc_lattice_create(const cmpmc_crystal_config* cfg, cmpmc_lattice** out) {
     if (!lat) return CMPMC_ERR_INVALID;
     lat->cfg = *cfg;
     build_tables(*lat);
+    static std::atomic<uint64_t> next_id{1};
+    lat->id = next_id.fetch_add(1);
     *out = lat;
     return CMPMC_OK;
 }

@@ -218,8 +218,8 @@ CMPMC_HD double ionization_yield(int model, double energy_eV, const cmpmc_crysta
             if (!si || energy_eV > 3.0 * 1e6) return lewin_smith_yield(energy_eV, cfg);
             if (energy_eV <= sarkis_knot(0).e_eV) return 0.0;
             if (energy_eV >= sarkis_knot(63).e_eV) return sarkis_knot(63).yield;
-            int hi = 1;  // first knot above the energy
-            while (!(energy_eV < sarkis_knot(hi).e_eV)) ++hi;
+            int hi = 1;  // first knot above the energy (bounded: a NaN energy stops at the last knot)
+            while (hi < 63 && !(energy_eV < sarkis_knot(hi).e_eV)) ++hi;
             const YieldKnot k0 = sarkis_knot(hi - 1);
             const YieldKnot k1 = sarkis_knot(hi);
             const double t = (energy_eV - k0.e_eV) / (k1.e_eV - k0.e_eV);

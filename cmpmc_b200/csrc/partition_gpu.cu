@@ -12,6 +12,13 @@ namespace cmpmc_gpu {
 
 namespace {
 
+// a deposit whose energy, position or time is not finite is refused (the reference's NIEL
+// yields and pair counts are undefined there)
+__device__ __forceinline__ bool deposit_finite(const cmpmc_deposit& e) {
+    return isfinite(e.edep_eV) && isfinite(e.pos[0]) && isfinite(e.pos[1]) && isfinite(e.pos[2]) &&
+           isfinite(e.time_s);
+}
+
 struct PlanRec {
     PartitionPlan d;
     uint64_t s[4];  // generator state after the plan's draws
@@ -21,9 +28,17 @@ __global__ void __launch_bounds__(128) k_partition_plan(const cmpmc_crystal_conf
                                                         const cmpmc_partition_options o,
                                                         const cmpmc_deposit* __restrict__ dep, uint64_t n,
                                                         const uint64_t* __restrict__ rng, PlanRec* __restrict__ plans,
-                                                        uint64_t* __restrict__ n_ch, uint64_t* __restrict__ n_ph) {
+                                                        uint64_t* __restrict__ n_ch, uint64_t* __restrict__ n_ph,
+                                                        unsigned long long* __restrict__ bad) {
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const cmpmc_deposit& e = dep[i];
+        if (!deposit_finite(e)) {  // counted and skipped: the call fails before the fill
+            atomicAdd(bad, 1ull);
+            n_ch[i] = 0;
+            n_ph[i] = 0;
+            continue;
+        }
         Rng r;
         for (int k = 0; k < 4; ++k) r.s[k] = rng[4 * i + k];
         PlanRec p;
@@ -62,10 +77,11 @@ size_t partition_plan_bytes() { return sizeof(PlanRec); }
 
 cudaError_t launch_partition_plan(const cmpmc_crystal_config& cfg, const cmpmc_partition_options& o,
                                   const cmpmc_deposit* dep, uint64_t n, const uint64_t* rng, void* plans,
-                                  uint64_t* n_charges, uint64_t* n_phonons, cudaStream_t s) {
+                                  uint64_t* n_charges, uint64_t* n_phonons, unsigned long long* n_bad,
+                                  cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     k_partition_plan<<<grid_for(n), 128, 0, s>>>(cfg, o, dep, n, rng, static_cast<PlanRec*>(plans), n_charges,
-                                                 n_phonons);
+                                                 n_phonons, n_bad);
     return cudaGetLastError();
 }
 

@@ -180,6 +180,10 @@ int cmpmc_partition_deposit(const cmpmc_lattice* lat, const double pos[3], doubl
     if (!lat || !pos || !rng_state || !n_charges || !n_phonons) return CMPMC_ERR_INVALID;
     const cmpmc_partition_options o = opts ? *opts : default_partition_options();
     if (!options_ok(o)) return CMPMC_ERR_INVALID;
+    // the NIEL yields and pair counts are undefined for a non-finite deposit: refuse it
+    if (!std::isfinite(total_edep_eV) || !std::isfinite(time_s) || !std::isfinite(pos[0]) || !std::isfinite(pos[1]) ||
+        !std::isfinite(pos[2]))
+        return CMPMC_ERR_INVALID;
     Rng r = rng_of(rng_state);
     const PartitionPlan d = plan_partition(lat->cfg, total_edep_eV, is_nuclear_recoil != 0, o, r);
     *n_charges = 2 * d.pairs_sampled;

@@ -352,34 +352,47 @@ __global__ void __launch_bounds__(1024) k_scan_inplace(uint64_t* __restrict__ a,
     if (t == 0) a[0] = 0;
 }
 
-// run totals over the per-event records, in event order, by one thread (small runs)
-__global__ void k_total_noalloc(const cmpmc_sim_stats* __restrict__ ev, uint64_t n, NoAllocCounters* cnt) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    cmpmc_sim_stats t;
-    memset(&t, 0, sizeof(t));
-    for (uint64_t i = 0; i < n; ++i) {
-        const cmpmc_sim_stats& s = ev[i];
-        t.total_steps += s.total_steps;
-        t.isotope_scatters += s.isotope_scatters;
-        t.polycrystal_scatters += s.polycrystal_scatters;
-        t.decays_L_to_TT += s.decays_L_to_TT;
-        t.decays_L_to_LT += s.decays_L_to_LT;
-        t.surface_refls += s.surface_refls;
-        t.surface_downconversions += s.surface_downconversions;
-        t.sensor_hits += s.sensor_hits;
-        t.killed_tracks += s.killed_tracks;
-        t.total_injected_eV += s.total_injected_eV;
-        t.total_deposited_eV += s.total_deposited_eV;
-        t.escaped_or_killed_eV += s.escaped_or_killed_eV;
+// run totals over the per-event records: one block of kTotThreads threads, each summing a
+// contiguous slice in event order, then a fixed-order pairwise tree over the slices (the
+// result does not depend on scheduling; it may differ from a serial sum in the last bits)
+constexpr int kTotThreads = 128;  // 128 x 208 B of shared memory
+__device__ __forceinline__ void add_stats(cmpmc_sim_stats& t, const cmpmc_sim_stats& s) {
+    t.total_steps += s.total_steps;
+    t.isotope_scatters += s.isotope_scatters;
+    t.polycrystal_scatters += s.polycrystal_scatters;
+    t.decays_L_to_TT += s.decays_L_to_TT;
+    t.decays_L_to_LT += s.decays_L_to_LT;
+    t.surface_refls += s.surface_refls;
+    t.surface_downconversions += s.surface_downconversions;
+    t.sensor_hits += s.sensor_hits;
+    t.killed_tracks += s.killed_tracks;
+    t.total_injected_eV += s.total_injected_eV;
+    t.total_deposited_eV += s.total_deposited_eV;
+    t.escaped_or_killed_eV += s.escaped_or_killed_eV;
+}
+__global__ void __launch_bounds__(kTotThreads)
+    k_total_noalloc(const cmpmc_sim_stats* __restrict__ ev, uint64_t n, NoAllocCounters* cnt) {
+    __shared__ cmpmc_sim_stats part[kTotThreads];
+    const int t = threadIdx.x;
+    const uint64_t chunk = (n + kTotThreads - 1) / kTotThreads;
+    const uint64_t lo = min(n, t * chunk), hi = min(n, lo + chunk);
+    cmpmc_sim_stats acc;
+    memset(&acc, 0, sizeof(acc));
+    for (uint64_t i = lo; i < hi; ++i) add_stats(acc, ev[i]);
+    part[t] = acc;
+    __syncthreads();
+    for (int d = kTotThreads / 2; d > 0; d >>= 1) {
+        if (t < d) add_stats(part[t], part[t + d]);
+        __syncthreads();
     }
-    cnt->total = t;
+    if (t == 0) cnt->total = part[0];
 }
 
 struct NoAllocDevice {
     bool ready = false;
     void* scratch = nullptr;
     void* tables = nullptr;
-    const cmpmc_lattice* uploaded = nullptr;
+    uint64_t uploaded = 0;  // id of the lattice whose tables are in g_noalloc_tables (0: none)
 };
 NoAllocDevice g_noalloc_dev[64];
 
@@ -399,6 +412,9 @@ extern "C" int cmpmc_gpu_run_events_noalloc(const cmpmc_lattice* lat, const cmpm
     if (n_events > 0 && (!rng_state || !injected_eV || !phonon_offsets || !phonons || !event_stats || !hit_offsets))
         return CMPMC_ERR_INVALID;
     if (n_events > (1ull << 31)) return CMPMC_ERR_INVALID;
+    // only the octahedral table is staged in the module array: the Exact and Bilinear modes
+    // read tables that live in host memory here, so they are refused before any device work
+    if (lat->view.kin_mode != kKinOctahedral) return CMPMC_ERR_INVALID;
     std::string err;
     if (validate_config(lat->cfg, *det, false, err) != CMPMC_OK) return CMPMC_ERR_INVALID;
     if (cudaSetDevice(device) != cudaSuccess) return CMPMC_ERR_NO_DEVICE;
@@ -411,7 +427,7 @@ extern "C" int cmpmc_gpu_run_events_noalloc(const cmpmc_lattice* lat, const cmpm
         nd.ready = true;
     }
     const size_t oct_bytes = lat->oct.size() * sizeof(OctEntry);
-    if (nd.uploaded != lat) {
+    if (nd.uploaded != lat->id) {
         if (cudaMemcpyAsync(nd.tables, lat->oct.data(), oct_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
             cudaMemcpyAsync(static_cast<char*>(nd.tables) + oct_bytes, lat->cdf_lt.data(), kNCdf * sizeof(double),
                             cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -419,9 +435,11 @@ extern "C" int cmpmc_gpu_run_events_noalloc(const cmpmc_lattice* lat, const cmpm
                             kNCdf * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
             return CMPMC_ERR_CUDA;
         if (cudaStreamSynchronize(s) != cudaSuccess) return CMPMC_ERR_CUDA;
-        nd.uploaded = lat;
+        nd.uploaded = lat->id;
     }
     Lattice L = lat->view;
+    L.stiff = nullptr;
+    L.bil = nullptr;
     L.oct = static_cast<const OctEntry*>(nd.tables);
     L.cdf_lt = reinterpret_cast<const double*>(static_cast<char*>(nd.tables) + oct_bytes);
     L.cdf_tt = L.cdf_lt + kNCdf;
@@ -446,7 +464,7 @@ extern "C" int cmpmc_gpu_run_events_noalloc(const cmpmc_lattice* lat, const cmpm
         if (cudaGetLastError() != cudaSuccess) return CMPMC_ERR_CUDA;
         if (pass == 0) {
             k_scan_inplace<<<1, 1024, 0, s>>>(hit_offsets, n_events);
-            k_total_noalloc<<<1, 32, 0, s>>>(event_stats, n_events, cnt);
+            k_total_noalloc<<<1, kTotThreads, 0, s>>>(event_stats, n_events, cnt);
             if (cudaGetLastError() != cudaSuccess) return CMPMC_ERR_CUDA;
             if (cudaMemcpyAsync(&hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
                 cudaMemcpyAsync(n_hits, hit_offsets + n_events, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||

@@ -565,6 +565,9 @@ int cmpmc_gpu_set_mesh2d(cmpmc_gpu_ctx* ctx, const cmpmc_mesh2d* mesh);
  * phonons[phonon_offsets[i] .. phonon_offsets[i+1]): the initial stacks of
  * cmpmc_gpu_run_events with inputs_on_device. deposits, rng_state, the offsets ([n + 1])
  * and the records are device memory; *n_charges / *n_phonons (host) receive the totals.
+ * A deposit whose energy, position or time is not finite makes the call return
+ * CMPMC_ERR_INVALID before any record is written (rng_state unchanged); so does the host
+ * cmpmc_partition_deposit.
  * A capacity that is too small returns CMPMC_ERR_CAPACITY with the totals and the offsets
  * written and rng_state unchanged. The device's transcendentals are correctly rounded, so
  * a record can differ from the host partition's (cmpmc_partition_deposit, which uses the
@@ -587,11 +590,15 @@ int cmpmc_gpu_partition_deposits(cmpmc_gpu_ctx* ctx, const cmpmc_deposit* deposi
  *   host   : *total (run SimStats), *n_hits (hits the run produced, also when they do not fit)
  * At most 64 tracks may sit on one event's stack at a time (CMPMC_ERR_CAPACITY otherwise);
  * CMPMC_ERR_CAPACITY is also returned when *n_hits > hit_capacity (nothing is written).
+ * The lattice must use the octahedral kinematics mode (the default); a lattice switched to
+ * Exact or Bilinear returns CMPMC_ERR_INVALID before any device work.
  * The transport runs twice (count, then write), so a call costs about two plain runs.
- * The first call on a device resolves the array's device address and uploads the tables:
- * make it before any stream capture. Calls share the array and clear what they use, so
- * calls whose work overlaps on the GPU race: serialize them. `stream` is a cudaStream_t
- * (NULL: the default stream). */
+ * The first call on a device resolves the array's device address, and the first call with
+ * a given lattice uploads its tables: make these calls before any stream capture. Every
+ * call waits for `stream` to finish before it returns (it reads the run totals and the hit
+ * count back to the host). Calls share the array and clear what they use, so calls whose
+ * work overlaps on the GPU race: serialize them. `stream` is a cudaStream_t (NULL: the
+ * default stream). */
 int cmpmc_gpu_run_events_noalloc(const cmpmc_lattice* lat, const cmpmc_detector* det, int device,
                                  uint64_t n_events, const uint64_t* rng_state, const double* injected_eV,
                                  const uint64_t* phonon_offsets, const cmpmc_phonon_track* phonons,

@@ -107,3 +107,30 @@ def test_device_partition_capacity_and_transport(ge_lattice):
     res = eng.run_packed(packed, cm.RunOptions(seed=13, form="batched_fp32", want_event_stats=True))
     assert res.stats.charge_steps > 0 and res.stats.total_steps > 0
     assert res.stats.charges_collected > 0
+
+
+def test_device_partition_refuses_non_finite_deposit(ge_lattice):
+    """One deposit with a NaN energy makes the call return CMPMC_ERR_INVALID before the fill:
+    no record is written and every generator state is left as it was."""
+    import ctypes as C
+    import torch
+    import cmpmc_b200 as cm
+    from cmpmc_b200 import _ffi
+    dep, states = _deposits(13)
+    dep, states = dep[:64].copy(), states[:64].copy()
+    dep[17]["edep_eV"] = np.nan
+    eng = cm.SimulationEngine(ge_lattice, cm.DetectorModel())
+    lib = _ffi.load()
+    h = eng.context(0)
+    t_dep = torch.from_numpy(dep.view(np.uint8).reshape(-1).copy()).to("cuda:0")
+    t_rng = torch.from_numpy(states.view(np.int64).copy()).to("cuda:0")
+    t_off = torch.zeros(2 * 65, dtype=torch.int64, device="cuda:0")
+    t_ch = torch.zeros(4096 * 128, dtype=torch.uint8, device="cuda:0")
+    t_ph = torch.zeros(4096 * 128, dtype=torch.uint8, device="cuda:0")
+    nc, nph = C.c_uint64(0), C.c_uint64(0)
+    st = lib.cmpmc_gpu_partition_deposits(h, t_dep.data_ptr(), 64, None, t_rng.data_ptr(), t_off.data_ptr(),
+                                          t_off.data_ptr() + 65 * 8, t_ch.data_ptr(), 4096, t_ph.data_ptr(), 4096,
+                                          C.byref(nc), C.byref(nph))
+    assert st == _ffi.ERR_INVALID
+    assert np.array_equal(t_rng.cpu().numpy().view(np.uint64), states)
+    assert int(t_ch.count_nonzero()) == 0 and int(t_ph.count_nonzero()) == 0

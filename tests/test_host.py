@@ -371,3 +371,26 @@ def test_no_device_fails_loudly(ge_lattice):
     eng = cm.SimulationEngine(ge_lattice, cm.DetectorModel())
     with pytest.raises(cm.CmpmcError):
         cm.run_events(eng, 4, cm.workloads.single_l_origin, cm.RunOptions(seed=42))
+
+
+def test_noalloc_refuses_non_octahedral_lattice_before_device_work(lib):
+    """The allocation-free entry stages only the octahedral table in its module array, so a
+    lattice in the Exact or Bilinear mode is refused with CMPMC_ERR_INVALID before any CUDA
+    call (without a device, an accepted lattice gets as far as selecting the device)."""
+    import ctypes as C
+    from tests.helpers import has_gpu
+    import cmpmc_b200 as cm
+    from cmpmc_b200 import _ffi
+    det = cm.DetectorModel().to_c()
+    total, n_hits = _ffi.SimStatsC(), C.c_uint64(0)
+
+    def call(lat):
+        return lib.cmpmc_gpu_run_events_noalloc(lat._h, C.byref(det), 0, 0, None, None, None, None, None, None,
+                                                None, 0, None, C.byref(total), C.byref(n_hits))
+
+    for mode in (cm.CrystalLattice.Exact, cm.CrystalLattice.Bilinear):
+        lat = cm.CrystalLattice(cm.materials.Germanium())
+        lat.set_kinematics_mode(mode)
+        assert call(lat) == _ffi.ERR_INVALID
+    octa = cm.CrystalLattice(cm.materials.Germanium())
+    assert call(octa) == (_ffi.OK if has_gpu() else _ffi.ERR_NO_DEVICE)

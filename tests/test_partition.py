@@ -142,3 +142,22 @@ def test_fano_sampler_moments(lattice):
         x = np.array([cm.physics.sample_fano_binomial(mean, fano, rng) for _ in range(4000)], dtype=np.float64)
         assert abs(x.mean() - mean) < 5 * np.sqrt(fano * mean / len(x)) + 0.5
         assert 0.5 * fano * mean < x.var() < 2.0 * fano * mean + 0.5
+
+
+def test_non_finite_deposits_are_refused():
+    """The Sarkis knot search is bounded (a NaN energy returns instead of walking past the
+    last knot), and partition_deposit refuses a non-finite energy, position or time before
+    drawing (the generator state is left alone)."""
+    import math
+    import cmpmc_b200 as cm
+    si = dataclasses.replace(cm.materials.Germanium(), atomic_Z=14.0, atomic_A=28.085)
+    assert math.isnan(cm.physics.sarkis_ionization_yield(float("nan"), si))
+    assert cm.physics.sarkis_ionization_yield(1e3, si) > 0.0
+    part = cm.EnergyPartition(cm.CrystalLattice(cm.materials.Germanium()))
+    for pos, t, e in (((0.0, 0.0, 0.0), 0.0, float("nan")), ((0.0, 0.0, 0.0), 0.0, float("inf")),
+                      ((float("nan"), 0.0, 0.0), 0.0, 100.0), ((0.0, 0.0, 0.0), float("nan"), 100.0)):
+        r = cm.Rng.for_stream(8, 0)
+        before = list(r.s)
+        with pytest.raises(cm.CmpmcError):
+            part.partition_deposit(pos, t, e, False, r)
+        assert r.s == before
