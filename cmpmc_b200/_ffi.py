@@ -20,6 +20,7 @@ OK, ERR_INVALID, ERR_CUDA, ERR_UNVALIDATED, ERR_CAPACITY, ERR_DEVICE, ERR_NO_DEV
 FORM_PLAIN_FP64, FORM_BATCHED_FP32, FORM_BATCHED_FP32_INLINE = 0, 1, 2
 WL_SINGLE_L_ORIGIN, WL_MIXED_ENERGY, WL_PAIR_DRIFT, WL_SINGLE_L_VOLUME, WL_TEST_PARALLEL = 0, 1, 2, 4, 5
 WL_RECOIL, WL_RECOIL_LIGHT = 3, 6
+WL_PUBLISHED_PHONON, WL_PUBLISHED_PAIR = 7, 8
 
 MAX_VALLEYS, MAX_IV, MAX_POLY = 8, 4, 8
 

@@ -13,6 +13,7 @@ The generator is either a Python callable taking an EventInput (as in the refere
 """
 from __future__ import annotations
 
+import copy
 import ctypes as C
 import math
 import os
@@ -735,6 +736,17 @@ class DetectorModel:
     russian_roulette_bounces: int = 0
     russian_roulette_survival: float = 0.5
 
+    @staticmethod
+    def published_benchmark(voltage_V: float = 0.0, luke_sample_fraction: float = 1.0) -> "DetectorModel":
+        """The detector of the reference's published benchmark (benchmarks/cmpmc_bench.cpp:45-57):
+        demo polynomial surfaces (sensor faces with prob_abs 1, a bare side wall; guarded, so
+        allow_unvalidated is set), max_bounces 100, a uniform field of voltage_V over 2.54 cm."""
+        sensor = SurfaceProperty.demo_polynomial_sensor_surface()
+        sensor.prob_abs = 1.0
+        return DetectorModel(e_field=UniformElectricField.from_bias(voltage_V, 2.54 * units.cm),
+                             surfaces=[sensor, copy.deepcopy(sensor), SurfaceProperty.demo_polynomial_bare_surface()],
+                             max_bounces=100, luke_sample_fraction=luke_sample_fraction, allow_unvalidated=True)
+
     def to_c(self) -> _ffi.DetectorC:
         d = _ffi.DetectorC()
         d.radius = self.solid.radius
@@ -896,6 +908,10 @@ class workloads:
     # 0.05 (recoil_light)
     recoil = Workload(_ffi.WL_RECOIL, 1, "electron_recoil_10eV_10keV")
     recoil_light = Workload(_ffi.WL_RECOIL_LIGHT, 1, "electron_recoil_10eV_100eV_light")
+    # the reference's published benchmark (benchmarks/cmpmc_bench.cpp:45-71): run them with
+    # DetectorModel.published_benchmark() (demo polynomial surfaces, max_bounces 100)
+    published_phonon = Workload(_ffi.WL_PUBLISHED_PHONON, 1, "published_phonon_7.5meV_dos_mode")
+    published_pair = Workload(_ffi.WL_PUBLISHED_PAIR, 2, "published_pair_origin")
 
 
 @dataclass

@@ -257,6 +257,8 @@ Counts counts_of(int wl, uint64_t ev) {
         case CMPMC_WL_PAIR_DRIFT: return {0, 2};
         case CMPMC_WL_SINGLE_L_VOLUME: return {1, 0};
         case CMPMC_WL_TEST_PARALLEL: return (ev % 2 == 0) ? Counts{1, 0} : Counts{0, 2};
+        case CMPMC_WL_PUBLISHED_PHONON: return {1, 0};
+        case CMPMC_WL_PUBLISHED_PAIR: return {0, 2};
         default: return {0, 0};
     }
 }
@@ -308,8 +310,17 @@ void gen_event(int wl, const Lattice& L, const cmpmc_crystal_config& cfg, const 
             injected += 7.5e-3;
             break;
         }
+        case CMPMC_WL_PUBLISHED_PHONON: {  // benchmarks/cmpmc_bench.cpp:63-67
+            const double u = rng.uniform();
+            const int m = u < 0.53539 ? 2 : (u < 0.90217 ? 1 : 0);
+            const V3 d = rng.isotropic_dir();
+            track_to_record(make_track(L, origin, d, m, 7.5e-3, 0.0, 1.0), ph[0]);
+            injected += 7.5e-3;
+            break;
+        }
+        case CMPMC_WL_PUBLISHED_PAIR:
         case CMPMC_WL_TEST_PARALLEL: {
-            if (ev % 2 == 0) {
+            if (wl == CMPMC_WL_TEST_PARALLEL && ev % 2 == 0) {
                 const V3 d = rng.isotropic_dir();
                 track_to_record(make_track(L, origin, d, 1, 7.5e-3, 0.0, 1.0), ph[0]);
                 injected += 7.5e-3;
@@ -420,7 +431,8 @@ int cmpmc_generate(const cmpmc_lattice* lat, const cmpmc_detector* det, int work
     if (!lat || !det || !rng_state || !injected_eV || !phonon_offsets || !charge_offsets) return CMPMC_ERR_INVALID;
     if (workload != CMPMC_WL_SINGLE_L_ORIGIN && workload != CMPMC_WL_MIXED_ENERGY &&
         workload != CMPMC_WL_PAIR_DRIFT && workload != CMPMC_WL_SINGLE_L_VOLUME &&
-        workload != CMPMC_WL_TEST_PARALLEL && !is_recoil(workload))
+        workload != CMPMC_WL_TEST_PARALLEL && workload != CMPMC_WL_PUBLISHED_PHONON &&
+        workload != CMPMC_WL_PUBLISHED_PAIR && !is_recoil(workload))
         return CMPMC_ERR_INVALID;
     const Lattice& L = lat->view;
     int nt = n_threads > 0 ? n_threads : static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));

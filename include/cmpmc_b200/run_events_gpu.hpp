@@ -1,27 +1,41 @@
 // run_events_gpu.hpp -- header-only C++ adapter from CMPMC's API to the B200 C ABI.
 //
-// Include this next to the reference's own headers ("cmpmc/cmpmc.hpp"), build one
-// cmpmc_b200::GpuEngine(lattice.config(), detector) and call gpu.run_events(n_events,
-// generate, options) where the reference code calls cmpmc::run_events(engine, n_events,
-// generate, options) (include/cmpmc/transport/parallel.hpp:76-148). The generator is the same user callback:
-// it runs on the host, once per event, from Rng::for_stream(options.seed, i), with the
-// reference's EventInput, Rng and SimulationEngine::make_track, so the initial stacks and
-// the post-generator random state are exactly the reference's. Transport runs on the
-// device; the RunResult is rebuilt from the device output (SensorHit and SimStats records
-// are byte-identical, include/cmpmc_gpu.h).
+// Include this next to the reference's own headers ("cmpmc/cmpmc.hpp"). A call site of
+// the reference's run_events (include/cmpmc/transport/parallel.hpp:76-148)
 //
-// The device needs the crystal's configuration (it rebuilds the CrystalLattice tables with
-// the same arithmetic) and the DetectorModel. Electrode masks are copied from the
-// surfaces' ElectrodePatternMask pads. A TriLinearMesh3D field keeps its nodes private in
-// the reference, so a detector with mesh_field_3d needs the same mesh handed over once with
-// GpuEngine::set_mesh (its node coordinates, potentials and tetrahedra) or
-// set_cartesian_mesh (the build_cartesian_grid arguments and the potential function); a
-// detector with only mesh_field_2d needs its BiLinearMesh2D handed over the same way with
-// set_mesh2d or set_grid_mesh2d.
+//     cmpmc::RunResult r = cmpmc::run_events(engine, n_events, generate, options);
+//
+// moves to the device by changing its namespace only:
+//
+//     cmpmc::RunResult r = cmpmc_b200::run_events(engine, n_events, generate, options);
+//
+// (an optional fifth argument, GpuRunOptions, picks the device and the form). The engine's
+// lattice and detector are turned into a device context once and cached per (lattice,
+// detector, device); a detector whose content changes gets a new context. The generator is
+// the same user callback: it runs on the host, once per event, from
+// Rng::for_stream(options.seed, i), with the reference's EventInput, Rng and
+// SimulationEngine::make_track, so the initial stacks and the post-generator random state
+// are exactly the reference's. Transport runs on the device; the RunResult is rebuilt from
+// the device output (SensorHit and SimStats records are byte-identical, include/cmpmc_gpu.h).
+//
+// The reference's SimulationEngine keeps its lattice and detector as references in its
+// first two data members (engine.hpp:871-872) and has no accessor for them; the adapter
+// reads the two references from the engine's storage. That relies on the Itanium C++ ABI
+// (GCC and Clang on Linux: a reference member is stored as a pointer, members in
+// declaration order) and is checked at compile time against the engine's size.
+//
+// The explicit form is a cmpmc_b200::GpuEngine(lattice, detector) with
+// gpu.run_events(n_events, generate, options); gpu_engine_for(engine) returns the cached
+// one of an engine. Electrode masks are copied from the surfaces' ElectrodePatternMask
+// pads. A TriLinearMesh3D field keeps its nodes private in the reference, so a detector
+// with mesh_field_3d needs the same mesh handed over once with GpuEngine::set_mesh (its
+// node coordinates, potentials and tetrahedra) or set_cartesian_mesh (the
+// build_cartesian_grid arguments and the potential function); a detector with only
+// mesh_field_2d needs its BiLinearMesh2D handed over the same way with set_mesh2d or
+// set_grid_mesh2d (on gpu_engine_for(engine) for the drop-in form).
 // Guarded modules raise the reference's UnvalidatedModuleError; configurations the device
 // does not support (in the batched forms, the Kaplan surrogate with Exact / Bilinear
-// kinematics) raise std::invalid_argument. Build the GpuEngine from the CrystalLattice
-// itself to carry its kinematics mode.
+// kinematics) raise std::invalid_argument.
 #pragma once
 
 #include <algorithm>
@@ -29,7 +43,9 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <deque>
 #include <exception>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -385,5 +401,106 @@ private:
     cmpmc_mesh* mesh_ = nullptr;
     cmpmc_mesh2d* mesh2_ = nullptr;
 };
+
+namespace detail {
+
+// The lattice and detector an engine was built with (see the file comment).
+struct EngineRefs {
+    const cmpmc::CrystalLattice* lattice;
+    const cmpmc::DetectorModel* detector;
+};
+inline EngineRefs refs_of(const cmpmc::SimulationEngine& engine) {
+    static_assert(sizeof(cmpmc::ChargePhysics) == sizeof(void*), "ChargePhysics holds one lattice reference");
+    static_assert(sizeof(cmpmc::SimulationEngine) == 3 * sizeof(void*) &&
+                      alignof(cmpmc::SimulationEngine) == alignof(void*),
+                  "SimulationEngine is {const CrystalLattice&, const DetectorModel&, ChargePhysics}");
+    EngineRefs r;
+    std::memcpy(&r, static_cast<const void*>(&engine), sizeof(r));
+    return r;
+}
+
+inline void append_bytes(std::vector<unsigned char>& k, const void* p, size_t n) {
+    const auto* b = static_cast<const unsigned char*>(p);
+    k.insert(k.end(), b, b + n);
+}
+
+// Everything a device context is built from: the crystal configuration, the kinematics
+// mode, the detector image and the electrode pads (mesh nodes are handed over separately).
+inline std::vector<unsigned char> context_key(const cmpmc::CrystalLattice& lat, const cmpmc::DetectorModel& det,
+                                              int device) {
+    std::vector<unsigned char> k;
+    const cmpmc_crystal_config c = to_c(lat.config());
+    const cmpmc_detector d = to_c(det);
+    const int mode = static_cast<int>(lat.kinematics_mode());
+    append_bytes(k, &device, sizeof(device));
+    append_bytes(k, &mode, sizeof(mode));
+    append_bytes(k, &c, sizeof(c));
+    append_bytes(k, &d, sizeof(d));
+    for (int i = 0; i < 3; ++i) {
+        if (!det.surfaces[i].electrode_mask.has_value()) continue;
+        const auto pads = pads_of(*det.surfaces[i].electrode_mask);
+        append_bytes(k, &i, sizeof(i));
+        if (!pads.empty()) append_bytes(k, pads.data(), pads.size() * sizeof(pads[0]));
+    }
+    return k;
+}
+
+struct CachedContext {
+    const void* lattice;
+    const void* detector;
+    int device;
+    std::vector<unsigned char> key;
+    std::unique_ptr<GpuEngine> gpu;
+    std::unique_ptr<std::mutex> busy;  // a device context serves one call at a time
+};
+
+struct ContextCache {
+    std::mutex m;
+    std::deque<CachedContext> entries;  // appends keep earlier entries in place
+};
+inline ContextCache& context_cache() {
+    static ContextCache cache;
+    return cache;
+}
+
+inline CachedContext& cached_context(const cmpmc::SimulationEngine& engine, int device) {
+    const EngineRefs r = refs_of(engine);
+    std::vector<unsigned char> key = context_key(*r.lattice, *r.detector, device);
+    ContextCache& cache = context_cache();
+    std::lock_guard<std::mutex> lock(cache.m);
+    for (CachedContext& e : cache.entries) {
+        if (e.lattice != r.lattice || e.detector != r.detector || e.device != device) continue;
+        if (e.key != key) {  // the detector or lattice changed since: rebuild the context
+            std::lock_guard<std::mutex> wait_idle(*e.busy);
+            e.gpu.reset(new GpuEngine(*r.lattice, *r.detector, device));
+            e.key = std::move(key);
+        }
+        return e;
+    }
+    CachedContext e{r.lattice, r.detector, device, std::move(key),
+                    std::unique_ptr<GpuEngine>(new GpuEngine(*r.lattice, *r.detector, device)),
+                    std::unique_ptr<std::mutex>(new std::mutex)};
+    cache.entries.push_back(std::move(e));
+    return cache.entries.back();
+}
+
+}  // namespace detail
+
+// The cached device context of a reference engine (built on first use): hand a mesh field
+// over with its set_mesh / set_cartesian_mesh / set_mesh2d / set_grid_mesh2d.
+inline GpuEngine& gpu_engine_for(const cmpmc::SimulationEngine& engine, int device = 0) {
+    return *detail::cached_context(engine, device).gpu;
+}
+
+// Drop-in for cmpmc::run_events(engine, n_events, generate, options) (parallel.hpp:76-78):
+// the same arguments, the same RunResult; gpu selects the device and the form. Calls on
+// the same engine and device are serialized; different engines run independently.
+template <class Generator>
+cmpmc::RunResult run_events(const cmpmc::SimulationEngine& engine, uint64_t n_events, Generator&& generate,
+                            const cmpmc::RunOptions& options = {}, const GpuRunOptions& gpu = {}) {
+    detail::CachedContext& c = detail::cached_context(engine, gpu.device);
+    std::lock_guard<std::mutex> lock(*c.busy);
+    return c.gpu->run_events(n_events, std::forward<Generator>(generate), options, gpu);
+}
 
 }  // namespace cmpmc_b200

@@ -411,9 +411,14 @@ enum {
                                       at 4096); all Luke phonons tracked; mesh field          */
     CMPMC_WL_SINGLE_L_VOLUME = 4,  /* one L phonon, 7.5 meV, uniform origin, isotropic          */
     CMPMC_WL_TEST_PARALLEL   = 5,  /* reference tests/test_parallel.cpp:110-125 generator        */
-    CMPMC_WL_RECOIL_LIGHT    = 6   /* as RECOIL with deposits 10-100 eV (log-uniform), at most 20
+    CMPMC_WL_RECOIL_LIGHT    = 6,  /* as RECOIL with deposits 10-100 eV (log-uniform), at most 20
                                       prompt phonons (weighted) and 5 % of the Luke phonons
                                       tracked (weight 20): the parity case                   */
+    CMPMC_WL_PUBLISHED_PHONON = 7, /* the reference's published phonon benchmark generator
+                                      (benchmarks/cmpmc_bench.cpp:63-67): one 7.5 meV phonon at
+                                      the origin, mode ST / FT / L by the DOS split, isotropic */
+    CMPMC_WL_PUBLISHED_PAIR  = 8   /* its `charge` mode (cmpmc_bench.cpp:68-71): one e-/h+ pair
+                                      at the origin, electron valley uniform                  */
 };
 /* Runs the workload's generator for events [first_event, first_event + n_events) from
  * Rng::for_stream(seed, ev) and writes, per event, the RNG state after the generator

@@ -93,6 +93,16 @@
 //   tpm tp with the same masks on both faces; seed 77
 //   c3s the same with E = 10 eV * 10^u, max_sampled_phonons 20 (prompt phonons carry the
 //       weight n_true / 20) and luke_sample_fraction 0.05
+//   c0r c0 with Russian roulette (russian_roulette_bounces 64, survival 0.5); seed 42
+//   tps tp with DetectorModel::ChargeStepping::LemanSecondOrder; seed 77
+//   tpt tp in a crystal with every trapping and trap-ionisation mean free path set
+//       (e 2 cm, h 3 cm; ionisation e 4 / 5 cm, h 4.5 / 6 cm); seed 77
+//   pub the reference's published phonon benchmark (benchmarks/cmpmc_bench.cpp:45-67):
+//       demo polynomial surfaces (sensor faces with prob_abs 1, bare side wall),
+//       max_bounces 100, no field; one 7.5 meV phonon at the origin, mode ST / FT / L at
+//       u < 0.53539 / < 0.90217 / else, isotropic; seed 12345 (the benchmark's default)
+//   pubc the same detector at 4 V with luke_sample_fraction 0 and one e-/h+ pair per event at
+//       the origin (the benchmark's `charge` mode); seed 12345
 //
 // Built with -DCMPMC_ORACLE_CRLIBM (as cmpmc_ref_crlibm) the transport uses a correctly
 // rounded libm (ref_crlibm.hpp); the generators and the lattice build keep the
@@ -127,7 +137,10 @@ struct Workload {
 Workload make_workload(const std::string& w) {
     Workload wl;
     wl.name = w;
-    if (w == "c0" || w == "c0m" || w == "c0a" || w == "c0x" || w == "c0b") wl.seed = 42;
+    if (w == "c0" || w == "c0m" || w == "c0a" || w == "c0x" || w == "c0b" || w == "c0r") wl.seed = 42;
+    else if (w == "pub") { wl.seed = 12345; wl.events_per_chunk = 64; }
+    else if (w == "pubc") { wl.seed = 12345; wl.events_per_chunk = 1; }
+    else if (w == "tps" || w == "tpt") wl.seed = 77;
     else if (w == "c1") wl.seed = 7;
     else if (w == "c2") { wl.seed = 11; wl.events_per_chunk = 1; }
     else if (w == "c4") wl.seed = 17;
@@ -172,6 +185,21 @@ geometry::BiLinearMesh2D planar_mesh(const CylinderSolid& s) {
         false);
 }
 
+// tpt: every trapping and trap-ionisation channel on (charge_kernels.hpp:103-126), mean
+// free paths of a few cm so that a fair share of the carriers trap or ionise a trap
+CrystalConfig config_for(const std::string& w) {
+    CrystalConfig c = materials::Germanium();
+    if (w == "tpt") {
+        c.e_trapping_mfp_m = 0.02;
+        c.h_trapping_mfp_m = 0.03;
+        c.e_trap_ion_d0_mfp_m = 0.04;
+        c.e_trap_ion_a_mfp_m = 0.05;
+        c.h_trap_ion_d_mfp_m = 0.045;
+        c.h_trap_ion_a0_mfp_m = 0.06;
+    }
+    return c;
+}
+
 void setup_lattice(const std::string& w, CrystalLattice& lattice) {
     if (w == "c0x") lattice.set_kinematics_mode(CrystalLattice::KinematicsMode::Exact);
     if (w == "c0b") lattice.set_kinematics_mode(CrystalLattice::KinematicsMode::Bilinear);
@@ -184,13 +212,26 @@ void setup_detector(const std::string& w, DetectorModel& det) {
     } else if (w == "c2") {
         det.e_field = UniformElectricField::from_bias(4.0, 2.54 * units::cm);
         det.luke_sample_fraction = 0.0;
-    } else if (w == "tp" || w == "tpl" || w == "tpm" || w == "tpd" || w == "tpe" || w == "tp2") {
+    } else if (w == "pub" || w == "pubc") {
+        // the published benchmark's detector (benchmarks/cmpmc_bench.cpp:45-57)
+        det.allow_unvalidated = true;
+        SurfaceProperty sensor = SurfaceProperty::demo_polynomial_sensor_surface();
+        sensor.prob_abs = 1.0;
+        const SurfaceProperty wall = SurfaceProperty::demo_polynomial_bare_surface();
+        det.surfaces = {sensor, sensor, wall};
+        det.max_bounces = 100;
+        det.e_field = UniformElectricField::from_bias(w == "pub" ? 0.0 : 4.0, 2.54 * units::cm);
+        det.luke_sample_fraction = (w == "pubc") ? 0.0 : 1.0;
+    } else if (w == "tp" || w == "tpl" || w == "tpm" || w == "tpd" || w == "tpe" || w == "tp2" || w == "tps" ||
+               w == "tpt") {
         det.e_field = UniformElectricField::from_bias(2.0, 2.54 * units::cm);
+        if (w == "tps") det.charge_stepping = DetectorModel::ChargeStepping::LemanSecondOrder;
         if (w == "tp2") det.mesh_field_2d = axisym_mesh(det.solid);
         det.luke_sample_fraction = (w == "tpl") ? 1.0 : 0.02;
         if (w == "tpd") det.charge_release = DetectorModel::ChargeRelease::BulkDebye;
         if (w == "tpe") det.charge_release = DetectorModel::ChargeRelease::ElectrodeFilm;
     }
+    if (w == "c0r") det.russian_roulette_bounces = 64;  // survival 0.5 (the default)
     if (w == "c0a")
         for (int f = 0; f < 2; ++f) det.surfaces[f].amm_interface = amm_ge_al();
     if (w == "c0m" || w == "tpm")
@@ -225,9 +266,18 @@ struct Generator {
     }
 
     void generate(EventInput& in) const {
-        if (w == "c0" || w == "c0m" || w == "c0a" || w == "c0x" || w == "c0b") {
+        if (w == "c0" || w == "c0m" || w == "c0a" || w == "c0x" || w == "c0b" || w == "c0r") {
             in.phonons.push_back(engine->make_track({0, 0, 0}, in.rng.isotropic_dir(), PhononMode::L, 7.5e-3));
             in.injected_eV += 7.5e-3;
+        } else if (w == "pub") {  // benchmarks/cmpmc_bench.cpp:63-67
+            const double u = in.rng.uniform();
+            const PhononMode m = u < 0.53539 ? PhononMode::ST : u < 0.90217 ? PhononMode::FT : PhononMode::L;
+            in.phonons.push_back(engine->make_track({0, 0, 0}, in.rng.isotropic_dir(), m, 7.5e-3));
+            in.injected_eV += 7.5e-3;
+        } else if (w == "pubc") {  // benchmarks/cmpmc_bench.cpp:68-71
+            const auto v = static_cast<uint16_t>(in.rng.uniform() * n_valleys) % n_valleys;
+            in.charges.push_back(charges->make_charge(ExcitationType::Electron, {0, 0, 0}, in.rng.isotropic_dir(), 1e-6, v));
+            in.charges.push_back(charges->make_charge(ExcitationType::Hole, {0, 0, 0}, in.rng.isotropic_dir(), 1e-6, 0));
         } else if (w == "c1") {
             for (int j = 0; j < 100; ++j) {
                 const double E = 1e-3 * std::exp(std::log(30.0) * in.rng.uniform());
@@ -289,7 +339,7 @@ FILE* open_or_die(const std::string& path) {
 
 int cmd_dump(const std::string& w, uint64_t first, uint64_t n, unsigned threads, const std::string& prefix) {
     const Workload wl = make_workload(w);
-    CrystalLattice lattice(materials::Germanium());
+    CrystalLattice lattice(config_for(w));
     setup_lattice(w, lattice);
     DetectorModel det;
     setup_detector(w, det);
@@ -353,7 +403,7 @@ int cmd_dump(const std::string& w, uint64_t first, uint64_t n, unsigned threads,
 int cmd_time(const std::string& w, uint64_t first, uint64_t n, unsigned threads) {
     const Workload wl = make_workload(w);
     const auto t0 = std::chrono::steady_clock::now();
-    CrystalLattice lattice(materials::Germanium());
+    CrystalLattice lattice(config_for(w));
     setup_lattice(w, lattice);
     DetectorModel det;
     setup_detector(w, det);

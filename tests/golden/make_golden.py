@@ -65,6 +65,11 @@ PLAN = {
     "c0x": (8, 1000),
     "c0b": (8, 2000),
     "tp2": (8, 1000),
+    "c0r": (16, 2000),
+    "tps": (8, 203),
+    "tpt": (8, 203),
+    "pub": (16, 2000),
+    "pubc": (8, 203),
 }
 
 

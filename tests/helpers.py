@@ -31,6 +31,15 @@ def detector_for(workload: str):
             det.mesh_field_2d = axisym_mesh(det)
         det.luke_sample_fraction = 1.0 if workload == "tpl" else 0.02
         det.charge_release = {"tpd": 1, "tpe": 2}.get(workload, 0)
+    elif workload in ("pub", "pubc"):
+        det = cm.DetectorModel.published_benchmark(0.0 if workload == "pub" else 4.0,
+                                                   1.0 if workload == "pub" else 0.0)
+    if workload in ("tps", "tpt"):
+        det.e_field = cm.UniformElectricField.from_bias(2.0, 2.54 * cm.units.cm)
+        det.luke_sample_fraction = 0.02
+        det.charge_stepping = 1 if workload == "tps" else 0
+    if workload == "c0r":
+        det.russian_roulette_bounces = 64
     if workload == "c0a":
         amm = cm.IsotropicAMMInterface(cm.IsotropicMedium(5323.0, 5324.2077, 3258.7879),
                                        cm.IsotropicMedium(2700.0, 6420.0, 3040.0))
@@ -45,7 +54,12 @@ def detector_for(workload: str):
 def lattice_for(workload: str, default_lattice):
     """The lattice of a fixture workload: the shared Ge lattice, or a Ge lattice in the
     Exact (c0x) or Bilinear (c0b) kinematics mode."""
+    import dataclasses
     import cmpmc_b200 as cm
+    if workload == "tpt":  # every trapping and trap-ionisation channel on (oracle/ref_driver.cpp)
+        return cm.CrystalLattice(dataclasses.replace(
+            cm.materials.Germanium(), e_trapping_mfp_m=0.02, h_trapping_mfp_m=0.03, e_trap_ion_d0_mfp_m=0.04,
+            e_trap_ion_a_mfp_m=0.05, h_trap_ion_d_mfp_m=0.045, h_trap_ion_a0_mfp_m=0.06))
     if workload not in ("c0x", "c0b"):
         return default_lattice
     lat = cm.CrystalLattice(cm.materials.Germanium())
@@ -83,7 +97,9 @@ def recoil_mesh():
     return _MESH[0]
 
 
-WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13, "c0m": 42, "tpm": 77, "c0a": 42, "tpd": 77, "tpe": 77, "c0x": 42, "c0b": 42, "tp2": 77}
+WORKLOAD_SEED = {"c0": 42, "c1": 7, "c2": 11, "c4": 17, "tp": 77, "tpl": 77, "c3s": 13, "c0m": 42, "tpm": 77, "c0a": 42,
+                 "tpd": 77, "tpe": 77, "c0x": 42, "c0b": 42, "tp2": 77, "c0r": 42, "tps": 77, "tpt": 77,
+                 "pub": 12345, "pubc": 12345}
 
 
 def workload_of(name: str):
@@ -94,7 +110,10 @@ def workload_of(name: str):
             "c0m": cm.workloads.single_l_origin, "tpm": cm.workloads.test_parallel,
             "c0a": cm.workloads.single_l_origin, "tpd": cm.workloads.test_parallel,
             "tpe": cm.workloads.test_parallel, "c0x": cm.workloads.single_l_origin,
-            "c0b": cm.workloads.single_l_origin, "tp2": cm.workloads.test_parallel}[name]
+            "c0b": cm.workloads.single_l_origin, "tp2": cm.workloads.test_parallel,
+            "c0r": cm.workloads.single_l_origin, "tps": cm.workloads.test_parallel,
+            "tpt": cm.workloads.test_parallel, "pub": cm.workloads.published_phonon,
+            "pubc": cm.workloads.published_pair}[name]
 
 
 def has_gpu() -> bool:

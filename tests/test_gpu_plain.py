@@ -41,7 +41,11 @@ def _device_summary(ge_lattice, wl, n):
     return _RESULTS[(wl, n)]
 
 
-@pytest.mark.parametrize("wl", ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b", "tp2"])
+ALL_WL = ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b", "tp2",
+          "c0r", "tps", "tpt", "pub", "pubc"]
+
+
+@pytest.mark.parametrize("wl", ALL_WL)
 def test_event_parity_correctly_rounded_reference(ge_lattice, wl):
     ref = golden(f"{wl}_cr_summary.npz")["summary"]
     got = _device_summary(ge_lattice, wl, len(ref))
@@ -53,7 +57,7 @@ def test_event_parity_correctly_rounded_reference(ge_lattice, wl):
         assert np.all(np.abs(a - b) <= 1e-12 * np.maximum(np.abs(a), 1e-300) + 1e-300), name
 
 
-@pytest.mark.parametrize("wl", ["c0", "c4", "c2", "tp", "tpl", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b", "tp2"])
+@pytest.mark.parametrize("wl", ALL_WL)
 def test_event_parity_glibc_reference(ge_lattice, wl):
     ref = golden(f"{wl}_summary.npz")["summary"]
     cr = golden(f"{wl}_cr_summary.npz")
@@ -64,9 +68,11 @@ def test_event_parity_glibc_reference(ge_lattice, wl):
     assert np.array_equal(cmp["agree_mask"], cr["floor_mask"])
     if wl in ("c0", "c4"):
         assert cmp["frac"] >= 0.985
+    if wl == "pub":  # the published benchmark workload: no libm-sensitive event in 2,000
+        assert cmp["frac"] == 1.0
 
 
-@pytest.mark.parametrize("wl", ["c0", "tp", "tpl", "c2", "c1", "c3s", "c0m", "tpm", "c0a", "tpd", "tpe", "c0x", "c0b", "tp2"])
+@pytest.mark.parametrize("wl", [w for w in ALL_WL if w != "c4"])
 def test_full_hit_records_match(ge_lattice, wl):
     """Hit-by-hit comparison from the reference's own initial stacks and Rng states."""
     import cmpmc_b200 as cm
@@ -88,6 +94,20 @@ def test_full_hit_records_match(ge_lattice, wl):
             np.testing.assert_allclose(res.event_stats[name], ev[name], rtol=1e-12, atol=1e-300)
         else:
             assert np.array_equal(res.event_stats[name], ev[name]), name
+
+
+def test_rare_branches_are_exercised(ge_lattice):
+    """The parity workloads of the opt-in branches really take them: roulette kills (c0r),
+    trapping and trap ionisation (tpt), and the demo polynomial surfaces' specular and
+    down-converting reflections (pub)."""
+    got = {}
+    for wl in ("c0r", "tpt", "pub"):
+        ref = golden(f"{wl}_cr_summary.npz")["summary"]
+        _, res = _run(ge_lattice, wl, len(ref))
+        got[wl] = res.stats
+    assert got["c0r"].killed_tracks > 0
+    assert got["tpt"].charges_trapped > 0 and got["tpt"].trap_ionizations > 0
+    assert got["pub"].surface_downconversions > 0
 
 
 def test_run_totals_and_closure(ge_lattice):

@@ -60,12 +60,12 @@ def test_lattice_tables_bit_identical_to_reference(ge_lattice):
     assert np.array_equal(t["oct"][:, idx[:, 0], idx[:, 1], :], g["sample"])
 
 
-@pytest.mark.parametrize("wl", ["c0", "c1", "c2", "tp", "tpl", "c3s"])
+@pytest.mark.parametrize("wl", ["c0", "c1", "c2", "tp", "tpl", "c3s", "tpt", "pub", "pubc"])
 def test_native_generators_match_reference(ge_lattice, wl):
     import cmpmc_b200 as cm
     g = golden(f"{wl}_full.npz")
     n = len(g["rng_state"])
-    eng = cm.SimulationEngine(ge_lattice, detector_for(wl))
+    eng = cm.SimulationEngine(lattice_for(wl, ge_lattice), detector_for(wl))
     ev = eng.generate(workload_of(wl), n, WORKLOAD_SEED[wl], threads=2)
     assert np.array_equal(ev.rng_state, g["rng_state"])
     assert np.array_equal(ev.injected_eV, g["injected"])
