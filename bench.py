@@ -5,15 +5,24 @@ tracks per GPU, energies log-uniform on [1, 30] meV, modes L/ST/FT 0.10/0.36/0.5
 uniform in the Ge cylinder (R 3.81 cm, half height 1.27 cm), isotropic directions, seed 7;
 default Ge lattice and detector (Al Kaplan films on both faces). One step = one run_events
 pass over the whole batch in the batched FP32 form (FP32 geometry, FP64 energy ledger and
-time of flight; wavefront split: transport phases and film-cascade phases alternate until
-every track is absorbed or lost), hits kept. The launch shape comes from the library's
-autotuner (results do not depend on it).
+time of flight; the warp pool: one persistent launch in which every warp refills its lanes
+from its own ring of pending phonons and the batch's primaries, and runs its film cascades
+32 at a time, until every track is absorbed or lost), hits kept. The launch shape comes
+from the library's autotuner (results do not depend on it).
 
   value  primary phonon tracks / s, inputs resident on the device, device-timed (CUDA
          events on the library's stream), max over ranks
   e2e    the same through the public API with host buffers: pinned host inputs copied in
          and every hit, the hit offsets and the statistics copied back, each step
+         (e2e_with_generator adds the host generator's time per step)
   plain_fp64  the plain FP64 form (bit-exact event streams) on the same workload, one step
+  matched     after the timed region: chi^2 p-values of the per-event hit histograms (time
+         256 bins over 0-2 ms, radius 64, edep 64) of one timed batched call against the
+         plain FP64 run and against the reference's histograms of the same 10,000 events
+         (tests/golden/c1_hist_full.npz), and the energy-ledger closure of both forms
+  published   the reference's published benchmark workload (benchmarks/cmpmc_bench.cpp:
+         demo polynomial surfaces, max_bounces 100, one 7.5 meV phonon per event) on the
+         device in both forms, beside the published CPU figures
 
 Multi-GPU (torchrun): every rank runs its own 10,000 events (events rank*10000 + i), no
 collective on the data path (weak scaling); barrier and max-over-ranks timing through
@@ -46,6 +55,9 @@ EVENTS = 10000
 PER_EVENT = 100
 SEED = 7
 BYTES_PER_STEP = 192  # algorithmic FP32 track state read + written per transport step: 2 x 96 B
+# the reference's published phonon benchmark (benchmarks/README.md:55, 71): 4-core Xeon 2.10 GHz
+PUBLISHED_MS_PER_EVENT_1T = 0.581
+PUBLISHED_EVENTS_PER_S_4T = 6190.0
 
 
 def dist_env():
@@ -61,9 +73,10 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic(split: bool = True):
+def profile_traffic(form: str):
     """DRAM bytes per transport step of the batched kernels from the committed ncu summary."""
-    name = "batched_fp32_split_mixed_energy.json" if split else "batched_fp32_inline_mixed_energy.json"
+    name = {"pool": "batched_fp32_pool_mixed_energy.json", "rounds": "batched_fp32_split_mixed_energy.json",
+            "inline": "batched_fp32_inline_mixed_energy.json"}[form]
     try:
         with open(os.path.join(ROOT, "profiles", name)) as f:
             return float(json.load(f)["dram_bytes_per_step"])
@@ -176,6 +189,58 @@ def cpu_baseline(sample_events: int):
             "steps_per_s": r["total_steps"] / r["wall_seconds"], "wall_seconds": r["wall_seconds"]}
 
 
+def matched_statistics(batched: dict, plain, first_event: int) -> dict:
+    """chi^2 of the batched call's per-event hit histograms against the plain FP64 form's on
+    the same events and against the reference's (10,000-event fixture, rank 0's events), and
+    the ledger closures."""
+    from tests.golden.records import event_histograms, hist_chi2
+    path = os.path.join(ROOT, "tests", "golden", "c1_hist_full.npz")
+    ref = dict(np.load(path)) if os.path.exists(path) else None
+    rng = tuple(ref["edep_range"]) if ref is not None else (
+        float(batched["hits"]["edep"].min()), float(batched["hits"]["edep"].max()) * (1 + 1e-9))
+    hb = event_histograms(batched["offsets"], batched["hits"], rng)
+    out = {"bins": {"time": "256 over 0-2 ms", "radius": "64 over 0-R", "edep": "64 over the reference range"},
+           "events": int(hb["n_events"]), "batched_hits": int(len(batched["hits"])),
+           "ledger_closure_batched": abs(batched["injected"] - batched["deposited"] - batched["escaped"]) /
+                                     batched["injected"]}
+    if plain is not None:
+        hp = event_histograms(plain["offsets"], plain["hits"], rng)
+        out["p_vs_plain_fp64"] = {k: round(hist_chi2(hb, hp, k)[2], 4) for k in ("time", "radius", "edep")}
+        out["plain_hits"] = int(len(plain["hits"]))
+        out["ledger_closure_plain_fp64"] = abs(plain["injected"] - plain["deposited"] - plain["escaped"]) / \
+            plain["injected"]
+    if ref is not None and first_event == 0 and int(ref["n_events"]) == hb["n_events"]:
+        out["p_vs_reference_cpu"] = {k: round(hist_chi2(hb, ref, k)[2], 4) for k in ("time", "radius", "edep")}
+        out["reference_hits"] = int(ref["n_hits"])
+    return out
+
+
+def published_workload(cm, lat, dev: int, n: int, lib) -> dict:
+    """The reference's published phonon benchmark workload (benchmarks/cmpmc_bench.cpp:45-67):
+    n events, device-resident inputs, hits not kept (as the benchmark), both forms; and the
+    reference's own CPU run_events on this host's cores on a sample of the same events."""
+    det = cm.DetectorModel.published_benchmark()
+    eng = cm.SimulationEngine(lat, det)
+    packed = eng.generate(cm.workloads.published_phonon, n, 12345)
+    out = {"workload": "published phonon benchmark (demo surfaces, max_bounces 100, 7.5 meV, seed 12345)",
+           "events": n, "reference_published_ms_per_event_1_thread": PUBLISHED_MS_PER_EVENT_1T,
+           "reference_published_events_per_s_4_threads": PUBLISHED_EVENTS_PER_S_4T}
+    for form in ("plain_fp64", "batched_fp32"):
+        opt = cm.RunOptions(seed=12345, form=form, keep_hits=False, device=dev)
+        eng.run_packed(packed, opt)  # warm-up (buffers, tables)
+        r = eng.run_packed(packed, opt)
+        out[form] = {"events_per_s": n / (r.device_ms * 1e-3), "us_per_event": 1e3 * r.device_ms / n,
+                     "steps": int(r.stats.total_steps), "sensor_hits": int(r.stats.sensor_hits)}
+    exe = os.path.join(ROOT, "oracle", "_ref", "cmpmc_ref")
+    if os.path.exists(exe):
+        m = min(n, 20000)
+        r = json.loads(subprocess.run([exe, "time", "pub", "0", str(m), "0"], check=True, capture_output=True,
+                                      text=True).stdout.strip().splitlines()[-1])
+        out["reference_cpu_this_host"] = {"events_per_s": m / r["wall_seconds"], "threads": r["threads"],
+                                          "sample_events": m}
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -192,6 +257,9 @@ def main() -> None:
     ap.add_argument("--form", default="batched_fp32", choices=["batched_fp32", "batched_fp32_inline"])
     ap.add_argument("--queue-capacity", type=int, default=0, help="phonon queue entries (0: library default)")
     ap.add_argument("--stack-capacity", type=int, default=0, help="tracks per device thread (0: library default)")
+    ap.add_argument("--rounds", action="store_true", help="host-driven film / transport rounds instead of the warp pool")
+    ap.add_argument("--no-matched", action="store_true", help="skip the matched-statistics check")
+    ap.add_argument("--pub-events", type=int, default=100000, help="events of the published workload (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -224,6 +292,9 @@ def main() -> None:
     if args.queue_capacity or args.stack_capacity:
         eng.configure(dev, stack_capacity=args.stack_capacity, queue_capacity=args.queue_capacity)
     form_id = _ffi.FORM_BATCHED_FP32 if args.form == "batched_fp32" else _ffi.FORM_BATCHED_FP32_INLINE
+    if args.rounds:
+        eng.configure_pool(False, device=dev)
+    launch_form = "inline" if args.form != "batched_fp32" else ("rounds" if args.rounds else "pool")
 
     # device-resident inputs (torch owns the memory)
     def to_dev(a):
@@ -259,6 +330,18 @@ def main() -> None:
         return out
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")  # 256 MiB > 126 MB L2
+
+    def fetch(out):
+        """hit offsets, hits and totals of a call whose outputs stayed on the device"""
+        n_h = int(out.n_hits)
+        offs = np.zeros(args.events + 1, dtype=np.uint64)
+        hits = np.zeros(n_h, dtype=_ffi.HIT_DTYPE)
+        lib.cmpmc_gpu_memcpy(offs.ctypes.data, C.c_void_p(out.hit_offsets), offs.nbytes)
+        if n_h:
+            lib.cmpmc_gpu_memcpy(hits.ctypes.data, C.c_void_p(out.hits), hits.nbytes)
+        st = out.stats
+        return {"offsets": offs, "hits": hits, "injected": st.total_injected_eV,
+                "deposited": st.total_deposited_eV, "escaped": st.escaped_or_killed_eV}
 
     def barrier():
         if world > 1:
@@ -310,6 +393,8 @@ def main() -> None:
             hits_total += o.n_hits
         barrier()
         wall = time.perf_counter() - t0
+    # the last timed call's outputs (device memory of the context) for the matched check
+    batched_res = fetch(o) if not args.no_matched else None
     step_ms = max_over_ranks(sum(ms) / args.steps)
     kernel_ms = max_over_ranks(sum(kms) / args.steps)
     value = world * n_prim / (step_ms * 1e-3)
@@ -332,11 +417,13 @@ def main() -> None:
         o = run(hd)
         e2e_ms.append(1e3 * (time.perf_counter() - t1))
     e2e_step = max_over_ranks(sum(e2e_ms) / args.steps)
+    gen_ms = max_over_ranks(1e3 * t_gen)
     h2d = sum(t.numel() for t in hp)
     d2h = int(o.n_hits) * 56 + (args.events + 1) * 8 + 208
 
     # plain FP64 form on the same workload (bit-exact event streams), one step
     plain = None
+    plain_res = None
     if not args.no_plain:
         dp = desc(True)
         dp.form = _ffi.FORM_PLAIN_FP64
@@ -344,11 +431,15 @@ def main() -> None:
         p_ms = max_over_ranks(o.total_ms)
         plain = {"value": world * n_prim / (p_ms * 1e-3), "unit": UNIT, "ms_per_step": p_ms,
                  "steps_per_s": o.stats.total_steps / (o.kernel_ms * 1e-3)}
+        if batched_res is not None:
+            plain_res = fetch(o)
+    matched = matched_statistics(batched_res, plain_res, first) if batched_res is not None else None
+    published = published_workload(cm, lat, dev, args.pub_events, lib) if args.pub_events and rank == 0 else None
 
     peak, peak_kind = measured_peaks()
     steps_per_launch = steps_total / args.steps
     achieved = steps_per_launch * BYTES_PER_STEP / (sum(kms) / args.steps * 1e-3) / 1e9
-    tps = profile_traffic(args.form == "batched_fp32")
+    tps = profile_traffic(launch_form)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -362,11 +453,15 @@ def main() -> None:
         "hits_per_step": hits_total / args.steps,
         "e2e": {"value": world * n_prim / (e2e_step * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
+        "e2e_with_generator": {"value": world * n_prim / ((e2e_step + gen_ms) * 1e-3), "unit": UNIT,
+                               "ms_per_step": e2e_step + gen_ms, "generator_ms": gen_ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "bytes_per_step": BYTES_PER_STEP,
                      "traffic": (tps * steps_per_launch if tps else None)},
         "gpu_launches": launches,
-        "launch": {"graph": use_graph, "autotune": tune},
+        "launch": {"form": {"pool": "warp_pool", "rounds": "host_rounds", "inline": "inline"}[launch_form],
+                   "graph": use_graph, "transport_launches_per_call": launches / args.steps,
+                   "host_syncs_per_call": 1 if launch_form != "rounds" else None, "autotune": tune},
         "clocks": clocks.summary(),
         "wall_s_timed": wall,
         "generator_s": t_gen,
@@ -374,6 +469,10 @@ def main() -> None:
     if plain is not None:
         line["plain_fp64"] = plain
         line["batched_over_plain"] = value / plain["value"]
+    if matched is not None:
+        line["matched"] = matched
+    if published is not None:
+        line["published"] = published
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args.cpu_events)
     if world > 1:

@@ -972,6 +972,12 @@ class SimulationEngine:
         if queue_capacity:
             _check(self._lib.cmpmc_gpu_configure_queue(h, int(queue_capacity)), h)
 
+    def configure_pool(self, enable: bool = True, ring_capacity: int = 0, device: int = 0) -> None:
+        """Launch form of the batched phonon transport: the warp pool (one persistent launch,
+        the default) or the host-driven film / transport rounds (cmpmc_gpu_configure_pool)."""
+        h = self.context(device)
+        _check(self._lib.cmpmc_gpu_configure_pool(h, int(enable), int(ring_capacity)), h)
+
     def configure_graph(self, enable: bool = True, device: int = 0) -> None:
         """Replay repeated batched calls on device-resident inputs as one CUDA graph."""
         h = self.context(device)

@@ -108,6 +108,9 @@ struct cmpmc_gpu_ctx {
     DevBuf film_a, queue_b;                             // wavefront split: film entries, second phonon queue
     uint64_t film_cap = 1ull << 22;                     // film entries per phase (64 B each)
     uint32_t phase_steps = 0;                           // steps a track takes per transport phase (0: any)
+    int pool = 1;                                       // batched phonon form: 1 warp pool, 0 host-driven rounds
+    uint32_t pool_ring_cap = 1024;                      // pending phonons per warp in the pool form
+    DevBuf pool_ring, pool_film;                        // warp pool: per-warp rings and film buffers
     uint64_t queue_cap = 1ull << 24;                    // Luke-phonon queue entries (64 B each)
     // CUDA-graph replay of the batched phonon call (cmpmc_gpu_configure_graph)
     bool graph_enabled = false;
@@ -638,6 +641,98 @@ int run_split_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, u
     return CMPMC_OK;
 }
 
+// The batched FP32 form of phonon-only events as one persistent launch (k_pool_fp32): every
+// warp refills its lanes from its own ring of pending phonons and from the batch's
+// primaries, queues film entries in its own buffer and runs them 32 at a time, and appends
+// re-emissions and daughters to its ring. The host only launches, reads the counters once
+// and merges; a ring, stack or hit-staging overflow reruns the call with more room (every
+// unit owns its substream, so the rerun reproduces the same hits).
+int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, uint64_t n, uint64_t n_ph,
+                     int& launches, Counters& hc, float& kms, uint64_t& n_hits, uint64_t*& ev_offsets,
+                     cmpmc_sim_stats*& ev_stats) {
+    cudaStream_t s = ctx->stream;
+    const int tpb = 128;  // the kernel's per-thread counters are laid out for 128-thread blocks
+    int bps = ctx->bps;
+    if (!bps) {
+        CK(pool_fp32_occupancy(tpb, &bps), "occupancy");
+        bps = std::max(bps, 1);
+    }
+    // no more warps than there are primaries to start them with
+    const uint64_t grid = std::max<uint64_t>(
+        1, std::min<uint64_t>(static_cast<uint64_t>(ctx->num_sms) * bps, (n_ph + tpb - 1) / tpb));
+    const uint64_t warps = grid * tpb / 32;
+    CK(ctx->ev_stats2.ensure(std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats)), "alloc event stats");
+    CK(ctx->ev_nhits.ensure(std::max<uint64_t>(n, 1) * 8), "alloc event hit counts");
+    CK(ctx->ev_offsets.ensure((n + 1) * 8), "alloc event offsets");
+    CK(ctx->cursor.ensure(std::max<uint64_t>(n, 1) * 8), "alloc event cursors");
+    CK(ctx->counters.ensure(sizeof(Counters)), "alloc counters");
+    CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
+    CK(ctx->partials.ensure(kReducePartials * sizeof(cmpmc_sim_stats)), "alloc partial totals");
+    CK(ctx->h_counters.ensure(sizeof(Counters)), "alloc host counters");
+    CK(ctx->pool_film.ensure(warps * pool_film_bytes_per_warp()), "alloc film buffers");
+    if (n_ph) {
+        CK(ctx->unit_event.ensure(n_ph * 4), "alloc unit map");
+        CK(launch_unit_event(a.ph_off, n, ctx->unit_event.as<uint32_t>(), s), "unit map");
+        ++launches;
+    }
+    a.ev_sink = 1;
+    a.ev_stats = ctx->ev_stats2.as<cmpmc_sim_stats>();
+    a.ev_nhits = ctx->ev_nhits.as<uint64_t>();
+    Counters* dc = ctx->counters.as<Counters>();
+    a.hit_count = &dc->hit_count;
+    a.next_work = &dc->next_work;
+    a.err = &dc->err;
+    a.film = nullptr;
+    a.phase_steps = 0;
+    a.n_events = n_ph;
+    uint64_t hit_cap = ctx->hit_cap;
+    if (!hit_cap) hit_cap = std::max<uint64_t>(1u << 20, n_ph * 32);
+    for (int attempt = 0;; ++attempt) {
+        if (!d->keep_hits) hit_cap = 1;
+        CK(ctx->pool_ring.ensure(warps * ctx->pool_ring_cap * pool_ring_entry_bytes()), "alloc warp rings");
+        CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
+        CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
+        a.hit_stage = ctx->hit_stage.as<cmpmc_sensor_hit>();
+        a.hit_key = ctx->hit_key.as<uint64_t>();
+        a.hit_cap = hit_cap;
+        CK(cudaMemsetAsync(ctx->ev_stats2.p, 0, std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats), s), "memset");
+        CK(cudaMemsetAsync(ctx->ev_nhits.p, 0, std::max<uint64_t>(n, 1) * 8, s), "memset");
+        CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s), "memset counters");
+        CK(cudaEventRecord(ctx->e_k0, s), "event");
+        if (n_ph) {
+            CK(launch_pool_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->pool_ring.p, ctx->pool_ring_cap, ctx->pool_film.p,
+                                ctx->unit_event.as<uint32_t>(), static_cast<int>(grid), tpb, s),
+               "pool launch");
+            ++launches;
+        }
+        CK(cudaEventRecord(ctx->e_k1, s), "event");
+        CK(cudaMemcpyAsync(ctx->h_counters.p, ctx->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s),
+           "copy counters");
+        CK(cudaStreamSynchronize(s), "transport kernel");
+        hc = *ctx->h_counters.as<Counters>();
+        CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
+        const bool ring_over = (hc.err & kErrQueue) != 0;
+        const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
+        if (!ring_over && !hits_over) break;
+        if (attempt >= 6) return fail(ctx, CMPMC_ERR_CAPACITY, "warp ring or hit buffer overflow persists");
+        if (ring_over) ctx->pool_ring_cap = std::min<uint32_t>(ctx->pool_ring_cap * 4, 1u << 20);
+        if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
+        hc.err = 0;
+    }
+    if (d->keep_hits) ctx->hit_cap = std::max<uint64_t>(ctx->hit_cap, hit_cap);
+    if (hc.err) return fail(ctx, CMPMC_ERR_DEVICE, "transport kernel reported error word " + std::to_string(hc.err));
+    n_hits = d->keep_hits ? hc.hit_count : 0;
+    CK(ctx->hits_out.ensure(std::max<uint64_t>(n_hits, 1) * sizeof(cmpmc_sensor_hit)), "alloc hits");
+    CK(cudaMemsetAsync(ctx->cursor.p, 0, std::max<uint64_t>(n, 1) * 8, s), "memset cursors");
+    ev_offsets = ctx->ev_offsets.as<uint64_t>();
+    ev_stats = ctx->ev_stats2.as<cmpmc_sim_stats>();
+    a.n_events = n;
+    CK(launch_sink_finish(a, n, ev_offsets, ctx->cursor.as<unsigned long long>(), ctx->hits_out.as<cmpmc_sensor_hit>(),
+                          n_hits, ctx->total.as<cmpmc_sim_stats>(), ctx->partials.as<cmpmc_sim_stats>(), s, &launches),
+       "merge kernels");
+    return CMPMC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -920,6 +1015,15 @@ int cmpmc_gpu_configure_phases(cmpmc_gpu_ctx* ctx, uint32_t phase_steps) {
     return CMPMC_OK;
 }
 
+int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int enable, uint32_t ring_capacity) {
+    if (!ctx || enable < 0 || enable > 1) return CMPMC_ERR_INVALID;
+    if (ring_capacity != 0 && (ring_capacity < 64 || (ring_capacity & (ring_capacity - 1)) != 0))
+        return fail(ctx, CMPMC_ERR_INVALID, "ring capacity: a power of two, at least 64");
+    ctx->pool = enable;
+    if (ring_capacity) ctx->pool_ring_cap = ring_capacity;
+    return CMPMC_OK;
+}
+
 int cmpmc_gpu_configure_graph(cmpmc_gpu_ctx* ctx, int enable) {
     if (!ctx) return CMPMC_ERR_INVALID;
     ctx->graph_enabled = enable != 0;
@@ -1137,8 +1241,12 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
         // carriers and their Luke phonons: alternating charge / queue phases, event sinks
         const int st = run_charges_batched(ctx, d, a, n, n_ph, n_ch, launches, hc, kms, n_hits, ev_offsets, ev_stats);
         if (st != CMPMC_OK) return st;
+    } else if (split && ctx->pool) {
+        // phonons, warp pool: one persistent launch, event sinks
+        const int st = run_pool_batched(ctx, d, a, n, n_ph, launches, hc, kms, n_hits, ev_offsets, ev_stats);
+        if (st != CMPMC_OK) return st;
     } else if (split) {
-        // phonons, wavefront split: transport phases and film phases, event sinks
+        // phonons, wavefront split: host-driven transport and film rounds, event sinks
         const int st = run_split_batched(ctx, d, a, n, n_ph, launches, hc, kms, n_hits, ev_offsets, ev_stats);
         if (st != CMPMC_OK) return st;
     } else {

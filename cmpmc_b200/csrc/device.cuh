@@ -297,6 +297,15 @@ cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detect
 cudaError_t launch_film_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                              const FilmRec* film, uint64_t n_film, int grid, int block, cudaStream_t s);
 cudaError_t film_fp32_occupancy(int block, int* blocks_per_sm);
+// warp pool form of the batched phonon transport (one persistent launch): `ring` holds
+// ring_cap pending-phonon entries (pool_ring_entry_bytes) per warp, `film`
+// pool_film_bytes_per_warp bytes per warp; grid * block / 32 warps
+cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
+                             uint32_t ring_cap, void* film, const uint32_t* unit_event, int grid, int block,
+                             cudaStream_t s);
+cudaError_t pool_fp32_occupancy(int block, int* blocks_per_sm);
+size_t pool_ring_entry_bytes();
+size_t pool_film_bytes_per_warp();
 cudaError_t launch_carrier_event(const uint64_t* ch_off, uint64_t n_events, uint32_t* carrier_event,
                                  cudaStream_t s);
 // merge of the event-sink runs: injected energies, hit offsets, hits into event order

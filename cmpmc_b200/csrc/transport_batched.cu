@@ -799,6 +799,543 @@ __global__ void __launch_bounds__(128, 8) k_film_fp32(const __grid_constant__ FL
     if (err) atomicOr(a.err, err);
 }
 
+// ---- warp pool form -------------------------------------------------------------------
+// One persistent launch transports the whole batch. Each warp owns a private ring of
+// pending phonons (film re-emissions and daughters, with their group velocity, so a refill
+// needs no table lookup) and a private buffer of film entries. Every iteration:
+//   1. refill: the lanes without a track (one ballot) take the ring's oldest entries, then
+//      the next primaries of the batch (one atomicAdd per warp for all of them);
+//   2. step: every live lane takes one transport step;
+//   3. regroup: the lanes whose step ended at an active film append a film record, the lanes
+//      that made a daughter (decay, surface down-conversion) append it to the ring, each
+//      class through one ballot and prefix count;
+//   4. when 32 film entries are waiting, the whole warp runs one cascade per lane (the
+//      film step, converged) and appends the re-emitted phonons to the ring.
+// A warp ends when the batch's primaries are handed out and its ring, film buffer and lanes
+// are empty. Work never moves between warps, so nothing waits on another warp (no spin, no
+// grid barrier); the batch ends with one tail instead of one per film / transport round.
+// Every unit (primary, ring phonon) has its own substream, so the hits of an event are a
+// fixed set whatever the launch shape; units add to per-event sinks.
+constexpr int kPoolFilmCap = 64;  // film records per warp (a batch of 32 runs when 32 wait)
+
+struct alignas(16) PoolPh {  // 80 B
+    float px, py, pz, kx, ky, kz, vx, vy, vz, vmag, w;
+    uint32_t bounces_mode;  // bounces << 2 | mode
+    double E, t;
+    uint64_t key;
+    uint32_t ev, pad;
+};
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ PoolPh pool_entry(const FTrack& t, uint64_t key, uint32_t ev) {
+    PoolPh q;
+    q.px = t.pos.x; q.py = t.pos.y; q.pz = t.pos.z;
+    q.kx = t.k.x; q.ky = t.k.y; q.kz = t.k.z;
+    q.vx = t.vg.x; q.vy = t.vg.y; q.vz = t.vg.z;
+    q.vmag = t.vmag;
+    q.w = t.w;
+    q.bounces_mode = (t.bounces << 2) | static_cast<uint32_t>(t.mode);
+    q.E = t.E;
+    q.t = t.t;
+    q.key = key;
+    q.ev = ev;
+    q.pad = 0;
+    return q;
+}
+
+__device__ __forceinline__ uint64_t draw_key(R128& g) {
+    const uint64_t hi = g.next();
+    return (hi << 32) | g.next();
+}
+
+// anharmonic decay of an L phonon (engine.hpp:938-988), FP32 angles: the parent continues
+// in *tp, the daughter is written to *dp (it runs later on a substream of its own)
+template <int kKin>
+__device__ __noinline__ void pool_decay(const FLat* Lp, FTrack* tp, FTrack* dp, const UStats* st, R128* gp) {
+    const FLat& L = *Lp;
+    FTrack& trk = *tp;
+    R128& g = *gp;
+    const F3 d1 = trk.k;
+    const F3 perp = forth(d1);
+    float sp, cp;
+    __sincosf(kTwoPiF * g.u(), &sp, &cp);
+    float x, th1, th2;
+    int m1, m2;
+    const float m = L.m_ratio, mm = m * m;
+    if (g.u() < L.fTT) {
+        ++st->tt();
+        x = fcdf(L.cdf_tt, g);
+        const float y = 1.0f - x;
+        th1 = facos_clamped((1.0f - mm * y * y + mm * x * x) / (2.0f * m * x));
+        th2 = facos_clamped((1.0f - mm * x * x + mm * y * y) / (2.0f * m * y));
+        m1 = ftrans(L, g);
+        m2 = ftrans(L, g);
+    } else {
+        ++st->lt();
+        x = fcdf(L.cdf_lt, g);
+        th1 = facos_clamped((1.0f + x * x * (1.0f - mm) + 2.0f * x * mm - mm) / (2.0f * x));
+        th2 = facos_clamped((1.0f - x * x + mm * (1.0f - x) * (1.0f - x)) / (2.0f * m * (1.0f - x)));
+        m1 = 0;
+        m2 = ftrans(L, g);
+    }
+    float s1, c1, s2, c2;
+    __sincosf(th1, &s1, &c1);
+    __sincosf(-th2, &s2, &c2);
+    const F3 k1 = funit(frotate(frotate(d1, perp, c1, s1), d1, cp, sp));
+    const F3 k2 = funit(frotate(frotate(d1, perp, c2, s2), d1, cp, sp));
+    const double xd = static_cast<double>(x);
+    FTrack& d = *dp;
+    d.pos = trk.pos;
+    d.k = k2;
+    const FKin kin2 = fmapk<kKin>(L, m2, k2);
+    d.vg = kin2.dir;
+    d.vmag = kin2.mag;
+    d.E = (1.0 - xd) * trk.E;
+    d.t = trk.t;
+    d.w = trk.w;
+    d.bounces = 0;
+    d.mode = m2;
+    trk.E = xd * trk.E;
+    trk.mode = m1;
+    trk.k = k1;
+    const FKin kin = fmapk<kKin>(L, m1, k1);
+    trk.vg = kin.dir;
+    trk.vmag = kin.mag;
+}
+
+enum { kStepOn = 0, kStepEnd = 1, kStepFilm = 2 };
+
+// One transport step of a live track (the physics of batched_loop's step): returns whether
+// the track goes on, ended (counters and ledger updated), or entered an active film (*fr
+// filled, the film kernel's input). A daughter made in the step is written to *dq
+// (*has_d set) with a substream key drawn from the track's stream.
+// A step's single output record (a film entry or a daughter), staged in shared memory so
+// that it holds no registers across the step; the warp copies it to its buffer afterwards.
+union PoolOut {
+    FilmRec film;
+    PoolPh ph;
+};
+
+template <int kKin>
+__device__ __forceinline__ int pool_step(const FLat& L, const Detector& D, FTrack& trk, R128& g, const UStats& st,
+                                         uint32_t ev, PoolOut& out, bool& has_d) {
+    has_d = false;
+    if (trk.E < D.min_phonon_eV || trk.bounces >= D.max_bounces) {
+        ++st.killed();
+        st.esc() += trk.E * trk.w;
+        return kStepEnd;
+    }
+    if (D.rr_bounces != 0 && trk.bounces > D.rr_bounces && (trk.bounces - D.rr_bounces) % 32 == 0) {
+        if (g.u() < static_cast<float>(D.rr_survival)) {
+            trk.w /= static_cast<float>(D.rr_survival);
+        } else {
+            ++st.killed();
+            return kStepEnd;
+        }
+    }
+    ++st.steps();
+    const float R = static_cast<float>(D.radius), H = static_cast<float>(D.half_z);
+    const float nu = static_cast<float>(trk.E) * L.inv_h_thz;
+    const float nu2 = nu * nu;
+    const float r_iso = L.b4 * (nu2 * nu2);
+    const float r_poly = trk.vmag * L.poly_inv;
+    const float r_down = (trk.mode == 0) ? L.a5 * (nu2 * nu2 * nu) : 0.0f;
+    const float r_tot = r_iso + r_poly + r_down;
+    const float d_phys = (r_tot > 1e-12f) ? (-logf(g.u()) * trk.vmag / r_tot) : __int_as_float(0x7f800000);
+    FBHit bh = fexit_d(R, H, trk.pos, trk.vg);
+    const bool bulk = d_phys < bh.d;
+    const float d = bulk ? d_phys : bh.d;
+    trk.pos = trk.pos + trk.vg * d;
+    trk.t += static_cast<double>(d / trk.vmag);
+    int sample = 2;  // 0: isotropic (bulk scatter), 1: Lambertian about bh.n, 2: nothing more
+    if (bulk) {
+        const float u_proc = g.u() * r_tot;
+        if (r_down > 0.0f && u_proc < r_down) {
+            FTrack t_c = trk, d_c;
+            R128 g_c = g;
+            pool_decay<kKin>(&L, &t_c, &d_c, &st, &g_c);
+            trk = t_c;
+            g = g_c;
+            out.ph = pool_entry(d_c, draw_key(g), ev);
+            has_d = true;
+        } else {
+            if (u_proc < r_down + r_iso) ++st.iso();
+            else ++st.poly();
+            trk.mode = fdos(L, g.u());
+            sample = 0;
+        }
+    } else {
+        bh.n = fnormal(bh.surf, trk.pos);
+        trk.bounces++;
+        const Surface& s = D.surf[bh.surf];
+        bool enter = false;
+        int ch_id = -1;
+        bool active_pad = true;
+        if (s.n_pads > 0) {  // electrode mask (engine.hpp:483-488)
+            R128 g_c = g;
+            ch_id = mask_call(s.pads, s.n_pads, trk.pos.x, trk.pos.y, &g_c);
+            g = g_c;
+            active_pad = ch_id >= 0;
+        }
+        if (active_pad && s.has_film && g.u() < static_cast<float>(s.prob_abs)) {
+            const float p_enter = s.has_amm ? amm_call(&s, trk.mode == 0, fdot(trk.k, bh.n))
+                                            : static_cast<float>(s.film.film_absorption);
+            enter = g.u() < p_enter;
+        }
+        if (enter) {
+            FilmRec fr;
+            fr.px = trk.pos.x; fr.py = trk.pos.y; fr.pz = trk.pos.z;
+            fr.w = trk.w;
+            fr.E = trk.E;
+            fr.t = trk.t;
+            fr.key = draw_key(g);
+            fr.ev = ev;
+            fr.ch_id = ch_id;
+            fr.bounces = trk.bounces;
+            fr.surf = static_cast<uint8_t>(bh.surf);
+            fr.mode = static_cast<uint8_t>(trk.mode);
+            fr.pad0 = fr.pad1 = 0;
+            out.film = fr;
+            return kStepFilm;
+        }
+        if (g.u() > static_cast<float>(s.prob_refl)) {
+            ++st.killed();
+            st.esc() += trk.E * trk.w;
+            return kStepEnd;
+        }
+        ++st.refl();
+        trk.pos = trk.pos + bh.n * kNudge;
+        float p_anh, p_anh_spec;
+        if (L.split_const[bh.surf]) {
+            p_anh = L.p_anh[bh.surf];
+            p_anh_spec = L.p_anh_spec[bh.surf];
+        } else {
+            const Split sp = reflection_split(s, trk.E);
+            p_anh = static_cast<float>(sp.p_anh);
+            p_anh_spec = static_cast<float>(sp.p_anh + sp.p_spec);
+        }
+        const float u_refl = g.u();
+        if (u_refl < p_anh) {
+            ++st.down();
+            const bool tt = g.u() < L.fTT;
+            const float x = tt ? fcdf(L.cdf_tt, g) : fcdf(L.cdf_lt, g);
+            const int m1 = tt ? ftrans(L, g) : 0;
+            const int m2 = ftrans(L, g);
+            FTrack dtr;
+            FKin k2kin;
+            dtr.k = finward<kKin>(L, m2, bh.n, g, k2kin);
+            dtr.pos = trk.pos;
+            dtr.vg = k2kin.dir;
+            dtr.vmag = k2kin.mag;
+            dtr.E = (1.0 - static_cast<double>(x)) * trk.E;
+            dtr.t = trk.t;
+            dtr.w = trk.w;
+            dtr.bounces = 0;
+            dtr.mode = m2;
+            out.ph = pool_entry(dtr, draw_key(g), ev);
+            has_d = true;
+            trk.E = static_cast<double>(x) * trk.E;
+            trk.mode = m1;
+            sample = 1;
+        } else if (u_refl < p_anh_spec) {
+            F3 kr = trk.k - bh.n * (2.0f * fdot(trk.k, bh.n));
+            FKin kin = fmapk<kKin>(L, trk.mode, kr);
+            if (fdot(kin.dir, bh.n) <= 1e-6f) kr = finward<kKin>(L, trk.mode, bh.n, g, kin);
+            trk.k = kr;
+            trk.vg = kin.dir;
+            trk.vmag = kin.mag;
+        } else {
+            sample = 1;
+        }
+    }
+    // shared new-direction path: isotropic (bulk scatter) or Lambertian about the inward
+    // normal (diffuse reflection), then the table lookup
+    if (sample != 2) {
+        const bool lam = (sample == 1);
+        const F3 e3 = lam ? bh.n : f3(0.0f, 0.0f, 1.0f);
+        const F3 e1 = lam ? forth(bh.n) : f3(1.0f, 0.0f, 0.0f);
+        const F3 e2 = lam ? fcross(bh.n, e1) : f3(0.0f, 1.0f, 0.0f);
+        FKin kin;
+        F3 kd;
+        for (int trial = 0;; ++trial) {
+            const float u1 = g.u();
+            const float u2 = g.u();
+            const float ct = lam ? sqrtf(u1) : 2.0f * u1 - 1.0f;
+            const float st_ = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+            float sphi, cphi;
+            __sincosf(kTwoPiF * u2, &sphi, &cphi);
+            kd = e1 * (st_ * cphi) + e2 * (st_ * sphi) + e3 * ct;
+            if (lam) kd = funit(kd);
+            kin = fmapk<kKin>(L, trk.mode, kd);
+            if (!lam || fdot(kin.dir, bh.n) > 1e-6f) break;
+            if (trial == 15) {
+                kd = bh.n;
+                kin = fmapk<kKin>(L, trk.mode, kd);
+                break;
+            }
+        }
+        trk.k = kd;
+        trk.vg = kin.dir;
+        trk.vmag = kin.mag;
+    }
+    return kStepOn;
+}
+
+struct PoolArgs {
+    PoolPh* ring;           // [warps][ring_cap]
+    FilmRec* film;          // [warps][kPoolFilmCap]
+    uint32_t ring_cap;      // a power of two
+    const uint32_t* unit_event;
+};
+
+// The film step of a warp, converged: lane l < n_rec runs the cascade of film record
+// fb[(f_head + l) % kPoolFilmCap] (from the record's own substream), records the hit and
+// the ledger in the record's event (hit slots reserved once per warp) and appends the
+// re-emitted phonons, inward Lambertian with DOS modes and their own substreams (the first
+// keeps the bounce count), to the warp's ring. Returns the new ring tail.
+template <bool kSur, int kKin>
+__device__ __noinline__ uint32_t pool_film_step(const FLat* Lp, const Detector* Dp, const RunArgs* ap,
+                                                const FilmRec* fb, uint32_t f_head, int n_rec, PoolPh* ring,
+                                                uint32_t ring_mask, uint32_t r_head, uint32_t r_tail,
+                                                double* refl_buf, double* kwork, unsigned* err) {
+    const FLat& L = *Lp;
+    const Detector& D = *Dp;
+    const RunArgs& a = *ap;
+    const int lane = threadIdx.x & 31;
+    const bool has = lane < n_rec;
+    FilmRec r;
+    double edep = 0.0;
+    int n_refl = 0;
+    R128 g;
+    if (has) {
+        r = fb[(f_head + lane) & (kPoolFilmCap - 1)];
+        const Surface& s = D.surf[r.surf];
+        R128 g_c;
+        g_c.seed(r.key);
+        if constexpr (kSur) {
+            edep = s.lut_abs ? surrogate_call(&s, r.E, refl_buf, &n_refl, kwork, &g_c)
+                             : kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
+        } else {
+            edep = kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
+        }
+        g = g_c;
+    }
+    // hits: one reservation for the warp
+    const bool hit = has && edep > 0.0;
+    const unsigned hit_mask = __ballot_sync(0xffffffffu, hit);
+    if (hit_mask) {
+        unsigned long long base = 0;
+        if (lane == 0 && a.keep_hits) base = atomicAdd(a.hit_count, static_cast<unsigned long long>(__popc(hit_mask)));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (hit) {
+            cmpmc_sim_stats& o = a.ev_stats[r.ev];
+            const double wedep = edep * static_cast<double>(r.w);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&o.sensor_hits), 1ull);
+            atomicAdd(&o.total_deposited_eV, wedep);
+            if (a.keep_hits) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(a.ev_nhits + r.ev), 1ull);
+                const unsigned long long idx = base + __popc(hit_mask & lanemask_lt());
+                if (idx < a.hit_cap) {
+                    cmpmc_sensor_hit h;
+                    h.pos[0] = r.px; h.pos[1] = r.py; h.pos[2] = r.pz;
+                    h.time = r.t;
+                    h.edep = wedep;
+                    h.incident_energy = r.E;
+                    h.surface_id = r.surf;
+                    h.excitation = 0;
+                    h.mode = r.mode;
+                    h._pad = 0;
+                    h.channel_id = r.ch_id;
+                    a.hit_stage[idx] = h;
+                    a.hit_key[idx] = r.ev;
+                }
+            }
+        }
+    }
+    if (has) {
+        double sum_refl = 0.0;
+        for (int j = 0; j < n_refl; ++j) sum_refl += refl_buf[j];
+        const double esc = dmax(0.0, r.E - edep - sum_refl) * static_cast<double>(r.w);
+        if (esc != 0.0) atomicAdd(&a.ev_stats[r.ev].escaped_or_killed_eV, esc);
+    }
+    // re-emissions: an exclusive warp scan of the counts places them in the ring
+    int incl = n_refl;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const uint32_t total = static_cast<uint32_t>(__shfl_sync(0xffffffffu, incl, 31));
+    if (r_tail + total - r_head > ring_mask + 1) {  // ring full: the call reruns with a larger ring
+        if (lane == 0) *err |= kErrQueue;
+        return r_tail;
+    }
+    if (n_refl > 0) {
+        uint32_t pos = r_tail + static_cast<uint32_t>(incl - n_refl);
+        F3 n;
+        if (r.surf == 0) n = f3(0.0f, 0.0f, -1.0f);
+        else if (r.surf == 1) n = f3(0.0f, 0.0f, 1.0f);
+        else {
+            const float rr = sqrtf(r.px * r.px + r.py * r.py);
+            n = (rr > 1e-15f) ? f3(-r.px / rr, -r.py / rr, 0.0f) : f3(-1.0f, 0.0f, 0.0f);
+        }
+        FTrack t;
+        t.pos = f3(r.px, r.py, r.pz) + n * kNudge;
+        t.t = r.t;
+        t.w = r.w;
+        for (int j = 0; j < n_refl; ++j, ++pos) {
+            t.mode = fdos(L, g.u());
+            FKin kin;
+            t.k = finward<kKin>(L, t.mode, n, g, kin);
+            t.vg = kin.dir;
+            t.vmag = kin.mag;
+            t.E = refl_buf[j];
+            t.bounces = (j == 0) ? r.bounces : 0u;
+            ring[pos & ring_mask] = pool_entry(t, mix64(r.key ^ (0x9e3779b97f4a7c15ULL * static_cast<uint64_t>(j + 1))),
+                                               r.ev);
+        }
+    }
+    return r_tail + total;
+}
+
+template <bool kSur, int kKin = 0>
+__global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FLat L,
+                                                      const __grid_constant__ Detector D,
+                                                      const __grid_constant__ RunArgs a,
+                                                      const __grid_constant__ PoolArgs p) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+    PoolPh* ring = p.ring + warp * p.ring_cap;
+    const FilmRec* fb_c = p.film + warp * kPoolFilmCap;
+    FilmRec* fb = p.film + warp * kPoolFilmCap;
+    const uint32_t ring_mask = p.ring_cap - 1;
+    uint32_t r_head = 0, r_tail = 0, f_head = 0, f_tail = 0;  // warp-uniform
+    bool input_left = true;                                    // warp-uniform
+    double refl_buf[kKaplanCap];
+    double kwork[4 * kKaplanCap];
+    unsigned err = 0;
+    const uint64_t seed_key = mix64(a.seed ^ 0x5851f42d4c957f2dULL);
+    __shared__ uint32_t s_cnt[kNCnt][kMaxBlock];
+    __shared__ double s_led[2][kMaxBlock];
+    __shared__ PoolOut s_out[kMaxBlock];
+    const UStats st{&s_cnt[0][threadIdx.x], &s_led[0][threadIdx.x]};
+    PoolOut& my_out = s_out[threadIdx.x];
+    FTrack trk;
+    R128 g;
+    uint32_t ev_cur = 0;
+    bool live = false;
+    for (;;) {
+        // ring and film entries written by other lanes of the warp are visible after this
+        __syncwarp();
+        // 1. refill the empty lanes: the ring first, then new primaries
+        const unsigned empty = __ballot_sync(full, !live);
+        if (empty) {
+            const int n_empty = __popc(empty);
+            const int rank = __popc(empty & lanemask_lt());
+            const uint32_t from_ring = min(r_tail - r_head, static_cast<uint32_t>(n_empty));
+            if (!live && rank < static_cast<int>(from_ring)) {
+                const PoolPh q = ring[(r_head + rank) & ring_mask];
+                trk.pos = f3(q.px, q.py, q.pz);
+                trk.k = f3(q.kx, q.ky, q.kz);
+                trk.vg = f3(q.vx, q.vy, q.vz);
+                trk.vmag = q.vmag;
+                trk.w = q.w;
+                trk.bounces = q.bounces_mode >> 2;
+                trk.mode = static_cast<int>(q.bounces_mode & 3u);
+                trk.E = q.E;
+                trk.t = q.t;
+                g.seed(q.key);
+                ev_cur = q.ev;
+                st.clear();
+                live = true;
+            }
+            r_head += from_ring;
+            const int need = n_empty - static_cast<int>(from_ring);
+            if (need > 0 && input_left) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(a.next_work, static_cast<unsigned long long>(need));
+                base = __shfl_sync(full, base, 0);
+                if (base + need >= a.n_events) input_left = false;
+                const uint64_t unit = base + static_cast<uint64_t>(rank - static_cast<int>(from_ring));
+                if (!live && rank >= static_cast<int>(from_ring) && unit < a.n_events) {
+                    const uint32_t ev = p.unit_event[unit];
+                    ev_cur = ev;
+                    const uint64_t j = unit - a.ph_off[ev];
+                    g.seed(seed_key ^ mix64(((a.first_event + ev) << 20) | j));
+                    const cmpmc_phonon_track& in = a.ph[unit];
+                    trk.pos = f3(static_cast<float>(in.pos[0]), static_cast<float>(in.pos[1]),
+                                 static_cast<float>(in.pos[2]));
+                    trk.k = f3(static_cast<float>(in.k_dir[0]), static_cast<float>(in.k_dir[1]),
+                               static_cast<float>(in.k_dir[2]));
+                    trk.vg = f3(static_cast<float>(in.vg_dir[0]), static_cast<float>(in.vg_dir[1]),
+                                static_cast<float>(in.vg_dir[2]));
+                    trk.vmag = static_cast<float>(in.vg_mag);
+                    trk.E = in.energy;
+                    trk.t = in.time;
+                    trk.w = static_cast<float>(in.weight);
+                    trk.bounces = in.bounces;
+                    trk.mode = in.mode;
+                    st.clear();
+                    live = true;
+                }
+            }
+        }
+        if (__ballot_sync(full, live) == 0) {
+            // no transport work left in this warp: drain the film buffer, then stop
+            if (f_tail != f_head) {
+                const int n_rec = static_cast<int>(min(f_tail - f_head, 32u));
+                r_tail = pool_film_step<kSur, kKin>(&L, &D, &a, fb_c, f_head, n_rec, ring, ring_mask, r_head, r_tail,
+                                                    refl_buf, kwork, &err);
+                f_head += n_rec;
+                if (__any_sync(full, err != 0)) break;
+                continue;
+            }
+            if (r_tail == r_head) break;
+            continue;
+        }
+        // 2. one step of every live track
+        int outcome = kStepOn;
+        bool has_d = false;
+        if (live) {
+            outcome = pool_step<kKin>(L, D, trk, g, st, ev_cur, my_out, has_d);
+            if (outcome != kStepOn) {
+                sink_unit(&a, ev_cur, st);
+                live = false;
+            }
+        }
+        // 3. regroup: daughters to the ring, film entries to the film buffer
+        const unsigned d_mask = __ballot_sync(full, has_d);
+        if (d_mask) {
+            if (r_tail + __popc(d_mask) - r_head > p.ring_cap) {
+                err |= kErrQueue;
+                break;
+            }
+            if (has_d) ring[(r_tail + __popc(d_mask & lanemask_lt())) & ring_mask] = my_out.ph;
+            r_tail += __popc(d_mask);
+        }
+        const unsigned f_mask = __ballot_sync(full, outcome == kStepFilm);
+        if (f_mask) {
+            if (outcome == kStepFilm) fb[(f_tail + __popc(f_mask & lanemask_lt())) & (kPoolFilmCap - 1)] = my_out.film;
+            f_tail += __popc(f_mask);
+        }
+        // 4. the film step, converged, once 32 entries wait
+        if (f_tail - f_head >= 32) {
+            __syncwarp();
+            r_tail = pool_film_step<kSur, kKin>(&L, &D, &a, fb_c, f_head, 32, ring, ring_mask, r_head, r_tail,
+                                                refl_buf, kwork, &err);
+            f_head += 32;
+            if (__any_sync(full, err != 0)) break;
+        }
+    }
+    if (err && lane == 0) atomicOr(a.err, err);
+}
+
 // Adjoint of the hit-time histogram: the batched transport with per-track scores. Bin
 // weights (dLoss/dh_b) and the block's histogram live in shared memory; the histogram is
 // added to the global FP64 bins once per block.
@@ -881,6 +1418,28 @@ cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detect
     }
     return cudaGetLastError();
 }
+
+cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
+                             uint32_t ring_cap, void* film, const uint32_t* unit_event, int grid, int block,
+                             cudaStream_t s) {
+    const FLat f = make_flat(L, cdf_f, D);
+    PoolArgs p;
+    p.ring = static_cast<PoolPh*>(ring);
+    p.film = static_cast<FilmRec*>(film);
+    p.ring_cap = ring_cap;
+    p.unit_event = unit_event;
+    if (L.kin_mode != kKinOctahedral) k_pool_fp32<false, 1><<<grid, block, 0, s>>>(f, D, a, p);
+    else if (a.surrogate) k_pool_fp32<true><<<grid, block, 0, s>>>(f, D, a, p);
+    else k_pool_fp32<false><<<grid, block, 0, s>>>(f, D, a, p);
+    return cudaGetLastError();
+}
+
+cudaError_t pool_fp32_occupancy(int block, int* blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_pool_fp32<false>, block, 0);
+}
+
+size_t pool_ring_entry_bytes() { return sizeof(PoolPh); }
+size_t pool_film_bytes_per_warp() { return sizeof(FilmRec) * kPoolFilmCap; }
 
 cudaError_t launch_adjoint_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a,
                                 const AdjArgs& adj, const uint32_t* unit_event, int grid, int block, cudaStream_t s) {

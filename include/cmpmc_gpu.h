@@ -446,12 +446,13 @@ typedef struct cmpmc_gpu_ctx cmpmc_gpu_ctx;
 enum {
     CMPMC_FORM_PLAIN_FP64          = 0,  /* bit-exact event streams, one event per device thread */
     CMPMC_FORM_BATCHED_FP32        = 1,  /* own substreams per primary, FP32 geometry, FP64
-                                            ledger and time of flight; wavefront split: film
-                                            entries run in a film kernel and their re-emitted
-                                            phonons re-enter through a device queue (hits of an
-                                            event in no fixed order, FP64 event sums by
-                                            atomics); with charges: per-carrier substreams, FP32
-                                            drift, Luke phonons through the queue             */
+                                            ledger and time of flight; film cascades run apart
+                                            from the transport steps and their re-emitted
+                                            phonons re-enter through device queues (the warp
+                                            pool, cmpmc_gpu_configure_pool; hits of an event in
+                                            no fixed order, FP64 event sums by atomics); with
+                                            charges: per-carrier substreams, FP32 drift, Luke
+                                            phonons through the queue                         */
     CMPMC_FORM_BATCHED_FP32_INLINE = 2   /* the batched form with each primary's whole lineage on
                                             one thread (film cascades inline): hits in a fixed
                                             order, the forward of cmpmc_gpu_adjoint           */
@@ -525,6 +526,19 @@ int cmpmc_gpu_configure_graph(cmpmc_gpu_ctx* ctx, int enable);
  * limit). A limit changes which substream a long track continues on: the results are then
  * statistically, not bitwise, those of the unlimited run; the autotuner leaves it alone. */
 int cmpmc_gpu_configure_phases(cmpmc_gpu_ctx* ctx, uint32_t phase_steps);
+
+/* Launch form of the batched FP32 phonon transport (no counterpart in the reference).
+ * enable = 1 (the default): the warp pool, one persistent launch per call in which every
+ * warp keeps its 32 lanes busy from a private ring of pending phonons (film re-emissions and
+ * daughters) and the batch's primaries, and runs the film cascades of its lanes 32 at a
+ * time; the host synchronizes once per call. enable = 0: the host-driven form, alternating
+ * transport and film launches until both device queues are empty (one host round trip per
+ * round; configure_phases applies to it only). ring_capacity: pending phonons per warp (a
+ * power of two >= 64, 80 B each; default 1024, grown 4x and the call rerun when a warp's
+ * ring overflows; 0 keeps the current value). Both forms sample the same process; a
+ * daughter runs on a substream drawn from its parent's in the pool form, on the parent's
+ * own stream in the host-driven form, so their hits agree in distribution, not bit for bit. */
+int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int enable, uint32_t ring_capacity);
 
 /* Autotuner of the launch configuration (no counterpart in the reference): runs `sample`
  * (a representative call, outputs discarded) `repeats` times for each candidate, keeps the

@@ -12,6 +12,8 @@ compiled from its own headers by `make -C oracle ref`) and stores compact record
                         sums over the hits, hash of the discrete hit fields)
   c1_hist.npz           per-event hit histograms (time, radius, energy) of 2000 mixed-energy
                         events (200,000 primaries), for the batched FP32 form's chi^2 tests
+  c1_hist_full.npz      the same over all 10,000 events of the benchmark batch (1,000,000
+                        primaries; histfull), for the bench's matched-statistics check
   <workload>_cr_*.npz   the same from oracle/_ref/cmpmc_ref_crlibm: the reference whose
                         transport uses a correctly rounded libm (oracle/ref_crlibm.hpp);
                         `floor` = fraction of events on which it agrees with the glibc build
@@ -26,7 +28,8 @@ compiled from its own headers by `make -C oracle ref`) and stores compact record
                         201,898 nodes): field_at and potential_at at 4096 points in the cylinder
 
 Usage: python tests/golden/make_golden.py [--only NAME,...]   (needs the reference build;
-       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist, kin, amm, kaplan, mask or mesh)
+       takes a few minutes; NAME is a workload of PLAN, rng, lattice, hist, histfull, kin, amm, kaplan,
+       mask or mesh)
 """
 from __future__ import annotations
 
@@ -149,6 +152,8 @@ def main() -> None:
         _workloads(tmp, want)
         if want("hist"):
             _hist(tmp)
+        if want("histfull"):
+            _hist_full(tmp)
     gl = subprocess.run(["ldd", "--version"], capture_output=True, text=True).stdout.split("\n")[0]
     with open(os.path.join(HERE, "PROVENANCE.txt"), "w") as f:
         f.write("Generated by tests/golden/make_golden.py from the unmodified reference CMPMC\n"
@@ -341,6 +346,33 @@ def _hist(tmp: str) -> None:
                         escaped=st["escaped_or_killed_eV"].sum(), steps=st["total_steps"].sum(),
                         n_hits=len(d["hits"]))
     print("c1 histograms from", len(d["hits"]), "hits")
+
+
+def _hist_full(tmp: str) -> None:
+    """The same histograms over the whole mixed-energy batch of the benchmark (10,000 events,
+    1,000,000 primaries), in chunks of 2,000 events, with the edep range of c1_hist.npz."""
+    rng = tuple(np.load(os.path.join(HERE, "c1_hist.npz"))["edep_range"])
+    tot, inj, dep, esc, steps, n_hits = None, 0.0, 0.0, 0.0, 0, 0
+    for first in range(0, 10000, 2000):
+        d = dump("c1", first, 2000, tmp)
+        h = event_histograms(d["hit_offsets"], d["hits"], rng)
+        if tot is None:
+            tot = h
+        else:
+            for k, v in h.items():
+                if k != "edep_range":
+                    tot[k] = tot[k] + v
+        st = d["events"]["stats"]
+        inj += float(d["injected"].sum())
+        dep += float(st["total_deposited_eV"].sum())
+        esc += float(st["escaped_or_killed_eV"].sum())
+        steps += int(st["total_steps"].sum())
+        n_hits += len(d["hits"])
+        for f in os.listdir(tmp):  # the hit dumps are large
+            os.remove(os.path.join(tmp, f))
+    np.savez_compressed(os.path.join(HERE, "c1_hist_full.npz"), **tot, injected=inj, deposited=dep, escaped=esc,
+                        steps=steps, n_hits=n_hits)
+    print("c1 histograms (10,000 events) from", n_hits, "hits")
 
 
 if __name__ == "__main__":

@@ -141,8 +141,7 @@ def event_histograms(hit_offsets: np.ndarray, hits: np.ndarray, edep_range: tupl
             lo, hi = edep_range
         b = np.floor((values[name] - lo) / (hi - lo) * nb).astype(np.int64)
         ok = (b >= 0) & (b < nb)
-        counts = np.zeros((n, nb), dtype=np.float64)
-        np.add.at(counts, (ev[ok], b[ok]), 1.0)
+        counts = np.bincount(ev[ok] * nb + b[ok], minlength=n * nb).astype(np.float64).reshape(n, nb)
         out[name + "_sum"] = counts.sum(axis=0)
         out[name + "_sumsq"] = (counts * counts).sum(axis=0)
     out["edep_range"] = np.array(edep_range, dtype=np.float64)

@@ -246,3 +246,47 @@ def test_batched_kinematics_modes_statistics(ge_lattice, wl, n):
     with pytest.raises(cm.CmpmcError):
         eng.run_packed(eng.generate(workload_of(wl), 8, WORKLOAD_SEED[wl]),
                        cm.RunOptions(seed=1, form="batched_fp32", kaplan_surrogate=True))
+
+
+def test_pool_and_host_driven_rounds_agree(ge_lattice):
+    """The warp pool (one persistent launch) and the host-driven film / transport rounds
+    sample the same process (a daughter's substream differs between them): hit histograms
+    chi^2 p > 0.01 on 2,000 mixed-energy events, the same deposited fraction within 1 %,
+    both ledgers closed."""
+    import cmpmc_b200 as cm
+    eng = _engine(ge_lattice, "c1")
+    packed = eng.generate(workload_of("c1"), 2000, 7)
+    a = eng.run_packed(packed, cm.RunOptions(seed=7, form="batched_fp32"))
+    eng2 = _engine(ge_lattice, "c1")
+    eng2.configure_pool(False)
+    b = eng2.run_packed(packed, cm.RunOptions(seed=7, form="batched_fp32"))
+    assert a.kernel_launches < b.kernel_launches  # one transport launch against the rounds
+    lo = min(a.hits["edep"].min(), b.hits["edep"].min())
+    hi = max(a.hits["edep"].max(), b.hits["edep"].max()) * (1 + 1e-9)
+    ha, hb = event_histograms(a.hit_offsets, a.hits, (lo, hi)), event_histograms(b.hit_offsets, b.hits, (lo, hi))
+    for name in ("time", "radius", "edep"):
+        c2, dof, p = hist_chi2(ha, hb, name)
+        print(f"pool vs rounds {name}: chi2 {c2:.1f} dof {dof} p {p:.3f}")
+        assert p > P_MIN, (name, c2, dof, p)
+    for st in (a.stats, b.stats):
+        assert abs(st.total_injected_eV - st.total_deposited_eV - st.escaped_or_killed_eV) / st.total_injected_eV <= LEDGER_TOL
+    fa = a.stats.total_deposited_eV / a.stats.total_injected_eV
+    fb = b.stats.total_deposited_eV / b.stats.total_injected_eV
+    assert abs(fa / fb - 1.0) < 0.01
+
+
+def test_pool_ring_overflow_reruns_to_the_same_hits(ge_lattice):
+    """A warp ring that is too small (64 entries) overflows on the device; the call grows it
+    and reruns, and the hits of every event (as a set) and the integer counters equal the
+    default ring's: every unit owns its substream."""
+    import cmpmc_b200 as cm
+    eng = _engine(ge_lattice, "c1")
+    a = _batched(eng, "c1", 300, want_event_stats=True)
+    eng2 = _engine(ge_lattice, "c1")
+    eng2.configure_pool(True, ring_capacity=64)
+    b = _batched(eng2, "c1", 300, want_event_stats=True)
+    assert np.array_equal(a.hit_offsets, b.hit_offsets)
+    assert _sorted_event_hits(a) == _sorted_event_hits(b)
+    for name in a.event_stats.dtype.names:
+        if a.event_stats.dtype[name].kind == "u":
+            assert np.array_equal(a.event_stats[name], b.event_stats[name]), name
