@@ -406,20 +406,49 @@ def main() -> None:
         return t
     hp = [pinned(packed.rng_state), pinned(packed.injected_eV), pinned(packed.phonon_offsets), pinned(packed.phonons)]
     hd = desc(False, tuple(t.data_ptr() for t in hp))
+    if world > 1:
+        # several GPUs: the outputs stay on each rank's device and are merged on rank 0 over
+        # NCCL (cmpmc_b200.dist.exchange), which then copies the merged hits to the host
+        from cmpmc_b200 import dist as cdist
+        hd.outputs_on_device = 1
+        out_host = None
+
+        def merge_to_root(o):
+            nonlocal out_host
+            d_hits = torch.empty(max(int(o.n_hits), 1) * 56, dtype=torch.uint8, device=f"cuda:{dev}")[:int(o.n_hits) * 56]
+            d_offs = torch.empty(args.events + 1, dtype=torch.int64, device=f"cuda:{dev}")
+            if o.n_hits:
+                lib.cmpmc_gpu_memcpy(C.c_void_p(d_hits.data_ptr()), C.c_void_p(o.hits), int(o.n_hits) * 56)
+            lib.cmpmc_gpu_memcpy(C.c_void_p(d_offs.data_ptr()), C.c_void_p(o.hit_offsets), (args.events + 1) * 8)
+            st = torch.from_numpy(np.frombuffer(bytes(o.stats), dtype=np.uint8).copy()).to(f"cuda:{dev}")
+            m = cdist.exchange(d_hits, d_offs, st)
+            if m["hits"] is not None:
+                if out_host is None or out_host.numel() < m["hits"].numel():
+                    out_host = torch.empty(m["hits"].numel(), dtype=torch.uint8, pin_memory=True)
+                out_host[:m["hits"].numel()].copy_(m["hits"])
+                torch.cuda.synchronize(dev)
+                return m["hits"].numel() + m["hit_offsets"].numel() * 8 + 208
+            return 0
     lib.cmpmc_gpu_configure_graph(h, 0)
-    run(hd)
+    o = run(hd)
+    if world > 1:
+        merge_to_root(o)
     barrier()
     e2e_ms = []
+    d2h = 0
     for _ in range(args.steps):
         flush.zero_()
         barrier()
         t1 = time.perf_counter()
         o = run(hd)
+        if world > 1:
+            d2h = merge_to_root(o)
         e2e_ms.append(1e3 * (time.perf_counter() - t1))
     e2e_step = max_over_ranks(sum(e2e_ms) / args.steps)
     gen_ms = max_over_ranks(1e3 * t_gen)
     h2d = sum(t.numel() for t in hp)
-    d2h = int(o.n_hits) * 56 + (args.events + 1) * 8 + 208
+    if world == 1:
+        d2h = int(o.n_hits) * 56 + (args.events + 1) * 8 + 208
 
     # plain FP64 form on the same workload (bit-exact event streams), one step
     plain = None
