@@ -266,6 +266,7 @@ _SIG = {
     "cmpmc_gpu_configure_graph": (_i32, [C.c_void_p, _i32]),
     "cmpmc_gpu_configure_phases": (_i32, [C.c_void_p, _u32]),
     "cmpmc_gpu_configure_pool": (_i32, [C.c_void_p, _i32, _u32]),
+    "cmpmc_gpu_configure_staging": (_i32, [C.c_void_p, _i32]),
     "cmpmc_gpu_memcpy": (_i32, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "cmpmc_gpu_autotune": (_i32, [C.c_void_p, C.POINTER(RunDescC), _i32, C.POINTER(TuneResultC)]),
     "cmpmc_kaplan_surrogate_create": (_i32, [C.POINTER(FilmConfigC), _u64, C.POINTER(C.c_void_p)]),

@@ -978,6 +978,12 @@ class SimulationEngine:
         h = self.context(device)
         _check(self._lib.cmpmc_gpu_configure_pool(h, int(enable), int(ring_capacity)), h)
 
+    def configure_staging(self, enable: bool = True, device: int = 0) -> None:
+        """Decay CDF tables staged in shared memory by a TMA bulk copy (default) or read from
+        global memory (cmpmc_gpu_configure_staging); the results are identical."""
+        h = self.context(device)
+        _check(self._lib.cmpmc_gpu_configure_staging(h, int(enable)), h)
+
     def configure_graph(self, enable: bool = True, device: int = 0) -> None:
         """Replay repeated batched calls on device-resident inputs as one CUDA graph."""
         h = self.context(device)

@@ -109,6 +109,7 @@ struct cmpmc_gpu_ctx {
     uint64_t film_cap = 1ull << 22;                     // film entries per phase (64 B each)
     uint32_t phase_steps = 0;                           // steps a track takes per transport phase (0: any)
     int pool = 1;                                       // batched phonon form: 1 warp pool, 0 host-driven rounds
+    int stage_tables = 1;                               // pool form: decay CDF tables staged in shared memory
     uint32_t pool_ring_cap = 1024;                      // pending phonons per warp in the pool form
     DevBuf pool_ring, pool_film;                        // warp pool: per-warp rings and film buffers
     uint64_t queue_cap = 1ull << 24;                    // Luke-phonon queue entries (64 B each)
@@ -701,7 +702,7 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
         CK(cudaEventRecord(ctx->e_k0, s), "event");
         if (n_ph) {
             CK(launch_pool_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->pool_ring.p, ctx->pool_ring_cap, ctx->pool_film.p,
-                                ctx->unit_event.as<uint32_t>(), static_cast<int>(grid), tpb, s),
+                                ctx->unit_event.as<uint32_t>(), ctx->stage_tables, static_cast<int>(grid), tpb, s),
                "pool launch");
             ++launches;
         }
@@ -1012,6 +1013,12 @@ int cmpmc_gpu_autotune(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* sample, int rep
 int cmpmc_gpu_configure_phases(cmpmc_gpu_ctx* ctx, uint32_t phase_steps) {
     if (!ctx) return CMPMC_ERR_INVALID;
     ctx->phase_steps = phase_steps;
+    return CMPMC_OK;
+}
+
+int cmpmc_gpu_configure_staging(cmpmc_gpu_ctx* ctx, int enable) {
+    if (!ctx || enable < 0 || enable > 1) return CMPMC_ERR_INVALID;
+    ctx->stage_tables = enable;
     return CMPMC_OK;
 }
 

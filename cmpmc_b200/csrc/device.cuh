@@ -16,6 +16,7 @@ enum : unsigned {
     kErrResume = 8u,
     kErrFilmQueue = 16u,
     kErrRelease = 32u,     // batched charge release: release records or their phonons overflowed
+    kErrStage = 64u,       // a shared-memory staging copy did not complete within its wait limit
 };
 
 // A pushed phonon in a per-thread global-memory LIFO (112 B, 16-byte aligned)
@@ -301,8 +302,8 @@ cudaError_t film_fp32_occupancy(int block, int* blocks_per_sm);
 // ring_cap pending-phonon entries (pool_ring_entry_bytes) per warp, `film`
 // pool_film_bytes_per_warp bytes per warp; grid * block / 32 warps
 cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
-                             uint32_t ring_cap, void* film, const uint32_t* unit_event, int grid, int block,
-                             cudaStream_t s);
+                             uint32_t ring_cap, void* film, const uint32_t* unit_event, int stage_tables, int grid,
+                             int block, cudaStream_t s);
 cudaError_t pool_fp32_occupancy(int block, int* blocks_per_sm);
 size_t pool_ring_entry_bytes();
 size_t pool_film_bytes_per_warp();

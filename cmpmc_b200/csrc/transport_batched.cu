@@ -799,6 +799,53 @@ __global__ void __launch_bounds__(128, 8) k_film_fp32(const __grid_constant__ FL
     if (err) atomicOr(a.err, err);
 }
 
+// ---- shared-memory staging of the small tables by the TMA engine -----------------------
+// One thread issues an untiled bulk copy (cp.async.bulk global -> shared, no multicast, the
+// source is this GPU's own memory) whose completion is counted on an mbarrier; every thread
+// then waits on the barrier's first phase. The wait is bounded: a copy that has not landed
+// after kStageSpins polls is reported (false) and the block must not touch the destination.
+constexpr int kStageSpins = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// src and dst 16-byte aligned, bytes a multiple of 16; called by every thread of the block
+__device__ __forceinline__ bool stage_bulk(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    const uint32_t b = smem_addr(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(b),
+                     "r"(bytes)
+                     : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(dst)),
+                     "l"(src), "r"(bytes), "r"(b)
+                     : "memory");
+    }
+    __syncthreads();  // the barrier is initialised before anyone polls it
+    for (int i = 0; i < kStageSpins; ++i) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(b)
+                     : "memory");
+        if (done) return true;
+        __nanosleep(32);
+    }
+    return false;
+}
+
+// inverse-CDF sample from a table in either memory space (plain loads: the staged copy
+// lives in shared memory)
+__device__ __forceinline__ float fcdf_any(const float* cdf, R128& g) {
+    const float u = g.u() * (kNCdf - 1);
+    const int i = min(static_cast<int>(u), kNCdf - 2);
+    const float f = u - i;
+    return cdf[i] * (1.0f - f) + cdf[i + 1] * f;
+}
+
 // ---- warp pool form -------------------------------------------------------------------
 // One persistent launch transports the whole batch. Each warp owns a private ring of
 // pending phonons (film re-emissions and daughters, with their group velocity, so a refill
@@ -856,7 +903,8 @@ __device__ __forceinline__ uint64_t draw_key(R128& g) {
 // anharmonic decay of an L phonon (engine.hpp:938-988), FP32 angles: the parent continues
 // in *tp, the daughter is written to *dp (it runs later on a substream of its own)
 template <int kKin>
-__device__ __noinline__ void pool_decay(const FLat* Lp, FTrack* tp, FTrack* dp, const UStats* st, R128* gp) {
+__device__ __noinline__ void pool_decay(const FLat* Lp, const float* cdf, FTrack* tp, FTrack* dp, const UStats* st,
+                                        R128* gp) {
     const FLat& L = *Lp;
     FTrack& trk = *tp;
     R128& g = *gp;
@@ -869,7 +917,7 @@ __device__ __noinline__ void pool_decay(const FLat* Lp, FTrack* tp, FTrack* dp, 
     const float m = L.m_ratio, mm = m * m;
     if (g.u() < L.fTT) {
         ++st->tt();
-        x = fcdf(L.cdf_tt, g);
+        x = fcdf_any(cdf + kNCdf, g);
         const float y = 1.0f - x;
         th1 = facos_clamped((1.0f - mm * y * y + mm * x * x) / (2.0f * m * x));
         th2 = facos_clamped((1.0f - mm * x * x + mm * y * y) / (2.0f * m * y));
@@ -877,7 +925,7 @@ __device__ __noinline__ void pool_decay(const FLat* Lp, FTrack* tp, FTrack* dp, 
         m2 = ftrans(L, g);
     } else {
         ++st->lt();
-        x = fcdf(L.cdf_lt, g);
+        x = fcdf_any(cdf, g);
         th1 = facos_clamped((1.0f + x * x * (1.0f - mm) + 2.0f * x * mm - mm) / (2.0f * x));
         th2 = facos_clamped((1.0f - x * x + mm * (1.0f - x) * (1.0f - x)) / (2.0f * m * (1.0f - x)));
         m1 = 0;
@@ -922,8 +970,8 @@ union PoolOut {
 };
 
 template <int kKin>
-__device__ __forceinline__ int pool_step(const FLat& L, const Detector& D, FTrack& trk, R128& g, const UStats& st,
-                                         uint32_t ev, PoolOut& out, bool& has_d) {
+__device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const Detector& D, FTrack& trk, R128& g,
+                                         const UStats& st, uint32_t ev, PoolOut& out, bool& has_d) {
     has_d = false;
     if (trk.E < D.min_phonon_eV || trk.bounces >= D.max_bounces) {
         ++st.killed();
@@ -958,7 +1006,7 @@ __device__ __forceinline__ int pool_step(const FLat& L, const Detector& D, FTrac
         if (r_down > 0.0f && u_proc < r_down) {
             FTrack t_c = trk, d_c;
             R128 g_c = g;
-            pool_decay<kKin>(&L, &t_c, &d_c, &st, &g_c);
+            pool_decay<kKin>(&L, cdf, &t_c, &d_c, &st, &g_c);
             trk = t_c;
             g = g_c;
             out.ph = pool_entry(d_c, draw_key(g), ev);
@@ -1023,7 +1071,7 @@ __device__ __forceinline__ int pool_step(const FLat& L, const Detector& D, FTrac
         if (u_refl < p_anh) {
             ++st.down();
             const bool tt = g.u() < L.fTT;
-            const float x = tt ? fcdf(L.cdf_tt, g) : fcdf(L.cdf_lt, g);
+            const float x = fcdf_any(tt ? cdf + kNCdf : cdf, g);
             const int m1 = tt ? ftrans(L, g) : 0;
             const int m2 = ftrans(L, g);
             FTrack dtr;
@@ -1091,6 +1139,7 @@ struct PoolArgs {
     FilmRec* film;          // [warps][kPoolFilmCap]
     uint32_t ring_cap;      // a power of two
     const uint32_t* unit_event;
+    int stage_tables;       // decay CDF tables read from a shared-memory copy staged by TMA
 };
 
 // The film step of a warp, converged: lane l < n_rec runs the cascade of film record
@@ -1224,8 +1273,18 @@ __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FL
     __shared__ uint32_t s_cnt[kNCnt][kMaxBlock];
     __shared__ double s_led[2][kMaxBlock];
     __shared__ PoolOut s_out[kMaxBlock];
+    __shared__ alignas(128) float s_cdf[2 * kNCdf];  // the decay CDF tables (L-LT, then TT)
+    __shared__ alignas(8) uint64_t s_bar;
     const UStats st{&s_cnt[0][threadIdx.x], &s_led[0][threadIdx.x]};
     PoolOut& my_out = s_out[threadIdx.x];
+    const float* cdf = L.cdf_lt;  // the two tables are contiguous in global memory
+    if (p.stage_tables) {
+        if (!stage_bulk(s_cdf, L.cdf_lt, 2 * kNCdf * sizeof(float), &s_bar)) {
+            if (threadIdx.x == 0) atomicOr(a.err, kErrStage);
+            return;
+        }
+        cdf = s_cdf;
+    }
     FTrack trk;
     R128 g;
     uint32_t ev_cur = 0;
@@ -1303,7 +1362,7 @@ __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FL
         int outcome = kStepOn;
         bool has_d = false;
         if (live) {
-            outcome = pool_step<kKin>(L, D, trk, g, st, ev_cur, my_out, has_d);
+            outcome = pool_step<kKin>(L, cdf, D, trk, g, st, ev_cur, my_out, has_d);
             if (outcome != kStepOn) {
                 sink_unit(&a, ev_cur, st);
                 live = false;
@@ -1420,14 +1479,15 @@ cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detect
 }
 
 cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
-                             uint32_t ring_cap, void* film, const uint32_t* unit_event, int grid, int block,
-                             cudaStream_t s) {
+                             uint32_t ring_cap, void* film, const uint32_t* unit_event, int stage_tables, int grid,
+                             int block, cudaStream_t s) {
     const FLat f = make_flat(L, cdf_f, D);
     PoolArgs p;
     p.ring = static_cast<PoolPh*>(ring);
     p.film = static_cast<FilmRec*>(film);
     p.ring_cap = ring_cap;
     p.unit_event = unit_event;
+    p.stage_tables = stage_tables;
     if (L.kin_mode != kKinOctahedral) k_pool_fp32<false, 1><<<grid, block, 0, s>>>(f, D, a, p);
     else if (a.surrogate) k_pool_fp32<true><<<grid, block, 0, s>>>(f, D, a, p);
     else k_pool_fp32<false><<<grid, block, 0, s>>>(f, D, a, p);

@@ -540,6 +540,13 @@ int cmpmc_gpu_configure_phases(cmpmc_gpu_ctx* ctx, uint32_t phase_steps);
  * own stream in the host-driven form, so their hits agree in distribution, not bit for bit. */
 int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int enable, uint32_t ring_capacity);
 
+/* Shared-memory staging of the small tables (no counterpart in the reference): with
+ * enable = 1 (the default) every block of the warp-pool kernel copies the two decay CDF
+ * tables (CrystalLattice::sample_lt/tt_energy_fraction's, crystal_lattice.hpp:200-212; 8 KiB
+ * as FP32) into shared memory with one TMA bulk copy and samples from there; 0 reads them
+ * from global memory. The results are identical either way. */
+int cmpmc_gpu_configure_staging(cmpmc_gpu_ctx* ctx, int enable);
+
 /* Autotuner of the launch configuration (no counterpart in the reference): runs `sample`
  * (a representative call, outputs discarded) `repeats` times for each candidate, keeps the
  * fastest transport-kernel time and applies it to the context. Candidates: the current

@@ -104,12 +104,14 @@
 //   pubc the same detector at 4 V with luke_sample_fraction 0 and one e-/h+ pair per event at
 //       the origin (the benchmark's `charge` mode); seed 12345
 //
-// Built with -DCMPMC_ORACLE_CRLIBM (as cmpmc_ref_crlibm) the transport uses a correctly
-// rounded libm (ref_crlibm.hpp); the generators and the lattice build keep the
-// platform libm, as they do in the device path (they run on the host there).
+// Built with -DCMPMC_ORACLE_CRLIBM and linked with crlibm_libm.cpp (as cmpmc_ref_crlibm),
+// the same program runs the reference against a correctly rounded libm in the transport;
+// the generators and the lattice build keep the platform libm, as they do in the device
+// path (they run on the host there). The reference's headers are compiled identically in
+// both builds.
 #ifdef CMPMC_ORACLE_CRLIBM
-#include "ref_crlibm.hpp"
-#define CMPMC_SET_CRLIBM(v) (cmpmc_oracle::g_crlibm = (v))
+extern "C" void cmpmc_oracle_set_crlibm(int on);
+#define CMPMC_SET_CRLIBM(v) cmpmc_oracle_set_crlibm((v) ? 1 : 0)
 #else
 #define CMPMC_SET_CRLIBM(v) ((void)0)
 #endif

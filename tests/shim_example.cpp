@@ -1,6 +1,7 @@
 // Test of the C++ drop-in (include/cmpmc_b200/run_events_gpu.hpp). Built by oracle/Makefile
-// (target _ref/shim_example) against the reference's own headers, with the correctly rounded
-// libm of oracle/ref_crlibm.hpp in the reference's CPU transport; run by tests/test_shim.py.
+// (target _ref/shim_example) against the reference's own headers and linked with the
+// correctly rounded libm of oracle/crlibm_libm.cpp for the reference's CPU transport; run by
+// tests/test_shim.py.
 //
 // Every call site below is the reference's `run_events(engine, n, generate, options)` with
 // its namespace changed to cmpmc_b200. Checks:
@@ -14,7 +15,6 @@
 //      within 5 standard errors of the CPU run, and the ledger closed to 1e-6;
 //   4. the cached context is reused for the same engine and rebuilt after a detector change.
 // Exit status: 0 all checks pass, 1 a check failed (the reason is printed), 3 no device.
-#include "../oracle/ref_crlibm.hpp"
 #include "cmpmc/cmpmc.hpp"
 #include "cmpmc_b200/run_events_gpu.hpp"
 
@@ -22,6 +22,10 @@
 #include <cstdio>
 #include <functional>
 #include <string>
+
+// oracle/crlibm_libm.cpp (linked in): the reference's transport runs against a correctly
+// rounded libm while the calling thread's flag is on
+extern "C" void cmpmc_oracle_set_crlibm(int on);
 
 namespace {
 
@@ -41,12 +45,12 @@ bool rel_close(double a, double b, double rel) { return std::fabs(a - b) <= rel 
 template <class Gen>
 cmpmc::RunResult cpu_run(const cmpmc::SimulationEngine& engine, uint64_t n, Gen&& gen, const cmpmc::RunOptions& opt) {
     auto wrapped = [&](cmpmc::EventInput& in) {
-        cmpmc_oracle::g_crlibm = false;
+        cmpmc_oracle_set_crlibm(0);
         gen(in);
-        cmpmc_oracle::g_crlibm = true;
+        cmpmc_oracle_set_crlibm(1);
     };
     cmpmc::RunResult r = cmpmc::run_events(engine, n, wrapped, opt);
-    cmpmc_oracle::g_crlibm = false;
+    cmpmc_oracle_set_crlibm(0);
     return r;
 }
 
