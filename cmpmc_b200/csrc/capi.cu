@@ -278,7 +278,18 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
     // wavefront split (the default batched form): the phonon phases end a track at film
     // entry; film phases run the cascades and queue the re-emissions, as in the phonon-only
     // split form, until the round's phonons are done
-    const bool split = d->form == CMPMC_FORM_BATCHED_FP32;
+    // warp pool (the default batched form): each phonon phase (the generator's phonons, then
+    // each round's queued Luke and released phonons) is one persistent pool launch with its
+    // film cascades inside; the host-driven rounds (configure_pool 0) split them instead
+    const bool pool = d->form == CMPMC_FORM_BATCHED_FP32 && ctx->pool;
+    const bool split = d->form == CMPMC_FORM_BATCHED_FP32 && !pool;
+    int bps_pool = ctx->bps;
+    if (pool && !bps_pool) {
+        CK(pool_fp32_occupancy(128, &bps_pool), "occupancy");
+        bps_pool = std::max(bps_pool, 1);
+    }
+    const uint64_t grid_pool = static_cast<uint64_t>(ctx->num_sms) * std::max(bps_pool, 1);
+    if (pool) CK(ctx->pool_film.ensure(grid_pool * 4 * pool_film_bytes_per_warp()), "alloc film buffers");
     int bps_f = ctx->bps;
     if (split && !bps_f) {
         CK(film_fp32_occupancy(tpb, &bps_f), "occupancy");
@@ -356,6 +367,20 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
                 ++launches;
             }
         };
+        if (pool) CK(ctx->pool_ring.ensure(grid_pool * 4 * ctx->pool_ring_cap * pool_ring_entry_bytes()),
+                     "alloc warp rings");
+        // one pool launch over `units` units: the primaries (queue == nullptr) or a queue
+        auto pool_phase = [&](uint64_t units, const QPhonon* queue) -> int {
+            CK(cudaMemsetAsync(&dc->next_work, 0, sizeof(unsigned long long), s), "memset work counter");
+            a.n_events = units;
+            const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(grid_pool, (units + 127) / 128));
+            CK(launch_pool_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->pool_ring.p, ctx->pool_ring_cap,
+                                ctx->pool_film.p, ctx->unit_event.as<uint32_t>(), queue, ctx->stage_tables,
+                                static_cast<int>(grid), 128, s),
+               "pool launch");
+            ++launches;
+            return CMPMC_OK;
+        };
         CK(ctx->stack.ensure(slots * stack_cap * batched_stack_entry_bytes()), "alloc phonon stacks");
         CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
         CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
@@ -370,7 +395,10 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
         CK(cudaMemsetAsync(ctx->ccounters.p, 0, sizeof(ChargeCounters), s), "memset counters");
         CK(cudaEventRecord(ctx->e_k0, s), "event");
         // phase 0: the generator's phonons
-        if (n_ph) {
+        if (n_ph && pool) {
+            const int st = pool_phase(n_ph, nullptr);
+            if (st != CMPMC_OK) return st;
+        } else if (n_ph) {
             a.n_events = n_ph;
             CK(launch_batched_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->unit_event.as<uint32_t>(),
                                    static_cast<int>(std::min<uint64_t>(grid_ph, (n_ph + tpb - 1) / tpb)), tpb, s),
@@ -413,7 +441,10 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
                 hcc = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
             }
             const uint64_t n_q = std::min<uint64_t>(hcc.q_tail, q_cap);
-            if (n_q && !split_over) {
+            if (n_q && pool) {
+                const int st = pool_phase(n_q, ca.queue);
+                if (st != CMPMC_OK) return st;
+            } else if (n_q && !split_over) {
                 CK(cudaMemsetAsync(&dc->next_work, 0, sizeof(unsigned long long), s), "memset work counter");
                 a.n_events = n_q;
                 if (split) {
@@ -448,8 +479,10 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
         const bool stack_over = (hc.err & kErrPhononStack) != 0;
         const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
         const bool queue_over = (hc.err & kErrRelease) != 0;  // released phonons did not fit the queue
-        split_over = split_over || (hc.err & (kErrQueue | kErrFilmQueue)) != 0;
-        if (!stack_over && !hits_over && !queue_over && !split_over) break;
+        const bool ring_over = pool && (hc.err & kErrQueue) != 0;  // a warp's ring of pending phonons
+        split_over = split_over || (!pool && (hc.err & (kErrQueue | kErrFilmQueue)) != 0);
+        if (!stack_over && !hits_over && !queue_over && !split_over && !ring_over) break;
+        if (ring_over) ctx->pool_ring_cap = std::min<uint32_t>(ctx->pool_ring_cap * 4, 1u << 20);
         if (attempt >= 8) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack, hit or queue overflow persists");
         if (stack_over) stack_cap = std::min<uint32_t>(stack_cap * 8, 1u << 20);
         if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
@@ -702,7 +735,8 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
         CK(cudaEventRecord(ctx->e_k0, s), "event");
         if (n_ph) {
             CK(launch_pool_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->pool_ring.p, ctx->pool_ring_cap, ctx->pool_film.p,
-                                ctx->unit_event.as<uint32_t>(), ctx->stage_tables, static_cast<int>(grid), tpb, s),
+                                ctx->unit_event.as<uint32_t>(), nullptr, ctx->stage_tables, static_cast<int>(grid),
+                                tpb, s),
                "pool launch");
             ++launches;
         }

@@ -301,9 +301,11 @@ cudaError_t film_fp32_occupancy(int block, int* blocks_per_sm);
 // warp pool form of the batched phonon transport (one persistent launch): `ring` holds
 // ring_cap pending-phonon entries (pool_ring_entry_bytes) per warp, `film`
 // pool_film_bytes_per_warp bytes per warp; grid * block / 32 warps
+// (queue != nullptr: the units are the a.n_events entries of a phonon queue instead of the
+// primary records)
 cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
-                             uint32_t ring_cap, void* film, const uint32_t* unit_event, int stage_tables, int grid,
-                             int block, cudaStream_t s);
+                             uint32_t ring_cap, void* film, const uint32_t* unit_event, const QPhonon* queue,
+                             int stage_tables, int grid, int block, cudaStream_t s);
 cudaError_t pool_fp32_occupancy(int block, int* blocks_per_sm);
 size_t pool_ring_entry_bytes();
 size_t pool_film_bytes_per_warp();

@@ -1139,6 +1139,7 @@ struct PoolArgs {
     FilmRec* film;          // [warps][kPoolFilmCap]
     uint32_t ring_cap;      // a power of two
     const uint32_t* unit_event;
+    const QPhonon* queue;   // queue units (kQueue kernels)
     int stage_tables;       // decay CDF tables read from a shared-memory copy staged by TMA
 };
 
@@ -1252,7 +1253,9 @@ __device__ __noinline__ uint32_t pool_film_step(const FLat* Lp, const Detector* 
     return r_tail + total;
 }
 
-template <bool kSur, int kKin = 0>
+// kQueue: the units are the entries of a phonon queue (the Luke phonons of the charge form,
+// p.queue; reserved-but-empty slots are skipped) instead of the batch's primary records
+template <bool kSur, int kKin = 0, bool kQueue = false>
 __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FLat L,
                                                       const __grid_constant__ Detector D,
                                                       const __grid_constant__ RunArgs a,
@@ -1322,7 +1325,27 @@ __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FL
                 base = __shfl_sync(full, base, 0);
                 if (base + need >= a.n_events) input_left = false;
                 const uint64_t unit = base + static_cast<uint64_t>(rank - static_cast<int>(from_ring));
-                if (!live && rank >= static_cast<int>(from_ring) && unit < a.n_events) {
+                if constexpr (kQueue) {
+                    if (!live && rank >= static_cast<int>(from_ring) && unit < a.n_events) {
+                        const QPhonon q = p.queue[unit];
+                        if (q.ev != kQEmpty) {
+                            ev_cur = q.ev;
+                            g.seed(q.key);
+                            trk.pos = f3(q.px, q.py, q.pz);
+                            trk.k = f3(q.kx, q.ky, q.kz);
+                            trk.mode = static_cast<int>(q.mode);
+                            const FKin kin = fmapk<kKin>(L, trk.mode, trk.k);
+                            trk.vg = kin.dir;
+                            trk.vmag = kin.mag;
+                            trk.E = q.E;
+                            trk.t = q.t;
+                            trk.w = q.w;
+                            trk.bounces = q.pad;
+                            st.clear();
+                            live = true;
+                        }
+                    }
+                } else if (!live && rank >= static_cast<int>(from_ring) && unit < a.n_events) {
                     const uint32_t ev = p.unit_event[unit];
                     ev_cur = ev;
                     const uint64_t j = unit - a.ph_off[ev];
@@ -1479,18 +1502,25 @@ cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detect
 }
 
 cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
-                             uint32_t ring_cap, void* film, const uint32_t* unit_event, int stage_tables, int grid,
-                             int block, cudaStream_t s) {
+                             uint32_t ring_cap, void* film, const uint32_t* unit_event, const QPhonon* queue,
+                             int stage_tables, int grid, int block, cudaStream_t s) {
     const FLat f = make_flat(L, cdf_f, D);
     PoolArgs p;
     p.ring = static_cast<PoolPh*>(ring);
     p.film = static_cast<FilmRec*>(film);
     p.ring_cap = ring_cap;
     p.unit_event = unit_event;
+    p.queue = queue;
     p.stage_tables = stage_tables;
-    if (L.kin_mode != kKinOctahedral) k_pool_fp32<false, 1><<<grid, block, 0, s>>>(f, D, a, p);
-    else if (a.surrogate) k_pool_fp32<true><<<grid, block, 0, s>>>(f, D, a, p);
-    else k_pool_fp32<false><<<grid, block, 0, s>>>(f, D, a, p);
+    if (queue) {
+        if (L.kin_mode != kKinOctahedral) k_pool_fp32<false, 1, true><<<grid, block, 0, s>>>(f, D, a, p);
+        else if (a.surrogate) k_pool_fp32<true, 0, true><<<grid, block, 0, s>>>(f, D, a, p);
+        else k_pool_fp32<false, 0, true><<<grid, block, 0, s>>>(f, D, a, p);
+    } else {
+        if (L.kin_mode != kKinOctahedral) k_pool_fp32<false, 1><<<grid, block, 0, s>>>(f, D, a, p);
+        else if (a.surrogate) k_pool_fp32<true><<<grid, block, 0, s>>>(f, D, a, p);
+        else k_pool_fp32<false><<<grid, block, 0, s>>>(f, D, a, p);
+    }
     return cudaGetLastError();
 }
 
