@@ -5,9 +5,10 @@ tracks per GPU, energies log-uniform on [1, 30] meV, modes L/ST/FT 0.10/0.36/0.5
 uniform in the Ge cylinder (R 3.81 cm, half height 1.27 cm), isotropic directions, seed 7;
 default Ge lattice and detector (Al Kaplan films on both faces). One step = one run_events
 pass over the whole batch in the batched FP32 form (FP32 geometry, FP64 energy ledger and
-time of flight; the warp pool: one persistent launch in which every warp refills its lanes
-from its own ring of pending phonons and the batch's primaries, and runs its film cascades
-32 at a time, until every track is absorbed or lost), hits kept. The launch shape comes
+time of flight; the SM-phase pool: one persistent launch, one block per SM alternating a
+transport phase, whose warps refill their lanes from the block's ring of pending phonons and
+the batch's primaries, and a film phase that runs the waiting film cascades, until every
+track is absorbed or lost), hits kept. The launch shape comes
 from the library's autotuner (results do not depend on it).
 
   value  primary phonon tracks / s, inputs resident on the device, device-timed (CUDA
@@ -75,8 +76,8 @@ def measured_peaks():
 
 def profile_traffic(form: str):
     """DRAM bytes per transport step of the batched kernels from the committed ncu summary."""
-    name = {"pool": "batched_fp32_pool_mixed_energy.json", "rounds": "batched_fp32_split_mixed_energy.json",
-            "inline": "batched_fp32_inline_mixed_energy.json"}[form]
+    name = {"sm_pool": "batched_fp32_sm_pool_mixed_energy.json", "warp_pool": "batched_fp32_warp_pool_mixed_energy.json",
+            "rounds": "batched_fp32_split_mixed_energy.json", "inline": "batched_fp32_inline_mixed_energy.json"}[form]
     try:
         with open(os.path.join(ROOT, "profiles", name)) as f:
             return float(json.load(f)["dram_bytes_per_step"])
@@ -257,7 +258,8 @@ def main() -> None:
     ap.add_argument("--form", default="batched_fp32", choices=["batched_fp32", "batched_fp32_inline"])
     ap.add_argument("--queue-capacity", type=int, default=0, help="phonon queue entries (0: library default)")
     ap.add_argument("--stack-capacity", type=int, default=0, help="tracks per device thread (0: library default)")
-    ap.add_argument("--rounds", action="store_true", help="host-driven film / transport rounds instead of the warp pool")
+    ap.add_argument("--launch", default="sm_pool", choices=["sm_pool", "warp_pool", "rounds"],
+                    help="launch form of the batched phonon transport")
     ap.add_argument("--no-matched", action="store_true", help="skip the matched-statistics check")
     ap.add_argument("--pub-events", type=int, default=100000, help="events of the published workload (0: skip)")
     args = ap.parse_args()
@@ -292,9 +294,8 @@ def main() -> None:
     if args.queue_capacity or args.stack_capacity:
         eng.configure(dev, stack_capacity=args.stack_capacity, queue_capacity=args.queue_capacity)
     form_id = _ffi.FORM_BATCHED_FP32 if args.form == "batched_fp32" else _ffi.FORM_BATCHED_FP32_INLINE
-    if args.rounds:
-        eng.configure_pool(False, device=dev)
-    launch_form = "inline" if args.form != "batched_fp32" else ("rounds" if args.rounds else "pool")
+    eng.configure_pool({"sm_pool": 1, "warp_pool": 2, "rounds": 0}[args.launch], device=dev)
+    launch_form = "inline" if args.form != "batched_fp32" else args.launch
 
     # device-resident inputs (torch owns the memory)
     def to_dev(a):
@@ -488,7 +489,8 @@ def main() -> None:
                      "peak_kind": peak_kind, "bytes_per_step": BYTES_PER_STEP,
                      "traffic": (tps * steps_per_launch if tps else None)},
         "gpu_launches": launches,
-        "launch": {"form": {"pool": "warp_pool", "rounds": "host_rounds", "inline": "inline"}[launch_form],
+        "launch": {"form": {"sm_pool": "sm_phase_pool", "warp_pool": "warp_pool", "rounds": "host_rounds",
+                            "inline": "inline"}[launch_form],
                    "graph": use_graph, "transport_launches_per_call": launches / args.steps,
                    "host_syncs_per_call": 1 if launch_form != "rounds" else None, "autotune": tune},
         "clocks": clocks.summary(),

@@ -972,11 +972,12 @@ class SimulationEngine:
         if queue_capacity:
             _check(self._lib.cmpmc_gpu_configure_queue(h, int(queue_capacity)), h)
 
-    def configure_pool(self, enable: bool = True, ring_capacity: int = 0, device: int = 0) -> None:
-        """Launch form of the batched phonon transport: the warp pool (one persistent launch,
-        the default) or the host-driven film / transport rounds (cmpmc_gpu_configure_pool)."""
+    def configure_pool(self, form=1, ring_capacity: int = 0, device: int = 0) -> None:
+        """Launch form of the batched phonon transport (cmpmc_gpu_configure_pool): 1 (or True)
+        the SM-phase pool, one persistent launch (the default); 2 the warp pool; 0 (or False)
+        the host-driven film / transport rounds."""
         h = self.context(device)
-        _check(self._lib.cmpmc_gpu_configure_pool(h, int(enable), int(ring_capacity)), h)
+        _check(self._lib.cmpmc_gpu_configure_pool(h, int(form), int(ring_capacity)), h)
 
     def configure_staging(self, enable: bool = True, device: int = 0) -> None:
         """Decay CDF tables staged in shared memory by a TMA bulk copy (default) or read from

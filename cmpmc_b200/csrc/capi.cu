@@ -108,9 +108,12 @@ struct cmpmc_gpu_ctx {
     DevBuf film_a, queue_b;                             // wavefront split: film entries, second phonon queue
     uint64_t film_cap = 1ull << 22;                     // film entries per phase (64 B each)
     uint32_t phase_steps = 0;                           // steps a track takes per transport phase (0: any)
-    int pool = 1;                                       // batched phonon form: 1 warp pool, 0 host-driven rounds
-    int stage_tables = 1;                               // pool form: decay CDF tables staged in shared memory
-    uint32_t pool_ring_cap = 1024;                      // pending phonons per warp in the pool form
+    int pool = 1;                                       // batched phonon form: 1 SM-phase pool, 2 warp pool,
+                                                        // 0 host-driven rounds
+    int stage_tables = 1;                               // pool forms: decay CDF tables staged in shared memory
+    uint32_t pool_ring_cap = 1024;                      // pending phonons per warp (warp pool)
+    uint32_t sm_ring_cap = 1u << 15;                    // pending phonons per block (SM-phase pool)
+    uint32_t sm_film_cap = 8192;                        // film records per block and phase (SM-phase pool)
     DevBuf pool_ring, pool_film;                        // warp pool: per-warp rings and film buffers
     uint64_t queue_cap = 1ull << 24;                    // Luke-phonon queue entries (64 B each)
     // CUDA-graph replay of the batched phonon call (cmpmc_gpu_configure_graph)
@@ -197,6 +200,54 @@ int ensure_surrogate(cmpmc_gpu_ctx* ctx) {
     return CMPMC_OK;
 }
 
+// ---- the persistent pool launches (SM-phase pool or warp pool) ----------------------
+// grid of a pool launch over `units` units: one 768-thread block per SM (SM-phase pool), or
+// the occupancy's 128-thread blocks (warp pool), never more than the units can start
+int pool_grid(cmpmc_gpu_ctx* ctx, uint64_t units, uint64_t* grid) {
+    if (ctx->pool == 1) {
+        const uint64_t per = static_cast<uint64_t>(sm_pool_threads());
+        *grid = std::max<uint64_t>(1, std::min<uint64_t>(ctx->num_sms, (units + per - 1) / per));
+        return CMPMC_OK;
+    }
+    int bps = ctx->bps;
+    if (!bps) {
+        CK(pool_fp32_occupancy(128, &bps), "occupancy");
+        bps = std::max(bps, 1);
+    }
+    *grid = std::max<uint64_t>(1, std::min<uint64_t>(static_cast<uint64_t>(ctx->num_sms) * bps, (units + 127) / 128));
+    return CMPMC_OK;
+}
+
+// ring and film buffers for launches of up to `grid` blocks
+int ensure_pool_buffers(cmpmc_gpu_ctx* ctx, uint64_t grid) {
+    if (ctx->pool == 1) {
+        CK(ctx->pool_ring.ensure(grid * ctx->sm_ring_cap * pool_ring_entry_bytes()), "alloc block rings");
+        CK(ctx->pool_film.ensure(grid * ctx->sm_film_cap * sizeof(FilmRec)), "alloc film buffers");
+    } else {
+        CK(ctx->pool_ring.ensure(grid * 4 * ctx->pool_ring_cap * pool_ring_entry_bytes()), "alloc warp rings");
+        CK(ctx->pool_film.ensure(grid * 4 * pool_film_bytes_per_warp()), "alloc film buffers");
+    }
+    return CMPMC_OK;
+}
+
+cudaError_t launch_pool(cmpmc_gpu_ctx* ctx, const RunArgs& a, uint64_t grid, const QPhonon* queue, cudaStream_t s) {
+    const uint32_t* ue = ctx->unit_event.as<uint32_t>();
+    if (ctx->pool == 1)
+        return launch_sm_pool_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->pool_ring.p, ctx->sm_ring_cap, ctx->pool_film.p,
+                                   ctx->sm_film_cap, ue, queue, ctx->stage_tables, static_cast<int>(grid), s);
+    return launch_pool_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->pool_ring.p, ctx->pool_ring_cap, ctx->pool_film.p, ue,
+                            queue, ctx->stage_tables, static_cast<int>(grid), 128, s);
+}
+
+// after an overflow of a pool's ring or film buffer: more room for the rerun
+void grow_pool(cmpmc_gpu_ctx* ctx, unsigned err) {
+    if (err & kErrQueue) {
+        if (ctx->pool == 1) ctx->sm_ring_cap = std::min<uint32_t>(ctx->sm_ring_cap * 4, 1u << 24);
+        else ctx->pool_ring_cap = std::min<uint32_t>(ctx->pool_ring_cap * 4, 1u << 20);
+    }
+    if ((err & kErrFilmQueue) && ctx->pool == 1) ctx->sm_film_cap = std::min<uint32_t>(ctx->sm_film_cap * 2, 1u << 20);
+}
+
 // Device counters of the batched charge form (reset per phase except next_carrier)
 struct ChargeCounters {
     unsigned long long q_tail, resume_next, n_resume_out, next_carrier, rel_tail;
@@ -281,15 +332,13 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
     // warp pool (the default batched form): each phonon phase (the generator's phonons, then
     // each round's queued Luke and released phonons) is one persistent pool launch with its
     // film cascades inside; the host-driven rounds (configure_pool 0) split them instead
-    const bool pool = d->form == CMPMC_FORM_BATCHED_FP32 && ctx->pool;
+    const bool pool = d->form == CMPMC_FORM_BATCHED_FP32 && ctx->pool != 0;
     const bool split = d->form == CMPMC_FORM_BATCHED_FP32 && !pool;
-    int bps_pool = ctx->bps;
-    if (pool && !bps_pool) {
-        CK(pool_fp32_occupancy(128, &bps_pool), "occupancy");
-        bps_pool = std::max(bps_pool, 1);
+    uint64_t grid_pool = 1;
+    if (pool) {
+        const int st = pool_grid(ctx, ~0ull >> 1, &grid_pool);
+        if (st != CMPMC_OK) return st;
     }
-    const uint64_t grid_pool = static_cast<uint64_t>(ctx->num_sms) * std::max(bps_pool, 1);
-    if (pool) CK(ctx->pool_film.ensure(grid_pool * 4 * pool_film_bytes_per_warp()), "alloc film buffers");
     int bps_f = ctx->bps;
     if (split && !bps_f) {
         CK(film_fp32_occupancy(tpb, &bps_f), "occupancy");
@@ -367,17 +416,18 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
                 ++launches;
             }
         };
-        if (pool) CK(ctx->pool_ring.ensure(grid_pool * 4 * ctx->pool_ring_cap * pool_ring_entry_bytes()),
-                     "alloc warp rings");
+        if (pool) {
+            const int st = ensure_pool_buffers(ctx, grid_pool);
+            if (st != CMPMC_OK) return st;
+        }
         // one pool launch over `units` units: the primaries (queue == nullptr) or a queue
         auto pool_phase = [&](uint64_t units, const QPhonon* queue) -> int {
             CK(cudaMemsetAsync(&dc->next_work, 0, sizeof(unsigned long long), s), "memset work counter");
             a.n_events = units;
-            const uint64_t grid = std::max<uint64_t>(1, std::min<uint64_t>(grid_pool, (units + 127) / 128));
-            CK(launch_pool_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->pool_ring.p, ctx->pool_ring_cap,
-                                ctx->pool_film.p, ctx->unit_event.as<uint32_t>(), queue, ctx->stage_tables,
-                                static_cast<int>(grid), 128, s),
-               "pool launch");
+            uint64_t grid = 1;
+            const int st = pool_grid(ctx, units, &grid);
+            if (st != CMPMC_OK) return st;
+            CK(launch_pool(ctx, a, std::min(grid, grid_pool), queue, s), "pool launch");
             ++launches;
             return CMPMC_OK;
         };
@@ -479,10 +529,10 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
         const bool stack_over = (hc.err & kErrPhononStack) != 0;
         const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
         const bool queue_over = (hc.err & kErrRelease) != 0;  // released phonons did not fit the queue
-        const bool ring_over = pool && (hc.err & kErrQueue) != 0;  // a warp's ring of pending phonons
+        const bool ring_over = pool && (hc.err & (kErrQueue | kErrFilmQueue)) != 0;  // a pool's ring or film buffer
         split_over = split_over || (!pool && (hc.err & (kErrQueue | kErrFilmQueue)) != 0);
         if (!stack_over && !hits_over && !queue_over && !split_over && !ring_over) break;
-        if (ring_over) ctx->pool_ring_cap = std::min<uint32_t>(ctx->pool_ring_cap * 4, 1u << 20);
+        if (ring_over) grow_pool(ctx, hc.err);
         if (attempt >= 8) return fail(ctx, CMPMC_ERR_CAPACITY, "device stack, hit or queue overflow persists");
         if (stack_over) stack_cap = std::min<uint32_t>(stack_cap * 8, 1u << 20);
         if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
@@ -685,16 +735,11 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
                      int& launches, Counters& hc, float& kms, uint64_t& n_hits, uint64_t*& ev_offsets,
                      cmpmc_sim_stats*& ev_stats) {
     cudaStream_t s = ctx->stream;
-    const int tpb = 128;  // the kernel's per-thread counters are laid out for 128-thread blocks
-    int bps = ctx->bps;
-    if (!bps) {
-        CK(pool_fp32_occupancy(tpb, &bps), "occupancy");
-        bps = std::max(bps, 1);
+    uint64_t grid = 1;
+    {
+        const int st = pool_grid(ctx, n_ph, &grid);
+        if (st != CMPMC_OK) return st;
     }
-    // no more warps than there are primaries to start them with
-    const uint64_t grid = std::max<uint64_t>(
-        1, std::min<uint64_t>(static_cast<uint64_t>(ctx->num_sms) * bps, (n_ph + tpb - 1) / tpb));
-    const uint64_t warps = grid * tpb / 32;
     CK(ctx->ev_stats2.ensure(std::max<uint64_t>(n, 1) * sizeof(cmpmc_sim_stats)), "alloc event stats");
     CK(ctx->ev_nhits.ensure(std::max<uint64_t>(n, 1) * 8), "alloc event hit counts");
     CK(ctx->ev_offsets.ensure((n + 1) * 8), "alloc event offsets");
@@ -703,7 +748,6 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
     CK(ctx->total.ensure(sizeof(cmpmc_sim_stats)), "alloc totals");
     CK(ctx->partials.ensure(kReducePartials * sizeof(cmpmc_sim_stats)), "alloc partial totals");
     CK(ctx->h_counters.ensure(sizeof(Counters)), "alloc host counters");
-    CK(ctx->pool_film.ensure(warps * pool_film_bytes_per_warp()), "alloc film buffers");
     if (n_ph) {
         CK(ctx->unit_event.ensure(n_ph * 4), "alloc unit map");
         CK(launch_unit_event(a.ph_off, n, ctx->unit_event.as<uint32_t>(), s), "unit map");
@@ -723,7 +767,10 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
     if (!hit_cap) hit_cap = std::max<uint64_t>(1u << 20, n_ph * 32);
     for (int attempt = 0;; ++attempt) {
         if (!d->keep_hits) hit_cap = 1;
-        CK(ctx->pool_ring.ensure(warps * ctx->pool_ring_cap * pool_ring_entry_bytes()), "alloc warp rings");
+        {
+            const int st = ensure_pool_buffers(ctx, grid);
+            if (st != CMPMC_OK) return st;
+        }
         CK(ctx->hit_stage.ensure(hit_cap * sizeof(cmpmc_sensor_hit)), "alloc hit staging");
         CK(ctx->hit_key.ensure(hit_cap * 8), "alloc hit keys");
         a.hit_stage = ctx->hit_stage.as<cmpmc_sensor_hit>();
@@ -734,10 +781,7 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
         CK(cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s), "memset counters");
         CK(cudaEventRecord(ctx->e_k0, s), "event");
         if (n_ph) {
-            CK(launch_pool_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->pool_ring.p, ctx->pool_ring_cap, ctx->pool_film.p,
-                                ctx->unit_event.as<uint32_t>(), nullptr, ctx->stage_tables, static_cast<int>(grid),
-                                tpb, s),
-               "pool launch");
+            CK(launch_pool(ctx, a, grid, nullptr, s), "pool launch");
             ++launches;
         }
         CK(cudaEventRecord(ctx->e_k1, s), "event");
@@ -746,11 +790,11 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
         CK(cudaStreamSynchronize(s), "transport kernel");
         hc = *ctx->h_counters.as<Counters>();
         CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
-        const bool ring_over = (hc.err & kErrQueue) != 0;
+        const bool ring_over = (hc.err & (kErrQueue | kErrFilmQueue)) != 0;
         const bool hits_over = d->keep_hits && hc.hit_count > hit_cap;
         if (!ring_over && !hits_over) break;
-        if (attempt >= 6) return fail(ctx, CMPMC_ERR_CAPACITY, "warp ring or hit buffer overflow persists");
-        if (ring_over) ctx->pool_ring_cap = std::min<uint32_t>(ctx->pool_ring_cap * 4, 1u << 20);
+        if (attempt >= 6) return fail(ctx, CMPMC_ERR_CAPACITY, "pool ring or hit buffer overflow persists");
+        if (ring_over) grow_pool(ctx, hc.err);
         if (hits_over) hit_cap = hc.hit_count + hc.hit_count / 16 + 1024;
         hc.err = 0;
     }
@@ -1056,12 +1100,15 @@ int cmpmc_gpu_configure_staging(cmpmc_gpu_ctx* ctx, int enable) {
     return CMPMC_OK;
 }
 
-int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int enable, uint32_t ring_capacity) {
-    if (!ctx || enable < 0 || enable > 1) return CMPMC_ERR_INVALID;
+int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int form, uint32_t ring_capacity) {
+    if (!ctx || form < 0 || form > 2) return CMPMC_ERR_INVALID;
     if (ring_capacity != 0 && (ring_capacity < 64 || (ring_capacity & (ring_capacity - 1)) != 0))
         return fail(ctx, CMPMC_ERR_INVALID, "ring capacity: a power of two, at least 64");
-    ctx->pool = enable;
-    if (ring_capacity) ctx->pool_ring_cap = ring_capacity;
+    ctx->pool = form;
+    if (ring_capacity) {
+        if (form == 1) ctx->sm_ring_cap = std::max<uint32_t>(ring_capacity, 2 * sm_pool_threads());
+        else ctx->pool_ring_cap = ring_capacity;
+    }
     return CMPMC_OK;
 }
 

@@ -307,6 +307,13 @@ cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detecto
                              uint32_t ring_cap, void* film, const uint32_t* unit_event, const QPhonon* queue,
                              int stage_tables, int grid, int block, cudaStream_t s);
 cudaError_t pool_fp32_occupancy(int block, int* blocks_per_sm);
+// SM-phase pool (one block of sm_pool_threads() threads per SM alternating transport and
+// film phases): `ring` holds ring_cap entries (pool_ring_entry_bytes) per block, `film`
+// film_cap film records (64 B) per block
+cudaError_t launch_sm_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
+                                uint32_t ring_cap, void* film, uint32_t film_cap, const uint32_t* unit_event,
+                                const QPhonon* queue, int stage_tables, int grid, cudaStream_t s);
+int sm_pool_threads();
 size_t pool_ring_entry_bytes();
 size_t pool_film_bytes_per_warp();
 cudaError_t launch_carrier_event(const uint64_t* ch_off, uint64_t n_events, uint32_t* carrier_event,

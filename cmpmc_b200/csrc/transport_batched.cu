@@ -122,10 +122,11 @@ __device__ __forceinline__ void pop_track(const EntryOf<kAdj>* stk, uint32_t& n,
 // the track state instead of spilling it.
 constexpr int kMaxBlock = 128;  // every kernel running the step loop has __launch_bounds__(128)
 enum { kCSteps = 0, kCIso, kCPoly, kCTT, kCLT, kCRefl, kCDown, kCHits, kCKilled, kNCnt };
-struct UStats {
-    uint32_t* c;  // &counters[0][threadIdx.x]
-    double* f;    // &ledger[0][threadIdx.x]: deposited, then escaped or killed
-    __device__ __forceinline__ uint32_t& at(int i) const { return c[i * kMaxBlock]; }
+template <int kStride>
+struct UStatsT {
+    uint32_t* c;  // &counters[0][thread]: counter i at c[i * kStride]
+    double* f;    // &ledger[0][thread]: deposited, then escaped or killed
+    __device__ __forceinline__ uint32_t& at(int i) const { return c[i * kStride]; }
     __device__ __forceinline__ uint32_t& steps() const { return at(kCSteps); }
     __device__ __forceinline__ uint32_t& iso() const { return at(kCIso); }
     __device__ __forceinline__ uint32_t& poly() const { return at(kCPoly); }
@@ -136,7 +137,7 @@ struct UStats {
     __device__ __forceinline__ uint32_t& hits() const { return at(kCHits); }
     __device__ __forceinline__ uint32_t& killed() const { return at(kCKilled); }
     __device__ __forceinline__ double& dep() const { return f[0]; }
-    __device__ __forceinline__ double& esc() const { return f[kMaxBlock]; }
+    __device__ __forceinline__ double& esc() const { return f[kStride]; }
     __device__ __forceinline__ void clear() const {
 #pragma unroll
         for (int i = 0; i < kNCnt; ++i) at(i) = 0;
@@ -144,6 +145,7 @@ struct UStats {
         esc() = 0.0;
     }
 };
+using UStats = UStatsT<kMaxBlock>;
 
 // Kaplan cascade out of line: its FP64 registers stay out of the step loop
 __device__ __noinline__ double kaplan_call(const Film* f, double E, double* refl, int* n_refl, double* work,
@@ -276,7 +278,8 @@ __device__ __forceinline__ void add_u64(unsigned long long* p, uint32_t v) {
 __device__ __forceinline__ void add_f64(double* p, double v) {
     if (v != 0.0) atomicAdd(p, v);
 }
-__device__ __noinline__ void sink_unit(const RunArgs* a, uint32_t ev, const UStats st) {
+template <class ST>
+__device__ __noinline__ void sink_unit(const RunArgs* a, uint32_t ev, const ST st) {
     cmpmc_sim_stats& o = a->ev_stats[ev];
     add_u64(reinterpret_cast<unsigned long long*>(&o.total_steps), st.steps());
     add_u64(reinterpret_cast<unsigned long long*>(&o.isotope_scatters), st.iso());
@@ -825,14 +828,25 @@ __device__ __forceinline__ bool stage_bulk(void* dst, const void* src, uint32_t 
                      : "memory");
     }
     __syncthreads();  // the barrier is initialised before anyone polls it
-    for (int i = 0; i < kStageSpins; ++i) {
+    auto landed = [b]() {
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
                      : "=r"(done)
                      : "r"(b)
                      : "memory");
-        if (done) return true;
-        __nanosleep(32);
+        return done != 0;
+    };
+    bool done = false;
+    for (int i = 0; i < kStageSpins && !done; ++i) {
+        done = landed();
+        if (!done) __nanosleep(32);
+    }
+    // the block agrees on the outcome; a copy that is late is still waited for (bounded)
+    // before the caller gives up, so no copy into this block's shared memory outlives it
+    if (!__syncthreads_or(!done)) return true;
+    for (int i = 0; i < kStageSpins && !done; ++i) {
+        done = landed();
+        if (!done) __nanosleep(32);
     }
     return false;
 }
@@ -902,8 +916,8 @@ __device__ __forceinline__ uint64_t draw_key(R128& g) {
 
 // anharmonic decay of an L phonon (engine.hpp:938-988), FP32 angles: the parent continues
 // in *tp, the daughter is written to *dp (it runs later on a substream of its own)
-template <int kKin>
-__device__ __noinline__ void pool_decay(const FLat* Lp, const float* cdf, FTrack* tp, FTrack* dp, const UStats* st,
+template <int kKin, class ST>
+__device__ __noinline__ void pool_decay(const FLat* Lp, const float* cdf, FTrack* tp, FTrack* dp, const ST* st,
                                         R128* gp) {
     const FLat& L = *Lp;
     FTrack& trk = *tp;
@@ -958,21 +972,30 @@ __device__ __noinline__ void pool_decay(const FLat* Lp, const float* cdf, FTrack
 
 enum { kStepOn = 0, kStepEnd = 1, kStepFilm = 2 };
 
-// One transport step of a live track (the physics of batched_loop's step): returns whether
-// the track goes on, ended (counters and ledger updated), or entered an active film (*fr
-// filled, the film kernel's input). A daughter made in the step is written to *dq
-// (*has_d set) with a substream key drawn from the track's stream.
 // A step's single output record (a film entry or a daughter), staged in shared memory so
 // that it holds no registers across the step; the warp copies it to its buffer afterwards.
 union PoolOut {
     FilmRec film;
     PoolPh ph;
 };
+// output of the warp pool's step: the record goes to the thread's staging slot
+struct WarpSink {
+    PoolOut* o;
+    bool has_d;
+    __device__ __forceinline__ void film(const FilmRec& r) { o->film = r; }
+    __device__ __forceinline__ void daughter(const PoolPh& q) {
+        o->ph = q;
+        has_d = true;
+    }
+};
 
-template <int kKin>
+// One transport step of a live track (the physics of batched_loop's step): returns whether
+// the track goes on, ended (counters and ledger updated), or entered an active film (the
+// film record handed to out.film). A daughter made in the step is handed to out.daughter
+// with a substream key drawn from the track's stream.
+template <int kKin, class ST, class Sink>
 __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const Detector& D, FTrack& trk, R128& g,
-                                         const UStats& st, uint32_t ev, PoolOut& out, bool& has_d) {
-    has_d = false;
+                                         const ST& st, uint32_t ev, Sink& out) {
     if (trk.E < D.min_phonon_eV || trk.bounces >= D.max_bounces) {
         ++st.killed();
         st.esc() += trk.E * trk.w;
@@ -1009,8 +1032,7 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
             pool_decay<kKin>(&L, cdf, &t_c, &d_c, &st, &g_c);
             trk = t_c;
             g = g_c;
-            out.ph = pool_entry(d_c, draw_key(g), ev);
-            has_d = true;
+            out.daughter(pool_entry(d_c, draw_key(g), ev));
         } else {
             if (u_proc < r_down + r_iso) ++st.iso();
             else ++st.poly();
@@ -1048,7 +1070,7 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
             fr.surf = static_cast<uint8_t>(bh.surf);
             fr.mode = static_cast<uint8_t>(trk.mode);
             fr.pad0 = fr.pad1 = 0;
-            out.film = fr;
+            out.film(fr);
             return kStepFilm;
         }
         if (g.u() > static_cast<float>(s.prob_refl)) {
@@ -1085,8 +1107,7 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
             dtr.w = trk.w;
             dtr.bounces = 0;
             dtr.mode = m2;
-            out.ph = pool_entry(dtr, draw_key(g), ev);
-            has_d = true;
+            out.daughter(pool_entry(dtr, draw_key(g), ev));
             trk.E = static_cast<double>(x) * trk.E;
             trk.mode = m1;
             sample = 1;
@@ -1383,14 +1404,15 @@ __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FL
         }
         // 2. one step of every live track
         int outcome = kStepOn;
-        bool has_d = false;
+        WarpSink sink{&my_out, false};
         if (live) {
-            outcome = pool_step<kKin>(L, cdf, D, trk, g, st, ev_cur, my_out, has_d);
+            outcome = pool_step<kKin>(L, cdf, D, trk, g, st, ev_cur, sink);
             if (outcome != kStepOn) {
                 sink_unit(&a, ev_cur, st);
                 live = false;
             }
         }
+        const bool has_d = sink.has_d;
         // 3. regroup: daughters to the ring, film entries to the film buffer
         const unsigned d_mask = __ballot_sync(full, has_d);
         if (d_mask) {
@@ -1416,6 +1438,328 @@ __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FL
         }
     }
     if (err && lane == 0) atomicOr(a.err, err);
+}
+
+// ---- SM-phase pool ----------------------------------------------------------------------
+// The warp pool runs a warp's film cascades among the other warps' transport steps, and the
+// two code paths then compete for the SM's instruction cache: measured, the transport
+// machinery alone steps 2.4e10 times a second, the mix half as fast as separate kernels.
+// Here one block of 768 threads (24 warps) owns an SM and alternates two phases, so the SM
+// runs one code path at a time:
+//   transport phase: every warp steps its lanes, refilling them from the block's ring of
+//     pending phonons (entries published at the last phase boundary) and then from the
+//     batch's primaries; a step that reaches an active film appends its record to the
+//     block's film buffer, a daughter goes to the ring (both reserved by shared-memory
+//     atomics, consumable after the boundary). A warp leaves the phase when the film buffer
+//     holds film_trigger records or when it has no work left;
+//   film phase: every thread takes film records from the buffer (a shared-memory counter)
+//     and runs their cascades, hits reserved once per coalesced group, re-emissions appended
+//     to the ring.
+// The block ends when a boundary finds no live lane, no published phonon and no primary
+// left. Nothing waits on another block; every wait is a block barrier that all threads
+// reach (each phase ends by itself).
+constexpr int kSmThreads = 768;
+constexpr int kSmWarps = kSmThreads / 32;
+
+struct SmPoolArgs {
+    PoolPh* ring;            // [blocks][ring_cap]
+    FilmRec* film;           // [blocks][film_cap]
+    uint32_t ring_cap;       // a power of two
+    uint32_t film_cap;       // film records per block and phase
+    uint32_t film_trigger;   // records that end a transport phase (<= film_cap - kSmThreads)
+    const uint32_t* unit_event;
+    const QPhonon* queue;    // queue units (kQueue kernels)
+    int stage_tables;
+};
+
+struct SmShared {
+    uint32_t r_head, r_tail, r_pub;  // ring: consumable [r_head, r_pub), appended at r_tail
+    uint32_t f_tail, f_next;         // film buffer: records [0, f_tail), next to run
+    uint32_t input_left;             // the batch still has primaries
+    uint32_t n_dry;                  // warps of this phase that ran out of work
+};
+
+// output of the SM pool's step: reserved in the block's buffers by shared-memory atomics
+struct SmSink {
+    SmShared* sh;
+    FilmRec* fbuf;
+    PoolPh* ring;
+    uint32_t film_cap, ring_mask, r_floor;
+    unsigned* err;
+    __device__ __forceinline__ void film_rec(const FilmRec& r) {
+        const uint32_t i = atomicAdd(&sh->f_tail, 1u);
+        if (i < film_cap) fbuf[i] = r;
+        else *err |= kErrFilmQueue;
+    }
+    __device__ __forceinline__ void daughter(const PoolPh& q) {
+        const uint32_t i = atomicAdd(&sh->r_tail, 1u);
+        if (i + 1u - r_floor <= ring_mask + 1u) ring[i & ring_mask] = q;
+        else *err |= kErrQueue;
+    }
+    __device__ __forceinline__ void film(const FilmRec& r) { film_rec(r); }
+};
+
+// the film phase of one thread: records from the block's buffer until it is drained
+template <bool kSur, int kKin>
+__device__ __noinline__ void sm_film_phase(const FLat* Lp, const Detector* Dp, const RunArgs* ap,
+                                           const FilmRec* film, uint32_t n_film, SmShared* sh, PoolPh* ring,
+                                           uint32_t ring_mask, uint32_t r_floor, unsigned* err) {
+    const FLat& L = *Lp;
+    const Detector& D = *Dp;
+    const RunArgs& a = *ap;
+    double refl_buf[kKaplanCap];
+    double kwork[4 * kKaplanCap];
+    for (;;) {
+        const uint32_t i = atomicAdd(&sh->f_next, 1u);
+        if (i >= n_film) break;
+        const FilmRec r = film[i];
+        const Surface& s = D.surf[r.surf];
+        R128 g;
+        int n_refl = 0;
+        double edep;
+        {
+            R128 g_c;
+            g_c.seed(r.key);
+            if constexpr (kSur) {
+                edep = s.lut_abs ? surrogate_call(&s, r.E, refl_buf, &n_refl, kwork, &g_c)
+                                 : kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
+            } else {
+                edep = kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
+            }
+            g = g_c;
+        }
+        cmpmc_sim_stats& o = a.ev_stats[r.ev];
+        if (edep > 0.0) {
+            const double wedep = edep * static_cast<double>(r.w);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&o.sensor_hits), 1ull);
+            atomicAdd(&o.total_deposited_eV, wedep);
+            if (a.keep_hits) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(a.ev_nhits + r.ev), 1ull);
+                // one reservation for the threads of the warp that hit together
+                const unsigned grp = __activemask();
+                const int leader = __ffs(grp) - 1;
+                const int lane = threadIdx.x & 31;
+                unsigned long long base = 0;
+                if (lane == leader) base = atomicAdd(a.hit_count, static_cast<unsigned long long>(__popc(grp)));
+                base = __shfl_sync(grp, base, leader);
+                const unsigned long long idx = base + __popc(grp & lanemask_lt());
+                if (idx < a.hit_cap) {
+                    cmpmc_sensor_hit h;
+                    h.pos[0] = r.px; h.pos[1] = r.py; h.pos[2] = r.pz;
+                    h.time = r.t;
+                    h.edep = wedep;
+                    h.incident_energy = r.E;
+                    h.surface_id = r.surf;
+                    h.excitation = 0;
+                    h.mode = r.mode;
+                    h._pad = 0;
+                    h.channel_id = r.ch_id;
+                    a.hit_stage[idx] = h;
+                    a.hit_key[idx] = r.ev;
+                }
+            }
+        }
+        double sum_refl = 0.0;
+        for (int j = 0; j < n_refl; ++j) sum_refl += refl_buf[j];
+        const double esc = dmax(0.0, r.E - edep - sum_refl) * static_cast<double>(r.w);
+        if (esc != 0.0) atomicAdd(&o.escaped_or_killed_eV, esc);
+        if (n_refl == 0) continue;
+        const uint32_t base = atomicAdd(&sh->r_tail, static_cast<uint32_t>(n_refl));
+        if (base + static_cast<uint32_t>(n_refl) - r_floor > ring_mask + 1u) {
+            *err |= kErrQueue;
+            continue;
+        }
+        F3 n;
+        if (r.surf == 0) n = f3(0.0f, 0.0f, -1.0f);
+        else if (r.surf == 1) n = f3(0.0f, 0.0f, 1.0f);
+        else {
+            const float rr = sqrtf(r.px * r.px + r.py * r.py);
+            n = (rr > 1e-15f) ? f3(-r.px / rr, -r.py / rr, 0.0f) : f3(-1.0f, 0.0f, 0.0f);
+        }
+        FTrack t;
+        t.pos = f3(r.px, r.py, r.pz) + n * kNudge;
+        t.t = r.t;
+        t.w = r.w;
+        for (int j = 0; j < n_refl; ++j) {
+            t.mode = fdos(L, g.u());
+            FKin kin;
+            t.k = finward<kKin>(L, t.mode, n, g, kin);
+            t.vg = kin.dir;
+            t.vmag = kin.mag;
+            t.E = refl_buf[j];
+            t.bounces = (j == 0) ? r.bounces : 0u;
+            ring[(base + j) & ring_mask] =
+                pool_entry(t, mix64(r.key ^ (0x9e3779b97f4a7c15ULL * static_cast<uint64_t>(j + 1))), r.ev);
+        }
+    }
+}
+
+template <bool kSur, int kKin = 0, bool kQueue = false>
+__global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_constant__ FLat L,
+                                                                const __grid_constant__ Detector D,
+                                                                const __grid_constant__ RunArgs a,
+                                                                const __grid_constant__ SmPoolArgs p) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    __shared__ uint32_t s_cnt[kSmWarps][kNCnt][32];
+    __shared__ double s_led[kSmWarps][2][32];
+    __shared__ alignas(128) float s_cdf[2 * kNCdf];  // the decay CDF tables (L-LT, then TT)
+    __shared__ alignas(8) uint64_t s_bar;
+    __shared__ SmShared sh;
+    const UStatsT<32> st{&s_cnt[wid][0][lane], &s_led[wid][0][lane]};
+    PoolPh* ring = p.ring + static_cast<uint64_t>(blockIdx.x) * p.ring_cap;
+    FilmRec* film = p.film + static_cast<uint64_t>(blockIdx.x) * p.film_cap;
+    const uint32_t ring_mask = p.ring_cap - 1;
+    if (threadIdx.x == 0) {
+        sh.r_head = sh.r_tail = sh.r_pub = 0;
+        sh.f_tail = sh.f_next = 0;
+        sh.input_left = 1;
+        sh.n_dry = 0;
+    }
+    const float* cdf = L.cdf_lt;  // the two tables are contiguous in global memory
+    if (p.stage_tables) {  // (stage_bulk synchronizes the block)
+        if (!stage_bulk(s_cdf, L.cdf_lt, 2 * kNCdf * sizeof(float), &s_bar)) {
+            if (threadIdx.x == 0) atomicOr(a.err, kErrStage);
+            return;
+        }
+        cdf = s_cdf;
+    }
+    __syncthreads();
+    const uint64_t seed_key = mix64(a.seed ^ 0x5851f42d4c957f2dULL);
+    volatile SmShared* vsh = &sh;
+    FTrack trk;
+    R128 g;
+    uint32_t ev_cur = 0;
+    bool live = false;
+    unsigned err = 0;
+    for (;;) {
+        // ---- transport phase --------------------------------------------------------
+        const uint32_t r_floor = vsh->r_head;  // ring slots below it are free
+        const uint32_t r_pub = vsh->r_pub;
+        SmSink sink{&sh, film, ring, p.film_cap, ring_mask, r_floor, &err};
+        for (;;) {
+            uint32_t ft = 0, inp = 0, dry = 0;
+            if (lane == 0) {
+                ft = vsh->f_tail;
+                inp = vsh->input_left;
+                dry = vsh->n_dry;
+            }
+            ft = __shfl_sync(full, ft, 0);
+            inp = __shfl_sync(full, inp, 0);
+            dry = __shfl_sync(full, dry, 0);
+            // the film phase starts once enough records wait, or earlier when half the
+            // block has run dry and the waiting cascades would give it work
+            if (ft >= p.film_trigger || (ft > 0 && 2 * dry >= kSmWarps)) break;
+            const unsigned empty = __ballot_sync(full, !live);
+            if (empty) {
+                const int n_empty = __popc(empty);
+                const int rank = __popc(empty & lanemask_lt());
+                uint32_t base = 0, got = 0;
+                if (lane == 0 && vsh->r_head < r_pub) {
+                    base = atomicAdd(&sh.r_head, static_cast<uint32_t>(n_empty));
+                    got = (base < r_pub) ? min(static_cast<uint32_t>(n_empty), r_pub - base) : 0u;
+                }
+                base = __shfl_sync(full, base, 0);
+                got = __shfl_sync(full, got, 0);
+                if (!live && rank < static_cast<int>(got)) {
+                    const PoolPh q = ring[(base + rank) & ring_mask];
+                    trk.pos = f3(q.px, q.py, q.pz);
+                    trk.k = f3(q.kx, q.ky, q.kz);
+                    trk.vg = f3(q.vx, q.vy, q.vz);
+                    trk.vmag = q.vmag;
+                    trk.w = q.w;
+                    trk.bounces = q.bounces_mode >> 2;
+                    trk.mode = static_cast<int>(q.bounces_mode & 3u);
+                    trk.E = q.E;
+                    trk.t = q.t;
+                    g.seed(q.key);
+                    ev_cur = q.ev;
+                    st.clear();
+                    live = true;
+                }
+                const int need = n_empty - static_cast<int>(got);
+                if (need > 0 && inp) {
+                    unsigned long long ub = 0;
+                    if (lane == 0) {
+                        ub = atomicAdd(a.next_work, static_cast<unsigned long long>(need));
+                        if (ub + need >= a.n_events) vsh->input_left = 0;
+                    }
+                    ub = __shfl_sync(full, ub, 0);
+                    const uint64_t unit = ub + static_cast<uint64_t>(rank - static_cast<int>(got));
+                    if (!live && rank >= static_cast<int>(got) && unit < a.n_events) {
+                        if constexpr (kQueue) {
+                            const QPhonon q = p.queue[unit];
+                            if (q.ev != kQEmpty) {
+                                ev_cur = q.ev;
+                                g.seed(q.key);
+                                trk.pos = f3(q.px, q.py, q.pz);
+                                trk.k = f3(q.kx, q.ky, q.kz);
+                                trk.mode = static_cast<int>(q.mode);
+                                const FKin kin = fmapk<kKin>(L, trk.mode, trk.k);
+                                trk.vg = kin.dir;
+                                trk.vmag = kin.mag;
+                                trk.E = q.E;
+                                trk.t = q.t;
+                                trk.w = q.w;
+                                trk.bounces = q.pad;
+                                st.clear();
+                                live = true;
+                            }
+                        } else {
+                            const uint32_t ev = p.unit_event[unit];
+                            ev_cur = ev;
+                            const uint64_t j = unit - a.ph_off[ev];
+                            g.seed(seed_key ^ mix64(((a.first_event + ev) << 20) | j));
+                            const cmpmc_phonon_track& in = a.ph[unit];
+                            trk.pos = f3(static_cast<float>(in.pos[0]), static_cast<float>(in.pos[1]),
+                                         static_cast<float>(in.pos[2]));
+                            trk.k = f3(static_cast<float>(in.k_dir[0]), static_cast<float>(in.k_dir[1]),
+                                       static_cast<float>(in.k_dir[2]));
+                            trk.vg = f3(static_cast<float>(in.vg_dir[0]), static_cast<float>(in.vg_dir[1]),
+                                        static_cast<float>(in.vg_dir[2]));
+                            trk.vmag = static_cast<float>(in.vg_mag);
+                            trk.E = in.energy;
+                            trk.t = in.time;
+                            trk.w = static_cast<float>(in.weight);
+                            trk.bounces = in.bounces;
+                            trk.mode = in.mode;
+                            st.clear();
+                            live = true;
+                        }
+                    }
+                }
+            }
+            if (__ballot_sync(full, live) == 0) {  // nothing more until the boundary
+                if (lane == 0) atomicAdd(&sh.n_dry, 1u);
+                break;
+            }
+            if (live) {
+                const int outcome = pool_step<kKin>(L, cdf, D, trk, g, st, ev_cur, sink);
+                if (outcome != kStepOn) {
+                    sink_unit(&a, ev_cur, st);
+                    live = false;
+                }
+            }
+        }
+        __syncthreads();
+        // ---- film phase -------------------------------------------------------------
+        const uint32_t n_film = min(vsh->f_tail, p.film_cap);
+        if (n_film) sm_film_phase<kSur, kKin>(&L, &D, &a, film, n_film, &sh, ring, ring_mask, r_floor, &err);
+        __syncthreads();
+        // ---- boundary: publish what the phases appended ---------------------------------
+        if (threadIdx.x == 0) {
+            if (sh.r_head > sh.r_pub) sh.r_head = sh.r_pub;  // claims past the published entries were void
+            sh.r_pub = sh.r_tail;
+            sh.f_tail = 0;
+            sh.f_next = 0;
+            sh.n_dry = 0;
+        }
+        __syncthreads();
+        if (__syncthreads_or(err != 0)) break;  // an overflow: the call reruns with more room
+        if (!__syncthreads_or(live || vsh->r_pub != vsh->r_head || vsh->input_left != 0)) break;
+    }
+    if (err) atomicOr(a.err, err);
 }
 
 // Adjoint of the hit-time histogram: the batched transport with per-track scores. Bin
@@ -1523,6 +1867,33 @@ cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detecto
     }
     return cudaGetLastError();
 }
+
+cudaError_t launch_sm_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
+                                uint32_t ring_cap, void* film, uint32_t film_cap, const uint32_t* unit_event,
+                                const QPhonon* queue, int stage_tables, int grid, cudaStream_t s) {
+    const FLat f = make_flat(L, cdf_f, D);
+    SmPoolArgs p;
+    p.ring = static_cast<PoolPh*>(ring);
+    p.film = static_cast<FilmRec*>(film);
+    p.ring_cap = ring_cap;
+    p.film_cap = film_cap;
+    p.film_trigger = film_cap > 2u * kSmThreads ? film_cap - 2u * kSmThreads : film_cap / 2u;
+    p.unit_event = unit_event;
+    p.queue = queue;
+    p.stage_tables = stage_tables;
+    if (queue) {
+        if (L.kin_mode != kKinOctahedral) k_sm_pool_fp32<false, 1, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        else if (a.surrogate) k_sm_pool_fp32<true, 0, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        else k_sm_pool_fp32<false, 0, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+    } else {
+        if (L.kin_mode != kKinOctahedral) k_sm_pool_fp32<false, 1><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        else if (a.surrogate) k_sm_pool_fp32<true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        else k_sm_pool_fp32<false><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+    }
+    return cudaGetLastError();
+}
+
+int sm_pool_threads() { return kSmThreads; }
 
 cudaError_t pool_fp32_occupancy(int block, int* blocks_per_sm) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_pool_fp32<false>, block, 0);

@@ -528,17 +528,22 @@ int cmpmc_gpu_configure_graph(cmpmc_gpu_ctx* ctx, int enable);
 int cmpmc_gpu_configure_phases(cmpmc_gpu_ctx* ctx, uint32_t phase_steps);
 
 /* Launch form of the batched FP32 phonon transport (no counterpart in the reference).
- * enable = 1 (the default): the warp pool, one persistent launch per call in which every
- * warp keeps its 32 lanes busy from a private ring of pending phonons (film re-emissions and
- * daughters) and the batch's primaries, and runs the film cascades of its lanes 32 at a
- * time; the host synchronizes once per call. enable = 0: the host-driven form, alternating
- * transport and film launches until both device queues are empty (one host round trip per
- * round; configure_phases applies to it only). ring_capacity: pending phonons per warp (a
- * power of two >= 64, 80 B each; default 1024, grown 4x and the call rerun when a warp's
- * ring overflows; 0 keeps the current value). Both forms sample the same process; a
- * daughter runs on a substream drawn from its parent's in the pool form, on the parent's
- * own stream in the host-driven form, so their hits agree in distribution, not bit for bit. */
-int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int enable, uint32_t ring_capacity);
+ * form = 1 (the default): the SM-phase pool, one persistent launch per call with one
+ *   768-thread block per SM that alternates a transport phase (every warp steps its lanes,
+ *   refilled from the block's ring of pending phonons and the batch's primaries; film
+ *   entries and daughters appended to block buffers) and a film phase (every thread runs
+ *   the waiting film cascades, their re-emissions appended to the ring), so an SM runs one
+ *   code path at a time; ring_capacity: pending phonons per block (default 2^15).
+ * form = 2: the warp pool, one persistent launch in which every warp runs its own film
+ *   cascades between its transport steps; ring_capacity: pending phonons per warp (default
+ *   1024).
+ * form = 0: the host-driven form, alternating transport and film launches until both device
+ *   queues are empty (one host round trip per round; configure_phases applies to it only).
+ * Rings are 80 B per entry; a ring (a power of two >= 64; 0 keeps the current value) that
+ * overflows is grown 4x and the call rerun. All forms sample the same process; a daughter
+ * runs on a substream drawn from its parent's in the pool forms, on the parent's own stream
+ * in the host-driven form, so their hits agree in distribution, not bit for bit. */
+int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int form, uint32_t ring_capacity);
 
 /* Shared-memory staging of the small tables (no counterpart in the reference): with
  * enable = 1 (the default) every block of the warp-pool kernel copies the two decay CDF

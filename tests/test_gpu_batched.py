@@ -249,7 +249,7 @@ def test_batched_kinematics_modes_statistics(ge_lattice, wl, n):
 
 
 def test_pool_and_host_driven_rounds_agree(ge_lattice):
-    """The warp pool (one persistent launch) and the host-driven film / transport rounds
+    """The SM-phase pool (one persistent launch) and the host-driven film / transport rounds
     sample the same process (a daughter's substream differs between them): hit histograms
     chi^2 p > 0.01 on 2,000 mixed-energy events, the same deposited fraction within 1 %,
     both ledgers closed."""
@@ -258,7 +258,7 @@ def test_pool_and_host_driven_rounds_agree(ge_lattice):
     packed = eng.generate(workload_of("c1"), 2000, 7)
     a = eng.run_packed(packed, cm.RunOptions(seed=7, form="batched_fp32"))
     eng2 = _engine(ge_lattice, "c1")
-    eng2.configure_pool(False)
+    eng2.configure_pool(0)
     b = eng2.run_packed(packed, cm.RunOptions(seed=7, form="batched_fp32"))
     assert a.kernel_launches < b.kernel_launches  # one transport launch against the rounds
     lo = min(a.hits["edep"].min(), b.hits["edep"].min())
@@ -275,15 +275,17 @@ def test_pool_and_host_driven_rounds_agree(ge_lattice):
     assert abs(fa / fb - 1.0) < 0.01
 
 
-def test_pool_ring_overflow_reruns_to_the_same_hits(ge_lattice):
-    """A warp ring that is too small (64 entries) overflows on the device; the call grows it
-    and reruns, and the hits of every event (as a set) and the integer counters equal the
-    default ring's: every unit owns its substream."""
-    import cmpmc_b200 as cm
+@pytest.mark.parametrize("form,ring", [(1, 64), (2, 64), (2, 0)])
+def test_pool_forms_give_the_same_hits(ge_lattice, form, ring):
+    """The two pool forms run the same step on the same substreams (a daughter's, a film
+    entry's and a re-emission's keys are drawn at the same points), so the SM-phase pool and
+    the warp pool give every event the same hits (as a set) and the same integer counters;
+    so does a pool whose ring is too small (it overflows on the device, and the call grows it
+    and reruns)."""
     eng = _engine(ge_lattice, "c1")
     a = _batched(eng, "c1", 300, want_event_stats=True)
     eng2 = _engine(ge_lattice, "c1")
-    eng2.configure_pool(True, ring_capacity=64)
+    eng2.configure_pool(form, ring_capacity=ring)
     b = _batched(eng2, "c1", 300, want_event_stats=True)
     assert np.array_equal(a.hit_offsets, b.hit_offsets)
     assert _sorted_event_hits(a) == _sorted_event_hits(b)
