@@ -1106,7 +1106,7 @@ int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int form, uint32_t ring_capacit
         return fail(ctx, CMPMC_ERR_INVALID, "ring capacity: a power of two, at least 64");
     ctx->pool = form;
     if (ring_capacity) {
-        if (form == 1) ctx->sm_ring_cap = std::max<uint32_t>(ring_capacity, 2 * sm_pool_threads());
+        if (form == 1) ctx->sm_ring_cap = std::max<uint32_t>(ring_capacity, 2048);  // a block appends up to 2 x 768 at once
         else ctx->pool_ring_cap = ring_capacity;
     }
     return CMPMC_OK;

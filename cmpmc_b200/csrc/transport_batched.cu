@@ -1848,6 +1848,7 @@ cudaError_t launch_queue_fp32(const Lattice& L, const float* cdf_f, const Detect
 cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
                              uint32_t ring_cap, void* film, const uint32_t* unit_event, const QPhonon* queue,
                              int stage_tables, int grid, int block, cudaStream_t s) {
+    if (ring_cap < 64 || (ring_cap & (ring_cap - 1u)) != 0) return cudaErrorInvalidValue;  // indexed by masking
     const FLat f = make_flat(L, cdf_f, D);
     PoolArgs p;
     p.ring = static_cast<PoolPh*>(ring);
@@ -1871,6 +1872,9 @@ cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detecto
 cudaError_t launch_sm_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
                                 uint32_t ring_cap, void* film, uint32_t film_cap, const uint32_t* unit_event,
                                 const QPhonon* queue, int stage_tables, int grid, cudaStream_t s) {
+    // the ring is indexed by masking: its capacity must be a power of two
+    if (ring_cap < 2u * kSmThreads || (ring_cap & (ring_cap - 1u)) != 0 || film_cap < 4u * kSmThreads)
+        return cudaErrorInvalidValue;
     const FLat f = make_flat(L, cdf_f, D);
     SmPoolArgs p;
     p.ring = static_cast<PoolPh*>(ring);
