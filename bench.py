@@ -261,6 +261,8 @@ def main() -> None:
     ap.add_argument("--launch", default="sm_pool", choices=["sm_pool", "warp_pool", "rounds"],
                     help="launch form of the batched phonon transport")
     ap.add_argument("--no-matched", action="store_true", help="skip the matched-statistics check")
+    ap.add_argument("--surrogate", action="store_true",
+                    help="film cascades from the KaplanSurrogateLUT table (not the headline configuration)")
     ap.add_argument("--pub-events", type=int, default=100000, help="events of the published workload (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -312,6 +314,7 @@ def main() -> None:
         d.keep_hits = 1
         d.form = form_id
         d.seed = SEED
+        d.kaplan_surrogate = 1 if args.surrogate else 0
         if on_device:
             d.rng_state, d.injected_eV = d_rng.data_ptr(), d_inj.data_ptr()
             d.phonon_offsets, d.phonons = d_off.data_ptr(), d_ph.data_ptr()
@@ -360,7 +363,8 @@ def main() -> None:
     # launch configuration from the project's autotuner (results do not depend on it), then
     # CUDA-graph replay of the device-resident call
     tune = None
-    if not args.no_tune:
+    # the SM-phase pool has one launch shape (one 768-thread block per SM): nothing to tune
+    if not args.no_tune and launch_form != "sm_pool":
         tr = _ffi.TuneResultC()
         if lib.cmpmc_gpu_autotune(h, C.byref(dd), 1, C.byref(tr)) != 0:
             buf = C.create_string_buffer(512)
@@ -476,6 +480,7 @@ def main() -> None:
         "data": "synthetic",
         "config": {"workload": "mixed_energy_phonons", "events": args.events * world, "primaries_per_event": PER_EVENT,
                    "primaries": n_prim * world, "form": args.form, "seed": SEED,
+                   "film_cascades": "surrogate table" if args.surrogate else "full Kaplan cascade",
                    "energy": "log-uniform 1-30 meV", "modes": "L/ST/FT 0.10/0.36/0.54",
                    "l2": "256 MiB buffer written between timed steps (L2 126 MB); inputs 128 MB, hits ~1.5 GB per step"},
         "kernel_ms_per_step": kernel_ms,

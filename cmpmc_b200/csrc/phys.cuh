@@ -778,11 +778,15 @@ CMPMC_HD double film_sample_phonon_energy(const Film& f, double E, G& rng) {
 // generation buffers of the reference are value-copied at the end of each stage; here
 // the same buffers are swapped, which leaves identical contents. `work` must hold
 // 4 * kKaplanCap doubles; `refl` receives the re-emitted phonon energies.
+// entry_checked: a phonon seed whose entry step (direct absorption, loss at entry) the caller
+// has already drawn and passed, so the cascade starts at once.
 template <class G>
-CMPMC_HD double film_absorb_quantum(const Film& f, double energy, KBuf& refl, double* work, G& rng, bool photon) {
+CMPMC_HD double film_absorb_quantum(const Film& f, double energy, KBuf& refl, double* work, G& rng, bool photon,
+                                    bool entry_checked = false) {
     refl.clear();
-    if (!photon && film_direct_absorption(f, energy, rng)) return energy;
-    if (film_is_subgap(f, energy) || (!photon && rng.uniform() <= film_loss_probability(f, energy, 4.0))) {
+    const bool entry = !photon && !entry_checked;
+    if (entry && film_direct_absorption(f, energy, rng)) return energy;
+    if (film_is_subgap(f, energy) || (entry && rng.uniform() <= film_loss_probability(f, energy, 4.0))) {
         refl.push(energy);
         return 0.0;
     }

@@ -156,6 +156,49 @@ __device__ __noinline__ double kaplan_call(const Film* f, double E, double* refl
     return edep;
 }
 
+// the pair-breaking cascade of a film entry whose entry step was drawn in line (film_quick)
+__device__ __noinline__ double kaplan_cascade_call(const Film* f, double E, double* refl, int* n_refl, double* work,
+                                                   R128* g) {
+    KBuf r{refl, 0};
+    const double edep = film_absorb_quantum(*f, E, r, work, *g, false, true);
+    *n_refl = r.n;
+    return edep;
+}
+
+// The entry step of KaplanFilm::absorb_quantum for a phonon seed (kaplan_film.hpp:106-120),
+// drawn in line by the transport step: direct absorption (the whole energy deposited), or the
+// phonon comes back out unchanged (sub-gap, or lost on its way in); only the rest needs the
+// pair-breaking cascade. With the surrogate table (whose stored outcomes include the entry
+// step) only sub-gap phonons are decided here: the table does not cover them.
+enum { kFilmAbsorbed = 0, kFilmReemit = 1, kFilmCascade = 2 };
+template <bool kSur>
+__device__ __noinline__ int film_quick(const Film* f, double E, R128* g) {
+    if (kSur && !film_is_subgap(*f, E)) return kFilmCascade;
+    if (film_direct_absorption(*f, E, *g)) return kFilmAbsorbed;
+    if (film_is_subgap(*f, E) || g->uniform() <= film_loss_probability(*f, E, 4.0)) return kFilmReemit;
+    return kFilmCascade;
+}
+
+// a hit of the transport step (film absorbed in line): staged with its event as key, the
+// slots reserved once per group of lanes that hit together
+__device__ __forceinline__ void stage_hit(const RunArgs& a, uint32_t ev, const cmpmc_sensor_hit& h) {
+    if (!a.keep_hits) return;
+    atomicAdd(reinterpret_cast<unsigned long long*>(a.ev_nhits + ev), 1ull);
+    const unsigned grp = __activemask();
+    const int leader = __ffs(grp) - 1;
+    const int lane = threadIdx.x & 31;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(a.hit_count, static_cast<unsigned long long>(__popc(grp)));
+    base = __shfl_sync(grp, base, leader);
+    unsigned lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    const unsigned long long idx = base + __popc(grp & lt);
+    if (idx < a.hit_cap) {
+        a.hit_stage[idx] = h;
+        a.hit_key[idx] = ev;
+    }
+}
+
 // electrode mask lookup out of line: the sector test's atan2 stays out of the step loop's
 // instruction stream
 __device__ __noinline__ int mask_call(const Pad* pads, int n_pads, float x, float y, R128* g) {
@@ -982,7 +1025,9 @@ union PoolOut {
 struct WarpSink {
     PoolOut* o;
     bool has_d;
+    const RunArgs* a;
     __device__ __forceinline__ void film(const FilmRec& r) { o->film = r; }
+    __device__ __forceinline__ void hit(uint32_t ev, const cmpmc_sensor_hit& h) { stage_hit(*a, ev, h); }
     __device__ __forceinline__ void daughter(const PoolPh& q) {
         o->ph = q;
         has_d = true;
@@ -993,7 +1038,7 @@ struct WarpSink {
 // the track goes on, ended (counters and ledger updated), or entered an active film (the
 // film record handed to out.film). A daughter made in the step is handed to out.daughter
 // with a substream key drawn from the track's stream.
-template <int kKin, class ST, class Sink>
+template <int kKin, bool kSur, class ST, class Sink>
 __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const Detector& D, FTrack& trk, R128& g,
                                          const ST& st, uint32_t ev, Sink& out) {
     if (trk.E < D.min_phonon_eV || trk.bounces >= D.max_bounces) {
@@ -1058,72 +1103,100 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
             enter = g.u() < p_enter;
         }
         if (enter) {
-            FilmRec fr;
-            fr.px = trk.pos.x; fr.py = trk.pos.y; fr.pz = trk.pos.z;
-            fr.w = trk.w;
-            fr.E = trk.E;
-            fr.t = trk.t;
-            fr.key = draw_key(g);
-            fr.ev = ev;
-            fr.ch_id = ch_id;
-            fr.bounces = trk.bounces;
-            fr.surf = static_cast<uint8_t>(bh.surf);
-            fr.mode = static_cast<uint8_t>(trk.mode);
-            fr.pad0 = fr.pad1 = 0;
-            out.film(fr);
-            return kStepFilm;
-        }
-        if (g.u() > static_cast<float>(s.prob_refl)) {
+            R128 g_c = g;
+            const int film = film_quick<kSur>(&s.film, trk.E, &g_c);
+            g = g_c;
+            if (film == kFilmAbsorbed) {
+                const double wedep = trk.E * trk.w;
+                ++st.hits();
+                st.dep() += wedep;
+                cmpmc_sensor_hit h;
+                h.pos[0] = trk.pos.x; h.pos[1] = trk.pos.y; h.pos[2] = trk.pos.z;
+                h.time = trk.t;
+                h.edep = wedep;
+                h.incident_energy = trk.E;
+                h.surface_id = static_cast<uint8_t>(bh.surf);
+                h.excitation = 0;
+                h.mode = static_cast<uint8_t>(trk.mode);
+                h._pad = 0;
+                h.channel_id = ch_id;
+                out.hit(ev, h);
+                return kStepEnd;
+            }
+            if (film == kFilmCascade) {
+                FilmRec fr;
+                fr.px = trk.pos.x; fr.py = trk.pos.y; fr.pz = trk.pos.z;
+                fr.w = trk.w;
+                fr.E = trk.E;
+                fr.t = trk.t;
+                fr.key = draw_key(g);
+                fr.ev = ev;
+                fr.ch_id = ch_id;
+                fr.bounces = trk.bounces;
+                fr.surf = static_cast<uint8_t>(bh.surf);
+                fr.mode = static_cast<uint8_t>(trk.mode);
+                fr.pad0 = fr.pad1 = 0;
+                out.film(fr);
+                return kStepFilm;
+            }
+            // re-emitted unchanged: back into the crystal (bounces kept), a DOS mode and an
+            // inward Lambertian direction from the shared sampling below
+            trk.pos = trk.pos + bh.n * kNudge;
+            trk.mode = fdos(L, g.u());
+            sample = 1;
+        } else if (g.u() > static_cast<float>(s.prob_refl)) {
             ++st.killed();
             st.esc() += trk.E * trk.w;
             return kStepEnd;
         }
-        ++st.refl();
-        trk.pos = trk.pos + bh.n * kNudge;
-        float p_anh, p_anh_spec;
-        if (L.split_const[bh.surf]) {
-            p_anh = L.p_anh[bh.surf];
-            p_anh_spec = L.p_anh_spec[bh.surf];
-        } else {
-            const Split sp = reflection_split(s, trk.E);
-            p_anh = static_cast<float>(sp.p_anh);
-            p_anh_spec = static_cast<float>(sp.p_anh + sp.p_spec);
-        }
-        const float u_refl = g.u();
-        if (u_refl < p_anh) {
-            ++st.down();
-            const bool tt = g.u() < L.fTT;
-            const float x = fcdf_any(tt ? cdf + kNCdf : cdf, g);
-            const int m1 = tt ? ftrans(L, g) : 0;
-            const int m2 = ftrans(L, g);
-            FTrack dtr;
-            FKin k2kin;
-            dtr.k = finward<kKin>(L, m2, bh.n, g, k2kin);
-            dtr.pos = trk.pos;
-            dtr.vg = k2kin.dir;
-            dtr.vmag = k2kin.mag;
-            dtr.E = (1.0 - static_cast<double>(x)) * trk.E;
-            dtr.t = trk.t;
-            dtr.w = trk.w;
-            dtr.bounces = 0;
-            dtr.mode = m2;
-            out.daughter(pool_entry(dtr, draw_key(g), ev));
-            trk.E = static_cast<double>(x) * trk.E;
-            trk.mode = m1;
-            sample = 1;
-        } else if (u_refl < p_anh_spec) {
-            F3 kr = trk.k - bh.n * (2.0f * fdot(trk.k, bh.n));
-            FKin kin = fmapk<kKin>(L, trk.mode, kr);
-            if (fdot(kin.dir, bh.n) <= 1e-6f) kr = finward<kKin>(L, trk.mode, bh.n, g, kin);
-            trk.k = kr;
-            trk.vg = kin.dir;
-            trk.vmag = kin.mag;
-        } else {
-            sample = 1;
+        if (!enter) {  // a surface reflection
+            ++st.refl();
+            trk.pos = trk.pos + bh.n * kNudge;
+            float p_anh, p_anh_spec;
+            if (L.split_const[bh.surf]) {
+                p_anh = L.p_anh[bh.surf];
+                p_anh_spec = L.p_anh_spec[bh.surf];
+            } else {
+                const Split sp = reflection_split(s, trk.E);
+                p_anh = static_cast<float>(sp.p_anh);
+                p_anh_spec = static_cast<float>(sp.p_anh + sp.p_spec);
+            }
+            const float u_refl = g.u();
+            if (u_refl < p_anh) {
+                ++st.down();
+                const bool tt = g.u() < L.fTT;
+                const float x = fcdf_any(tt ? cdf + kNCdf : cdf, g);
+                const int m1 = tt ? ftrans(L, g) : 0;
+                const int m2 = ftrans(L, g);
+                FTrack dtr;
+                FKin k2kin;
+                dtr.k = finward<kKin>(L, m2, bh.n, g, k2kin);
+                dtr.pos = trk.pos;
+                dtr.vg = k2kin.dir;
+                dtr.vmag = k2kin.mag;
+                dtr.E = (1.0 - static_cast<double>(x)) * trk.E;
+                dtr.t = trk.t;
+                dtr.w = trk.w;
+                dtr.bounces = 0;
+                dtr.mode = m2;
+                out.daughter(pool_entry(dtr, draw_key(g), ev));
+                trk.E = static_cast<double>(x) * trk.E;
+                trk.mode = m1;
+                sample = 1;
+            } else if (u_refl < p_anh_spec) {
+                F3 kr = trk.k - bh.n * (2.0f * fdot(trk.k, bh.n));
+                FKin kin = fmapk<kKin>(L, trk.mode, kr);
+                if (fdot(kin.dir, bh.n) <= 1e-6f) kr = finward<kKin>(L, trk.mode, bh.n, g, kin);
+                trk.k = kr;
+                trk.vg = kin.dir;
+                trk.vmag = kin.mag;
+            } else {
+                sample = 1;
+            }
         }
     }
     // shared new-direction path: isotropic (bulk scatter) or Lambertian about the inward
-    // normal (diffuse reflection), then the table lookup
+    // normal (diffuse reflection, film re-emission), then the table lookup
     if (sample != 2) {
         const bool lam = (sample == 1);
         const F3 e3 = lam ? bh.n : f3(0.0f, 0.0f, 1.0f);
@@ -1188,11 +1261,12 @@ __device__ __noinline__ uint32_t pool_film_step(const FLat* Lp, const Detector* 
         const Surface& s = D.surf[r.surf];
         R128 g_c;
         g_c.seed(r.key);
+        // the entry step was drawn by the transport step (film_quick): the cascade starts at once
         if constexpr (kSur) {
             edep = s.lut_abs ? surrogate_call(&s, r.E, refl_buf, &n_refl, kwork, &g_c)
                              : kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
         } else {
-            edep = kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
+            edep = kaplan_cascade_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
         }
         g = g_c;
     }
@@ -1404,9 +1478,9 @@ __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FL
         }
         // 2. one step of every live track
         int outcome = kStepOn;
-        WarpSink sink{&my_out, false};
+        WarpSink sink{&my_out, false, &a};
         if (live) {
-            outcome = pool_step<kKin>(L, cdf, D, trk, g, st, ev_cur, sink);
+            outcome = pool_step<kKin, kSur>(L, cdf, D, trk, g, st, ev_cur, sink);
             if (outcome != kStepOn) {
                 sink_unit(&a, ev_cur, st);
                 live = false;
@@ -1486,6 +1560,8 @@ struct SmSink {
     PoolPh* ring;
     uint32_t film_cap, ring_mask, r_floor;
     unsigned* err;
+    const RunArgs* a;
+    __device__ __forceinline__ void hit(uint32_t ev, const cmpmc_sensor_hit& h) { stage_hit(*a, ev, h); }
     __device__ __forceinline__ void film_rec(const FilmRec& r) {
         const uint32_t i = atomicAdd(&sh->f_tail, 1u);
         if (i < film_cap) fbuf[i] = r;
@@ -1520,11 +1596,12 @@ __device__ __noinline__ void sm_film_phase(const FLat* Lp, const Detector* Dp, c
         {
             R128 g_c;
             g_c.seed(r.key);
+            // the entry step was drawn by the transport step (film_quick): the cascade starts at once
             if constexpr (kSur) {
                 edep = s.lut_abs ? surrogate_call(&s, r.E, refl_buf, &n_refl, kwork, &g_c)
                                  : kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
             } else {
-                edep = kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
+                edep = kaplan_cascade_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
             }
             g = g_c;
         }
@@ -1637,7 +1714,7 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_con
         // ---- transport phase --------------------------------------------------------
         const uint32_t r_floor = vsh->r_head;  // ring slots below it are free
         const uint32_t r_pub = vsh->r_pub;
-        SmSink sink{&sh, film, ring, p.film_cap, ring_mask, r_floor, &err};
+        SmSink sink{&sh, film, ring, p.film_cap, ring_mask, r_floor, &err, &a};
         for (;;) {
             uint32_t ft = 0, inp = 0, dry = 0;
             if (lane == 0) {
@@ -1735,7 +1812,7 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_con
                 break;
             }
             if (live) {
-                const int outcome = pool_step<kKin>(L, cdf, D, trk, g, st, ev_cur, sink);
+                const int outcome = pool_step<kKin, kSur>(L, cdf, D, trk, g, st, ev_cur, sink);
                 if (outcome != kStepOn) {
                     sink_unit(&a, ev_cur, st);
                     live = false;
