@@ -17,6 +17,8 @@ from the library's autotuner (results do not depend on it).
          and every hit, the hit offsets and the statistics copied back, each step
          (e2e_with_generator adds the host generator's time per step)
   plain_fp64  the plain FP64 form (bit-exact event streams) on the same workload, one step
+  batched_fp64  the same SM-phase pool computed in FP64 throughout on the same substreams
+         (pool form 3), one step: fp32_over_fp64 is what the FP32 form gains
   matched     after the timed region: chi^2 p-values of the per-event hit histograms (time
          256 bins over 0-2 ms, radius 64, edep 64) of one timed batched call against the
          plain FP64 run and against the reference's histograms of the same 10,000 events
@@ -190,10 +192,10 @@ def cpu_baseline(sample_events: int):
             "steps_per_s": r["total_steps"] / r["wall_seconds"], "wall_seconds": r["wall_seconds"]}
 
 
-def matched_statistics(batched: dict, plain, first_event: int) -> dict:
+def matched_statistics(batched: dict, plain, first_event: int, fp64=None) -> dict:
     """chi^2 of the batched call's per-event hit histograms against the plain FP64 form's on
-    the same events and against the reference's (10,000-event fixture, rank 0's events), and
-    the ledger closures."""
+    the same events, against the batched form computed in FP64 on the same substreams and
+    against the reference's (10,000-event fixture, rank 0's events), and the ledger closures."""
     from tests.golden.records import event_histograms, hist_chi2
     path = os.path.join(ROOT, "tests", "golden", "c1_hist_full.npz")
     ref = dict(np.load(path)) if os.path.exists(path) else None
@@ -210,6 +212,12 @@ def matched_statistics(batched: dict, plain, first_event: int) -> dict:
         out["plain_hits"] = int(len(plain["hits"]))
         out["ledger_closure_plain_fp64"] = abs(plain["injected"] - plain["deposited"] - plain["escaped"]) / \
             plain["injected"]
+    if fp64 is not None:
+        hf = event_histograms(fp64["offsets"], fp64["hits"], rng)
+        out["p_vs_batched_fp64"] = {k: round(hist_chi2(hb, hf, k)[2], 4) for k in ("time", "radius", "edep")}
+        out["batched_fp64_hits"] = int(len(fp64["hits"]))
+        out["ledger_closure_batched_fp64"] = abs(fp64["injected"] - fp64["deposited"] - fp64["escaped"]) / \
+            fp64["injected"]
     if ref is not None and first_event == 0 and int(ref["n_events"]) == hb["n_events"]:
         out["p_vs_reference_cpu"] = {k: round(hist_chi2(hb, ref, k)[2], 4) for k in ("time", "radius", "edep")}
         out["reference_hits"] = int(ref["n_hits"])
@@ -290,6 +298,7 @@ def main() -> None:
     ap.add_argument("--launch", default="sm_pool", choices=["sm_pool", "warp_pool", "rounds"],
                     help="launch form of the batched phonon transport")
     ap.add_argument("--no-matched", action="store_true", help="skip the matched-statistics check")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the batched FP64 comparison step")
     ap.add_argument("--recoil", type=int, default=0,
                     help="instead of the headline line: time the recoil batch of this many events once")
     ap.add_argument("--surrogate", action="store_true",
@@ -505,7 +514,24 @@ def main() -> None:
                  "steps_per_s": o.stats.total_steps / (o.kernel_ms * 1e-3)}
         if batched_res is not None:
             plain_res = fetch(o)
-    matched = matched_statistics(batched_res, plain_res, first) if batched_res is not None else None
+    # the same SM-phase pool computed in FP64 on the same substreams (pool form 3), one step
+    fp64 = None
+    fp64_res = None
+    if not args.no_fp64 and launch_form == "sm_pool" and not args.surrogate:
+        eng.configure_pool(3, device=dev)
+        run(dd)  # warm-up (its ring and film buffers)
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        o = run(dd)
+        f_ms = max_over_ranks(o.total_ms)
+        f_kms = max_over_ranks(o.kernel_ms)
+        fp64 = {"value": world * n_prim / (f_ms * 1e-3), "unit": UNIT, "ms_per_step": f_ms,
+                "kernel_ms_per_step": f_kms, "steps_per_s": o.stats.total_steps / (o.kernel_ms * 1e-3),
+                "hits": int(o.n_hits)}
+        if batched_res is not None:
+            fp64_res = fetch(o)
+        eng.configure_pool(1, device=dev)
+    matched = matched_statistics(batched_res, plain_res, first, fp64_res) if batched_res is not None else None
     published = published_workload(cm, lat, dev, args.pub_events, lib) if args.pub_events and rank == 0 else None
 
     peak, peak_kind = measured_peaks()
@@ -543,6 +569,9 @@ def main() -> None:
     if plain is not None:
         line["plain_fp64"] = plain
         line["batched_over_plain"] = value / plain["value"]
+    if fp64 is not None:
+        line["batched_fp64"] = fp64
+        line["fp32_over_fp64"] = value / fp64["value"]
     if matched is not None:
         line["matched"] = matched
     if published is not None:

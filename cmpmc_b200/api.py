@@ -975,7 +975,8 @@ class SimulationEngine:
     def configure_pool(self, form=1, ring_capacity: int = 0, device: int = 0) -> None:
         """Launch form of the batched phonon transport (cmpmc_gpu_configure_pool): 1 (or True)
         the SM-phase pool, one persistent launch (the default); 2 the warp pool; 0 (or False)
-        the host-driven film / transport rounds."""
+        the host-driven film / transport rounds; 3 the SM-phase pool computed in FP64 on the
+        same substreams (phonon-only batches, full film cascades)."""
         h = self.context(device)
         _check(self._lib.cmpmc_gpu_configure_pool(h, int(form), int(ring_capacity)), h)
 

@@ -109,10 +109,10 @@ struct cmpmc_gpu_ctx {
     uint64_t film_cap = 1ull << 22;                     // film entries per phase (64 B each)
     uint32_t phase_steps = 0;                           // steps a track takes per transport phase (0: any)
     int pool = 1;                                       // batched phonon form: 1 SM-phase pool, 2 warp pool,
-                                                        // 0 host-driven rounds
+                                                        // 0 host-driven rounds, 3 SM-phase pool in FP64
     int stage_tables = 1;                               // pool forms: decay CDF tables staged in shared memory
     uint32_t pool_ring_cap = 1024;                      // pending phonons per warp (warp pool)
-    uint32_t sm_ring_cap = 1u << 15;                    // pending phonons per block (SM-phase pool)
+    uint32_t sm_ring_cap = 1u << 17;                    // pending phonons per block (SM-phase pool)
     uint32_t sm_film_cap = 8192;                        // film records per block and phase (SM-phase pool)
     DevBuf pool_ring, pool_film;                        // warp pool: per-warp rings and film buffers
     uint64_t queue_cap = 1ull << 24;                    // Luke-phonon queue entries (64 B each)
@@ -201,10 +201,13 @@ int ensure_surrogate(cmpmc_gpu_ctx* ctx) {
 }
 
 // ---- the persistent pool launches (SM-phase pool or warp pool) ----------------------
+bool sm_pool(const cmpmc_gpu_ctx* ctx) { return ctx->pool == 1 || ctx->pool == 3; }
+int pool_fp64(const cmpmc_gpu_ctx* ctx) { return ctx->pool == 3 ? 1 : 0; }
+
 // grid of a pool launch over `units` units: one 768-thread block per SM (SM-phase pool), or
 // the occupancy's 128-thread blocks (warp pool), never more than the units can start
 int pool_grid(cmpmc_gpu_ctx* ctx, uint64_t units, uint64_t* grid) {
-    if (ctx->pool == 1) {
+    if (sm_pool(ctx)) {
         const uint64_t per = static_cast<uint64_t>(sm_pool_threads());
         *grid = std::max<uint64_t>(1, std::min<uint64_t>(ctx->num_sms, (units + per - 1) / per));
         return CMPMC_OK;
@@ -220,9 +223,9 @@ int pool_grid(cmpmc_gpu_ctx* ctx, uint64_t units, uint64_t* grid) {
 
 // ring and film buffers for launches of up to `grid` blocks
 int ensure_pool_buffers(cmpmc_gpu_ctx* ctx, uint64_t grid) {
-    if (ctx->pool == 1) {
-        CK(ctx->pool_ring.ensure(grid * ctx->sm_ring_cap * pool_ring_entry_bytes()), "alloc block rings");
-        CK(ctx->pool_film.ensure(grid * ctx->sm_film_cap * sizeof(FilmRec)), "alloc film buffers");
+    if (sm_pool(ctx)) {
+        CK(ctx->pool_ring.ensure(grid * ctx->sm_ring_cap * sm_pool_entry_bytes(pool_fp64(ctx))), "alloc block rings");
+        CK(ctx->pool_film.ensure(grid * ctx->sm_film_cap * sm_pool_film_bytes(pool_fp64(ctx))), "alloc film buffers");
     } else {
         CK(ctx->pool_ring.ensure(grid * 4 * ctx->pool_ring_cap * pool_ring_entry_bytes()), "alloc warp rings");
         CK(ctx->pool_film.ensure(grid * 4 * pool_film_bytes_per_warp()), "alloc film buffers");
@@ -232,9 +235,10 @@ int ensure_pool_buffers(cmpmc_gpu_ctx* ctx, uint64_t grid) {
 
 cudaError_t launch_pool(cmpmc_gpu_ctx* ctx, const RunArgs& a, uint64_t grid, const QPhonon* queue, cudaStream_t s) {
     const uint32_t* ue = ctx->unit_event.as<uint32_t>();
-    if (ctx->pool == 1)
+    if (sm_pool(ctx))
         return launch_sm_pool_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->pool_ring.p, ctx->sm_ring_cap, ctx->pool_film.p,
-                                   ctx->sm_film_cap, ue, queue, ctx->stage_tables, static_cast<int>(grid), s);
+                                   ctx->sm_film_cap, ue, queue, ctx->stage_tables, pool_fp64(ctx),
+                                   static_cast<int>(grid), s);
     return launch_pool_fp32(ctx->L, ctx->cdf_f, ctx->D, a, ctx->pool_ring.p, ctx->pool_ring_cap, ctx->pool_film.p, ue,
                             queue, ctx->stage_tables, static_cast<int>(grid), 128, s);
 }
@@ -242,10 +246,10 @@ cudaError_t launch_pool(cmpmc_gpu_ctx* ctx, const RunArgs& a, uint64_t grid, con
 // after an overflow of a pool's ring or film buffer: more room for the rerun
 void grow_pool(cmpmc_gpu_ctx* ctx, unsigned err) {
     if (err & kErrQueue) {
-        if (ctx->pool == 1) ctx->sm_ring_cap = std::min<uint32_t>(ctx->sm_ring_cap * 4, 1u << 24);
+        if (sm_pool(ctx)) ctx->sm_ring_cap = std::min<uint32_t>(ctx->sm_ring_cap * 4, 1u << 24);
         else ctx->pool_ring_cap = std::min<uint32_t>(ctx->pool_ring_cap * 4, 1u << 20);
     }
-    if ((err & kErrFilmQueue) && ctx->pool == 1) ctx->sm_film_cap = std::min<uint32_t>(ctx->sm_film_cap * 2, 1u << 20);
+    if ((err & kErrFilmQueue) && sm_pool(ctx)) ctx->sm_film_cap = std::min<uint32_t>(ctx->sm_film_cap * 2, 1u << 20);
 }
 
 // Device counters of the batched charge form (reset per phase except next_carrier)
@@ -264,6 +268,7 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
                         uint64_t n_ch, int& launches, Counters& hc, float& kms, uint64_t& n_hits,
                         uint64_t*& ev_offsets, cmpmc_sim_stats*& ev_stats) {
     cudaStream_t s = ctx->stream;
+    if (pool_fp64(ctx)) return fail(ctx, CMPMC_ERR_INVALID, "the FP64 pool form runs phonon-only batches");
     const int tpb = ctx->tpb;
     int bps_ph = ctx->bps, bps_ch = ctx->bps;
     if (!bps_ph) {
@@ -475,8 +480,12 @@ int run_charges_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a,
             ++launches;
             CK(cudaMemcpyAsync(hbuf + sizeof(Counters), cc, sizeof(ChargeCounters), cudaMemcpyDeviceToHost, s),
                "copy counters");
+            CK(cudaMemcpyAsync(hbuf, ctx->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s), "copy counters");
             CK(cudaStreamSynchronize(s), "charge kernel");
             ChargeCounters hcc = *reinterpret_cast<const ChargeCounters*>(hbuf + sizeof(Counters));
+            // a pool phase that overflowed its ring: the call reruns with more room, so the
+            // remaining rounds are not run
+            if (pool && (reinterpret_cast<const Counters*>(hbuf)->err & (kErrQueue | kErrFilmQueue)) != 0) break;
             if (release && hcc.rel_tail > 0) {
                 // the round's collections release their energy into the phonon queue
                 if (hcc.rel_tail > rel_cap) return fail(ctx, CMPMC_ERR_CAPACITY, "release-record buffer overflow");
@@ -735,6 +744,8 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
                      int& launches, Counters& hc, float& kms, uint64_t& n_hits, uint64_t*& ev_offsets,
                      cmpmc_sim_stats*& ev_stats) {
     cudaStream_t s = ctx->stream;
+    if (pool_fp64(ctx) && a.surrogate)
+        return fail(ctx, CMPMC_ERR_INVALID, "the FP64 pool form runs the full film cascades (no surrogate)");
     uint64_t grid = 1;
     {
         const int st = pool_grid(ctx, n_ph, &grid);
@@ -1101,12 +1112,12 @@ int cmpmc_gpu_configure_staging(cmpmc_gpu_ctx* ctx, int enable) {
 }
 
 int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int form, uint32_t ring_capacity) {
-    if (!ctx || form < 0 || form > 2) return CMPMC_ERR_INVALID;
+    if (!ctx || form < 0 || form > 3) return CMPMC_ERR_INVALID;
     if (ring_capacity != 0 && (ring_capacity < 64 || (ring_capacity & (ring_capacity - 1)) != 0))
         return fail(ctx, CMPMC_ERR_INVALID, "ring capacity: a power of two, at least 64");
     ctx->pool = form;
     if (ring_capacity) {
-        if (form == 1) ctx->sm_ring_cap = std::max<uint32_t>(ring_capacity, 2048);  // a block appends up to 2 x 768 at once
+        if (form == 1 || form == 3) ctx->sm_ring_cap = std::max<uint32_t>(ring_capacity, 2048);  // a block appends up to 2 x 768 at once
         else ctx->pool_ring_cap = ring_capacity;
     }
     return CMPMC_OK;

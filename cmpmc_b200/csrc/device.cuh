@@ -310,10 +310,15 @@ cudaError_t pool_fp32_occupancy(int block, int* blocks_per_sm);
 // SM-phase pool (one block of sm_pool_threads() threads per SM alternating transport and
 // film phases): `ring` holds ring_cap entries (pool_ring_entry_bytes) per block, `film`
 // film_cap film records (64 B) per block
+// (fp64 = 1: the FP64 comparison form of the same pool, phonon batches without the
+// surrogate; its ring entries and film records are sm_pool_entry_bytes(1) and
+// sm_pool_film_bytes(1) bytes)
 cudaError_t launch_sm_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
                                 uint32_t ring_cap, void* film, uint32_t film_cap, const uint32_t* unit_event,
-                                const QPhonon* queue, int stage_tables, int grid, cudaStream_t s);
+                                const QPhonon* queue, int stage_tables, int fp64, int grid, cudaStream_t s);
 int sm_pool_threads();
+size_t sm_pool_entry_bytes(int fp64);
+size_t sm_pool_film_bytes(int fp64);
 size_t pool_ring_entry_bytes();
 size_t pool_film_bytes_per_warp();
 cudaError_t launch_carrier_event(const uint64_t* ch_off, uint64_t n_events, uint32_t* carrier_event,

@@ -40,9 +40,10 @@ struct FTrack {
 
 // A track of the adjoint kernel also carries its score: the derivative of the log density
 // of every random decision of its lineage so far with respect to log theta_k (k = isotope
-// coefficient, anharmonic coefficient, diffuse fraction, film absorption).
+// coefficient, anharmonic coefficient, diffuse fraction, film absorption). It is summed in
+// FP64: a long lineage adds thousands of free-flight terms.
 struct FTrackA : FTrack {
-    float s[4];
+    double s[4];
 };
 
 template <bool kAdj>
@@ -55,7 +56,7 @@ struct alignas(16) GFTrack {
 };
 struct alignas(16) GFTrackA {
     GFTrack g;
-    float4 s;
+    double s[4];
 };
 template <bool kAdj>
 using EntryOf = typename std::conditional<kAdj, GFTrackA, GFTrack>::type;
@@ -88,7 +89,7 @@ __device__ __forceinline__ void push_track(EntryOf<kAdj>* stk, uint32_t& n, uint
     if constexpr (kAdj) {
         GFTrackA e;
         e.g = g;
-        e.s = make_float4(t.s[0], t.s[1], t.s[2], t.s[3]);
+        for (int i = 0; i < 4; ++i) e.s[i] = t.s[i];
         stk[n++] = e;
     } else {
         stk[n++] = g;
@@ -101,7 +102,7 @@ __device__ __forceinline__ void pop_track(const EntryOf<kAdj>* stk, uint32_t& n,
     if constexpr (kAdj) {
         const GFTrackA e = stk[n];
         g = e.g;
-        t.s[0] = e.s.x; t.s[1] = e.s.y; t.s[2] = e.s.z; t.s[3] = e.s.w;
+        for (int i = 0; i < 4; ++i) t.s[i] = e.s[i];
     } else {
         g = stk[n];
     }
@@ -429,7 +430,7 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
                 trk.bounces = in.bounces;
                 trk.mode = in.mode;
                 if constexpr (kAdj) {
-                    trk.s[0] = trk.s[1] = trk.s[2] = trk.s[3] = 0.0f;
+                    trk.s[0] = trk.s[1] = trk.s[2] = trk.s[3] = 0.0;
                     double* row = adj.prim + unit * kAdjCols;
 #pragma unroll
                     for (int c = 0; c < kAdjCols; ++c) row[c] = 0.0;
@@ -494,8 +495,8 @@ __device__ __forceinline__ void batched_loop(const FLat& L, const Detector& D, c
         if constexpr (kAdj) {
             // free flight: survival exp(-r t) of each theta-dependent channel over the segment
             const float seg = d / trk.vmag;
-            trk.s[0] -= r_iso * seg;
-            trk.s[1] -= r_down * seg;
+            trk.s[0] -= static_cast<double>(r_iso * seg);
+            trk.s[1] -= static_cast<double>(r_down * seg);
         }
         // 0: new isotropic direction (bulk scatter), 1: Lambertian about bh.n, 2: nothing more
         int sample = 2;
@@ -1536,8 +1537,8 @@ constexpr int kSmThreads = 768;
 constexpr int kSmWarps = kSmThreads / 32;
 
 struct SmPoolArgs {
-    PoolPh* ring;            // [blocks][ring_cap]
-    FilmRec* film;           // [blocks][film_cap]
+    void* ring;              // [blocks][ring_cap] entries of the precision's ring type
+    void* film;              // [blocks][film_cap] film records of the precision's type
     uint32_t ring_cap;       // a power of two
     uint32_t film_cap;       // film records per block and phase
     uint32_t film_trigger;   // records that end a transport phase (<= film_cap - kSmThreads)
@@ -1554,97 +1555,142 @@ struct SmShared {
 };
 
 // output of the SM pool's step: reserved in the block's buffers by shared-memory atomics
+template <class Film, class Entry>
 struct SmSink {
     SmShared* sh;
-    FilmRec* fbuf;
-    PoolPh* ring;
+    Film* fbuf;
+    Entry* ring;
     uint32_t film_cap, ring_mask, r_floor;
     unsigned* err;
     const RunArgs* a;
     __device__ __forceinline__ void hit(uint32_t ev, const cmpmc_sensor_hit& h) { stage_hit(*a, ev, h); }
-    __device__ __forceinline__ void film_rec(const FilmRec& r) {
+    __device__ __forceinline__ void film(const Film& r) {
         const uint32_t i = atomicAdd(&sh->f_tail, 1u);
         if (i < film_cap) fbuf[i] = r;
         else *err |= kErrFilmQueue;
     }
-    __device__ __forceinline__ void daughter(const PoolPh& q) {
+    __device__ __forceinline__ void daughter(const Entry& q) {
         const uint32_t i = atomicAdd(&sh->r_tail, 1u);
         if (i + 1u - r_floor <= ring_mask + 1u) ring[i & ring_mask] = q;
         else *err |= kErrQueue;
     }
-    __device__ __forceinline__ void film(const FilmRec& r) { film_rec(r); }
 };
 
-// the film phase of one thread: records from the block's buffer until it is drained
-template <bool kSur, int kKin>
-__device__ __noinline__ void sm_film_phase(const FLat* Lp, const Detector* Dp, const RunArgs* ap,
-                                           const FilmRec* film, uint32_t n_film, SmShared* sh, PoolPh* ring,
-                                           uint32_t ring_mask, uint32_t r_floor, unsigned* err) {
-    const FLat& L = *Lp;
-    const Detector& D = *Dp;
-    const RunArgs& a = *ap;
-    double refl_buf[kKaplanCap];
-    double kwork[4 * kKaplanCap];
-    for (;;) {
-        const uint32_t i = atomicAdd(&sh->f_next, 1u);
-        if (i >= n_film) break;
-        const FilmRec r = film[i];
-        const Surface& s = D.surf[r.surf];
+// the cascade of one film record (from the record's own substream) with its hit and ledger
+// in the record's event; returns the energies to re-emit in refl[0, n_refl) and the record's
+// generator, positioned after the cascade
+template <bool kSur, class Film>
+__device__ __forceinline__ int film_cascade(const Detector& D, const RunArgs& a, const Film& r, double hx, double hy,
+                                            double hz, double* refl_buf, double* kwork, R128& g) {
+    const Surface& s = D.surf[r.surf];
+    int n_refl = 0;
+    double edep;
+    {
+        R128 g_c;
+        g_c.seed(r.key);
+        // the entry step was drawn by the transport step (film_quick): the cascade starts at once
+        if constexpr (kSur) {
+            edep = s.lut_abs ? surrogate_call(&s, r.E, refl_buf, &n_refl, kwork, &g_c)
+                             : kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
+        } else {
+            edep = kaplan_cascade_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
+        }
+        g = g_c;
+    }
+    cmpmc_sim_stats& o = a.ev_stats[r.ev];
+    if (edep > 0.0) {
+        const double wedep = edep * static_cast<double>(r.w);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&o.sensor_hits), 1ull);
+        atomicAdd(&o.total_deposited_eV, wedep);
+        cmpmc_sensor_hit h;
+        h.pos[0] = hx; h.pos[1] = hy; h.pos[2] = hz;
+        h.time = r.t;
+        h.edep = wedep;
+        h.incident_energy = r.E;
+        h.surface_id = r.surf;
+        h.excitation = 0;
+        h.mode = r.mode;
+        h._pad = 0;
+        h.channel_id = r.ch_id;
+        stage_hit(a, r.ev, h);
+    }
+    double sum_refl = 0.0;
+    for (int j = 0; j < n_refl; ++j) sum_refl += refl_buf[j];
+    const double esc = dmax(0.0, r.E - edep - sum_refl) * static_cast<double>(r.w);
+    if (esc != 0.0) atomicAdd(&o.escaped_or_killed_eV, esc);
+    return n_refl;
+}
+
+__device__ __forceinline__ uint64_t reemit_key(uint64_t key, int j) {
+    return mix64(key ^ (0x9e3779b97f4a7c15ULL * static_cast<uint64_t>(j + 1)));
+}
+
+// ---- precision policies of the SM-phase pool ----------------------------------------------
+// PF32: the batched FP32 form (FP32 geometry, directions and table blend; FP64 energy,
+// time and ledger). PF64: the same process in FP64 throughout on the same substreams (the
+// geometry, rates and samplers of the reference's FP64 code, 53-bit uniforms, the
+// reference's 1e-11 m inward nudge, the lattice's own map_k_to_vg in every kinematics
+// mode): the comparison point that isolates what FP32 buys.
+struct PF32 {
+    using Track = FTrack;
+    using Entry = PoolPh;
+    using Film = FilmRec;
+    using Lat = FLat;
+    static constexpr bool kStage = true;
+    __device__ static __forceinline__ void from_entry(const Entry& q, Track& t) {
+        t.pos = f3(q.px, q.py, q.pz);
+        t.k = f3(q.kx, q.ky, q.kz);
+        t.vg = f3(q.vx, q.vy, q.vz);
+        t.vmag = q.vmag;
+        t.w = q.w;
+        t.bounces = q.bounces_mode >> 2;
+        t.mode = static_cast<int>(q.bounces_mode & 3u);
+        t.E = q.E;
+        t.t = q.t;
+    }
+    __device__ static __forceinline__ void from_primary(const cmpmc_phonon_track& in, Track& t) {
+        t.pos = f3(static_cast<float>(in.pos[0]), static_cast<float>(in.pos[1]), static_cast<float>(in.pos[2]));
+        t.k = f3(static_cast<float>(in.k_dir[0]), static_cast<float>(in.k_dir[1]), static_cast<float>(in.k_dir[2]));
+        t.vg = f3(static_cast<float>(in.vg_dir[0]), static_cast<float>(in.vg_dir[1]),
+                  static_cast<float>(in.vg_dir[2]));
+        t.vmag = static_cast<float>(in.vg_mag);
+        t.E = in.energy;
+        t.t = in.time;
+        t.w = static_cast<float>(in.weight);
+        t.bounces = in.bounces;
+        t.mode = in.mode;
+    }
+    template <int kKin>
+    __device__ static __forceinline__ void from_queue(const Lat& L, const QPhonon& q, Track& t) {
+        t.pos = f3(q.px, q.py, q.pz);
+        t.k = f3(q.kx, q.ky, q.kz);
+        t.mode = static_cast<int>(q.mode);
+        const FKin kin = fmapk<kKin>(L, t.mode, t.k);
+        t.vg = kin.dir;
+        t.vmag = kin.mag;
+        t.E = q.E;
+        t.t = q.t;
+        t.w = q.w;
+        t.bounces = q.pad;
+    }
+    template <int kKin, bool kSur, class ST, class Sink>
+    __device__ static __forceinline__ int step(const Lat& L, const float* cdf, const Detector& D, Track& trk, R128& g,
+                                               const ST& st, uint32_t ev, Sink& out) {
+        return pool_step<kKin, kSur>(L, cdf, D, trk, g, st, ev, out);
+    }
+    // one film record of the film phase: cascade, then the re-emissions into the ring
+    template <bool kSur, int kKin>
+    __device__ static __forceinline__ void film_record(const Lat& L, const Detector& D, const RunArgs& a,
+                                                       const Film& r, double* refl_buf, double* kwork, SmShared* sh,
+                                                       Entry* ring, uint32_t ring_mask, uint32_t r_floor,
+                                                       unsigned* err) {
         R128 g;
-        int n_refl = 0;
-        double edep;
-        {
-            R128 g_c;
-            g_c.seed(r.key);
-            // the entry step was drawn by the transport step (film_quick): the cascade starts at once
-            if constexpr (kSur) {
-                edep = s.lut_abs ? surrogate_call(&s, r.E, refl_buf, &n_refl, kwork, &g_c)
-                                 : kaplan_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
-            } else {
-                edep = kaplan_cascade_call(&s.film, r.E, refl_buf, &n_refl, kwork, &g_c);
-            }
-            g = g_c;
-        }
-        cmpmc_sim_stats& o = a.ev_stats[r.ev];
-        if (edep > 0.0) {
-            const double wedep = edep * static_cast<double>(r.w);
-            atomicAdd(reinterpret_cast<unsigned long long*>(&o.sensor_hits), 1ull);
-            atomicAdd(&o.total_deposited_eV, wedep);
-            if (a.keep_hits) {
-                atomicAdd(reinterpret_cast<unsigned long long*>(a.ev_nhits + r.ev), 1ull);
-                // one reservation for the threads of the warp that hit together
-                const unsigned grp = __activemask();
-                const int leader = __ffs(grp) - 1;
-                const int lane = threadIdx.x & 31;
-                unsigned long long base = 0;
-                if (lane == leader) base = atomicAdd(a.hit_count, static_cast<unsigned long long>(__popc(grp)));
-                base = __shfl_sync(grp, base, leader);
-                const unsigned long long idx = base + __popc(grp & lanemask_lt());
-                if (idx < a.hit_cap) {
-                    cmpmc_sensor_hit h;
-                    h.pos[0] = r.px; h.pos[1] = r.py; h.pos[2] = r.pz;
-                    h.time = r.t;
-                    h.edep = wedep;
-                    h.incident_energy = r.E;
-                    h.surface_id = r.surf;
-                    h.excitation = 0;
-                    h.mode = r.mode;
-                    h._pad = 0;
-                    h.channel_id = r.ch_id;
-                    a.hit_stage[idx] = h;
-                    a.hit_key[idx] = r.ev;
-                }
-            }
-        }
-        double sum_refl = 0.0;
-        for (int j = 0; j < n_refl; ++j) sum_refl += refl_buf[j];
-        const double esc = dmax(0.0, r.E - edep - sum_refl) * static_cast<double>(r.w);
-        if (esc != 0.0) atomicAdd(&o.escaped_or_killed_eV, esc);
-        if (n_refl == 0) continue;
+        const int n_refl = film_cascade<kSur>(D, a, r, r.px, r.py, r.pz, refl_buf, kwork, g);
+        if (n_refl == 0) return;
         const uint32_t base = atomicAdd(&sh->r_tail, static_cast<uint32_t>(n_refl));
         if (base + static_cast<uint32_t>(n_refl) - r_floor > ring_mask + 1u) {
             *err |= kErrQueue;
-            continue;
+            return;
         }
         F3 n;
         if (r.surf == 0) n = f3(0.0f, 0.0f, -1.0f);
@@ -1665,28 +1711,432 @@ __device__ __noinline__ void sm_film_phase(const FLat* Lp, const Detector* Dp, c
             t.vmag = kin.mag;
             t.E = refl_buf[j];
             t.bounces = (j == 0) ? r.bounces : 0u;
-            ring[(base + j) & ring_mask] =
-                pool_entry(t, mix64(r.key ^ (0x9e3779b97f4a7c15ULL * static_cast<uint64_t>(j + 1))), r.ev);
+            ring[(base + j) & ring_mask] = pool_entry(t, reemit_key(r.key, j), r.ev);
         }
+    }
+};
+
+// ---- the FP64 policy ----------------------------------------------------------------------
+constexpr double kNudge64 = 1e-11;  // the reference's inward move after a boundary event
+
+struct DTrack {
+    V3 pos, k, vg;
+    double vmag, E, t, w;
+    uint32_t bounces;
+    int mode;
+};
+
+struct alignas(16) PoolPh64 {  // 128 B
+    double px, py, pz, kx, ky, kz, vx, vy, vz, vmag, w, E, t;
+    uint64_t key;
+    uint32_t ev;
+    uint32_t bounces_mode;  // bounces << 2 | mode
+};
+
+struct alignas(16) FilmRec64 {  // 80 B
+    double px, py, pz, w, E, t;
+    uint64_t key;
+    uint32_t ev;
+    int32_t ch_id;
+    uint32_t bounces;
+    uint8_t surf, mode, pad0, pad1;
+};
+
+__device__ __forceinline__ PoolPh64 pool_entry64(const DTrack& t, uint64_t key, uint32_t ev) {
+    PoolPh64 q;
+    q.px = t.pos.x; q.py = t.pos.y; q.pz = t.pos.z;
+    q.kx = t.k.x; q.ky = t.k.y; q.kz = t.k.z;
+    q.vx = t.vg.x; q.vy = t.vg.y; q.vz = t.vg.z;
+    q.vmag = t.vmag;
+    q.w = t.w;
+    q.E = t.E;
+    q.t = t.t;
+    q.key = key;
+    q.ev = ev;
+    q.bounces_mode = (t.bounces << 2) | static_cast<uint32_t>(t.mode);
+    return q;
+}
+
+// the reference's samplers (rng.hpp:78-96, phonon_kernels.hpp:53-63, crystal_lattice.hpp:200-212)
+// on a substream's 53-bit uniforms
+__device__ __forceinline__ V3 iso_dir64(R128& g) {
+    const double cos_theta = 2.0 * g.uniform() - 1.0;
+    const double sin_theta = sqrt(dmax(0.0, 1.0 - cos_theta * cos_theta));
+    double s, c;
+    sincos(kTwoPi * g.uniform(), &s, &c);
+    return v3(sin_theta * c, sin_theta * s, cos_theta);
+}
+__device__ __forceinline__ V3 lambert_dir64(V3 n, R128& g) {
+    double s, c;
+    sincos(kTwoPi * g.uniform(), &s, &c);
+    const double sin_theta = sqrt(g.uniform());
+    const double cos_theta = sqrt(dmax(0.0, 1.0 - sin_theta * sin_theta));
+    const V3 u = orthogonal_unit(n);
+    const V3 v = cross(n, u);
+    return unit(u * (sin_theta * c) + v * (sin_theta * s) + n * cos_theta);
+}
+__device__ __forceinline__ int dos64(const Lattice& L, double u) {
+    return (u < L.fLDOS) ? 0 : ((u < L.fLDOS + L.fSTDOS) ? 2 : 1);
+}
+__device__ __forceinline__ int trans64(const Lattice& L, R128& g) {
+    return (g.uniform() < L.fSTDOS / (L.fSTDOS + L.fFTDOS)) ? 2 : 1;
+}
+__device__ __forceinline__ double cdf64(const double* cdf, R128& g) {
+    const double u = g.uniform() * (kNCdf - 1);
+    const int i = imin(static_cast<int>(u), kNCdf - 2);
+    const double f = u - i;
+    return cdf[i] * (1.0 - f) + cdf[i + 1] * f;
+}
+// SimulationEngine::sample_inward_wavevector (engine.hpp:927-936)
+__device__ __noinline__ V3 inward64(const Lattice* Lp, int mode, V3 n, R128* gp, Kin* kin) {
+    for (int trial = 0; trial < 16; ++trial) {
+        const V3 kd = lambert_dir64(n, *gp);
+        *kin = map_k_to_vg(*Lp, mode, kd);
+        if (dot(kin->vg_dir, n) > 1e-6) return kd;
+    }
+    *kin = map_k_to_vg(*Lp, mode, n);
+    return n;
+}
+__device__ __noinline__ Kin map64_call(const Lattice* Lp, int mode, V3 k) { return map_k_to_vg(*Lp, mode, k); }
+
+// anharmonic decay of an L phonon (engine.hpp:938-988) in FP64; the daughter goes to *dp
+template <class ST>
+__device__ __noinline__ void decay64(const Lattice* Lp, DTrack* tp, DTrack* dp, const ST* st, R128* gp) {
+    const Lattice& L = *Lp;
+    DTrack& trk = *tp;
+    R128& g = *gp;
+    const V3 d1 = trk.k;
+    const V3 perp = orthogonal_unit(d1);
+    const double phi = kTwoPi * g.uniform();
+    double sp, cp;
+    sincos(phi, &sp, &cp);
+    double x, th1, th2;
+    int m1, m2;
+    if (g.uniform() < L.fTT_frac) {
+        ++st->tt();
+        x = cdf64(L.cdf_tt, g);
+        th1 = decay_angle_TT(x, L.v_sound, L.v_trans);
+        th2 = decay_angle_TT(1.0 - x, L.v_sound, L.v_trans);
+        m1 = trans64(L, g);
+        m2 = trans64(L, g);
+    } else {
+        ++st->lt();
+        x = cdf64(L.cdf_lt, g);
+        th1 = decay_angle_L_to_LT(x, L.v_sound, L.v_trans);
+        th2 = decay_angle_T_from_LT(x, L.v_sound, L.v_trans);
+        m1 = 0;
+        m2 = trans64(L, g);
+    }
+    double s1, c1, s2, c2;
+    sincos(th1, &s1, &c1);
+    sincos(-th2, &s2, &c2);
+    const V3 k1 = unit(rotate_around(rotate_around(d1, perp, c1, s1), d1, cp, sp));
+    const V3 k2 = unit(rotate_around(rotate_around(d1, perp, c2, s2), d1, cp, sp));
+    DTrack& d = *dp;
+    d.pos = trk.pos;
+    d.k = k2;
+    const Kin kin2 = map_k_to_vg(L, m2, k2);
+    d.vg = kin2.vg_dir;
+    d.vmag = kin2.vg_mag;
+    d.E = (1.0 - x) * trk.E;
+    d.t = trk.t;
+    d.w = trk.w;
+    d.bounces = 0;
+    d.mode = m2;
+    trk.E = x * trk.E;
+    trk.mode = m1;
+    trk.k = k1;
+    const Kin kin = map_k_to_vg(L, m1, k1);
+    trk.vg = kin.vg_dir;
+    trk.vmag = kin.vg_mag;
+}
+
+// one transport step in FP64: the branches and draws of pool_step
+template <bool kSur, class ST, class Sink>
+__device__ __forceinline__ int pool_step64(const Lattice& L, const Detector& D, DTrack& trk, R128& g, const ST& st,
+                                           uint32_t ev, Sink& out) {
+    if (trk.E < D.min_phonon_eV || trk.bounces >= D.max_bounces) {
+        ++st.killed();
+        st.esc() += trk.E * trk.w;
+        return kStepEnd;
+    }
+    if (D.rr_bounces != 0 && trk.bounces > D.rr_bounces && (trk.bounces - D.rr_bounces) % 32 == 0) {
+        if (g.uniform() < D.rr_survival) {
+            trk.w /= D.rr_survival;
+        } else {
+            ++st.killed();
+            return kStepEnd;
+        }
+    }
+    ++st.steps();
+    const double r_iso = isotope_rate(L, trk.E);
+    const double r_poly = polycrystal_rate(L, trk.vmag);
+    const double r_down = downconversion_rate(L, trk.mode, trk.E);
+    const double r_tot = r_iso + r_poly + r_down;
+    const double d_phys = (r_tot > 1e-12) ? (-log(g.uniform()) * trk.vmag / r_tot) : kInf;
+    const BHit bh = intersect_exit(D.radius, D.half_z, trk.pos, trk.vg);
+    const bool bulk = d_phys < bh.distance;
+    const double d = bulk ? d_phys : bh.distance;
+    trk.pos = trk.pos + trk.vg * d;
+    trk.t += d / trk.vmag;
+    int sample = 2;  // 0: isotropic, 1: Lambertian about bh.n_in, 2: nothing more
+    if (bulk) {
+        const double u_proc = g.uniform() * r_tot;
+        if (r_down > 0.0 && u_proc < r_down) {
+            DTrack t_c = trk, d_c;
+            R128 g_c = g;
+            decay64(&L, &t_c, &d_c, &st, &g_c);
+            trk = t_c;
+            g = g_c;
+            out.daughter(pool_entry64(d_c, draw_key(g), ev));
+        } else {
+            if (u_proc < r_down + r_iso) ++st.iso();
+            else ++st.poly();
+            trk.mode = dos64(L, g.uniform());
+            sample = 0;
+        }
+    } else {
+        const V3 n = bh.n_in;
+        trk.bounces++;
+        const Surface& s = D.surf[bh.surf];
+        bool enter = false;
+        int ch_id = -1;
+        bool active_pad = true;
+        if (s.n_pads > 0) {
+            R128 g_c = g;
+            ch_id = mask_call(s.pads, s.n_pads, static_cast<float>(trk.pos.x), static_cast<float>(trk.pos.y), &g_c);
+            g = g_c;
+            active_pad = ch_id >= 0;
+        }
+        if (active_pad && s.has_film && g.uniform() < s.prob_abs) {
+            const double p_enter = s.has_amm ? amm_transmission(s.amm_sub, s.amm_film, trk.mode == 0, dot(trk.k, n))
+                                             : s.film.film_absorption;
+            enter = g.uniform() < p_enter;
+        }
+        if (enter) {
+            R128 g_c = g;
+            const int film = film_quick<kSur>(&s.film, trk.E, &g_c);
+            g = g_c;
+            if (film == kFilmAbsorbed) {
+                const double wedep = trk.E * trk.w;
+                ++st.hits();
+                st.dep() += wedep;
+                cmpmc_sensor_hit h;
+                h.pos[0] = trk.pos.x; h.pos[1] = trk.pos.y; h.pos[2] = trk.pos.z;
+                h.time = trk.t;
+                h.edep = wedep;
+                h.incident_energy = trk.E;
+                h.surface_id = static_cast<uint8_t>(bh.surf);
+                h.excitation = 0;
+                h.mode = static_cast<uint8_t>(trk.mode);
+                h._pad = 0;
+                h.channel_id = ch_id;
+                out.hit(ev, h);
+                return kStepEnd;
+            }
+            if (film == kFilmCascade) {
+                FilmRec64 fr;
+                fr.px = trk.pos.x; fr.py = trk.pos.y; fr.pz = trk.pos.z;
+                fr.w = trk.w;
+                fr.E = trk.E;
+                fr.t = trk.t;
+                fr.key = draw_key(g);
+                fr.ev = ev;
+                fr.ch_id = ch_id;
+                fr.bounces = trk.bounces;
+                fr.surf = static_cast<uint8_t>(bh.surf);
+                fr.mode = static_cast<uint8_t>(trk.mode);
+                fr.pad0 = fr.pad1 = 0;
+                out.film(fr);
+                return kStepFilm;
+            }
+            trk.pos = trk.pos + n * kNudge64;
+            trk.mode = dos64(L, g.uniform());
+            sample = 1;
+        } else if (g.uniform() > s.prob_refl) {
+            ++st.killed();
+            st.esc() += trk.E * trk.w;
+            return kStepEnd;
+        }
+        if (!enter) {
+            ++st.refl();
+            trk.pos = trk.pos + n * kNudge64;
+            const Split sp = reflection_split(s, trk.E);
+            const double u_refl = g.uniform();
+            if (u_refl < sp.p_anh) {
+                ++st.down();
+                const bool tt = g.uniform() < L.fTT_frac;
+                const double x = cdf64(tt ? L.cdf_tt : L.cdf_lt, g);
+                const int m1 = tt ? trans64(L, g) : 0;
+                const int m2 = trans64(L, g);
+                DTrack dtr;
+                Kin k2kin;
+                R128 g_c = g;
+                dtr.k = inward64(&L, m2, n, &g_c, &k2kin);
+                g = g_c;
+                dtr.pos = trk.pos;
+                dtr.vg = k2kin.vg_dir;
+                dtr.vmag = k2kin.vg_mag;
+                dtr.E = (1.0 - x) * trk.E;
+                dtr.t = trk.t;
+                dtr.w = trk.w;
+                dtr.bounces = 0;
+                dtr.mode = m2;
+                out.daughter(pool_entry64(dtr, draw_key(g), ev));
+                trk.E = x * trk.E;
+                trk.mode = m1;
+                sample = 1;
+            } else if (u_refl < sp.p_anh + sp.p_spec) {
+                V3 kr = trk.k - n * (2.0 * dot(trk.k, n));
+                Kin kin = map64_call(&L, trk.mode, kr);
+                if (dot(kin.vg_dir, n) <= 1e-6) {
+                    R128 g_c = g;
+                    kr = inward64(&L, trk.mode, n, &g_c, &kin);
+                    g = g_c;
+                }
+                trk.k = kr;
+                trk.vg = kin.vg_dir;
+                trk.vmag = kin.vg_mag;
+            } else {
+                sample = 1;
+            }
+        }
+        if (sample == 1) {
+            Kin kin;
+            R128 g_c = g;
+            trk.k = inward64(&L, trk.mode, n, &g_c, &kin);
+            g = g_c;
+            trk.vg = kin.vg_dir;
+            trk.vmag = kin.vg_mag;
+        }
+        return kStepOn;
+    }
+    if (sample == 0) {
+        trk.k = iso_dir64(g);
+        const Kin kin = map_k_to_vg(L, trk.mode, trk.k);
+        trk.vg = kin.vg_dir;
+        trk.vmag = kin.vg_mag;
+    }
+    return kStepOn;
+}
+
+struct PF64 {
+    using Track = DTrack;
+    using Entry = PoolPh64;
+    using Film = FilmRec64;
+    using Lat = Lattice;
+    static constexpr bool kStage = false;
+    __device__ static __forceinline__ void from_entry(const Entry& q, Track& t) {
+        t.pos = v3(q.px, q.py, q.pz);
+        t.k = v3(q.kx, q.ky, q.kz);
+        t.vg = v3(q.vx, q.vy, q.vz);
+        t.vmag = q.vmag;
+        t.w = q.w;
+        t.bounces = q.bounces_mode >> 2;
+        t.mode = static_cast<int>(q.bounces_mode & 3u);
+        t.E = q.E;
+        t.t = q.t;
+    }
+    __device__ static __forceinline__ void from_primary(const cmpmc_phonon_track& in, Track& t) {
+        t.pos = v3(in.pos[0], in.pos[1], in.pos[2]);
+        t.k = v3(in.k_dir[0], in.k_dir[1], in.k_dir[2]);
+        t.vg = v3(in.vg_dir[0], in.vg_dir[1], in.vg_dir[2]);
+        t.vmag = in.vg_mag;
+        t.E = in.energy;
+        t.t = in.time;
+        t.w = in.weight;
+        t.bounces = in.bounces;
+        t.mode = in.mode;
+    }
+    template <int kKin>
+    __device__ static __forceinline__ void from_queue(const Lat& L, const QPhonon& q, Track& t) {
+        t.pos = v3(q.px, q.py, q.pz);
+        t.k = v3(q.kx, q.ky, q.kz);
+        t.mode = static_cast<int>(q.mode);
+        const Kin kin = map64_call(&L, t.mode, t.k);
+        t.vg = kin.vg_dir;
+        t.vmag = kin.vg_mag;
+        t.E = q.E;
+        t.t = q.t;
+        t.w = q.w;
+        t.bounces = q.pad;
+    }
+    template <int kKin, bool kSur, class ST, class Sink>
+    __device__ static __forceinline__ int step(const Lat& L, const float*, const Detector& D, Track& trk, R128& g,
+                                               const ST& st, uint32_t ev, Sink& out) {
+        return pool_step64<kSur>(L, D, trk, g, st, ev, out);
+    }
+    template <bool kSur, int kKin>
+    __device__ static __forceinline__ void film_record(const Lat& L, const Detector& D, const RunArgs& a,
+                                                       const Film& r, double* refl_buf, double* kwork, SmShared* sh,
+                                                       Entry* ring, uint32_t ring_mask, uint32_t r_floor,
+                                                       unsigned* err) {
+        R128 g;
+        const int n_refl = film_cascade<kSur>(D, a, r, r.px, r.py, r.pz, refl_buf, kwork, g);
+        if (n_refl == 0) return;
+        const uint32_t base = atomicAdd(&sh->r_tail, static_cast<uint32_t>(n_refl));
+        if (base + static_cast<uint32_t>(n_refl) - r_floor > ring_mask + 1u) {
+            *err |= kErrQueue;
+            return;
+        }
+        V3 n;
+        if (r.surf == 0) n = v3(0.0, 0.0, -1.0);
+        else if (r.surf == 1) n = v3(0.0, 0.0, 1.0);
+        else {
+            const double rr = m_hypot(r.px, r.py);
+            n = (rr > 1e-15) ? v3(-r.px / rr, -r.py / rr, 0.0) : v3(-1.0, 0.0, 0.0);
+        }
+        DTrack t;
+        t.pos = v3(r.px, r.py, r.pz) + n * kNudge64;
+        t.t = r.t;
+        t.w = r.w;
+        for (int j = 0; j < n_refl; ++j) {
+            t.mode = dos64(L, g.uniform());
+            Kin kin;
+            t.k = inward64(&L, t.mode, n, &g, &kin);
+            t.vg = kin.vg_dir;
+            t.vmag = kin.vg_mag;
+            t.E = refl_buf[j];
+            t.bounces = (j == 0) ? r.bounces : 0u;
+            ring[(base + j) & ring_mask] = pool_entry64(t, reemit_key(r.key, j), r.ev);
+        }
+    }
+};
+
+// the film phase of one thread: records from the block's buffer until it is drained
+template <class P, bool kSur, int kKin>
+__device__ __noinline__ void sm_film_phase(const typename P::Lat* Lp, const Detector* Dp, const RunArgs* ap,
+                                           const typename P::Film* film, uint32_t n_film, SmShared* sh,
+                                           typename P::Entry* ring, uint32_t ring_mask, uint32_t r_floor,
+                                           unsigned* err) {
+    double refl_buf[kKaplanCap];
+    double kwork[4 * kKaplanCap];
+    for (;;) {
+        const uint32_t i = atomicAdd(&sh->f_next, 1u);
+        if (i >= n_film) break;
+        const typename P::Film r = film[i];
+        P::template film_record<kSur, kKin>(*Lp, *Dp, *ap, r, refl_buf, kwork, sh, ring, ring_mask, r_floor, err);
     }
 }
 
-template <bool kSur, int kKin = 0, bool kQueue = false>
-__global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_constant__ FLat L,
-                                                                const __grid_constant__ Detector D,
-                                                                const __grid_constant__ RunArgs a,
-                                                                const __grid_constant__ SmPoolArgs p) {
+template <class P, bool kSur, int kKin = 0, bool kQueue = false>
+__global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool(const __grid_constant__ typename P::Lat L,
+                                                           const __grid_constant__ Detector D,
+                                                           const __grid_constant__ RunArgs a,
+                                                           const __grid_constant__ SmPoolArgs p) {
+    using Entry = typename P::Entry;
+    using Film = typename P::Film;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     __shared__ uint32_t s_cnt[kSmWarps][kNCnt][32];
     __shared__ double s_led[kSmWarps][2][32];
-    __shared__ alignas(128) float s_cdf[2 * kNCdf];  // the decay CDF tables (L-LT, then TT)
+    __shared__ alignas(128) float s_cdf[P::kStage ? 2 * kNCdf : 4];  // decay CDF tables (L-LT, then TT)
     __shared__ alignas(8) uint64_t s_bar;
     __shared__ SmShared sh;
     const UStatsT<32> st{&s_cnt[wid][0][lane], &s_led[wid][0][lane]};
-    PoolPh* ring = p.ring + static_cast<uint64_t>(blockIdx.x) * p.ring_cap;
-    FilmRec* film = p.film + static_cast<uint64_t>(blockIdx.x) * p.film_cap;
+    Entry* ring = static_cast<Entry*>(p.ring) + static_cast<uint64_t>(blockIdx.x) * p.ring_cap;
+    Film* film = static_cast<Film*>(p.film) + static_cast<uint64_t>(blockIdx.x) * p.film_cap;
     const uint32_t ring_mask = p.ring_cap - 1;
     if (threadIdx.x == 0) {
         sh.r_head = sh.r_tail = sh.r_pub = 0;
@@ -1694,18 +2144,21 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_con
         sh.input_left = 1;
         sh.n_dry = 0;
     }
-    const float* cdf = L.cdf_lt;  // the two tables are contiguous in global memory
-    if (p.stage_tables) {  // (stage_bulk synchronizes the block)
-        if (!stage_bulk(s_cdf, L.cdf_lt, 2 * kNCdf * sizeof(float), &s_bar)) {
-            if (threadIdx.x == 0) atomicOr(a.err, kErrStage);
-            return;
+    const float* cdf = nullptr;
+    if constexpr (P::kStage) {
+        cdf = L.cdf_lt;  // the two tables are contiguous in global memory
+        if (p.stage_tables) {  // (stage_bulk synchronizes the block)
+            if (!stage_bulk(s_cdf, L.cdf_lt, 2 * kNCdf * sizeof(float), &s_bar)) {
+                if (threadIdx.x == 0) atomicOr(a.err, kErrStage);
+                return;
+            }
+            cdf = s_cdf;
         }
-        cdf = s_cdf;
     }
     __syncthreads();
     const uint64_t seed_key = mix64(a.seed ^ 0x5851f42d4c957f2dULL);
     volatile SmShared* vsh = &sh;
-    FTrack trk;
+    typename P::Track trk;
     R128 g;
     uint32_t ev_cur = 0;
     bool live = false;
@@ -1714,7 +2167,7 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_con
         // ---- transport phase --------------------------------------------------------
         const uint32_t r_floor = vsh->r_head;  // ring slots below it are free
         const uint32_t r_pub = vsh->r_pub;
-        SmSink sink{&sh, film, ring, p.film_cap, ring_mask, r_floor, &err, &a};
+        SmSink<Film, Entry> sink{&sh, film, ring, p.film_cap, ring_mask, r_floor, &err, &a};
         for (;;) {
             uint32_t ft = 0, inp = 0, dry = 0;
             if (lane == 0) {
@@ -1740,16 +2193,8 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_con
                 base = __shfl_sync(full, base, 0);
                 got = __shfl_sync(full, got, 0);
                 if (!live && rank < static_cast<int>(got)) {
-                    const PoolPh q = ring[(base + rank) & ring_mask];
-                    trk.pos = f3(q.px, q.py, q.pz);
-                    trk.k = f3(q.kx, q.ky, q.kz);
-                    trk.vg = f3(q.vx, q.vy, q.vz);
-                    trk.vmag = q.vmag;
-                    trk.w = q.w;
-                    trk.bounces = q.bounces_mode >> 2;
-                    trk.mode = static_cast<int>(q.bounces_mode & 3u);
-                    trk.E = q.E;
-                    trk.t = q.t;
+                    const Entry q = ring[(base + rank) & ring_mask];
+                    P::from_entry(q, trk);
                     g.seed(q.key);
                     ev_cur = q.ev;
                     st.clear();
@@ -1770,16 +2215,7 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_con
                             if (q.ev != kQEmpty) {
                                 ev_cur = q.ev;
                                 g.seed(q.key);
-                                trk.pos = f3(q.px, q.py, q.pz);
-                                trk.k = f3(q.kx, q.ky, q.kz);
-                                trk.mode = static_cast<int>(q.mode);
-                                const FKin kin = fmapk<kKin>(L, trk.mode, trk.k);
-                                trk.vg = kin.dir;
-                                trk.vmag = kin.mag;
-                                trk.E = q.E;
-                                trk.t = q.t;
-                                trk.w = q.w;
-                                trk.bounces = q.pad;
+                                P::template from_queue<kKin>(L, q, trk);
                                 st.clear();
                                 live = true;
                             }
@@ -1788,19 +2224,7 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_con
                             ev_cur = ev;
                             const uint64_t j = unit - a.ph_off[ev];
                             g.seed(seed_key ^ mix64(((a.first_event + ev) << 20) | j));
-                            const cmpmc_phonon_track& in = a.ph[unit];
-                            trk.pos = f3(static_cast<float>(in.pos[0]), static_cast<float>(in.pos[1]),
-                                         static_cast<float>(in.pos[2]));
-                            trk.k = f3(static_cast<float>(in.k_dir[0]), static_cast<float>(in.k_dir[1]),
-                                       static_cast<float>(in.k_dir[2]));
-                            trk.vg = f3(static_cast<float>(in.vg_dir[0]), static_cast<float>(in.vg_dir[1]),
-                                        static_cast<float>(in.vg_dir[2]));
-                            trk.vmag = static_cast<float>(in.vg_mag);
-                            trk.E = in.energy;
-                            trk.t = in.time;
-                            trk.w = static_cast<float>(in.weight);
-                            trk.bounces = in.bounces;
-                            trk.mode = in.mode;
+                            P::from_primary(a.ph[unit], trk);
                             st.clear();
                             live = true;
                         }
@@ -1812,7 +2236,7 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_con
                 break;
             }
             if (live) {
-                const int outcome = pool_step<kKin, kSur>(L, cdf, D, trk, g, st, ev_cur, sink);
+                const int outcome = P::template step<kKin, kSur>(L, cdf, D, trk, g, st, ev_cur, sink);
                 if (outcome != kStepOn) {
                     sink_unit(&a, ev_cur, st);
                     live = false;
@@ -1822,7 +2246,7 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool_fp32(const __grid_con
         __syncthreads();
         // ---- film phase -------------------------------------------------------------
         const uint32_t n_film = min(vsh->f_tail, p.film_cap);
-        if (n_film) sm_film_phase<kSur, kKin>(&L, &D, &a, film, n_film, &sh, ring, ring_mask, r_floor, &err);
+        if (n_film) sm_film_phase<P, kSur, kKin>(&L, &D, &a, film, n_film, &sh, ring, ring_mask, r_floor, &err);
         __syncthreads();
         // ---- boundary: publish what the phases appended ---------------------------------
         if (threadIdx.x == 0) {
@@ -1948,31 +2372,39 @@ cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detecto
 
 cudaError_t launch_sm_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
                                 uint32_t ring_cap, void* film, uint32_t film_cap, const uint32_t* unit_event,
-                                const QPhonon* queue, int stage_tables, int grid, cudaStream_t s) {
+                                const QPhonon* queue, int stage_tables, int fp64, int grid, cudaStream_t s) {
     // the ring is indexed by masking: its capacity must be a power of two
     if (ring_cap < 2u * kSmThreads || (ring_cap & (ring_cap - 1u)) != 0 || film_cap < 4u * kSmThreads)
         return cudaErrorInvalidValue;
-    const FLat f = make_flat(L, cdf_f, D);
     SmPoolArgs p;
-    p.ring = static_cast<PoolPh*>(ring);
-    p.film = static_cast<FilmRec*>(film);
+    p.ring = ring;
+    p.film = film;
     p.ring_cap = ring_cap;
     p.film_cap = film_cap;
     p.film_trigger = film_cap > 2u * kSmThreads ? film_cap - 2u * kSmThreads : film_cap / 2u;
     p.unit_event = unit_event;
     p.queue = queue;
     p.stage_tables = stage_tables;
+    if (fp64) {  // the FP64 comparison form: phonon batches, every kinematics mode, full cascades
+        if (queue || a.surrogate) return cudaErrorInvalidValue;
+        k_sm_pool<PF64, false><<<grid, kSmThreads, 0, s>>>(L, D, a, p);
+        return cudaGetLastError();
+    }
+    const FLat f = make_flat(L, cdf_f, D);
     if (queue) {
-        if (L.kin_mode != kKinOctahedral) k_sm_pool_fp32<false, 1, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
-        else if (a.surrogate) k_sm_pool_fp32<true, 0, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
-        else k_sm_pool_fp32<false, 0, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        if (L.kin_mode != kKinOctahedral) k_sm_pool<PF32, false, 1, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        else if (a.surrogate) k_sm_pool<PF32, true, 0, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        else k_sm_pool<PF32, false, 0, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
     } else {
-        if (L.kin_mode != kKinOctahedral) k_sm_pool_fp32<false, 1><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
-        else if (a.surrogate) k_sm_pool_fp32<true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
-        else k_sm_pool_fp32<false><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        if (L.kin_mode != kKinOctahedral) k_sm_pool<PF32, false, 1><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        else if (a.surrogate) k_sm_pool<PF32, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        else k_sm_pool<PF32, false><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
     }
     return cudaGetLastError();
 }
+
+size_t sm_pool_entry_bytes(int fp64) { return fp64 ? sizeof(PoolPh64) : sizeof(PoolPh); }
+size_t sm_pool_film_bytes(int fp64) { return fp64 ? sizeof(FilmRec64) : sizeof(FilmRec); }
 
 int sm_pool_threads() { return kSmThreads; }
 

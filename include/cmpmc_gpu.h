@@ -533,12 +533,17 @@ int cmpmc_gpu_configure_phases(cmpmc_gpu_ctx* ctx, uint32_t phase_steps);
  *   refilled from the block's ring of pending phonons and the batch's primaries; film
  *   entries and daughters appended to block buffers) and a film phase (every thread runs
  *   the waiting film cascades, their re-emissions appended to the ring), so an SM runs one
- *   code path at a time; ring_capacity: pending phonons per block (default 2^15).
+ *   code path at a time; ring_capacity: pending phonons per block (default 2^17).
  * form = 2: the warp pool, one persistent launch in which every warp runs its own film
  *   cascades between its transport steps; ring_capacity: pending phonons per warp (default
  *   1024).
  * form = 0: the host-driven form, alternating transport and film launches until both device
  *   queues are empty (one host round trip per round; configure_phases applies to it only).
+ * form = 3: the SM-phase pool computed in FP64 throughout (geometry, directions, rates and
+ *   samplers of the plain form, 53-bit uniforms, the reference's 1e-11 m inward nudge) on
+ *   the same substreams as form 1: the comparison point that shows what the FP32 form
+ *   gains. Phonon-only batches with full film cascades (CMPMC_ERR_INVALID with charges or
+ *   the Kaplan surrogate); ring entries 128 B, film records 80 B.
  * Rings are 80 B per entry; a ring (a power of two >= 64; 0 keeps the current value) that
  * overflows is grown 4x and the call rerun. All forms sample the same process; a daughter
  * runs on a substream drawn from its parent's in the pool forms, on the parent's own stream

@@ -292,3 +292,52 @@ def test_pool_forms_give_the_same_hits(ge_lattice, form, ring):
     for name in a.event_stats.dtype.names:
         if a.event_stats.dtype[name].kind == "u":
             assert np.array_equal(a.event_stats[name], b.event_stats[name]), name
+
+
+@pytest.mark.parametrize("wl,n", [("c1", 2000), ("c0x", 1000), ("c0m", 1000)])
+def test_fp64_pool_statistics(ge_lattice, wl, n):
+    """Pool form 3 (the SM-phase pool computed in FP64 throughout, on the FP32 pool's
+    substreams) against the plain FP64 form (identical to the reference event by event) on
+    the mixed-energy, Exact-kinematics and electrode-mask workloads, and against the FP32
+    pool: hit histograms chi^2 p > 0.01, the same deposited fraction within 1 %, the ledgers
+    closed."""
+    import cmpmc_b200 as cm
+    from tests.helpers import lattice_for
+    eng = cm.SimulationEngine(lattice_for(wl, ge_lattice), detector_for(wl))
+    plain = cm.run_events(eng, n, workload_of(wl), cm.RunOptions(seed=WORKLOAD_SEED[wl]))
+    f32 = _batched(eng, wl, n)
+    eng64 = cm.SimulationEngine(lattice_for(wl, ge_lattice), detector_for(wl))
+    eng64.configure_pool(3)
+    f64 = _batched(eng64, wl, n)
+    lo = min(r.hits["edep"].min() for r in (plain, f32, f64))
+    hi = max(r.hits["edep"].max() for r in (plain, f32, f64)) * (1 + 1e-9)
+    h = {k: event_histograms(r.hit_offsets, r.hits, (lo, hi)) for k, r in
+         (("plain", plain), ("f32", f32), ("f64", f64))}
+    for other in ("plain", "f32"):
+        for name in ("time", "radius", "edep"):
+            c2, dof, p = hist_chi2(h["f64"], h[other], name)
+            print(f"{wl} fp64 pool vs {other} {name}: chi2 {c2:.1f} dof {dof} p {p:.3f}")
+            assert p > P_MIN, (other, name, c2, dof, p)
+    for st in (f32.stats, f64.stats):
+        assert abs(st.total_injected_eV - st.total_deposited_eV - st.escaped_or_killed_eV) <= \
+            LEDGER_TOL * st.total_injected_eV
+    fp = plain.stats.total_deposited_eV / plain.stats.total_injected_eV
+    f6 = f64.stats.total_deposited_eV / f64.stats.total_injected_eV
+    assert abs(f6 / fp - 1.0) < 0.01
+    assert f64.stats.total_injected_eV == f32.stats.total_injected_eV
+
+
+def test_fp64_pool_refuses_charges_and_the_surrogate(ge_lattice):
+    """The FP64 pool form runs phonon-only batches with full film cascades: a batch with
+    charges and a surrogate run are refused with an error, not run in another form."""
+    import cmpmc_b200 as cm
+    eng = _engine(ge_lattice, "c2")
+    eng.configure_pool(3)
+    with pytest.raises(cm.CmpmcError):
+        _batched(eng, "c2", 4)
+    eng = _engine(ge_lattice, "c1")
+    eng.configure_pool(3)
+    with pytest.raises(cm.CmpmcError):
+        eng.run_packed(eng.generate(workload_of("c1"), 8, 7),
+                       cm.RunOptions(seed=1, form="batched_fp32", kaplan_surrogate=True))
+    eng.run_packed(eng.generate(workload_of("c1"), 8, 7), cm.RunOptions(seed=1, form="batched_fp32"))
