@@ -14,7 +14,10 @@ from the library's autotuner (results do not depend on it).
   value  primary phonon tracks / s, inputs resident on the device, device-timed (CUDA
          events on the library's stream), max over ranks
   e2e    the same through the public API with host buffers: pinned host inputs copied in
-         and every hit, the hit offsets and the statistics copied back, each step
+         and every hit, the hit offsets and the statistics copied back, each step. On one
+         GPU two calls are kept in flight (two contexts on two host threads, wall clock over
+         the K steps), so one call's copies overlap the other's transport;
+         e2e_one_call_at_a_time is the same with one call at a time
          (e2e_with_generator adds the host generator's time per step)
   plain_fp64  the plain FP64 form (bit-exact event streams) on the same workload, one step
   batched_fp64  the same SM-phase pool computed in FP64 throughout on the same substreams
@@ -45,6 +48,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -298,6 +302,8 @@ def main() -> None:
     ap.add_argument("--launch", default="sm_pool", choices=["sm_pool", "warp_pool", "rounds"],
                     help="launch form of the batched phonon transport")
     ap.add_argument("--no-matched", action="store_true", help="skip the matched-statistics check")
+    ap.add_argument("--no-pipeline", action="store_true",
+                    help="e2e with one call at a time only (no second context in flight)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the batched FP64 comparison step")
     ap.add_argument("--recoil", type=int, default=0,
                     help="instead of the headline line: time the recoil batch of this many events once")
@@ -371,14 +377,17 @@ def main() -> None:
             d.rng_state, d.injected_eV, d.phonon_offsets, d.phonons = host
         return d
 
-    def run(d):
+    def run_on(hh, d):
         out = _ffi.RunOutC()
-        st = lib.cmpmc_gpu_run_events(h, C.byref(d), C.byref(out))
+        st = lib.cmpmc_gpu_run_events(hh, C.byref(d), C.byref(out))
         if st != 0:
             buf = C.create_string_buffer(512)
-            lib.cmpmc_gpu_last_error(h, buf, 512)
+            lib.cmpmc_gpu_last_error(hh, buf, 512)
             raise RuntimeError(buf.value.decode())
         return out
+
+    def run(d):
+        return run_on(h, d)
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")  # 256 MiB > 126 MB L2
 
@@ -502,6 +511,48 @@ def main() -> None:
     if world == 1:
         d2h = int(o.n_hits) * 56 + (args.events + 1) * 8 + 208
 
+    # e2e with two calls in flight: a second context (its own stream, device buffers and pinned
+    # output buffers) on a second host thread, the K steps taken in turn from a shared counter,
+    # so that one call's input and hit copies run while the other call's transport runs; every
+    # step still copies its inputs in and its hits, offsets and totals out
+    e2e_pipe = None
+    if world == 1 and not args.no_pipeline:
+        eng_b = cm.SimulationEngine(lat, det)
+        h_b = eng_b.context(dev)
+        if args.queue_capacity or args.stack_capacity:
+            eng_b.configure(dev, stack_capacity=args.stack_capacity, queue_capacity=args.queue_capacity)
+        eng_b.configure_pool({"sm_pool": 1, "warp_pool": 2, "rounds": 0}[args.launch], device=dev)
+        run_on(h_b, hd)  # sizes the second context's buffers
+        lock = threading.Lock()
+        left = [args.steps]
+        errors = []
+
+        def worker(hh):
+            while True:
+                with lock:
+                    if left[0] == 0:
+                        return
+                    left[0] -= 1
+                try:
+                    run_on(hh, hd)
+                except Exception as e:  # reported after the join
+                    errors.append(e)
+                    return
+        torch.cuda.synchronize(dev)
+        t1 = time.perf_counter()
+        threads = [threading.Thread(target=worker, args=(x,)) for x in (h, h_b)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        wall_pipe = time.perf_counter() - t1
+        if errors:
+            raise errors[0]
+        pipe_ms = 1e3 * wall_pipe / args.steps
+        e2e_pipe = {"value": n_prim / (pipe_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": pipe_ms, "calls_in_flight": 2,
+                    "how": "two contexts on two host threads, steps taken in turn; wall clock over all K steps"}
+
     # plain FP64 form on the same workload (bit-exact event streams), one step
     plain = None
     plain_res = None
@@ -534,6 +585,9 @@ def main() -> None:
     matched = matched_statistics(batched_res, plain_res, first, fp64_res) if batched_res is not None else None
     published = published_workload(cm, lat, dev, args.pub_events, lib) if args.pub_events and rank == 0 else None
 
+    e2e_one = {"value": world * n_prim / (e2e_step * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step, "calls_in_flight": 1}
+    e2e_ms_used = e2e_pipe["ms_per_step"] if e2e_pipe is not None else e2e_step
     peak, peak_kind = measured_peaks()
     steps_per_launch = steps_total / args.steps
     achieved = steps_per_launch * BYTES_PER_STEP / (sum(kms) / args.steps * 1e-3) / 1e9
@@ -550,10 +604,10 @@ def main() -> None:
         "kernel_ms_per_step": kernel_ms,
         "steps_per_s": world * steps_per_launch / (kernel_ms * 1e-3),
         "hits_per_step": hits_total / args.steps,
-        "e2e": {"value": world * n_prim / (e2e_step * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
-        "e2e_with_generator": {"value": world * n_prim / ((e2e_step + gen_ms) * 1e-3), "unit": UNIT,
-                               "ms_per_step": e2e_step + gen_ms, "generator_ms": gen_ms},
+        "e2e": e2e_pipe if e2e_pipe is not None else e2e_one,
+        "e2e_one_call_at_a_time": e2e_one,
+        "e2e_with_generator": {"value": world * n_prim / ((e2e_ms_used + gen_ms) * 1e-3), "unit": UNIT,
+                               "ms_per_step": e2e_ms_used + gen_ms, "generator_ms": gen_ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "bytes_per_step": BYTES_PER_STEP,
                      "traffic": (tps * steps_per_launch if tps else None)},
