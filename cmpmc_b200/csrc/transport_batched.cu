@@ -1039,22 +1039,30 @@ struct WarpSink {
 // the track goes on, ended (counters and ledger updated), or entered an active film (the
 // film record handed to out.film). A daughter made in the step is handed to out.daughter
 // with a substream key drawn from the track's stream.
+// The step has no early return: every lane that entered meets the others again before the
+// new-direction sampling, which the bulk scatters and the diffuse reflections of a warp then
+// run together (with early returns in the boundary branch the two groups ran it one after
+// the other).
 template <int kKin, bool kSur, class ST, class Sink>
 __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const Detector& D, FTrack& trk, R128& g,
                                          const ST& st, uint32_t ev, Sink& out) {
+    const unsigned m_in = __activemask();
+    int outcome = kStepOn;
+    int sample = 2;  // 0: isotropic (bulk scatter), 1: Lambertian about bh.n, 2: nothing more
+    FBHit bh;
     if (trk.E < D.min_phonon_eV || trk.bounces >= D.max_bounces) {
         ++st.killed();
         st.esc() += trk.E * trk.w;
-        return kStepEnd;
-    }
-    if (D.rr_bounces != 0 && trk.bounces > D.rr_bounces && (trk.bounces - D.rr_bounces) % 32 == 0) {
+        outcome = kStepEnd;
+    } else if (D.rr_bounces != 0 && trk.bounces > D.rr_bounces && (trk.bounces - D.rr_bounces) % 32 == 0) {
         if (g.u() < static_cast<float>(D.rr_survival)) {
             trk.w /= static_cast<float>(D.rr_survival);
         } else {
             ++st.killed();
-            return kStepEnd;
+            outcome = kStepEnd;
         }
     }
+    if (outcome == kStepOn) {
     ++st.steps();
     const float R = static_cast<float>(D.radius), H = static_cast<float>(D.half_z);
     const float nu = static_cast<float>(trk.E) * L.inv_h_thz;
@@ -1064,12 +1072,11 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
     const float r_down = (trk.mode == 0) ? L.a5 * (nu2 * nu2 * nu) : 0.0f;
     const float r_tot = r_iso + r_poly + r_down;
     const float d_phys = (r_tot > 1e-12f) ? (-logf(g.u()) * trk.vmag / r_tot) : __int_as_float(0x7f800000);
-    FBHit bh = fexit_d(R, H, trk.pos, trk.vg);
+    bh = fexit_d(R, H, trk.pos, trk.vg);
     const bool bulk = d_phys < bh.d;
     const float d = bulk ? d_phys : bh.d;
     trk.pos = trk.pos + trk.vg * d;
     trk.t += static_cast<double>(d / trk.vmag);
-    int sample = 2;  // 0: isotropic (bulk scatter), 1: Lambertian about bh.n, 2: nothing more
     if (bulk) {
         const float u_proc = g.u() * r_tot;
         if (r_down > 0.0f && u_proc < r_down) {
@@ -1122,9 +1129,8 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
                 h._pad = 0;
                 h.channel_id = ch_id;
                 out.hit(ev, h);
-                return kStepEnd;
-            }
-            if (film == kFilmCascade) {
+                outcome = kStepEnd;
+            } else if (film == kFilmCascade) {
                 FilmRec fr;
                 fr.px = trk.pos.x; fr.py = trk.pos.y; fr.pz = trk.pos.z;
                 fr.w = trk.w;
@@ -1138,19 +1144,19 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
                 fr.mode = static_cast<uint8_t>(trk.mode);
                 fr.pad0 = fr.pad1 = 0;
                 out.film(fr);
-                return kStepFilm;
+                outcome = kStepFilm;
+            } else {
+                // re-emitted unchanged: back into the crystal (bounces kept), a DOS mode and an
+                // inward Lambertian direction from the shared sampling below
+                trk.pos = trk.pos + bh.n * kNudge;
+                trk.mode = fdos(L, g.u());
+                sample = 1;
             }
-            // re-emitted unchanged: back into the crystal (bounces kept), a DOS mode and an
-            // inward Lambertian direction from the shared sampling below
-            trk.pos = trk.pos + bh.n * kNudge;
-            trk.mode = fdos(L, g.u());
-            sample = 1;
         } else if (g.u() > static_cast<float>(s.prob_refl)) {
             ++st.killed();
             st.esc() += trk.E * trk.w;
-            return kStepEnd;
-        }
-        if (!enter) {  // a surface reflection
+            outcome = kStepEnd;
+        } else {  // a surface reflection
             ++st.refl();
             trk.pos = trk.pos + bh.n * kNudge;
             float p_anh, p_anh_spec;
@@ -1196,6 +1202,8 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
             }
         }
     }
+    }
+    __syncwarp(m_in);
     // shared new-direction path: isotropic (bulk scatter) or Lambertian about the inward
     // normal (diffuse reflection, film re-emission), then the table lookup
     if (sample != 2) {
@@ -1226,7 +1234,7 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
         trk.vg = kin.dir;
         trk.vmag = kin.mag;
     }
-    return kStepOn;
+    return outcome;
 }
 
 struct PoolArgs {
@@ -2169,18 +2177,21 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool(const __grid_constant
         const uint32_t r_pub = vsh->r_pub;
         SmSink<Film, Entry> sink{&sh, film, ring, p.film_cap, ring_mask, r_floor, &err, &a};
         for (;;) {
-            uint32_t ft = 0, inp = 0, dry = 0;
+            uint32_t ft = 0, inp = 0, dry = 0, unpub = 0;
             if (lane == 0) {
                 ft = vsh->f_tail;
                 inp = vsh->input_left;
                 dry = vsh->n_dry;
+                unpub = vsh->r_tail - r_pub;
             }
             ft = __shfl_sync(full, ft, 0);
             inp = __shfl_sync(full, inp, 0);
             dry = __shfl_sync(full, dry, 0);
+            unpub = __shfl_sync(full, unpub, 0);
             // the film phase starts once enough records wait, or earlier when half the
-            // block has run dry and the waiting cascades would give it work
-            if (ft >= p.film_trigger || (ft > 0 && 2 * dry >= kSmWarps)) break;
+            // block has run dry and the waiting cascades or the phonons appended to the ring
+            // since the last boundary would give it work
+            if (ft >= p.film_trigger || ((ft > 0 || unpub > 0) && 2 * dry >= kSmWarps)) break;
             const unsigned empty = __ballot_sync(full, !live);
             if (empty) {
                 const int n_empty = __popc(empty);
