@@ -417,7 +417,7 @@ def main() -> None:
     # launch configuration from the project's autotuner (results do not depend on it), then
     # CUDA-graph replay of the device-resident call
     tune = None
-    # the SM-phase pool has one launch shape (one 768-thread block per SM): nothing to tune
+    # the SM-phase pool has one launch shape (one 512-thread block per SM): nothing to tune
     if not args.no_tune and launch_form != "sm_pool":
         tr = _ffi.TuneResultC()
         if lib.cmpmc_gpu_autotune(h, C.byref(dd), 1, C.byref(tr)) != 0:

@@ -204,11 +204,12 @@ int ensure_surrogate(cmpmc_gpu_ctx* ctx) {
 bool sm_pool(const cmpmc_gpu_ctx* ctx) { return ctx->pool == 1 || ctx->pool == 3; }
 int pool_fp64(const cmpmc_gpu_ctx* ctx) { return ctx->pool == 3 ? 1 : 0; }
 
-// grid of a pool launch over `units` units: one 768-thread block per SM (SM-phase pool), or
-// the occupancy's 128-thread blocks (warp pool), never more than the units can start
+// grid of a pool launch over `units` units: one block per SM (SM-phase pool; 512 threads in
+// FP32, 768 in FP64), or the occupancy's 128-thread blocks (warp pool), never more than the
+// units can start
 int pool_grid(cmpmc_gpu_ctx* ctx, uint64_t units, uint64_t* grid) {
     if (sm_pool(ctx)) {
-        const uint64_t per = static_cast<uint64_t>(sm_pool_threads());
+        const uint64_t per = static_cast<uint64_t>(sm_pool_threads(pool_fp64(ctx)));
         *grid = std::max<uint64_t>(1, std::min<uint64_t>(ctx->num_sms, (units + per - 1) / per));
         return CMPMC_OK;
     }
@@ -1117,7 +1118,7 @@ int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int form, uint32_t ring_capacit
         return fail(ctx, CMPMC_ERR_INVALID, "ring capacity: a power of two, at least 64");
     ctx->pool = form;
     if (ring_capacity) {
-        if (form == 1 || form == 3) ctx->sm_ring_cap = std::max<uint32_t>(ring_capacity, 2048);  // a block appends up to 2 x 768 at once
+        if (form == 1 || form == 3) ctx->sm_ring_cap = std::max<uint32_t>(ring_capacity, 2048);  // a block appends up to 2 x 512 at once
         else ctx->pool_ring_cap = ring_capacity;
     }
     return CMPMC_OK;

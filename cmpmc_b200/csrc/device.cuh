@@ -307,7 +307,7 @@ cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detecto
                              uint32_t ring_cap, void* film, const uint32_t* unit_event, const QPhonon* queue,
                              int stage_tables, int grid, int block, cudaStream_t s);
 cudaError_t pool_fp32_occupancy(int block, int* blocks_per_sm);
-// SM-phase pool (one block of sm_pool_threads() threads per SM alternating transport and
+// SM-phase pool (one block of sm_pool_threads(fp64) threads per SM alternating transport and
 // film phases): `ring` holds ring_cap entries (pool_ring_entry_bytes) per block, `film`
 // film_cap film records (64 B) per block
 // (fp64 = 1: the FP64 comparison form of the same pool, phonon batches without the
@@ -316,7 +316,7 @@ cudaError_t pool_fp32_occupancy(int block, int* blocks_per_sm);
 cudaError_t launch_sm_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
                                 uint32_t ring_cap, void* film, uint32_t film_cap, const uint32_t* unit_event,
                                 const QPhonon* queue, int stage_tables, int fp64, int grid, cudaStream_t s);
-int sm_pool_threads();
+int sm_pool_threads(int fp64);
 size_t sm_pool_entry_bytes(int fp64);
 size_t sm_pool_film_bytes(int fp64);
 size_t pool_ring_entry_bytes();

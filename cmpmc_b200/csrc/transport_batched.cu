@@ -1527,7 +1527,7 @@ __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FL
 // The warp pool runs a warp's film cascades among the other warps' transport steps, and the
 // two code paths then compete for the SM's instruction cache: measured, the transport
 // machinery alone steps 2.4e10 times a second, the mix half as fast as separate kernels.
-// Here one block of 768 threads (24 warps) owns an SM and alternates two phases, so the SM
+// Here one block of 512 threads (16 warps) owns an SM and alternates two phases, so the SM
 // runs one code path at a time:
 //   transport phase: every warp steps its lanes, refilling them from the block's ring of
 //     pending phonons (entries published at the last phase boundary) and then from the
@@ -1541,15 +1541,31 @@ __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FL
 // The block ends when a boundary finds no live lane, no published phonon and no primary
 // left. Nothing waits on another block; every wait is a block barrier that all threads
 // reach (each phase ends by itself).
-constexpr int kSmThreads = 768;
-constexpr int kSmWarps = kSmThreads / 32;
+// Threads of the block (build-time, per precision). FP32: 512 threads keep the step loop's
+// state in 128 registers with no spills; measured on the 1M-primary batch, 384 threads (168
+// registers) 231 ms, 512 (128) 204 ms, 576 (96) 228 ms, 768 (80) 223 ms, 1024 (64) 263 ms.
+// FP64: 768 threads (1,481 ms; 512 threads 1,564 ms).
+#ifndef CMPMC_SM_THREADS
+#define CMPMC_SM_THREADS 512
+#endif
+#ifndef CMPMC_SM_THREADS_FP64
+#define CMPMC_SM_THREADS_FP64 768
+#endif
+// the block's shape: threads, warps and the per-lane unit counters and ledgers (dynamic
+// shared memory: [warps][kNCnt][32] u32, then [warps][2][32] f64)
+template <int kThreads>
+struct SmShape {
+    static constexpr int kWarps = kThreads / 32;
+    static constexpr int kCntBytes = kWarps * kNCnt * 32 * 4;
+    static constexpr int kDynBytes = kCntBytes + kWarps * 2 * 32 * 8;
+};
 
 struct SmPoolArgs {
     void* ring;              // [blocks][ring_cap] entries of the precision's ring type
     void* film;              // [blocks][film_cap] film records of the precision's type
     uint32_t ring_cap;       // a power of two
     uint32_t film_cap;       // film records per block and phase
-    uint32_t film_trigger;   // records that end a transport phase (<= film_cap - kSmThreads)
+    uint32_t film_trigger;   // records that end a transport phase (<= film_cap - threads)
     const uint32_t* unit_event;
     const QPhonon* queue;    // queue units (kQueue kernels)
     int stage_tables;
@@ -1640,6 +1656,7 @@ __device__ __forceinline__ uint64_t reemit_key(uint64_t key, int j) {
 // reference's 1e-11 m inward nudge, the lattice's own map_k_to_vg in every kinematics
 // mode): the comparison point that isolates what FP32 buys.
 struct PF32 {
+    static constexpr int kThreads = CMPMC_SM_THREADS;
     using Track = FTrack;
     using Entry = PoolPh;
     using Film = FilmRec;
@@ -2029,6 +2046,7 @@ __device__ __forceinline__ int pool_step64(const Lattice& L, const Detector& D, 
 }
 
 struct PF64 {
+    static constexpr int kThreads = CMPMC_SM_THREADS_FP64;
     using Track = DTrack;
     using Entry = PoolPh64;
     using Film = FilmRec64;
@@ -2128,7 +2146,7 @@ __device__ __noinline__ void sm_film_phase(const typename P::Lat* Lp, const Dete
 }
 
 template <class P, bool kSur, int kKin = 0, bool kQueue = false>
-__global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool(const __grid_constant__ typename P::Lat L,
+__global__ void __launch_bounds__(P::kThreads, 1) k_sm_pool(const __grid_constant__ typename P::Lat L,
                                                            const __grid_constant__ Detector D,
                                                            const __grid_constant__ RunArgs a,
                                                            const __grid_constant__ SmPoolArgs p) {
@@ -2137,8 +2155,9 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool(const __grid_constant
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
-    __shared__ uint32_t s_cnt[kSmWarps][kNCnt][32];
-    __shared__ double s_led[kSmWarps][2][32];
+    extern __shared__ __align__(16) unsigned char sm_dyn[];
+    uint32_t(*s_cnt)[kNCnt][32] = reinterpret_cast<uint32_t(*)[kNCnt][32]>(sm_dyn);
+    double(*s_led)[2][32] = reinterpret_cast<double(*)[2][32]>(sm_dyn + SmShape<P::kThreads>::kCntBytes);
     __shared__ alignas(128) float s_cdf[P::kStage ? 2 * kNCdf : 4];  // decay CDF tables (L-LT, then TT)
     __shared__ alignas(8) uint64_t s_bar;
     __shared__ SmShared sh;
@@ -2191,7 +2210,7 @@ __global__ void __launch_bounds__(kSmThreads, 1) k_sm_pool(const __grid_constant
             // the film phase starts once enough records wait, or earlier when half the
             // block has run dry and the waiting cascades or the phonons appended to the ring
             // since the last boundary would give it work
-            if (ft >= p.film_trigger || ((ft > 0 || unpub > 0) && 2 * dry >= kSmWarps)) break;
+            if (ft >= p.film_trigger || ((ft > 0 || unpub > 0) && 2 * dry >= SmShape<P::kThreads>::kWarps)) break;
             const unsigned empty = __ballot_sync(full, !live);
             if (empty) {
                 const int n_empty = __popc(empty);
@@ -2381,43 +2400,54 @@ cudaError_t launch_pool_fp32(const Lattice& L, const float* cdf_f, const Detecto
     return cudaGetLastError();
 }
 
+template <class P, bool kSur, int kKin = 0, bool kQueue = false>
+cudaError_t sm_launch(const typename P::Lat& L, const Detector& D, const RunArgs& a, const SmPoolArgs& p, int grid,
+                      cudaStream_t s) {
+    constexpr int kDyn = SmShape<P::kThreads>::kDynBytes;
+    if (kDyn > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(k_sm_pool<P, kSur, kKin, kQueue>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kDyn);
+        if (e != cudaSuccess) return e;
+    }
+    k_sm_pool<P, kSur, kKin, kQueue><<<grid, P::kThreads, kDyn, s>>>(L, D, a, p);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sm_pool_fp32(const Lattice& L, const float* cdf_f, const Detector& D, const RunArgs& a, void* ring,
                                 uint32_t ring_cap, void* film, uint32_t film_cap, const uint32_t* unit_event,
                                 const QPhonon* queue, int stage_tables, int fp64, int grid, cudaStream_t s) {
     // the ring is indexed by masking: its capacity must be a power of two
-    if (ring_cap < 2u * kSmThreads || (ring_cap & (ring_cap - 1u)) != 0 || film_cap < 4u * kSmThreads)
+    const uint32_t threads = static_cast<uint32_t>(fp64 ? PF64::kThreads : PF32::kThreads);
+    if (ring_cap < 2u * threads || (ring_cap & (ring_cap - 1u)) != 0 || film_cap < 4u * threads)
         return cudaErrorInvalidValue;
     SmPoolArgs p;
     p.ring = ring;
     p.film = film;
     p.ring_cap = ring_cap;
     p.film_cap = film_cap;
-    p.film_trigger = film_cap > 2u * kSmThreads ? film_cap - 2u * kSmThreads : film_cap / 2u;
+    p.film_trigger = film_cap > 2u * threads ? film_cap - 2u * threads : film_cap / 2u;
     p.unit_event = unit_event;
     p.queue = queue;
     p.stage_tables = stage_tables;
     if (fp64) {  // the FP64 comparison form: phonon batches, every kinematics mode, full cascades
         if (queue || a.surrogate) return cudaErrorInvalidValue;
-        k_sm_pool<PF64, false><<<grid, kSmThreads, 0, s>>>(L, D, a, p);
-        return cudaGetLastError();
+        return sm_launch<PF64, false>(L, D, a, p, grid, s);
     }
     const FLat f = make_flat(L, cdf_f, D);
     if (queue) {
-        if (L.kin_mode != kKinOctahedral) k_sm_pool<PF32, false, 1, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
-        else if (a.surrogate) k_sm_pool<PF32, true, 0, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
-        else k_sm_pool<PF32, false, 0, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
-    } else {
-        if (L.kin_mode != kKinOctahedral) k_sm_pool<PF32, false, 1><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
-        else if (a.surrogate) k_sm_pool<PF32, true><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
-        else k_sm_pool<PF32, false><<<grid, kSmThreads, 0, s>>>(f, D, a, p);
+        if (L.kin_mode != kKinOctahedral) return sm_launch<PF32, false, 1, true>(f, D, a, p, grid, s);
+        if (a.surrogate) return sm_launch<PF32, true, 0, true>(f, D, a, p, grid, s);
+        return sm_launch<PF32, false, 0, true>(f, D, a, p, grid, s);
     }
-    return cudaGetLastError();
+    if (L.kin_mode != kKinOctahedral) return sm_launch<PF32, false, 1>(f, D, a, p, grid, s);
+    if (a.surrogate) return sm_launch<PF32, true>(f, D, a, p, grid, s);
+    return sm_launch<PF32, false>(f, D, a, p, grid, s);
 }
 
 size_t sm_pool_entry_bytes(int fp64) { return fp64 ? sizeof(PoolPh64) : sizeof(PoolPh); }
 size_t sm_pool_film_bytes(int fp64) { return fp64 ? sizeof(FilmRec64) : sizeof(FilmRec); }
 
-int sm_pool_threads() { return kSmThreads; }
+int sm_pool_threads(int fp64) { return fp64 ? PF64::kThreads : PF32::kThreads; }
 
 cudaError_t pool_fp32_occupancy(int block, int* blocks_per_sm) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_pool_fp32<false>, block, 0);

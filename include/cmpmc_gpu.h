@@ -529,7 +529,7 @@ int cmpmc_gpu_configure_phases(cmpmc_gpu_ctx* ctx, uint32_t phase_steps);
 
 /* Launch form of the batched FP32 phonon transport (no counterpart in the reference).
  * form = 1 (the default): the SM-phase pool, one persistent launch per call with one
- *   768-thread block per SM that alternates a transport phase (every warp steps its lanes,
+ *   512-thread block per SM that alternates a transport phase (every warp steps its lanes,
  *   refilled from the block's ring of pending phonons and the batch's primaries; film
  *   entries and daughters appended to block buffers) and a film phase (every thread runs
  *   the waiting film cascades, their re-emissions appended to the ring), so an SM runs one
