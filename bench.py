@@ -303,6 +303,8 @@ def main() -> None:
     ap.add_argument("--pipeline", action="store_true",
                     help="also time e2e with two calls in flight (two contexts on two host threads)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the batched FP64 comparison step")
+    ap.add_argument("--no-stage", action="store_true",
+                    help="decay CDF tables read from global memory instead of the TMA-staged shared copy")
     ap.add_argument("--recoil", type=int, default=0,
                     help="instead of the headline line: time the recoil batch of this many events once")
     ap.add_argument("--surrogate", action="store_true",
@@ -348,6 +350,8 @@ def main() -> None:
         eng.configure(dev, stack_capacity=args.stack_capacity, queue_capacity=args.queue_capacity)
     form_id = _ffi.FORM_BATCHED_FP32 if args.form == "batched_fp32" else _ffi.FORM_BATCHED_FP32_INLINE
     eng.configure_pool({"sm_pool": 1, "warp_pool": 2, "rounds": 0}[args.launch], device=dev)
+    if args.no_stage:
+        eng.configure_staging(False, device=dev)
     launch_form = "inline" if args.form != "batched_fp32" else args.launch
 
     # device-resident inputs (torch owns the memory)
@@ -602,6 +606,7 @@ def main() -> None:
                    "primaries": n_prim * world, "form": args.form, "seed": SEED,
                    "film_cascades": "surrogate table" if args.surrogate else "full Kaplan cascade",
                    "energy": "log-uniform 1-30 meV", "modes": "L/ST/FT 0.10/0.36/0.54",
+                   "decay_tables": "global memory" if args.no_stage else "shared memory (TMA bulk copy)",
                    "l2": "256 MiB buffer written between timed steps (L2 126 MB); inputs 128 MB, hits ~1.5 GB per step"},
         "kernel_ms_per_step": kernel_ms,
         "steps_per_s": world * steps_per_launch / (kernel_ms * 1e-3),

@@ -170,10 +170,12 @@ __device__ __noinline__ double kaplan_cascade_call(const Film* f, double E, doub
 // drawn in line by the transport step: direct absorption (the whole energy deposited), or the
 // phonon comes back out unchanged (sub-gap, or lost on its way in); only the rest needs the
 // pair-breaking cascade. With the surrogate table (whose stored outcomes include the entry
-// step) only sub-gap phonons are decided here: the table does not cover them.
+// step) only sub-gap phonons are decided here: the table does not cover them. Inlined: as an
+// out-of-line call in the boundary branch (which ~3 lanes of a warp take) it cost 8 % of the
+// batch (198 -> 181 ms).
 enum { kFilmAbsorbed = 0, kFilmReemit = 1, kFilmCascade = 2 };
 template <bool kSur>
-__device__ __noinline__ int film_quick(const Film* f, double E, R128* g) {
+__device__ __forceinline__ int film_quick(const Film* f, double E, R128* g) {
     if (kSur && !film_is_subgap(*f, E)) return kFilmCascade;
     if (film_direct_absorption(*f, E, *g)) return kFilmAbsorbed;
     if (film_is_subgap(*f, E) || g->uniform() <= film_loss_probability(*f, E, 4.0)) return kFilmReemit;
@@ -315,7 +317,8 @@ __device__ __forceinline__ void write_unit(const RunArgs& a, uint64_t unit, cons
 }
 
 // event sink: a finished unit adds its counters to its event (units of one event run on
-// many threads; the doubles are FP64 atomics, so their last bits depend on the order)
+// many threads; the doubles are FP64 atomics, so their last bits depend on the order).
+// Inlined: out of line it cost the SM-phase pool 5 % of the batch (181 -> 172 ms).
 __device__ __forceinline__ void add_u64(unsigned long long* p, uint32_t v) {
     if (v) atomicAdd(p, static_cast<unsigned long long>(v));
 }
@@ -323,7 +326,7 @@ __device__ __forceinline__ void add_f64(double* p, double v) {
     if (v != 0.0) atomicAdd(p, v);
 }
 template <class ST>
-__device__ __noinline__ void sink_unit(const RunArgs* a, uint32_t ev, const ST st) {
+__device__ __forceinline__ void sink_unit(const RunArgs* a, uint32_t ev, const ST st) {
     cmpmc_sim_stats& o = a->ev_stats[ev];
     add_u64(reinterpret_cast<unsigned long long*>(&o.total_steps), st.steps());
     add_u64(reinterpret_cast<unsigned long long*>(&o.isotope_scatters), st.iso());
@@ -1023,6 +1026,34 @@ union PoolOut {
     PoolPh ph;
 };
 // output of the warp pool's step: the record goes to the thread's staging slot
+// The per-surface constants of the boundary branch (staged in shared memory by every block
+// that runs pool_step: the branch reads them by the surface a lane hit, which differs between
+// lanes; read from the kernel parameters, each field would be a separate constant-bank load
+// per distinct surface)
+enum { kHotFilm = 1, kHotAmm = 2, kHotMask = 4, kHotSplitConst = 8 };
+struct alignas(16) SurfHot {
+    float prob_abs, p_enter, prob_refl, p_anh;  // p_enter: the film's film_absorption
+    float p_anh_spec;                           // p_anh + p_spec (constant split)
+    int flags;                                  // kHot*
+    int pad0, pad1;
+};
+__device__ __forceinline__ SurfHot surf_hot(const FLat& L, const Surface& s, int i) {
+    SurfHot h;
+    h.prob_abs = static_cast<float>(s.prob_abs);
+    h.p_enter = static_cast<float>(s.film.film_absorption);
+    h.prob_refl = static_cast<float>(s.prob_refl);
+    h.p_anh = L.p_anh[i];
+    h.p_anh_spec = L.p_anh_spec[i];
+    h.flags = (s.has_film ? kHotFilm : 0) | (s.has_amm ? kHotAmm : 0) | (s.n_pads > 0 ? kHotMask : 0) |
+              (L.split_const[i] ? kHotSplitConst : 0);
+    h.pad0 = h.pad1 = 0;
+    return h;
+}
+// threads 0-2 of the block fill hot[3]; the caller synchronizes the block before use
+__device__ __forceinline__ void stage_surf_hot(const FLat& L, const Detector& D, SurfHot* hot) {
+    if (threadIdx.x < 3) hot[threadIdx.x] = surf_hot(L, D.surf[threadIdx.x], static_cast<int>(threadIdx.x));
+}
+
 struct WarpSink {
     PoolOut* o;
     bool has_d;
@@ -1044,8 +1075,8 @@ struct WarpSink {
 // run together (with early returns in the boundary branch the two groups ran it one after
 // the other).
 template <int kKin, bool kSur, class ST, class Sink>
-__device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const Detector& D, FTrack& trk, R128& g,
-                                         const ST& st, uint32_t ev, Sink& out) {
+__device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const Detector& D, const SurfHot* hot,
+                                         FTrack& trk, R128& g, const ST& st, uint32_t ev, Sink& out) {
     const unsigned m_in = __activemask();
     int outcome = kStepOn;
     int sample = 2;  // 0: isotropic (bulk scatter), 1: Lambertian about bh.n, 2: nothing more
@@ -1095,19 +1126,19 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
     } else {
         bh.n = fnormal(bh.surf, trk.pos);
         trk.bounces++;
-        const Surface& s = D.surf[bh.surf];
+        const SurfHot hs = hot[bh.surf];
+        const Surface& s = D.surf[bh.surf];  // read by the out-of-line calls only
         bool enter = false;
         int ch_id = -1;
         bool active_pad = true;
-        if (s.n_pads > 0) {  // electrode mask (engine.hpp:483-488)
+        if (hs.flags & kHotMask) {  // electrode mask (engine.hpp:483-488)
             R128 g_c = g;
             ch_id = mask_call(s.pads, s.n_pads, trk.pos.x, trk.pos.y, &g_c);
             g = g_c;
             active_pad = ch_id >= 0;
         }
-        if (active_pad && s.has_film && g.u() < static_cast<float>(s.prob_abs)) {
-            const float p_enter = s.has_amm ? amm_call(&s, trk.mode == 0, fdot(trk.k, bh.n))
-                                            : static_cast<float>(s.film.film_absorption);
+        if (active_pad && (hs.flags & kHotFilm) && g.u() < hs.prob_abs) {
+            const float p_enter = (hs.flags & kHotAmm) ? amm_call(&s, trk.mode == 0, fdot(trk.k, bh.n)) : hs.p_enter;
             enter = g.u() < p_enter;
         }
         if (enter) {
@@ -1152,7 +1183,7 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
                 trk.mode = fdos(L, g.u());
                 sample = 1;
             }
-        } else if (g.u() > static_cast<float>(s.prob_refl)) {
+        } else if (g.u() > hs.prob_refl) {
             ++st.killed();
             st.esc() += trk.E * trk.w;
             outcome = kStepEnd;
@@ -1160,9 +1191,9 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
             ++st.refl();
             trk.pos = trk.pos + bh.n * kNudge;
             float p_anh, p_anh_spec;
-            if (L.split_const[bh.surf]) {
-                p_anh = L.p_anh[bh.surf];
-                p_anh_spec = L.p_anh_spec[bh.surf];
+            if (hs.flags & kHotSplitConst) {
+                p_anh = hs.p_anh;
+                p_anh_spec = hs.p_anh_spec;
             } else {
                 const Split sp = reflection_split(s, trk.E);
                 p_anh = static_cast<float>(sp.p_anh);
@@ -1382,8 +1413,11 @@ __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FL
     __shared__ PoolOut s_out[kMaxBlock];
     __shared__ alignas(128) float s_cdf[2 * kNCdf];  // the decay CDF tables (L-LT, then TT)
     __shared__ alignas(8) uint64_t s_bar;
+    __shared__ SurfHot s_hot[3];
     const UStats st{&s_cnt[0][threadIdx.x], &s_led[0][threadIdx.x]};
     PoolOut& my_out = s_out[threadIdx.x];
+    stage_surf_hot(L, D, s_hot);
+    __syncthreads();
     const float* cdf = L.cdf_lt;  // the two tables are contiguous in global memory
     if (p.stage_tables) {
         if (!stage_bulk(s_cdf, L.cdf_lt, 2 * kNCdf * sizeof(float), &s_bar)) {
@@ -1489,7 +1523,7 @@ __global__ void __launch_bounds__(128, 6) k_pool_fp32(const __grid_constant__ FL
         int outcome = kStepOn;
         WarpSink sink{&my_out, false, &a};
         if (live) {
-            outcome = pool_step<kKin, kSur>(L, cdf, D, trk, g, st, ev_cur, sink);
+            outcome = pool_step<kKin, kSur>(L, cdf, D, s_hot, trk, g, st, ev_cur, sink);
             if (outcome != kStepOn) {
                 sink_unit(&a, ev_cur, st);
                 live = false;
@@ -1699,9 +1733,9 @@ struct PF32 {
         t.bounces = q.pad;
     }
     template <int kKin, bool kSur, class ST, class Sink>
-    __device__ static __forceinline__ int step(const Lat& L, const float* cdf, const Detector& D, Track& trk, R128& g,
-                                               const ST& st, uint32_t ev, Sink& out) {
-        return pool_step<kKin, kSur>(L, cdf, D, trk, g, st, ev, out);
+    __device__ static __forceinline__ int step(const Lat& L, const float* cdf, const Detector& D, const SurfHot* hot,
+                                               Track& trk, R128& g, const ST& st, uint32_t ev, Sink& out) {
+        return pool_step<kKin, kSur>(L, cdf, D, hot, trk, g, st, ev, out);
     }
     // one film record of the film phase: cascade, then the re-emissions into the ring
     template <bool kSur, int kKin>
@@ -2088,8 +2122,8 @@ struct PF64 {
         t.bounces = q.pad;
     }
     template <int kKin, bool kSur, class ST, class Sink>
-    __device__ static __forceinline__ int step(const Lat& L, const float*, const Detector& D, Track& trk, R128& g,
-                                               const ST& st, uint32_t ev, Sink& out) {
+    __device__ static __forceinline__ int step(const Lat& L, const float*, const Detector& D, const SurfHot*,
+                                               Track& trk, R128& g, const ST& st, uint32_t ev, Sink& out) {
         return pool_step64<kSur>(L, D, trk, g, st, ev, out);
     }
     template <bool kSur, int kKin>
@@ -2161,10 +2195,12 @@ __global__ void __launch_bounds__(P::kThreads, 1) k_sm_pool(const __grid_constan
     __shared__ alignas(128) float s_cdf[P::kStage ? 2 * kNCdf : 4];  // decay CDF tables (L-LT, then TT)
     __shared__ alignas(8) uint64_t s_bar;
     __shared__ SmShared sh;
+    __shared__ SurfHot s_hot[3];
     const UStatsT<32> st{&s_cnt[wid][0][lane], &s_led[wid][0][lane]};
     Entry* ring = static_cast<Entry*>(p.ring) + static_cast<uint64_t>(blockIdx.x) * p.ring_cap;
     Film* film = static_cast<Film*>(p.film) + static_cast<uint64_t>(blockIdx.x) * p.film_cap;
     const uint32_t ring_mask = p.ring_cap - 1;
+    if constexpr (P::kStage) stage_surf_hot(L, D, s_hot);  // FP32 policy (the FP64 step reads D)
     if (threadIdx.x == 0) {
         sh.r_head = sh.r_tail = sh.r_pub = 0;
         sh.f_tail = sh.f_next = 0;
@@ -2266,7 +2302,7 @@ __global__ void __launch_bounds__(P::kThreads, 1) k_sm_pool(const __grid_constan
                 break;
             }
             if (live) {
-                const int outcome = P::template step<kKin, kSur>(L, cdf, D, trk, g, st, ev_cur, sink);
+                const int outcome = P::template step<kKin, kSur>(L, cdf, D, s_hot, trk, g, st, ev_cur, sink);
                 if (outcome != kStepOn) {
                     sink_unit(&a, ev_cur, st);
                     live = false;
