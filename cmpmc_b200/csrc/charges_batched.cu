@@ -315,10 +315,20 @@ __device__ __forceinline__ uint64_t luke_key(uint64_t ckey, uint32_t idx) {
     return mix64(ckey ^ (0x9e3779b97f4a7c15ULL * (static_cast<uint64_t>(idx) + 1)));
 }
 
-__global__ void __launch_bounds__(128, 4) k_charges_fp32(const __grid_constant__ FCLat L,
+__global__ void __launch_bounds__(128, 4) k_charges_fp32(const __grid_constant__ FCLat Lp,
                                                          const __grid_constant__ FCDet D,
                                                          const __grid_constant__ RunArgs a,
                                                          const __grid_constant__ ChargeArgs ca) {
+    // the crystal constants (the Herring-Vogt valley rotations and mass tensor among them) in
+    // shared memory: the step reads the rotation of each carrier's own valley, an index that
+    // differs between the lanes of a warp, which the constant bank of the kernel parameters
+    // serves one distinct address at a time
+    __shared__ alignas(16) FCLat sL;
+    static_assert(sizeof(FCLat) % 4 == 0, "FCLat is copied in 4-byte words");
+    for (int i = threadIdx.x; i < static_cast<int>(sizeof(FCLat) / 4); i += blockDim.x)
+        reinterpret_cast<uint32_t*>(&sL)[i] = reinterpret_cast<const uint32_t*>(&Lp)[i];
+    __syncthreads();
+    const FCLat& L = sL;
     Carrier k;
     CStats st{};
     QCharge knock[kKnockCap];
