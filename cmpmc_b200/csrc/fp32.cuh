@@ -113,9 +113,14 @@ __device__ __noinline__ FKin fmap_solve(const FLat* Lp, int mode, F3 k) {
     return f;
 }
 
+// kRot = false: the crystal frame is the detector frame (identity orientation, the default
+// lattice), so both rotations are skipped
+template <bool kRot = true>
 __device__ __forceinline__ FKin fmap(const FLat& L, int mode, F3 k) {
-    const F3 kc = f3(L.o[0] * k.x + L.o[3] * k.y + L.o[6] * k.z, L.o[1] * k.x + L.o[4] * k.y + L.o[7] * k.z,
-                     L.o[2] * k.x + L.o[5] * k.y + L.o[8] * k.z);
+    F3 kc = k;
+    if constexpr (kRot)
+        kc = f3(L.o[0] * k.x + L.o[3] * k.y + L.o[6] * k.z, L.o[1] * k.x + L.o[4] * k.y + L.o[7] * k.z,
+                L.o[2] * k.x + L.o[5] * k.y + L.o[8] * k.z);
     const float l1 = fabsf(kc.x) + fabsf(kc.y) + fabsf(kc.z);
     const float inv = (l1 > 1e-18f) ? __frcp_rn(l1) : 1.0f;
     float px = kc.x * inv, py = kc.y * inv;
@@ -140,18 +145,30 @@ __device__ __forceinline__ FKin fmap(const FLat& L, int mode, F3 k) {
     const float mag = sqrtf(fdot(vc, vc));
     const F3 vn = vc * __frcp_rn(fmaxf(mag, 1e-12f));
     FKin r;
-    r.dir = f3(L.o[0] * vn.x + L.o[1] * vn.y + L.o[2] * vn.z, L.o[3] * vn.x + L.o[4] * vn.y + L.o[5] * vn.z,
-               L.o[6] * vn.x + L.o[7] * vn.y + L.o[8] * vn.z);
+    r.dir = vn;
+    if constexpr (kRot)
+        r.dir = f3(L.o[0] * vn.x + L.o[1] * vn.y + L.o[2] * vn.z, L.o[3] * vn.x + L.o[4] * vn.y + L.o[5] * vn.z,
+                   L.o[6] * vn.x + L.o[7] * vn.y + L.o[8] * vn.z);
     r.mag = mag;
     return r;
 }
 
-// The group-velocity map of the kernel's kinematics: the octahedral table (kKin 0) or the
-// lattice's Exact / Bilinear map (kKin 1, out of line). A compile-time choice: an
+// the orientation is the identity (the kernels' kKin = 2 variant may be used)
+inline bool flat_identity_orientation(const FLat& f) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            if (f.o[3 * i + j] != (i == j ? 1.0f : 0.0f)) return false;
+    return true;
+}
+
+// The group-velocity map of the kernel's kinematics: the octahedral table (kKin 0), the
+// lattice's Exact / Bilinear map (kKin 1, out of line) or the octahedral table of a crystal
+// with the identity orientation (kKin 2: no rotations). A compile-time choice: an
 // out-of-line call in the octahedral kernels' step loop would cost them a third.
 template <int kKin>
 __device__ __forceinline__ FKin fmapk(const FLat& L, int mode, F3 k) {
-    if constexpr (kKin != 0) return fmap_solve(&L, mode, k);
+    if constexpr (kKin == 1) return fmap_solve(&L, mode, k);
+    else if constexpr (kKin == 2) return fmap<false>(L, mode, k);
     else return fmap(L, mode, k);
 }
 

@@ -2473,10 +2473,12 @@ cudaError_t launch_sm_pool_fp32(const Lattice& L, const float* cdf_f, const Dete
     if (queue) {
         if (L.kin_mode != kKinOctahedral) return sm_launch<PF32, false, 1, true>(f, D, a, p, grid, s);
         if (a.surrogate) return sm_launch<PF32, true, 0, true>(f, D, a, p, grid, s);
+        if (flat_identity_orientation(f)) return sm_launch<PF32, false, 2, true>(f, D, a, p, grid, s);
         return sm_launch<PF32, false, 0, true>(f, D, a, p, grid, s);
     }
     if (L.kin_mode != kKinOctahedral) return sm_launch<PF32, false, 1>(f, D, a, p, grid, s);
     if (a.surrogate) return sm_launch<PF32, true>(f, D, a, p, grid, s);
+    if (flat_identity_orientation(f)) return sm_launch<PF32, false, 2>(f, D, a, p, grid, s);
     return sm_launch<PF32, false>(f, D, a, p, grid, s);
 }
 
