@@ -432,9 +432,10 @@ def main() -> None:
                 "phase_steps": tr.phase_steps,
                 "best_kernel_ms": tr.best_ms, "default_kernel_ms": tr.first_ms,
                 "tried": [[tr.tried_tpb[i], tr.tried_bps[i], round(tr.tried_ms[i], 2)] for i in range(tr.n_tried)]}
-    # graph replay covers the inline form's fixed launch sequence; the split form's film and
-    # transport rounds depend on the queue counts, so it runs eagerly
-    use_graph = not args.no_graph and args.form == "batched_fp32_inline"
+    # graph replay covers the pool forms' call (counter resets, unit map, the persistent
+    # transport launch, merge) and the inline form's; the host-driven rounds depend on the
+    # queue counts, so they run eagerly
+    use_graph = not args.no_graph and launch_form != "rounds"
     if use_graph:
         lib.cmpmc_gpu_configure_graph(h, 1)
     for _ in range(args.warmup):

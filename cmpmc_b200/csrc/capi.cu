@@ -121,6 +121,7 @@ struct cmpmc_gpu_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<uint64_t> graph_key;
     uint64_t graph_hits_cap = 0;                        // hit records the captured merge can write
+    uint64_t graph_stage_cap = 0;                       // hit staging records of the captured transport
     int graph_launches = 0;
     const float* cdf_f = nullptr;              // FP32 copies of the decay tables (in `tables`)
     HostBuf h_hits, h_offsets, h_evstats, h_total, h_counters;
@@ -158,15 +159,32 @@ void drop_graph(cmpmc_gpu_ctx* ctx) {
     ctx->graph_key.clear();
 }
 
-// The call signature a captured graph is valid for: the descriptor's pointers and sizes
-// and the context's launch configuration (device buffers only move when an eager call
-// grows them, and every eager call recaptures).
+// The call signature a captured graph is valid for: the descriptor's pointers and sizes,
+// the context's launch configuration, and the address and capacity of every device and host
+// buffer a captured call touches (a call of another form may grow, and so move, a shared
+// buffer without recapturing: the key then no longer matches and the next call runs eagerly
+// and recaptures).
 std::vector<uint64_t> graph_key_of(const cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d) {
-    return {d->n_events, d->first_event, reinterpret_cast<uint64_t>(d->rng_state),
-            reinterpret_cast<uint64_t>(d->injected_eV), reinterpret_cast<uint64_t>(d->phonon_offsets),
-            reinterpret_cast<uint64_t>(d->phonons), static_cast<uint64_t>(d->keep_hits), d->seed,
-            static_cast<uint64_t>(d->want_event_stats), static_cast<uint64_t>(d->kaplan_surrogate),
-            static_cast<uint64_t>(ctx->tpb), static_cast<uint64_t>(ctx->bps), ctx->stack_cap_batched, ctx->hit_cap};
+    std::vector<uint64_t> k = {d->n_events, d->first_event, reinterpret_cast<uint64_t>(d->rng_state),
+                               reinterpret_cast<uint64_t>(d->injected_eV), reinterpret_cast<uint64_t>(d->phonon_offsets),
+                               reinterpret_cast<uint64_t>(d->phonons), static_cast<uint64_t>(d->keep_hits), d->seed,
+                               static_cast<uint64_t>(d->want_event_stats), static_cast<uint64_t>(d->kaplan_surrogate),
+                               static_cast<uint64_t>(d->form), static_cast<uint64_t>(ctx->tpb),
+                               static_cast<uint64_t>(ctx->bps), ctx->stack_cap_batched, ctx->hit_cap,
+                               static_cast<uint64_t>(ctx->pool), static_cast<uint64_t>(ctx->stage_tables),
+                               ctx->sm_ring_cap, ctx->sm_film_cap, ctx->pool_ring_cap};
+    for (const DevBuf* b : {&ctx->stack, &ctx->cstack, &ctx->hit_stage, &ctx->hit_key, &ctx->counters, &ctx->ev_stats,
+                            &ctx->ev_nhits, &ctx->offsets, &ctx->hits_out, &ctx->total, &ctx->unit_event,
+                            &ctx->ev_offsets, &ctx->ev_stats2, &ctx->partials, &ctx->cursor, &ctx->pool_ring,
+                            &ctx->pool_film}) {
+        k.push_back(reinterpret_cast<uint64_t>(b->p));
+        k.push_back(b->cap);
+    }
+    for (const HostBuf* b : {&ctx->h_counters, &ctx->h_total}) {
+        k.push_back(reinterpret_cast<uint64_t>(b->p));
+        k.push_back(b->cap);
+    }
+    return k;
 }
 
 // Builds (once per context) the Kaplan surrogate table of every film on the host
@@ -747,6 +765,26 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
     cudaStream_t s = ctx->stream;
     if (pool_fp64(ctx) && a.surrogate)
         return fail(ctx, CMPMC_ERR_INVALID, "the FP64 pool form runs the full film cascades (no surrogate)");
+    // ---- CUDA-graph replay: the same device-resident batch again (the persistent transport
+    // launch with its counter resets, unit map and merge as one graph launch) ---------------
+    const bool graph_ok = ctx->graph_enabled && n > 0 && n_ph > 0 && d->inputs_on_device && d->outputs_on_device;
+    if (graph_ok && ctx->graph_exec && ctx->graph_key == graph_key_of(ctx, d)) {
+        CK(cudaGraphLaunch(ctx->graph_exec, s), "graph launch");
+        CK(cudaStreamSynchronize(s), "graph");
+        hc = *ctx->h_counters.as<Counters>();
+        const bool over = hc.err != 0 || (d->keep_hits && (hc.hit_count > ctx->graph_stage_cap ||
+                                                          hc.hit_count > ctx->graph_hits_cap));
+        if (!over) {
+            CK(cudaEventElapsedTime(&kms, ctx->e_k0, ctx->e_k1), "event time");
+            n_hits = d->keep_hits ? hc.hit_count : 0;
+            ev_offsets = ctx->ev_offsets.as<uint64_t>();
+            ev_stats = ctx->ev_stats2.as<cmpmc_sim_stats>();
+            launches += ctx->graph_launches;
+            return CMPMC_OK;
+        }
+        drop_graph(ctx);  // a ring, film buffer or hit buffer overflowed: rerun eagerly with more room
+        hc = Counters{};
+    }
     uint64_t grid = 1;
     {
         const int st = pool_grid(ctx, n_ph, &grid);
@@ -821,6 +859,43 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
     CK(launch_sink_finish(a, n, ev_offsets, ctx->cursor.as<unsigned long long>(), ctx->hits_out.as<cmpmc_sensor_hit>(),
                           n_hits, ctx->total.as<cmpmc_sim_stats>(), ctx->partials.as<cmpmc_sim_stats>(), s, &launches),
        "merge kernels");
+    // ---- capture the clean call for replay: counter and sink resets, unit map, the pool
+    // launch (between external timing events), the copy of the counters and the merge ------
+    if (graph_ok) {
+        drop_graph(ctx);
+        const uint64_t out_cap = ctx->hits_out.cap / sizeof(cmpmc_sensor_hit);
+        RunArgs ag = a;  // the transport's view (n_events = units), as the eager launch had it
+        ag.n_events = n_ph;
+        int gl = 0;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+        cudaError_t e = cudaMemsetAsync(ctx->ev_stats2.p, 0, n * sizeof(cmpmc_sim_stats), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->ev_nhits.p, 0, n * 8, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters.p, 0, sizeof(Counters), s);
+        if (e == cudaSuccess) e = launch_unit_event(a.ph_off, n, ctx->unit_event.as<uint32_t>(), s), ++gl;
+        if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->e_k0, s, cudaEventRecordExternal);
+        if (e == cudaSuccess) e = launch_pool(ctx, ag, grid, nullptr, s), ++gl;
+        if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->e_k1, s, cudaEventRecordExternal);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ctx->h_counters.p, ctx->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->cursor.p, 0, n * 8, s);
+        if (e == cudaSuccess)
+            e = launch_sink_finish(a, n, ev_offsets, ctx->cursor.as<unsigned long long>(),
+                                   ctx->hits_out.as<cmpmc_sensor_hit>(), out_cap, ctx->total.as<cmpmc_sim_stats>(),
+                                   ctx->partials.as<cmpmc_sim_stats>(), s, &gl);
+        const cudaError_t ec = cudaStreamEndCapture(s, &g);
+        if (e == cudaSuccess) e = ec;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            ctx->graph_exec = nullptr;
+            return cuda_fail(ctx, e, "graph capture");
+        }
+        ctx->graph_key = graph_key_of(ctx, d);
+        ctx->graph_hits_cap = out_cap;
+        ctx->graph_stage_cap = d->keep_hits ? a.hit_cap : 0;
+        ctx->graph_launches = gl;
+    }
     return CMPMC_OK;
 }
 
@@ -975,6 +1050,7 @@ int cmpmc_gpu_configure(cmpmc_gpu_ctx* ctx, int threads_per_block, int blocks_pe
     if (!ctx) return CMPMC_ERR_INVALID;
     if (threads_per_block < 0 || threads_per_block > 128 || (threads_per_block % 32) != 0 || blocks_per_sm < 0)
         return fail(ctx, CMPMC_ERR_INVALID, "threads_per_block must be a multiple of 32 in [32, 128]");
+    drop_graph(ctx);  // a captured call holds the launch configuration and kernel arguments
     if (threads_per_block) ctx->tpb = threads_per_block;
     if (blocks_per_sm) ctx->bps = blocks_per_sm;
     if (stack_capacity) {
@@ -992,6 +1068,7 @@ int cmpmc_gpu_set_electrode_mask(cmpmc_gpu_ctx* ctx, int surface, const cmpmc_el
     if (surface < 0 || surface > 2) return fail(ctx, CMPMC_ERR_INVALID, "surface must be 0 (top), 1 (bottom) or 2 (side)");
     if (n && !pads) return fail(ctx, CMPMC_ERR_INVALID, "pads is NULL");
     if (n > 4096) return fail(ctx, CMPMC_ERR_INVALID, "at most 4096 pads per surface");
+    drop_graph(ctx);  // the detector view (its mask pointers) is a kernel argument of a captured call
     std::vector<Pad> p(n);
     for (uint64_t i = 0; i < n; ++i) {
         if (pads[i].shape < 0 || pads[i].shape > 2)
@@ -1102,12 +1179,14 @@ int cmpmc_gpu_autotune(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* sample, int rep
 
 int cmpmc_gpu_configure_phases(cmpmc_gpu_ctx* ctx, uint32_t phase_steps) {
     if (!ctx) return CMPMC_ERR_INVALID;
+    drop_graph(ctx);
     ctx->phase_steps = phase_steps;
     return CMPMC_OK;
 }
 
 int cmpmc_gpu_configure_staging(cmpmc_gpu_ctx* ctx, int enable) {
     if (!ctx || enable < 0 || enable > 1) return CMPMC_ERR_INVALID;
+    drop_graph(ctx);
     ctx->stage_tables = enable;
     return CMPMC_OK;
 }
@@ -1116,6 +1195,7 @@ int cmpmc_gpu_configure_pool(cmpmc_gpu_ctx* ctx, int form, uint32_t ring_capacit
     if (!ctx || form < 0 || form > 3) return CMPMC_ERR_INVALID;
     if (ring_capacity != 0 && (ring_capacity < 64 || (ring_capacity & (ring_capacity - 1)) != 0))
         return fail(ctx, CMPMC_ERR_INVALID, "ring capacity: a power of two, at least 64");
+    drop_graph(ctx);
     ctx->pool = form;
     if (ring_capacity) {
         if (form == 1 || form == 3) ctx->sm_ring_cap = std::max<uint32_t>(ring_capacity, 2048);  // a block appends up to 2 x 512 at once
@@ -1133,6 +1213,7 @@ int cmpmc_gpu_configure_graph(cmpmc_gpu_ctx* ctx, int enable) {
 
 int cmpmc_gpu_configure_queue(cmpmc_gpu_ctx* ctx, uint64_t queue_capacity) {
     if (!ctx) return CMPMC_ERR_INVALID;
+    drop_graph(ctx);
     if (queue_capacity) ctx->queue_cap = std::max<uint64_t>(queue_capacity, 64);
     return CMPMC_OK;
 }
@@ -1143,6 +1224,7 @@ int cmpmc_gpu_set_mesh(cmpmc_gpu_ctx* ctx, const cmpmc_mesh* mesh) {
     ctx->last_error.clear();
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     CK(cudaStreamSynchronize(ctx->stream), "sync");
+    drop_graph(ctx);
     ctx->D.mesh.tet = nullptr;
     ctx->D.mesh.n_tets = 0;
     ctx->D.mesh32.tet = nullptr;
@@ -1179,6 +1261,7 @@ int cmpmc_gpu_set_mesh2d(cmpmc_gpu_ctx* ctx, const cmpmc_mesh2d* mesh) {
     ctx->last_error.clear();
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     CK(cudaStreamSynchronize(ctx->stream), "sync");
+    drop_graph(ctx);
     ctx->D.mesh2 = MeshView2{nullptr, 0, 1};
     ctx->D.mesh2_32 = MeshView2_32{nullptr, 0, 1};
     if (!mesh || mesh->rec.empty()) return CMPMC_OK;

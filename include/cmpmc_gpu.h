@@ -513,11 +513,12 @@ int cmpmc_gpu_memcpy(void* dst, const void* src, size_t bytes);
  * small queue only adds phases. 0 keeps the current value. */
 int cmpmc_gpu_configure_queue(cmpmc_gpu_ctx* ctx, uint64_t queue_capacity);
 /* CUDA-graph replay (no counterpart in the reference): with enable = 1, a batched-form call
- * of phonon events whose inputs and outputs stay on the device is captured after it ran
- * cleanly (counters, transport, merge and the copies of the counters and totals as one
- * graph) and replayed by later calls with the same descriptor pointers, sizes and
- * configuration: one graph launch per call. A replay whose buffers overflow falls back to
- * the eager call, which grows them and recaptures. */
+ * of phonon events whose inputs and outputs stay on the device (SM-phase pool, warp pool or
+ * inline form) is captured after it ran cleanly (counter resets, unit map, the transport
+ * launch, merge and the copies of the counters as one graph) and replayed by later calls
+ * with the same descriptor pointers, sizes and configuration: one graph launch per call. A
+ * replay whose buffers overflow falls back to the eager call, which grows them and
+ * recaptures; any configure / set call on the context drops the captured graph. */
 int cmpmc_gpu_configure_graph(cmpmc_gpu_ctx* ctx, int enable);
 
 /* Wavefront split of the batched form (no counterpart in the reference): a track that has

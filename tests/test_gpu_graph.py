@@ -72,6 +72,54 @@ def test_graph_replay_repeats_the_eager_call(ge_lattice):
     eng.configure_graph(False)
 
 
+def _event_sets(hits, offs):
+    """the hits of every event as a sorted multiset of records (the pool forms write an
+    event's hits in no fixed order)"""
+    raw = hits.view(np.uint8).reshape(len(hits), -1)
+    out = []
+    for e in range(len(offs) - 1):
+        rows = raw[int(offs[e]):int(offs[e + 1])]
+        out.append(sorted(r.tobytes() for r in rows))
+    return out
+
+
+@pytest.mark.parametrize("pool", [1, 2])
+def test_pool_graph_replay_repeats_the_eager_call(ge_lattice, pool):
+    """SM-phase pool (1) and warp pool (2): the call (counter resets, unit map, the persistent
+    transport launch, the merge) captured after a clean eager call and replayed as one graph
+    launch gives every event the same hits and the same integer counters."""
+    import cmpmc_b200 as cm
+    from cmpmc_b200 import _ffi
+    lib = _ffi.load()
+    eng = cm.SimulationEngine(ge_lattice, detector_for("c1"))
+    packed = eng.generate(workload_of("c1"), 300, WORKLOAD_SEED["c1"])
+    keep = []
+    d = _device_desc(packed, 7, keep)
+    d.form = _ffi.FORM_BATCHED_FP32
+    h = eng.context(0)
+    eng.configure_pool(pool)
+    eager, h0, o0 = _run(lib, h, d)
+    ref = _event_sets(h0, o0)
+    eng.configure_graph(True)
+    runs = [_run(lib, h, d) for _ in range(3)]  # eager + capture, then two graph launches
+    ints = [n for n, t in _ffi.SimStatsC._fields_ if t is C.c_uint64]
+    for out, hh, oo in runs:
+        assert np.array_equal(oo, o0)
+        assert _event_sets(hh, oo) == ref
+        for name in ints:
+            assert getattr(out.stats, name) == getattr(eager.stats, name), name
+        inj, dep = out.stats.total_injected_eV, out.stats.total_deposited_eV
+        assert abs(dep - eager.stats.total_deposited_eV) <= 1e-12 * inj
+        assert out.kernel_ms > 0
+    assert runs[1][0].kernel_launches == runs[2][0].kernel_launches
+    # another configuration drops the captured call: the next call runs eagerly again
+    eng.configure_staging(False)
+    after, h4, o4 = _run(lib, h, d)
+    assert _event_sets(h4, o4) == ref
+    eng.configure_staging(True)
+    eng.configure_graph(False)
+
+
 def test_autotune_keeps_results(ge_lattice):
     import cmpmc_b200 as cm
     eng = cm.SimulationEngine(ge_lattice, detector_for("c1"))
