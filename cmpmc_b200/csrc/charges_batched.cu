@@ -315,7 +315,9 @@ __device__ __forceinline__ uint64_t luke_key(uint64_t ckey, uint32_t idx) {
     return mix64(ckey ^ (0x9e3779b97f4a7c15ULL * (static_cast<uint64_t>(idx) + 1)));
 }
 
-__global__ void __launch_bounds__(128, 4) k_charges_fp32(const __grid_constant__ FCLat Lp,
+// (128, 5): 96 registers, five blocks per SM (pair drift of 200,000 events 467 -> 431 ms
+// against (128, 4) at 104 registers; (128, 6) at 80 registers 432 ms)
+__global__ void __launch_bounds__(128, 5) k_charges_fp32(const __grid_constant__ FCLat Lp,
                                                          const __grid_constant__ FCDet D,
                                                          const __grid_constant__ RunArgs a,
                                                          const __grid_constant__ ChargeArgs ca) {
