@@ -159,13 +159,14 @@ void drop_graph(cmpmc_gpu_ctx* ctx) {
     ctx->graph_key.clear();
 }
 
-// The call signature a captured graph is valid for: the descriptor's pointers and sizes,
+// The call signature a captured graph is valid for: the descriptor's pointers and sizes (the
+// number of phonon records too: it is read from the device offsets and baked into the launch),
 // the context's launch configuration, and the address and capacity of every device and host
 // buffer a captured call touches (a call of another form may grow, and so move, a shared
 // buffer without recapturing: the key then no longer matches and the next call runs eagerly
 // and recaptures).
-std::vector<uint64_t> graph_key_of(const cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d) {
-    std::vector<uint64_t> k = {d->n_events, d->first_event, reinterpret_cast<uint64_t>(d->rng_state),
+std::vector<uint64_t> graph_key_of(const cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, uint64_t n_ph) {
+    std::vector<uint64_t> k = {d->n_events, n_ph, d->first_event, reinterpret_cast<uint64_t>(d->rng_state),
                                reinterpret_cast<uint64_t>(d->injected_eV), reinterpret_cast<uint64_t>(d->phonon_offsets),
                                reinterpret_cast<uint64_t>(d->phonons), static_cast<uint64_t>(d->keep_hits), d->seed,
                                static_cast<uint64_t>(d->want_event_stats), static_cast<uint64_t>(d->kaplan_surrogate),
@@ -768,7 +769,7 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
     // ---- CUDA-graph replay: the same device-resident batch again (the persistent transport
     // launch with its counter resets, unit map and merge as one graph launch) ---------------
     const bool graph_ok = ctx->graph_enabled && n > 0 && n_ph > 0 && d->inputs_on_device && d->outputs_on_device;
-    if (graph_ok && ctx->graph_exec && ctx->graph_key == graph_key_of(ctx, d)) {
+    if (graph_ok && ctx->graph_exec && ctx->graph_key == graph_key_of(ctx, d, n_ph)) {
         CK(cudaGraphLaunch(ctx->graph_exec, s), "graph launch");
         CK(cudaStreamSynchronize(s), "graph");
         hc = *ctx->h_counters.as<Counters>();
@@ -891,7 +892,7 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
             ctx->graph_exec = nullptr;
             return cuda_fail(ctx, e, "graph capture");
         }
-        ctx->graph_key = graph_key_of(ctx, d);
+        ctx->graph_key = graph_key_of(ctx, d, n_ph);
         ctx->graph_hits_cap = out_cap;
         ctx->graph_stage_cap = d->keep_hits ? a.hit_cap : 0;
         ctx->graph_launches = gl;
@@ -1435,7 +1436,7 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
     } else {
         // ---- CUDA-graph replay: the same device-resident batch again ----------------------
         const bool graph_ok = ctx->graph_enabled && batched && n > 0 && d->inputs_on_device && d->outputs_on_device;
-        if (graph_ok && ctx->graph_exec && ctx->graph_key == graph_key_of(ctx, d)) {
+        if (graph_ok && ctx->graph_exec && ctx->graph_key == graph_key_of(ctx, d, n_ph)) {
             CK(cudaGraphLaunch(ctx->graph_exec, s), "graph launch");
             CK(cudaStreamSynchronize(s), "graph");
             hc = *ctx->h_counters.as<Counters>();
@@ -1599,7 +1600,7 @@ int cmpmc_gpu_run_events(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, cmpmc_run_
                 ctx->graph_exec = nullptr;
                 return cuda_fail(ctx, e, "graph capture");
             }
-            ctx->graph_key = graph_key_of(ctx, d);
+            ctx->graph_key = graph_key_of(ctx, d, n_ph);
             ctx->graph_hits_cap = out_cap;
             ctx->graph_launches = gl;
         }
