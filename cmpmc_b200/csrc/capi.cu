@@ -784,6 +784,7 @@ int run_pool_batched(cmpmc_gpu_ctx* ctx, const cmpmc_run_desc* d, RunArgs& a, ui
             return CMPMC_OK;
         }
         drop_graph(ctx);  // a ring, film buffer or hit buffer overflowed: rerun eagerly with more room
+        if (hc.err & (kErrQueue | kErrFilmQueue)) grow_pool(ctx, hc.err);
         hc = Counters{};
     }
     uint64_t grid = 1;
