@@ -1094,145 +1094,146 @@ __device__ __forceinline__ int pool_step(const FLat& L, const float* cdf, const 
         }
     }
     if (outcome == kStepOn) {
-    ++st.steps();
-    const float R = static_cast<float>(D.radius), H = static_cast<float>(D.half_z);
-    const float nu = static_cast<float>(trk.E) * L.inv_h_thz;
-    const float nu2 = nu * nu;
-    const float r_iso = L.b4 * (nu2 * nu2);
-    const float r_poly = trk.vmag * L.poly_inv;
-    const float r_down = (trk.mode == 0) ? L.a5 * (nu2 * nu2 * nu) : 0.0f;
-    const float r_tot = r_iso + r_poly + r_down;
-    const float d_phys = (r_tot > 1e-12f) ? (-logf(g.u()) * trk.vmag / r_tot) : __int_as_float(0x7f800000);
-    bh = fexit_d(R, H, trk.pos, trk.vg);
-    const bool bulk = d_phys < bh.d;
-    const float d = bulk ? d_phys : bh.d;
-    trk.pos = trk.pos + trk.vg * d;
-    trk.t += static_cast<double>(d / trk.vmag);
-    if (bulk) {
-        const float u_proc = g.u() * r_tot;
-        if (r_down > 0.0f && u_proc < r_down) {
-            FTrack t_c = trk, d_c;
-            R128 g_c = g;
-            pool_decay<kKin>(&L, cdf, &t_c, &d_c, &st, &g_c);
-            trk = t_c;
-            g = g_c;
-            out.daughter(pool_entry(d_c, draw_key(g), ev));
-        } else {
-            if (u_proc < r_down + r_iso) ++st.iso();
-            else ++st.poly();
-            trk.mode = fdos(L, g.u());
-            sample = 0;
-        }
-    } else {
-        bh.n = fnormal(bh.surf, trk.pos);
-        trk.bounces++;
-        const SurfHot hs = hot[bh.surf];
-        const Surface& s = D.surf[bh.surf];  // read by the out-of-line calls only
-        bool enter = false;
-        int ch_id = -1;
-        bool active_pad = true;
-        if (hs.flags & kHotMask) {  // electrode mask (engine.hpp:483-488)
-            R128 g_c = g;
-            ch_id = mask_call(s.pads, s.n_pads, trk.pos.x, trk.pos.y, &g_c);
-            g = g_c;
-            active_pad = ch_id >= 0;
-        }
-        if (active_pad && (hs.flags & kHotFilm) && g.u() < hs.prob_abs) {
-            const float p_enter = (hs.flags & kHotAmm) ? amm_call(&s, trk.mode == 0, fdot(trk.k, bh.n)) : hs.p_enter;
-            enter = g.u() < p_enter;
-        }
-        if (enter) {
-            R128 g_c = g;
-            const int film = film_quick<kSur>(&s.film, trk.E, &g_c);
-            g = g_c;
-            if (film == kFilmAbsorbed) {
-                const double wedep = trk.E * trk.w;
-                ++st.hits();
-                st.dep() += wedep;
-                cmpmc_sensor_hit h;
-                h.pos[0] = trk.pos.x; h.pos[1] = trk.pos.y; h.pos[2] = trk.pos.z;
-                h.time = trk.t;
-                h.edep = wedep;
-                h.incident_energy = trk.E;
-                h.surface_id = static_cast<uint8_t>(bh.surf);
-                h.excitation = 0;
-                h.mode = static_cast<uint8_t>(trk.mode);
-                h._pad = 0;
-                h.channel_id = ch_id;
-                out.hit(ev, h);
-                outcome = kStepEnd;
-            } else if (film == kFilmCascade) {
-                FilmRec fr;
-                fr.px = trk.pos.x; fr.py = trk.pos.y; fr.pz = trk.pos.z;
-                fr.w = trk.w;
-                fr.E = trk.E;
-                fr.t = trk.t;
-                fr.key = draw_key(g);
-                fr.ev = ev;
-                fr.ch_id = ch_id;
-                fr.bounces = trk.bounces;
-                fr.surf = static_cast<uint8_t>(bh.surf);
-                fr.mode = static_cast<uint8_t>(trk.mode);
-                fr.pad0 = fr.pad1 = 0;
-                out.film(fr);
-                outcome = kStepFilm;
+        ++st.steps();
+        const float R = static_cast<float>(D.radius), H = static_cast<float>(D.half_z);
+        const float nu = static_cast<float>(trk.E) * L.inv_h_thz;
+        const float nu2 = nu * nu;
+        const float r_iso = L.b4 * (nu2 * nu2);
+        const float r_poly = trk.vmag * L.poly_inv;
+        const float r_down = (trk.mode == 0) ? L.a5 * (nu2 * nu2 * nu) : 0.0f;
+        const float r_tot = r_iso + r_poly + r_down;
+        const float d_phys = (r_tot > 1e-12f) ? (-logf(g.u()) * trk.vmag / r_tot) : __int_as_float(0x7f800000);
+        bh = fexit_d(R, H, trk.pos, trk.vg);
+        const bool bulk = d_phys < bh.d;
+        const float d = bulk ? d_phys : bh.d;
+        trk.pos = trk.pos + trk.vg * d;
+        trk.t += static_cast<double>(d / trk.vmag);
+        if (bulk) {
+            const float u_proc = g.u() * r_tot;
+            if (r_down > 0.0f && u_proc < r_down) {
+                FTrack t_c = trk, d_c;
+                R128 g_c = g;
+                pool_decay<kKin>(&L, cdf, &t_c, &d_c, &st, &g_c);
+                trk = t_c;
+                g = g_c;
+                out.daughter(pool_entry(d_c, draw_key(g), ev));
             } else {
-                // re-emitted unchanged: back into the crystal (bounces kept), a DOS mode and an
-                // inward Lambertian direction from the shared sampling below
-                trk.pos = trk.pos + bh.n * kNudge;
+                if (u_proc < r_down + r_iso) ++st.iso();
+                else ++st.poly();
                 trk.mode = fdos(L, g.u());
-                sample = 1;
+                sample = 0;
             }
-        } else if (g.u() > hs.prob_refl) {
-            ++st.killed();
-            st.esc() += trk.E * trk.w;
-            outcome = kStepEnd;
-        } else {  // a surface reflection
-            ++st.refl();
-            trk.pos = trk.pos + bh.n * kNudge;
-            float p_anh, p_anh_spec;
-            if (hs.flags & kHotSplitConst) {
-                p_anh = hs.p_anh;
-                p_anh_spec = hs.p_anh_spec;
-            } else {
-                const Split sp = reflection_split(s, trk.E);
-                p_anh = static_cast<float>(sp.p_anh);
-                p_anh_spec = static_cast<float>(sp.p_anh + sp.p_spec);
+        } else {
+            bh.n = fnormal(bh.surf, trk.pos);
+            trk.bounces++;
+            const SurfHot hs = hot[bh.surf];
+            const Surface& s = D.surf[bh.surf];  // read by the out-of-line calls only
+            bool enter = false;
+            int ch_id = -1;
+            bool active_pad = true;
+            if (hs.flags & kHotMask) {  // electrode mask (engine.hpp:483-488)
+                R128 g_c = g;
+                ch_id = mask_call(s.pads, s.n_pads, trk.pos.x, trk.pos.y, &g_c);
+                g = g_c;
+                active_pad = ch_id >= 0;
             }
-            const float u_refl = g.u();
-            if (u_refl < p_anh) {
-                ++st.down();
-                const bool tt = g.u() < L.fTT;
-                const float x = fcdf_any(tt ? cdf + kNCdf : cdf, g);
-                const int m1 = tt ? ftrans(L, g) : 0;
-                const int m2 = ftrans(L, g);
-                FTrack dtr;
-                FKin k2kin;
-                dtr.k = finward<kKin>(L, m2, bh.n, g, k2kin);
-                dtr.pos = trk.pos;
-                dtr.vg = k2kin.dir;
-                dtr.vmag = k2kin.mag;
-                dtr.E = (1.0 - static_cast<double>(x)) * trk.E;
-                dtr.t = trk.t;
-                dtr.w = trk.w;
-                dtr.bounces = 0;
-                dtr.mode = m2;
-                out.daughter(pool_entry(dtr, draw_key(g), ev));
-                trk.E = static_cast<double>(x) * trk.E;
-                trk.mode = m1;
-                sample = 1;
-            } else if (u_refl < p_anh_spec) {
-                F3 kr = trk.k - bh.n * (2.0f * fdot(trk.k, bh.n));
-                FKin kin = fmapk<kKin>(L, trk.mode, kr);
-                if (fdot(kin.dir, bh.n) <= 1e-6f) kr = finward<kKin>(L, trk.mode, bh.n, g, kin);
-                trk.k = kr;
-                trk.vg = kin.dir;
-                trk.vmag = kin.mag;
-            } else {
-                sample = 1;
+            if (active_pad && (hs.flags & kHotFilm) && g.u() < hs.prob_abs) {
+                const float p_enter =
+                    (hs.flags & kHotAmm) ? amm_call(&s, trk.mode == 0, fdot(trk.k, bh.n)) : hs.p_enter;
+                enter = g.u() < p_enter;
+            }
+            if (enter) {
+                R128 g_c = g;
+                const int film = film_quick<kSur>(&s.film, trk.E, &g_c);
+                g = g_c;
+                if (film == kFilmAbsorbed) {
+                    const double wedep = trk.E * trk.w;
+                    ++st.hits();
+                    st.dep() += wedep;
+                    cmpmc_sensor_hit h;
+                    h.pos[0] = trk.pos.x; h.pos[1] = trk.pos.y; h.pos[2] = trk.pos.z;
+                    h.time = trk.t;
+                    h.edep = wedep;
+                    h.incident_energy = trk.E;
+                    h.surface_id = static_cast<uint8_t>(bh.surf);
+                    h.excitation = 0;
+                    h.mode = static_cast<uint8_t>(trk.mode);
+                    h._pad = 0;
+                    h.channel_id = ch_id;
+                    out.hit(ev, h);
+                    outcome = kStepEnd;
+                } else if (film == kFilmCascade) {
+                    FilmRec fr;
+                    fr.px = trk.pos.x; fr.py = trk.pos.y; fr.pz = trk.pos.z;
+                    fr.w = trk.w;
+                    fr.E = trk.E;
+                    fr.t = trk.t;
+                    fr.key = draw_key(g);
+                    fr.ev = ev;
+                    fr.ch_id = ch_id;
+                    fr.bounces = trk.bounces;
+                    fr.surf = static_cast<uint8_t>(bh.surf);
+                    fr.mode = static_cast<uint8_t>(trk.mode);
+                    fr.pad0 = fr.pad1 = 0;
+                    out.film(fr);
+                    outcome = kStepFilm;
+                } else {
+                    // re-emitted unchanged: back into the crystal (bounces kept), a DOS mode and an
+                    // inward Lambertian direction from the shared sampling below
+                    trk.pos = trk.pos + bh.n * kNudge;
+                    trk.mode = fdos(L, g.u());
+                    sample = 1;
+                }
+            } else if (g.u() > hs.prob_refl) {
+                ++st.killed();
+                st.esc() += trk.E * trk.w;
+                outcome = kStepEnd;
+            } else {  // a surface reflection
+                ++st.refl();
+                trk.pos = trk.pos + bh.n * kNudge;
+                float p_anh, p_anh_spec;
+                if (hs.flags & kHotSplitConst) {
+                    p_anh = hs.p_anh;
+                    p_anh_spec = hs.p_anh_spec;
+                } else {
+                    const Split sp = reflection_split(s, trk.E);
+                    p_anh = static_cast<float>(sp.p_anh);
+                    p_anh_spec = static_cast<float>(sp.p_anh + sp.p_spec);
+                }
+                const float u_refl = g.u();
+                if (u_refl < p_anh) {
+                    ++st.down();
+                    const bool tt = g.u() < L.fTT;
+                    const float x = fcdf_any(tt ? cdf + kNCdf : cdf, g);
+                    const int m1 = tt ? ftrans(L, g) : 0;
+                    const int m2 = ftrans(L, g);
+                    FTrack dtr;
+                    FKin k2kin;
+                    dtr.k = finward<kKin>(L, m2, bh.n, g, k2kin);
+                    dtr.pos = trk.pos;
+                    dtr.vg = k2kin.dir;
+                    dtr.vmag = k2kin.mag;
+                    dtr.E = (1.0 - static_cast<double>(x)) * trk.E;
+                    dtr.t = trk.t;
+                    dtr.w = trk.w;
+                    dtr.bounces = 0;
+                    dtr.mode = m2;
+                    out.daughter(pool_entry(dtr, draw_key(g), ev));
+                    trk.E = static_cast<double>(x) * trk.E;
+                    trk.mode = m1;
+                    sample = 1;
+                } else if (u_refl < p_anh_spec) {
+                    F3 kr = trk.k - bh.n * (2.0f * fdot(trk.k, bh.n));
+                    FKin kin = fmapk<kKin>(L, trk.mode, kr);
+                    if (fdot(kin.dir, bh.n) <= 1e-6f) kr = finward<kKin>(L, trk.mode, bh.n, g, kin);
+                    trk.k = kr;
+                    trk.vg = kin.dir;
+                    trk.vmag = kin.mag;
+                } else {
+                    sample = 1;
+                }
             }
         }
-    }
     }
     __syncwarp(m_in);
     // shared new-direction path: isotropic (bulk scatter) or Lambertian about the inward
