@@ -13,10 +13,13 @@ from the library's autotuner (results do not depend on it).
 
   value  primary phonon tracks / s, inputs resident on the device, device-timed (CUDA
          events on the library's stream), max over ranks
-  e2e    the same through the public API with host buffers: pinned host inputs copied in
-         and every hit, the hit offsets and the statistics copied back, each step, one call
-         at a time (e2e_with_generator adds the host generator's time per step;
-         --pipeline adds e2e_two_calls_in_flight: two contexts on two host threads)
+  e2e    the same through the public API: every step copies its inputs in from pinned host
+         memory and its hits, hit offsets and statistics out to pinned host memory. On one
+         GPU two contexts take the steps in turn and a step's output copy (a copy stream)
+         overlaps the next step's call; the outputs are checked against the device-resident
+         call. e2e_one_call_at_a_time: host buffers through the call itself, one call at a
+         time (e2e_with_generator adds the host generator's time per step; --pipeline adds
+         e2e_two_calls_in_flight: two contexts on two host threads)
   plain_fp64  the plain FP64 form (bit-exact event streams) on the same workload, one step
   batched_fp64  the same SM-phase pool computed in FP64 throughout on the same substreams
          (pool form 3), one step: fp32_over_fp64 is what the FP32 form gains
@@ -252,6 +255,104 @@ def published_workload(cm, lat, dev: int, n: int, lib) -> dict:
     return out
 
 
+class _DevView:
+    """A device allocation of the library seen as a flat uint8 array (CUDA array interface),
+    so that torch can queue a copy of it on one of its streams without owning it."""
+
+    def __init__(self, ptr: int, nbytes: int):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (int(ptr), False),
+                                         "version": 2}
+
+
+def overlapped_e2e(args, cm, lat, det, dev: int, lib, h, run_on, hp, packed, desc, ref) -> dict:
+    """End-to-end steps whose output copies overlap the next step's transport: two contexts in
+    turn, inputs copied from pinned host memory into the context's device input buffers, the
+    call leaving its outputs on the device, and the copy of the hits and offsets to pinned host
+    memory queued on a copy stream while the other context's call runs."""
+    import torch
+    eng_b = cm.SimulationEngine(lat, det)
+    h_b = eng_b.context(dev)
+    if args.queue_capacity or args.stack_capacity:
+        eng_b.configure(dev, stack_capacity=args.stack_capacity, queue_capacity=args.queue_capacity)
+    eng_b.configure_pool({"sm_pool": 1, "warp_pool": 2, "rounds": 0}[args.launch], device=dev)
+    if args.no_stage:
+        eng_b.configure_staging(False, device=dev)
+    ctxs = (h, h_b)
+    n = args.events
+    cuda = f"cuda:{dev}"
+    dev_in = [[torch.empty(t.numel(), dtype=torch.uint8, device=cuda) for t in hp] for _ in range(2)]
+    descs = []
+    for s in range(2):
+        d = desc(True)
+        d.rng_state, d.injected_eV = dev_in[s][0].data_ptr(), dev_in[s][1].data_ptr()
+        d.phonon_offsets, d.phonons = dev_in[s][2].data_ptr(), dev_in[s][3].data_ptr()
+        descs.append(d)
+    h2d_s, d2h_s = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+    kChunk = 16 << 20
+
+    def inputs(s):
+        with torch.cuda.stream(h2d_s):
+            for k in range(4):
+                dev_in[s][k].copy_(hp[k], non_blocking=True)
+        h2d_s.synchronize()
+
+    n_hits0 = 0
+    for s in range(2):  # warm-up: the contexts size their buffers
+        inputs(s)
+        n_hits0 = max(n_hits0, int(run_on(ctxs[s], descs[s]).n_hits))
+    cap = (n_hits0 + n_hits0 // 8 + 1024) * 56
+    host_hits = [torch.empty(cap, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    host_offs = [torch.empty((n + 1) * 8, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    done = [None, None]
+    last = None
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        s = i % 2
+        if done[s] is not None:
+            done[s].synchronize()  # this context's previous copy has finished
+        inputs(s)
+        o = run_on(ctxs[s], descs[s])
+        nh = int(o.n_hits) * 56
+        if nh > cap:
+            raise RuntimeError("host hit buffer too small")
+        with torch.cuda.stream(d2h_s):
+            # in 16 MiB pieces: the next call's own small device-to-host reads (the batch's
+            # track count, its counters) take the same copy engine and would otherwise wait
+            # behind the whole 1.5 GB copy
+            if nh:
+                hv = torch.as_tensor(_DevView(o.hits, nh), device=cuda)
+                for a0 in range(0, nh, kChunk):
+                    a1 = min(nh, a0 + kChunk)
+                    host_hits[s][a0:a1].copy_(hv[a0:a1], non_blocking=True)
+            host_offs[s].copy_(torch.as_tensor(_DevView(o.hit_offsets, (n + 1) * 8), device=cuda), non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(d2h_s)
+        done[s] = ev
+        last = (s, int(o.n_hits))
+    for ev in done:
+        if ev is not None:
+            ev.synchronize()
+    ms = 1e3 * (time.perf_counter() - t0) / args.steps
+    s, nh = last
+    offs = host_offs[s].numpy().view(np.uint64)
+    checked = None
+    if ref is not None:
+        # the offsets exactly, the hits as an order-free checksum (a modular sum of their 8-byte
+        # words: the hits of an event come in no fixed order)
+        got = host_hits[s][:nh * 56].numpy().view(np.uint64)
+        want = np.ascontiguousarray(ref["hits"]).view(np.uint8).reshape(-1).view(np.uint64)
+        checked = bool(np.array_equal(offs, ref["offsets"]) and nh == len(ref["hits"]) and
+                       int(got.sum(dtype=np.uint64)) == int(want.sum(dtype=np.uint64)))
+        if not checked:
+            raise RuntimeError("overlapped e2e outputs differ from the device-resident call")
+    return {"value": int(packed.phonon_offsets[-1]) / (ms * 1e-3), "unit": UNIT,
+            "h2d_bytes_per_step": int(sum(t.numel() for t in hp)), "d2h_bytes_per_step": nh * 56 + (n + 1) * 8 + 208,
+            "ms_per_step": ms, "checked_against_device_resident_call": checked,
+            "how": "two contexts in turn on one host thread; each step's hit and offset copy to pinned host "
+                   "memory runs on a copy stream during the next step's call; wall clock over all K steps"}
+
+
 def recoil_batch(cm, lat, dev: int, n: int) -> None:
     """The uneven recoil batch (electron recoils of 10 eV-10 keV, log-uniform, split by
     EnergyPartition::partition_deposit with up to 4,096 pairs, every Luke phonon tracked, in
@@ -302,6 +403,8 @@ def main() -> None:
     ap.add_argument("--no-matched", action="store_true", help="skip the matched-statistics check")
     ap.add_argument("--pipeline", action="store_true",
                     help="also time e2e with two calls in flight (two contexts on two host threads)")
+    ap.add_argument("--no-overlap", action="store_true",
+                    help="e2e one call at a time only (no output copy overlapping the next call)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the batched FP64 comparison step")
     ap.add_argument("--no-stage", action="store_true",
                     help="decay CDF tables read from global memory instead of the TMA-staged shared copy")
@@ -556,6 +659,20 @@ def main() -> None:
                     "d2h_bytes_per_step": d2h, "ms_per_step": pipe_ms, "calls_in_flight": 2,
                     "how": "two contexts on two host threads, steps taken in turn; wall clock over all K steps"}
 
+    # e2e with each step's output copy overlapping the next step's transport (one host thread,
+    # two contexts in turn): a step copies its inputs from pinned host memory into the device
+    # input buffers of its context, calls run_events with the outputs left on the device, and
+    # queues the device-to-host copy of its hits and offsets on a copy stream; the next step's
+    # call (the other context, whose buffers the copy does not touch) runs meanwhile. A context
+    # is reused only after its previous copy has finished. Checked against the device-resident
+    # call: the same offsets and hit count.
+    e2e_overlap = None
+    if world == 1 and not args.no_overlap:
+        try:
+            e2e_overlap = overlapped_e2e(args, cm, lat, det, dev, lib, h, run_on, hp, packed, desc, batched_res)
+        except Exception as e:  # reported in the line; the one-call-at-a-time figure stands
+            e2e_overlap = {"error": str(e)}
+
     # plain FP64 form on the same workload (bit-exact event streams), one step
     plain = None
     plain_res = None
@@ -612,7 +729,8 @@ def main() -> None:
         "kernel_ms_per_step": kernel_ms,
         "steps_per_s": world * steps_per_launch / (kernel_ms * 1e-3),
         "hits_per_step": hits_total / args.steps,
-        "e2e": e2e_one,
+        "e2e": e2e_overlap if (e2e_overlap is not None and "error" not in e2e_overlap) else e2e_one,
+        "e2e_one_call_at_a_time": e2e_one,
         "e2e_with_generator": {"value": world * n_prim / ((e2e_step + gen_ms) * 1e-3), "unit": UNIT,
                                "ms_per_step": e2e_step + gen_ms, "generator_ms": gen_ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -629,6 +747,8 @@ def main() -> None:
     }
     if e2e_pipe is not None:
         line["e2e_two_calls_in_flight"] = e2e_pipe
+    if e2e_overlap is not None and "error" in e2e_overlap:
+        line["e2e_overlapped_copies"] = e2e_overlap
     if plain is not None:
         line["plain_fp64"] = plain
         line["batched_over_plain"] = value / plain["value"]
